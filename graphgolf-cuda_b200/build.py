@@ -1,0 +1,92 @@
+"""Build the engine's shared libraries in-tree (sm_100a).
+
+    python graphgolf-cuda_b200/build.py          # engine + reference shim (+ oracle)
+
+Outputs (git-ignored, but shipped with the working tree):
+  graphgolf-cuda_b200/libggb200.so      C ABI of include/gg.h (CUDA engine)
+  graphgolf-cuda_b200/libgg_refshim.so  the reference calculator classes defined on
+                                        top of the C ABI (needs the reference headers
+                                        at build time; skipped when they are absent)
+"""
+from __future__ import annotations
+
+import os
+import shutil
+import subprocess
+import sys
+
+PKG = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(PKG)
+CSRC = os.path.join(PKG, "csrc")
+INC = os.path.join(ROOT, "include")
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+REF = os.environ.get("GG_REFERENCE_TREE", "/root/reference")
+
+ENGINE_SRC = ["gg_engine.cu", "gg_gen.cpp"]
+ENGINE_LIB = os.path.join(PKG, "libggb200.so")
+SHIM_LIB = os.path.join(PKG, "libgg_refshim.so")
+
+
+def nvcc():
+    for p in (shutil.which("nvcc"), "/usr/local/cuda/bin/nvcc"):
+        if p and os.path.exists(p):
+            return p
+    raise RuntimeError("nvcc not found")
+
+
+def _run(cmd):
+    print(" ".join(cmd), flush=True)
+    subprocess.run(cmd, check=True)
+
+
+def _stale(target, sources):
+    if not os.path.exists(target):
+        return True
+    t = os.path.getmtime(target)
+    return any(os.path.getmtime(s) > t for s in sources)
+
+
+def build_engine(force=False, extra=()):
+    srcs = [os.path.join(CSRC, s) for s in ENGINE_SRC]
+    deps = srcs + [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".cuh", ".h"))]
+    deps.append(os.path.join(INC, "gg.h"))
+    if not force and not _stale(ENGINE_LIB, deps):
+        return ENGINE_LIB
+    cmd = [nvcc(), "-O3", "-std=c++17", *ARCH, "-lineinfo", "-Xcompiler", "-fPIC,-O3",
+           "-shared", "-I", INC, "-I", CSRC, "-o", ENGINE_LIB, *srcs, *extra]
+    _run(cmd)
+    return ENGINE_LIB
+
+
+def build_shim(force=False):
+    """libgg_refshim.so: compiled against the reference headers in place."""
+    src = os.path.join(CSRC, "refshim.cpp")
+    hdr = os.path.join(REF, "cudacode", "cudaASPLconv.hpp")
+    if not os.path.exists(src) or not os.path.exists(hdr):
+        return None
+    if not force and not _stale(SHIM_LIB, [src, ENGINE_LIB]):
+        return SHIM_LIB
+    cmd = ["g++", "-O2", "-std=c++17", "-fPIC", "-shared",
+           "-I", INC, "-I", os.path.join(REF, "cudacode"), "-I", os.path.join(REF, "cppcode"),
+           "-o", SHIM_LIB, src, "-L", PKG, "-lggb200", "-Wl,-rpath,$ORIGIN"]
+    _run(cmd)
+    return SHIM_LIB
+
+
+def build_oracle():
+    """The oracle (test infrastructure) and, when the reference tree is here,
+    the reference's own calculators in oracle/_ref/."""
+    od = os.path.join(ROOT, "oracle")
+    _run(["make", "-s", "-C", od, "liboracle.so"])
+    if os.path.isdir(os.path.join(REF, "cppcode")):
+        _run(["make", "-s", "-C", od, f"REF={REF}", "ref"])
+
+
+def build_all(force=False):
+    build_engine(force)
+    build_shim(force)
+    build_oracle()
+
+
+if __name__ == "__main__":
+    build_all(force="--force" in sys.argv)

@@ -1,0 +1,706 @@
+// gg_engine.cu -- host side of the engine and the C ABI declared in include/gg.h.
+//
+// One gg_engine owns every device and pinned buffer of one calculator, sized at
+// construction from its form and dimensions, the way the reference calculators
+// size theirs in their constructors (cudaASPLconv.cu:122-137,
+// cudaASPLgraph.cu:114-127).  An evaluation is:
+//   H2D of the packed table -> expand_kernel (lifted forms) -> one cooperative
+//   bfs_batch_kernel launch per source batch -> one D2H of the level counters
+//   -> exact host fold into gg_result -> the reference's return convention.
+// There is no per-level host round trip: the level loop, its termination test
+// and the connectivity test live on the device.
+#include "gg.h"
+#include "gg_kernels.cuh"
+
+#include <algorithm>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <string>
+#include <vector>
+
+using gg::BfsArgs;
+using gg::Ctl;
+using gg::ExpandArgs;
+using gg::FastDiv;
+
+namespace {
+
+thread_local std::string g_err;
+
+gg_status fail(gg_status s, const std::string &msg) {
+    g_err = msg;
+    return s;
+}
+
+#define GG_CK(call)                                                                     \
+    do {                                                                                \
+        cudaError_t e_ = (call);                                                        \
+        if (e_ != cudaSuccess) {                                                        \
+            (void)cudaGetLastError();                                                   \
+            return fail(e_ == cudaErrorMemoryAllocation ? GG_OUT_OF_MEMORY : GG_CUDA_ERROR, \
+                        std::string(#call) + ": " + cudaGetErrorString(e_));            \
+        }                                                                               \
+    } while (0)
+
+enum Form { FORM_GRAPH = 0, FORM_PART = 1, FORM_PIECE = 2, FORM_BOX = 3 };
+
+constexpr int kBeamerRows = 1000000;   // cudaASPLbeamer.cu:10-12
+constexpr int kBeamerLevels = 7;       // cudaASPLbeamer.cu:17
+constexpr int kSentinel = 100000000;   // cudaASPLconv.cu:207
+
+int env_int(const char *name, int dflt) {
+    const char *s = std::getenv(name);
+    return (s && *s) ? std::atoi(s) : dflt;
+}
+
+// Host-side fault injection for the failure-path tests (GG_FAULT_INJECT):
+//   "barrier" -- the grid barrier waits for one block more than is launched, so
+//                its bounded wait runs out and the call returns GG_TIMEOUT;
+//   "alloc"   -- engine creation reports an allocation failure;
+//   "launch"  -- the BFS launch reports a CUDA error before anything is enqueued.
+// Nothing here faults, traps or hangs the GPU.
+bool fault(const char *what) {
+    const char *s = std::getenv("GG_FAULT_INJECT");
+    return s && std::strcmp(s, what) == 0;
+}
+
+}  // namespace
+
+struct gg_engine {
+    int form = FORM_PART;
+    int device = 0;
+    int N = 0, M = 0, d = 0, rows = 0;
+    int dims[6] = {0, 0, 0, 0, 0, 0};    // Nx Ny Nz Mx My Mz
+    uint64_t scale = 1;
+    size_t table_elems = 0;
+    std::vector<int32_t> reps;           // source vertex ids, in source order
+
+    // plan
+    int batch_bits = 0;                  // sources per batch (multiple of 128)
+    int nC = 0;                          // uint4 chunks per row
+    uint32_t items = 0;
+    int grid = 0;
+    int bu_permille = 500;
+    long long wait_ns = 10ll * 1000 * 1000 * 1000;
+    int cap_alloc = 0;                   // levels the counter arrays hold
+    int nb_alloc = 0;                    // batches the counter arrays hold
+
+    // device
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    int32_t *d_table = nullptr, *d_adj = nullptr, *d_src = nullptr;
+    int *d_bad = nullptr;
+    uint4 *d_V = nullptr, *d_F0 = nullptr, *d_F1 = nullptr;
+    uint32_t *d_fl0 = nullptr, *d_fl1 = nullptr;
+    unsigned long long *d_counts = nullptr;
+    unsigned *d_masks = nullptr;
+    Ctl *d_ctl = nullptr;
+    // pinned host
+    int32_t *h_table = nullptr;
+    unsigned long long *h_counts = nullptr;
+    unsigned *h_masks = nullptr;
+    Ctl *h_ctl = nullptr;
+    int *h_bad = nullptr;
+
+    double last_ms = 0.0;
+    int last_launches = 0;
+    uint64_t last_h2d = 0, last_d2h = 0;
+};
+
+namespace {
+
+void free_batch_buffers(gg_engine *e) {
+    cudaFree(e->d_V); cudaFree(e->d_F0); cudaFree(e->d_F1);
+    cudaFree(e->d_fl0); cudaFree(e->d_fl1);
+    e->d_V = e->d_F0 = e->d_F1 = nullptr;
+    e->d_fl0 = e->d_fl1 = nullptr;
+}
+
+void free_counters(gg_engine *e) {
+    cudaFree(e->d_counts); cudaFree(e->d_masks); cudaFree(e->d_ctl);
+    cudaFreeHost(e->h_counts); cudaFreeHost(e->h_masks); cudaFreeHost(e->h_ctl);
+    e->d_counts = nullptr; e->d_masks = nullptr; e->d_ctl = nullptr;
+    e->h_counts = nullptr; e->h_masks = nullptr; e->h_ctl = nullptr;
+    e->cap_alloc = e->nb_alloc = 0;
+}
+
+void destroy_all(gg_engine *e) {
+    if (!e) return;
+    cudaSetDevice(e->device);
+    if (e->stream) cudaStreamSynchronize(e->stream);
+    free_batch_buffers(e);
+    free_counters(e);
+    cudaFree(e->d_table); cudaFree(e->d_adj); cudaFree(e->d_src); cudaFree(e->d_bad);
+    cudaFreeHost(e->h_table); cudaFreeHost(e->h_bad);
+    if (e->ev0) cudaEventDestroy(e->ev0);
+    if (e->ev1) cudaEventDestroy(e->ev1);
+    if (e->stream) cudaStreamDestroy(e->stream);
+    delete e;
+}
+
+int kernel_degree_slot(int d) {
+    switch (d) {
+        case 3: case 4: case 6: case 8: case 12: case 16: return d;
+        default: return 0;
+    }
+}
+
+void *kernel_for(int d) {
+    switch (kernel_degree_slot(d)) {
+        case 3: return (void *)gg::bfs_batch_kernel<3>;
+        case 4: return (void *)gg::bfs_batch_kernel<4>;
+        case 6: return (void *)gg::bfs_batch_kernel<6>;
+        case 8: return (void *)gg::bfs_batch_kernel<8>;
+        case 12: return (void *)gg::bfs_batch_kernel<12>;
+        case 16: return (void *)gg::bfs_batch_kernel<16>;
+        default: return (void *)gg::bfs_batch_kernel<0>;
+    }
+}
+
+// Source-batch plan: batch width, chunks per row, grid size.
+gg_status plan(gg_engine *e, int want_bits) {
+    const int n_src = (int)e->reps.size();
+    int bits;
+    if (want_bits > 0) {
+        bits = want_bits;
+    } else {
+        const int env = env_int("GG_BATCH_SOURCES", 0);
+        if (env > 0) {
+            bits = env;
+        } else {
+            // All sources in one batch while the three bitsets stay within a
+            // fixed device budget; otherwise the widest batch that fits.
+            const double budget = 6.0e9;
+            const double per_bit = 3.0 * e->rows / 8.0;
+            long long fit = (long long)(budget / per_bit);
+            bits = (int)std::min<long long>(fit, n_src);
+        }
+    }
+    bits = std::max(128, ((std::min(bits, std::max(n_src, 1)) + 127) / 128) * 128);
+    const long long items = (long long)e->rows * (bits / 128);
+    if (items >= (1ll << 31)) return fail(GG_BAD_ARG, "rows x batch width exceeds 2^31 uint4 chunks");
+    if (bits != e->batch_bits) {
+        free_batch_buffers(e);
+        e->batch_bits = bits;
+        e->nC = bits / 128;
+        e->items = (uint32_t)items;
+        const size_t vbytes = (size_t)items * sizeof(uint4);
+        const size_t fwords = (size_t)((items + 31) / 32);
+        GG_CK(cudaMalloc(&e->d_V, vbytes));
+        GG_CK(cudaMalloc(&e->d_F0, vbytes));
+        GG_CK(cudaMalloc(&e->d_F1, vbytes));
+        GG_CK(cudaMalloc(&e->d_fl0, fwords * 4));
+        GG_CK(cudaMalloc(&e->d_fl1, fwords * 4));
+    }
+    int per_sm = 0, sms = 0;
+    GG_CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, e->device));
+    GG_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel_for(e->d), gg::kBlock, 0));
+    if (per_sm < 1) return fail(GG_CUDA_ERROR, "BFS kernel cannot be resident");
+    const long long tiles = ((long long)e->items + 31) / 32;
+    const long long want = (tiles + (gg::kBlock / 32) - 1) / (gg::kBlock / 32);
+    e->grid = (int)std::max<long long>(1, std::min<long long>((long long)per_sm * sms, want));
+    return GG_OK;
+}
+
+gg_status ensure_counters(gg_engine *e, int cap, int nb) {
+    if (cap <= e->cap_alloc && nb <= e->nb_alloc) return GG_OK;
+    cap = std::max(cap, e->cap_alloc);
+    nb = std::max(nb, e->nb_alloc);
+    free_counters(e);
+    const size_t n = (size_t)(cap + 1) * nb;
+    GG_CK(cudaMalloc(&e->d_counts, n * sizeof(unsigned long long)));
+    GG_CK(cudaMalloc(&e->d_masks, n * sizeof(unsigned)));
+    GG_CK(cudaMalloc(&e->d_ctl, (size_t)nb * sizeof(Ctl)));
+    GG_CK(cudaMallocHost(&e->h_counts, n * sizeof(unsigned long long)));
+    GG_CK(cudaMallocHost(&e->h_masks, n * sizeof(unsigned)));
+    GG_CK(cudaMallocHost(&e->h_ctl, (size_t)nb * sizeof(Ctl)));
+    e->cap_alloc = cap;
+    e->nb_alloc = nb;
+    return GG_OK;
+}
+
+gg_status create_common(gg_engine *e) {
+    if (fault("alloc")) return fail(GG_OUT_OF_MEMORY, "injected allocation failure");
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+        (void)cudaGetLastError();
+        return fail(GG_NO_DEVICE, "no CUDA device");
+    }
+    if (e->device < 0 || e->device >= ndev) return fail(GG_NO_DEVICE, "device index out of range");
+    GG_CK(cudaSetDevice(e->device));
+    GG_CK(cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking));
+    GG_CK(cudaEventCreate(&e->ev0));
+    GG_CK(cudaEventCreate(&e->ev1));
+    const size_t tb = std::max<size_t>(e->table_elems, 1) * sizeof(int32_t);
+    GG_CK(cudaMalloc(&e->d_table, tb));
+    GG_CK(cudaMallocHost(&e->h_table, tb));
+    if (e->form == FORM_GRAPH) {
+        e->d_adj = e->d_table;  // the graph table is the adjacency
+    } else {
+        GG_CK(cudaMalloc(&e->d_adj, std::max<size_t>((size_t)e->rows * e->d, 1) * sizeof(int32_t)));
+    }
+    GG_CK(cudaMalloc(&e->d_src, std::max<size_t>(e->reps.size(), 1) * sizeof(int32_t)));
+    GG_CK(cudaMemcpy(e->d_src, e->reps.data(), e->reps.size() * sizeof(int32_t),
+                     cudaMemcpyHostToDevice));
+    GG_CK(cudaMalloc(&e->d_bad, sizeof(int)));
+    GG_CK(cudaMallocHost(&e->h_bad, sizeof(int)));
+    e->bu_permille = env_int("GG_BOTTOM_UP_PERMILLE", 500);
+    const int wait_ms = env_int("GG_WAIT_LIMIT_MS", 10000);
+    e->wait_ns = (long long)std::max(wait_ms, 1) * 1000000ll;
+    gg_status s = plan(e, 0);
+    if (s != GG_OK) return s;
+    return ensure_counters(e, 128, 1);
+}
+
+gg_status finish_create(gg_engine *e, gg_engine **out) {
+    gg_status s = create_common(e);
+    if (s != GG_OK) {
+        destroy_all(e);
+        *out = nullptr;
+        return s;
+    }
+    *out = e;
+    return GG_OK;
+}
+
+// Core evaluation with the table already on the device (d_table_in) on `st`.
+gg_status run_eval(gg_engine *e, const int32_t *d_table_in, const gg_eval_opts *o, gg_result *r,
+                   cudaStream_t st) {
+    const int n_src_all = (int)e->reps.size();
+    int s0 = 0, s1 = n_src_all;
+    if (o && (o->src_begin || o->src_end)) {
+        s0 = o->src_begin;
+        s1 = o->src_end;
+        if (s0 < 0 || s1 > n_src_all || s0 >= s1) return fail(GG_BAD_ARG, "bad source range");
+        if (o->want_wvc && (s0 % 32)) return fail(GG_BAD_ARG, "WVC needs a 32-aligned source range");
+    }
+    const int cap_req = (o && o->max_levels > 0) ? o->max_levels : std::max(e->rows, 1);
+    const bool wvc = o && o->want_wvc;
+    const int ns_all = s1 - s0;
+    const int nb = (ns_all + e->batch_bits - 1) / e->batch_bits;
+    gg_status s = ensure_counters(e, cap_req, nb);
+    if (s != GG_OK) return s;
+    const int stride = e->cap_alloc + 1;
+
+    GG_CK(cudaEventRecord(e->ev0, st));
+    int launches = 0;
+    // Table -> adjacency.
+    if (e->form == FORM_GRAPH) {
+        if (d_table_in != e->d_table) {
+            GG_CK(cudaMemcpyAsync(e->d_table, d_table_in, e->table_elems * 4,
+                                  cudaMemcpyDeviceToDevice, st));
+        }
+        GG_CK(cudaMemsetAsync(e->d_bad, 0, sizeof(int), st));
+        const long long n = (long long)e->rows * e->d;
+        if (n > 0) {
+            gg::check_table_kernel<<<(int)std::min<long long>((n + 255) / 256, 4096), 256, 0, st>>>(
+                e->d_table, n, e->rows, e->d_bad);
+            ++launches;
+        }
+    } else {
+        ExpandArgs x{};
+        x.table = d_table_in;
+        x.adj = e->d_adj;
+        x.form = (e->form == FORM_PART) ? 1 : (e->form == FORM_PIECE ? 2 : 3);
+        x.rows = e->rows; x.d = e->d; x.N = e->N; x.M = e->M;
+        x.Nx = e->dims[0]; x.Ny = e->dims[1]; x.Nz = e->dims[2];
+        x.Mx = e->dims[3]; x.My = e->dims[4]; x.Mz = e->dims[5];
+        const long long n = (long long)e->rows * e->d;
+        if (n > 0) {
+            gg::expand_kernel<<<(int)std::min<long long>((n + 255) / 256, 8192), 256, 0, st>>>(x);
+            GG_CK(cudaGetLastError());
+            ++launches;
+        }
+    }
+    GG_CK(cudaMemsetAsync(e->d_ctl, 0, (size_t)nb * sizeof(Ctl), st));
+
+    void *kern = kernel_for(e->d);
+    if (fault("launch")) return fail(GG_CUDA_ERROR, "injected launch failure");
+    const unsigned extra = fault("barrier") ? 1u : 0u;
+    for (int b = 0; b < nb; ++b) {
+        BfsArgs a{};
+        a.adj = e->d_adj;
+        a.src = e->d_src + s0 + (size_t)b * e->batch_bits;
+        a.ns = std::min(e->batch_bits, ns_all - b * e->batch_bits);
+        a.V = e->d_V; a.F0 = e->d_F0; a.F1 = e->d_F1;
+        a.fl0 = e->d_fl0; a.fl1 = e->d_fl1;
+        a.counts = e->d_counts + (size_t)b * stride;
+        a.masks = wvc ? e->d_masks + (size_t)b * stride : nullptr;
+        a.ctl = e->d_ctl + b;
+        a.rows = e->rows; a.d = e->d; a.nC = e->nC; a.items = e->items;
+        a.div_nc = FastDiv((uint32_t)e->nC);
+        a.max_levels = cap_req;
+        a.bu_permille = e->bu_permille;
+        a.wait_ns = e->wait_ns;
+        a.expected = (unsigned)e->grid + extra;
+        a.bad = e->form == FORM_GRAPH ? e->d_bad : nullptr;
+        void *args[] = {&a};
+        GG_CK(cudaLaunchCooperativeKernel(kern, dim3(e->grid), dim3(gg::kBlock), args, 0, st));
+        ++launches;
+    }
+    GG_CK(cudaEventRecord(e->ev1, st));
+    // Read back only the levels that can hold counts (cap_req + 1 per batch).
+    uint64_t d2h = 0;
+    const size_t lv = (size_t)cap_req + 1;
+    GG_CK(cudaMemcpy2DAsync(e->h_counts, stride * sizeof(unsigned long long), e->d_counts,
+                            stride * sizeof(unsigned long long), lv * sizeof(unsigned long long), nb,
+                            cudaMemcpyDeviceToHost, st));
+    d2h += lv * nb * sizeof(unsigned long long);
+    if (wvc) {
+        GG_CK(cudaMemcpy2DAsync(e->h_masks, stride * sizeof(unsigned), e->d_masks,
+                                stride * sizeof(unsigned), lv * sizeof(unsigned), nb,
+                                cudaMemcpyDeviceToHost, st));
+        d2h += lv * nb * sizeof(unsigned);
+    }
+    GG_CK(cudaMemcpyAsync(e->h_ctl, e->d_ctl, (size_t)nb * sizeof(Ctl), cudaMemcpyDeviceToHost, st));
+    d2h += (size_t)nb * sizeof(Ctl);
+    if (e->form == FORM_GRAPH) {
+        GG_CK(cudaMemcpyAsync(e->h_bad, e->d_bad, sizeof(int), cudaMemcpyDeviceToHost, st));
+        d2h += sizeof(int);
+    }
+    e->last_d2h = d2h;
+    GG_CK(cudaStreamSynchronize(st));
+    float ms = 0.f;
+    GG_CK(cudaEventElapsedTime(&ms, e->ev0, e->ev1));
+    e->last_ms = ms;
+    e->last_launches = launches;
+
+    if (e->form == FORM_GRAPH && *e->h_bad)
+        return fail(GG_BAD_ARG, "adjacency entry outside [0, N)");
+    for (int b = 0; b < nb; ++b)
+        if (e->h_ctl[b].err)
+            return fail(GG_TIMEOUT, "grid barrier wait exceeded its limit at level " +
+                                        std::to_string(e->h_ctl[b].err_level));
+
+    // Exact fold of the per-batch level counters.
+    gg_result R{};
+    R.scale = e->scale;
+    R.pairs = (uint64_t)ns_all * (uint64_t)e->rows;
+    R.n_sources = ns_all;
+    R.batches = nb;
+    R.wvc = -1;
+    std::vector<int> lev(nb, 0);
+    std::vector<unsigned long long> agg(cap_req + 1, 0ull);
+    for (int b = 0; b < nb; ++b) {
+        const unsigned long long *c = e->h_counts + (size_t)b * stride;
+        const int run = e->h_ctl[b].levels_run;
+        int last = 0;
+        for (int L = 0; L <= run && L <= cap_req; ++L) {
+            R.reached += c[L];
+            R.total += (uint64_t)L * c[L];
+            agg[L] += c[L];
+            if (L > 0 && c[L]) last = L;
+        }
+        lev[b] = last;
+        R.level_steps += run;
+        R.levels = std::max(R.levels, last);
+        if (run >= cap_req && c[cap_req]) R.capped = 1;
+    }
+    R.connected = (!R.capped && R.reached == R.pairs) ? 1 : 0;
+    if (wvc) {
+        // Lane-aggregated completion masks across batches: a batch's mask stays
+        // at its final value after its last level.
+        auto mask_at = [&](int L) {
+            unsigned m = 0xffffffffu;
+            for (int b = 0; b < nb; ++b)
+                m &= e->h_masks[(size_t)b * stride + std::min(L, lev[b])];
+            return m;
+        };
+        const int E = R.levels;
+        R.wvc = E > 0 ? __builtin_popcount(mask_at(E - 1) ^ mask_at(E)) : 0;
+    }
+    if (o && o->level_counts)
+        std::memcpy(o->level_counts, agg.data(), (size_t)(cap_req + 1) * sizeof(uint64_t));
+    *r = R;
+    return GG_OK;
+}
+
+gg_status eval_host(gg_engine *e, const int32_t *table, const gg_eval_opts *o, gg_result *r) {
+    if (!e || !r) return fail(GG_BAD_ARG, "null engine or result");
+    if (e->table_elems && !table) return fail(GG_BAD_ARG, "null table");
+    GG_CK(cudaSetDevice(e->device));
+    if (e->table_elems) {
+        std::memcpy(e->h_table, table, e->table_elems * sizeof(int32_t));
+        GG_CK(cudaMemcpyAsync(e->d_table, e->h_table, e->table_elems * sizeof(int32_t),
+                              cudaMemcpyHostToDevice, e->stream));
+    }
+    gg_status s = run_eval(e, e->d_table, o, r, e->stream);
+    e->last_h2d = e->table_elems * sizeof(int32_t);
+    return s;
+}
+
+double aspl_of(uint64_t total, uint64_t scale, int N) {
+    // total *= N/M; double(total)/(int64_t(N)*(N-1))  (cudaASPLconv.cu:241-242)
+    const int64_t t = (int64_t)(total * scale);
+    return double(t) / (int64_t(N) * (N - 1));
+}
+
+// The level loop `for(step=1; step<100; ...)` of cudaASPLconv::diameterASPL and
+// its piece/box twins (cudaASPLconv.cu:208-242, cudaASPLpiece.cu:181-215,
+// cudaASPLbox.cu:191-225).
+gg_status lifted_diameter_aspl(gg_engine *e, const int32_t *table, int *diameter, double *aspl) {
+    if (!diameter || !aspl) return fail(GG_BAD_ARG, "null output");
+    gg_eval_opts o{};
+    o.max_levels = 99;
+    gg_result r;
+    gg_status s = eval_host(e, table, &o, &r);
+    if (s != GG_OK) return s;
+    if (r.capped) {  // step 99 still found pairs: loop ends, diameter stays 1e8
+        *diameter = kSentinel;
+        *aspl = aspl_of(r.total, r.scale, e->N);
+    } else if (!r.connected) {
+        *diameter = kSentinel;
+        *aspl = 100000000.0;
+    } else {
+        *diameter = r.levels;
+        *aspl = aspl_of(r.total, r.scale, e->N);
+    }
+    return GG_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int gg_abi_version(void) { return GG_ABI_VERSION; }
+
+const char *gg_status_str(gg_status s) {
+    switch (s) {
+        case GG_OK: return "ok";
+        case GG_BAD_ARG: return "bad argument";
+        case GG_CUDA_ERROR: return "CUDA error";
+        case GG_TIMEOUT: return "bounded wait timed out";
+        case GG_OUT_OF_MEMORY: return "out of memory";
+        case GG_NO_DEVICE: return "no device";
+    }
+    return "unknown status";
+}
+
+const char *gg_last_error(void) { return g_err.c_str(); }
+
+gg_status gg_graph_create(int N, int degree_max, int device, gg_engine **out) {
+    if (!out) return fail(GG_BAD_ARG, "null out");
+    *out = nullptr;
+    if (N < 1 || degree_max < 0) return fail(GG_BAD_ARG, "need N >= 1, degree_max >= 0");
+    gg_engine *e = new gg_engine();
+    e->form = FORM_GRAPH; e->device = device;
+    e->N = N; e->M = N; e->d = degree_max; e->rows = N; e->scale = 1;
+    e->table_elems = (size_t)N * degree_max;
+    e->reps.resize(N);
+    for (int i = 0; i < N; ++i) e->reps[i] = i;
+    return finish_create(e, out);
+}
+
+gg_status gg_conv_create(int N, int M, int degree, int device, gg_engine **out) {
+    if (!out) return fail(GG_BAD_ARG, "null out");
+    *out = nullptr;
+    if (N < 1 || M < 1 || M > N || degree < 0) return fail(GG_BAD_ARG, "need 1 <= M <= N, degree >= 0");
+    gg_engine *e = new gg_engine();
+    e->form = FORM_PART; e->device = device;
+    e->N = N; e->M = M; e->d = degree; e->rows = N; e->scale = (uint64_t)(N / M);
+    e->table_elems = (size_t)M * degree;
+    e->reps.resize(M);
+    for (int i = 0; i < M; ++i) e->reps[i] = i;
+    return finish_create(e, out);
+}
+
+gg_status gg_beamer_create(int N, int M, int degree, int device, gg_engine **out) {
+    if (!out) return fail(GG_BAD_ARG, "null out");
+    *out = nullptr;
+    if (N < 1 || M < 1 || M > N || degree < 0 || N > kBeamerRows)
+        return fail(GG_BAD_ARG, "need 1 <= M <= N <= 10^6, degree >= 0");
+    gg_engine *e = new gg_engine();
+    e->form = FORM_PART; e->device = device;
+    e->N = N; e->M = M; e->d = degree; e->rows = kBeamerRows; e->scale = (uint64_t)(N / M);
+    e->table_elems = (size_t)M * degree;
+    e->reps.resize(M);
+    for (int i = 0; i < M; ++i) e->reps[i] = i;
+    return finish_create(e, out);
+}
+
+gg_status gg_piece_create(int Nx, int Ny, int Mx, int My, int degree, int device, gg_engine **out) {
+    if (!out) return fail(GG_BAD_ARG, "null out");
+    *out = nullptr;
+    if (Nx < 1 || Ny < 1 || Mx < 1 || My < 1 || Mx > Nx || My > Ny || degree < 0 ||
+        (long long)Nx * Ny >= (1ll << 31))
+        return fail(GG_BAD_ARG, "need 1 <= Mx <= Nx, 1 <= My <= Ny, degree >= 0");
+    gg_engine *e = new gg_engine();
+    e->form = FORM_PIECE; e->device = device;
+    e->dims[0] = Nx; e->dims[1] = Ny; e->dims[2] = 1; e->dims[3] = Mx; e->dims[4] = My; e->dims[5] = 1;
+    e->N = Nx * Ny; e->M = Mx * My; e->d = degree; e->rows = e->N;
+    e->scale = (uint64_t)(e->N / e->M);
+    e->table_elems = (size_t)e->M * degree * 2;
+    // representatives: corner tile, source index x*My+y (cudaASPLpiece.cu:23-29)
+    for (int x = 0; x < Mx; ++x)
+        for (int y = 0; y < My; ++y) e->reps.push_back(x * Ny + y);
+    return finish_create(e, out);
+}
+
+gg_status gg_box_create(int Nx, int Ny, int Nz, int Mx, int My, int Mz, int degree, int device,
+                        gg_engine **out) {
+    if (!out) return fail(GG_BAD_ARG, "null out");
+    *out = nullptr;
+    if (Nx < 1 || Ny < 1 || Nz < 1 || Mx < 1 || My < 1 || Mz < 1 || Mx > Nx || My > Ny || Mz > Nz ||
+        degree < 0 || (long long)Nx * Ny * Nz >= (1ll << 31))
+        return fail(GG_BAD_ARG, "need 1 <= M* <= N*, degree >= 0");
+    gg_engine *e = new gg_engine();
+    e->form = FORM_BOX; e->device = device;
+    e->dims[0] = Nx; e->dims[1] = Ny; e->dims[2] = Nz; e->dims[3] = Mx; e->dims[4] = My; e->dims[5] = Mz;
+    e->N = Nx * Ny * Nz; e->M = Mx * My * Mz; e->d = degree; e->rows = e->N;
+    e->scale = (uint64_t)(e->N / e->M);
+    e->table_elems = (size_t)e->M * degree * 3;
+    // representatives: corner tile, source index (x*My+y)*Mz+z (cudaASPLbox.cu:25-32)
+    for (int x = 0; x < Mx; ++x)
+        for (int y = 0; y < My; ++y)
+            for (int z = 0; z < Mz; ++z) e->reps.push_back((x * Ny + y) * Nz + z);
+    return finish_create(e, out);
+}
+
+gg_status gg_destroy(gg_engine *e) {
+    destroy_all(e);
+    return GG_OK;
+}
+
+gg_status gg_eval(gg_engine *e, const int32_t *table, const gg_eval_opts *opts, gg_result *out) {
+    return eval_host(e, table, opts, out);
+}
+
+gg_status gg_eval_device(gg_engine *e, const int32_t *d_table, const gg_eval_opts *opts,
+                         gg_result *out, void *stream) {
+    if (!e || !out) return fail(GG_BAD_ARG, "null engine or result");
+    if (e->table_elems && !d_table) return fail(GG_BAD_ARG, "null table");
+    GG_CK(cudaSetDevice(e->device));
+    cudaStream_t st = stream ? (cudaStream_t)stream : e->stream;
+    gg_status s = run_eval(e, d_table ? d_table : e->d_table, opts, out, st);
+    e->last_h2d = 0;
+    return s;
+}
+
+gg_status gg_last_transfer_bytes(gg_engine *e, uint64_t *h2d, uint64_t *d2h) {
+    if (!e || !h2d || !d2h) return fail(GG_BAD_ARG, "null argument");
+    *h2d = e->last_h2d;
+    *d2h = e->last_d2h;
+    return GG_OK;
+}
+
+gg_status gg_last_device_ms(gg_engine *e, double *ms) {
+    if (!e || !ms) return fail(GG_BAD_ARG, "null argument");
+    *ms = e->last_ms;
+    return GG_OK;
+}
+
+gg_status gg_last_launches(gg_engine *e, int *launches) {
+    if (!e || !launches) return fail(GG_BAD_ARG, "null argument");
+    *launches = e->last_launches;
+    return GG_OK;
+}
+
+gg_status gg_set_batch_sources(gg_engine *e, int sources) {
+    if (!e || sources < 0) return fail(GG_BAD_ARG, "bad batch width");
+    GG_CK(cudaSetDevice(e->device));
+    GG_CK(cudaStreamSynchronize(e->stream));
+    return plan(e, sources);
+}
+
+gg_status gg_set_wait_limit_ms(gg_engine *e, int ms) {
+    if (!e || ms < 1) return fail(GG_BAD_ARG, "bad wait limit");
+    e->wait_ns = (long long)ms * 1000000ll;
+    return GG_OK;
+}
+
+// cudaASPLgraph::calc (cudaASPLgraph.cu:141-199)
+gg_status gg_graph_calc(gg_engine *e, const int32_t *adj, int *diameter, int64_t *total) {
+    if (!e || !diameter || !total) return fail(GG_BAD_ARG, "null argument");
+    if (e->form != FORM_GRAPH) return fail(GG_BAD_ARG, "not a graph engine");
+    gg_eval_opts o{};
+    o.max_levels = 199;
+    gg_result r;
+    gg_status s = eval_host(e, adj, &o, &r);
+    if (s != GG_OK) return s;
+    if (!r.capped && r.connected) {
+        *diameter = r.levels;
+        *total = (int64_t)r.total;
+        return GG_OK;
+    }
+    // Some source hits the 199-step limit or misses a vertex: the reference
+    // answers for the first 1024-source chunk (in source order) that does
+    // either, so resolve chunk by chunk with the table already on the device.
+    for (int off = 0; off < e->N; off += 1024) {
+        gg_eval_opts c{};
+        c.max_levels = 199;
+        c.src_begin = off;
+        c.src_end = std::min(off + 1024, e->N);
+        gg_result rc;
+        s = run_eval(e, e->d_table, &c, &rc, e->stream);
+        if (s != GG_OK) return s;
+        if (rc.capped) { *diameter = -2; *total = -2; return GG_OK; }
+        if (!rc.connected) { *diameter = -1; *total = -1; return GG_OK; }
+    }
+    return fail(GG_CUDA_ERROR, "inconsistent chunk resolution");
+}
+
+gg_status gg_conv_calc(gg_engine *e, const int32_t *diffs, double *aspl) {
+    if (!e || !aspl) return fail(GG_BAD_ARG, "null argument");
+    gg_eval_opts o{};
+    o.max_levels = 99;
+    gg_result r;
+    gg_status s = eval_host(e, diffs, &o, &r);
+    if (s != GG_OK) return s;
+    if (!r.capped && !r.connected) *aspl = 1e9;  // cudaASPLconv.cu:182
+    else *aspl = aspl_of(r.total, r.scale, e->N);
+    return GG_OK;
+}
+
+gg_status gg_conv_diameter_aspl(gg_engine *e, const int32_t *diffs, int *diameter, double *aspl) {
+    if (!e) return fail(GG_BAD_ARG, "null engine");
+    if (e->form != FORM_PART) return fail(GG_BAD_ARG, "not a part engine");
+    return lifted_diameter_aspl(e, diffs, diameter, aspl);
+}
+
+// cudaASPLconv::WVCdiameterASPL (cudaASPLconv.cu:244-308)
+gg_status gg_conv_wvc_diameter_aspl(gg_engine *e, const int32_t *diffs, int *wvc, int *diameter,
+                                    double *aspl) {
+    if (!e || !wvc || !diameter || !aspl) return fail(GG_BAD_ARG, "null argument");
+    if (e->form != FORM_PART) return fail(GG_BAD_ARG, "not a part engine");
+    gg_eval_opts o{};
+    o.max_levels = 100;
+    o.want_wvc = 1;
+    gg_result r;
+    gg_status s = eval_host(e, diffs, &o, &r);
+    if (s != GG_OK) return s;
+    if (r.capped || !r.connected) {
+        *wvc = kSentinel; *diameter = kSentinel; *aspl = 100000000.0;
+    } else {
+        *wvc = r.wvc; *diameter = r.levels; *aspl = aspl_of(r.total, r.scale, e->N);
+    }
+    return GG_OK;
+}
+
+gg_status gg_piece_diameter_aspl(gg_engine *e, const int32_t *vals, int *diameter, double *aspl) {
+    if (!e) return fail(GG_BAD_ARG, "null engine");
+    if (e->form != FORM_PIECE) return fail(GG_BAD_ARG, "not a piece engine");
+    return lifted_diameter_aspl(e, vals, diameter, aspl);
+}
+
+gg_status gg_box_diameter_aspl(gg_engine *e, const int32_t *vals, int *diameter, double *aspl) {
+    if (!e) return fail(GG_BAD_ARG, "null engine");
+    if (e->form != FORM_BOX) return fail(GG_BAD_ARG, "not a box engine");
+    return lifted_diameter_aspl(e, vals, diameter, aspl);
+}
+
+// cudaASPLbeamer::calc (cudaASPLbeamer.cu:71-84)
+gg_status gg_beamer_calc(gg_engine *e, const int32_t *diffs, int regular, double *aspl) {
+    if (!e || !aspl) return fail(GG_BAD_ARG, "null argument");
+    if (e->form != FORM_PART || e->rows != kBeamerRows) return fail(GG_BAD_ARG, "not a beamer engine");
+    if (!regular) { *aspl = 100000000; return GG_OK; }
+    gg_eval_opts o{};
+    o.max_levels = kBeamerLevels;
+    gg_result r;
+    gg_status s = eval_host(e, diffs, &o, &r);
+    if (s != GG_OK) return s;
+    *aspl = aspl_of(r.total, r.scale, e->N);
+    return GG_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,187 @@
+// gg_gen.cpp -- deterministic instance generators (host only, no GPU).
+//
+// Random numbers: SplitMix64 seeds xoshiro256** (Blackman & Vigna, "Scrambled
+// linear pseudorandom number generators", 2021); bounded integers use Lemire's
+// multiply-and-reject method ("Fast random integer generation in an interval",
+// ACM TOMACS 2019).  Both are spelled out here so that a seed means the same
+// graph on every platform (std::uniform_int_distribution is library-defined).
+//
+// The reference draws its random instances with std::mt19937 + std::shuffle
+// stub pairing and does not reject loops or multi-edges (cppcode/initTemp.cpp:399-405,
+// cppcode/RNDpiecegen.cpp).  The generators here are the seeded synthetic
+// inputs of the benchmark configurations instead: simple and connected by
+// construction.
+#include "gg.h"
+
+#include <algorithm>
+#include <cstdint>
+#include <string>
+#include <unordered_set>
+#include <vector>
+
+namespace {
+
+struct Rng {
+    uint64_t s[4];
+    explicit Rng(uint64_t seed) {
+        uint64_t x = seed;
+        for (auto &w : s) {  // SplitMix64
+            x += 0x9e3779b97f4a7c15ull;
+            uint64_t z = x;
+            z = (z ^ (z >> 30)) * 0xbf58476d1ce4e5b9ull;
+            z = (z ^ (z >> 27)) * 0x94d049bb133111ebull;
+            w = z ^ (z >> 31);
+        }
+    }
+    static uint64_t rotl(uint64_t x, int k) { return (x << k) | (x >> (64 - k)); }
+    uint64_t next() {  // xoshiro256**
+        const uint64_t r = rotl(s[1] * 5, 7) * 9;
+        const uint64_t t = s[1] << 17;
+        s[2] ^= s[0]; s[3] ^= s[1]; s[1] ^= s[2]; s[0] ^= s[3];
+        s[2] ^= t;
+        s[3] = rotl(s[3], 45);
+        return r;
+    }
+    uint32_t below(uint32_t n) {  // uniform in [0, n), Lemire
+        uint32_t x = (uint32_t)(next() >> 32);
+        uint64_t m = (uint64_t)x * n;
+        uint32_t l = (uint32_t)m;
+        if (l < n) {
+            const uint32_t t = (uint32_t)(-n) % n;
+            while (l < t) {
+                x = (uint32_t)(next() >> 32);
+                m = (uint64_t)x * n;
+                l = (uint32_t)m;
+            }
+        }
+        return (uint32_t)(m >> 32);
+    }
+};
+
+inline uint64_t ekey(int a, int b) {
+    if (a > b) std::swap(a, b);
+    return ((uint64_t)(uint32_t)a << 32) | (uint32_t)b;
+}
+
+bool connected(int n, const std::vector<std::vector<int>> &g) {
+    std::vector<char> seen(n, 0);
+    std::vector<int> st{0};
+    seen[0] = 1;
+    int cnt = 1;
+    while (!st.empty()) {
+        int v = st.back();
+        st.pop_back();
+        for (int u : g[v])
+            if (!seen[u]) { seen[u] = 1; ++cnt; st.push_back(u); }
+    }
+    return cnt == n;
+}
+
+// One attempt: stub pairing, then double-edge switches that move every loop and
+// repeated edge onto a uniformly drawn partner edge until the multigraph is simple.
+bool regular_attempt(int n, int d, Rng &rng, std::vector<std::pair<int, int>> &E) {
+    std::vector<int> stubs((size_t)n * d);
+    for (int v = 0; v < n; ++v)
+        for (int k = 0; k < d; ++k) stubs[(size_t)v * d + k] = v;
+    for (size_t i = stubs.size(); i > 1; --i) std::swap(stubs[i - 1], stubs[rng.below((uint32_t)i)]);
+    const size_t m = stubs.size() / 2;
+    E.resize(m);
+    for (size_t i = 0; i < m; ++i) E[i] = {stubs[2 * i], stubs[2 * i + 1]};
+    std::unordered_multiset<uint64_t> ms;
+    ms.reserve(m * 2);
+    for (auto &e : E) ms.insert(ekey(e.first, e.second));
+    auto bad = [&](size_t i) {
+        const auto &e = E[i];
+        return e.first == e.second || ms.count(ekey(e.first, e.second)) > 1;
+    };
+    const size_t budget = 200 * m + 100000;
+    size_t tries = 0;
+    for (size_t i = 0; i < m; ++i) {
+        while (bad(i)) {
+            if (++tries > budget) return false;
+            const size_t j = rng.below((uint32_t)m);
+            if (j == i) continue;
+            int a = E[i].first, b = E[i].second, c = E[j].first, x = E[j].second;
+            if (rng.below(2)) std::swap(c, x);
+            // (a,b),(c,x) -> (a,c),(b,x)
+            if (a == c || b == x) continue;
+            if (ms.count(ekey(a, c)) || ms.count(ekey(b, x))) continue;
+            if (ekey(a, c) == ekey(b, x)) continue;
+            ms.erase(ms.find(ekey(E[i].first, E[i].second)));
+            ms.erase(ms.find(ekey(E[j].first, E[j].second)));
+            E[i] = {a, c};
+            E[j] = {b, x};
+            ms.insert(ekey(a, c));
+            ms.insert(ekey(b, x));
+            if (j < i && bad(j)) i = j;  // re-examine an earlier edge if it became bad
+        }
+    }
+    return true;
+}
+
+}  // namespace
+
+extern "C" {
+
+gg_status gg_gen_random_regular(int n, int d, uint64_t seed, int32_t *adj) {
+    if (!adj || n < 2 || d < 1 || d >= n || ((long long)n * d) % 2 != 0 || (long long)n * d > (1ll << 31))
+        return GG_BAD_ARG;
+    Rng rng(seed);
+    std::vector<std::pair<int, int>> E;
+    for (int attempt = 0; attempt < 1000; ++attempt) {
+        if (!regular_attempt(n, d, rng, E)) continue;
+        std::vector<std::vector<int>> g(n);
+        for (auto &e : E) { g[e.first].push_back(e.second); g[e.second].push_back(e.first); }
+        if (!connected(n, g)) continue;
+        for (int v = 0; v < n; ++v) {
+            std::sort(g[v].begin(), g[v].end());
+            std::copy(g[v].begin(), g[v].end(), adj + (size_t)v * d);
+        }
+        return GG_OK;
+    }
+    return GG_BAD_ARG;
+}
+
+gg_status gg_gen_cyclic_lift(int m, int g, int d, uint64_t seed, int32_t *diffs) {
+    if (!diffs || m < 1 || g < 1 || d < 1 || ((long long)m * d) % 2 != 0 ||
+        (long long)m * g >= (1ll << 31))
+        return GG_BAD_ARG;
+    const int N = m * g;
+    Rng rng(seed);
+    for (int attempt = 0; attempt < 100000; ++attempt) {
+        std::vector<int> stubs((size_t)m * d);
+        for (int v = 0; v < m; ++v)
+            for (int k = 0; k < d; ++k) stubs[(size_t)v * d + k] = v;
+        for (size_t i = stubs.size(); i > 1; --i) std::swap(stubs[i - 1], stubs[rng.below((uint32_t)i)]);
+        std::vector<std::vector<int>> rows(m);
+        for (size_t i = 0; i + 1 < stubs.size(); i += 2) {
+            int a = stubs[i], b = stubs[i + 1];
+            if (a > b) std::swap(a, b);
+            const int s = (int)rng.below((uint32_t)g);
+            const int diff = (b - a) + m * s;  // quotient edge (a, b, s)
+            rows[a].push_back(diff);
+            rows[b].push_back(-diff);
+        }
+        // Simple lift: the neighbours (u + diff) mod N of each orbit vertex u are
+        // distinct and differ from u (then every lifted copy of u is simple too).
+        bool ok = true;
+        for (int u = 0; u < m && ok; ++u) {
+            std::unordered_set<long long> seen;
+            for (int df : rows[u]) {
+                long long to = (((long long)u + df) % N + N) % N;
+                if (to == u || !seen.insert(to).second) { ok = false; break; }
+            }
+        }
+        if (!ok) continue;
+        // Connected lift.
+        std::vector<std::vector<int>> gl(N);
+        for (int v = 0; v < N; ++v)
+            for (int df : rows[v % m]) gl[v].push_back((int)((((long long)v + df) % N + N) % N));
+        if (!connected(N, gl)) continue;
+        for (int u = 0; u < m; ++u) std::copy(rows[u].begin(), rows[u].end(), diffs + (size_t)u * d);
+        return GG_OK;
+    }
+    return GG_BAD_ARG;
+}
+
+}  // extern "C"

@@ -1,0 +1,539 @@
+"""graphgolf -- Python mirror of the reference calculator API over libggb200.so.
+
+The reference (C++) exposes calculators constructed from the graph dimensions
+and called once per candidate (cudacode/cudaASPL*.hpp).  This module keeps
+those names, constructor arguments, method names and return conventions:
+
+=========================  ===========================================  =====================
+Python                     reference                                    C ABI (include/gg.h)
+=========================  ===========================================  =====================
+``graph``                  ``graphgolf::graph`` (cppcode/graph.hpp)     --
+``part``                   ``graphgolf::part`` (cppcode/part.hpp)       --
+``piece``                  ``graphgolf::piece`` (cppcode/piece.hpp)     --
+``box``                    ``graphgolf::box`` (cppcode/box.hpp)         --
+``cudaASPLgraph``          cudacode/cudaASPLgraph.hpp:14-18             ``gg_graph_*``
+``cudaASPLconv``           cudacode/cudaASPLconv.hpp:16-22              ``gg_conv_*``
+``cudaASPLpiece``          cudacode/cudaASPLpiece.hpp:16-20             ``gg_piece_*``
+``cudaASPLbox``            cudacode/cudaASPLbox.hpp:16-20               ``gg_box_*``
+``cudaASPLbeamer``         cudacode/cudaASPLbeamer.hpp:12-16            ``gg_beamer_*``
+=========================  ===========================================  =====================
+
+Every calculator call runs on the GPU through the C ABI.  There is no CPU
+fallback: if the library cannot be loaded, or no GPU is present, the calls
+raise ``GGError``.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import re
+from dataclasses import dataclass, field
+from typing import List, Optional, Sequence
+
+import numpy as np
+
+PKG = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(PKG, "libggb200.so")
+HEADER = os.path.join(os.path.dirname(PKG), "include", "gg.h")
+
+GG_OK, GG_BAD_ARG, GG_CUDA_ERROR, GG_TIMEOUT, GG_OUT_OF_MEMORY, GG_NO_DEVICE = range(6)
+STATUS_NAMES = {0: "GG_OK", 1: "GG_BAD_ARG", 2: "GG_CUDA_ERROR", 3: "GG_TIMEOUT",
+                4: "GG_OUT_OF_MEMORY", 5: "GG_NO_DEVICE"}
+
+
+class GGError(RuntimeError):
+    def __init__(self, status, msg=""):
+        super().__init__(f"{STATUS_NAMES.get(status, status)}: {msg}")
+        self.status = status
+
+
+class Result(ctypes.Structure):
+    """gg_result (include/gg.h)."""
+    _fields_ = [("total", ctypes.c_uint64), ("reached", ctypes.c_uint64),
+                ("pairs", ctypes.c_uint64), ("scale", ctypes.c_uint64),
+                ("levels", ctypes.c_int32), ("capped", ctypes.c_int32),
+                ("connected", ctypes.c_int32), ("wvc", ctypes.c_int32),
+                ("n_sources", ctypes.c_int32), ("batches", ctypes.c_int32),
+                ("level_steps", ctypes.c_int32), ("reserved", ctypes.c_int32)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+class EvalOpts(ctypes.Structure):
+    """gg_eval_opts (include/gg.h)."""
+    _fields_ = [("max_levels", ctypes.c_int32), ("src_begin", ctypes.c_int32),
+                ("src_end", ctypes.c_int32), ("want_wvc", ctypes.c_int32),
+                ("level_counts", ctypes.c_void_p)]
+
+
+_lib = None
+_P = ctypes.c_void_p
+_I = ctypes.c_int
+_IP = ctypes.POINTER(ctypes.c_int)
+_DP = ctypes.POINTER(ctypes.c_double)
+_EPP = ctypes.POINTER(ctypes.c_void_p)
+
+_SIGS = {
+    "gg_graph_create": [_I, _I, _I, _EPP],
+    "gg_graph_calc": [_P, _P, _IP, ctypes.POINTER(ctypes.c_int64)],
+    "gg_conv_create": [_I, _I, _I, _I, _EPP],
+    "gg_conv_calc": [_P, _P, _DP],
+    "gg_conv_diameter_aspl": [_P, _P, _IP, _DP],
+    "gg_conv_wvc_diameter_aspl": [_P, _P, _IP, _IP, _DP],
+    "gg_piece_create": [_I, _I, _I, _I, _I, _I, _EPP],
+    "gg_piece_diameter_aspl": [_P, _P, _IP, _DP],
+    "gg_box_create": [_I, _I, _I, _I, _I, _I, _I, _I, _EPP],
+    "gg_box_diameter_aspl": [_P, _P, _IP, _DP],
+    "gg_beamer_create": [_I, _I, _I, _I, _EPP],
+    "gg_beamer_calc": [_P, _P, _I, _DP],
+    "gg_eval": [_P, _P, ctypes.POINTER(EvalOpts), ctypes.POINTER(Result)],
+    "gg_eval_device": [_P, _P, ctypes.POINTER(EvalOpts), ctypes.POINTER(Result), _P],
+    "gg_last_device_ms": [_P, _DP],
+    "gg_last_launches": [_P, _IP],
+    "gg_last_transfer_bytes": [_P, ctypes.POINTER(ctypes.c_uint64), ctypes.POINTER(ctypes.c_uint64)],
+    "gg_set_batch_sources": [_P, _I],
+    "gg_set_wait_limit_ms": [_P, _I],
+    "gg_destroy": [_P],
+    "gg_gen_random_regular": [_I, _I, ctypes.c_uint64, _P],
+    "gg_gen_cyclic_lift": [_I, _I, _I, ctypes.c_uint64, _P],
+}
+
+
+def lib():
+    """Load libggb200.so (built in-tree by graphgolf-cuda_b200/build.py)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise GGError(GG_CUDA_ERROR, f"{LIB_PATH} is missing: run graphgolf-cuda_b200/build.py")
+    L = ctypes.CDLL(LIB_PATH)
+    for name, args in _SIGS.items():
+        f = getattr(L, name)
+        f.argtypes = args
+        f.restype = ctypes.c_int
+    L.gg_status_str.restype = ctypes.c_char_p
+    L.gg_status_str.argtypes = [_I]
+    L.gg_last_error.restype = ctypes.c_char_p
+    L.gg_abi_version.restype = ctypes.c_int
+    _lib = L
+    return L
+
+
+def header_functions(path=HEADER):
+    """Names of every function declared in include/gg.h."""
+    text = open(path).read()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"\b(gg_[a-z0-9_]+)\s*\(", text)))
+
+
+def _check(status):
+    if status != GG_OK:
+        raise GGError(status, lib().gg_last_error().decode())
+
+
+def _i32(a):
+    return np.ascontiguousarray(np.asarray(a, dtype=np.int32))
+
+
+def _ptr(a):
+    return a.ctypes.data_as(ctypes.c_void_p)
+
+
+# ----------------------------------------------------------------------------
+# Generators (host, deterministic)
+# ----------------------------------------------------------------------------
+
+def random_regular(n, d, seed):
+    """Simple connected random d-regular graph -> int32 adjacency [n, d]."""
+    out = np.empty((n, d), dtype=np.int32)
+    _check(lib().gg_gen_random_regular(n, d, seed, _ptr(out)))
+    return out
+
+
+def cyclic_lift(m, g, d, seed):
+    """Simple connected random cyclic lift in part form -> (N, M, diffs [m, d])."""
+    out = np.empty((m, d), dtype=np.int32)
+    _check(lib().gg_gen_cyclic_lift(m, g, d, seed, _ptr(out)))
+    return m * g, m, out
+
+
+# ----------------------------------------------------------------------------
+# Data model (cppcode/graph.hpp, part.hpp, piece.hpp, box.hpp) and text formats
+# ----------------------------------------------------------------------------
+
+@dataclass
+class graph:
+    """Edge-list graph (cppcode/graph.hpp:11-52).  load() reads "u v" lines;
+    N = max id + 1, each edge is stored at both ends."""
+    edges: List[List[int]] = field(default_factory=list)
+    N: int = 0
+    degree_max: int = 0
+
+    def load(self, ist):
+        pairs = []
+        n = 0
+        for line in ist.read().splitlines() if hasattr(ist, "read") else ist:
+            parts = line.split()
+            if len(parts) < 2:
+                continue
+            u, v = int(parts[0]), int(parts[1])
+            pairs.append((u, v))
+            n = max(n, u, v)
+        self.N = n + 1
+        self.edges = [[] for _ in range(self.N)]
+        for u, v in pairs:
+            self.edges[u].append(v)
+            self.edges[v].append(u)
+        self.degree_max = max((len(e) for e in self.edges), default=0)
+        return self
+
+    def is_regular(self):
+        return all(len(e) == self.degree_max for e in self.edges)
+
+    def print(self, ost):
+        for v, lst in enumerate(self.edges):
+            for u in lst:
+                if u < v:
+                    ost.write(f"{u} {v}\n")
+
+    @classmethod
+    def from_adjacency(cls, adj):
+        adj = np.asarray(adj)
+        g = cls(edges=[list(map(int, r)) for r in adj], N=len(adj), degree_max=adj.shape[1])
+        return g
+
+    def table(self, degree_max=None):
+        """N x degree_max int32, padded with self-loops (cudaASPLgraph.cu:144-153)."""
+        dm = self.degree_max if degree_max is None else degree_max
+        t = np.repeat(np.arange(self.N, dtype=np.int32)[:, None], max(dm, 0), axis=1)
+        for v, lst in enumerate(self.edges):
+            k = min(len(lst), dm)
+            t[v, :k] = lst[:k]
+        return t
+
+
+@dataclass
+class part:
+    """Cyclic lift (cppcode/part.hpp:6-44): N vertices, M orbit rows of diffs."""
+    N: int = 0
+    M: int = 0
+    regular: bool = True
+    degree: int = 0
+    edges: List[List[int]] = field(default_factory=list)
+
+    def load(self, ist):
+        tok = (ist.read() if hasattr(ist, "read") else ist).split()
+        it = iter(tok)
+        self.N, self.M = int(next(it)), int(next(it))
+        self.edges = []
+        self.degree, self.regular = 0, True
+        for _ in range(self.M):
+            E = int(next(it))
+            if not self.degree:
+                self.degree = E
+            elif self.degree != E:
+                self.regular = False
+                self.degree = max(self.degree, E)
+            self.edges.append([int(next(it)) for _ in range(E)])
+        return self
+
+    def print(self, ost):
+        ost.write(f"{self.N} {self.M}\n")
+        for row in self.edges:
+            ost.write(" ".join([str(len(row))] + [str(x) for x in row]) + "\n")
+
+    @classmethod
+    def from_diffs(cls, N, M, diffs):
+        rows = [list(map(int, r)) for r in np.asarray(diffs).reshape(M, -1)]
+        return cls(N=N, M=M, regular=True, degree=len(rows[0]) if rows else 0, edges=rows)
+
+    def table(self, degree):
+        """M x degree int32, padding diff 0 (cudaASPLconv.cu:199-201)."""
+        t = np.zeros((self.M, degree), dtype=np.int32)
+        for i, row in enumerate(self.edges):
+            k = min(len(row), degree)
+            t[i, :k] = row[:k]
+        return t
+
+
+@dataclass
+class piece:
+    """2-D torus lift (cppcode/piece.hpp:7-53): edges[x][y] = [(dx, dy), ...]."""
+    Nx: int = 0
+    Ny: int = 0
+    Mx: int = 0
+    My: int = 0
+    regular: bool = True
+    degree: int = 0
+    edges: list = field(default_factory=list)
+
+    def load(self, ist):
+        tok = (ist.read() if hasattr(ist, "read") else ist).split()
+        it = iter(tok)
+        self.Nx, self.Ny, self.Mx, self.My = (int(next(it)) for _ in range(4))
+        self.degree, self.regular = 0, True
+        self.edges = [[[] for _ in range(self.My)] for _ in range(self.Mx)]
+        for x in range(self.Mx):
+            for y in range(self.My):
+                E = int(next(it))
+                if not self.degree:
+                    self.degree = E
+                elif self.degree != E:
+                    self.regular = False
+                self.edges[x][y] = [(int(next(it)), int(next(it))) for _ in range(E)]
+        return self
+
+    def print(self, ost):
+        ost.write(f"{self.Nx} {self.Ny} {self.Mx} {self.My}\n")
+        for x in range(self.Mx):
+            for y in range(self.My):
+                row = self.edges[x][y]
+                ost.write(" ".join([str(len(row))] + [f"{a} {b}" for a, b in row]) + "\n")
+
+    def table(self, degree):
+        """Mx*My*degree*2 int32, padding (0,0) (cudaASPLpiece.cu:166-176)."""
+        t = np.zeros((self.Mx * self.My, degree, 2), dtype=np.int32)
+        for x in range(self.Mx):
+            for y in range(self.My):
+                for e, (a, b) in enumerate(self.edges[x][y][:degree]):
+                    t[x * self.My + y, e] = (a, b)
+        return t
+
+
+@dataclass
+class box:
+    """3-D torus lift (cppcode/box.hpp:6-81): edges[x][y][z] = [(dx, dy, dz), ...]."""
+    Nx: int = 0
+    Ny: int = 0
+    Nz: int = 0
+    Mx: int = 0
+    My: int = 0
+    Mz: int = 0
+    regular: bool = True
+    degree: int = 0
+    edges: list = field(default_factory=list)
+
+    @property
+    def N(self):
+        return self.Nx * self.Ny * self.Nz
+
+    @property
+    def M(self):
+        return self.Mx * self.My * self.Mz
+
+    def load(self, ist):
+        tok = (ist.read() if hasattr(ist, "read") else ist).split()
+        it = iter(tok)
+        self.Nx, self.Ny, self.Nz, self.Mx, self.My, self.Mz = (int(next(it)) for _ in range(6))
+        self.regular = True
+        self.edges = [[[[] for _ in range(self.Mz)] for _ in range(self.My)] for _ in range(self.Mx)]
+        for x in range(self.Mx):
+            for y in range(self.My):
+                for z in range(self.Mz):
+                    E = int(next(it))
+                    if not self.degree:
+                        self.degree = E
+                    elif self.degree != E:
+                        self.regular = False
+                    self.edges[x][y][z] = [(int(next(it)), int(next(it)), int(next(it)))
+                                           for _ in range(E)]
+        return self
+
+    def print(self, ost):
+        ost.write(f"{self.Nx} {self.Ny} {self.Nz} {self.Mx} {self.My} {self.Mz}\n")
+        for x in range(self.Mx):
+            for y in range(self.My):
+                for z in range(self.Mz):
+                    row = self.edges[x][y][z]
+                    ost.write(" ".join([str(len(row))] + [f"{a} {b} {c}" for a, b, c in row]) + "\n")
+
+    def table(self, degree):
+        """Mx*My*Mz*degree*3 int32, padding (0,0,0) (cudaASPLbox.cu:170-184)."""
+        t = np.zeros((self.M, degree, 3), dtype=np.int32)
+        for x in range(self.Mx):
+            for y in range(self.My):
+                for z in range(self.Mz):
+                    for e, tr in enumerate(self.edges[x][y][z][:degree]):
+                        t[(x * self.My + y) * self.Mz + z, e] = tr
+        return t
+
+
+# ----------------------------------------------------------------------------
+# Engine handle
+# ----------------------------------------------------------------------------
+
+class Engine:
+    """One gg_engine.  Use the calculator classes below for the reference API;
+    this class adds the raw exact counts (gg_eval)."""
+
+    def __init__(self, handle, table_shape):
+        self._h = handle
+        self.table_shape = table_shape
+
+    def _table(self, t):
+        t = _i32(t)
+        if t.size != int(np.prod(self.table_shape)):
+            raise GGError(GG_BAD_ARG, f"table has {t.size} entries, expected {self.table_shape}")
+        return t
+
+    def eval(self, table, max_levels=0, src_range=None, want_wvc=False, level_counts=False):
+        t = self._table(table)
+        o = EvalOpts()
+        o.max_levels = max_levels
+        if src_range is not None:
+            o.src_begin, o.src_end = src_range
+        o.want_wvc = int(want_wvc)
+        lc = None
+        if level_counts:
+            if max_levels <= 0:
+                raise GGError(GG_BAD_ARG, "level_counts needs max_levels > 0")
+            lc = np.zeros(max_levels + 1, dtype=np.uint64)
+            o.level_counts = lc.ctypes.data
+        r = Result()
+        _check(lib().gg_eval(self._h, _ptr(t), ctypes.byref(o), ctypes.byref(r)))
+        d = r.as_dict()
+        if lc is not None:
+            d["level_counts"] = lc
+        return d
+
+    def eval_device(self, dev_ptr, max_levels=0, stream=0):
+        o = EvalOpts()
+        o.max_levels = max_levels
+        r = Result()
+        _check(lib().gg_eval_device(self._h, ctypes.c_void_p(dev_ptr), ctypes.byref(o),
+                                    ctypes.byref(r), ctypes.c_void_p(stream)))
+        return r.as_dict()
+
+    def last_device_ms(self):
+        ms = ctypes.c_double()
+        _check(lib().gg_last_device_ms(self._h, ctypes.byref(ms)))
+        return ms.value
+
+    def last_launches(self):
+        n = ctypes.c_int()
+        _check(lib().gg_last_launches(self._h, ctypes.byref(n)))
+        return n.value
+
+    def last_transfer_bytes(self):
+        a, b = ctypes.c_uint64(), ctypes.c_uint64()
+        _check(lib().gg_last_transfer_bytes(self._h, ctypes.byref(a), ctypes.byref(b)))
+        return a.value, b.value
+
+    def set_batch_sources(self, bits):
+        _check(lib().gg_set_batch_sources(self._h, bits))
+
+    def set_wait_limit_ms(self, ms):
+        _check(lib().gg_set_wait_limit_ms(self._h, ms))
+
+    def close(self):
+        if self._h:
+            lib().gg_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def _create(fn, *args):
+    h = ctypes.c_void_p()
+    _check(getattr(lib(), fn)(*args, ctypes.byref(h)))
+    return h
+
+
+# ----------------------------------------------------------------------------
+# Calculators (reference API)
+# ----------------------------------------------------------------------------
+
+class cudaASPLgraph(Engine):
+    """cudaASPLgraph(N, degree_max, device); calc(graph) -> (diameter, total)
+    with (-1,-1) disconnected, (-2,-2) diameter >= 199 (cudaASPLgraph.cu:141-199)."""
+
+    def __init__(self, N, degree_max, device=0):
+        super().__init__(_create("gg_graph_create", N, degree_max, device), (N, degree_max))
+        self.N, self.degree_max, self.device = N, degree_max, device
+
+    def calc(self, g):
+        t = self._table(g.table(self.degree_max) if isinstance(g, graph) else g)
+        d, tot = ctypes.c_int(), ctypes.c_int64()
+        _check(lib().gg_graph_calc(self._h, _ptr(t), ctypes.byref(d), ctypes.byref(tot)))
+        return d.value, tot.value
+
+
+class cudaASPLconv(Engine):
+    """cudaASPLconv(N, M, degree, device) (cudaASPLconv.hpp:16-22)."""
+
+    def __init__(self, N, M, degree, device=0):
+        super().__init__(_create("gg_conv_create", N, M, degree, device), (M, degree))
+        self.N, self.M, self.degree, self.device = N, M, degree, device
+
+    def _t(self, p):
+        return self._table(p.table(self.degree) if isinstance(p, part) else p)
+
+    def calc(self, p):
+        t, a = self._t(p), ctypes.c_double()
+        _check(lib().gg_conv_calc(self._h, _ptr(t), ctypes.byref(a)))
+        return a.value
+
+    def diameterASPL(self, p):
+        t, d, a = self._t(p), ctypes.c_int(), ctypes.c_double()
+        _check(lib().gg_conv_diameter_aspl(self._h, _ptr(t), ctypes.byref(d), ctypes.byref(a)))
+        return d.value, a.value
+
+    def WVCdiameterASPL(self, p):
+        t, w, d, a = self._t(p), ctypes.c_int(), ctypes.c_int(), ctypes.c_double()
+        _check(lib().gg_conv_wvc_diameter_aspl(self._h, _ptr(t), ctypes.byref(w), ctypes.byref(d),
+                                               ctypes.byref(a)))
+        return w.value, d.value, a.value
+
+
+class cudaASPLpiece(Engine):
+    """cudaASPLpiece(Nx, Ny, Mx, My, degree, device) (cudaASPLpiece.hpp:16-20)."""
+
+    def __init__(self, Nx, Ny, Mx, My, degree, device=0):
+        super().__init__(_create("gg_piece_create", Nx, Ny, Mx, My, degree, device),
+                         (Mx * My, degree, 2))
+        self.Nx, self.Ny, self.Mx, self.My, self.degree = Nx, Ny, Mx, My, degree
+
+    def diameterASPL(self, p):
+        t = self._table(p.table(self.degree) if isinstance(p, piece) else p)
+        d, a = ctypes.c_int(), ctypes.c_double()
+        _check(lib().gg_piece_diameter_aspl(self._h, _ptr(t), ctypes.byref(d), ctypes.byref(a)))
+        return d.value, a.value
+
+
+class cudaASPLbox(Engine):
+    """cudaASPLbox(Nx, Ny, Nz, Mx, My, Mz, degree, device) (cudaASPLbox.hpp:16-20)."""
+
+    def __init__(self, Nx, Ny, Nz, Mx, My, Mz, degree, device=0):
+        super().__init__(_create("gg_box_create", Nx, Ny, Nz, Mx, My, Mz, degree, device),
+                         (Mx * My * Mz, degree, 3))
+        self.degree = degree
+
+    def diameterASPL(self, p):
+        t = self._table(p.table(self.degree) if isinstance(p, box) else p)
+        d, a = ctypes.c_int(), ctypes.c_double()
+        _check(lib().gg_box_diameter_aspl(self._h, _ptr(t), ctypes.byref(d), ctypes.byref(a)))
+        return d.value, a.value
+
+
+class cudaASPLbeamer(Engine):
+    """cudaASPLbeamer(N, M, degree, device) (cudaASPLbeamer.hpp:12-16)."""
+
+    def __init__(self, N, M, degree, device=0):
+        super().__init__(_create("gg_beamer_create", N, M, degree, device), (M, degree))
+        self.N, self.M, self.degree = N, M, degree
+
+    def calc(self, p, regular=None):
+        if isinstance(p, part):
+            regular = p.regular if regular is None else regular
+            t = self._table(p.table(self.degree))
+        else:
+            t = self._table(p)
+            regular = True if regular is None else regular
+        a = ctypes.c_double()
+        _check(lib().gg_beamer_calc(self._h, _ptr(t), int(bool(regular)), ctypes.byref(a)))
+        return a.value

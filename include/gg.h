@@ -1,0 +1,161 @@
+/*
+ * gg.h -- C ABI of the B200 ASPL/diameter engine (libggb200.so).
+ *
+ * The engine computes, for a Graph Golf candidate graph, the exact all-pairs
+ * shortest-path total and the diameter by a bit-parallel BFS on the GPU
+ * (one bit per (source, vertex) pair, one BFS level per grid-wide step).
+ *
+ * Two layers:
+ *  1. Calculator entry points that mirror the reference calculators one for
+ *     one -- same constructor arguments, same packed edge tables the reference
+ *     builds before its cudaMemcpy, same return values and sentinels:
+ *       gg_graph_*   <- graphgolf::cudaASPLgraph   (cudacode/cudaASPLgraph.hpp:14-18)
+ *       gg_conv_*    <- graphgolf::cudaASPLconv    (cudacode/cudaASPLconv.hpp:16-22)
+ *       gg_piece_*   <- graphgolf::cudaASPLpiece   (cudacode/cudaASPLpiece.hpp:16-20)
+ *       gg_box_*     <- graphgolf::cudaASPLbox     (cudacode/cudaASPLbox.hpp:16-20)
+ *       gg_beamer_*  <- graphgolf::cudaASPLbeamer  (cudacode/cudaASPLbeamer.hpp:12-16)
+ *     The C++ classes themselves are provided by libgg_refshim.so, which
+ *     defines the reference member functions on top of these calls.
+ *  2. gg_eval / gg_eval_device: the raw engine call returning exact counts
+ *     (total distance, reached pairs, levels, WVC) with no sentinel folding.
+ *
+ * Conventions: every call returns a gg_status; GG_OK means the outputs are
+ * valid.  All calls are blocking (the result is on the host when they return).
+ * An engine handle must not be used by two host threads at once.  Pointers are
+ * host pointers unless the name says device.
+ */
+#ifndef GG_H_
+#define GG_H_
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define GG_ABI_VERSION 1
+
+typedef struct gg_engine gg_engine;
+
+typedef enum gg_status {
+    GG_OK = 0,
+    GG_BAD_ARG = 1,        /* argument outside the documented domain */
+    GG_CUDA_ERROR = 2,     /* a CUDA runtime call failed (see gg_last_error) */
+    GG_TIMEOUT = 3,        /* a bounded in-kernel wait gave up; the context stays usable */
+    GG_OUT_OF_MEMORY = 4,  /* device or pinned allocation failed */
+    GG_NO_DEVICE = 5       /* no CUDA device / the requested device does not exist */
+} gg_status;
+
+/* Exact outcome of one engine evaluation over the engine's sources. */
+typedef struct gg_result {
+    uint64_t total;      /* sum over levels L=1..levels of L * (#pairs first reached at L) */
+    uint64_t reached;    /* (source, vertex) pairs reached, each source itself included */
+    uint64_t pairs;      /* n_sources * n_vertices: the value `reached` has when connected */
+    uint64_t scale;      /* N / M (integer division) multiplier of the lifted forms, 1 for graphs */
+    int32_t levels;      /* last level that found new pairs (max eccentricity within components) */
+    int32_t capped;      /* 1 if the BFS stopped at max_levels while level max_levels still found pairs */
+    int32_t connected;   /* 1 if not capped and reached == pairs */
+    int32_t wvc;         /* lane-aggregated completion count at the last level (want_wvc), else -1 */
+    int32_t n_sources;   /* sources evaluated */
+    int32_t batches;     /* source batches the engine ran */
+    int32_t level_steps; /* BFS levels executed, summed over batches (the empty last level included) */
+    int32_t reserved;
+} gg_result;
+
+/* Options for gg_eval; pass NULL for the defaults (all sources, no level cap). */
+typedef struct gg_eval_opts {
+    int32_t max_levels;       /* stop after this many levels; 0 = run to completion */
+    int32_t src_begin;        /* source index range [src_begin, src_end); 0,0 = all */
+    int32_t src_end;
+    int32_t want_wvc;         /* track the per-level AND of the visited words (cudaASPLconv.cu:258-285) */
+    uint64_t *level_counts;   /* optional host array [max_levels+1] (or [n_vertices] if uncapped):
+                                 pairs first reached at each level, summed over batches */
+} gg_eval_opts;
+
+/* ---- calculator: plain graph (cudaASPLgraph) ------------------------------
+ * adj: N * degree_max int32, row v = neighbours of v, unused slots padded with
+ * v itself (self loops), exactly the table cudaASPLgraph.cu:144-153 builds.
+ * calc -> (diameter, total over ordered pairs); (-1,-1) disconnected,
+ * (-2,-2) if a level loop reaches step 199 (cudaASPLgraph.cu:179-190). */
+gg_status gg_graph_create(int N, int degree_max, int device, gg_engine **out);
+gg_status gg_graph_calc(gg_engine *e, const int32_t *adj, int *diameter, int64_t *total);
+
+/* ---- calculator: cyclic lift "part" (cudaASPLconv) ------------------------
+ * diffs: M * degree int32, row i = the diffs of orbit vertex i (padding 0),
+ * exactly cudaASPLconv.cu:199-201.  Vertex v has neighbours (v + diffs[v%M]) mod N;
+ * BFS runs from the M vertices 0..M-1 and the total is scaled by N/M. */
+gg_status gg_conv_create(int N, int M, int degree, int device, gg_engine **out);
+/* ASPL only; 1e9 if disconnected (cudaASPLconv.cu:151-196). */
+gg_status gg_conv_calc(gg_engine *e, const int32_t *diffs, double *aspl);
+/* (diameter, ASPL); (1e8, 1e8) if disconnected; diameter 1e8 with the ASPL of
+ * levels 1..99 if the level loop ends at step 99 (cudaASPLconv.cu:197-243). */
+gg_status gg_conv_diameter_aspl(gg_engine *e, const int32_t *diffs, int *diameter, double *aspl);
+/* (WVC, diameter, ASPL); (1e8, 1e8, 1e8) if disconnected or step 100 still
+ * finds pairs (cudaASPLconv.cu:244-308). */
+gg_status gg_conv_wvc_diameter_aspl(gg_engine *e, const int32_t *diffs, int *wvc, int *diameter,
+                                    double *aspl);
+
+/* ---- calculator: 2-D torus lift "piece" (cudaASPLpiece) -------------------
+ * vals: Mx*My * degree * 2 int32 (dx,dy), padding (0,0) (cudaASPLpiece.cu:166-176).
+ * Sources = corner tile x<Mx, y<My; same return convention as gg_conv_diameter_aspl. */
+gg_status gg_piece_create(int Nx, int Ny, int Mx, int My, int degree, int device, gg_engine **out);
+gg_status gg_piece_diameter_aspl(gg_engine *e, const int32_t *vals, int *diameter, double *aspl);
+
+/* ---- calculator: 3-D torus lift "box" (cudaASPLbox) -----------------------
+ * vals: Mx*My*Mz * degree * 3 int32 (dx,dy,dz), padding (0,0,0) (cudaASPLbox.cu:170-184). */
+gg_status gg_box_create(int Nx, int Ny, int Nz, int Mx, int My, int Mz, int degree, int device,
+                        gg_engine **out);
+gg_status gg_box_diameter_aspl(gg_engine *e, const int32_t *vals, int *diameter, double *aspl);
+
+/* ---- calculator: fixed-depth pull BFS (cudaASPLbeamer) --------------------
+ * Same diff table as gg_conv_*.  Reproduces cudaASPLbeamer.cu:7-84: 1e8 if
+ * `regular` is 0 (:72); otherwise the pairs found within 7 levels over the
+ * kernel's fixed 10^6-row scan (rows v >= N pull from (v + diff) mod N), scaled
+ * by N/M, with no connectivity test.  N must be <= 10^6 (the reference's
+ * bitset size). */
+gg_status gg_beamer_create(int N, int M, int degree, int device, gg_engine **out);
+gg_status gg_beamer_calc(gg_engine *e, const int32_t *diffs, int regular, double *aspl);
+
+/* ---- raw engine ----------------------------------------------------------- */
+/* table: the form's packed table (as for the calculator calls above). */
+gg_status gg_eval(gg_engine *e, const int32_t *table, const gg_eval_opts *opts, gg_result *out);
+/* Same, with the table already in device memory; `stream` (a cudaStream_t, or
+ * NULL for the engine's own stream) orders the work after the caller's. */
+gg_status gg_eval_device(gg_engine *e, const int32_t *d_table, const gg_eval_opts *opts,
+                         gg_result *out, void *stream);
+
+/* Milliseconds the BFS kernels of the last evaluation took on the device
+ * (CUDA events on the engine stream, expansion included). */
+gg_status gg_last_device_ms(gg_engine *e, double *ms);
+/* Kernel launches issued by the last evaluation. */
+gg_status gg_last_launches(gg_engine *e, int *launches);
+/* Bytes the last evaluation copied host->device and device->host. */
+gg_status gg_last_transfer_bytes(gg_engine *e, uint64_t *h2d, uint64_t *d2h);
+
+/* Tuning: source-batch width in bits (multiple of 128; 0 = automatic). */
+gg_status gg_set_batch_sources(gg_engine *e, int sources);
+/* Bounded-wait limit of the in-kernel grid barrier, in milliseconds. */
+gg_status gg_set_wait_limit_ms(gg_engine *e, int ms);
+
+gg_status gg_destroy(gg_engine *e);
+
+/* ---- generators (host, deterministic, no GPU) ----------------------------
+ * Random simple connected d-regular graph on n vertices: configuration-model
+ * stub pairing followed by double-edge switches that remove loops and
+ * multi-edges, retried until connected.  adj: n*d, rows sorted ascending. */
+gg_status gg_gen_random_regular(int n, int d, uint64_t seed, int32_t *adj);
+/* Random simple connected cyclic lift: quotient on m orbit vertices, degree d,
+ * voltages in Z_g.  Output in the part form of cudaASPLconv: N = m*g, M = m,
+ * diffs m*d with diff = (v-u) + m*s for the quotient edge (u,v,s) and -diff on
+ * the reverse end. */
+gg_status gg_gen_cyclic_lift(int m, int g, int d, uint64_t seed, int32_t *diffs);
+
+const char *gg_status_str(gg_status s);
+/* Text of the last error raised on this host thread ("" if none). */
+const char *gg_last_error(void);
+int gg_abi_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* GG_H_ */

@@ -131,7 +131,8 @@ void destroy_all(gg_engine *e) {
     if (e->stream) cudaStreamSynchronize(e->stream);
     free_batch_buffers(e);
     free_counters(e);
-    cudaFree(e->d_table); cudaFree(e->d_adj); cudaFree(e->d_src); cudaFree(e->d_bad);
+    if (e->d_adj != e->d_table) cudaFree(e->d_adj);  // the graph form aliases the two
+    cudaFree(e->d_table); cudaFree(e->d_src); cudaFree(e->d_bad);
     cudaFreeHost(e->h_table); cudaFreeHost(e->h_bad);
     if (e->ev0) cudaEventDestroy(e->ev0);
     if (e->ev1) cudaEventDestroy(e->ev1);
@@ -283,6 +284,7 @@ gg_status run_eval(gg_engine *e, const int32_t *d_table_in, const gg_eval_opts *
     if (s != GG_OK) return s;
     const int stride = e->cap_alloc + 1;
 
+    (void)cudaGetLastError();  // launch checks below must not see an earlier, unrelated error
     GG_CK(cudaEventRecord(e->ev0, st));
     int launches = 0;
     // Table -> adjacency.
@@ -296,6 +298,7 @@ gg_status run_eval(gg_engine *e, const int32_t *d_table_in, const gg_eval_opts *
         if (n > 0) {
             gg::check_table_kernel<<<(int)std::min<long long>((n + 255) / 256, 4096), 256, 0, st>>>(
                 e->d_table, n, e->rows, e->d_bad);
+            GG_CK(cudaGetLastError());
             ++launches;
         }
     } else {

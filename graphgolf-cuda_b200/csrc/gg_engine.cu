@@ -67,6 +67,11 @@ bool fault(const char *what) {
 
 }  // namespace
 
+namespace gg {
+// Shared with the other translation units of the library (not exported).
+__attribute__((visibility("hidden"))) void set_last_error(const char *msg) { g_err = msg; }
+}  // namespace gg
+
 struct gg_engine {
     int form = FORM_PART;
     int device = 0;

@@ -300,7 +300,7 @@ __device__ __forceinline__ int pmod64(long long a, int n) {
     return (int)(r < 0 ? r + n : r);
 }
 
-__global__ void expand_kernel(const ExpandArgs e) {
+static __global__ void expand_kernel(const ExpandArgs e) {
     const long long total = (long long)e.rows * e.d;
     for (long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x; k < total;
          k += (long long)gridDim.x * blockDim.x) {
@@ -332,7 +332,7 @@ __global__ void expand_kernel(const ExpandArgs e) {
 
 // Range check of a plain-graph table (every entry a vertex id), so that a bad
 // table becomes GG_BAD_ARG instead of an out-of-bounds gather.
-__global__ void check_table_kernel(const int32_t *t, long long n, int rows, int *bad) {
+static __global__ void check_table_kernel(const int32_t *t, long long n, int rows, int *bad) {
     for (long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x; k < n;
          k += (long long)gridDim.x * blockDim.x)
         if ((unsigned)t[k] >= (unsigned)rows) atomicExch(bad, 1);

@@ -95,6 +95,7 @@ _SIGS = {
     "gg_set_batch_sources": [_P, _I],
     "gg_set_wait_limit_ms": [_P, _I],
     "gg_destroy": [_P],
+    "gg_graph_eval_noalloc": [_P, _I, _I, _I, _P, _P],
     "gg_gen_random_regular": [_I, _I, ctypes.c_uint64, _P],
     "gg_gen_cyclic_lift": [_I, _I, _I, ctypes.c_uint64, _P],
 }

@@ -139,6 +139,31 @@ gg_status gg_set_wait_limit_ms(gg_engine *e, int ms);
 
 gg_status gg_destroy(gg_engine *e);
 
+/* ---- evaluation without device allocation --------------------------------
+ * No counterpart in the reference (its calculators always cudaMalloc their
+ * bitsets in the constructor).  For callers that cannot allocate device memory:
+ * a host whose GPU memory is all owned by another framework's pool, or a search
+ * loop that cannot afford the device-wide synchronisation cudaFree implies.
+ * The caller passes the inputs and outputs as device pointers:
+ *   d_adj            N * degree int32 pull adjacency (entries in [0, N); pad with v itself),
+ *   d_level_counts   max_levels + 1 uint64: on return, [L] = ordered pairs first
+ *                    reached at BFS level L over all N sources ([0] = N); levels past
+ *                    the last non-empty one are 0.  The diameter is the last L with a
+ *                    nonzero count; the total distance is sum L * [L]; the graph is
+ *                    connected when sum [L] == N*N (and [max_levels] == 0).
+ * Working memory is one fixed device array of GG_NOALLOC_SCRATCH_BYTES compiled into
+ * the library, held by every GPU that loads it until the process exits.  N must be
+ * small enough for one batch of N sources to fit in it (N <= 4096 always fits);
+ * larger N returns GG_BAD_ARG.  The first call on a device looks up the array's
+ * device address (cudaGetSymbolAddress) with that device current; make that first
+ * call before any stream capture.  Calls share the array: calls whose GPU work
+ * overlaps race and give undefined results.  Blocking; runs on `stream` (a
+ * cudaStream_t, NULL = legacy default stream) of the current device.  Calls no
+ * cudaMalloc/cudaFree. */
+#define GG_NOALLOC_SCRATCH_BYTES (8u * 1024u * 1024u)
+gg_status gg_graph_eval_noalloc(const int32_t *d_adj, int N, int degree, int max_levels,
+                                uint64_t *d_level_counts, void *stream);
+
 /* ---- generators (host, deterministic, no GPU) ----------------------------
  * Random simple connected d-regular graph on n vertices: configuration-model
  * stub pairing followed by double-edge switches that remove loops and

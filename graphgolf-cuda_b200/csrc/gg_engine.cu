@@ -86,7 +86,11 @@ struct gg_engine {
     int nC = 0;                          // uint4 chunks per row
     uint32_t items = 0;
     int grid = 0;
-    int bu_permille = 500;
+    int dense_w_ppm = 1000;              // level-mode thresholds (see bfs_batch_kernel)
+    int dense_r_ppm = 4000;
+    int full_skip_ppm = 995000;
+    int adj_smem_rows = 0;               // shared-memory adjacency slice (rows per block)
+    size_t smem_bytes = 0;
     long long wait_ns = 10ll * 1000 * 1000 * 1000;
     int cap_alloc = 0;                   // levels the counter arrays hold
     int nb_alloc = 0;                    // batches the counter arrays hold
@@ -100,6 +104,7 @@ struct gg_engine {
     uint32_t *d_fl0 = nullptr, *d_fl1 = nullptr;
     unsigned long long *d_counts = nullptr;
     unsigned *d_masks = nullptr;
+    unsigned long long *d_level_ns = nullptr, *h_level_ns = nullptr;
     Ctl *d_ctl = nullptr;
     // pinned host
     int32_t *h_table = nullptr;
@@ -123,10 +128,11 @@ void free_batch_buffers(gg_engine *e) {
 }
 
 void free_counters(gg_engine *e) {
-    cudaFree(e->d_counts); cudaFree(e->d_masks); cudaFree(e->d_ctl);
+    cudaFree(e->d_counts); cudaFree(e->d_masks); cudaFree(e->d_ctl); cudaFree(e->d_level_ns);
     cudaFreeHost(e->h_counts); cudaFreeHost(e->h_masks); cudaFreeHost(e->h_ctl);
-    e->d_counts = nullptr; e->d_masks = nullptr; e->d_ctl = nullptr;
-    e->h_counts = nullptr; e->h_masks = nullptr; e->h_ctl = nullptr;
+    cudaFreeHost(e->h_level_ns);
+    e->d_counts = nullptr; e->d_masks = nullptr; e->d_ctl = nullptr; e->d_level_ns = nullptr;
+    e->h_counts = nullptr; e->h_masks = nullptr; e->h_ctl = nullptr; e->h_level_ns = nullptr;
     e->cap_alloc = e->nb_alloc = 0;
 }
 
@@ -205,7 +211,29 @@ gg_status plan(gg_engine *e, int want_bits) {
     if (per_sm < 1) return fail(GG_CUDA_ERROR, "BFS kernel cannot be resident");
     const long long tiles = ((long long)e->items + 31) / 32;
     const long long want = (tiles + (gg::kBlock / 32) - 1) / (gg::kBlock / 32);
+    // GG_BLOCKS_PER_SM caps the resident blocks per SM (tuning; never above what fits).
+    const int cap_per_sm = env_int("GG_BLOCKS_PER_SM", 0);
+    if (cap_per_sm > 0) per_sm = std::min(per_sm, cap_per_sm);
     e->grid = (int)std::max<long long>(1, std::min<long long>((long long)per_sm * sms, want));
+    // Shared-memory adjacency slice: a block's contiguous tile range spans at most
+    // ceil(tiles/grid)*32/nC + 2 vertices.  Cached when it fits a small budget and
+    // does not lower the number of resident blocks.
+    e->adj_smem_rows = 0;
+    e->smem_bytes = 0;
+    if (env_int("GG_ADJ_SMEM", 1) && e->d > 0) {
+        const long long per_block = (tiles + e->grid - 1) / e->grid;
+        const long long rows = per_block * 32 / e->nC + 2;
+        const long long bytes = rows * e->d * 4;
+        if (bytes <= 32 * 1024) {
+            int per_sm2 = 0;
+            GG_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm2, kernel_for(e->d), gg::kBlock,
+                                                                (size_t)bytes));
+            if (per_sm2 >= per_sm) {
+                e->adj_smem_rows = (int)rows;
+                e->smem_bytes = (size_t)bytes;
+            }
+        }
+    }
     return GG_OK;
 }
 
@@ -221,6 +249,8 @@ gg_status ensure_counters(gg_engine *e, int cap, int nb) {
     GG_CK(cudaMallocHost(&e->h_counts, n * sizeof(unsigned long long)));
     GG_CK(cudaMallocHost(&e->h_masks, n * sizeof(unsigned)));
     GG_CK(cudaMallocHost(&e->h_ctl, (size_t)nb * sizeof(Ctl)));
+    GG_CK(cudaMalloc(&e->d_level_ns, (size_t)(cap + 1) * sizeof(unsigned long long)));
+    GG_CK(cudaMallocHost(&e->h_level_ns, (size_t)(cap + 1) * sizeof(unsigned long long)));
     e->cap_alloc = cap;
     e->nb_alloc = nb;
     return GG_OK;
@@ -251,7 +281,9 @@ gg_status create_common(gg_engine *e) {
                      cudaMemcpyHostToDevice));
     GG_CK(cudaMalloc(&e->d_bad, sizeof(int)));
     GG_CK(cudaMallocHost(&e->h_bad, sizeof(int)));
-    e->bu_permille = env_int("GG_BOTTOM_UP_PERMILLE", 500);
+    e->dense_w_ppm = env_int("GG_DENSE_W_PPM", e->dense_w_ppm);
+    e->dense_r_ppm = env_int("GG_DENSE_R_PPM", e->dense_r_ppm);
+    e->full_skip_ppm = env_int("GG_FULL_SKIP_PPM", e->full_skip_ppm);
     const int wait_ms = env_int("GG_WAIT_LIMIT_MS", 10000);
     e->wait_ns = (long long)std::max(wait_ms, 1) * 1000000ll;
     gg_status s = plan(e, 0);
@@ -283,6 +315,7 @@ gg_status run_eval(gg_engine *e, const int32_t *d_table_in, const gg_eval_opts *
     }
     const int cap_req = (o && o->max_levels > 0) ? o->max_levels : std::max(e->rows, 1);
     const bool wvc = o && o->want_wvc;
+    const bool want_ns = o && o->level_ns;
     const int ns_all = s1 - s0;
     const int nb = (ns_all + e->batch_bits - 1) / e->batch_bits;
     gg_status s = ensure_counters(e, cap_req, nb);
@@ -322,6 +355,8 @@ gg_status run_eval(gg_engine *e, const int32_t *d_table_in, const gg_eval_opts *
         }
     }
     GG_CK(cudaMemsetAsync(e->d_ctl, 0, (size_t)nb * sizeof(Ctl), st));
+    if (want_ns)
+        GG_CK(cudaMemsetAsync(e->d_level_ns, 0, (size_t)(cap_req + 1) * sizeof(unsigned long long), st));
 
     void *kern = kernel_for(e->d);
     if (fault("launch")) return fail(GG_CUDA_ERROR, "injected launch failure");
@@ -335,16 +370,20 @@ gg_status run_eval(gg_engine *e, const int32_t *d_table_in, const gg_eval_opts *
         a.fl0 = e->d_fl0; a.fl1 = e->d_fl1;
         a.counts = e->d_counts + (size_t)b * stride;
         a.masks = wvc ? e->d_masks + (size_t)b * stride : nullptr;
+        a.level_ns = (b == 0 && want_ns) ? e->d_level_ns : nullptr;
         a.ctl = e->d_ctl + b;
         a.rows = e->rows; a.d = e->d; a.nC = e->nC; a.items = e->items;
         a.div_nc = FastDiv((uint32_t)e->nC);
         a.max_levels = cap_req;
-        a.bu_permille = e->bu_permille;
+        a.dense_w_ppm = e->dense_w_ppm;
+        a.dense_r_ppm = e->dense_r_ppm;
+        a.full_skip_ppm = e->full_skip_ppm;
+        a.adj_smem_rows = e->adj_smem_rows;
         a.wait_ns = e->wait_ns;
         a.expected = (unsigned)e->grid + extra;
         a.bad = e->form == FORM_GRAPH ? e->d_bad : nullptr;
         void *args[] = {&a};
-        GG_CK(cudaLaunchCooperativeKernel(kern, dim3(e->grid), dim3(gg::kBlock), args, 0, st));
+        GG_CK(cudaLaunchCooperativeKernel(kern, dim3(e->grid), dim3(gg::kBlock), args, e->smem_bytes, st));
         ++launches;
     }
     GG_CK(cudaEventRecord(e->ev1, st));
@@ -367,6 +406,11 @@ gg_status run_eval(gg_engine *e, const int32_t *d_table_in, const gg_eval_opts *
         GG_CK(cudaMemcpyAsync(e->h_bad, e->d_bad, sizeof(int), cudaMemcpyDeviceToHost, st));
         d2h += sizeof(int);
     }
+    if (want_ns) {
+        GG_CK(cudaMemcpyAsync(e->h_level_ns, e->d_level_ns, lv * sizeof(unsigned long long),
+                              cudaMemcpyDeviceToHost, st));
+        d2h += lv * sizeof(unsigned long long);
+    }
     e->last_d2h = d2h;
     GG_CK(cudaStreamSynchronize(st));
     float ms = 0.f;
@@ -377,9 +421,10 @@ gg_status run_eval(gg_engine *e, const int32_t *d_table_in, const gg_eval_opts *
     if (e->form == FORM_GRAPH && *e->h_bad)
         return fail(GG_BAD_ARG, "adjacency entry outside [0, N)");
     for (int b = 0; b < nb; ++b)
-        if (e->h_ctl[b].err)
+        if (e->h_ctl[b].err) {
             return fail(GG_TIMEOUT, "grid barrier wait exceeded its limit at level " +
                                         std::to_string(e->h_ctl[b].err_level));
+        }
 
     // Exact fold of the per-batch level counters.
     gg_result R{};
@@ -420,6 +465,8 @@ gg_status run_eval(gg_engine *e, const int32_t *d_table_in, const gg_eval_opts *
     }
     if (o && o->level_counts)
         std::memcpy(o->level_counts, agg.data(), (size_t)(cap_req + 1) * sizeof(uint64_t));
+    if (want_ns)
+        std::memcpy(o->level_ns, e->h_level_ns, (size_t)(cap_req + 1) * sizeof(uint64_t));
     *r = R;
     return GG_OK;
 }

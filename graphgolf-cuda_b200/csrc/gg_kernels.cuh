@@ -64,6 +64,7 @@ struct BfsArgs {
     uint32_t *fl0, *fl1;
     unsigned long long *counts;   // [max_levels + 1]
     unsigned int *masks;          // [max_levels + 1] or nullptr
+    unsigned long long *level_ns; // [max_levels + 1] or nullptr: globaltimer at each level end
     Ctl *ctl;
     const int *bad;           // nonzero: the table failed its range check; do nothing
     unsigned int expected;    // blocks the barrier waits for (the grid size)
@@ -71,7 +72,11 @@ struct BfsArgs {
     uint32_t items;           // rows * nC
     int rows, d, nC, ns;
     int max_levels;
-    int bu_permille;          // switch to own-first order once reached > permille/1000 of pairs
+    int dense_w_ppm;          // write F whole when the feeding frontier >= ppm of the pairs
+    int dense_r_ppm;          // read F without flags when it was written whole and >= ppm
+    int full_skip_ppm;        // own-first, skip full chunks once reached >= ppm of the pairs
+    int adj_smem_rows;        // >0: each block keeps its vertex range's adjacency rows
+                              // (at most this many) in dynamic shared memory
     long long wait_ns;        // barrier wait limit
 };
 
@@ -164,18 +169,108 @@ __device__ __forceinline__ uint4 pad_mask(int c, int ns) {
                       pad_word(b + 96, ns));
 }
 
+constexpr int kGrab = 1;  // tiles a warp takes (and keeps in flight) at once
+
+// One level's work on tiles [tile0, tile0 + U) of the calling warp (a tile is 32
+// consecutive uint4 chunks, one per lane).  Every load of the U tiles is issued
+// before any result is used, so each warp keeps U*(d+1) 16-byte loads in flight.
+template <int D, int U>
+__device__ __forceinline__ void level_tiles(const BfsArgs &a, const int d, const int32_t *adj,
+                                            const unsigned v_base, const unsigned tile0,
+                                            const unsigned t_hi, const uint4 *Fc, uint4 *Fn,
+                                            const uint32_t *fc, uint32_t *fn, const bool dense,
+                                            const bool write_all, const bool skip_full,
+                                            const unsigned lane, unsigned &cnt, unsigned &and_pre,
+                                            unsigned &and_post) {
+    unsigned t[U], c[U];
+    bool ok[U], have[U];
+    uint4 own[U], acc[U], nw[U];
+    const int32_t *arow[U];
+    const bool own_early = skip_full || dense || a.masks != nullptr;
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+        t[u] = (tile0 + u) * 32u + lane;
+        ok[u] = (tile0 + u) < t_hi && t[u] < a.items;
+        const unsigned v = ok[u] ? a.div_nc.div(t[u]) : v_base;
+        c[u] = t[u] - v * (unsigned)a.nC;
+        arow[u] = adj + (size_t)(v - v_base) * (size_t)d;
+        own[u] = acc[u] = nw[u] = u4zero();
+        have[u] = false;
+        if (ok[u] && own_early) { own[u] = __ldcg(a.V + t[u]); have[u] = true; }
+    }
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+        if (!ok[u] || (skip_full && u4full(own[u]))) continue;
+        if (dense) {
+#pragma unroll 8
+            for (int i = 0; i < d; ++i)
+                or_into(acc[u], __ldcg(Fc + (unsigned)arow[u][i] * (unsigned)a.nC + c[u]));
+        } else {
+#pragma unroll 8
+            for (int i = 0; i < d; ++i) {
+                const unsigned tu = (unsigned)arow[u][i] * (unsigned)a.nC + c[u];
+                if ((__ldcg(fc + (tu >> 5)) >> (tu & 31u)) & 1u) or_into(acc[u], __ldcg(Fc + tu));
+            }
+        }
+    }
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+        if (ok[u]) {
+            if (u4any(acc[u])) {
+                if (!have[u]) { own[u] = __ldcg(a.V + t[u]); have[u] = true; }
+                nw[u] = andnot(acc[u], own[u]);
+                if (u4any(nw[u])) a.V[t[u]] = u4or(own[u], nw[u]);
+            }
+            if (write_all || u4any(nw[u])) Fn[t[u]] = nw[u];
+            if (a.masks) {
+                and_pre &= u4and(own[u]);
+                and_post &= u4and(u4or(own[u], nw[u]));
+            }
+            cnt += u4popc(nw[u]);
+        }
+        const unsigned b = __ballot_sync(0xffffffffu, u4any(nw[u]));
+        if (lane == 0 && (tile0 + u) < t_hi) fn[tile0 + u] = b;
+    }
+}
+
+// Resident blocks per SM the register allocation targets: 6 (40 registers)
+// fits the small degrees without spills; larger degrees keep the default.
+constexpr int min_blocks_for(int D) { return (D > 0 && D <= 8) ? 6 : 1; }
+
 // One cooperative launch = one source batch, all levels.
 template <int D>
-__global__ void __launch_bounds__(kBlock) bfs_batch_kernel(const BfsArgs a) {
+__global__ void __launch_bounds__(kBlock, min_blocks_for(D)) bfs_batch_kernel(const BfsArgs a) {
     const int d = D > 0 ? D : a.d;
     const unsigned lane = threadIdx.x & 31u;
     const unsigned gtid = blockIdx.x * blockDim.x + threadIdx.x;
     const unsigned nthr = gridDim.x * blockDim.x;
-    const unsigned wid = gtid >> 5, nwarps = nthr >> 5;
     const unsigned items = a.items, ntiles = (items + 31u) >> 5;
     __shared__ unsigned long long s_sum[kBlock / 32];
     __shared__ unsigned s_and[2][kBlock / 32];
+    __shared__ unsigned s_next;
     if (a.bad && *a.bad) return;  // uniform across the grid: no block reaches a barrier
+    const unsigned t_lo = (unsigned)((unsigned long long)ntiles * blockIdx.x / gridDim.x);
+    const unsigned t_hi = (unsigned)((unsigned long long)ntiles * (blockIdx.x + 1) / gridDim.x);
+
+    // The block's tile range covers vertices [v_lo, v_hi]; their adjacency rows
+    // stay in shared memory for the whole launch when they fit.
+    extern __shared__ int32_t s_adj[];
+    const int32_t *adj = a.adj;
+    unsigned v_base = 0;
+    if (a.adj_smem_rows > 0 && t_hi > t_lo) {
+        const unsigned v_lo = a.div_nc.div(t_lo * 32u);
+        const unsigned last = min(t_hi * 32u, items) - 1u;
+        const unsigned v_hi = a.div_nc.div(last);
+        const unsigned nv = v_hi - v_lo + 1u;
+        if (nv <= (unsigned)a.adj_smem_rows) {
+            const size_t n = (size_t)nv * (size_t)d;
+            const int32_t *g = a.adj + (size_t)v_lo * (size_t)d;
+            for (size_t k = threadIdx.x; k < n; k += blockDim.x) s_adj[k] = __ldg(g + k);
+            adj = s_adj;
+            v_base = v_lo;
+        }
+        __syncthreads();
+    }
 
     // Phase 0: per-batch reset (cudaASPLconv.cu:9-33): padding bits visited,
     // frontier and flags cleared, counters zeroed.
@@ -202,11 +297,21 @@ __global__ void __launch_bounds__(kBlock) bfs_batch_kernel(const BfsArgs a) {
     }
     if (gtid == 0) a.counts[0] = (unsigned long long)a.ns;
     if (!grid_barrier(a.ctl, a.expected, a.wait_ns, 0)) return;
+    if (a.level_ns && gtid == 0) a.level_ns[0] = gtimer();
 
+    // Per-level access modes.  Every block derives them from the same level
+    // counts (read after the barrier), so writer and reader always agree:
+    //  * write_all(L): F' is stored for every chunk, zeros included, when the
+    //    frontier feeding level L already covered >= dense_w_ppm of the pairs;
+    //  * dense(L): level L reads F without its flag words (one dependent memory
+    //    round trip fewer) when F was written whole and covers >= dense_r_ppm;
+    //  * skip_full(L): own visited chunk first and no gathers when it is full,
+    //    once >= full_skip_ppm of the pairs are reached (late, bottom-up levels).
     const unsigned long long pairs = (unsigned long long)a.ns * (unsigned long long)a.rows;
-    const unsigned long long bu_at =
-        a.bu_permille >= 1000 ? ~0ull : pairs / 1000ull * (unsigned long long)a.bu_permille;
+    const unsigned long long pairs_ppm = pairs;  // compare x*1e6 >= pairs*ppm
     unsigned long long reached = (unsigned long long)a.ns;
+    unsigned long long c_prev = (unsigned long long)a.ns;  // frontier size feeding the level
+    bool wrote_all_prev = true;                               // F0 is zeroed whole in phase 0
 
     for (int L = 1;; ++L) {
         const bool odd = (L & 1) != 0;
@@ -214,45 +319,22 @@ __global__ void __launch_bounds__(kBlock) bfs_batch_kernel(const BfsArgs a) {
         uint4 *Fn = odd ? a.F1 : a.F0;
         const uint32_t *fc = odd ? a.fl0 : a.fl1;
         uint32_t *fn = odd ? a.fl1 : a.fl0;
-        // Own-first ("bottom-up") order once most pairs are reached: a chunk
-        // whose visited bits are all set skips its gathers entirely.
-        const bool own_first = reached > bu_at || a.masks != nullptr;
+        const bool write_all = c_prev * 1000000ull >= pairs_ppm * (unsigned long long)a.dense_w_ppm;
+        const bool dense = wrote_all_prev &&
+                           c_prev * 1000000ull >= pairs_ppm * (unsigned long long)a.dense_r_ppm;
+        const bool skip_full = reached * 1000000ull >= pairs_ppm * (unsigned long long)a.full_skip_ppm;
         unsigned cnt = 0u, and_pre = 0xffffffffu, and_post = 0xffffffffu;
-
-        for (unsigned tile = wid; tile < ntiles; tile += nwarps) {
-            const unsigned t = tile * 32u + lane;
-            uint4 nw = u4zero();
-            if (t < items) {
-                const unsigned v = a.div_nc.div(t);
-                const unsigned c = t - v * (unsigned)a.nC;
-                const int32_t *arow = a.adj + (size_t)v * (size_t)d;
-                uint4 own = u4zero();
-                bool have = false;
-                if (own_first) { own = __ldcg(a.V + t); have = true; }
-                if (!(have && u4full(own))) {
-                    uint4 acc = u4zero();
-#pragma unroll 8
-                    for (int i = 0; i < d; ++i) {
-                        const unsigned tu = (unsigned)__ldg(arow + i) * (unsigned)a.nC + c;
-                        if ((__ldcg(fc + (tu >> 5)) >> (tu & 31u)) & 1u) or_into(acc, __ldcg(Fc + tu));
-                    }
-                    if (u4any(acc)) {
-                        if (!have) { own = __ldcg(a.V + t); have = true; }
-                        nw = andnot(acc, own);
-                        if (u4any(nw)) {
-                            a.V[t] = u4or(own, nw);
-                            Fn[t] = nw;
-                        }
-                    }
-                }
-                if (a.masks) {
-                    and_pre &= u4and(own);
-                    and_post &= u4and(u4or(own, nw));
-                }
-                cnt += u4popc(nw);
-            }
-            const unsigned b = __ballot_sync(0xffffffffu, u4any(nw));
-            if (lane == 0) fn[tile] = b;
+        // Balanced contiguous tile range per block; the block's warps pull
+        // kGrab tiles at a time from it through a shared-memory counter.
+        if (threadIdx.x == 0) s_next = t_lo;
+        __syncthreads();
+        for (;;) {
+            unsigned tile0 = 0;
+            if (lane == 0) tile0 = atomicAdd(&s_next, (unsigned)kGrab);
+            tile0 = __shfl_sync(0xffffffffu, tile0, 0);
+            if (tile0 >= t_hi) break;
+            level_tiles<D, kGrab>(a, d, adj, v_base, tile0, t_hi, Fc, Fn, fc, fn, dense, write_all, skip_full,
+                                  lane, cnt, and_pre, and_post);
         }
 
         // Level reduction: one 64-bit atomic per block (cudaASPLconv.cu:59-99 fused).
@@ -276,8 +358,11 @@ __global__ void __launch_bounds__(kBlock) bfs_batch_kernel(const BfsArgs a) {
             }
         }
         if (!grid_barrier(a.ctl, a.expected, a.wait_ns, L)) return;
+        if (a.level_ns && gtid == 0) a.level_ns[L] = gtimer();
         const unsigned long long cL = ld_relaxed_u64(a.counts + L);
         reached += cL;
+        c_prev = cL;
+        wrote_all_prev = write_all;
         if (cL == 0ull || L >= a.max_levels) {
             if (gtid == 0) a.ctl->levels_run = L;
             break;

@@ -64,7 +64,7 @@ class EvalOpts(ctypes.Structure):
     """gg_eval_opts (include/gg.h)."""
     _fields_ = [("max_levels", ctypes.c_int32), ("src_begin", ctypes.c_int32),
                 ("src_end", ctypes.c_int32), ("want_wvc", ctypes.c_int32),
-                ("level_counts", ctypes.c_void_p)]
+                ("level_counts", ctypes.c_void_p), ("level_ns", ctypes.c_void_p)]
 
 
 _lib = None
@@ -398,13 +398,22 @@ class Engine:
             d["level_counts"] = lc
         return d
 
-    def eval_device(self, dev_ptr, max_levels=0, stream=0):
+    def eval_device(self, dev_ptr, max_levels=0, stream=0, level_ns=False):
         o = EvalOpts()
         o.max_levels = max_levels
+        ns = None
+        if level_ns:
+            if max_levels <= 0:
+                raise GGError(GG_BAD_ARG, "level_ns needs max_levels > 0")
+            ns = np.zeros(max_levels + 1, dtype=np.uint64)
+            o.level_ns = ns.ctypes.data
         r = Result()
         _check(lib().gg_eval_device(self._h, ctypes.c_void_p(dev_ptr), ctypes.byref(o),
                                     ctypes.byref(r), ctypes.c_void_p(stream)))
-        return r.as_dict()
+        d = r.as_dict()
+        if ns is not None:
+            d["level_ns"] = ns
+        return d
 
     def last_device_ms(self):
         ms = ctypes.c_double()

@@ -70,6 +70,9 @@ typedef struct gg_eval_opts {
     int32_t want_wvc;         /* track the per-level AND of the visited words (cudaASPLconv.cu:258-285) */
     uint64_t *level_counts;   /* optional host array [max_levels+1] (or [n_vertices] if uncapped):
                                  pairs first reached at each level, summed over batches */
+    uint64_t *level_ns;       /* optional host array [max_levels+1]: device clock (ns) at the
+                                 end of each level of the first source batch, [0] = start of
+                                 level 1; entries past the last level are 0 */
 } gg_eval_opts;
 
 /* ---- calculator: plain graph (cudaASPLgraph) ------------------------------

@@ -86,7 +86,7 @@ struct gg_engine {
     int nC = 0;                          // uint4 chunks per row
     uint32_t items = 0;
     int grid = 0;
-    int dense_w_ppm = 1000;              // level-mode thresholds (see bfs_batch_kernel)
+    int dense_w_ppm = 100;               // level-mode thresholds (see bfs_batch_kernel)
     int dense_r_ppm = 4000;
     int full_skip_ppm = 995000;
     int adj_smem_rows = 0;               // shared-memory adjacency slice (rows per block)
@@ -181,12 +181,20 @@ gg_status plan(gg_engine *e, int want_bits) {
         if (env > 0) {
             bits = env;
         } else {
-            // All sources in one batch while the three bitsets stay within a
-            // fixed device budget; otherwise the widest batch that fits.
-            const double budget = 6.0e9;
+            // The widest batch whose three bitsets (3 * rows * bits / 8 bytes)
+            // stay within 3/4 of the L2, so that the gathers hit L2 rather than
+            // HBM; at least 4096 sources (one 512-byte row segment per vertex)
+            // when there are that many.
+            int l2 = 0;
+            if (cudaDeviceGetAttribute(&l2, cudaDevAttrL2CacheSize, e->device) != cudaSuccess || l2 <= 0) {
+                (void)cudaGetLastError();
+                l2 = 64 << 20;
+            }
             const double per_bit = 3.0 * e->rows / 8.0;
-            long long fit = (long long)(budget / per_bit);
+            long long fit = (long long)(0.75 * l2 / per_bit);
+            fit = std::max<long long>(fit, 4096);
             bits = (int)std::min<long long>(fit, n_src);
+            if (bits > 4096) bits = (bits / 4096) * 4096;
         }
     }
     bits = std::max(128, ((std::min(bits, std::max(n_src, 1)) + 127) / 128) * 128);

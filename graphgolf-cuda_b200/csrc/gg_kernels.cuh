@@ -48,13 +48,16 @@ struct FastDiv {
 };
 
 // Control block of one cooperative launch (zeroed by the host before launch).
+constexpr int kBarSub = 16;   // first-level arrival counters of the grid barrier
+
 struct Ctl {
-    unsigned int bar_count;   // arrivals at the current barrier
+    unsigned int bar_count;   // second-level arrivals at the current barrier
     unsigned int bar_gen;     // barrier generation
     int err;                  // 0, or 1 = a barrier wait exceeded the limit
     int err_level;            // level at which the first wait gave up
     int levels_run;           // last level executed
-    int pad[3];
+    int pad[27];
+    unsigned int sub[kBarSub][32];  // first-level counters, one 128-byte line each
 };
 
 struct BfsArgs {
@@ -102,22 +105,39 @@ __device__ __forceinline__ unsigned long long ld_relaxed_u64(const unsigned long
 }
 
 // Grid-wide barrier with a bounded wait.  Requires co-resident blocks
-// (cooperative launch).  Returns false on every block once any block's wait
-// ran past the limit; the kernel then returns and the host reports GG_TIMEOUT.
+// (cooperative launch).  Arrival is two-level: block b counts on sub-counter
+// b % kBarSub, and the last arrival of each sub-counter counts on the top one,
+// so no counter sees more than ~gridDim/kBarSub same-address atomics.
+// `expected` is the number of arrivals the barrier waits for (gridDim.x, or
+// more when a test makes the wait run out).  Returns false on every block once
+// any block's wait ran past the limit; the kernel then returns and the host
+// reports GG_TIMEOUT.
 __device__ __forceinline__ bool grid_barrier(Ctl *ctl, unsigned expected, long long wait_ns,
                                              int level) {
     __shared__ int s_ok;
     __syncthreads();
     if (threadIdx.x == 0) {
         int ok = 1;
+        const unsigned nb = gridDim.x;
+        const unsigned s = blockIdx.x % kBarSub;
+        const unsigned sub_expected = (nb - s + kBarSub - 1) / kBarSub;  // blocks b < nb with b%kBarSub == s
+        const unsigned top_expected = min(nb, (unsigned)kBarSub) + (expected - nb);
         const unsigned gen = ld_acquire(&ctl->bar_gen);
         __threadfence();
-        const unsigned prev = atomicAdd(&ctl->bar_count, 1u);
-        if (prev + 1 == expected) {
-            atomicExch(&ctl->bar_count, 0u);
+        bool released = false;
+        const unsigned prev = atomicAdd(&ctl->sub[s][0], 1u);
+        if (prev + 1 == sub_expected) {
+            atomicExch(&ctl->sub[s][0], 0u);
             __threadfence();
-            atomicAdd(&ctl->bar_gen, 1u);
-        } else {
+            const unsigned prev2 = atomicAdd(&ctl->bar_count, 1u);
+            if (prev2 + 1 == top_expected) {
+                atomicExch(&ctl->bar_count, 0u);
+                __threadfence();
+                atomicAdd(&ctl->bar_gen, 1u);
+                released = true;
+            }
+        }
+        if (!released) {
             const unsigned long long t0 = gtimer();
             while (ld_acquire(&ctl->bar_gen) == gen) {
                 if (ld_acquire_i(&ctl->err)) { ok = 0; break; }
@@ -201,12 +221,30 @@ __device__ __forceinline__ void level_tiles(const BfsArgs &a, const int d, const
 #pragma unroll
     for (int u = 0; u < U; ++u) {
         if (!ok[u] || (skip_full && u4full(own[u]))) continue;
-        if (dense) {
-#pragma unroll 8
+        if constexpr (D > 0) {
+            // Staged so that each step's loads are all in flight together:
+            // neighbour ids, then (sparse) their flag words, then the gathers.
+            unsigned tu[D];
+#pragma unroll
+            for (int i = 0; i < D; ++i) tu[i] = (unsigned)arow[u][i] * (unsigned)a.nC + c[u];
+            if (dense) {
+                uint4 x[D];
+#pragma unroll
+                for (int i = 0; i < D; ++i) x[i] = __ldcg(Fc + tu[i]);
+#pragma unroll
+                for (int i = 0; i < D; ++i) or_into(acc[u], x[i]);
+            } else {
+                unsigned fw[D];
+#pragma unroll
+                for (int i = 0; i < D; ++i) fw[i] = __ldcg(fc + (tu[i] >> 5));
+#pragma unroll
+                for (int i = 0; i < D; ++i)
+                    if ((fw[i] >> (tu[i] & 31u)) & 1u) or_into(acc[u], __ldcg(Fc + tu[i]));
+            }
+        } else if (dense) {
             for (int i = 0; i < d; ++i)
                 or_into(acc[u], __ldcg(Fc + (unsigned)arow[u][i] * (unsigned)a.nC + c[u]));
         } else {
-#pragma unroll 8
             for (int i = 0; i < d; ++i) {
                 const unsigned tu = (unsigned)arow[u][i] * (unsigned)a.nC + c[u];
                 if ((__ldcg(fc + (tu >> 5)) >> (tu & 31u)) & 1u) or_into(acc[u], __ldcg(Fc + tu));
@@ -234,8 +272,8 @@ __device__ __forceinline__ void level_tiles(const BfsArgs &a, const int d, const
 }
 
 // Resident blocks per SM the register allocation targets: 6 (40 registers)
-// fits the small degrees without spills; larger degrees keep the default.
-constexpr int min_blocks_for(int D) { return (D > 0 && D <= 8) ? 6 : 1; }
+// fits the small degrees without spills, 4 (64 registers) the larger ones.
+__host__ __device__ constexpr int min_blocks_for(int D) { return (D > 0 && D <= 8) ? 6 : 4; }
 
 // One cooperative launch = one source batch, all levels.
 template <int D>
@@ -333,8 +371,8 @@ __global__ void __launch_bounds__(kBlock, min_blocks_for(D)) bfs_batch_kernel(co
             if (lane == 0) tile0 = atomicAdd(&s_next, (unsigned)kGrab);
             tile0 = __shfl_sync(0xffffffffu, tile0, 0);
             if (tile0 >= t_hi) break;
-            level_tiles<D, kGrab>(a, d, adj, v_base, tile0, t_hi, Fc, Fn, fc, fn, dense, write_all, skip_full,
-                                  lane, cnt, and_pre, and_post);
+            level_tiles<D, kGrab>(a, d, adj, v_base, tile0, t_hi, Fc, Fn, fc, fn, dense, write_all,
+                                  skip_full, lane, cnt, and_pre, and_post);
         }
 
         // Level reduction: one 64-bit atomic per block (cudaASPLconv.cu:59-99 fused).
@@ -363,7 +401,9 @@ __global__ void __launch_bounds__(kBlock, min_blocks_for(D)) bfs_batch_kernel(co
         reached += cL;
         c_prev = cL;
         wrote_all_prev = write_all;
-        if (cL == 0ull || L >= a.max_levels) {
+        // Stop on an empty level, at the cap, or as soon as every pair is reached
+        // (the next level is then empty by construction).
+        if (cL == 0ull || L >= a.max_levels || reached == pairs) {
             if (gtid == 0) a.ctl->levels_run = L;
             break;
         }

@@ -154,7 +154,7 @@ extern "C" gg_status gg_graph_eval_noalloc(const int32_t *d_adj, int N, int degr
     a.items = items;
     a.rows = N; a.d = degree; a.nC = nC;
     a.max_levels = max_levels;
-    a.dense_w_ppm = 1000;
+    a.dense_w_ppm = 100;
     a.dense_r_ppm = 4000;
     a.full_skip_ppm = 995000;
     a.wait_ns = 10ll * 1000 * 1000 * 1000;

@@ -73,6 +73,27 @@ def build_shim(force=False):
     return SHIM_LIB
 
 
+DRIVER_SRC = os.path.join(ROOT, "tests", "shim_driver.cpp")
+DRIVER_BIN = os.path.join(ROOT, "tests", "_bin", "shim_driver")
+
+
+def build_driver(force=False):
+    """tests/_bin/shim_driver: the reference-style caller of libgg_refshim.so
+    (compiled against the reference headers; skipped when they are absent)."""
+    hdr = os.path.join(REF, "cudacode", "cudaASPLconv.hpp")
+    if not os.path.exists(hdr) or not os.path.exists(SHIM_LIB):
+        return None
+    if not force and not _stale(DRIVER_BIN, [DRIVER_SRC, SHIM_LIB]):
+        return DRIVER_BIN
+    os.makedirs(os.path.dirname(DRIVER_BIN), exist_ok=True)
+    cmd = ["g++", "-O2", "-std=c++17", "-I", os.path.join(REF, "cudacode"),
+           "-I", os.path.join(REF, "cppcode"), "-o", DRIVER_BIN, DRIVER_SRC,
+           "-L", PKG, "-lgg_refshim", "-lggb200",
+           "-Wl,-rpath,$ORIGIN/../../graphgolf-cuda_b200"]
+    _run(cmd)
+    return DRIVER_BIN
+
+
 def build_oracle():
     """The oracle (test infrastructure) and, when the reference tree is here,
     the reference's own calculators in oracle/_ref/."""
@@ -85,6 +106,7 @@ def build_oracle():
 def build_all(force=False):
     build_engine(force)
     build_shim(force)
+    build_driver(force)
     build_oracle()
 
 

@@ -1,0 +1,444 @@
+// gg_batch.cu -- batched exact evaluation of 2-opt candidates (gg_batch_* in gg.h).
+//
+// One persistent launch scores every candidate of a batch.  Work unit ("task") =
+// one candidate x one chunk of its sources.  A CTA takes a task, builds the
+// candidate's adjacency in shared memory (the base rows as uint16, then the four
+// rows the 2-opt edit touches), and runs the whole BFS of the chunk's sources
+// with both visited bitsets resident in shared memory:
+//     next[v][c] = cur[v][c] | (OR_{u in adj[v]} cur[u][c])        (all rows, one level)
+// i.e. the level step of cudaASPLconv.cu:35-56 with the reduction of :59-99
+// folded into per-thread popcounts and one __syncthreads_or per level.  The grid
+// barrier of the single-graph path is not needed: a task never leaves its CTA.
+//
+// Task order: t -> chunk = maxchunks-1 - t / n_cand, cand = t % n_cand, so the
+// extra chunks of the largest bases come first and the common chunks fill the
+// tail (largest-first scheduling with no task list on the host).  Both n_cand and
+// maxchunks are read from device memory, so one captured CUDA graph serves every
+// batch size up to the capacity it was captured for.
+#include "gg.h"
+
+#include <algorithm>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+namespace gg {
+void set_last_error(const char *msg);  // gg_engine.cu
+}
+
+namespace {
+
+constexpr int kBatchBlock = 1024;
+constexpr size_t kSmemBudget = 220 * 1024;
+
+struct BatchBase {
+    const int32_t *adj;   // [n][d] in global memory
+    int n, d;
+    int log_nc;           // chunks (of 128 sources) per task row = 1 << log_nc
+    int chunks;           // tasks per candidate = ceil(n / (128 << log_nc))
+};
+
+struct BatchCtl {
+    unsigned task_ctr;
+    int n_cand;
+    int max_chunks;
+    int pad;
+};
+
+struct BatchArgs {
+    const BatchBase *bases;
+    const gg_swap *cands;
+    gg_cand_result *out;
+    BatchCtl *ctl;
+};
+
+__device__ __forceinline__ uint4 z4() { return make_uint4(0u, 0u, 0u, 0u); }
+__device__ __forceinline__ unsigned padw(int lo, int ns) {
+    if (ns <= lo) return 0xffffffffu;
+    if (ns >= lo + 32) return 0u;
+    return ~((1u << (ns - lo)) - 1u);
+}
+
+__global__ void __launch_bounds__(kBatchBlock, 1) batch_kernel(const BatchArgs a) {
+    extern __shared__ uint4 sm[];
+    __shared__ unsigned s_task;
+    __shared__ unsigned long long s_tot[kBatchBlock / 32], s_reach[kBatchBlock / 32];
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int n_cand = a.ctl->n_cand, max_chunks = a.ctl->max_chunks;
+    const unsigned n_tasks = (unsigned)n_cand * (unsigned)max_chunks;
+
+    for (;;) {
+        if (tid == 0) s_task = atomicAdd(&a.ctl->task_ctr, 1u);
+        __syncthreads();
+        const unsigned task = s_task;
+        if (task >= n_tasks) return;
+        const int cand = (int)(task % (unsigned)n_cand);
+        const int chunk = max_chunks - 1 - (int)(task / (unsigned)n_cand);
+        const gg_swap sw = a.cands[cand];
+        const BatchBase B = a.bases[sw.base];
+        if (chunk >= B.chunks) {  // this candidate has fewer chunks
+            __syncthreads();
+            continue;
+        }
+        const int n = B.n, d = B.d, lnc = B.log_nc, nC = 1 << lnc;
+        const int S = 128 << lnc;
+        const int s0 = chunk * S;
+        const int ns = min(S, n - s0);
+        const int items = n << lnc;
+
+        // shared memory: adjacency (uint16, padded to 16 bytes), then two bitsets
+        uint16_t *adj = reinterpret_cast<uint16_t *>(sm);
+        uint4 *cur = sm + (((size_t)n * d * 2 + 15) / 16);
+        uint4 *nxt = cur + items;
+        for (int k = tid; k < n * d; k += kBatchBlock) adj[k] = (uint16_t)B.adj[k];
+        __syncthreads();
+        if (sw.a >= 0 && tid < 4) {
+            // 2-opt: (a,b),(c,d) -> (a,c),(b,d) [mode 0] or (a,d),(b,c) [mode 1]
+            const int x[4] = {sw.a, sw.b, sw.c, sw.d};
+            const int from[4] = {sw.b, sw.a, sw.d, sw.c};
+            const int to0[4] = {sw.c, sw.d, sw.a, sw.b};
+            const int to1[4] = {sw.d, sw.c, sw.b, sw.a};
+            const int row = x[tid], f = from[tid], t = sw.mode ? to1[tid] : to0[tid];
+            for (int j = 0; j < d; ++j)
+                if (adj[row * d + j] == (uint16_t)f) { adj[row * d + j] = (uint16_t)t; break; }
+        }
+        // visited after level 0: the diagonal plus the padding sources
+        for (int t = tid; t < items; t += kBatchBlock) {
+            const int v = t >> lnc, c = t & (nC - 1);
+            const int b = c * 128;
+            uint4 w = make_uint4(padw(b, ns), padw(b + 32, ns), padw(b + 64, ns), padw(b + 96, ns));
+            const int i = v - s0;
+            if (i >= b && i < b + 128 && i < ns) {
+                const unsigned bit = 1u << (i & 31);
+                switch ((i - b) >> 5) {
+                    case 0: w.x |= bit; break;
+                    case 1: w.y |= bit; break;
+                    case 2: w.z |= bit; break;
+                    default: w.w |= bit; break;
+                }
+            }
+            cur[t] = w;
+        }
+        __syncthreads();
+
+        unsigned long long tot = 0, reach = 0;
+        int L = 1;
+        for (;; ++L) {
+            unsigned cnt = 0;
+            for (int t = tid; t < items; t += kBatchBlock) {
+                const int v = t >> lnc, c = t & (nC - 1);
+                const uint4 own = cur[t];
+                uint4 out = own;
+                if ((own.x & own.y & own.z & own.w) != 0xffffffffu) {
+                    uint4 acc = z4();
+                    const uint16_t *ar = adj + v * d;
+                    for (int i = 0; i < d; ++i) {
+                        const uint4 x = cur[((int)ar[i] << lnc) + c];
+                        acc.x |= x.x; acc.y |= x.y; acc.z |= x.z; acc.w |= x.w;
+                    }
+                    out = make_uint4(own.x | acc.x, own.y | acc.y, own.z | acc.z, own.w | acc.w);
+                    cnt += __popc(acc.x & ~own.x) + __popc(acc.y & ~own.y) + __popc(acc.z & ~own.z) +
+                           __popc(acc.w & ~own.w);
+                }
+                nxt[t] = out;
+            }
+            tot += (unsigned long long)L * cnt;
+            reach += cnt;
+            if (!__syncthreads_or(cnt != 0)) break;
+            uint4 *sw2 = cur; cur = nxt; nxt = sw2;
+        }
+        // L is the first level without new pairs
+        unsigned long long wt = tot, wr = reach;
+        for (int o = 16; o; o >>= 1) {
+            wt += __shfl_down_sync(0xffffffffu, wt, o);
+            wr += __shfl_down_sync(0xffffffffu, wr, o);
+        }
+        if (lane == 0) { s_tot[warp] = wt; s_reach[warp] = wr; }
+        __syncthreads();
+        if (tid == 0) {
+            unsigned long long bt = 0, br = (unsigned long long)ns;
+            for (int w = 0; w < kBatchBlock / 32; ++w) { bt += s_tot[w]; br += s_reach[w]; }
+            atomicAdd(reinterpret_cast<unsigned long long *>(&a.out[cand].total), bt);
+            atomicAdd(reinterpret_cast<unsigned long long *>(&a.out[cand].reached), br);
+            atomicMax(&a.out[cand].levels, L - 1);
+        }
+        __syncthreads();  // the next task overwrites shared memory
+    }
+}
+
+__global__ void batch_finalize(const BatchArgs a) {
+    const int n_cand = a.ctl->n_cand;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n_cand; i += gridDim.x * blockDim.x) {
+        const BatchBase B = a.bases[a.cands[i].base];
+        a.out[i].connected = a.out[i].reached == (unsigned long long)B.n * (unsigned long long)B.n;
+    }
+}
+
+__global__ void batch_reset(const BatchArgs a) {
+    const int n_cand = a.ctl->n_cand;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n_cand; i += gridDim.x * blockDim.x)
+        a.out[i] = gg_cand_result{0ull, 0ull, 0, 0};
+    if (blockIdx.x == 0 && threadIdx.x == 0) a.ctl->task_ctr = 0u;
+}
+
+gg_status bfail(gg_status s, const std::string &m) {
+    (void)cudaGetLastError();
+    gg::set_last_error(m.c_str());
+    return s;
+}
+
+#define GB_CK(call)                                                                          \
+    do {                                                                                     \
+        cudaError_t e_ = (call);                                                             \
+        if (e_ != cudaSuccess)                                                               \
+            return bfail(e_ == cudaErrorMemoryAllocation ? GG_OUT_OF_MEMORY : GG_CUDA_ERROR, \
+                         std::string(#call) + ": " + cudaGetErrorString(e_));                \
+    } while (0)
+
+}  // namespace
+
+struct gg_batch {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    std::vector<BatchBase> bases;          // host copy (adj = device pointers)
+    std::vector<int32_t *> base_adj;       // device adjacency per base
+    BatchBase *d_bases = nullptr;
+    BatchCtl *d_ctl = nullptr, *h_ctl = nullptr;
+    int cap = 0;                           // candidates the buffers hold
+    gg_swap *d_cands = nullptr, *h_cands = nullptr;
+    gg_cand_result *d_out = nullptr, *h_out = nullptr;
+    size_t smem = 0;
+    int grid = 0;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    const gg_swap *graph_cands = nullptr;  // pointers baked into the graph
+    gg_cand_result *graph_out = nullptr;
+    cudaStream_t graph_stream = nullptr;
+    double last_ms = 0.0;
+};
+
+namespace {
+
+void drop_graph(gg_batch *b) {
+    if (b->exec) cudaGraphExecDestroy(b->exec);
+    if (b->graph) cudaGraphDestroy(b->graph);
+    b->exec = nullptr;
+    b->graph = nullptr;
+}
+
+// Smallest chunk count per task row (a power of two) whose bitsets and
+// adjacency fit the shared-memory budget, as wide as possible.
+int auto_log_nc(int n, int d) {
+    const size_t adj = ((size_t)n * d * 2 + 15) / 16 * 16;
+    int best = -1;
+    for (int l = 0; l <= 4; ++l) {
+        const size_t need = adj + 2 * (size_t)n * (16u << l);
+        if (need <= kSmemBudget) best = l;
+        if ((128 << l) >= n) break;
+    }
+    return best;
+}
+
+gg_status refresh_plan(gg_batch *b) {
+    size_t smem = 0;
+    int max_chunks = 1;
+    for (auto &B : b->bases) {
+        const size_t need = ((size_t)B.n * B.d * 2 + 15) / 16 * 16 + 2 * (size_t)B.n * (16u << B.log_nc);
+        smem = std::max(smem, need);
+        max_chunks = std::max(max_chunks, B.chunks);
+    }
+    b->smem = smem;
+    GB_CK(cudaFuncSetAttribute(batch_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    int per_sm = 0, sms = 0;
+    GB_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, batch_kernel, kBatchBlock, smem));
+    GB_CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, b->device));
+    if (per_sm < 1) return bfail(GG_BAD_ARG, "batch task does not fit in shared memory");
+    b->grid = per_sm * sms;
+    b->h_ctl->max_chunks = max_chunks;
+    GB_CK(cudaMemcpy(b->d_bases, b->bases.data(), b->bases.size() * sizeof(BatchBase),
+                     cudaMemcpyHostToDevice));
+    drop_graph(b);
+    return GG_OK;
+}
+
+gg_status ensure_cap(gg_batch *b, int n) {
+    if (n <= b->cap) return GG_OK;
+    const int cap = std::max(n, 2 * b->cap);
+    cudaFree(b->d_cands); cudaFree(b->d_out);
+    cudaFreeHost(b->h_cands); cudaFreeHost(b->h_out);
+    b->d_cands = nullptr; b->d_out = nullptr; b->h_cands = nullptr; b->h_out = nullptr;
+    GB_CK(cudaMalloc(&b->d_cands, (size_t)cap * sizeof(gg_swap)));
+    GB_CK(cudaMalloc(&b->d_out, (size_t)cap * sizeof(gg_cand_result)));
+    GB_CK(cudaMallocHost(&b->h_cands, (size_t)cap * sizeof(gg_swap)));
+    GB_CK(cudaMallocHost(&b->h_out, (size_t)cap * sizeof(gg_cand_result)));
+    b->cap = cap;
+    drop_graph(b);
+    return GG_OK;
+}
+
+// Enqueue reset -> batch kernel -> finalize on `st` for candidates `cands`,
+// results `out`; the candidate count and task geometry come from d_ctl.
+gg_status enqueue(gg_batch *b, const gg_swap *cands, gg_cand_result *out, cudaStream_t st) {
+    BatchArgs a{b->d_bases, cands, out, b->d_ctl};
+    batch_reset<<<64, 256, 0, st>>>(a);
+    batch_kernel<<<b->grid, kBatchBlock, b->smem, st>>>(a);
+    batch_finalize<<<64, 256, 0, st>>>(a);
+    GB_CK(cudaGetLastError());
+    return GG_OK;
+}
+
+gg_status validate(const gg_batch *b, int n_cand, const gg_swap *c) {
+    for (int i = 0; i < n_cand; ++i) {
+        const gg_swap &s = c[i];
+        if (s.base < 0 || s.base >= (int)b->bases.size())
+            return bfail(GG_BAD_ARG, "candidate " + std::to_string(i) + ": unknown base");
+        if (s.a < 0) continue;
+        const int n = b->bases[s.base].n;
+        if (s.a >= n || s.b < 0 || s.b >= n || s.c < 0 || s.c >= n || s.d < 0 || s.d >= n ||
+            (s.mode != 0 && s.mode != 1))
+            return bfail(GG_BAD_ARG, "candidate " + std::to_string(i) + ": vertex or mode out of range");
+        if (s.a == s.b || s.a == s.c || s.a == s.d || s.b == s.c || s.b == s.d || s.c == s.d)
+            return bfail(GG_BAD_ARG, "candidate " + std::to_string(i) + ": endpoints must be distinct");
+    }
+    return GG_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+gg_status gg_batch_create(int device, gg_batch **out) {
+    if (!out) return bfail(GG_BAD_ARG, "null out");
+    *out = nullptr;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return bfail(GG_NO_DEVICE, "no CUDA device");
+    if (device < 0 || device >= ndev) return bfail(GG_NO_DEVICE, "device index out of range");
+    gg_batch *b = new gg_batch();
+    b->device = device;
+    auto fail_and_free = [&](gg_status s) { gg_batch_destroy(b); return s; };
+    if (cudaSetDevice(device) != cudaSuccess ||
+        cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreate(&b->ev0) != cudaSuccess || cudaEventCreate(&b->ev1) != cudaSuccess ||
+        cudaMalloc(&b->d_ctl, sizeof(BatchCtl)) != cudaSuccess ||
+        cudaMallocHost(&b->h_ctl, sizeof(BatchCtl)) != cudaSuccess ||
+        cudaMalloc(&b->d_bases, 256 * sizeof(BatchBase)) != cudaSuccess)
+        return fail_and_free(bfail(GG_CUDA_ERROR, "batch set-up failed"));
+    std::memset(b->h_ctl, 0, sizeof(BatchCtl));
+    *out = b;
+    return GG_OK;
+}
+
+gg_status gg_batch_add_base(gg_batch *b, int n, int degree, const int32_t *adj, int *base_id) {
+    if (!b || !adj || !base_id || n < 1 || n > 65535 || degree < 1 || b->bases.size() >= 256)
+        return bfail(GG_BAD_ARG, "need 1 <= n <= 65535, degree >= 1, at most 256 bases");
+    for (long long k = 0; k < (long long)n * degree; ++k)
+        if (adj[k] < 0 || adj[k] >= n) return bfail(GG_BAD_ARG, "adjacency entry outside [0, n)");
+    const int lnc = auto_log_nc(n, degree);
+    if (lnc < 0) return bfail(GG_BAD_ARG, "base graph too large for a shared-memory task");
+    GB_CK(cudaSetDevice(b->device));
+    int32_t *d = nullptr;
+    GB_CK(cudaMalloc(&d, (size_t)n * degree * sizeof(int32_t)));
+    GB_CK(cudaMemcpy(d, adj, (size_t)n * degree * sizeof(int32_t), cudaMemcpyHostToDevice));
+    BatchBase B{d, n, degree, lnc, (n + (128 << lnc) - 1) / (128 << lnc)};
+    b->bases.push_back(B);
+    b->base_adj.push_back(d);
+    *base_id = (int)b->bases.size() - 1;
+    return refresh_plan(b);
+}
+
+gg_status gg_batch_set_chunk(gg_batch *b, int base_id, int sources) {
+    if (!b || base_id < 0 || base_id >= (int)b->bases.size() || sources < 128 || sources % 128)
+        return bfail(GG_BAD_ARG, "bad base or chunk width");
+    int l = 0;
+    while ((128 << l) < sources) ++l;
+    if ((128 << l) != sources) return bfail(GG_BAD_ARG, "chunk width must be 128 * 2^k");
+    BatchBase &B = b->bases[base_id];
+    const size_t need = ((size_t)B.n * B.d * 2 + 15) / 16 * 16 + 2 * (size_t)B.n * (16u << l);
+    if (need > kSmemBudget) return bfail(GG_BAD_ARG, "chunk does not fit in shared memory");
+    B.log_nc = l;
+    B.chunks = (B.n + (128 << l) - 1) / (128 << l);
+    GB_CK(cudaSetDevice(b->device));
+    return refresh_plan(b);
+}
+
+gg_status gg_batch_eval(gg_batch *b, int n_cand, const gg_swap *cands, gg_cand_result *out) {
+    if (!b || n_cand < 0 || (n_cand && (!cands || !out))) return bfail(GG_BAD_ARG, "bad arguments");
+    if (n_cand == 0) return GG_OK;
+    gg_status s = validate(b, n_cand, cands);
+    if (s != GG_OK) return s;
+    GB_CK(cudaSetDevice(b->device));
+    s = ensure_cap(b, n_cand);
+    if (s != GG_OK) return s;
+    std::memcpy(b->h_cands, cands, (size_t)n_cand * sizeof(gg_swap));
+    b->h_ctl->n_cand = n_cand;
+    b->h_ctl->task_ctr = 0;
+    GB_CK(cudaMemcpyAsync(b->d_cands, b->h_cands, (size_t)n_cand * sizeof(gg_swap),
+                          cudaMemcpyHostToDevice, b->stream));
+    GB_CK(cudaMemcpyAsync(b->d_ctl, b->h_ctl, sizeof(BatchCtl), cudaMemcpyHostToDevice, b->stream));
+    if (!b->exec) {  // capture reset -> kernel -> finalize once per buffer set
+        GB_CK(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
+        gg_status es = enqueue(b, b->d_cands, b->d_out, b->stream);
+        cudaGraph_t g = nullptr;
+        cudaError_t ce = cudaStreamEndCapture(b->stream, &g);
+        if (es != GG_OK) { if (g) cudaGraphDestroy(g); return es; }
+        GB_CK(ce);
+        b->graph = g;
+        GB_CK(cudaGraphInstantiate(&b->exec, b->graph, 0));
+    }
+    GB_CK(cudaEventRecord(b->ev0, b->stream));
+    GB_CK(cudaGraphLaunch(b->exec, b->stream));
+    GB_CK(cudaEventRecord(b->ev1, b->stream));
+    GB_CK(cudaMemcpyAsync(b->h_out, b->d_out, (size_t)n_cand * sizeof(gg_cand_result),
+                          cudaMemcpyDeviceToHost, b->stream));
+    GB_CK(cudaStreamSynchronize(b->stream));
+    float ms = 0.f;
+    GB_CK(cudaEventElapsedTime(&ms, b->ev0, b->ev1));
+    b->last_ms = ms;
+    std::memcpy(out, b->h_out, (size_t)n_cand * sizeof(gg_cand_result));
+    return GG_OK;
+}
+
+gg_status gg_batch_eval_device(gg_batch *b, int n_cand, const gg_swap *d_cands,
+                               gg_cand_result *d_out, void *stream) {
+    if (!b || n_cand < 0 || (n_cand && (!d_cands || !d_out))) return bfail(GG_BAD_ARG, "bad arguments");
+    if (n_cand == 0) return GG_OK;
+    GB_CK(cudaSetDevice(b->device));
+    cudaStream_t st = stream ? (cudaStream_t)stream : b->stream;
+    b->h_ctl->n_cand = n_cand;
+    b->h_ctl->task_ctr = 0;
+    GB_CK(cudaMemcpyAsync(b->d_ctl, b->h_ctl, sizeof(BatchCtl), cudaMemcpyHostToDevice, st));
+    GB_CK(cudaEventRecord(b->ev0, st));
+    gg_status s = enqueue(b, d_cands, d_out, st);
+    if (s != GG_OK) return s;
+    GB_CK(cudaEventRecord(b->ev1, st));
+    return GG_OK;
+}
+
+gg_status gg_batch_last_ms(gg_batch *b, double *ms) {
+    if (!b || !ms) return bfail(GG_BAD_ARG, "null argument");
+    float f = 0.f;
+    if (cudaEventElapsedTime(&f, b->ev0, b->ev1) == cudaSuccess) b->last_ms = f;
+    else (void)cudaGetLastError();
+    *ms = b->last_ms;
+    return GG_OK;
+}
+
+gg_status gg_batch_destroy(gg_batch *b) {
+    if (!b) return GG_OK;
+    cudaSetDevice(b->device);
+    if (b->stream) cudaStreamSynchronize(b->stream);
+    drop_graph(b);
+    for (auto p : b->base_adj) cudaFree(p);
+    cudaFree(b->d_bases); cudaFree(b->d_ctl); cudaFreeHost(b->h_ctl);
+    cudaFree(b->d_cands); cudaFree(b->d_out); cudaFreeHost(b->h_cands); cudaFreeHost(b->h_out);
+    if (b->ev0) cudaEventDestroy(b->ev0);
+    if (b->ev1) cudaEventDestroy(b->ev1);
+    if (b->stream) cudaStreamDestroy(b->stream);
+    delete b;
+    return GG_OK;
+}
+
+}  // extern "C"

@@ -142,6 +142,43 @@ gg_status gg_gen_random_regular(int n, int d, uint64_t seed, int32_t *adj) {
     return GG_BAD_ARG;
 }
 
+gg_status gg_gen_swaps(int n, int degree, const int32_t *adj, int base_id, int count, uint64_t seed,
+                       gg_swap *out) {
+    if (!adj || !out || n < 4 || degree < 1 || count < 0) return GG_BAD_ARG;
+    // undirected edge list, each edge once
+    std::vector<std::pair<int, int>> E;
+    for (int v = 0; v < n; ++v)
+        for (int k = 0; k < degree; ++k) {
+            const int u = adj[(size_t)v * degree + k];
+            if (u < 0 || u >= n) return GG_BAD_ARG;
+            if (v < u) E.emplace_back(v, u);
+        }
+    if (E.size() < 2) return GG_BAD_ARG;
+    auto has_edge = [&](int x, int y) {
+        for (int k = 0; k < degree; ++k)
+            if (adj[(size_t)x * degree + k] == y) return true;
+        return false;
+    };
+    Rng rng(seed);
+    const uint32_t m = (uint32_t)E.size();
+    for (int i = 0; i < count; ++i) {
+        for (int tries = 0;; ++tries) {
+            if (tries > 1000000) return GG_BAD_ARG;
+            auto e1 = E[rng.below(m)], e2 = E[rng.below(m)];
+            if (rng.below(2)) std::swap(e1.first, e1.second);
+            if (rng.below(2)) std::swap(e2.first, e2.second);
+            const int a = e1.first, b = e1.second, c = e2.first, d = e2.second;
+            if (a == c || a == d || b == c || b == d) continue;  // needs two disjoint edges
+            const int mode = (int)rng.below(2);
+            const int p = mode ? d : c, q = mode ? c : d;       // new edges (a,p), (b,q)
+            if (has_edge(a, p) || has_edge(b, q)) continue;    // would repeat an edge
+            out[i] = gg_swap{base_id, a, b, c, d, mode};
+            break;
+        }
+    }
+    return GG_OK;
+}
+
 gg_status gg_gen_cyclic_lift(int m, int g, int d, uint64_t seed, int32_t *diffs) {
     if (!diffs || m < 1 || g < 1 || d < 1 || ((long long)m * d) % 2 != 0 ||
         (long long)m * g >= (1ll << 31))

@@ -96,6 +96,14 @@ _SIGS = {
     "gg_set_wait_limit_ms": [_P, _I],
     "gg_destroy": [_P],
     "gg_graph_eval_noalloc": [_P, _I, _I, _I, _P, _P],
+    "gg_batch_create": [_I, _EPP],
+    "gg_batch_add_base": [_P, _I, _I, _P, _IP],
+    "gg_batch_set_chunk": [_P, _I, _I],
+    "gg_batch_eval": [_P, _I, _P, _P],
+    "gg_batch_eval_device": [_P, _I, _P, _P, _P],
+    "gg_batch_last_ms": [_P, _DP],
+    "gg_batch_destroy": [_P],
+    "gg_gen_swaps": [_I, _I, _P, _I, _I, ctypes.c_uint64, _P],
     "gg_gen_random_regular": [_I, _I, ctypes.c_uint64, _P],
     "gg_gen_cyclic_lift": [_I, _I, _I, ctypes.c_uint64, _P],
 }
@@ -547,3 +555,80 @@ class cudaASPLbeamer(Engine):
         a = ctypes.c_double()
         _check(lib().gg_beamer_calc(self._h, _ptr(t), int(bool(regular)), ctypes.byref(a)))
         return a.value
+
+
+# ----------------------------------------------------------------------------
+# Batched candidate evaluation (gg_batch_* in include/gg.h)
+# ----------------------------------------------------------------------------
+
+SWAP_DTYPE = np.dtype([("base", np.int32), ("a", np.int32), ("b", np.int32), ("c", np.int32),
+                       ("d", np.int32), ("mode", np.int32)])
+CAND_RESULT_DTYPE = np.dtype([("total", np.uint64), ("reached", np.uint64), ("levels", np.int32),
+                              ("connected", np.int32)])
+
+
+def gen_swaps(adj, base_id, count, seed):
+    """Uniform random 2-opt proposals (no loops, no repeated edges) -> SWAP_DTYPE array."""
+    adj = _i32(adj)
+    n, d = adj.shape
+    out = np.zeros(count, dtype=SWAP_DTYPE)
+    _check(lib().gg_gen_swaps(n, d, _ptr(adj), base_id, count, seed, _ptr(out)))
+    return out
+
+
+def apply_swap(adj, s):
+    """Host copy of the edit the batch kernel applies (first occurrence replaced)."""
+    adj = np.array(adj, dtype=np.int32, copy=True)
+    if s["a"] < 0:
+        return adj
+    a, b, c, d = int(s["a"]), int(s["b"]), int(s["c"]), int(s["d"])
+    to = (c, d, a, b) if s["mode"] == 0 else (d, c, b, a)
+    for row, frm, t in zip((a, b, c, d), (b, a, d, c), to):
+        j = int(np.nonzero(adj[row] == frm)[0][0])
+        adj[row, j] = t
+    return adj
+
+
+class Batch:
+    """Scores many 2-opt candidates of registered base graphs in one launch."""
+
+    def __init__(self, device=0):
+        self._h = _create("gg_batch_create", device)
+        self.bases = []
+
+    def add_base(self, adj):
+        adj = _i32(adj)
+        n, d = adj.shape
+        bid = ctypes.c_int()
+        _check(lib().gg_batch_add_base(self._h, n, d, _ptr(adj), ctypes.byref(bid)))
+        self.bases.append(adj)
+        return bid.value
+
+    def set_chunk(self, base_id, sources):
+        _check(lib().gg_batch_set_chunk(self._h, base_id, sources))
+
+    def eval(self, swaps):
+        swaps = np.ascontiguousarray(swaps, dtype=SWAP_DTYPE)
+        out = np.zeros(len(swaps), dtype=CAND_RESULT_DTYPE)
+        _check(lib().gg_batch_eval(self._h, len(swaps), _ptr(swaps), _ptr(out)))
+        return out
+
+    def eval_device(self, n, d_swaps, d_out, stream=0):
+        _check(lib().gg_batch_eval_device(self._h, n, ctypes.c_void_p(d_swaps), ctypes.c_void_p(d_out),
+                                          ctypes.c_void_p(stream)))
+
+    def last_ms(self):
+        ms = ctypes.c_double()
+        _check(lib().gg_batch_last_ms(self._h, ctypes.byref(ms)))
+        return ms.value
+
+    def close(self):
+        if self._h:
+            lib().gg_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -167,6 +167,54 @@ gg_status gg_destroy(gg_engine *e);
 gg_status gg_graph_eval_noalloc(const int32_t *d_adj, int N, int degree, int max_levels,
                                 uint64_t *d_level_counts, void *stream);
 
+/* ---- batched candidate evaluation (no reference counterpart) -------------
+ * Replaces the reference's propose -> diameterASPL -> accept loop, which scores
+ * one candidate per call (cppcode/annealing.cpp:397-403), with one launch that
+ * scores thousands: every candidate is a registered base graph plus one 2-opt
+ * edit (cppcode/annealing.cpp:140-197 proposes the same move).  Each candidate
+ * gets the exact all-pairs total and diameter of its own graph.
+ * Base graphs are plain regular graphs with fewer than 65536 vertices. */
+typedef struct gg_batch gg_batch;
+
+/* 2-opt edit of base graph `base`: remove edges (a,b) and (c,d); add (a,c),(b,d)
+ * when mode == 0, or (a,d),(b,c) when mode == 1.  a < 0 means "no edit" (the base
+ * itself).  In each of the four rows the first occurrence of the removed
+ * neighbour is replaced. */
+typedef struct gg_swap {
+    int32_t base;
+    int32_t a, b, c, d;
+    int32_t mode;
+} gg_swap;
+
+typedef struct gg_cand_result {
+    uint64_t total;       /* sum of distances over reached ordered pairs */
+    uint64_t reached;     /* ordered pairs reached (n*n when connected) */
+    int32_t levels;       /* eccentricity maximum = diameter when connected */
+    int32_t connected;    /* reached == n*n */
+} gg_cand_result;
+
+gg_status gg_batch_create(int device, gg_batch **out);
+/* Register a base graph: adj is n*degree int32 (simple, regular). */
+gg_status gg_batch_add_base(gg_batch *b, int n, int degree, const int32_t *adj, int *base_id);
+/* Source bits per shared-memory task for a base (multiple of 128; 0 = automatic). */
+gg_status gg_batch_set_chunk(gg_batch *b, int base_id, int sources);
+/* Host arrays in and out; blocking.  The launch for a given candidate count is
+ * captured once in a CUDA graph and replayed. */
+gg_status gg_batch_eval(gg_batch *b, int n_cand, const gg_swap *cands, gg_cand_result *out);
+/* Device arrays in and out, ordered on `stream` (NULL = the batch's stream); returns
+ * after enqueueing.  The caller synchronises before reading `d_out`. */
+gg_status gg_batch_eval_device(gg_batch *b, int n_cand, const gg_swap *d_cands,
+                               gg_cand_result *d_out, void *stream);
+/* Device milliseconds of the last evaluation's launch (CUDA events). */
+gg_status gg_batch_last_ms(gg_batch *b, double *ms);
+gg_status gg_batch_destroy(gg_batch *b);
+
+/* Uniform random 2-opt proposals on a base graph (adj n*degree, simple):
+ * edges (a,b), (c,d) drawn uniformly, mode uniform; proposals that would create a
+ * loop or a repeated edge are redrawn.  Writes `count` swaps with base = base_id. */
+gg_status gg_gen_swaps(int n, int degree, const int32_t *adj, int base_id, int count, uint64_t seed,
+                       gg_swap *out);
+
 /* ---- generators (host, deterministic, no GPU) ----------------------------
  * Random simple connected d-regular graph on n vertices: configuration-model
  * stub pairing followed by double-edge switches that remove loops and

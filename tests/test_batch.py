@@ -1,0 +1,102 @@
+"""Batched 2-opt evaluation (gg_batch_*): every candidate's exact total,
+reach and diameter equal the oracle's on the edited graph.  Host logic (the
+proposal generator, the edit) is checked on CPU; the kernel on the GPU."""
+import numpy as np
+import pytest
+
+import graphgolf as G
+import instances as I
+import oracle as O
+
+
+def exact(adj):
+    r = O.bfs_pull(adj, np.arange(len(adj)))
+    return r.total(), int(r.reached.sum()), r.levels, r.connected
+
+
+# ---- CPU: proposals -------------------------------------------------------
+
+def test_gen_swaps_are_valid_2opt_moves():
+    adj = G.random_regular(300, 4, 3)
+    sw = G.gen_swaps(adj, 0, 500, 9)
+    assert len(sw) == 500 and np.all(sw["base"] == 0)
+    edges = {(min(u, v), max(u, v)) for v in range(300) for u in adj[v]}
+    for s in sw[:200]:
+        a, b, c, d = (int(s[k]) for k in "abcd")
+        assert len({a, b, c, d}) == 4
+        assert (min(a, b), max(a, b)) in edges and (min(c, d), max(c, d)) in edges
+        new = G.apply_swap(adj, s)
+        assert np.all(np.sort(new, axis=1)[:, 1:] != np.sort(new, axis=1)[:, :-1])  # no repeats
+        assert not np.any(new == np.arange(300)[:, None])                            # no loops
+        for v in range(300):  # still symmetric
+            for u in new[v]:
+                assert v in new[u]
+    assert np.array_equal(sw, G.gen_swaps(adj, 0, 500, 9))
+
+
+# ---- GPU -------------------------------------------------------------------
+
+@pytest.mark.gpu
+def test_batch_mixed_bases_vs_oracle():
+    b = G.Batch(0)
+    g1 = G.random_regular(1024, 6, 1)
+    g2 = G.random_regular(3000, 4, 1)
+    g3 = I.random_regular_np(130, 3 if 130 * 3 % 2 == 0 else 4, 5)  # multigraph, ragged chunk
+    ids = [b.add_base(g) for g in (g1, g2, g3)]
+    sw = np.concatenate([G.gen_swaps(g1, ids[0], 24, 1), G.gen_swaps(g2, ids[1], 8, 2)])
+    none = np.zeros(3, dtype=G.SWAP_DTYPE)
+    none["base"] = ids
+    none["a"] = -1
+    sw = np.concatenate([sw, none])
+    res = b.eval(sw)
+    graphs = [g1, g2, g3]
+    for s, r in zip(sw, res):
+        want = exact(G.apply_swap(graphs[s["base"]], s))
+        assert (int(r["total"]), int(r["reached"]), int(r["levels"]), bool(r["connected"])) == want
+    # the same batch again (the captured graph is replayed) gives the same answers
+    assert np.array_equal(b.eval(sw), res)
+
+
+@pytest.mark.gpu
+def test_batch_config_2048_plus_512():
+    b = G.Batch(0)
+    g1 = G.random_regular(1024, 6, 11)
+    g2 = G.random_regular(3000, 4, 12)
+    i1, i2 = b.add_base(g1), b.add_base(g2)
+    sw = np.concatenate([G.gen_swaps(g1, i1, 2048, 21), G.gen_swaps(g2, i2, 512, 22)])
+    res = b.eval(sw)
+    assert np.all(res["connected"] == 1)
+    rng = np.random.default_rng(0)
+    for k in rng.choice(len(sw), 12, replace=False):
+        s = sw[k]
+        want = exact(G.apply_swap((g1, g2)[s["base"]], s))
+        assert (int(res[k]["total"]), int(res[k]["reached"]), int(res[k]["levels"]), True) == want
+
+
+@pytest.mark.gpu
+def test_batch_chunk_width_invariance():
+    b = G.Batch(0)
+    g = G.random_regular(1000, 6, 4)
+    i = b.add_base(g)
+    sw = G.gen_swaps(g, i, 64, 5)
+    base = b.eval(sw)
+    for w in (128, 256, 512):
+        b.set_chunk(i, w)
+        assert np.array_equal(b.eval(sw), base)
+    with pytest.raises(G.GGError):  # 2 x 1000 x 128 B of bitsets exceed the shared memory
+        b.set_chunk(i, 1024)
+
+
+@pytest.mark.gpu
+def test_batch_rejects_bad_candidates():
+    b = G.Batch(0)
+    g = G.random_regular(100, 4, 4)
+    i = b.add_base(g)
+    sw = G.gen_swaps(g, i, 2, 5)
+    sw[1]["c"] = 100
+    with pytest.raises(G.GGError):
+        b.eval(sw)
+    sw = G.gen_swaps(g, i, 2, 5)
+    sw[0]["base"] = 7
+    with pytest.raises(G.GGError):
+        b.eval(sw)

@@ -1,0 +1,144 @@
+"""Batched simulated annealing of a regular graph, with or without the surrogate.
+
+The reference's annealer proposes one move, scores it with one calculator call
+and accepts it by Metropolis (cppcode/annealing.cpp:397-443).  Here every step
+scores a batch of 2-opt proposals exactly in one launch (gg_batch_eval):
+
+  plain      `exact` uniform random proposals;
+  surrogate  `pool` uniform random proposals ranked by the surrogate network;
+             the `exact - explore` best-ranked plus `explore` random ones of the
+             rest are scored exactly.  The exact results train the network online
+             (one Adam step per annealing step), so it learns on the annealer's
+             own (swap, exact ΔASPL) pairs.
+
+Acceptance uses only exact values: the best proposal of the step (smallest
+diameter, then smallest total) replaces the current graph if it lowers the
+diameter, or keeps it and lowers the total, or else with probability
+exp(-ΔASPL / T); a larger diameter is never accepted (cppcode/annealing.cpp:407-412).
+T follows a geometric schedule from T0 = t0_frac * ASPL(start) to t_end.
+"""
+from __future__ import annotations
+
+import math
+import time
+from dataclasses import dataclass, field
+
+import numpy as np
+
+import graphgolf as G
+
+HIST_K = 4
+
+
+def features(batch, bid):
+    """Per-vertex inputs of the surrogate: the distance histogram to depth 4,
+    standardised over the graph, and a constant."""
+    h = batch.vertex_hist(bid, HIST_K).astype(np.float64)
+    h = (h - h.mean(0)) / (h.std(0) + 1e-6)
+    return np.concatenate([h, np.ones((len(h), 1))], axis=1).astype(np.float32)
+
+
+@dataclass
+class Trace:
+    times: list = field(default_factory=list)      # wall seconds at each improvement of the best
+    best: list = field(default_factory=list)       # best ASPL after each improvement
+    steps: int = 0
+    accepted: int = 0
+    exact_evals: int = 0
+    train_pairs: int = 0
+    wall: float = 0.0
+    final_best: float = math.inf
+    hit_time: float | None = None                  # wall seconds when best <= target
+    hit_step: int | None = None
+
+
+def anneal(adj0, steps, *, seed=1, exact=32, pool=4096, explore=8, surrogate=False, t0_frac=1e-3,
+           t_end=1e-6, target=None, time_limit=None, lr=2e-3, device=0):
+    """Anneal from `adj0` (n x d simple regular graph).  Returns (best_adj, Trace)."""
+    adj = np.array(adj0, dtype=np.int32, copy=True)
+    n, d = adj.shape
+    npairs = n * (n - 1)
+    b = G.Batch(device)
+    bid = b.add_base(adj)
+    me = np.array([(bid, -1, -1, -1, -1, 0)], dtype=G.SWAP_DTYPE)
+    r0 = b.eval(me)[0]
+    if not r0["connected"]:
+        raise ValueError("start graph is disconnected")
+    cur_total, cur_diam = int(r0["total"]), int(r0["levels"])
+    best_aspl, best_adj = cur_total / npairs, adj.copy()
+    T0 = t0_frac * best_aspl
+    rng = np.random.default_rng(seed)
+    net = None
+    scale = None
+    if surrogate:
+        net = G.Surrogate(n, d, HIST_K + 1, seed=seed)
+        net.set_graph(adj, features(b, bid))
+    tr = Trace()
+    t_start = time.perf_counter()
+    tr.times.append(0.0)
+    tr.best.append(best_aspl)
+    for i in range(steps):
+        T = T0 * (t_end / T0) ** (i / max(steps - 1, 1))
+        step_seed = (seed << 32) ^ i
+        if net is None:
+            props = G.gen_swaps(adj, bid, exact, step_seed)
+        else:
+            cand = G.gen_swaps(adj, bid, pool, step_seed)
+            pred = net.predict(cand)
+            order = np.argsort(pred, kind="stable")
+            top = order[:exact - explore]
+            rest = order[exact - explore:]
+            pick = np.concatenate([top, rng.choice(rest, explore, replace=False)])
+            props = cand[pick]
+        res = b.eval(props)
+        tr.exact_evals += len(props)
+        ok = res["connected"] == 1
+        totals = res["total"].astype(np.int64)
+        if net is not None:
+            delta = (totals - cur_total).astype(np.float64) / npairs
+            if scale is None and ok.any():
+                scale = max(float(np.std(delta[ok])), 1e-12)
+            tgt = (delta / scale).astype(np.float32)
+            net.train(props, tgt, lr=lr, mask=ok.astype(np.int32))
+            tr.train_pairs += int(ok.sum())
+        if ok.any():
+            key = np.where(ok, res["levels"].astype(np.int64) * (1 << 40) + totals, np.iinfo(np.int64).max)
+            k = int(np.argmin(key))
+            dy, ty = int(res["levels"][k]), int(totals[k])
+            dA = (ty - cur_total) / npairs
+            accept = dy < cur_diam or (dy == cur_diam and (dA < 0 or rng.random() < math.exp(-dA / T)))
+            if dy > cur_diam:
+                accept = False
+            if accept:
+                adj = G.apply_swap(adj, props[k])
+                b.set_base(bid, adj)
+                cur_total, cur_diam = ty, dy
+                tr.accepted += 1
+                if net is not None:
+                    net.set_graph(adj, features(b, bid))
+                aspl = cur_total / npairs
+                if aspl < best_aspl:
+                    best_aspl, best_adj = aspl, adj.copy()
+                    tr.times.append(time.perf_counter() - t_start)
+                    tr.best.append(best_aspl)
+                    if target is not None and tr.hit_time is None and best_aspl <= target:
+                        tr.hit_time, tr.hit_step = tr.times[-1], i + 1
+        tr.steps = i + 1
+        if target is not None and tr.hit_time is not None:
+            break
+        if time_limit is not None and time.perf_counter() - t_start > time_limit:
+            break
+    tr.wall = time.perf_counter() - t_start
+    tr.final_best = best_aspl
+    b.close()
+    if net is not None:
+        net.close()
+    return best_adj, tr
+
+
+def time_to(trace, target):
+    """Wall seconds at which a finished trace's best first reached `target`."""
+    for t, v in zip(trace.times, trace.best):
+        if v <= target:
+            return t
+    return None

@@ -52,6 +52,8 @@ struct BatchArgs {
     const gg_swap *cands;
     gg_cand_result *out;
     BatchCtl *ctl;
+    unsigned *hist;       // nullptr, or [n][hist_k]: per-vertex new pairs at levels 1..hist_k
+    int hist_k;           // (only meaningful for a launch of one candidate)
 };
 
 __device__ __forceinline__ uint4 z4() { return make_uint4(0u, 0u, 0u, 0u); }
@@ -139,8 +141,10 @@ __global__ void __launch_bounds__(kBatchBlock, 1) batch_kernel(const BatchArgs a
                         acc.x |= x.x; acc.y |= x.y; acc.z |= x.z; acc.w |= x.w;
                     }
                     out = make_uint4(own.x | acc.x, own.y | acc.y, own.z | acc.z, own.w | acc.w);
-                    cnt += __popc(acc.x & ~own.x) + __popc(acc.y & ~own.y) + __popc(acc.z & ~own.z) +
-                           __popc(acc.w & ~own.w);
+                    const unsigned pc = __popc(acc.x & ~own.x) + __popc(acc.y & ~own.y) +
+                                        __popc(acc.z & ~own.z) + __popc(acc.w & ~own.w);
+                    cnt += pc;
+                    if (a.hist && L <= a.hist_k && pc) atomicAdd(a.hist + (size_t)v * a.hist_k + (L - 1), pc);
                 }
                 nxt[t] = out;
             }
@@ -217,6 +221,8 @@ struct gg_batch {
     const gg_swap *graph_cands = nullptr;  // pointers baked into the graph
     gg_cand_result *graph_out = nullptr;
     cudaStream_t graph_stream = nullptr;
+    unsigned *d_hist = nullptr;            // vertex histogram output
+    size_t hist_cap = 0;
     double last_ms = 0.0;
 };
 
@@ -281,8 +287,9 @@ gg_status ensure_cap(gg_batch *b, int n) {
 
 // Enqueue reset -> batch kernel -> finalize on `st` for candidates `cands`,
 // results `out`; the candidate count and task geometry come from d_ctl.
-gg_status enqueue(gg_batch *b, const gg_swap *cands, gg_cand_result *out, cudaStream_t st) {
-    BatchArgs a{b->d_bases, cands, out, b->d_ctl};
+gg_status enqueue(gg_batch *b, const gg_swap *cands, gg_cand_result *out, cudaStream_t st,
+                  unsigned *hist = nullptr, int hist_k = 0) {
+    BatchArgs a{b->d_bases, cands, out, b->d_ctl, hist, hist_k};
     batch_reset<<<64, 256, 0, st>>>(a);
     batch_kernel<<<b->grid, kBatchBlock, b->smem, st>>>(a);
     batch_finalize<<<64, 256, 0, st>>>(a);
@@ -347,6 +354,20 @@ gg_status gg_batch_add_base(gg_batch *b, int n, int degree, const int32_t *adj, 
     b->base_adj.push_back(d);
     *base_id = (int)b->bases.size() - 1;
     return refresh_plan(b);
+}
+
+gg_status gg_batch_set_base(gg_batch *b, int base_id, const int32_t *adj) {
+    if (!b || !adj || base_id < 0 || base_id >= (int)b->bases.size())
+        return bfail(GG_BAD_ARG, "bad base or adjacency");
+    const BatchBase &B = b->bases[base_id];
+    for (long long k = 0; k < (long long)B.n * B.d; ++k)
+        if (adj[k] < 0 || adj[k] >= B.n) return bfail(GG_BAD_ARG, "adjacency entry outside [0, n)");
+    GB_CK(cudaSetDevice(b->device));
+    // ordered on the batch stream: launches already enqueued see the old table
+    GB_CK(cudaMemcpyAsync(b->base_adj[base_id], adj, (size_t)B.n * B.d * sizeof(int32_t),
+                          cudaMemcpyHostToDevice, b->stream));
+    GB_CK(cudaStreamSynchronize(b->stream));
+    return GG_OK;
 }
 
 gg_status gg_batch_set_chunk(gg_batch *b, int base_id, int sources) {
@@ -417,6 +438,40 @@ gg_status gg_batch_eval_device(gg_batch *b, int n_cand, const gg_swap *d_cands,
     return GG_OK;
 }
 
+gg_status gg_batch_vertex_hist(gg_batch *b, int base_id, int K, uint32_t *hist) {
+    if (!b || !hist || base_id < 0 || base_id >= (int)b->bases.size() || K < 1 || K > 64)
+        return bfail(GG_BAD_ARG, "bad base, K or output");
+    GB_CK(cudaSetDevice(b->device));
+    gg_status s = ensure_cap(b, 1);
+    if (s != GG_OK) return s;
+    const int n = b->bases[base_id].n;
+    const size_t need = (size_t)n * K;
+    if (need > b->hist_cap) {
+        cudaFree(b->d_hist);
+        b->d_hist = nullptr;
+        b->hist_cap = 0;
+        GB_CK(cudaMalloc(&b->d_hist, need * sizeof(unsigned)));
+        b->hist_cap = need;
+    }
+    unsigned *d_hist = b->d_hist;
+    const gg_swap self{base_id, -1, -1, -1, -1, 0};
+    b->h_cands[0] = self;
+    b->h_ctl->n_cand = 1;
+    b->h_ctl->task_ctr = 0;
+    cudaError_t e = cudaMemsetAsync(d_hist, 0, (size_t)n * K * sizeof(unsigned), b->stream);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(b->d_cands, b->h_cands, sizeof(gg_swap), cudaMemcpyHostToDevice, b->stream);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(b->d_ctl, b->h_ctl, sizeof(BatchCtl), cudaMemcpyHostToDevice, b->stream);
+    if (e == cudaSuccess) s = enqueue(b, b->d_cands, b->d_out, b->stream, d_hist, K);
+    if (e == cudaSuccess && s == GG_OK)
+        e = cudaMemcpyAsync(hist, d_hist, (size_t)n * K * sizeof(unsigned), cudaMemcpyDeviceToHost, b->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(b->stream);
+    if (s != GG_OK) return s;
+    GB_CK(e);
+    return GG_OK;
+}
+
 gg_status gg_batch_last_ms(gg_batch *b, double *ms) {
     if (!b || !ms) return bfail(GG_BAD_ARG, "null argument");
     float f = 0.f;
@@ -434,6 +489,7 @@ gg_status gg_batch_destroy(gg_batch *b) {
     for (auto p : b->base_adj) cudaFree(p);
     cudaFree(b->d_bases); cudaFree(b->d_ctl); cudaFreeHost(b->h_ctl);
     cudaFree(b->d_cands); cudaFree(b->d_out); cudaFreeHost(b->h_cands); cudaFreeHost(b->h_out);
+    cudaFree(b->d_hist);
     if (b->ev0) cudaEventDestroy(b->ev0);
     if (b->ev1) cudaEventDestroy(b->ev1);
     if (b->stream) cudaStreamDestroy(b->stream);

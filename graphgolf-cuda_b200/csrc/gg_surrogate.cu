@@ -1,0 +1,568 @@
+// gg_surrogate.cu -- the surrogate ΔASPL ranker (gg_surrogate_* in gg.h).
+//
+// All products go through one hand-written tile GEMM: 128 threads, a 64x64
+// output tile, k steps of 16; operands are read from fp32 memory through
+// arbitrary strides (so transposes cost nothing), rounded to bf16 (round to
+// nearest even) into shared memory, and multiplied with mma.sync m16n8k16
+// (bf16 in, fp32 accumulate).  Long reductions (weight gradients, K = number of
+// vertices or swaps) split K over blocks and accumulate with fp32 atomics.
+// The remaining kernels are gathers/scatters (neighbour means, the swap
+// readout), elementwise epilogues and Adam.
+#include "gg.h"
+
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstring>
+#include <string>
+#include <vector>
+
+namespace gg {
+void set_last_error(const char *msg);  // gg_engine.cu
+}
+
+namespace {
+
+constexpr int kH = 64;           // hidden width
+constexpr int kZ = 3 * kH;       // swap readout width
+constexpr int kLayers = 3;       // message-passing layers
+
+// ---------------------------------------------------------------------------
+// bf16 tile GEMM:  C(m, n) (=|+=) sum_k A(m, k) * B(k, n)
+// A(m, k) = A[m*sam + k*sak], B(k, n) = B[k*sbk + n*sbn], C(m, n) = C[m*scm + n*scn]
+// ---------------------------------------------------------------------------
+struct GemmArgs {
+    const float *A;
+    long long sam, sak;
+    const float *B;
+    long long sbk, sbn;
+    float *C;
+    long long scm, scn;
+    int M, N, K, kchunk;
+    int atomic;   // 0: C = result; 1: C += result (atomicAdd; used with split K)
+};
+
+__device__ __forceinline__ uint16_t bf16_bits(float x) {
+    __nv_bfloat16 h = __float2bfloat16_rn(x);
+    return *reinterpret_cast<uint16_t *>(&h);
+}
+
+__device__ __forceinline__ void mma_bf16(float c[4], const uint32_t a[4], const uint32_t b[2]) {
+    asm volatile(
+        "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 "
+        "{%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, {%0,%1,%2,%3};\n"
+        : "+f"(c[0]), "+f"(c[1]), "+f"(c[2]), "+f"(c[3])
+        : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b[0]), "r"(b[1]));
+}
+
+__global__ void __launch_bounds__(128) gemm_bf16_kernel(const GemmArgs g) {
+    // row stride 24 bf16 (48 B): the fragment loads of a warp hit 32 distinct banks
+    __shared__ __align__(16) uint16_t As[64][24];
+    __shared__ __align__(16) uint16_t Bt[64][24];   // B transposed: Bt[n][k]
+    const int m0 = blockIdx.x * 64, n0 = blockIdx.y * 64;
+    const int k_begin = blockIdx.z * g.kchunk;
+    const int k_end = min(g.K, k_begin + g.kchunk);
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31, gid = lane >> 2, tg = lane & 3;
+    float acc[8][4];
+#pragma unroll
+    for (int j = 0; j < 8; ++j) acc[j][0] = acc[j][1] = acc[j][2] = acc[j][3] = 0.f;
+
+    for (int k0 = k_begin; k0 < k_end; k0 += 16) {
+        for (int e = tid; e < 64 * 16; e += 128) {
+            const int r = e >> 4, k = e & 15, m = m0 + r, kk = k0 + k;
+            const float x = (m < g.M && kk < k_end) ? g.A[m * g.sam + kk * g.sak] : 0.f;
+            As[r][k] = bf16_bits(x);
+        }
+        for (int e = tid; e < 64 * 16; e += 128) {
+            const int n = e >> 4, k = e & 15, nn = n0 + n, kk = k0 + k;
+            const float x = (nn < g.N && kk < k_end) ? g.B[kk * g.sbk + nn * g.sbn] : 0.f;
+            Bt[n][k] = bf16_bits(x);
+        }
+        __syncthreads();
+        const int r = warp * 16;
+        uint32_t a[4];
+        a[0] = *reinterpret_cast<const uint32_t *>(&As[r + gid][2 * tg]);
+        a[1] = *reinterpret_cast<const uint32_t *>(&As[r + gid + 8][2 * tg]);
+        a[2] = *reinterpret_cast<const uint32_t *>(&As[r + gid][2 * tg + 8]);
+        a[3] = *reinterpret_cast<const uint32_t *>(&As[r + gid + 8][2 * tg + 8]);
+#pragma unroll
+        for (int j = 0; j < 8; ++j) {
+            uint32_t b[2];
+            b[0] = *reinterpret_cast<const uint32_t *>(&Bt[8 * j + gid][2 * tg]);
+            b[1] = *reinterpret_cast<const uint32_t *>(&Bt[8 * j + gid][2 * tg + 8]);
+            mma_bf16(acc[j], a, b);
+        }
+        __syncthreads();
+    }
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+        const int c = n0 + 8 * j + 2 * tg;
+#pragma unroll
+        for (int h = 0; h < 4; ++h) {
+            const int m = m0 + warp * 16 + gid + ((h >> 1) << 3);
+            const int n = c + (h & 1);
+            if (m < g.M && n < g.N) {
+                float *p = g.C + m * g.scm + n * g.scn;
+                if (g.atomic) atomicAdd(p, acc[j][h]);
+                else *p = acc[j][h];
+            }
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// graph and readout kernels
+// ---------------------------------------------------------------------------
+
+// out[v] (=|+=) (1/d) sum_i H[adj[v][i]]   (rows of kH floats)
+__global__ void nbr_mean_kernel(const float *H, const int32_t *adj, int n, int d, float *out, int add) {
+    const float inv = 1.f / (float)d;
+    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < (long long)n * kH;
+         t += (long long)gridDim.x * blockDim.x) {
+        const int v = (int)(t / kH), j = (int)(t % kH);
+        float s = 0.f;
+        for (int i = 0; i < d; ++i) s += H[(size_t)adj[(size_t)v * d + i] * kH + j];
+        out[t] = add ? out[t] + s * inv : s * inv;
+    }
+}
+
+// Y = relu(Y + b)
+__global__ void bias_relu_kernel(float *Y, const float *b, long long rows, int width) {
+    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < rows * width;
+         t += (long long)gridDim.x * blockDim.x) {
+        const float y = Y[t] + b[t % width];
+        Y[t] = y > 0.f ? y : 0.f;
+    }
+}
+
+__device__ __forceinline__ void partners(const gg_swap &s, int &p, int &q) {
+    p = s.mode ? s.d : s.c;  // new edges (a,p), (b,q)
+    q = s.mode ? s.c : s.d;
+}
+
+// Z[p] = [Ha+Hb+Hc+Hd, Ha*Hb + Hc*Hd, Ha*Hp + Hb*Hq]
+__global__ void readout_z_kernel(const float *H, const gg_swap *sw, int P, float *Z) {
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < P * kH; t += gridDim.x * blockDim.x) {
+        const int p = t / kH, j = t % kH;
+        const gg_swap s = sw[p];
+        int pa, qb;
+        partners(s, pa, qb);
+        const float ha = H[(size_t)s.a * kH + j], hb = H[(size_t)s.b * kH + j];
+        const float hc = H[(size_t)s.c * kH + j], hd = H[(size_t)s.d * kH + j];
+        const float hp = H[(size_t)pa * kH + j], hq = H[(size_t)qb * kH + j];
+        float *z = Z + (size_t)p * kZ;
+        z[j] = ha + hb + hc + hd;
+        z[kH + j] = ha * hb + hc * hd;
+        z[2 * kH + j] = ha * hp + hb * hq;
+    }
+}
+
+// y[p] = O[p] . w + b0   (one warp per swap)
+__global__ void readout_out_kernel(const float *O, const float *w, const float *b0, int P, float *y) {
+    const int lane = threadIdx.x & 31;
+    for (int p = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; p < P; p += (gridDim.x * blockDim.x) >> 5) {
+        float s = O[(size_t)p * kH + lane] * w[lane] + O[(size_t)p * kH + 32 + lane] * w[32 + lane];
+        for (int o = 16; o; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+        if (lane == 0) y[p] = s + b0[0];
+    }
+}
+
+// dy = mask * 2 (y - t) / cnt ; loss += mask * (y - t)^2 / cnt
+__global__ void mse_kernel(const float *y, const float *t, const int32_t *mask, int P, float inv_cnt,
+                           float *dy, float *loss) {
+    for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < P; p += gridDim.x * blockDim.x) {
+        const float m = mask ? (mask[p] ? 1.f : 0.f) : 1.f;
+        const float e = (y[p] - t[p]) * m;
+        dy[p] = 2.f * e * inv_cnt;
+        atomicAdd(loss, e * e * inv_cnt);
+    }
+}
+
+// dO[p][j] = dy[p] * w[j] * (O[p][j] > 0);  dw[j] += dy[p] O[p][j];  db0 += dy[p]
+__global__ void readout_out_back_kernel(const float *O, const float *w, const float *dy, int P, float *dO,
+                                        float *dw, float *db0) {
+    const int j = threadIdx.x;  // blockDim.x == kH
+    float gw = 0.f, gb = 0.f;
+    for (int p = blockIdx.x; p < P; p += gridDim.x) {
+        const float o = O[(size_t)p * kH + j];
+        dO[(size_t)p * kH + j] = o > 0.f ? dy[p] * w[j] : 0.f;
+        gw += dy[p] * o;
+        if (j == 0) gb += dy[p];
+    }
+    atomicAdd(dw + j, gw);
+    if (j == 0) atomicAdd(db0, gb);
+}
+
+// db[j] += sum_rows D[r][j]
+__global__ void colsum_kernel(const float *D, long long rows, float *db) {
+    const int j = threadIdx.x;  // blockDim.x == kH
+    float s = 0.f;
+    for (long long r = blockIdx.x; r < rows; r += gridDim.x) s += D[r * kH + j];
+    atomicAdd(db + j, s);
+}
+
+// D = D * (Y > 0)
+__global__ void relu_back_kernel(float *D, const float *Y, long long count) {
+    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < count;
+         t += (long long)gridDim.x * blockDim.x)
+        if (!(Y[t] > 0.f)) D[t] = 0.f;
+}
+
+// dH[a],dH[b],dH[c],dH[d] += d(Z[p]) / d(H rows)
+__global__ void readout_scatter_kernel(const float *H, const gg_swap *sw, const float *dZ, int P, float *dH) {
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < P * kH; t += gridDim.x * blockDim.x) {
+        const int p = t / kH, j = t % kH;
+        const gg_swap s = sw[p];
+        int pa, qb;
+        partners(s, pa, qb);
+        const float g0 = dZ[(size_t)p * kZ + j], g1 = dZ[(size_t)p * kZ + kH + j],
+                    g2 = dZ[(size_t)p * kZ + 2 * kH + j];
+        const float ha = H[(size_t)s.a * kH + j], hb = H[(size_t)s.b * kH + j];
+        const float hc = H[(size_t)s.c * kH + j], hd = H[(size_t)s.d * kH + j];
+        const float hp = H[(size_t)pa * kH + j], hq = H[(size_t)qb * kH + j];
+        atomicAdd(dH + (size_t)s.a * kH + j, g0 + g1 * hb + g2 * hp);
+        atomicAdd(dH + (size_t)s.b * kH + j, g0 + g1 * ha + g2 * hq);
+        atomicAdd(dH + (size_t)s.c * kH + j, g0 + g1 * hd);
+        atomicAdd(dH + (size_t)s.d * kH + j, g0 + g1 * hc);
+        atomicAdd(dH + (size_t)pa * kH + j, g2 * ha);
+        atomicAdd(dH + (size_t)qb * kH + j, g2 * hb);
+    }
+}
+
+__global__ void adam_kernel(float *p, const float *g, float *m, float *v, int count, float lr, float b1,
+                            float b2, float c1, float c2, float eps) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x) {
+        const float gi = g[i];
+        const float mi = b1 * m[i] + (1.f - b1) * gi;
+        const float vi = b2 * v[i] + (1.f - b2) * gi * gi;
+        m[i] = mi;
+        v[i] = vi;
+        p[i] -= lr * (mi / c1) / (sqrtf(vi / c2) + eps);
+    }
+}
+
+int blocks_for(long long n, int per = 256) { return (int)std::min<long long>((n + per - 1) / per, 4096); }
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// host object
+// ---------------------------------------------------------------------------
+struct gg_surrogate {
+    int device = 0, n = 0, d = 0, F = 0;
+    cudaStream_t st = nullptr;
+    // parameter layout offsets (floats)
+    int o_win = 0, o_bin = 0, o_ws[kLayers], o_wn[kLayers], o_b[kLayers], o_wr1 = 0, o_br1 = 0,
+        o_wr2 = 0, o_br2 = 0, n_params = 0;
+    float *params = nullptr, *grad = nullptr, *adam_m = nullptr, *adam_v = nullptr;
+    int32_t *adj = nullptr;
+    float *X = nullptr;
+    float *Hs[kLayers + 1] = {};
+    float *Ms[kLayers] = {};
+    float *dH0 = nullptr, *dH1 = nullptr, *G = nullptr;
+    int cap = 0;  // swap capacity
+    gg_swap *sw = nullptr;
+    float *Z = nullptr, *O = nullptr, *y = nullptr, *t = nullptr, *dy = nullptr, *dO = nullptr, *dZ = nullptr;
+    int32_t *mask = nullptr;
+    float *loss = nullptr;
+    bool fwd_valid = false, graph_set = false;
+    long long adam_step = 0;
+};
+
+namespace {
+
+gg_status sfail(gg_status s, const std::string &m) {
+    (void)cudaGetLastError();
+    gg::set_last_error(m.c_str());
+    return s;
+}
+
+#define GS_CK(call)                                                                          \
+    do {                                                                                     \
+        cudaError_t e_ = (call);                                                             \
+        if (e_ != cudaSuccess)                                                               \
+            return sfail(e_ == cudaErrorMemoryAllocation ? GG_OUT_OF_MEMORY : GG_CUDA_ERROR, \
+                         std::string(#call) + ": " + cudaGetErrorString(e_));                \
+    } while (0)
+
+void gemm(cudaStream_t st, int M, int N, int K, const float *A, long long sam, long long sak, const float *B,
+          long long sbk, long long sbn, float *C, long long scm, long long scn, bool atomic, int splitk = 1) {
+    GemmArgs g{A, sam, sak, B, sbk, sbn, C, scm, scn, M, N, K, 0, atomic ? 1 : 0};
+    int kc = (K + splitk - 1) / splitk;
+    kc = std::max(16, (kc + 15) / 16 * 16);
+    g.kchunk = kc;
+    dim3 grid((M + 63) / 64, (N + 63) / 64, (K + kc - 1) / kc);
+    if (grid.z > 1) g.atomic = 1;
+    gemm_bf16_kernel<<<grid, 128, 0, st>>>(g);
+}
+
+int split_for(long long K) { return (int)std::max<long long>(1, std::min<long long>(K / 256, 64)); }
+
+gg_status ensure_swaps(gg_surrogate *s, int P) {
+    if (P <= s->cap) return GG_OK;
+    const int cap = std::max(P, 2 * s->cap);
+    cudaFree(s->sw); cudaFree(s->Z); cudaFree(s->O); cudaFree(s->y); cudaFree(s->t);
+    cudaFree(s->dy); cudaFree(s->dO); cudaFree(s->dZ); cudaFree(s->mask);
+    s->cap = 0;
+    GS_CK(cudaMalloc(&s->sw, (size_t)cap * sizeof(gg_swap)));
+    GS_CK(cudaMalloc(&s->Z, (size_t)cap * kZ * 4));
+    GS_CK(cudaMalloc(&s->O, (size_t)cap * kH * 4));
+    GS_CK(cudaMalloc(&s->y, (size_t)cap * 4));
+    GS_CK(cudaMalloc(&s->t, (size_t)cap * 4));
+    GS_CK(cudaMalloc(&s->dy, (size_t)cap * 4));
+    GS_CK(cudaMalloc(&s->dO, (size_t)cap * kH * 4));
+    GS_CK(cudaMalloc(&s->dZ, (size_t)cap * kZ * 4));
+    GS_CK(cudaMalloc(&s->mask, (size_t)cap * 4));
+    s->cap = cap;
+    return GG_OK;
+}
+
+// Embeddings of the current graph: H0 .. H3 (and the neighbour means M0 .. M2).
+void forward_graph(gg_surrogate *s) {
+    const int n = s->n;
+    float *P = s->params;
+    gemm(s->st, n, kH, s->F, s->X, s->F, 1, P + s->o_win, kH, 1, s->Hs[0], kH, 1, false);
+    bias_relu_kernel<<<blocks_for((long long)n * kH), 256, 0, s->st>>>(s->Hs[0], P + s->o_bin, n, kH);
+    for (int l = 0; l < kLayers; ++l) {
+        nbr_mean_kernel<<<blocks_for((long long)n * kH), 256, 0, s->st>>>(s->Hs[l], s->adj, n, s->d, s->Ms[l], 0);
+        gemm(s->st, n, kH, kH, s->Hs[l], kH, 1, P + s->o_ws[l], kH, 1, s->Hs[l + 1], kH, 1, false);
+        gemm(s->st, n, kH, kH, s->Ms[l], kH, 1, P + s->o_wn[l], kH, 1, s->Hs[l + 1], kH, 1, true);
+        bias_relu_kernel<<<blocks_for((long long)n * kH), 256, 0, s->st>>>(s->Hs[l + 1], P + s->o_b[l], n, kH);
+    }
+    s->fwd_valid = true;
+}
+
+// Readout of the P swaps already in s->sw: Z, O, y.
+void forward_readout(gg_surrogate *s, int P) {
+    float *Pm = s->params;
+    readout_z_kernel<<<blocks_for((long long)P * kH), 256, 0, s->st>>>(s->Hs[kLayers], s->sw, P, s->Z);
+    gemm(s->st, P, kH, kZ, s->Z, kZ, 1, Pm + s->o_wr1, kH, 1, s->O, kH, 1, false);
+    bias_relu_kernel<<<blocks_for((long long)P * kH), 256, 0, s->st>>>(s->O, Pm + s->o_br1, P, kH);
+    readout_out_kernel<<<blocks_for((long long)P * 32), 256, 0, s->st>>>(s->O, Pm + s->o_wr2, Pm + s->o_br2, P, s->y);
+}
+
+// Loss and full gradient into s->grad (zeroed here) for the swaps/targets on the device.
+void backward(gg_surrogate *s, int P, float inv_cnt, bool use_mask) {
+    const int n = s->n;
+    float *Pm = s->params, *Gd = s->grad;
+    cudaMemsetAsync(Gd, 0, (size_t)s->n_params * 4, s->st);
+    cudaMemsetAsync(s->loss, 0, 4, s->st);
+    mse_kernel<<<blocks_for(P), 256, 0, s->st>>>(s->y, s->t, use_mask ? s->mask : nullptr, P, inv_cnt, s->dy, s->loss);
+    readout_out_back_kernel<<<std::min(P, 256), kH, 0, s->st>>>(s->O, Pm + s->o_wr2, s->dy, P, s->dO,
+                                                                Gd + s->o_wr2, Gd + s->o_br2);
+    colsum_kernel<<<std::min(P, 256), kH, 0, s->st>>>(s->dO, P, Gd + s->o_br1);
+    // dWr1 = Z^T dO ; dZ = dO Wr1^T
+    gemm(s->st, kZ, kH, P, s->Z, 1, kZ, s->dO, kH, 1, Gd + s->o_wr1, kH, 1, true, split_for(P));
+    gemm(s->st, P, kZ, kH, s->dO, kH, 1, Pm + s->o_wr1, 1, kH, s->dZ, kZ, 1, false);
+    cudaMemsetAsync(s->dH0, 0, (size_t)n * kH * 4, s->st);
+    readout_scatter_kernel<<<blocks_for((long long)P * kH), 256, 0, s->st>>>(s->Hs[kLayers], s->sw, s->dZ, P, s->dH0);
+    float *dH = s->dH0, *dHp = s->dH1;
+    for (int l = kLayers - 1; l >= 0; --l) {
+        // dH holds dL/dH_{l+1}; make it dL/dpre_{l+1}
+        relu_back_kernel<<<blocks_for((long long)n * kH), 256, 0, s->st>>>(dH, s->Hs[l + 1], (long long)n * kH);
+        colsum_kernel<<<std::min(n, 256), kH, 0, s->st>>>(dH, n, Gd + s->o_b[l]);
+        gemm(s->st, kH, kH, n, s->Hs[l], 1, kH, dH, kH, 1, Gd + s->o_ws[l], kH, 1, true, split_for(n));
+        gemm(s->st, kH, kH, n, s->Ms[l], 1, kH, dH, kH, 1, Gd + s->o_wn[l], kH, 1, true, split_for(n));
+        // dH_l = dPre Ws^T + mean_nbr(dPre Wn^T)   (symmetric adjacency)
+        gemm(s->st, n, kH, kH, dH, kH, 1, Pm + s->o_ws[l], 1, kH, dHp, kH, 1, false);
+        gemm(s->st, n, kH, kH, dH, kH, 1, Pm + s->o_wn[l], 1, kH, s->G, kH, 1, false);
+        nbr_mean_kernel<<<blocks_for((long long)n * kH), 256, 0, s->st>>>(s->G, s->adj, n, s->d, dHp, 1);
+        float *tmp = dH; dH = dHp; dHp = tmp;
+    }
+    relu_back_kernel<<<blocks_for((long long)n * kH), 256, 0, s->st>>>(dH, s->Hs[0], (long long)n * kH);
+    colsum_kernel<<<std::min(n, 256), kH, 0, s->st>>>(dH, n, Gd + s->o_bin);
+    gemm(s->st, s->F, kH, n, s->X, 1, s->F, dH, kH, 1, Gd + s->o_win, kH, 1, true, split_for(n));
+}
+
+gg_status load_swaps(gg_surrogate *s, int P, const gg_swap *swaps) {
+    for (int i = 0; i < P; ++i) {
+        const gg_swap &w = swaps[i];
+        if (w.a < 0 || w.a >= s->n || w.b < 0 || w.b >= s->n || w.c < 0 || w.c >= s->n || w.d < 0 ||
+            w.d >= s->n || (w.mode != 0 && w.mode != 1))
+            return sfail(GG_BAD_ARG, "swap " + std::to_string(i) + " out of range");
+    }
+    gg_status r = ensure_swaps(s, P);
+    if (r != GG_OK) return r;
+    GS_CK(cudaMemcpyAsync(s->sw, swaps, (size_t)P * sizeof(gg_swap), cudaMemcpyHostToDevice, s->st));
+    return GG_OK;
+}
+
+gg_status grad_common(gg_surrogate *s, int P, const gg_swap *swaps, const float *target,
+                      const int32_t *mask, float *loss) {
+    if (!s || P < 1 || !swaps || !target) return sfail(GG_BAD_ARG, "bad arguments");
+    if (!s->graph_set) return sfail(GG_BAD_ARG, "no graph set");
+    GS_CK(cudaSetDevice(s->device));
+    gg_status r = load_swaps(s, P, swaps);
+    if (r != GG_OK) return r;
+    int cnt = P;
+    if (mask) {
+        cnt = 0;
+        for (int i = 0; i < P; ++i) cnt += mask[i] != 0;
+        GS_CK(cudaMemcpyAsync(s->mask, mask, (size_t)P * 4, cudaMemcpyHostToDevice, s->st));
+    }
+    GS_CK(cudaMemcpyAsync(s->t, target, (size_t)P * 4, cudaMemcpyHostToDevice, s->st));
+    if (!s->fwd_valid) forward_graph(s);
+    forward_readout(s, P);
+    backward(s, P, cnt ? 1.f / (float)cnt : 0.f, mask != nullptr);
+    GS_CK(cudaGetLastError());
+    float h = 0.f;
+    GS_CK(cudaMemcpyAsync(&h, s->loss, 4, cudaMemcpyDeviceToHost, s->st));
+    GS_CK(cudaStreamSynchronize(s->st));
+    if (loss) *loss = h;
+    return GG_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+gg_status gg_surrogate_create(int device, int n, int degree, int in_features, uint64_t seed,
+                              gg_surrogate **out) {
+    if (!out || n < 2 || degree < 1 || in_features < 1 || in_features > 256)
+        return sfail(GG_BAD_ARG, "need n >= 2, degree >= 1, 1 <= in_features <= 256");
+    *out = nullptr;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return sfail(GG_NO_DEVICE, "no CUDA device");
+    if (device < 0 || device >= ndev) return sfail(GG_NO_DEVICE, "device index out of range");
+    gg_surrogate *s = new gg_surrogate();
+    s->device = device; s->n = n; s->d = degree; s->F = in_features;
+    int o = 0;
+    s->o_win = o; o += in_features * kH;
+    s->o_bin = o; o += kH;
+    for (int l = 0; l < kLayers; ++l) {
+        s->o_ws[l] = o; o += kH * kH;
+        s->o_wn[l] = o; o += kH * kH;
+        s->o_b[l] = o; o += kH;
+    }
+    s->o_wr1 = o; o += kZ * kH;
+    s->o_br1 = o; o += kH;
+    s->o_wr2 = o; o += kH;
+    s->o_br2 = o; o += 1;
+    s->n_params = o;
+    // Glorot-uniform weights, zero biases, from a seeded host generator
+    std::vector<float> p(o, 0.f);
+    uint64_t x = seed * 0x9e3779b97f4a7c15ull + 1;
+    auto unif = [&]() {
+        x ^= x << 13; x ^= x >> 7; x ^= x << 17;  // xorshift64
+        return (double)(x >> 11) * (1.0 / 9007199254740992.0);
+    };
+    auto fill = [&](int off, int fin, int fout) {
+        const double a = std::sqrt(6.0 / (fin + fout));
+        for (int i = 0; i < fin * fout; ++i) p[off + i] = (float)((2 * unif() - 1) * a);
+    };
+    fill(s->o_win, in_features, kH);
+    for (int l = 0; l < kLayers; ++l) { fill(s->o_ws[l], kH, kH); fill(s->o_wn[l], kH, kH); }
+    fill(s->o_wr1, kZ, kH);
+    fill(s->o_wr2, kH, 1);
+    auto bad = [&](gg_status st) { gg_surrogate_destroy(s); return st; };
+    if (cudaSetDevice(device) != cudaSuccess || cudaStreamCreateWithFlags(&s->st, cudaStreamNonBlocking) != cudaSuccess)
+        return bad(sfail(GG_CUDA_ERROR, "stream creation failed"));
+    const size_t pb = (size_t)o * 4;
+    bool ok = cudaMalloc(&s->params, pb) == cudaSuccess && cudaMalloc(&s->grad, pb) == cudaSuccess &&
+              cudaMalloc(&s->adam_m, pb) == cudaSuccess && cudaMalloc(&s->adam_v, pb) == cudaSuccess &&
+              cudaMalloc(&s->adj, (size_t)n * degree * 4) == cudaSuccess &&
+              cudaMalloc(&s->X, (size_t)n * in_features * 4) == cudaSuccess &&
+              cudaMalloc(&s->dH0, (size_t)n * kH * 4) == cudaSuccess &&
+              cudaMalloc(&s->dH1, (size_t)n * kH * 4) == cudaSuccess &&
+              cudaMalloc(&s->G, (size_t)n * kH * 4) == cudaSuccess &&
+              cudaMalloc(&s->loss, 4) == cudaSuccess;
+    for (int l = 0; l <= kLayers && ok; ++l) ok = cudaMalloc(&s->Hs[l], (size_t)n * kH * 4) == cudaSuccess;
+    for (int l = 0; l < kLayers && ok; ++l) ok = cudaMalloc(&s->Ms[l], (size_t)n * kH * 4) == cudaSuccess;
+    if (!ok) return bad(sfail(GG_OUT_OF_MEMORY, "surrogate allocation failed"));
+    if (cudaMemcpy(s->params, p.data(), pb, cudaMemcpyHostToDevice) != cudaSuccess ||
+        cudaMemset(s->adam_m, 0, pb) != cudaSuccess || cudaMemset(s->adam_v, 0, pb) != cudaSuccess)
+        return bad(sfail(GG_CUDA_ERROR, "surrogate initialisation failed"));
+    *out = s;
+    return GG_OK;
+}
+
+gg_status gg_surrogate_set_graph(gg_surrogate *s, const int32_t *adj, const float *features) {
+    if (!s || !adj || !features) return sfail(GG_BAD_ARG, "null argument");
+    for (long long k = 0; k < (long long)s->n * s->d; ++k)
+        if (adj[k] < 0 || adj[k] >= s->n) return sfail(GG_BAD_ARG, "adjacency entry outside [0, n)");
+    GS_CK(cudaSetDevice(s->device));
+    GS_CK(cudaMemcpyAsync(s->adj, adj, (size_t)s->n * s->d * 4, cudaMemcpyHostToDevice, s->st));
+    GS_CK(cudaMemcpyAsync(s->X, features, (size_t)s->n * s->F * 4, cudaMemcpyHostToDevice, s->st));
+    s->graph_set = true;
+    s->fwd_valid = false;
+    GS_CK(cudaStreamSynchronize(s->st));
+    return GG_OK;
+}
+
+gg_status gg_surrogate_predict(gg_surrogate *s, int P, const gg_swap *swaps, float *pred) {
+    if (!s || P < 0 || (P && (!swaps || !pred))) return sfail(GG_BAD_ARG, "bad arguments");
+    if (!s->graph_set) return sfail(GG_BAD_ARG, "no graph set");
+    if (P == 0) return GG_OK;
+    GS_CK(cudaSetDevice(s->device));
+    gg_status r = load_swaps(s, P, swaps);
+    if (r != GG_OK) return r;
+    if (!s->fwd_valid) forward_graph(s);
+    forward_readout(s, P);
+    GS_CK(cudaGetLastError());
+    GS_CK(cudaMemcpyAsync(pred, s->y, (size_t)P * 4, cudaMemcpyDeviceToHost, s->st));
+    GS_CK(cudaStreamSynchronize(s->st));
+    return GG_OK;
+}
+
+gg_status gg_surrogate_grad(gg_surrogate *s, int P, const gg_swap *swaps, const float *target,
+                            const int32_t *mask, float *grad, float *loss) {
+    if (!grad) return sfail(GG_BAD_ARG, "null grad");
+    gg_status r = grad_common(s, P, swaps, target, mask, loss);
+    if (r != GG_OK) return r;
+    GS_CK(cudaMemcpy(grad, s->grad, (size_t)s->n_params * 4, cudaMemcpyDeviceToHost));
+    return GG_OK;
+}
+
+gg_status gg_surrogate_train(gg_surrogate *s, int P, const gg_swap *swaps, const float *target,
+                             const int32_t *mask, float lr, float *loss) {
+    gg_status r = grad_common(s, P, swaps, target, mask, loss);
+    if (r != GG_OK) return r;
+    const float b1 = 0.9f, b2 = 0.999f, eps = 1e-8f;
+    s->adam_step += 1;
+    const float c1 = 1.f - std::pow(b1, (float)s->adam_step), c2 = 1.f - std::pow(b2, (float)s->adam_step);
+    adam_kernel<<<blocks_for(s->n_params), 256, 0, s->st>>>(s->params, s->grad, s->adam_m, s->adam_v,
+                                                           s->n_params, lr, b1, b2, c1, c2, eps);
+    GS_CK(cudaGetLastError());
+    s->fwd_valid = false;
+    GS_CK(cudaStreamSynchronize(s->st));
+    return GG_OK;
+}
+
+gg_status gg_surrogate_param_count(gg_surrogate *s, int *count) {
+    if (!s || !count) return sfail(GG_BAD_ARG, "null argument");
+    *count = s->n_params;
+    return GG_OK;
+}
+
+gg_status gg_surrogate_get_params(gg_surrogate *s, float *params) {
+    if (!s || !params) return sfail(GG_BAD_ARG, "null argument");
+    GS_CK(cudaSetDevice(s->device));
+    GS_CK(cudaMemcpy(params, s->params, (size_t)s->n_params * 4, cudaMemcpyDeviceToHost));
+    return GG_OK;
+}
+
+gg_status gg_surrogate_set_params(gg_surrogate *s, const float *params) {
+    if (!s || !params) return sfail(GG_BAD_ARG, "null argument");
+    GS_CK(cudaSetDevice(s->device));
+    GS_CK(cudaMemcpy(s->params, params, (size_t)s->n_params * 4, cudaMemcpyHostToDevice));
+    s->fwd_valid = false;
+    return GG_OK;
+}
+
+gg_status gg_surrogate_destroy(gg_surrogate *s) {
+    if (!s) return GG_OK;
+    cudaSetDevice(s->device);
+    if (s->st) cudaStreamSynchronize(s->st);
+    cudaFree(s->params); cudaFree(s->grad); cudaFree(s->adam_m); cudaFree(s->adam_v);
+    cudaFree(s->adj); cudaFree(s->X); cudaFree(s->dH0); cudaFree(s->dH1); cudaFree(s->G); cudaFree(s->loss);
+    for (auto p : s->Hs) cudaFree(p);
+    for (auto p : s->Ms) cudaFree(p);
+    cudaFree(s->sw); cudaFree(s->Z); cudaFree(s->O); cudaFree(s->y); cudaFree(s->t);
+    cudaFree(s->dy); cudaFree(s->dO); cudaFree(s->dZ); cudaFree(s->mask);
+    if (s->st) cudaStreamDestroy(s->st);
+    delete s;
+    return GG_OK;
+}
+
+}  // extern "C"

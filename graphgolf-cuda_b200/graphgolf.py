@@ -99,11 +99,22 @@ _SIGS = {
     "gg_batch_create": [_I, _EPP],
     "gg_batch_add_base": [_P, _I, _I, _P, _IP],
     "gg_batch_set_chunk": [_P, _I, _I],
+    "gg_batch_set_base": [_P, _I, _P],
+    "gg_batch_vertex_hist": [_P, _I, _I, _P],
     "gg_batch_eval": [_P, _I, _P, _P],
     "gg_batch_eval_device": [_P, _I, _P, _P, _P],
     "gg_batch_last_ms": [_P, _DP],
     "gg_batch_destroy": [_P],
     "gg_gen_swaps": [_I, _I, _P, _I, _I, ctypes.c_uint64, _P],
+    "gg_surrogate_create": [_I, _I, _I, _I, ctypes.c_uint64, _EPP],
+    "gg_surrogate_set_graph": [_P, _P, _P],
+    "gg_surrogate_predict": [_P, _I, _P, _P],
+    "gg_surrogate_train": [_P, _I, _P, _P, _P, ctypes.c_float, ctypes.POINTER(ctypes.c_float)],
+    "gg_surrogate_param_count": [_P, _IP],
+    "gg_surrogate_get_params": [_P, _P],
+    "gg_surrogate_set_params": [_P, _P],
+    "gg_surrogate_grad": [_P, _I, _P, _P, _P, _P, ctypes.POINTER(ctypes.c_float)],
+    "gg_surrogate_destroy": [_P],
     "gg_gen_random_regular": [_I, _I, ctypes.c_uint64, _P],
     "gg_gen_cyclic_lift": [_I, _I, _I, ctypes.c_uint64, _P],
 }
@@ -589,6 +600,72 @@ def apply_swap(adj, s):
     return adj
 
 
+class Surrogate:
+    """ΔASPL ranker (gg_surrogate_*): message passing over the current graph,
+    bf16 products with fp32 accumulation, Adam on fp32 master weights."""
+
+    def __init__(self, n, degree, in_features, seed=0, device=0):
+        self._h = _create("gg_surrogate_create", device, n, degree, in_features, seed)
+        self.n, self.degree, self.in_features = n, degree, in_features
+
+    def set_graph(self, adj, features):
+        adj = _i32(adj)
+        f = np.ascontiguousarray(features, dtype=np.float32)
+        _check(lib().gg_surrogate_set_graph(self._h, _ptr(adj), _ptr(f)))
+
+    def predict(self, swaps):
+        swaps = np.ascontiguousarray(swaps, dtype=SWAP_DTYPE)
+        out = np.zeros(len(swaps), dtype=np.float32)
+        _check(lib().gg_surrogate_predict(self._h, len(swaps), _ptr(swaps), _ptr(out)))
+        return out
+
+    def _common(self, swaps, target, mask):
+        swaps = np.ascontiguousarray(swaps, dtype=SWAP_DTYPE)
+        t = np.ascontiguousarray(target, dtype=np.float32)
+        m = None if mask is None else np.ascontiguousarray(mask, dtype=np.int32)
+        return swaps, t, m
+
+    def train(self, swaps, target, lr=1e-3, mask=None):
+        swaps, t, m = self._common(swaps, target, mask)
+        loss = ctypes.c_float()
+        _check(lib().gg_surrogate_train(self._h, len(swaps), _ptr(swaps), _ptr(t),
+                                        None if m is None else _ptr(m), lr, ctypes.byref(loss)))
+        return loss.value
+
+    def grad(self, swaps, target, mask=None):
+        swaps, t, m = self._common(swaps, target, mask)
+        g = np.zeros(self.param_count(), dtype=np.float32)
+        loss = ctypes.c_float()
+        _check(lib().gg_surrogate_grad(self._h, len(swaps), _ptr(swaps), _ptr(t),
+                                       None if m is None else _ptr(m), _ptr(g), ctypes.byref(loss)))
+        return g, loss.value
+
+    def param_count(self):
+        c = ctypes.c_int()
+        _check(lib().gg_surrogate_param_count(self._h, ctypes.byref(c)))
+        return c.value
+
+    def get_params(self):
+        p = np.zeros(self.param_count(), dtype=np.float32)
+        _check(lib().gg_surrogate_get_params(self._h, _ptr(p)))
+        return p
+
+    def set_params(self, p):
+        p = np.ascontiguousarray(p, dtype=np.float32)
+        _check(lib().gg_surrogate_set_params(self._h, _ptr(p)))
+
+    def close(self):
+        if self._h:
+            lib().gg_surrogate_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
 class Batch:
     """Scores many 2-opt candidates of registered base graphs in one launch."""
 
@@ -606,6 +683,18 @@ class Batch:
 
     def set_chunk(self, base_id, sources):
         _check(lib().gg_batch_set_chunk(self._h, base_id, sources))
+
+    def set_base(self, base_id, adj):
+        adj = _i32(adj)
+        _check(lib().gg_batch_set_base(self._h, base_id, _ptr(adj)))
+        self.bases[base_id] = adj
+
+    def vertex_hist(self, base_id, K):
+        """[n, K] uint32: vertices at distance 1..K from each vertex of the base."""
+        n = len(self.bases[base_id])
+        out = np.zeros((n, K), dtype=np.uint32)
+        _check(lib().gg_batch_vertex_hist(self._h, base_id, K, _ptr(out)))
+        return out
 
     def eval(self, swaps):
         swaps = np.ascontiguousarray(swaps, dtype=SWAP_DTYPE)

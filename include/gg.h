@@ -196,6 +196,9 @@ typedef struct gg_cand_result {
 gg_status gg_batch_create(int device, gg_batch **out);
 /* Register a base graph: adj is n*degree int32 (simple, regular). */
 gg_status gg_batch_add_base(gg_batch *b, int n, int degree, const int32_t *adj, int *base_id);
+/* Replace a registered base graph's adjacency (same n and degree), e.g. after an
+ * annealer accepted a move. */
+gg_status gg_batch_set_base(gg_batch *b, int base_id, const int32_t *adj);
 /* Source bits per shared-memory task for a base (multiple of 128; 0 = automatic). */
 gg_status gg_batch_set_chunk(gg_batch *b, int base_id, int sources);
 /* Host arrays in and out; blocking.  The launch for a given candidate count is
@@ -205,6 +208,10 @@ gg_status gg_batch_eval(gg_batch *b, int n_cand, const gg_swap *cands, gg_cand_r
  * after enqueueing.  The caller synchronises before reading `d_out`. */
 gg_status gg_batch_eval_device(gg_batch *b, int n_cand, const gg_swap *d_cands,
                                gg_cand_result *d_out, void *stream);
+/* Per-vertex distance histogram of a base graph: hist[v*K + k] = number of
+ * vertices at distance k+1 from v, k < K (the per-row popcounts of BFS levels
+ * 1..K).  hist: host array n*K. */
+gg_status gg_batch_vertex_hist(gg_batch *b, int base_id, int K, uint32_t *hist);
 /* Device milliseconds of the last evaluation's launch (CUDA events). */
 gg_status gg_batch_last_ms(gg_batch *b, double *ms);
 gg_status gg_batch_destroy(gg_batch *b);
@@ -214,6 +221,41 @@ gg_status gg_batch_destroy(gg_batch *b);
  * loop or a repeated edge are redrawn.  Writes `count` swaps with base = base_id. */
 gg_status gg_gen_swaps(int n, int degree, const int32_t *adj, int base_id, int count, uint64_t seed,
                        gg_swap *out);
+
+/* ---- surrogate ΔASPL ranker (no reference counterpart) -------------------
+ * A message-passing network over the current graph that predicts, for a 2-opt
+ * swap, the change of the all-pairs total it would cause; trained online on
+ * exact results.  It only ranks proposals: exact BFS decides everything else.
+ *   x_v          per-vertex input features (in_features floats; e.g. the distance
+ *                histogram of gg_batch_vertex_hist, standardised)
+ *   H0 = relu(X W_in + b_in)                                    (in -> 64)
+ *   H_l = relu(H_{l-1} Ws_l + mean_{u~v} H_{l-1}[u] Wn_l + b_l)  l = 1..3 (64 -> 64)
+ *   swap (a,b,c,d,mode), new partners p,q ((c,d) for mode 0, (d,c) for mode 1):
+ *   z = [Ha+Hb+Hc+Hd, Ha*Hb + Hc*Hd, Ha*Hp + Hb*Hq]             (192)
+ *   y = relu(z Wr1 + br1) . wr2 + br2                             (prediction)
+ * Weights are kept in fp32 (Adam state too) and rounded to bf16 for every
+ * product; products accumulate in fp32 (mma.sync m16n8k16 bf16).  The loss is
+ * the mean squared error over the swaps of a training call. */
+typedef struct gg_surrogate gg_surrogate;
+gg_status gg_surrogate_create(int device, int n, int degree, int in_features, uint64_t seed,
+                              gg_surrogate **out);
+/* Current graph (n*degree int32, symmetric) and its features (n*in_features). */
+gg_status gg_surrogate_set_graph(gg_surrogate *s, const int32_t *adj, const float *features);
+/* Predictions for P swaps (host arrays). */
+gg_status gg_surrogate_predict(gg_surrogate *s, int P, const gg_swap *swaps, float *pred);
+/* One Adam step on P (swap, target) pairs; swaps with mask[i] == 0 are ignored
+ * (mask may be NULL).  *loss = the mean squared error before the step. */
+gg_status gg_surrogate_train(gg_surrogate *s, int P, const gg_swap *swaps, const float *target,
+                             const int32_t *mask, float lr, float *loss);
+/* Parameters as one flat fp32 vector (layout: W_in, b_in, {Ws, Wn, b} x 3,
+ * Wr1, br1, wr2, br2; matrices row-major [in][out]); count = number of floats. */
+gg_status gg_surrogate_param_count(gg_surrogate *s, int *count);
+gg_status gg_surrogate_get_params(gg_surrogate *s, float *params);
+gg_status gg_surrogate_set_params(gg_surrogate *s, const float *params);
+/* Gradient of the loss (same layout) without updating the parameters. */
+gg_status gg_surrogate_grad(gg_surrogate *s, int P, const gg_swap *swaps, const float *target,
+                            const int32_t *mask, float *grad, float *loss);
+gg_status gg_surrogate_destroy(gg_surrogate *s);
 
 /* ---- generators (host, deterministic, no GPU) ----------------------------
  * Random simple connected d-regular graph on n vertices: configuration-model

@@ -53,8 +53,12 @@ class Trace:
 
 
 def anneal(adj0, steps, *, seed=1, exact=32, pool=4096, explore=8, surrogate=False, t0_frac=1e-3,
-           t_end=1e-6, target=None, time_limit=None, lr=2e-3, device=0):
-    """Anneal from `adj0` (n x d simple regular graph).  Returns (best_adj, Trace)."""
+           t_end=1e-6, target=None, time_limit=None, lr=2e-3, feature_every=32, train_every=2,
+           device=0):
+    """Anneal from `adj0` (n x d simple regular graph).  Returns (best_adj, Trace).
+    With the surrogate, the adjacency it passes messages over follows every
+    accepted move; its distance-histogram features are recomputed every
+    `feature_every` accepted moves (one 2-opt changes them only locally)."""
     adj = np.array(adj0, dtype=np.int32, copy=True)
     n, d = adj.shape
     npairs = n * (n - 1)
@@ -70,9 +74,12 @@ def anneal(adj0, steps, *, seed=1, exact=32, pool=4096, explore=8, surrogate=Fal
     rng = np.random.default_rng(seed)
     net = None
     scale = None
+    feats = None
+    pending = []
     if surrogate:
         net = G.Surrogate(n, d, HIST_K + 1, seed=seed)
-        net.set_graph(adj, features(b, bid))
+        feats = features(b, bid)
+        net.set_graph(adj, feats)
     tr = Trace()
     t_start = time.perf_counter()
     tr.times.append(0.0)
@@ -95,12 +102,17 @@ def anneal(adj0, steps, *, seed=1, exact=32, pool=4096, explore=8, surrogate=Fal
         ok = res["connected"] == 1
         totals = res["total"].astype(np.int64)
         if net is not None:
+            # label the exact results and train every `train_every` steps on the
+            # pairs gathered since the last update (one backward over the graph)
             delta = (totals - cur_total).astype(np.float64) / npairs
             if scale is None and ok.any():
                 scale = max(float(np.std(delta[ok])), 1e-12)
-            tgt = (delta / scale).astype(np.float32)
-            net.train(props, tgt, lr=lr, mask=ok.astype(np.int32))
-            tr.train_pairs += int(ok.sum())
+            pending.append((props, (delta / scale).astype(np.float32), ok.astype(np.int32)))
+            if len(pending) >= train_every:
+                net.train(np.concatenate([p[0] for p in pending]), np.concatenate([p[1] for p in pending]),
+                          lr=lr, mask=np.concatenate([p[2] for p in pending]))
+                tr.train_pairs += int(sum(p[2].sum() for p in pending))
+                pending.clear()
         if ok.any():
             key = np.where(ok, res["levels"].astype(np.int64) * (1 << 40) + totals, np.iinfo(np.int64).max)
             k = int(np.argmin(key))
@@ -115,7 +127,9 @@ def anneal(adj0, steps, *, seed=1, exact=32, pool=4096, explore=8, surrogate=Fal
                 cur_total, cur_diam = ty, dy
                 tr.accepted += 1
                 if net is not None:
-                    net.set_graph(adj, features(b, bid))
+                    if tr.accepted % feature_every == 0:
+                        feats = features(b, bid)
+                    net.set_graph(adj, feats)
                 aspl = cur_total / npairs
                 if aspl < best_aspl:
                     best_aspl, best_adj = aspl, adj.copy()

@@ -68,14 +68,18 @@ __global__ void __launch_bounds__(128) gemm_bf16_kernel(const GemmArgs g) {
 #pragma unroll
     for (int j = 0; j < 8; ++j) acc[j][0] = acc[j][1] = acc[j][2] = acc[j][3] = 0.f;
 
+    // consecutive threads walk whichever operand axis is contiguous in memory
+    const bool a_m_fast = g.sam == 1, b_n_fast = g.sbn == 1;
     for (int k0 = k_begin; k0 < k_end; k0 += 16) {
         for (int e = tid; e < 64 * 16; e += 128) {
-            const int r = e >> 4, k = e & 15, m = m0 + r, kk = k0 + k;
+            const int r = a_m_fast ? (e & 63) : (e >> 4), k = a_m_fast ? (e >> 6) : (e & 15);
+            const int m = m0 + r, kk = k0 + k;
             const float x = (m < g.M && kk < k_end) ? g.A[m * g.sam + kk * g.sak] : 0.f;
             As[r][k] = bf16_bits(x);
         }
         for (int e = tid; e < 64 * 16; e += 128) {
-            const int n = e >> 4, k = e & 15, nn = n0 + n, kk = k0 + k;
+            const int n = b_n_fast ? (e & 63) : (e >> 4), k = b_n_fast ? (e >> 6) : (e & 15);
+            const int nn = n0 + n, kk = k0 + k;
             const float x = (nn < g.N && kk < k_end) ? g.B[kk * g.sbk + nn * g.sbn] : 0.f;
             Bt[n][k] = bf16_bits(x);
         }
@@ -168,11 +172,16 @@ __global__ void readout_out_kernel(const float *O, const float *w, const float *
     }
 }
 
+// Per-call scalars, written by the host before each replay: [0] 1/count of
+// unmasked swaps, [1] learning rate, [2] 1 - beta1^t, [3] 1 - beta2^t.
+enum { kHypInvCnt = 0, kHypLr = 1, kHypC1 = 2, kHypC2 = 3, kHypN = 4 };
+
 // dy = mask * 2 (y - t) / cnt ; loss += mask * (y - t)^2 / cnt
-__global__ void mse_kernel(const float *y, const float *t, const int32_t *mask, int P, float inv_cnt,
+__global__ void mse_kernel(const float *y, const float *t, const int32_t *mask, int P, const float *hyper,
                            float *dy, float *loss) {
+    const float inv_cnt = hyper[kHypInvCnt];
     for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < P; p += gridDim.x * blockDim.x) {
-        const float m = mask ? (mask[p] ? 1.f : 0.f) : 1.f;
+        const float m = mask[p] ? 1.f : 0.f;
         const float e = (y[p] - t[p]) * m;
         dy[p] = 2.f * e * inv_cnt;
         atomicAdd(loss, e * e * inv_cnt);
@@ -230,8 +239,9 @@ __global__ void readout_scatter_kernel(const float *H, const gg_swap *sw, const 
     }
 }
 
-__global__ void adam_kernel(float *p, const float *g, float *m, float *v, int count, float lr, float b1,
-                            float b2, float c1, float c2, float eps) {
+__global__ void adam_kernel(float *p, const float *g, float *m, float *v, int count, const float *hyper,
+                            float b1, float b2, float eps) {
+    const float lr = hyper[kHypLr], c1 = hyper[kHypC1], c2 = hyper[kHypC2];
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x) {
         const float gi = g[i];
         const float mi = b1 * m[i] + (1.f - b1) * gi;
@@ -261,13 +271,20 @@ struct gg_surrogate {
     float *Hs[kLayers + 1] = {};
     float *Ms[kLayers] = {};
     float *dH0 = nullptr, *dH1 = nullptr, *G = nullptr;
-    int cap = 0;  // swap capacity
-    gg_swap *sw = nullptr;
+    // per-swap device buffers and their pinned host staging (capacity `cap`)
+    int cap = 0;
+    gg_swap *sw = nullptr, *h_sw = nullptr;
     float *Z = nullptr, *O = nullptr, *y = nullptr, *t = nullptr, *dy = nullptr, *dO = nullptr, *dZ = nullptr;
-    int32_t *mask = nullptr;
-    float *loss = nullptr;
+    float *h_y = nullptr, *h_t = nullptr;
+    int32_t *mask = nullptr, *h_mask = nullptr;
+    float *loss = nullptr, *h_loss = nullptr;
+    float *hyper = nullptr, *h_hyper = nullptr;
     bool fwd_valid = false, graph_set = false;
     long long adam_step = 0;
+    // captured launch sequences, per swap count: predict (with the graph
+    // forward), readout+backward (grad), readout+backward+Adam (train)
+    struct Cached { int P; int kind; cudaGraphExec_t exec; };
+    std::vector<Cached> graphs;
 };
 
 namespace {
@@ -297,13 +314,22 @@ void gemm(cudaStream_t st, int M, int N, int K, const float *A, long long sam, l
     gemm_bf16_kernel<<<grid, 128, 0, st>>>(g);
 }
 
-int split_for(long long K) { return (int)std::max<long long>(1, std::min<long long>(K / 256, 64)); }
+// K split so that each block runs about four k-steps of 16 (the weight
+// gradients reduce over all vertices or swaps and have only one 64x64 tile).
+int split_for(long long K) { return (int)std::max<long long>(1, std::min<long long>(K / 64, 128)); }
+
+void drop_graphs(gg_surrogate *s) {
+    for (auto &c : s->graphs) cudaGraphExecDestroy(c.exec);
+    s->graphs.clear();
+}
 
 gg_status ensure_swaps(gg_surrogate *s, int P) {
     if (P <= s->cap) return GG_OK;
     const int cap = std::max(P, 2 * s->cap);
+    drop_graphs(s);
     cudaFree(s->sw); cudaFree(s->Z); cudaFree(s->O); cudaFree(s->y); cudaFree(s->t);
     cudaFree(s->dy); cudaFree(s->dO); cudaFree(s->dZ); cudaFree(s->mask);
+    cudaFreeHost(s->h_sw); cudaFreeHost(s->h_y); cudaFreeHost(s->h_t); cudaFreeHost(s->h_mask);
     s->cap = 0;
     GS_CK(cudaMalloc(&s->sw, (size_t)cap * sizeof(gg_swap)));
     GS_CK(cudaMalloc(&s->Z, (size_t)cap * kZ * 4));
@@ -314,6 +340,10 @@ gg_status ensure_swaps(gg_surrogate *s, int P) {
     GS_CK(cudaMalloc(&s->dO, (size_t)cap * kH * 4));
     GS_CK(cudaMalloc(&s->dZ, (size_t)cap * kZ * 4));
     GS_CK(cudaMalloc(&s->mask, (size_t)cap * 4));
+    GS_CK(cudaMallocHost(&s->h_sw, (size_t)cap * sizeof(gg_swap)));
+    GS_CK(cudaMallocHost(&s->h_y, (size_t)cap * 4));
+    GS_CK(cudaMallocHost(&s->h_t, (size_t)cap * 4));
+    GS_CK(cudaMallocHost(&s->h_mask, (size_t)cap * 4));
     s->cap = cap;
     return GG_OK;
 }
@@ -330,10 +360,9 @@ void forward_graph(gg_surrogate *s) {
         gemm(s->st, n, kH, kH, s->Ms[l], kH, 1, P + s->o_wn[l], kH, 1, s->Hs[l + 1], kH, 1, true);
         bias_relu_kernel<<<blocks_for((long long)n * kH), 256, 0, s->st>>>(s->Hs[l + 1], P + s->o_b[l], n, kH);
     }
-    s->fwd_valid = true;
 }
 
-// Readout of the P swaps already in s->sw: Z, O, y.
+// Readout of the P swaps in s->sw: Z, O, y.
 void forward_readout(gg_surrogate *s, int P) {
     float *Pm = s->params;
     readout_z_kernel<<<blocks_for((long long)P * kH), 256, 0, s->st>>>(s->Hs[kLayers], s->sw, P, s->Z);
@@ -342,13 +371,13 @@ void forward_readout(gg_surrogate *s, int P) {
     readout_out_kernel<<<blocks_for((long long)P * 32), 256, 0, s->st>>>(s->O, Pm + s->o_wr2, Pm + s->o_br2, P, s->y);
 }
 
-// Loss and full gradient into s->grad (zeroed here) for the swaps/targets on the device.
-void backward(gg_surrogate *s, int P, float inv_cnt, bool use_mask) {
+// Loss and full gradient into s->grad (zeroed here) for the swaps/targets/mask on the device.
+void backward(gg_surrogate *s, int P) {
     const int n = s->n;
     float *Pm = s->params, *Gd = s->grad;
     cudaMemsetAsync(Gd, 0, (size_t)s->n_params * 4, s->st);
     cudaMemsetAsync(s->loss, 0, 4, s->st);
-    mse_kernel<<<blocks_for(P), 256, 0, s->st>>>(s->y, s->t, use_mask ? s->mask : nullptr, P, inv_cnt, s->dy, s->loss);
+    mse_kernel<<<blocks_for(P), 256, 0, s->st>>>(s->y, s->t, s->mask, P, s->hyper, s->dy, s->loss);
     readout_out_back_kernel<<<std::min(P, 256), kH, 0, s->st>>>(s->O, Pm + s->o_wr2, s->dy, P, s->dO,
                                                                 Gd + s->o_wr2, Gd + s->o_br2);
     colsum_kernel<<<std::min(P, 256), kH, 0, s->st>>>(s->dO, P, Gd + s->o_br1);
@@ -375,7 +404,49 @@ void backward(gg_surrogate *s, int P, float inv_cnt, bool use_mask) {
     gemm(s->st, s->F, kH, n, s->X, 1, s->F, dH, kH, 1, Gd + s->o_win, kH, 1, true, split_for(n));
 }
 
-gg_status load_swaps(gg_surrogate *s, int P, const gg_swap *swaps) {
+enum { kPredict = 0, kGrad = 1, kTrain = 2 };
+
+// The launch sequence of one call kind for P swaps, staged from/to pinned memory.
+void enqueue_kind(gg_surrogate *s, int kind, int P) {
+    cudaMemcpyAsync(s->sw, s->h_sw, (size_t)P * sizeof(gg_swap), cudaMemcpyHostToDevice, s->st);
+    if (kind == kPredict) {
+        forward_graph(s);
+        forward_readout(s, P);
+        cudaMemcpyAsync(s->h_y, s->y, (size_t)P * 4, cudaMemcpyDeviceToHost, s->st);
+        return;
+    }
+    cudaMemcpyAsync(s->t, s->h_t, (size_t)P * 4, cudaMemcpyHostToDevice, s->st);
+    cudaMemcpyAsync(s->mask, s->h_mask, (size_t)P * 4, cudaMemcpyHostToDevice, s->st);
+    cudaMemcpyAsync(s->hyper, s->h_hyper, kHypN * 4, cudaMemcpyHostToDevice, s->st);
+    forward_readout(s, P);
+    backward(s, P);
+    if (kind == kTrain)
+        adam_kernel<<<blocks_for(s->n_params), 256, 0, s->st>>>(s->params, s->grad, s->adam_m, s->adam_v,
+                                                               s->n_params, s->hyper, 0.9f, 0.999f, 1e-8f);
+    cudaMemcpyAsync(s->h_loss, s->loss, 4, cudaMemcpyDeviceToHost, s->st);
+}
+
+// Replay (capturing on first use) the sequence `kind` for P swaps, then wait.
+gg_status run_kind(gg_surrogate *s, int kind, int P) {
+    cudaGraphExec_t exec = nullptr;
+    for (auto &c : s->graphs)
+        if (c.P == P && c.kind == kind) exec = c.exec;
+    if (!exec) {
+        GS_CK(cudaStreamBeginCapture(s->st, cudaStreamCaptureModeThreadLocal));
+        enqueue_kind(s, kind, P);
+        cudaGraph_t g = nullptr;
+        GS_CK(cudaStreamEndCapture(s->st, &g));
+        const cudaError_t e = cudaGraphInstantiate(&exec, g, 0);
+        cudaGraphDestroy(g);
+        GS_CK(e);
+        s->graphs.push_back({P, kind, exec});
+    }
+    GS_CK(cudaGraphLaunch(exec, s->st));
+    GS_CK(cudaStreamSynchronize(s->st));
+    return GG_OK;
+}
+
+gg_status stage_swaps(gg_surrogate *s, int P, const gg_swap *swaps) {
     for (int i = 0; i < P; ++i) {
         const gg_swap &w = swaps[i];
         if (w.a < 0 || w.a >= s->n || w.b < 0 || w.b >= s->n || w.c < 0 || w.c >= s->n || w.d < 0 ||
@@ -384,32 +455,42 @@ gg_status load_swaps(gg_surrogate *s, int P, const gg_swap *swaps) {
     }
     gg_status r = ensure_swaps(s, P);
     if (r != GG_OK) return r;
-    GS_CK(cudaMemcpyAsync(s->sw, swaps, (size_t)P * sizeof(gg_swap), cudaMemcpyHostToDevice, s->st));
+    std::memcpy(s->h_sw, swaps, (size_t)P * sizeof(gg_swap));
     return GG_OK;
 }
 
-gg_status grad_common(gg_surrogate *s, int P, const gg_swap *swaps, const float *target,
-                      const int32_t *mask, float *loss) {
+gg_status grad_common(gg_surrogate *s, int kind, int P, const gg_swap *swaps, const float *target,
+                      const int32_t *mask, float lr, float *loss) {
     if (!s || P < 1 || !swaps || !target) return sfail(GG_BAD_ARG, "bad arguments");
     if (!s->graph_set) return sfail(GG_BAD_ARG, "no graph set");
     GS_CK(cudaSetDevice(s->device));
-    gg_status r = load_swaps(s, P, swaps);
+    gg_status r = stage_swaps(s, P, swaps);
     if (r != GG_OK) return r;
-    int cnt = P;
-    if (mask) {
-        cnt = 0;
-        for (int i = 0; i < P; ++i) cnt += mask[i] != 0;
-        GS_CK(cudaMemcpyAsync(s->mask, mask, (size_t)P * 4, cudaMemcpyHostToDevice, s->st));
+    int cnt = 0;
+    for (int i = 0; i < P; ++i) {
+        s->h_mask[i] = mask ? (mask[i] != 0) : 1;
+        cnt += s->h_mask[i];
     }
-    GS_CK(cudaMemcpyAsync(s->t, target, (size_t)P * 4, cudaMemcpyHostToDevice, s->st));
-    if (!s->fwd_valid) forward_graph(s);
-    forward_readout(s, P);
-    backward(s, P, cnt ? 1.f / (float)cnt : 0.f, mask != nullptr);
-    GS_CK(cudaGetLastError());
-    float h = 0.f;
-    GS_CK(cudaMemcpyAsync(&h, s->loss, 4, cudaMemcpyDeviceToHost, s->st));
-    GS_CK(cudaStreamSynchronize(s->st));
-    if (loss) *loss = h;
+    std::memcpy(s->h_t, target, (size_t)P * 4);
+    s->h_hyper[kHypInvCnt] = cnt ? 1.f / (float)cnt : 0.f;
+    s->h_hyper[kHypLr] = lr;
+    if (kind == kTrain) {
+        const long long t = s->adam_step + 1;
+        s->h_hyper[kHypC1] = 1.f - std::pow(0.9f, (float)t);
+        s->h_hyper[kHypC2] = 1.f - std::pow(0.999f, (float)t);
+    }
+    if (!s->fwd_valid) {  // embeddings of the current graph and parameters
+        forward_graph(s);
+        GS_CK(cudaGetLastError());
+        s->fwd_valid = true;
+    }
+    r = run_kind(s, kind, P);
+    if (r != GG_OK) return r;
+    if (kind == kTrain) {
+        s->adam_step += 1;
+        s->fwd_valid = false;
+    }
+    if (loss) *loss = *s->h_loss;
     return GG_OK;
 }
 
@@ -466,10 +547,12 @@ gg_status gg_surrogate_create(int device, int n, int degree, int in_features, ui
               cudaMalloc(&s->dH0, (size_t)n * kH * 4) == cudaSuccess &&
               cudaMalloc(&s->dH1, (size_t)n * kH * 4) == cudaSuccess &&
               cudaMalloc(&s->G, (size_t)n * kH * 4) == cudaSuccess &&
-              cudaMalloc(&s->loss, 4) == cudaSuccess;
+              cudaMalloc(&s->loss, 4) == cudaSuccess && cudaMalloc(&s->hyper, kHypN * 4) == cudaSuccess &&
+              cudaMallocHost(&s->h_loss, 4) == cudaSuccess && cudaMallocHost(&s->h_hyper, kHypN * 4) == cudaSuccess;
     for (int l = 0; l <= kLayers && ok; ++l) ok = cudaMalloc(&s->Hs[l], (size_t)n * kH * 4) == cudaSuccess;
     for (int l = 0; l < kLayers && ok; ++l) ok = cudaMalloc(&s->Ms[l], (size_t)n * kH * 4) == cudaSuccess;
     if (!ok) return bad(sfail(GG_OUT_OF_MEMORY, "surrogate allocation failed"));
+    std::memset(s->h_hyper, 0, kHypN * 4);
     if (cudaMemcpy(s->params, p.data(), pb, cudaMemcpyHostToDevice) != cudaSuccess ||
         cudaMemset(s->adam_m, 0, pb) != cudaSuccess || cudaMemset(s->adam_v, 0, pb) != cudaSuccess)
         return bad(sfail(GG_CUDA_ERROR, "surrogate initialisation failed"));
@@ -495,20 +578,19 @@ gg_status gg_surrogate_predict(gg_surrogate *s, int P, const gg_swap *swaps, flo
     if (!s->graph_set) return sfail(GG_BAD_ARG, "no graph set");
     if (P == 0) return GG_OK;
     GS_CK(cudaSetDevice(s->device));
-    gg_status r = load_swaps(s, P, swaps);
+    gg_status r = stage_swaps(s, P, swaps);
     if (r != GG_OK) return r;
-    if (!s->fwd_valid) forward_graph(s);
-    forward_readout(s, P);
-    GS_CK(cudaGetLastError());
-    GS_CK(cudaMemcpyAsync(pred, s->y, (size_t)P * 4, cudaMemcpyDeviceToHost, s->st));
-    GS_CK(cudaStreamSynchronize(s->st));
+    r = run_kind(s, kPredict, P);  // recomputes the embeddings: they are valid afterwards
+    if (r != GG_OK) return r;
+    s->fwd_valid = true;
+    std::memcpy(pred, s->h_y, (size_t)P * 4);
     return GG_OK;
 }
 
 gg_status gg_surrogate_grad(gg_surrogate *s, int P, const gg_swap *swaps, const float *target,
                             const int32_t *mask, float *grad, float *loss) {
     if (!grad) return sfail(GG_BAD_ARG, "null grad");
-    gg_status r = grad_common(s, P, swaps, target, mask, loss);
+    gg_status r = grad_common(s, kGrad, P, swaps, target, mask, 0.f, loss);
     if (r != GG_OK) return r;
     GS_CK(cudaMemcpy(grad, s->grad, (size_t)s->n_params * 4, cudaMemcpyDeviceToHost));
     return GG_OK;
@@ -516,17 +598,7 @@ gg_status gg_surrogate_grad(gg_surrogate *s, int P, const gg_swap *swaps, const 
 
 gg_status gg_surrogate_train(gg_surrogate *s, int P, const gg_swap *swaps, const float *target,
                              const int32_t *mask, float lr, float *loss) {
-    gg_status r = grad_common(s, P, swaps, target, mask, loss);
-    if (r != GG_OK) return r;
-    const float b1 = 0.9f, b2 = 0.999f, eps = 1e-8f;
-    s->adam_step += 1;
-    const float c1 = 1.f - std::pow(b1, (float)s->adam_step), c2 = 1.f - std::pow(b2, (float)s->adam_step);
-    adam_kernel<<<blocks_for(s->n_params), 256, 0, s->st>>>(s->params, s->grad, s->adam_m, s->adam_v,
-                                                           s->n_params, lr, b1, b2, c1, c2, eps);
-    GS_CK(cudaGetLastError());
-    s->fwd_valid = false;
-    GS_CK(cudaStreamSynchronize(s->st));
-    return GG_OK;
+    return grad_common(s, kTrain, P, swaps, target, mask, lr, loss);
 }
 
 gg_status gg_surrogate_param_count(gg_surrogate *s, int *count) {
@@ -554,12 +626,15 @@ gg_status gg_surrogate_destroy(gg_surrogate *s) {
     if (!s) return GG_OK;
     cudaSetDevice(s->device);
     if (s->st) cudaStreamSynchronize(s->st);
+    drop_graphs(s);
     cudaFree(s->params); cudaFree(s->grad); cudaFree(s->adam_m); cudaFree(s->adam_v);
     cudaFree(s->adj); cudaFree(s->X); cudaFree(s->dH0); cudaFree(s->dH1); cudaFree(s->G); cudaFree(s->loss);
+    cudaFree(s->hyper); cudaFreeHost(s->h_loss); cudaFreeHost(s->h_hyper);
     for (auto p : s->Hs) cudaFree(p);
     for (auto p : s->Ms) cudaFree(p);
     cudaFree(s->sw); cudaFree(s->Z); cudaFree(s->O); cudaFree(s->y); cudaFree(s->t);
     cudaFree(s->dy); cudaFree(s->dO); cudaFree(s->dZ); cudaFree(s->mask);
+    cudaFreeHost(s->h_sw); cudaFreeHost(s->h_y); cudaFreeHost(s->h_t); cudaFreeHost(s->h_mask);
     if (s->st) cudaStreamDestroy(s->st);
     delete s;
     return GG_OK;

@@ -48,6 +48,9 @@ WORKLOADS = {
     # batched 2-opt candidates: 2048 on a 6-regular n=1024 base + 512 on a
     # 4-regular n=3000 base, one launch per step
     "batch_2opt_2048x1024d6_512x3000d4": dict(form="batch", seed=11),
+    # surrogate-ranked vs plain batched annealing: random 8-regular n=4096 start,
+    # geometric schedule 1e-3*ASPL -> 1e-6 over 1e5 steps, 32 exact scores per step
+    "anneal_n4096_d8_time_to_target": dict(form="anneal", n=4096, d=8, seed=1, steps=100000),
 }
 METRIC = "ASPL evals/s"
 UNIT = "evals/s"
@@ -234,7 +237,11 @@ def run_ours(args):
     if args.batch_sources:
         eng.set_batch_sources(args.batch_sources)
     table_dev = torch.from_numpy(np.ascontiguousarray(wl["table"])).cuda()
-    stream = torch.cuda.current_stream()
+    # an explicit stream: the engine runs on it, and the events and the L2
+    # flush are recorded on it (the legacy default stream has the handle 0,
+    # which the engine reads as "use your own stream")
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
     sptr = stream.cuda_stream
 
     def step():
@@ -359,12 +366,49 @@ def main():
     ap.add_argument("--cpu-s", type=float, default=10.0)
     ap.add_argument("--ref-step-s", type=float, default=4.0)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--anneal-steps", type=int, default=0, help="annealing schedule length (time-to-target workload)")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
     if WORKLOADS[args.workload]["form"] == "batch":
         return run_batch(args)
+    if WORKLOADS[args.workload]["form"] == "anneal":
+        return run_anneal(args)
     return run_ours(args)
+
+
+def run_anneal(args):
+    """Time-to-target: plain batched annealing runs its whole schedule; its final
+    best ASPL is the target; the surrogate-ranked annealer (same seed, same
+    schedule) runs until it reaches that exact-verified ASPL.  value = plain wall
+    time to its final best / surrogate wall time to the same ASPL."""
+    import torch
+    import graphgolf as G
+    import anneal as A
+    rank, world, local = env_rank()
+    torch.cuda.set_device(local)
+    w = WORKLOADS[args.workload]
+    steps = args.anneal_steps or w["steps"]
+    adj = G.random_regular(w["n"], w["d"], w["seed"] + 1000 * rank)
+    A.anneal(adj, 50, seed=w["seed"])                      # warm-up (graphs, caches)
+    A.anneal(adj, 50, seed=w["seed"], surrogate=True)
+    _, plain = A.anneal(adj, steps, seed=w["seed"], exact=32, device=local)
+    target = plain.final_best
+    t_plain = A.time_to(plain, target)
+    _, sur = A.anneal(adj, steps, seed=w["seed"], exact=32, surrogate=True, target=target, device=local)
+    line = {"metric": "ASPL time-to-target, plain / surrogate", "value":
+            (t_plain / sur.hit_time) if sur.hit_time else None, "unit": "x", "n_gpus": world,
+            "steps": steps, "warmup": 1, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "u32 exact BFS; bf16/fp32 surrogate", "data": "synthetic",
+            "config": {"workload": args.workload, "n": w["n"], "degree": w["d"], "exact_per_step": 32,
+                       "surrogate_pool": 4096, "schedule": "geometric 1e-3*ASPL -> 1e-6"},
+            "plain": {"wall_s": plain.wall, "time_to_final_s": t_plain, "steps": plain.steps,
+                      "start_aspl": plain.best[0], "final_aspl": target, "ms_per_step": 1000 * plain.wall / plain.steps},
+            "surrogate": {"hit_s": sur.hit_time, "hit_step": sur.hit_step, "final_aspl": sur.final_best,
+                          "train_pairs": sur.train_pairs, "ms_per_step": 1000 * sur.wall / max(sur.steps, 1)}}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    return 0
 
 
 def run_batch(args):
@@ -385,7 +429,8 @@ def run_batch(args):
     n = len(sw)
     d_sw = torch.from_numpy(sw.view(np.int32).copy()).cuda()
     d_out = torch.zeros(n * G.CAND_RESULT_DTYPE.itemsize // 4, dtype=torch.int32, device="cuda")
-    stream = torch.cuda.current_stream()
+    stream = torch.cuda.Stream()  # explicit: the launch, the events and the flush share it
+    torch.cuda.set_stream(stream)
     flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
     for _ in range(max(args.warmup, 1)):
         b.eval_device(n, d_sw.data_ptr(), d_out.data_ptr(), stream.cuda_stream)

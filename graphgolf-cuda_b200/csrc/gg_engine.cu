@@ -17,6 +17,9 @@
 #include <cstdlib>
 #include <cstring>
 #include <string>
+#include <map>
+#include <mutex>
+#include <tuple>
 #include <vector>
 
 using gg::BfsArgs;
@@ -171,6 +174,22 @@ void *kernel_for(int d) {
 }
 
 // Source-batch plan: batch width, chunks per row, grid size.
+// Batch widths chosen by gg_autotune, by (device, form, rows, degree, sources).
+struct TuneKey {
+    int device, form, rows, d, n_src;
+    bool operator<(const TuneKey &o) const {
+        return std::tie(device, form, rows, d, n_src) < std::tie(o.device, o.form, o.rows, o.d, o.n_src);
+    }
+};
+std::mutex g_tune_mu;
+std::map<TuneKey, int> g_tuned;
+
+int tuned_width(const gg_engine *e) {
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    auto it = g_tuned.find({e->device, e->form, e->rows, e->d, (int)e->reps.size()});
+    return it == g_tuned.end() ? 0 : it->second;
+}
+
 gg_status plan(gg_engine *e, int want_bits) {
     const int n_src = (int)e->reps.size();
     int bits;
@@ -178,8 +197,11 @@ gg_status plan(gg_engine *e, int want_bits) {
         bits = want_bits;
     } else {
         const int env = env_int("GG_BATCH_SOURCES", 0);
+        const int tuned = tuned_width(e);
         if (env > 0) {
             bits = env;
+        } else if (tuned > 0) {
+            bits = tuned;
         } else {
             // The widest batch whose three bitsets (3 * rows * bits / 8 bytes)
             // stay within 3/4 of the L2, so that the gathers hit L2 rather than
@@ -664,6 +686,64 @@ gg_status gg_set_batch_sources(gg_engine *e, int sources) {
     GG_CK(cudaSetDevice(e->device));
     GG_CK(cudaStreamSynchronize(e->stream));
     return plan(e, sources);
+}
+
+gg_status gg_autotune(gg_engine *e, const int32_t *table, int trials, int *best_sources, double *best_ms) {
+    if (!e || (e->table_elems && !table) || trials < 1) return fail(GG_BAD_ARG, "bad arguments");
+    GG_CK(cudaSetDevice(e->device));
+    GG_CK(cudaStreamSynchronize(e->stream));
+    const int n_src = (int)e->reps.size();
+    // the L2-resident width the default plan picks, and its neighbours
+    int base = 0;
+    {
+        const int keep = e->batch_bits;
+        gg_status s = plan(e, 0);
+        if (s != GG_OK) return s;
+        base = e->batch_bits;
+        if (keep != base && keep > 0) { s = plan(e, keep); if (s != GG_OK) return s; }
+    }
+    std::vector<int> cands;
+    for (double f : {0.25, 0.5, 1.0, 2.0, 4.0}) {
+        int w = (int)(base * f);
+        w = std::max(128, std::min(((w + 127) / 128) * 128, ((n_src + 127) / 128) * 128));
+        cands.push_back(w);
+    }
+    cands.push_back(((n_src + 127) / 128) * 128);
+    std::sort(cands.begin(), cands.end());
+    cands.erase(std::unique(cands.begin(), cands.end()), cands.end());
+    if (e->table_elems) {
+        std::memcpy(e->h_table, table, e->table_elems * sizeof(int32_t));
+        GG_CK(cudaMemcpyAsync(e->d_table, e->h_table, e->table_elems * sizeof(int32_t),
+                              cudaMemcpyHostToDevice, e->stream));
+    }
+    int best = 0;
+    double best_t = 1e300;
+    gg_result r;
+    for (int w : cands) {
+        if ((long long)e->rows * (w / 128) >= (1ll << 31)) continue;
+        gg_status s = plan(e, w);
+        if (s == GG_OUT_OF_MEMORY) { (void)cudaGetLastError(); continue; }  // too wide for this device
+        if (s != GG_OK) return s;
+        s = run_eval(e, e->d_table, nullptr, &r, e->stream);  // warm
+        if (s != GG_OK) return s;
+        double t = 1e300;
+        for (int k = 0; k < trials; ++k) {
+            s = run_eval(e, e->d_table, nullptr, &r, e->stream);
+            if (s != GG_OK) return s;
+            t = std::min(t, e->last_ms);
+        }
+        if (t < best_t) { best_t = t; best = w; }
+    }
+    if (!best) return fail(GG_OUT_OF_MEMORY, "no batch width fits");
+    gg_status s = plan(e, best);
+    if (s != GG_OK) return s;
+    {
+        std::lock_guard<std::mutex> lk(g_tune_mu);
+        g_tuned[{e->device, e->form, e->rows, e->d, n_src}] = best;
+    }
+    if (best_sources) *best_sources = best;
+    if (best_ms) *best_ms = best_t;
+    return GG_OK;
 }
 
 gg_status gg_set_wait_limit_ms(gg_engine *e, int ms) {

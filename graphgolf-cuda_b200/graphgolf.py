@@ -93,6 +93,7 @@ _SIGS = {
     "gg_last_launches": [_P, _IP],
     "gg_last_transfer_bytes": [_P, ctypes.POINTER(ctypes.c_uint64), ctypes.POINTER(ctypes.c_uint64)],
     "gg_set_batch_sources": [_P, _I],
+    "gg_autotune": [_P, _P, _I, _IP, _DP],
     "gg_set_wait_limit_ms": [_P, _I],
     "gg_destroy": [_P],
     "gg_graph_eval_noalloc": [_P, _I, _I, _I, _P, _P],
@@ -451,6 +452,13 @@ class Engine:
 
     def set_batch_sources(self, bits):
         _check(lib().gg_set_batch_sources(self._h, bits))
+
+    def autotune(self, table, trials=3):
+        """Pick the fastest source-batch width for this table; returns (sources, ms)."""
+        t = self._table(table)
+        w, ms = ctypes.c_int(), ctypes.c_double()
+        _check(lib().gg_autotune(self._h, _ptr(t), trials, ctypes.byref(w), ctypes.byref(ms)))
+        return w.value, ms.value
 
     def set_wait_limit_ms(self, ms):
         _check(lib().gg_set_wait_limit_ms(self._h, ms))

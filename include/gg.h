@@ -137,6 +137,13 @@ gg_status gg_last_transfer_bytes(gg_engine *e, uint64_t *h2d, uint64_t *d2h);
 
 /* Tuning: source-batch width in bits (multiple of 128; 0 = automatic). */
 gg_status gg_set_batch_sources(gg_engine *e, int sources);
+/* Autotuner: times `trials` evaluations of `table` for each candidate source-batch
+ * width (fractions and multiples of the L2-resident width, and all sources at once),
+ * keeps the fastest in this engine's plan and records it for engines of the same
+ * form, size and degree created later in the process.  best_sources / best_ms may be
+ * NULL. */
+gg_status gg_autotune(gg_engine *e, const int32_t *table, int trials, int *best_sources,
+                      double *best_ms);
 /* Bounded-wait limit of the in-kernel grid barrier, in milliseconds. */
 gg_status gg_set_wait_limit_ms(gg_engine *e, int ms);
 

@@ -187,6 +187,33 @@ def test_batch_width_invariance_and_source_ranges():
     assert sub["total"] == os_.total()
 
 
+def test_autotune_keeps_results_and_is_adopted():
+    adj = G.random_regular(3000, 6, 4)
+    e = G.cudaASPLgraph(3000, 6, 0)
+    base = e.eval(adj)
+    width, ms = e.autotune(adj, trials=2)
+    assert 0 < width and ms > 0
+    r = e.eval(adj)
+    assert (r["total"], r["levels"], r["reached"]) == (base["total"], base["levels"], base["reached"])
+    # a later engine of the same shape on the same device starts from the tuned width
+    e2 = G.cudaASPLgraph(3000, 6, 0)
+    r2 = e2.eval(adj)
+    assert r2["batches"] == r["batches"]
+    assert r2["total"] == base["total"]
+
+
+def test_shards_of_distributed_helper_sum_to_whole():
+    import distributed as D
+    adj = G.random_regular(2000, 6, 8)
+    e = G.cudaASPLgraph(2000, 6, 0)
+    whole = e.eval(adj)
+    for world in (2, 3, 8):
+        parts = [e.eval(adj, src_range=D.shard(2000, r, world)) for r in range(world)]
+        assert sum(p["total"] for p in parts) == whole["total"]
+        assert sum(p["reached"] for p in parts) == whole["reached"]
+        assert max(p["levels"] for p in parts) == whole["levels"]
+
+
 # ---- benchmark configurations ---------------------------------------------
 
 def test_config_regular_4096_16():

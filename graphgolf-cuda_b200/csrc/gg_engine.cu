@@ -92,6 +92,8 @@ struct gg_engine {
     int dense_w_ppm = 100;               // level-mode thresholds (see bfs_batch_kernel)
     int dense_r_ppm = 4000;
     int full_skip_ppm = 995000;
+    int push_ppm = 300;                  // push (top-down) levels below this frontier share
+    int push_min_items = 1 << 20;        // ... on bitsets of at least this many chunks
     int adj_smem_rows = 0;               // shared-memory adjacency slice (rows per block)
     size_t smem_bytes = 0;
     long long wait_ns = 10ll * 1000 * 1000 * 1000;
@@ -103,8 +105,13 @@ struct gg_engine {
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     int32_t *d_table = nullptr, *d_adj = nullptr, *d_src = nullptr;
     int *d_bad = nullptr;
+    int *d_asym = nullptr;               // adjacency not symmetric: no push levels
     uint4 *d_V = nullptr, *d_F0 = nullptr, *d_F1 = nullptr;
     uint32_t *d_fl0 = nullptr, *d_fl1 = nullptr;
+    uint4 *d_P0 = nullptr, *d_P1 = nullptr;     // push-level frontier, all zero between launches
+    uint32_t *d_pf0 = nullptr, *d_pf1 = nullptr;
+    uint32_t *d_nf = nullptr;            // not-full bit per visited chunk
+    bool p_dirty = true;                 // push buffers must be zeroed before the next launch
     unsigned long long *d_counts = nullptr;
     unsigned *d_masks = nullptr;
     unsigned long long *d_level_ns = nullptr, *h_level_ns = nullptr;
@@ -126,8 +133,13 @@ namespace {
 void free_batch_buffers(gg_engine *e) {
     cudaFree(e->d_V); cudaFree(e->d_F0); cudaFree(e->d_F1);
     cudaFree(e->d_fl0); cudaFree(e->d_fl1);
+    cudaFree(e->d_P0); cudaFree(e->d_P1); cudaFree(e->d_pf0); cudaFree(e->d_pf1);
+    cudaFree(e->d_nf);
+    e->d_nf = nullptr;
     e->d_V = e->d_F0 = e->d_F1 = nullptr;
     e->d_fl0 = e->d_fl1 = nullptr;
+    e->d_P0 = e->d_P1 = nullptr;
+    e->d_pf0 = e->d_pf1 = nullptr;
 }
 
 void free_counters(gg_engine *e) {
@@ -146,7 +158,7 @@ void destroy_all(gg_engine *e) {
     free_batch_buffers(e);
     free_counters(e);
     if (e->d_adj != e->d_table) cudaFree(e->d_adj);  // the graph form aliases the two
-    cudaFree(e->d_table); cudaFree(e->d_src); cudaFree(e->d_bad);
+    cudaFree(e->d_table); cudaFree(e->d_src); cudaFree(e->d_bad); cudaFree(e->d_asym);
     cudaFreeHost(e->h_table); cudaFreeHost(e->h_bad);
     if (e->ev0) cudaEventDestroy(e->ev0);
     if (e->ev1) cudaEventDestroy(e->ev1);
@@ -234,6 +246,12 @@ gg_status plan(gg_engine *e, int want_bits) {
         GG_CK(cudaMalloc(&e->d_F1, vbytes));
         GG_CK(cudaMalloc(&e->d_fl0, fwords * 4));
         GG_CK(cudaMalloc(&e->d_fl1, fwords * 4));
+        GG_CK(cudaMalloc(&e->d_P0, vbytes));
+        GG_CK(cudaMalloc(&e->d_P1, vbytes));
+        GG_CK(cudaMalloc(&e->d_pf0, fwords * 4));
+        GG_CK(cudaMalloc(&e->d_pf1, fwords * 4));
+        GG_CK(cudaMalloc(&e->d_nf, fwords * 4));
+        e->p_dirty = true;
     }
     int per_sm = 0, sms = 0;
     GG_CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, e->device));
@@ -310,10 +328,13 @@ gg_status create_common(gg_engine *e) {
     GG_CK(cudaMemcpy(e->d_src, e->reps.data(), e->reps.size() * sizeof(int32_t),
                      cudaMemcpyHostToDevice));
     GG_CK(cudaMalloc(&e->d_bad, sizeof(int)));
+    GG_CK(cudaMalloc(&e->d_asym, sizeof(int)));
     GG_CK(cudaMallocHost(&e->h_bad, sizeof(int)));
     e->dense_w_ppm = env_int("GG_DENSE_W_PPM", e->dense_w_ppm);
     e->dense_r_ppm = env_int("GG_DENSE_R_PPM", e->dense_r_ppm);
     e->full_skip_ppm = env_int("GG_FULL_SKIP_PPM", e->full_skip_ppm);
+    e->push_ppm = env_int("GG_PUSH_PPM", e->push_ppm);
+    e->push_min_items = env_int("GG_PUSH_MIN_ITEMS", e->push_min_items);
     const int wait_ms = env_int("GG_WAIT_LIMIT_MS", 10000);
     e->wait_ns = (long long)std::max(wait_ms, 1) * 1000000ll;
     gg_status s = plan(e, 0);
@@ -385,12 +406,24 @@ gg_status run_eval(gg_engine *e, const int32_t *d_table_in, const gg_eval_opts *
         }
     }
     GG_CK(cudaMemsetAsync(e->d_ctl, 0, (size_t)nb * sizeof(Ctl), st));
+    GG_CK(cudaMemsetAsync(e->d_asym, 0, sizeof(int), st));
+    if (e->p_dirty) {
+        // New buffers, or a launch that stopped early: the push buffers are
+        // zero again only after these four writes.
+        const size_t vbytes = (size_t)e->items * sizeof(uint4), fbytes = (size_t)((e->items + 31) / 32) * 4;
+        GG_CK(cudaMemsetAsync(e->d_P0, 0, vbytes, st));
+        GG_CK(cudaMemsetAsync(e->d_P1, 0, vbytes, st));
+        GG_CK(cudaMemsetAsync(e->d_pf0, 0, fbytes, st));
+        GG_CK(cudaMemsetAsync(e->d_pf1, 0, fbytes, st));
+        e->p_dirty = false;
+    }
     if (want_ns)
         GG_CK(cudaMemsetAsync(e->d_level_ns, 0, (size_t)(cap_req + 1) * sizeof(unsigned long long), st));
 
     void *kern = kernel_for(e->d);
     if (fault("launch")) return fail(GG_CUDA_ERROR, "injected launch failure");
     const unsigned extra = fault("barrier") ? 1u : 0u;
+    e->p_dirty = true;  // until the launches are known to have finished cleanly
     for (int b = 0; b < nb; ++b) {
         BfsArgs a{};
         a.adj = e->d_adj;
@@ -398,6 +431,12 @@ gg_status run_eval(gg_engine *e, const int32_t *d_table_in, const gg_eval_opts *
         a.ns = std::min(e->batch_bits, ns_all - b * e->batch_bits);
         a.V = e->d_V; a.F0 = e->d_F0; a.F1 = e->d_F1;
         a.fl0 = e->d_fl0; a.fl1 = e->d_fl1;
+        a.P0 = e->d_P0; a.P1 = e->d_P1; a.pf0 = e->d_pf0; a.pf1 = e->d_pf1;
+        // Below ~1M chunks a pull level costs about one grid barrier anyway.
+        a.push_ppm = (long long)e->items >= (long long)e->push_min_items ? e->push_ppm : 0;
+        a.nf = e->d_nf;
+        a.asym = e->d_asym;
+        a.sym_check = b == 0;
         a.counts = e->d_counts + (size_t)b * stride;
         a.masks = wvc ? e->d_masks + (size_t)b * stride : nullptr;
         a.level_ns = (b == 0 && want_ns) ? e->d_level_ns : nullptr;
@@ -455,6 +494,7 @@ gg_status run_eval(gg_engine *e, const int32_t *d_table_in, const gg_eval_opts *
             return fail(GG_TIMEOUT, "grid barrier wait exceeded its limit at level " +
                                         std::to_string(e->h_ctl[b].err_level));
         }
+    e->p_dirty = false;
 
     // Exact fold of the per-batch level counters.
     gg_result R{};

@@ -48,16 +48,16 @@ struct FastDiv {
 };
 
 // Control block of one cooperative launch (zeroed by the host before launch).
-constexpr int kBarSub = 16;   // first-level arrival counters of the grid barrier
-
+// The barrier's arrival counter and the word the blocks wait on sit on
+// separate 128-byte lines, so the waiting loads do not contend with arrivals.
 struct Ctl {
-    unsigned int bar_count;   // second-level arrivals at the current barrier
-    unsigned int bar_gen;     // barrier generation
+    unsigned int arrive;      // grid-barrier arrivals, counted over the whole launch
     int err;                  // 0, or 1 = a barrier wait exceeded the limit
     int err_level;            // level at which the first wait gave up
     int levels_run;           // last level executed
-    int pad[27];
-    unsigned int sub[kBarSub][32];  // first-level counters, one 128-byte line each
+    int pad0[28];
+    unsigned int passed;      // grid barriers completed so far
+    int pad1[31];
 };
 
 struct BfsArgs {
@@ -81,6 +81,23 @@ struct BfsArgs {
     int adj_smem_rows;        // >0: each block keeps its vertex range's adjacency rows
                               // (at most this many) in dynamic shared memory
     long long wait_ns;        // barrier wait limit
+    // Push (top-down) levels.  P0/P1 [rows][nC] uint4 and pf0/pf1 (one bit per
+    // uint4) hold the frontier of push levels; both are all zero between
+    // launches (every consumer clears what it read).  nullptr or push_ppm 0:
+    // every level pulls.
+    uint4 *P0, *P1;
+    uint32_t *pf0, *pf1;
+    int push_ppm;             // push while the feeding frontier < ppm of the pairs
+    // A push level equals the reference's pull level only when the adjacency is
+    // symmetric (u in adj[w] <=> w in adj[u]).  With sym_check set, phase 0
+    // tests that and stores 1 into *asym on any one-way entry; launches after
+    // the first of an evaluation read the stored answer.  asym nullptr: no push.
+    int *asym;
+    int sym_check;
+    // [ceil(rows * nC / 32)] bit per uint4 of V: set iff that chunk is not yet
+    // full.  Written by levels that load every visited chunk; a later level in
+    // the skip-full stage passes over tiles whose word is 0.  nullptr: unused.
+    uint32_t *nf;
 };
 
 __device__ __forceinline__ unsigned long long gtimer() {
@@ -104,44 +121,39 @@ __device__ __forceinline__ unsigned long long ld_relaxed_u64(const unsigned long
     return v;
 }
 
+__device__ __forceinline__ unsigned ld_relaxed(const unsigned *p) {
+    unsigned v;
+    asm volatile("ld.relaxed.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+
 // Grid-wide barrier with a bounded wait.  Requires co-resident blocks
-// (cooperative launch).  Arrival is two-level: block b counts on sub-counter
-// b % kBarSub, and the last arrival of each sub-counter counts on the top one,
-// so no counter sees more than ~gridDim/kBarSub same-address atomics.
-// `expected` is the number of arrivals the barrier waits for (gridDim.x, or
-// more when a test makes the wait run out).  Returns false on every block once
-// any block's wait ran past the limit; the kernel then returns and the host
-// reports GG_TIMEOUT.
-__device__ __forceinline__ bool grid_barrier(Ctl *ctl, unsigned expected, long long wait_ns,
-                                             int level) {
+// (cooperative launch).  `epoch` counts the barriers this block has passed in
+// the launch (the same number in every block).  Each block adds 1 to `arrive`;
+// the block whose add makes it (epoch + 1) * expected is the last one and
+// publishes `passed` = epoch + 1; every block waits until it reads that value.
+// One atomic per block, and the waiting loads go to a line no arrival touches.
+// `expected` above gridDim.x makes the wait run out (fault-injection tests).
+// Returns false on every block once any block's wait ran past `wait_ns`; the
+// kernel then returns and the host reports GG_TIMEOUT.
+__device__ __forceinline__ bool grid_sync(Ctl *ctl, unsigned expected, long long wait_ns, int level,
+                                          unsigned &epoch) {
     __shared__ int s_ok;
     __syncthreads();
+    const unsigned next = epoch + 1u;
     if (threadIdx.x == 0) {
         int ok = 1;
-        const unsigned nb = gridDim.x;
-        const unsigned s = blockIdx.x % kBarSub;
-        const unsigned sub_expected = (nb - s + kBarSub - 1) / kBarSub;  // blocks b < nb with b%kBarSub == s
-        const unsigned top_expected = min(nb, (unsigned)kBarSub) + (expected - nb);
-        const unsigned gen = ld_acquire(&ctl->bar_gen);
         __threadfence();
-        bool released = false;
-        const unsigned prev = atomicAdd(&ctl->sub[s][0], 1u);
-        if (prev + 1 == sub_expected) {
-            atomicExch(&ctl->sub[s][0], 0u);
+        const unsigned old = atomicAdd(&ctl->arrive, 1u);
+        if (old + 1u == next * expected) {
             __threadfence();
-            const unsigned prev2 = atomicAdd(&ctl->bar_count, 1u);
-            if (prev2 + 1 == top_expected) {
-                atomicExch(&ctl->bar_count, 0u);
-                __threadfence();
-                atomicAdd(&ctl->bar_gen, 1u);
-                released = true;
-            }
+            atomicExch(&ctl->passed, next);
         }
-        if (!released) {
-            const unsigned long long t0 = gtimer();
-            while (ld_acquire(&ctl->bar_gen) == gen) {
+        const unsigned long long t0 = gtimer();
+        for (unsigned it = 1;; ++it) {
+            if (ld_relaxed(&ctl->passed) == next) break;
+            if ((it & 255u) == 0u) {
                 if (ld_acquire_i(&ctl->err)) { ok = 0; break; }
-                __nanosleep(64);
                 if ((long long)(gtimer() - t0) > wait_ns) {
                     if (atomicCAS(&ctl->err, 0, 1) == 0) ctl->err_level = level;
                     ok = 0;
@@ -150,9 +162,9 @@ __device__ __forceinline__ bool grid_barrier(Ctl *ctl, unsigned expected, long l
             }
         }
         __threadfence();
-        if (ok && ld_acquire_i(&ctl->err)) ok = 0;
         s_ok = ok;
     }
+    epoch = next;
     __syncthreads();
     return s_ok != 0;
 }
@@ -268,6 +280,110 @@ __device__ __forceinline__ void level_tiles(const BfsArgs &a, const int d, const
         }
         const unsigned b = __ballot_sync(0xffffffffu, u4any(nw[u]));
         if (lane == 0 && (tile0 + u) < t_hi) fn[tile0 + u] = b;
+        if (a.nf && own_early) {
+            // not-full bits of the tile after this level (own is loaded for every chunk)
+            const unsigned nfb = __ballot_sync(0xffffffffu, ok[u] && !u4full(u4or(own[u], nw[u])));
+            if (lane == 0 && (tile0 + u) < t_hi) a.nf[tile0 + u] = nfb;
+        }
+    }
+}
+
+// Component k of a uint4 (k is a compile-time constant after unrolling).
+__device__ __forceinline__ unsigned comp_of(const uint4 &f, const int k) {
+    return k == 0 ? f.x : (k == 1 ? f.y : (k == 2 ? f.z : f.w));
+}
+
+// Push item (u, c) with frontier chunk f to the neighbours tw[i] = (w_i, c).
+// The visited words are ORed first, all of them in flight together (nothing
+// waits on a returned value before the last one is issued); the bits that were
+// not visited yet -- exact under concurrency, atomicOr returns the old word --
+// are this level's new pairs and go into Pn and the flag words with
+// fire-and-forget reductions.
+template <int D>
+__device__ __forceinline__ void push_item(const BfsArgs &a, const uint4 f, const unsigned *tw,
+                                          uint4 *Pn, uint32_t *pfn, unsigned &cnt) {
+    unsigned any[D];
+#pragma unroll
+    for (int i = 0; i < D; ++i) any[i] = 0u;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        const unsigned fk = comp_of(f, k);
+        if (!fk) continue;
+        unsigned old[D];
+#pragma unroll
+        for (int i = 0; i < D; ++i) old[i] = atomicOr(reinterpret_cast<unsigned *>(a.V + tw[i]) + k, fk);
+#pragma unroll
+        for (int i = 0; i < D; ++i) {
+            const unsigned nb = fk & ~old[i];
+            if (nb) {
+                atomicOr(reinterpret_cast<unsigned *>(Pn + tw[i]) + k, nb);
+                cnt += __popc(nb);
+                any[i] = 1u;
+            }
+        }
+    }
+#pragma unroll
+    for (int i = 0; i < D; ++i)
+        if (any[i]) atomicOr(pfn + (tw[i] >> 5), 1u << (tw[i] & 31u));
+}
+
+// One push level.  The frontier of level L-1 is the set bits of the flag words
+// `pfc` (item t = (u, c) of `Pc`).  Thread (k, i) of a group of D lanes takes
+// flag word k and neighbour slot i: for each item (u, c) of the word it pushes
+// F[u][c] to w = adj[u][i] (the adjacency is symmetric, so the pull rows are also
+// the push rows): new = F[u][c] & ~V[w][c] goes into V, into Pn[w][c], and sets
+// the flag bit of (w, c) in `pfn`.  Each thread thus waits on one atomic per
+// item, and the D pushes of an item run in parallel.  After the group's lanes
+// have read them, lane 0 zeroes the items and the flag word, so Pc is all zero
+// again when the level ends.  Work is proportional to the frontier, not to
+// rows * nC.  Needs D to divide 32 (a group never straddles two warps).
+template <int D>
+__device__ __forceinline__ unsigned push_level(const BfsArgs &a, uint4 *Pc, uint4 *Pn, uint32_t *pfc,
+                                               uint32_t *pfn, const unsigned fwords,
+                                               const unsigned gtid, const unsigned nthr) {
+    static_assert(D > 0 && 32 % D == 0, "push levels need D | 32");
+    unsigned cnt = 0u;
+    const unsigned nC = (unsigned)a.nC;
+    const unsigned lane = threadIdx.x & 31u;
+    const unsigned i = lane % (unsigned)D;
+    const unsigned long long total = (unsigned long long)fwords * D;
+    // warp-uniform trip count: every lane reaches the __syncwarp below
+    for (unsigned long long base = gtid - lane; base < total; base += nthr) {
+        const unsigned long long g = base + lane;
+        const unsigned k = (unsigned)(g / D);
+        const unsigned m0 = g < total ? __ldcg(pfc + k) : 0u;
+        for (unsigned m = m0; m;) {
+            const unsigned b = (unsigned)(__ffs((int)m) - 1);
+            m &= m - 1u;
+            const unsigned t = k * 32u + b;
+            const unsigned u = a.div_nc.div(t);
+            const unsigned c = t - u * nC;
+            const uint4 f = __ldcg(Pc + t);
+            const unsigned tw = (unsigned)__ldg(a.adj + (size_t)u * D + i) * nC + c;
+            push_item<1>(a, f, &tw, Pn, pfn, cnt);
+        }
+        __syncwarp();
+        if (i == 0u && m0) {
+            for (unsigned m = m0; m; m &= m - 1u) Pc[k * 32u + (unsigned)(__ffs((int)m) - 1)] = u4zero();
+            pfc[k] = 0u;
+        }
+    }
+    return cnt;
+}
+
+// Zero the items flagged in `pf` and the flag words themselves (the push buffer
+// a pull level read last), restoring the all-zero state the next launch expects.
+__device__ __forceinline__ void clear_push_buffer(uint4 *P, uint32_t *pf, const unsigned fwords,
+                                                  const unsigned gtid, const unsigned nthr) {
+    for (unsigned k = gtid; k < fwords; k += nthr) {
+        unsigned m = __ldcg(pf + k);
+        if (!m) continue;
+        do {
+            const unsigned b = (unsigned)(__ffs((int)m) - 1);
+            m &= m - 1u;
+            P[k * 32u + b] = u4zero();
+        } while (m);
+        pf[k] = 0u;
     }
 }
 
@@ -287,6 +403,7 @@ __global__ void __launch_bounds__(kBlock, min_blocks_for(D)) bfs_batch_kernel(co
     __shared__ unsigned s_and[2][kBlock / 32];
     __shared__ unsigned s_next;
     if (a.bad && *a.bad) return;  // uniform across the grid: no block reaches a barrier
+    unsigned epoch = 0u;          // grid barriers passed
     const unsigned t_lo = (unsigned)((unsigned long long)ntiles * blockIdx.x / gridDim.x);
     const unsigned t_hi = (unsigned)((unsigned long long)ntiles * (blockIdx.x + 1) / gridDim.x);
 
@@ -310,8 +427,25 @@ __global__ void __launch_bounds__(kBlock, min_blocks_for(D)) bfs_batch_kernel(co
         __syncthreads();
     }
 
+    // Push levels need the all-zero push buffers, a symmetric adjacency and
+    // plain OR rows (the WVC masks are taken over every chunk, which only pull
+    // levels visit).
+    const bool push_req = D > 0 && 32 % D == 0 && a.push_ppm > 0 && a.P0 != nullptr &&
+                          a.asym != nullptr && a.masks == nullptr;
+    if (push_req && a.sym_check) {
+        const unsigned long long n = (unsigned long long)a.rows * (unsigned long long)d;
+        for (unsigned long long k = gtid; k < n; k += nthr) {
+            const unsigned v = (unsigned)(k / (unsigned)d);
+            const int32_t *row = a.adj + (size_t)__ldg(a.adj + k) * (size_t)d;
+            bool found = false;
+            for (int j = 0; j < d; ++j) found |= (unsigned)__ldg(row + j) == v;
+            if (!found) *a.asym = 1;
+        }
+    }
+
     // Phase 0: per-batch reset (cudaASPLconv.cu:9-33): padding bits visited,
-    // frontier and flags cleared, counters zeroed.
+    // flags cleared, counters zeroed.  F0 itself is not cleared: a reader only
+    // touches the chunks whose flag bit is set, and phase 1 stores those whole.
     if (blockIdx.x == 0)
         for (int i = threadIdx.x; i <= a.max_levels; i += blockDim.x) {
             a.counts[i] = 0ull;
@@ -320,21 +454,30 @@ __global__ void __launch_bounds__(kBlock, min_blocks_for(D)) bfs_batch_kernel(co
     for (unsigned t = gtid; t < items; t += nthr) {
         const unsigned c = t - a.div_nc.div(t) * (unsigned)a.nC;
         a.V[t] = pad_mask((int)c, a.ns);
-        a.F0[t] = u4zero();
     }
     for (unsigned w = gtid; w < ntiles; w += nthr) a.fl0[w] = 0u;
-    if (!grid_barrier(a.ctl, a.expected, a.wait_ns, 0)) return;
+    if (!grid_sync(a.ctl, a.expected, a.wait_ns, 0, epoch)) return;
+    const bool push_on = push_req && ld_acquire_i(a.asym) == 0;
 
     // Phase 1: the diagonal -- source i has reached its own vertex at level 0.
+    // The sources of a batch are distinct vertices, so each chunk holds at most
+    // one of them and is stored whole.
     for (unsigned i = gtid; i < (unsigned)a.ns; i += nthr) {
         const unsigned t = (unsigned)a.src[i] * (unsigned)a.nC + (i >> 7);
         const unsigned bit = 1u << (i & 31u), comp = (i >> 5) & 3u;
         atomicOr(reinterpret_cast<unsigned *>(a.V + t) + comp, bit);
-        atomicOr(reinterpret_cast<unsigned *>(a.F0 + t) + comp, bit);
-        atomicOr(a.fl0 + (t >> 5), 1u << (t & 31u));
+        uint4 one = u4zero();
+        if (comp == 0u) one.x = bit; else if (comp == 1u) one.y = bit; else if (comp == 2u) one.z = bit; else one.w = bit;
+        if (push_on) {
+            a.P0[t] = one;
+            atomicOr(a.pf0 + (t >> 5), 1u << (t & 31u));
+        } else {
+            a.F0[t] = one;
+            atomicOr(a.fl0 + (t >> 5), 1u << (t & 31u));
+        }
     }
     if (gtid == 0) a.counts[0] = (unsigned long long)a.ns;
-    if (!grid_barrier(a.ctl, a.expected, a.wait_ns, 0)) return;
+    if (!grid_sync(a.ctl, a.expected, a.wait_ns, 0, epoch)) return;
     if (a.level_ns && gtid == 0) a.level_ns[0] = gtimer();
 
     // Per-level access modes.  Every block derives them from the same level
@@ -349,30 +492,68 @@ __global__ void __launch_bounds__(kBlock, min_blocks_for(D)) bfs_batch_kernel(co
     const unsigned long long pairs_ppm = pairs;  // compare x*1e6 >= pairs*ppm
     unsigned long long reached = (unsigned long long)a.ns;
     unsigned long long c_prev = (unsigned long long)a.ns;  // frontier size feeding the level
-    bool wrote_all_prev = true;                               // F0 is zeroed whole in phase 0
+    bool wrote_all_prev = false;
+    // The frontier of the previous level is in push buffer P[in_p] (-1: in F).
+    int in_p = push_on ? 0 : -1;
+    int dirty_p = -1;
+    bool nf_valid = false;        // a.nf describes V as the previous level left it
 
     for (int L = 1;; ++L) {
         const bool odd = (L & 1) != 0;
-        const uint4 *Fc = odd ? a.F0 : a.F1;
-        uint4 *Fn = odd ? a.F1 : a.F0;
-        const uint32_t *fc = odd ? a.fl0 : a.fl1;
-        uint32_t *fn = odd ? a.fl1 : a.fl0;
-        const bool write_all = c_prev * 1000000ull >= pairs_ppm * (unsigned long long)a.dense_w_ppm;
+        const bool push = in_p >= 0 &&
+                          c_prev * 1000000ull < pairs_ppm * (unsigned long long)a.push_ppm;
+        const bool write_all_c = c_prev * 1000000ull >= pairs_ppm * (unsigned long long)a.dense_w_ppm;
         const bool dense = wrote_all_prev &&
                            c_prev * 1000000ull >= pairs_ppm * (unsigned long long)a.dense_r_ppm;
         const bool skip_full = reached * 1000000ull >= pairs_ppm * (unsigned long long)a.full_skip_ppm;
+        // Skipping full tiles leaves their F' chunks unwritten, so F' is then
+        // written only where it is nonzero (the next level reads it by flags).
+        const bool nf_use = !push && skip_full && nf_valid;
+        const bool write_all = write_all_c && !nf_use;
         unsigned cnt = 0u, and_pre = 0xffffffffu, and_post = 0xffffffffu;
-        // Balanced contiguous tile range per block; the block's warps pull
-        // kGrab tiles at a time from it through a shared-memory counter.
-        if (threadIdx.x == 0) s_next = t_lo;
-        __syncthreads();
-        for (;;) {
-            unsigned tile0 = 0;
-            if (lane == 0) tile0 = atomicAdd(&s_next, (unsigned)kGrab);
-            tile0 = __shfl_sync(0xffffffffu, tile0, 0);
-            if (tile0 >= t_hi) break;
-            level_tiles<D, kGrab>(a, d, adj, v_base, tile0, t_hi, Fc, Fn, fc, fn, dense, write_all,
-                                  skip_full, lane, cnt, and_pre, and_post);
+        if (push) {
+            uint4 *Pc = in_p ? a.P1 : a.P0;
+            uint4 *Pn = in_p ? a.P0 : a.P1;
+            uint32_t *pfc = in_p ? a.pf1 : a.pf0;
+            uint32_t *pfn = in_p ? a.pf0 : a.pf1;
+            if constexpr (D > 0 && 32 % D == 0) cnt = push_level<D>(a, Pc, Pn, pfc, pfn, ntiles, gtid, nthr);
+        } else {
+            const uint4 *Fc = in_p >= 0 ? (in_p ? a.P1 : a.P0) : (odd ? a.F0 : a.F1);
+            const uint32_t *fc = in_p >= 0 ? (in_p ? a.pf1 : a.pf0) : (odd ? a.fl0 : a.fl1);
+            uint4 *Fn = odd ? a.F1 : a.F0;
+            uint32_t *fn = odd ? a.fl1 : a.fl0;
+            // Balanced contiguous tile range per block; the block's warps pull
+            // kGrab tiles at a time from it through a shared-memory counter.
+            if (threadIdx.x == 0) s_next = t_lo;
+            __syncthreads();
+            if (nf_use) {
+                // Skip-full stage: a warp takes 32 tiles, reads their not-full
+                // words in one load, clears the frontier flags of the full ones
+                // and works only on the others.
+                for (;;) {
+                    unsigned tile0 = 0;
+                    if (lane == 0) tile0 = atomicAdd(&s_next, 32u);
+                    tile0 = __shfl_sync(0xffffffffu, tile0, 0);
+                    if (tile0 >= t_hi) break;
+                    const unsigned my = tile0 + lane;
+                    const unsigned w = my < t_hi ? __ldcg(a.nf + my) : 0u;
+                    if (my < t_hi && w == 0u) fn[my] = 0u;
+                    for (unsigned todo = __ballot_sync(0xffffffffu, w != 0u); todo; todo &= todo - 1u) {
+                        const unsigned tj = tile0 + (unsigned)(__ffs((int)todo) - 1);
+                        level_tiles<D, 1>(a, d, adj, v_base, tj, t_hi, Fc, Fn, fc, fn, dense, write_all,
+                                          skip_full, lane, cnt, and_pre, and_post);
+                    }
+                }
+            } else {
+                for (;;) {
+                    unsigned tile0 = 0;
+                    if (lane == 0) tile0 = atomicAdd(&s_next, (unsigned)kGrab);
+                    tile0 = __shfl_sync(0xffffffffu, tile0, 0);
+                    if (tile0 >= t_hi) break;
+                    level_tiles<D, kGrab>(a, d, adj, v_base, tile0, t_hi, Fc, Fn, fc, fn, dense,
+                                          write_all, skip_full, lane, cnt, and_pre, and_post);
+                }
+            }
         }
 
         // Level reduction: one 64-bit atomic per block (cudaASPLconv.cu:59-99 fused).
@@ -395,12 +576,19 @@ __global__ void __launch_bounds__(kBlock, min_blocks_for(D)) bfs_batch_kernel(co
                 atomicAnd(a.masks + L, m1);
             }
         }
-        if (!grid_barrier(a.ctl, a.expected, a.wait_ns, L)) return;
+        if (!grid_sync(a.ctl, a.expected, a.wait_ns, L, epoch)) return;
         if (a.level_ns && gtid == 0) a.level_ns[L] = gtimer();
         const unsigned long long cL = ld_relaxed_u64(a.counts + L);
         reached += cL;
         c_prev = cL;
-        wrote_all_prev = write_all;
+        wrote_all_prev = !push && write_all;
+        nf_valid = a.nf != nullptr && !push && (skip_full || dense || a.masks != nullptr);
+        if (push) {
+            in_p ^= 1;            // the frontier is now in Pn; Pc was cleared by its readers
+        } else if (in_p >= 0) {
+            dirty_p = in_p;       // read by this pull level; cleared after the loop
+            in_p = -1;
+        }
         // Stop on an empty level, at the cap, or as soon as every pair is reached
         // (the next level is then empty by construction).
         if (cL == 0ull || L >= a.max_levels || reached == pairs) {
@@ -408,6 +596,10 @@ __global__ void __launch_bounds__(kBlock, min_blocks_for(D)) bfs_batch_kernel(co
             break;
         }
     }
+    // Nothing reads the push buffers any more: return the one still holding
+    // bits to all zero (the other was cleared by the push level that read it).
+    const int p = in_p >= 0 ? in_p : dirty_p;
+    if (p >= 0) clear_push_buffer(p ? a.P1 : a.P0, p ? a.pf1 : a.pf0, ntiles, gtid, nthr);
 }
 
 // Expansion of the calculator tables into the pull adjacency adj[rows][d].

@@ -224,6 +224,12 @@ class graph:
         g = cls(edges=[list(map(int, r)) for r in adj], N=len(adj), degree_max=adj.shape[1])
         return g
 
+    @classmethod
+    def from_pairs(cls, pairs):
+        """The graph load() makes from these "u v" lines, in order."""
+        pairs = np.asarray(pairs, dtype=np.int64).reshape(-1, 2)
+        return cls().load(f"{u} {v}" for u, v in pairs.tolist())
+
     def table(self, degree_max=None):
         """N x degree_max int32, padded with self-loops (cudaASPLgraph.cu:144-153)."""
         dm = self.degree_max if degree_max is None else degree_max
@@ -378,6 +384,84 @@ class box:
                     for e, tr in enumerate(self.edges[x][y][z][:degree]):
                         t[(x * self.My + y) * self.Mz + z, e] = tr
         return t
+
+
+# ----------------------------------------------------------------------------
+# Form -> plain graph converters (cppcode/piece2graph.cpp:84-103,
+# cppcode/box2graph.cpp:86-106): every vertex's lifted edges, each pair written
+# once as (min, max), sorted, duplicates dropped.
+# ----------------------------------------------------------------------------
+
+def _unique_pairs(a, b):
+    lo, hi = np.minimum(a, b), np.maximum(a, b)
+    if lo.size == 0:
+        return np.zeros((0, 2), dtype=np.int64)
+    return np.unique(np.stack([lo, hi], axis=1), axis=0)
+
+
+def part_pairs(p: part):
+    """Edge list of a cyclic lift: vertex v has edges v -> (v + diff) mod N for
+    the diffs of orbit row v mod M (cudaASPLconv.cu:35-48 applies the same rule)."""
+    a, b = [], []
+    for r, row in enumerate(p.edges):
+        if not row:
+            continue
+        v = np.arange(r, p.N, p.M, dtype=np.int64)
+        for e in row:
+            a.append(v)
+            b.append((v + e) % p.N)
+    if not a:
+        return _unique_pairs(np.zeros(0, np.int64), np.zeros(0, np.int64))
+    return _unique_pairs(np.concatenate(a), np.concatenate(b))
+
+
+def piece_pairs(p: piece):
+    """piece2graph: vertex x*Ny + y, neighbour ((x+dx) mod Nx)*Ny + (y+dy) mod Ny,
+    diffs of tile (x mod Mx, y mod My)."""
+    a, b = [], []
+    for tx in range(p.Mx):
+        for ty in range(p.My):
+            xs = np.arange(tx, p.Nx, p.Mx, dtype=np.int64)[:, None]
+            ys = np.arange(ty, p.Ny, p.My, dtype=np.int64)[None, :]
+            for dx, dy in p.edges[tx][ty]:
+                a.append((xs * p.Ny + ys).ravel())
+                b.append((((xs + dx) % p.Nx) * p.Ny + (ys + dy) % p.Ny).ravel())
+    if not a:
+        return _unique_pairs(np.zeros(0, np.int64), np.zeros(0, np.int64))
+    return _unique_pairs(np.concatenate(a), np.concatenate(b))
+
+
+def box_pairs(p: box):
+    """box2graph: vertex (x*Ny + y)*Nz + z (box.hpp xyz2id), neighbour at the
+    wrapped (x+dx, y+dy, z+dz), diffs of tile (x mod Mx, y mod My, z mod Mz)."""
+    a, b = [], []
+    for tx in range(p.Mx):
+        for ty in range(p.My):
+            for tz in range(p.Mz):
+                xs = np.arange(tx, p.Nx, p.Mx, dtype=np.int64)[:, None, None]
+                ys = np.arange(ty, p.Ny, p.My, dtype=np.int64)[None, :, None]
+                zs = np.arange(tz, p.Nz, p.Mz, dtype=np.int64)[None, None, :]
+                for dx, dy, dz in p.edges[tx][ty][tz]:
+                    a.append(((xs * p.Ny + ys) * p.Nz + zs).ravel())
+                    b.append(((((xs + dx) % p.Nx) * p.Ny + (ys + dy) % p.Ny) * p.Nz
+                              + (zs + dz) % p.Nz).ravel())
+    if not a:
+        return _unique_pairs(np.zeros(0, np.int64), np.zeros(0, np.int64))
+    return _unique_pairs(np.concatenate(a), np.concatenate(b))
+
+
+def to_graph(p):
+    """Any form as the plain graph its edge list loads into."""
+    if isinstance(p, graph):
+        return p
+    fn = {part: part_pairs, piece: piece_pairs, box: box_pairs}[type(p)]
+    return graph.from_pairs(fn(p))
+
+
+def write_pairs(pairs, ost):
+    """"a b" lines, as piece2graph/box2graph print them."""
+    for a, b in np.asarray(pairs).tolist():
+        ost.write(f"{a} {b}\n")
 
 
 # ----------------------------------------------------------------------------

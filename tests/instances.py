@@ -149,3 +149,50 @@ def disjoint_union(adj_a, adj_b):
 
 def all_subsets(n):
     return itertools.chain.from_iterable(itertools.combinations(range(n), k) for k in range(n + 1))
+
+
+def random_nonregular(n, dmax, seed, extra=1.5):
+    """Connected simple graph with degrees in [1, dmax] (a random spanning tree
+    plus random extra edges), padded to [n, dmax] with self-loops as the
+    reference pads missing edges (cudaASPLgraph.cu:149-151)."""
+    rng = np.random.default_rng(seed)
+    lists = [[] for _ in range(n)]
+    order = rng.permutation(n)
+    for i in range(1, n):
+        v = int(order[i])
+        for _ in range(64):
+            u = int(order[rng.integers(0, i)])
+            if len(lists[u]) < dmax:
+                break
+        else:
+            u = next(int(order[j]) for j in range(i) if len(lists[int(order[j])]) < dmax)
+        lists[u].append(v)
+        lists[v].append(u)
+    for _ in range(int(extra * n)):
+        a, b = (int(x) for x in rng.integers(0, n, size=2))
+        if a != b and b not in lists[a] and len(lists[a]) < dmax and len(lists[b]) < dmax:
+            lists[a].append(b)
+            lists[b].append(a)
+    t = np.repeat(np.arange(n, dtype=np.int32)[:, None], dmax, axis=1)
+    for v, l in enumerate(lists):
+        t[v, :len(l)] = l
+    return t, lists
+
+
+def ragged_part(m, g, d, drop, seed):
+    """A cyclic lift whose orbit rows have different lengths: random_part with
+    `drop` orbit edges removed (both ends), rows padded with diff 0."""
+    N, M, rows = random_part(m, g, d, seed)
+    rows = [list(map(int, r)) for r in rows]
+    rng = np.random.default_rng(seed + 7)
+    for _ in range(drop):
+        a = int(rng.integers(0, m))
+        if not rows[a]:
+            continue
+        diff = rows[a].pop(int(rng.integers(0, len(rows[a]))))
+        b = (a + diff) % m
+        rows[b].remove(-diff)
+    t = np.zeros((m, d), dtype=np.int32)
+    for i, r in enumerate(rows):
+        t[i, :len(r)] = r
+    return N, M, t, rows

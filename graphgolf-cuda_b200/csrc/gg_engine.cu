@@ -103,7 +103,7 @@ struct gg_engine {
     // device
     cudaStream_t stream = nullptr;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
-    int32_t *d_table = nullptr, *d_adj = nullptr, *d_src = nullptr;
+    int32_t *d_table = nullptr, *d_adj = nullptr;
     int *d_bad = nullptr;
     int *d_asym = nullptr;               // adjacency not symmetric: no push levels
     uint4 *d_V = nullptr, *d_F0 = nullptr, *d_F1 = nullptr;
@@ -115,6 +115,10 @@ struct gg_engine {
     unsigned long long *d_counts = nullptr;
     unsigned *d_masks = nullptr;
     unsigned long long *d_level_ns = nullptr, *h_level_ns = nullptr;
+    int *d_levels_run = nullptr, *h_levels_run = nullptr;                 // [nb_alloc]
+    unsigned long long *d_batch_ns = nullptr, *h_batch_ns = nullptr;     // [2 * nb_alloc]
+    int32_t *d_inv = nullptr;            // source index of each vertex, when the sources
+    int src_first = 0;                   // are not the consecutive ids src_first, src_first+1, ...
     Ctl *d_ctl = nullptr;
     // pinned host
     int32_t *h_table = nullptr;
@@ -125,6 +129,7 @@ struct gg_engine {
 
     double last_ms = 0.0;
     int last_launches = 0;
+    int last_batches = 0;                // batches of the last evaluation
     uint64_t last_h2d = 0, last_d2h = 0;
 };
 
@@ -146,6 +151,10 @@ void free_counters(gg_engine *e) {
     cudaFree(e->d_counts); cudaFree(e->d_masks); cudaFree(e->d_ctl); cudaFree(e->d_level_ns);
     cudaFreeHost(e->h_counts); cudaFreeHost(e->h_masks); cudaFreeHost(e->h_ctl);
     cudaFreeHost(e->h_level_ns);
+    cudaFree(e->d_levels_run); cudaFreeHost(e->h_levels_run);
+    cudaFree(e->d_batch_ns); cudaFreeHost(e->h_batch_ns);
+    e->d_levels_run = e->h_levels_run = nullptr;
+    e->d_batch_ns = e->h_batch_ns = nullptr;
     e->d_counts = nullptr; e->d_masks = nullptr; e->d_ctl = nullptr; e->d_level_ns = nullptr;
     e->h_counts = nullptr; e->h_masks = nullptr; e->h_ctl = nullptr; e->h_level_ns = nullptr;
     e->cap_alloc = e->nb_alloc = 0;
@@ -158,7 +167,7 @@ void destroy_all(gg_engine *e) {
     free_batch_buffers(e);
     free_counters(e);
     if (e->d_adj != e->d_table) cudaFree(e->d_adj);  // the graph form aliases the two
-    cudaFree(e->d_table); cudaFree(e->d_src); cudaFree(e->d_bad); cudaFree(e->d_asym);
+    cudaFree(e->d_table); cudaFree(e->d_inv); cudaFree(e->d_bad); cudaFree(e->d_asym);
     cudaFreeHost(e->h_table); cudaFreeHost(e->h_bad);
     if (e->ev0) cudaEventDestroy(e->ev0);
     if (e->ev1) cudaEventDestroy(e->ev1);
@@ -293,10 +302,14 @@ gg_status ensure_counters(gg_engine *e, int cap, int nb) {
     const size_t n = (size_t)(cap + 1) * nb;
     GG_CK(cudaMalloc(&e->d_counts, n * sizeof(unsigned long long)));
     GG_CK(cudaMalloc(&e->d_masks, n * sizeof(unsigned)));
-    GG_CK(cudaMalloc(&e->d_ctl, (size_t)nb * sizeof(Ctl)));
+    GG_CK(cudaMalloc(&e->d_ctl, sizeof(Ctl)));
     GG_CK(cudaMallocHost(&e->h_counts, n * sizeof(unsigned long long)));
     GG_CK(cudaMallocHost(&e->h_masks, n * sizeof(unsigned)));
-    GG_CK(cudaMallocHost(&e->h_ctl, (size_t)nb * sizeof(Ctl)));
+    GG_CK(cudaMallocHost(&e->h_ctl, sizeof(Ctl)));
+    GG_CK(cudaMalloc(&e->d_levels_run, (size_t)nb * sizeof(int)));
+    GG_CK(cudaMallocHost(&e->h_levels_run, (size_t)nb * sizeof(int)));
+    GG_CK(cudaMalloc(&e->d_batch_ns, (size_t)nb * 2 * sizeof(unsigned long long)));
+    GG_CK(cudaMallocHost(&e->h_batch_ns, (size_t)nb * 2 * sizeof(unsigned long long)));
     GG_CK(cudaMalloc(&e->d_level_ns, (size_t)(cap + 1) * sizeof(unsigned long long)));
     GG_CK(cudaMallocHost(&e->h_level_ns, (size_t)(cap + 1) * sizeof(unsigned long long)));
     e->cap_alloc = cap;
@@ -324,9 +337,23 @@ gg_status create_common(gg_engine *e) {
     } else {
         GG_CK(cudaMalloc(&e->d_adj, std::max<size_t>((size_t)e->rows * e->d, 1) * sizeof(int32_t)));
     }
-    GG_CK(cudaMalloc(&e->d_src, std::max<size_t>(e->reps.size(), 1) * sizeof(int32_t)));
-    GG_CK(cudaMemcpy(e->d_src, e->reps.data(), e->reps.size() * sizeof(int32_t),
-                     cudaMemcpyHostToDevice));
+    // The kernel finds a chunk's source from its vertex: directly when the
+    // sources are consecutive vertex ids, else through the inverse list.
+    bool consecutive = true;
+    for (size_t i = 0; i < e->reps.size() && consecutive; ++i)
+        consecutive = e->reps[i] == e->reps[0] + (int32_t)i;
+    e->src_first = e->reps.empty() ? 0 : e->reps[0];
+    if (!consecutive) {
+        std::vector<int32_t> inv((size_t)std::max(e->rows, 1), -1);
+        for (size_t i = 0; i < e->reps.size(); ++i) {
+            const int32_t v = e->reps[i];
+            if (v < 0 || v >= e->rows || inv[(size_t)v] != -1)
+                return fail(GG_BAD_ARG, "sources must be distinct vertices");
+            inv[(size_t)v] = (int32_t)i;
+        }
+        GG_CK(cudaMalloc(&e->d_inv, inv.size() * sizeof(int32_t)));
+        GG_CK(cudaMemcpy(e->d_inv, inv.data(), inv.size() * sizeof(int32_t), cudaMemcpyHostToDevice));
+    }
     GG_CK(cudaMalloc(&e->d_bad, sizeof(int)));
     GG_CK(cudaMalloc(&e->d_asym, sizeof(int)));
     GG_CK(cudaMallocHost(&e->h_bad, sizeof(int)));
@@ -405,7 +432,7 @@ gg_status run_eval(gg_engine *e, const int32_t *d_table_in, const gg_eval_opts *
             ++launches;
         }
     }
-    GG_CK(cudaMemsetAsync(e->d_ctl, 0, (size_t)nb * sizeof(Ctl), st));
+    GG_CK(cudaMemsetAsync(e->d_ctl, 0, sizeof(Ctl), st));
     GG_CK(cudaMemsetAsync(e->d_asym, 0, sizeof(int), st));
     if (e->p_dirty) {
         // New buffers, or a launch that stopped early: the push buffers are
@@ -420,41 +447,45 @@ gg_status run_eval(gg_engine *e, const int32_t *d_table_in, const gg_eval_opts *
     if (want_ns)
         GG_CK(cudaMemsetAsync(e->d_level_ns, 0, (size_t)(cap_req + 1) * sizeof(unsigned long long), st));
 
+    // One cooperative launch runs every source batch of the evaluation.
     void *kern = kernel_for(e->d);
     if (fault("launch")) return fail(GG_CUDA_ERROR, "injected launch failure");
     const unsigned extra = fault("barrier") ? 1u : 0u;
-    e->p_dirty = true;  // until the launches are known to have finished cleanly
-    for (int b = 0; b < nb; ++b) {
-        BfsArgs a{};
-        a.adj = e->d_adj;
-        a.src = e->d_src + s0 + (size_t)b * e->batch_bits;
-        a.ns = std::min(e->batch_bits, ns_all - b * e->batch_bits);
-        a.V = e->d_V; a.F0 = e->d_F0; a.F1 = e->d_F1;
-        a.fl0 = e->d_fl0; a.fl1 = e->d_fl1;
-        a.P0 = e->d_P0; a.P1 = e->d_P1; a.pf0 = e->d_pf0; a.pf1 = e->d_pf1;
-        // Below ~1M chunks a pull level costs about one grid barrier anyway.
-        a.push_ppm = (long long)e->items >= (long long)e->push_min_items ? e->push_ppm : 0;
-        a.nf = e->d_nf;
-        a.asym = e->d_asym;
-        a.sym_check = b == 0;
-        a.counts = e->d_counts + (size_t)b * stride;
-        a.masks = wvc ? e->d_masks + (size_t)b * stride : nullptr;
-        a.level_ns = (b == 0 && want_ns) ? e->d_level_ns : nullptr;
-        a.ctl = e->d_ctl + b;
-        a.rows = e->rows; a.d = e->d; a.nC = e->nC; a.items = e->items;
-        a.div_nc = FastDiv((uint32_t)e->nC);
-        a.max_levels = cap_req;
-        a.dense_w_ppm = e->dense_w_ppm;
-        a.dense_r_ppm = e->dense_r_ppm;
-        a.full_skip_ppm = e->full_skip_ppm;
-        a.adj_smem_rows = e->adj_smem_rows;
-        a.wait_ns = e->wait_ns;
-        a.expected = (unsigned)e->grid + extra;
-        a.bad = e->form == FORM_GRAPH ? e->d_bad : nullptr;
-        void *args[] = {&a};
-        GG_CK(cudaLaunchCooperativeKernel(kern, dim3(e->grid), dim3(gg::kBlock), args, e->smem_bytes, st));
-        ++launches;
-    }
+    e->p_dirty = true;  // until the launch is known to have finished cleanly
+    BfsArgs a{};
+    a.adj = e->d_adj;
+    a.inv = e->d_inv;
+    a.src_first = e->src_first;
+    a.src_begin = s0;
+    a.ns_total = ns_all;
+    a.nb = nb;
+    a.V = e->d_V; a.F0 = e->d_F0; a.F1 = e->d_F1;
+    a.fl0 = e->d_fl0; a.fl1 = e->d_fl1;
+    a.P0 = e->d_P0; a.P1 = e->d_P1; a.pf0 = e->d_pf0; a.pf1 = e->d_pf1;
+    // Below ~1M chunks a pull level costs about one grid barrier anyway.
+    a.push_ppm = (long long)e->items >= (long long)e->push_min_items ? e->push_ppm : 0;
+    a.nf = e->d_nf;
+    a.asym = e->d_asym;
+    a.counts = e->d_counts;
+    a.masks = wvc ? e->d_masks : nullptr;
+    a.stride = stride;
+    a.levels_run = e->d_levels_run;
+    a.level_ns = want_ns ? e->d_level_ns : nullptr;
+    a.batch_ns = e->d_batch_ns;
+    a.ctl = e->d_ctl;
+    a.rows = e->rows; a.d = e->d; a.nC = e->nC; a.items = e->items;
+    a.div_nc = FastDiv((uint32_t)e->nC);
+    a.max_levels = cap_req;
+    a.dense_w_ppm = e->dense_w_ppm;
+    a.dense_r_ppm = e->dense_r_ppm;
+    a.full_skip_ppm = e->full_skip_ppm;
+    a.adj_smem_rows = e->adj_smem_rows;
+    a.wait_ns = e->wait_ns;
+    a.expected = (unsigned)e->grid + extra;
+    a.bad = e->form == FORM_GRAPH ? e->d_bad : nullptr;
+    void *args[] = {&a};
+    GG_CK(cudaLaunchCooperativeKernel(kern, dim3(e->grid), dim3(gg::kBlock), args, e->smem_bytes, st));
+    ++launches;
     GG_CK(cudaEventRecord(e->ev1, st));
     // Read back only the levels that can hold counts (cap_req + 1 per batch).
     uint64_t d2h = 0;
@@ -469,8 +500,11 @@ gg_status run_eval(gg_engine *e, const int32_t *d_table_in, const gg_eval_opts *
                                 cudaMemcpyDeviceToHost, st));
         d2h += lv * nb * sizeof(unsigned);
     }
-    GG_CK(cudaMemcpyAsync(e->h_ctl, e->d_ctl, (size_t)nb * sizeof(Ctl), cudaMemcpyDeviceToHost, st));
-    d2h += (size_t)nb * sizeof(Ctl);
+    GG_CK(cudaMemcpyAsync(e->h_ctl, e->d_ctl, sizeof(Ctl), cudaMemcpyDeviceToHost, st));
+    GG_CK(cudaMemcpyAsync(e->h_levels_run, e->d_levels_run, (size_t)nb * sizeof(int), cudaMemcpyDeviceToHost, st));
+    GG_CK(cudaMemcpyAsync(e->h_batch_ns, e->d_batch_ns, (size_t)nb * 2 * sizeof(unsigned long long),
+                          cudaMemcpyDeviceToHost, st));
+    d2h += sizeof(Ctl) + (size_t)nb * (sizeof(int) + 2 * sizeof(unsigned long long));
     if (e->form == FORM_GRAPH) {
         GG_CK(cudaMemcpyAsync(e->h_bad, e->d_bad, sizeof(int), cudaMemcpyDeviceToHost, st));
         d2h += sizeof(int);
@@ -486,14 +520,13 @@ gg_status run_eval(gg_engine *e, const int32_t *d_table_in, const gg_eval_opts *
     GG_CK(cudaEventElapsedTime(&ms, e->ev0, e->ev1));
     e->last_ms = ms;
     e->last_launches = launches;
+    e->last_batches = nb;
 
     if (e->form == FORM_GRAPH && *e->h_bad)
         return fail(GG_BAD_ARG, "adjacency entry outside [0, N)");
-    for (int b = 0; b < nb; ++b)
-        if (e->h_ctl[b].err) {
-            return fail(GG_TIMEOUT, "grid barrier wait exceeded its limit at level " +
-                                        std::to_string(e->h_ctl[b].err_level));
-        }
+    if (e->h_ctl->err)
+        return fail(GG_TIMEOUT, "grid barrier wait exceeded its limit at level " +
+                                    std::to_string(e->h_ctl->err_level));
     e->p_dirty = false;
 
     // Exact fold of the per-batch level counters.
@@ -507,7 +540,7 @@ gg_status run_eval(gg_engine *e, const int32_t *d_table_in, const gg_eval_opts *
     std::vector<unsigned long long> agg(cap_req + 1, 0ull);
     for (int b = 0; b < nb; ++b) {
         const unsigned long long *c = e->h_counts + (size_t)b * stride;
-        const int run = e->h_ctl[b].levels_run;
+        const int run = e->h_levels_run[b];
         int last = 0;
         for (int L = 0; L <= run && L <= cap_req; ++L) {
             R.reached += c[L];
@@ -712,6 +745,15 @@ gg_status gg_last_transfer_bytes(gg_engine *e, uint64_t *h2d, uint64_t *d2h) {
 gg_status gg_last_device_ms(gg_engine *e, double *ms) {
     if (!e || !ms) return fail(GG_BAD_ARG, "null argument");
     *ms = e->last_ms;
+    return GG_OK;
+}
+
+gg_status gg_last_batch_ns(gg_engine *e, uint64_t *ns, int n) {
+    if (!e || !ns || n < 0) return fail(GG_BAD_ARG, "bad arguments");
+    for (int b = 0; b < n && b < e->last_batches; ++b) {
+        ns[2 * b] = e->h_batch_ns[2 * b];
+        ns[2 * b + 1] = e->h_batch_ns[2 * b + 1];
+    }
     return GG_OK;
 }
 

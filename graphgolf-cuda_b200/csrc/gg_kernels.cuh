@@ -17,6 +17,7 @@
 // The whole level loop runs inside one cooperative launch; levels are separated
 // by a grid barrier whose waits are bounded (globaltimer) and report GG_TIMEOUT.
 #pragma once
+#include <cstddef>
 #include <cstdint>
 #include <cuda_runtime.h>
 
@@ -54,26 +55,35 @@ struct Ctl {
     unsigned int arrive;      // grid-barrier arrivals, counted over the whole launch
     int err;                  // 0, or 1 = a barrier wait exceeded the limit
     int err_level;            // level at which the first wait gave up
-    int levels_run;           // last level executed
+    int levels_run;           // last level executed (single-batch callers)
     int pad0[28];
     unsigned int passed;      // grid barriers completed so far
     int pad1[31];
 };
+static_assert(offsetof(Ctl, passed) == 128 && sizeof(Ctl) == 256, "one 128-byte line each");
 
 struct BfsArgs {
     const int32_t *adj;       // [rows][d] pull adjacency
-    const int32_t *src;       // batch sources: vertex id of source i, i < ns
+    // Sources.  The evaluation's sources are entries [src_begin, src_begin +
+    // ns_total) of a source list; batch b holds the next 128 * nC of them.
+    // inv[v] = index of vertex v in the list (-1: not a source); inv nullptr:
+    // entry i of the list is vertex src_first + i.
+    const int32_t *inv;
+    int src_first, src_begin, ns_total, nb;
     uint4 *V, *F0, *F1;
     uint32_t *fl0, *fl1;
-    unsigned long long *counts;   // [max_levels + 1]
-    unsigned int *masks;          // [max_levels + 1] or nullptr
-    unsigned long long *level_ns; // [max_levels + 1] or nullptr: globaltimer at each level end
+    unsigned long long *counts;   // [nb][stride]: pairs first reached at level L of batch b
+    unsigned int *masks;          // [nb][stride] or nullptr (WVC)
+    int stride;
+    int *levels_run;              // [nb]: last level executed in batch b
+    unsigned long long *level_ns; // [max_levels + 1] or nullptr: globaltimer at each level end (batch 0)
+    unsigned long long *batch_ns; // [2 * nb] or nullptr: globaltimer at each batch's start and end
     Ctl *ctl;
     const int *bad;           // nonzero: the table failed its range check; do nothing
     unsigned int expected;    // blocks the barrier waits for (the grid size)
     FastDiv div_nc;           // division by nC
     uint32_t items;           // rows * nC
-    int rows, d, nC, ns;
+    int rows, d, nC;
     int max_levels;
     int dense_w_ppm;          // write F whole when the feeding frontier >= ppm of the pairs
     int dense_r_ppm;          // read F without flags when it was written whole and >= ppm
@@ -89,11 +99,10 @@ struct BfsArgs {
     uint32_t *pf0, *pf1;
     int push_ppm;             // push while the feeding frontier < ppm of the pairs
     // A push level equals the reference's pull level only when the adjacency is
-    // symmetric (u in adj[w] <=> w in adj[u]).  With sym_check set, phase 0
-    // tests that and stores 1 into *asym on any one-way entry; launches after
-    // the first of an evaluation read the stored answer.  asym nullptr: no push.
+    // symmetric (u in adj[w] <=> w in adj[u]); the launch tests that first and
+    // stores 1 into *asym (zeroed by the host) on any one-way entry.  nullptr:
+    // no push levels.
     int *asym;
-    int sym_check;
     // [ceil(rows * nC / 32)] bit per uint4 of V: set iff that chunk is not yet
     // full.  Written by levels that load every visited chunk; a later level in
     // the skip-full stage passes over tiles whose word is 0.  nullptr: unused.
@@ -293,38 +302,26 @@ __device__ __forceinline__ unsigned comp_of(const uint4 &f, const int k) {
     return k == 0 ? f.x : (k == 1 ? f.y : (k == 2 ? f.z : f.w));
 }
 
-// Push item (u, c) with frontier chunk f to the neighbours tw[i] = (w_i, c).
-// The visited words are ORed first, all of them in flight together (nothing
-// waits on a returned value before the last one is issued); the bits that were
-// not visited yet -- exact under concurrency, atomicOr returns the old word --
-// are this level's new pairs and go into Pn and the flag words with
-// fire-and-forget reductions.
-template <int D>
-__device__ __forceinline__ void push_item(const BfsArgs &a, const uint4 f, const unsigned *tw,
-                                          uint4 *Pn, uint32_t *pfn, unsigned &cnt) {
-    unsigned any[D];
-#pragma unroll
-    for (int i = 0; i < D; ++i) any[i] = 0u;
+// Push item (u, c) with frontier chunk f to the neighbour chunk tw = (w, c).
+// The visited words are ORed first (all four in flight before any returned value
+// is used); the bits that were not visited yet -- exact under concurrency,
+// atomicOr returns the old word -- are this level's new pairs and go into Pn and
+// the flag words with fire-and-forget reductions.
+__device__ __forceinline__ void push_item(uint4 *V, const uint4 f, const unsigned tw, uint4 *Pn,
+                                          uint32_t *pfn, unsigned &cnt) {
+    unsigned any = 0u;
 #pragma unroll
     for (int k = 0; k < 4; ++k) {
         const unsigned fk = comp_of(f, k);
         if (!fk) continue;
-        unsigned old[D];
-#pragma unroll
-        for (int i = 0; i < D; ++i) old[i] = atomicOr(reinterpret_cast<unsigned *>(a.V + tw[i]) + k, fk);
-#pragma unroll
-        for (int i = 0; i < D; ++i) {
-            const unsigned nb = fk & ~old[i];
-            if (nb) {
-                atomicOr(reinterpret_cast<unsigned *>(Pn + tw[i]) + k, nb);
-                cnt += __popc(nb);
-                any[i] = 1u;
-            }
+        const unsigned nb = fk & ~atomicOr(reinterpret_cast<unsigned *>(V + tw) + k, fk);
+        if (nb) {
+            atomicOr(reinterpret_cast<unsigned *>(Pn + tw) + k, nb);
+            cnt += __popc(nb);
+            any = 1u;
         }
     }
-#pragma unroll
-    for (int i = 0; i < D; ++i)
-        if (any[i]) atomicOr(pfn + (tw[i] >> 5), 1u << (tw[i] & 31u));
+    if (any) atomicOr(pfn + (tw >> 5), 1u << (tw & 31u));
 }
 
 // One push level.  The frontier of level L-1 is the set bits of the flag words
@@ -336,14 +333,16 @@ __device__ __forceinline__ void push_item(const BfsArgs &a, const uint4 f, const
 // item, and the D pushes of an item run in parallel.  After the group's lanes
 // have read them, lane 0 zeroes the items and the flag word, so Pc is all zero
 // again when the level ends.  Work is proportional to the frontier, not to
-// rows * nC.  Needs D to divide 32 (a group never straddles two warps).
+// rows * nC.  Needs D to divide 32 (a group never straddles two warps).  Kept
+// out of line: it runs a few times per batch, and inlined it would take
+// registers from the pull levels.
 template <int D>
-__device__ __forceinline__ unsigned push_level(const BfsArgs &a, uint4 *Pc, uint4 *Pn, uint32_t *pfc,
-                                               uint32_t *pfn, const unsigned fwords,
-                                               const unsigned gtid, const unsigned nthr) {
+static __device__ __noinline__ unsigned push_level(const int32_t *adj, uint4 *V, const FastDiv div_nc,
+                                            const unsigned nC, uint4 *Pc, uint4 *Pn, uint32_t *pfc,
+                                            uint32_t *pfn, const unsigned fwords, const unsigned gtid,
+                                            const unsigned nthr) {
     static_assert(D > 0 && 32 % D == 0, "push levels need D | 32");
     unsigned cnt = 0u;
-    const unsigned nC = (unsigned)a.nC;
     const unsigned lane = threadIdx.x & 31u;
     const unsigned i = lane % (unsigned)D;
     const unsigned long long total = (unsigned long long)fwords * D;
@@ -356,11 +355,11 @@ __device__ __forceinline__ unsigned push_level(const BfsArgs &a, uint4 *Pc, uint
             const unsigned b = (unsigned)(__ffs((int)m) - 1);
             m &= m - 1u;
             const unsigned t = k * 32u + b;
-            const unsigned u = a.div_nc.div(t);
+            const unsigned u = div_nc.div(t);
             const unsigned c = t - u * nC;
             const uint4 f = __ldcg(Pc + t);
-            const unsigned tw = (unsigned)__ldg(a.adj + (size_t)u * D + i) * nC + c;
-            push_item<1>(a, f, &tw, Pn, pfn, cnt);
+            const unsigned tw = (unsigned)__ldg(adj + (size_t)u * D + i) * nC + c;
+            push_item(V, f, tw, Pn, pfn, cnt);
         }
         __syncwarp();
         if (i == 0u && m0) {
@@ -372,9 +371,9 @@ __device__ __forceinline__ unsigned push_level(const BfsArgs &a, uint4 *Pc, uint
 }
 
 // Zero the items flagged in `pf` and the flag words themselves (the push buffer
-// a pull level read last), restoring the all-zero state the next launch expects.
-__device__ __forceinline__ void clear_push_buffer(uint4 *P, uint32_t *pf, const unsigned fwords,
-                                                  const unsigned gtid, const unsigned nthr) {
+// a pull level read last), restoring the all-zero state the next batch expects.
+static __device__ __noinline__ void clear_push_buffer(uint4 *P, uint32_t *pf, const unsigned fwords,
+                                               const unsigned gtid, const unsigned nthr) {
     for (unsigned k = gtid; k < fwords; k += nthr) {
         unsigned m = __ldcg(pf + k);
         if (!m) continue;
@@ -387,11 +386,73 @@ __device__ __forceinline__ void clear_push_buffer(uint4 *P, uint32_t *pf, const 
     }
 }
 
+// Phase 0 of batch b: every visited chunk rewritten with its padding bits and
+// the diagonal, the diagonal stored as the level-1 frontier (push buffer P_diag
+// or F0) with its flag words.  The sources of a batch are distinct vertices, so a
+// chunk holds at most one of them.  One warp per tile of 32 chunks.  Out of line
+// for the same reason as push_level.
+static __device__ __noinline__ void phase0_tiles(const int32_t *inv, const int src_first, const int first,
+                                          const int ns, uint4 *V, uint4 *F0, uint32_t *fl0,
+                                          uint4 *P_diag, uint32_t *pf_diag, const FastDiv div_nc,
+                                          const unsigned nC, const unsigned items, const bool push_on,
+                                          const unsigned gtid, const unsigned nthr) {
+    const unsigned lane = threadIdx.x & 31u;
+    const unsigned ntiles = (items + 31u) >> 5;
+    for (unsigned tile = gtid >> 5; tile < ntiles; tile += nthr >> 5) {
+        const unsigned t = tile * 32u + lane;
+        const bool ok = t < items;
+        const unsigned v = ok ? div_nc.div(t) : 0u;
+        const unsigned c = t - v * nC;
+        const int g = ok ? (inv ? __ldg(inv + v) : (int)v - src_first) : -1;
+        const int j = g - first;
+        const bool has = ok && g >= 0 && j >= 0 && j < ns && (unsigned)(j >> 7) == c;
+        uint4 one = u4zero();
+        if (has) {
+            const unsigned bit = 1u << (j & 31), comp = ((unsigned)j >> 5) & 3u;
+            if (comp == 0u) one.x = bit; else if (comp == 1u) one.y = bit; else if (comp == 2u) one.z = bit; else one.w = bit;
+        }
+        if (ok) V[t] = u4or(pad_mask((int)c, ns), one);
+        const unsigned fb = __ballot_sync(0xffffffffu, has);
+        if (push_on) {
+            if (has) P_diag[t] = one;
+            if (lane == 0 && fb) pf_diag[tile] = fb;
+        } else {
+            if (has) F0[t] = one;
+            if (lane == 0) fl0[tile] = fb;
+        }
+    }
+}
+
 // Resident blocks per SM the register allocation targets: 6 (40 registers)
 // fits the small degrees without spills, 4 (64 registers) the larger ones.
-__host__ __device__ constexpr int min_blocks_for(int D) { return (D > 0 && D <= 8) ? 6 : 4; }
+#ifndef GG_MIN_BLOCKS_SMALL_D
+#define GG_MIN_BLOCKS_SMALL_D 6
+#endif
+__host__ __device__ constexpr int min_blocks_for(int D) {
+    return (D > 0 && D <= 8) ? GG_MIN_BLOCKS_SMALL_D : 4;
+}
 
-// One cooperative launch = one source batch, all levels.
+// Block-uniform state of the batch and level loops.  It lives in shared memory
+// (thread 0 updates it between barriers) so that the level work keeps its
+// registers.
+struct LoopState {
+    unsigned long long reached;  // pairs reached so far in the batch
+    unsigned long long c_prev;   // pairs first reached at the previous level
+    unsigned long long pairs;    // sources x rows of the batch
+    int push_on;                 // push levels allowed in this launch
+    int in_p;                    // push buffer holding the previous level's frontier, or -1
+    int dirty_p;                 // push buffer still to be cleared, or -1
+    int wrote_all_prev;          // the previous level wrote F whole
+    int nf_valid;                // a.nf describes V as the previous level left it
+    int done;                    // the batch's level loop ends
+};
+
+// One cooperative launch = every source batch of an evaluation, all levels.
+//
+// Per batch: phase 0 (one pass over the chunks: visited bits reset, padding and
+// the diagonal set, level-1 frontier and its flags written) -> grid barrier ->
+// levels, each ended by a grid barrier.  One launch instead of one per batch
+// saves the launch gap and the shared-memory adjacency reload per batch.
 template <int D>
 __global__ void __launch_bounds__(kBlock, min_blocks_for(D)) bfs_batch_kernel(const BfsArgs a) {
     const int d = D > 0 ? D : a.d;
@@ -402,6 +463,7 @@ __global__ void __launch_bounds__(kBlock, min_blocks_for(D)) bfs_batch_kernel(co
     __shared__ unsigned long long s_sum[kBlock / 32];
     __shared__ unsigned s_and[2][kBlock / 32];
     __shared__ unsigned s_next;
+    __shared__ LoopState S;
     if (a.bad && *a.bad) return;  // uniform across the grid: no block reaches a barrier
     unsigned epoch = 0u;          // grid barriers passed
     const unsigned t_lo = (unsigned)((unsigned long long)ntiles * blockIdx.x / gridDim.x);
@@ -424,15 +486,17 @@ __global__ void __launch_bounds__(kBlock, min_blocks_for(D)) bfs_batch_kernel(co
             adj = s_adj;
             v_base = v_lo;
         }
-        __syncthreads();
     }
-
     // Push levels need the all-zero push buffers, a symmetric adjacency and
     // plain OR rows (the WVC masks are taken over every chunk, which only pull
     // levels visit).
-    const bool push_req = D > 0 && 32 % D == 0 && a.push_ppm > 0 && a.P0 != nullptr &&
-                          a.asym != nullptr && a.masks == nullptr;
-    if (push_req && a.sym_check) {
+    if (threadIdx.x == 0) {
+        S.push_on = D > 0 && 32 % D == 0 && a.push_ppm > 0 && a.P0 != nullptr && a.asym != nullptr &&
+                    a.masks == nullptr;
+        S.dirty_p = -1;
+    }
+    __syncthreads();
+    if (S.push_on) {
         const unsigned long long n = (unsigned long long)a.rows * (unsigned long long)d;
         for (unsigned long long k = gtid; k < n; k += nthr) {
             const unsigned v = (unsigned)(k / (unsigned)d);
@@ -441,165 +505,171 @@ __global__ void __launch_bounds__(kBlock, min_blocks_for(D)) bfs_batch_kernel(co
             for (int j = 0; j < d; ++j) found |= (unsigned)__ldg(row + j) == v;
             if (!found) *a.asym = 1;
         }
+        if (!grid_sync(a.ctl, a.expected, a.wait_ns, 0, epoch)) return;
+        if (threadIdx.x == 0) S.push_on = ld_acquire_i(a.asym) == 0;
+        __syncthreads();
     }
 
-    // Phase 0: per-batch reset (cudaASPLconv.cu:9-33): padding bits visited,
-    // flags cleared, counters zeroed.  F0 itself is not cleared: a reader only
-    // touches the chunks whose flag bit is set, and phase 1 stores those whole.
-    if (blockIdx.x == 0)
-        for (int i = threadIdx.x; i <= a.max_levels; i += blockDim.x) {
-            a.counts[i] = 0ull;
-            if (a.masks) a.masks[i] = 0xffffffffu;
-        }
-    for (unsigned t = gtid; t < items; t += nthr) {
-        const unsigned c = t - a.div_nc.div(t) * (unsigned)a.nC;
-        a.V[t] = pad_mask((int)c, a.ns);
-    }
-    for (unsigned w = gtid; w < ntiles; w += nthr) a.fl0[w] = 0u;
-    if (!grid_sync(a.ctl, a.expected, a.wait_ns, 0, epoch)) return;
-    const bool push_on = push_req && ld_acquire_i(a.asym) == 0;
-
-    // Phase 1: the diagonal -- source i has reached its own vertex at level 0.
-    // The sources of a batch are distinct vertices, so each chunk holds at most
-    // one of them and is stored whole.
-    for (unsigned i = gtid; i < (unsigned)a.ns; i += nthr) {
-        const unsigned t = (unsigned)a.src[i] * (unsigned)a.nC + (i >> 7);
-        const unsigned bit = 1u << (i & 31u), comp = (i >> 5) & 3u;
-        atomicOr(reinterpret_cast<unsigned *>(a.V + t) + comp, bit);
-        uint4 one = u4zero();
-        if (comp == 0u) one.x = bit; else if (comp == 1u) one.y = bit; else if (comp == 2u) one.z = bit; else one.w = bit;
-        if (push_on) {
-            a.P0[t] = one;
-            atomicOr(a.pf0 + (t >> 5), 1u << (t & 31u));
-        } else {
-            a.F0[t] = one;
-            atomicOr(a.fl0 + (t >> 5), 1u << (t & 31u));
-        }
-    }
-    if (gtid == 0) a.counts[0] = (unsigned long long)a.ns;
-    if (!grid_sync(a.ctl, a.expected, a.wait_ns, 0, epoch)) return;
-    if (a.level_ns && gtid == 0) a.level_ns[0] = gtimer();
-
-    // Per-level access modes.  Every block derives them from the same level
-    // counts (read after the barrier), so writer and reader always agree:
-    //  * write_all(L): F' is stored for every chunk, zeros included, when the
-    //    frontier feeding level L already covered >= dense_w_ppm of the pairs;
-    //  * dense(L): level L reads F without its flag words (one dependent memory
-    //    round trip fewer) when F was written whole and covers >= dense_r_ppm;
-    //  * skip_full(L): own visited chunk first and no gathers when it is full,
-    //    once >= full_skip_ppm of the pairs are reached (late, bottom-up levels).
-    const unsigned long long pairs = (unsigned long long)a.ns * (unsigned long long)a.rows;
-    const unsigned long long pairs_ppm = pairs;  // compare x*1e6 >= pairs*ppm
-    unsigned long long reached = (unsigned long long)a.ns;
-    unsigned long long c_prev = (unsigned long long)a.ns;  // frontier size feeding the level
-    bool wrote_all_prev = false;
-    // The frontier of the previous level is in push buffer P[in_p] (-1: in F).
-    int in_p = push_on ? 0 : -1;
-    int dirty_p = -1;
-    bool nf_valid = false;        // a.nf describes V as the previous level left it
-
-    for (int L = 1;; ++L) {
-        const bool odd = (L & 1) != 0;
-        const bool push = in_p >= 0 &&
-                          c_prev * 1000000ull < pairs_ppm * (unsigned long long)a.push_ppm;
-        const bool write_all_c = c_prev * 1000000ull >= pairs_ppm * (unsigned long long)a.dense_w_ppm;
-        const bool dense = wrote_all_prev &&
-                           c_prev * 1000000ull >= pairs_ppm * (unsigned long long)a.dense_r_ppm;
-        const bool skip_full = reached * 1000000ull >= pairs_ppm * (unsigned long long)a.full_skip_ppm;
-        // Skipping full tiles leaves their F' chunks unwritten, so F' is then
-        // written only where it is nonzero (the next level reads it by flags).
-        const bool nf_use = !push && skip_full && nf_valid;
-        const bool write_all = write_all_c && !nf_use;
-        unsigned cnt = 0u, and_pre = 0xffffffffu, and_post = 0xffffffffu;
-        if (push) {
-            uint4 *Pc = in_p ? a.P1 : a.P0;
-            uint4 *Pn = in_p ? a.P0 : a.P1;
-            uint32_t *pfc = in_p ? a.pf1 : a.pf0;
-            uint32_t *pfn = in_p ? a.pf0 : a.pf1;
-            if constexpr (D > 0 && 32 % D == 0) cnt = push_level<D>(a, Pc, Pn, pfc, pfn, ntiles, gtid, nthr);
-        } else {
-            const uint4 *Fc = in_p >= 0 ? (in_p ? a.P1 : a.P0) : (odd ? a.F0 : a.F1);
-            const uint32_t *fc = in_p >= 0 ? (in_p ? a.pf1 : a.pf0) : (odd ? a.fl0 : a.fl1);
-            uint4 *Fn = odd ? a.F1 : a.F0;
-            uint32_t *fn = odd ? a.fl1 : a.fl0;
-            // Balanced contiguous tile range per block; the block's warps pull
-            // kGrab tiles at a time from it through a shared-memory counter.
-            if (threadIdx.x == 0) s_next = t_lo;
+    for (int b = 0; b < a.nb; ++b) {
+        const int ns = min(128 * a.nC, a.ns_total - b * 128 * a.nC);
+        if (a.batch_ns && gtid == 0) a.batch_ns[2 * b] = gtimer();
+        {
+            // Phase 0 (cudaASPLconv.cu:9-33): counters zeroed, padding bits and
+            // the diagonal visited, the diagonal as the level-1 frontier.  The
+            // sources of a batch are distinct vertices, so a chunk holds at most
+            // one of them.
+            unsigned long long *counts = a.counts + (size_t)b * (size_t)a.stride;
+            unsigned *masks = a.masks ? a.masks + (size_t)b * (size_t)a.stride : nullptr;
+            if (blockIdx.x == 0)
+                for (int i = threadIdx.x; i <= a.max_levels; i += blockDim.x) {
+                    counts[i] = i == 0 ? (unsigned long long)ns : 0ull;
+                    if (masks) masks[i] = 0xffffffffu;
+                }
+            const int dirty = S.dirty_p, clean = dirty == 0 ? 1 : 0;
+            const bool push_on = S.push_on != 0;
+            if (dirty >= 0) clear_push_buffer(dirty ? a.P1 : a.P0, dirty ? a.pf1 : a.pf0, ntiles, gtid, nthr);
+            phase0_tiles(a.inv, a.src_first, a.src_begin + b * 128 * a.nC, ns, a.V, a.F0, a.fl0,
+                         clean ? a.P1 : a.P0, clean ? a.pf1 : a.pf0, a.div_nc, (unsigned)a.nC, items,
+                         push_on, gtid, nthr);
+            if (!grid_sync(a.ctl, a.expected, a.wait_ns, 0, epoch)) return;
+            if (threadIdx.x == 0) {
+                S.reached = S.c_prev = (unsigned long long)ns;
+                S.pairs = (unsigned long long)ns * (unsigned long long)a.rows;
+                S.in_p = push_on ? clean : -1;
+                S.dirty_p = -1;
+                S.wrote_all_prev = 0;
+                S.nf_valid = 0;
+                S.done = 0;
+            }
             __syncthreads();
-            if (nf_use) {
-                // Skip-full stage: a warp takes 32 tiles, reads their not-full
-                // words in one load, clears the frontier flags of the full ones
-                // and works only on the others.
-                for (;;) {
-                    unsigned tile0 = 0;
-                    if (lane == 0) tile0 = atomicAdd(&s_next, 32u);
-                    tile0 = __shfl_sync(0xffffffffu, tile0, 0);
-                    if (tile0 >= t_hi) break;
-                    const unsigned my = tile0 + lane;
-                    const unsigned w = my < t_hi ? __ldcg(a.nf + my) : 0u;
-                    if (my < t_hi && w == 0u) fn[my] = 0u;
-                    for (unsigned todo = __ballot_sync(0xffffffffu, w != 0u); todo; todo &= todo - 1u) {
-                        const unsigned tj = tile0 + (unsigned)(__ffs((int)todo) - 1);
-                        level_tiles<D, 1>(a, d, adj, v_base, tj, t_hi, Fc, Fn, fc, fn, dense, write_all,
-                                          skip_full, lane, cnt, and_pre, and_post);
+        }
+        if (b == 0 && a.level_ns && gtid == 0) a.level_ns[0] = gtimer();
+
+        int L = 1;
+        for (;; ++L) {
+            // Per-level access modes.  Every block derives them from the same level
+            // counts (read after the barrier), so writer and reader always agree:
+            //  * push(L): top-down from the push buffer while the frontier feeding
+            //    level L is below push_ppm of the pairs (only from the start);
+            //  * write_all(L): F' is stored for every chunk, zeros included, when the
+            //    frontier feeding level L already covered >= dense_w_ppm of the pairs;
+            //  * dense(L): level L reads F without its flag words (one dependent memory
+            //    round trip fewer) when F was written whole and covers >= dense_r_ppm;
+            //  * skip_full(L): own visited chunk first and no gathers when it is full,
+            //    once >= full_skip_ppm of the pairs are reached (late, bottom-up levels);
+            //    with not-full words from the previous level, full tiles are passed
+            //    over (and F' is then written only where it is nonzero).
+            const unsigned long long c_prev = S.c_prev, pairs = S.pairs;
+            const int in_p = S.in_p;
+            const bool push = in_p >= 0 && c_prev * 1000000ull < pairs * (unsigned long long)a.push_ppm;
+            const bool dense = S.wrote_all_prev &&
+                               c_prev * 1000000ull >= pairs * (unsigned long long)a.dense_r_ppm;
+            const bool skip_full = S.reached * 1000000ull >= pairs * (unsigned long long)a.full_skip_ppm;
+            const bool nf_use = !push && skip_full && S.nf_valid;
+            const bool write_all =
+                !nf_use && c_prev * 1000000ull >= pairs * (unsigned long long)a.dense_w_ppm;
+            const bool odd = (L & 1) != 0;
+            unsigned cnt = 0u, and_pre = 0xffffffffu, and_post = 0xffffffffu;
+            if (push) {
+                uint4 *Pc = in_p ? a.P1 : a.P0;
+                uint4 *Pn = in_p ? a.P0 : a.P1;
+                uint32_t *pfc = in_p ? a.pf1 : a.pf0;
+                uint32_t *pfn = in_p ? a.pf0 : a.pf1;
+                if constexpr (D > 0 && 32 % D == 0) cnt = push_level<D>(a.adj, a.V, a.div_nc, (unsigned)a.nC, Pc, Pn, pfc, pfn, ntiles,
+                                       gtid, nthr);
+            } else {
+                const uint4 *Fc = in_p >= 0 ? (in_p ? a.P1 : a.P0) : (odd ? a.F0 : a.F1);
+                const uint32_t *fc = in_p >= 0 ? (in_p ? a.pf1 : a.pf0) : (odd ? a.fl0 : a.fl1);
+                uint4 *Fn = odd ? a.F1 : a.F0;
+                uint32_t *fn = odd ? a.fl1 : a.fl0;
+                // Balanced contiguous tile range per block; the block's warps pull
+                // tiles from it through a shared-memory counter.
+                if (threadIdx.x == 0) s_next = t_lo;
+                __syncthreads();
+                if (nf_use) {
+                    // Skip-full stage: a warp takes 32 tiles, reads their not-full
+                    // words in one load, clears the frontier flags of the full ones
+                    // and works only on the others.
+                    for (;;) {
+                        unsigned tile0 = 0;
+                        if (lane == 0) tile0 = atomicAdd(&s_next, 32u);
+                        tile0 = __shfl_sync(0xffffffffu, tile0, 0);
+                        if (tile0 >= t_hi) break;
+                        const unsigned my = tile0 + lane;
+                        const unsigned w = my < t_hi ? __ldcg(a.nf + my) : 0u;
+                        if (my < t_hi && w == 0u) fn[my] = 0u;
+                        for (unsigned todo = __ballot_sync(0xffffffffu, w != 0u); todo; todo &= todo - 1u) {
+                            const unsigned tj = tile0 + (unsigned)(__ffs((int)todo) - 1);
+                            level_tiles<D, 1>(a, d, adj, v_base, tj, t_hi, Fc, Fn, fc, fn, dense, write_all,
+                                              skip_full, lane, cnt, and_pre, and_post);
+                        }
+                    }
+                } else {
+                    for (;;) {
+                        unsigned tile0 = 0;
+                        if (lane == 0) tile0 = atomicAdd(&s_next, (unsigned)kGrab);
+                        tile0 = __shfl_sync(0xffffffffu, tile0, 0);
+                        if (tile0 >= t_hi) break;
+                        level_tiles<D, kGrab>(a, d, adj, v_base, tile0, t_hi, Fc, Fn, fc, fn, dense,
+                                              write_all, skip_full, lane, cnt, and_pre, and_post);
                     }
                 }
-            } else {
-                for (;;) {
-                    unsigned tile0 = 0;
-                    if (lane == 0) tile0 = atomicAdd(&s_next, (unsigned)kGrab);
-                    tile0 = __shfl_sync(0xffffffffu, tile0, 0);
-                    if (tile0 >= t_hi) break;
-                    level_tiles<D, kGrab>(a, d, adj, v_base, tile0, t_hi, Fc, Fn, fc, fn, dense,
-                                          write_all, skip_full, lane, cnt, and_pre, and_post);
+            }
+
+            // Level reduction: one 64-bit atomic per block (cudaASPLconv.cu:59-99 fused).
+            unsigned long long *counts = a.counts + (size_t)b * (size_t)a.stride;
+            unsigned *masks = a.masks ? a.masks + (size_t)b * (size_t)a.stride : nullptr;
+            const unsigned wsum = __reduce_add_sync(0xffffffffu, cnt);
+            if (lane == 0) s_sum[threadIdx.x >> 5] = wsum;
+            if (masks) {
+                const unsigned w0 = __reduce_and_sync(0xffffffffu, and_pre);
+                const unsigned w1 = __reduce_and_sync(0xffffffffu, and_post);
+                if (lane == 0) { s_and[0][threadIdx.x >> 5] = w0; s_and[1][threadIdx.x >> 5] = w1; }
+            }
+            __syncthreads();
+            if (threadIdx.x == 0) {
+                unsigned long long bsum = 0;
+                for (int w = 0; w < kBlock / 32; ++w) bsum += s_sum[w];
+                if (bsum) atomicAdd(counts + L, bsum);
+                if (masks) {
+                    unsigned m0 = 0xffffffffu, m1 = 0xffffffffu;
+                    for (int w = 0; w < kBlock / 32; ++w) { m0 &= s_and[0][w]; m1 &= s_and[1][w]; }
+                    if (L == 1) atomicAnd(masks, m0);
+                    atomicAnd(masks + L, m1);
                 }
             }
+            if (!grid_sync(a.ctl, a.expected, a.wait_ns, L, epoch)) return;
+            if (b == 0 && a.level_ns && gtid == 0) a.level_ns[L] = gtimer();
+            if (threadIdx.x == 0) {
+                const unsigned long long cL = ld_relaxed_u64(counts + L);
+                S.reached += cL;
+                S.c_prev = cL;
+                S.wrote_all_prev = !push && write_all;
+                S.nf_valid = a.nf != nullptr && !push && (skip_full || dense || masks != nullptr);
+                if (push) {
+                    S.in_p = in_p ^ 1;    // the frontier is now in Pn; Pc was cleared by its readers
+                } else if (in_p >= 0) {
+                    S.dirty_p = in_p;     // read by this pull level; cleared before it is written again
+                    S.in_p = -1;
+                }
+                // Stop on an empty level, at the cap, or as soon as every pair is
+                // reached (the next level is then empty by construction).
+                S.done = cL == 0ull || L >= a.max_levels || S.reached == S.pairs;
+            }
+            __syncthreads();
+            if (S.done) break;
         }
-
-        // Level reduction: one 64-bit atomic per block (cudaASPLconv.cu:59-99 fused).
-        const unsigned wsum = __reduce_add_sync(0xffffffffu, cnt);
-        if (lane == 0) s_sum[threadIdx.x >> 5] = wsum;
-        if (a.masks) {
-            const unsigned w0 = __reduce_and_sync(0xffffffffu, and_pre);
-            const unsigned w1 = __reduce_and_sync(0xffffffffu, and_post);
-            if (lane == 0) { s_and[0][threadIdx.x >> 5] = w0; s_and[1][threadIdx.x >> 5] = w1; }
+        if (threadIdx.x == 0) {
+            if (blockIdx.x == 0) a.levels_run[b] = L;
+            if (S.in_p >= 0) S.dirty_p = S.in_p;
         }
         __syncthreads();
-        if (threadIdx.x == 0) {
-            unsigned long long bsum = 0;
-            for (int w = 0; w < kBlock / 32; ++w) bsum += s_sum[w];
-            if (bsum) atomicAdd(a.counts + L, bsum);
-            if (a.masks) {
-                unsigned m0 = 0xffffffffu, m1 = 0xffffffffu;
-                for (int w = 0; w < kBlock / 32; ++w) { m0 &= s_and[0][w]; m1 &= s_and[1][w]; }
-                if (L == 1) atomicAnd(a.masks, m0);
-                atomicAnd(a.masks + L, m1);
-            }
-        }
-        if (!grid_sync(a.ctl, a.expected, a.wait_ns, L, epoch)) return;
-        if (a.level_ns && gtid == 0) a.level_ns[L] = gtimer();
-        const unsigned long long cL = ld_relaxed_u64(a.counts + L);
-        reached += cL;
-        c_prev = cL;
-        wrote_all_prev = !push && write_all;
-        nf_valid = a.nf != nullptr && !push && (skip_full || dense || a.masks != nullptr);
-        if (push) {
-            in_p ^= 1;            // the frontier is now in Pn; Pc was cleared by its readers
-        } else if (in_p >= 0) {
-            dirty_p = in_p;       // read by this pull level; cleared after the loop
-            in_p = -1;
-        }
-        // Stop on an empty level, at the cap, or as soon as every pair is reached
-        // (the next level is then empty by construction).
-        if (cL == 0ull || L >= a.max_levels || reached == pairs) {
-            if (gtid == 0) a.ctl->levels_run = L;
-            break;
-        }
+        if (a.batch_ns && gtid == 0) a.batch_ns[2 * b + 1] = gtimer();
     }
     // Nothing reads the push buffers any more: return the one still holding
-    // bits to all zero (the other was cleared by the push level that read it).
-    const int p = in_p >= 0 ? in_p : dirty_p;
-    if (p >= 0) clear_push_buffer(p ? a.P1 : a.P0, p ? a.pf1 : a.pf0, ntiles, gtid, nthr);
+    // bits to all zero.
+    const int dirty = S.dirty_p;
+    if (dirty >= 0) clear_push_buffer(dirty ? a.P1 : a.P0, dirty ? a.pf1 : a.pf0, ntiles, gtid, nthr);
 }
 
 // Expansion of the calculator tables into the pull adjacency adj[rows][d].

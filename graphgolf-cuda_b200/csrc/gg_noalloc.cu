@@ -62,19 +62,14 @@ size_t scratch_need(int N) {
     const size_t nC = ((size_t)N + 127) / 128;
     const size_t items = (size_t)N * nC;
     const size_t fwords = (items + 31) / 32;
-    return align256(sizeof(gg::Ctl)) + align256(sizeof(int)) + align256((size_t)N * 4) +
-           3 * align256(items * 16) + 2 * align256(fwords * 4);
+    return align256(sizeof(gg::Ctl)) + align256(sizeof(int)) + 3 * align256(items * 16) +
+           2 * align256(fwords * 4);
 }
 
 gg_status noalloc_fail(gg_status s, const char *msg) {
     (void)cudaGetLastError();
     gg::set_last_error(msg);
     return s;
-}
-
-// Source ids 0..N-1 (the plain-graph calculator evaluates every vertex).
-__global__ void noalloc_iota(int32_t *src, int n) {
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) src[i] = i;
 }
 
 void *noalloc_kernel_for(int d) {
@@ -112,7 +107,6 @@ extern "C" gg_status gg_graph_eval_noalloc(const int32_t *d_adj, int N, int degr
     unsigned char *p = base;
     gg::Ctl *ctl = (gg::Ctl *)p;           p += align256(sizeof(gg::Ctl));
     int *bad = (int *)p;                   p += align256(sizeof(int));
-    int32_t *src = (int32_t *)p;           p += align256((size_t)N * 4);
     uint4 *V = (uint4 *)p;                 p += align256((size_t)items * 16);
     uint4 *F0 = (uint4 *)p;                p += align256((size_t)items * 16);
     uint4 *F1 = (uint4 *)p;                p += align256((size_t)items * 16);
@@ -133,7 +127,6 @@ extern "C" gg_status gg_graph_eval_noalloc(const int32_t *d_adj, int N, int degr
     if (cudaMemsetAsync(ctl, 0, sizeof(gg::Ctl), st) != cudaSuccess ||
         cudaMemsetAsync(bad, 0, sizeof(int), st) != cudaSuccess)
         return noalloc_fail(GG_CUDA_ERROR, "cudaMemsetAsync on the scratch array failed");
-    noalloc_iota<<<(N + 255) / 256, 256, 0, st>>>(src, N);
     const long long nent = (long long)N * degree;
     if (nent > 0)
         gg::check_table_kernel<<<(int)std::min<long long>((nent + 255) / 256, 4096), 256, 0, st>>>(
@@ -142,11 +135,16 @@ extern "C" gg_status gg_graph_eval_noalloc(const int32_t *d_adj, int N, int degr
 
     gg::BfsArgs a{};
     a.adj = d_adj;
-    a.src = src;
-    a.ns = N;
+    a.inv = nullptr;              // source i is vertex i
+    a.src_first = 0;
+    a.src_begin = 0;
+    a.ns_total = N;
+    a.nb = 1;
     a.V = V; a.F0 = F0; a.F1 = F1; a.fl0 = fl0; a.fl1 = fl1;
     a.counts = (unsigned long long *)d_level_counts;
     a.masks = nullptr;
+    a.stride = max_levels + 1;
+    a.levels_run = &ctl->levels_run;
     a.ctl = ctl;
     a.bad = bad;
     a.expected = (unsigned)grid;

@@ -91,6 +91,7 @@ _SIGS = {
     "gg_eval_device": [_P, _P, ctypes.POINTER(EvalOpts), ctypes.POINTER(Result), _P],
     "gg_last_device_ms": [_P, _DP],
     "gg_last_launches": [_P, _IP],
+    "gg_last_batch_ns": [_P, _P, _I],
     "gg_last_transfer_bytes": [_P, ctypes.POINTER(ctypes.c_uint64), ctypes.POINTER(ctypes.c_uint64)],
     "gg_set_batch_sources": [_P, _I],
     "gg_autotune": [_P, _P, _I, _IP, _DP],
@@ -528,6 +529,12 @@ class Engine:
         n = ctypes.c_int()
         _check(lib().gg_last_launches(self._h, ctypes.byref(n)))
         return n.value
+
+    def last_batch_ns(self, n):
+        """(start, end) device-clock ns of each source batch of the last evaluation."""
+        out = np.zeros(2 * n, dtype=np.uint64)
+        _check(lib().gg_last_batch_ns(self._h, _ptr(out), n))
+        return out.reshape(n, 2)
 
     def last_transfer_bytes(self):
         a, b = ctypes.c_uint64(), ctypes.c_uint64()

@@ -132,6 +132,9 @@ gg_status gg_eval_device(gg_engine *e, const int32_t *d_table, const gg_eval_opt
 gg_status gg_last_device_ms(gg_engine *e, double *ms);
 /* Kernel launches issued by the last evaluation. */
 gg_status gg_last_launches(gg_engine *e, int *launches);
+/* Device clock (ns, %globaltimer) at the start and at the end of each source batch
+ * of the last evaluation: ns[2*b], ns[2*b+1] for b < min(n, batches). */
+gg_status gg_last_batch_ns(gg_engine *e, uint64_t *ns, int n);
 /* Bytes the last evaluation copied host->device and device->host. */
 gg_status gg_last_transfer_bytes(gg_engine *e, uint64_t *h2d, uint64_t *d2h);
 

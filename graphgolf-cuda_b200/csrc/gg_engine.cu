@@ -92,6 +92,7 @@ struct gg_engine {
     int dense_w_ppm = 100;               // level-mode thresholds (see bfs_batch_kernel)
     int dense_r_ppm = 4000;
     int full_skip_ppm = 995000;
+    int split_ppm = 850000;
     int push_ppm = 300;                  // push (top-down) levels below this frontier share
     int push_min_items = 1 << 20;        // ... on bitsets of at least this many chunks
     int adj_smem_rows = 0;               // shared-memory adjacency slice (rows per block)
@@ -360,6 +361,7 @@ gg_status create_common(gg_engine *e) {
     e->dense_w_ppm = env_int("GG_DENSE_W_PPM", e->dense_w_ppm);
     e->dense_r_ppm = env_int("GG_DENSE_R_PPM", e->dense_r_ppm);
     e->full_skip_ppm = env_int("GG_FULL_SKIP_PPM", e->full_skip_ppm);
+    e->split_ppm = env_int("GG_SPLIT_PPM", e->split_ppm);
     e->push_ppm = env_int("GG_PUSH_PPM", e->push_ppm);
     e->push_min_items = env_int("GG_PUSH_MIN_ITEMS", e->push_min_items);
     const int wait_ms = env_int("GG_WAIT_LIMIT_MS", 10000);
@@ -479,6 +481,7 @@ gg_status run_eval(gg_engine *e, const int32_t *d_table_in, const gg_eval_opts *
     a.dense_w_ppm = e->dense_w_ppm;
     a.dense_r_ppm = e->dense_r_ppm;
     a.full_skip_ppm = e->full_skip_ppm;
+    a.split_ppm = e->split_ppm;
     a.adj_smem_rows = e->adj_smem_rows;
     a.wait_ns = e->wait_ns;
     a.expected = (unsigned)e->grid + extra;

@@ -88,6 +88,8 @@ struct BfsArgs {
     int dense_w_ppm;          // write F whole when the feeding frontier >= ppm of the pairs
     int dense_r_ppm;          // read F without flags when it was written whole and >= ppm
     int full_skip_ppm;        // own-first, skip full chunks once reached >= ppm of the pairs
+    int split_ppm;            // dense levels gather half the neighbours first, and the rest
+                              // only where the chunk is not yet covered, once reached >= ppm
     int adj_smem_rows;        // >0: each block keeps its vertex range's adjacency rows
                               // (at most this many) in dynamic shared memory
     long long wait_ns;        // barrier wait limit
@@ -221,7 +223,7 @@ __device__ __forceinline__ void level_tiles(const BfsArgs &a, const int d, const
                                             const unsigned t_hi, const uint4 *Fc, uint4 *Fn,
                                             const uint32_t *fc, uint32_t *fn, const bool dense,
                                             const bool write_all, const bool skip_full,
-                                            const unsigned lane, unsigned &cnt, unsigned &and_pre,
+                                            const bool split, const unsigned lane, unsigned &cnt, unsigned &and_pre,
                                             unsigned &and_post) {
     unsigned t[U], c[U];
     bool ok[U], have[U];
@@ -248,7 +250,22 @@ __device__ __forceinline__ void level_tiles(const BfsArgs &a, const int d, const
             unsigned tu[D];
 #pragma unroll
             for (int i = 0; i < D; ++i) tu[i] = (unsigned)arow[u][i] * (unsigned)a.nC + c[u];
-            if (dense) {
+            if (dense && split && D >= 8) {
+                // Late dense level: few sources still miss this chunk, and half
+                // the neighbours usually bring all of them.
+                constexpr int H = D / 2;
+                uint4 x[H];
+#pragma unroll
+                for (int i = 0; i < H; ++i) x[i] = __ldcg(Fc + tu[i]);
+#pragma unroll
+                for (int i = 0; i < H; ++i) or_into(acc[u], x[i]);
+                if (!u4full(u4or(own[u], acc[u]))) {
+#pragma unroll
+                    for (int i = 0; i < D - H; ++i) x[i] = __ldcg(Fc + tu[H + i]);
+#pragma unroll
+                    for (int i = 0; i < D - H; ++i) or_into(acc[u], x[i]);
+                }
+            } else if (dense) {
                 uint4 x[D];
 #pragma unroll
                 for (int i = 0; i < D; ++i) x[i] = __ldcg(Fc + tu[i]);
@@ -566,6 +583,7 @@ __global__ void __launch_bounds__(kBlock, min_blocks_for(D)) bfs_batch_kernel(co
                                c_prev * 1000000ull >= pairs * (unsigned long long)a.dense_r_ppm;
             const bool skip_full = S.reached * 1000000ull >= pairs * (unsigned long long)a.full_skip_ppm;
             const bool nf_use = !push && skip_full && S.nf_valid;
+            const bool split = dense && S.reached * 1000000ull >= pairs * (unsigned long long)a.split_ppm;
             const bool write_all =
                 !nf_use && c_prev * 1000000ull >= pairs * (unsigned long long)a.dense_w_ppm;
             const bool odd = (L & 1) != 0;
@@ -601,7 +619,7 @@ __global__ void __launch_bounds__(kBlock, min_blocks_for(D)) bfs_batch_kernel(co
                         for (unsigned todo = __ballot_sync(0xffffffffu, w != 0u); todo; todo &= todo - 1u) {
                             const unsigned tj = tile0 + (unsigned)(__ffs((int)todo) - 1);
                             level_tiles<D, 1>(a, d, adj, v_base, tj, t_hi, Fc, Fn, fc, fn, dense, write_all,
-                                              skip_full, lane, cnt, and_pre, and_post);
+                                              skip_full, split, lane, cnt, and_pre, and_post);
                         }
                     }
                 } else {
@@ -611,7 +629,8 @@ __global__ void __launch_bounds__(kBlock, min_blocks_for(D)) bfs_batch_kernel(co
                         tile0 = __shfl_sync(0xffffffffu, tile0, 0);
                         if (tile0 >= t_hi) break;
                         level_tiles<D, kGrab>(a, d, adj, v_base, tile0, t_hi, Fc, Fn, fc, fn, dense,
-                                              write_all, skip_full, lane, cnt, and_pre, and_post);
+                                              write_all, skip_full, split, lane, cnt, and_pre,
+                                              and_post);
                     }
                 }
             }

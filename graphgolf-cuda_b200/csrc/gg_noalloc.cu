@@ -155,6 +155,7 @@ extern "C" gg_status gg_graph_eval_noalloc(const int32_t *d_adj, int N, int degr
     a.dense_w_ppm = 100;
     a.dense_r_ppm = 4000;
     a.full_skip_ppm = 995000;
+    a.split_ppm = 850000;
     a.wait_ns = 10ll * 1000 * 1000 * 1000;
     void *args[] = {&a};
     if (cudaLaunchCooperativeKernel(kern, dim3(grid), dim3(gg::kBlock), args, 0, st) != cudaSuccess)

@@ -91,3 +91,18 @@ def test_disconnected_and_lifted_forms_with_push(monkeypatch):
     Nx, Ny, Mx, My, rows = I.random_piece(4, 3, 8, 5, 4, 3)
     assert G.cudaASPLpiece(Nx, Ny, Mx, My, 4, 0).diameterASPL(rows) == \
         O.piece_diameter_aspl(Nx, Ny, Mx, My, rows)
+
+
+@pytest.mark.parametrize("n,d,seed", [(3000, 8, 1), (20000, 16, 2), (4100, 12, 3)])
+def test_half_gathers_in_dense_levels(monkeypatch, n, d, seed):
+    """Dense levels that gather half the neighbours first (forced on every dense
+    level with GG_SPLIT_PPM=0, never with 1000001) count the same pairs."""
+    adj = G.random_regular(n, d, seed)
+    o = O.bfs_pull(adj, np.arange(n))
+    for ppm in ("0", "1000001"):
+        monkeypatch.setenv("GG_SPLIT_PPM", ppm)
+        e = G.cudaASPLgraph(n, d, 0)
+        r = e.eval(adj, max_levels=n + 1, level_counts=True)
+        assert np.array_equal(r["level_counts"][:o.levels + 1], o.level_counts[:o.levels + 1]), ppm
+        assert r["total"] == o.total()
+        e.close()

@@ -212,7 +212,10 @@ __device__ __forceinline__ uint4 pad_mask(int c, int ns) {
                       pad_word(b + 96, ns));
 }
 
-constexpr int kGrab = 1;  // tiles a warp takes (and keeps in flight) at once
+#ifndef GG_GRAB
+#define GG_GRAB 1
+#endif
+constexpr int kGrab = GG_GRAB;  // tiles a warp takes (and keeps in flight) at once
 
 // One level's work on tiles [tile0, tile0 + U) of the calling warp (a tile is 32
 // consecutive uint4 chunks, one per lane).  Every load of the U tiles is issued

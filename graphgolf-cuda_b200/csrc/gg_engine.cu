@@ -105,7 +105,13 @@ struct gg_engine {
     cudaStream_t stream = nullptr;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     int32_t *d_table = nullptr, *d_adj = nullptr;
-    int *d_bad = nullptr;
+    // Status block of an evaluation (one device allocation, mirrored in pinned
+    // host memory, so that an evaluation needs one memset and one copy back):
+    //   [0, 256) Ctl | bad, asym | levels_run[nb_alloc] | batch_ns[2 nb_alloc] |
+    //   counts[nb][cap_req + 1]
+    unsigned char *d_status = nullptr, *h_status = nullptr;
+    size_t off_levels_run = 0, off_batch_ns = 0, off_counts = 0;
+    int *d_bad = nullptr;                // the table failed its range check
     int *d_asym = nullptr;               // adjacency not symmetric: no push levels
     uint4 *d_V = nullptr, *d_F0 = nullptr, *d_F1 = nullptr;
     uint32_t *d_fl0 = nullptr, *d_fl1 = nullptr;
@@ -149,11 +155,11 @@ void free_batch_buffers(gg_engine *e) {
 }
 
 void free_counters(gg_engine *e) {
-    cudaFree(e->d_counts); cudaFree(e->d_masks); cudaFree(e->d_ctl); cudaFree(e->d_level_ns);
-    cudaFreeHost(e->h_counts); cudaFreeHost(e->h_masks); cudaFreeHost(e->h_ctl);
+    cudaFree(e->d_status); cudaFree(e->d_masks); cudaFree(e->d_level_ns);
+    cudaFreeHost(e->h_status); cudaFreeHost(e->h_masks);
     cudaFreeHost(e->h_level_ns);
-    cudaFree(e->d_levels_run); cudaFreeHost(e->h_levels_run);
-    cudaFree(e->d_batch_ns); cudaFreeHost(e->h_batch_ns);
+    e->d_status = e->h_status = nullptr;
+    e->d_bad = e->d_asym = e->h_bad = nullptr;
     e->d_levels_run = e->h_levels_run = nullptr;
     e->d_batch_ns = e->h_batch_ns = nullptr;
     e->d_counts = nullptr; e->d_masks = nullptr; e->d_ctl = nullptr; e->d_level_ns = nullptr;
@@ -168,8 +174,8 @@ void destroy_all(gg_engine *e) {
     free_batch_buffers(e);
     free_counters(e);
     if (e->d_adj != e->d_table) cudaFree(e->d_adj);  // the graph form aliases the two
-    cudaFree(e->d_table); cudaFree(e->d_inv); cudaFree(e->d_bad); cudaFree(e->d_asym);
-    cudaFreeHost(e->h_table); cudaFreeHost(e->h_bad);
+    cudaFree(e->d_table); cudaFree(e->d_inv);
+    cudaFreeHost(e->h_table);
     if (e->ev0) cudaEventDestroy(e->ev0);
     if (e->ev1) cudaEventDestroy(e->ev1);
     if (e->stream) cudaStreamDestroy(e->stream);
@@ -301,16 +307,25 @@ gg_status ensure_counters(gg_engine *e, int cap, int nb) {
     nb = std::max(nb, e->nb_alloc);
     free_counters(e);
     const size_t n = (size_t)(cap + 1) * nb;
-    GG_CK(cudaMalloc(&e->d_counts, n * sizeof(unsigned long long)));
+    e->off_levels_run = 512;
+    e->off_batch_ns = e->off_levels_run + (((size_t)nb * sizeof(int) + 15) & ~size_t(15));
+    e->off_counts = e->off_batch_ns + (size_t)nb * 2 * sizeof(unsigned long long);
+    const size_t bytes = e->off_counts + n * sizeof(unsigned long long);
+    GG_CK(cudaMalloc(&e->d_status, bytes));
+    GG_CK(cudaMallocHost(&e->h_status, bytes));
+    e->d_ctl = reinterpret_cast<Ctl *>(e->d_status);
+    e->h_ctl = reinterpret_cast<Ctl *>(e->h_status);
+    e->d_bad = reinterpret_cast<int *>(e->d_status + sizeof(Ctl));
+    e->h_bad = reinterpret_cast<int *>(e->h_status + sizeof(Ctl));
+    e->d_asym = e->d_bad + 1;
+    e->d_levels_run = reinterpret_cast<int *>(e->d_status + e->off_levels_run);
+    e->h_levels_run = reinterpret_cast<int *>(e->h_status + e->off_levels_run);
+    e->d_batch_ns = reinterpret_cast<unsigned long long *>(e->d_status + e->off_batch_ns);
+    e->h_batch_ns = reinterpret_cast<unsigned long long *>(e->h_status + e->off_batch_ns);
+    e->d_counts = reinterpret_cast<unsigned long long *>(e->d_status + e->off_counts);
+    e->h_counts = reinterpret_cast<unsigned long long *>(e->h_status + e->off_counts);
     GG_CK(cudaMalloc(&e->d_masks, n * sizeof(unsigned)));
-    GG_CK(cudaMalloc(&e->d_ctl, sizeof(Ctl)));
-    GG_CK(cudaMallocHost(&e->h_counts, n * sizeof(unsigned long long)));
     GG_CK(cudaMallocHost(&e->h_masks, n * sizeof(unsigned)));
-    GG_CK(cudaMallocHost(&e->h_ctl, sizeof(Ctl)));
-    GG_CK(cudaMalloc(&e->d_levels_run, (size_t)nb * sizeof(int)));
-    GG_CK(cudaMallocHost(&e->h_levels_run, (size_t)nb * sizeof(int)));
-    GG_CK(cudaMalloc(&e->d_batch_ns, (size_t)nb * 2 * sizeof(unsigned long long)));
-    GG_CK(cudaMallocHost(&e->h_batch_ns, (size_t)nb * 2 * sizeof(unsigned long long)));
     GG_CK(cudaMalloc(&e->d_level_ns, (size_t)(cap + 1) * sizeof(unsigned long long)));
     GG_CK(cudaMallocHost(&e->h_level_ns, (size_t)(cap + 1) * sizeof(unsigned long long)));
     e->cap_alloc = cap;
@@ -355,9 +370,6 @@ gg_status create_common(gg_engine *e) {
         GG_CK(cudaMalloc(&e->d_inv, inv.size() * sizeof(int32_t)));
         GG_CK(cudaMemcpy(e->d_inv, inv.data(), inv.size() * sizeof(int32_t), cudaMemcpyHostToDevice));
     }
-    GG_CK(cudaMalloc(&e->d_bad, sizeof(int)));
-    GG_CK(cudaMalloc(&e->d_asym, sizeof(int)));
-    GG_CK(cudaMallocHost(&e->h_bad, sizeof(int)));
     e->dense_w_ppm = env_int("GG_DENSE_W_PPM", e->dense_w_ppm);
     e->dense_r_ppm = env_int("GG_DENSE_R_PPM", e->dense_r_ppm);
     e->full_skip_ppm = env_int("GG_FULL_SKIP_PPM", e->full_skip_ppm);
@@ -400,10 +412,12 @@ gg_status run_eval(gg_engine *e, const int32_t *d_table_in, const gg_eval_opts *
     const int nb = (ns_all + e->batch_bits - 1) / e->batch_bits;
     gg_status s = ensure_counters(e, cap_req, nb);
     if (s != GG_OK) return s;
-    const int stride = e->cap_alloc + 1;
+    const int stride = cap_req + 1;      // counts of batch b at [b * stride, (b + 1) * stride)
 
     (void)cudaGetLastError();  // launch checks below must not see an earlier, unrelated error
     GG_CK(cudaEventRecord(e->ev0, st));
+    // control block, range-check and symmetry words
+    GG_CK(cudaMemsetAsync(e->d_status, 0, sizeof(Ctl) + 2 * sizeof(int), st));
     int launches = 0;
     // Table -> adjacency.
     if (e->form == FORM_GRAPH) {
@@ -411,7 +425,6 @@ gg_status run_eval(gg_engine *e, const int32_t *d_table_in, const gg_eval_opts *
             GG_CK(cudaMemcpyAsync(e->d_table, d_table_in, e->table_elems * 4,
                                   cudaMemcpyDeviceToDevice, st));
         }
-        GG_CK(cudaMemsetAsync(e->d_bad, 0, sizeof(int), st));
         const long long n = (long long)e->rows * e->d;
         if (n > 0) {
             gg::check_table_kernel<<<(int)std::min<long long>((n + 255) / 256, 4096), 256, 0, st>>>(
@@ -434,8 +447,6 @@ gg_status run_eval(gg_engine *e, const int32_t *d_table_in, const gg_eval_opts *
             ++launches;
         }
     }
-    GG_CK(cudaMemsetAsync(e->d_ctl, 0, sizeof(Ctl), st));
-    GG_CK(cudaMemsetAsync(e->d_asym, 0, sizeof(int), st));
     if (e->p_dirty) {
         // New buffers, or a launch that stopped early: the push buffers are
         // zero again only after these four writes.
@@ -490,28 +501,16 @@ gg_status run_eval(gg_engine *e, const int32_t *d_table_in, const gg_eval_opts *
     GG_CK(cudaLaunchCooperativeKernel(kern, dim3(e->grid), dim3(gg::kBlock), args, e->smem_bytes, st));
     ++launches;
     GG_CK(cudaEventRecord(e->ev1, st));
-    // Read back only the levels that can hold counts (cap_req + 1 per batch).
-    uint64_t d2h = 0;
-    const size_t lv = (size_t)cap_req + 1;
-    GG_CK(cudaMemcpy2DAsync(e->h_counts, stride * sizeof(unsigned long long), e->d_counts,
-                            stride * sizeof(unsigned long long), lv * sizeof(unsigned long long), nb,
-                            cudaMemcpyDeviceToHost, st));
-    d2h += lv * nb * sizeof(unsigned long long);
+    // One copy back: control block, status words, per-batch levels and times,
+    // and the counts of every batch (cap_req + 1 each).
+    uint64_t d2h = e->off_counts + (size_t)nb * stride * sizeof(unsigned long long);
+    GG_CK(cudaMemcpyAsync(e->h_status, e->d_status, d2h, cudaMemcpyDeviceToHost, st));
     if (wvc) {
-        GG_CK(cudaMemcpy2DAsync(e->h_masks, stride * sizeof(unsigned), e->d_masks,
-                                stride * sizeof(unsigned), lv * sizeof(unsigned), nb,
-                                cudaMemcpyDeviceToHost, st));
-        d2h += lv * nb * sizeof(unsigned);
+        GG_CK(cudaMemcpyAsync(e->h_masks, e->d_masks, (size_t)nb * stride * sizeof(unsigned),
+                              cudaMemcpyDeviceToHost, st));
+        d2h += (size_t)nb * stride * sizeof(unsigned);
     }
-    GG_CK(cudaMemcpyAsync(e->h_ctl, e->d_ctl, sizeof(Ctl), cudaMemcpyDeviceToHost, st));
-    GG_CK(cudaMemcpyAsync(e->h_levels_run, e->d_levels_run, (size_t)nb * sizeof(int), cudaMemcpyDeviceToHost, st));
-    GG_CK(cudaMemcpyAsync(e->h_batch_ns, e->d_batch_ns, (size_t)nb * 2 * sizeof(unsigned long long),
-                          cudaMemcpyDeviceToHost, st));
-    d2h += sizeof(Ctl) + (size_t)nb * (sizeof(int) + 2 * sizeof(unsigned long long));
-    if (e->form == FORM_GRAPH) {
-        GG_CK(cudaMemcpyAsync(e->h_bad, e->d_bad, sizeof(int), cudaMemcpyDeviceToHost, st));
-        d2h += sizeof(int);
-    }
+    const size_t lv = (size_t)cap_req + 1;
     if (want_ns) {
         GG_CK(cudaMemcpyAsync(e->h_level_ns, e->d_level_ns, lv * sizeof(unsigned long long),
                               cudaMemcpyDeviceToHost, st));

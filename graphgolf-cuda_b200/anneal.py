@@ -156,3 +156,53 @@ def time_to(trace, target):
         if v <= target:
             return t
     return None
+
+
+@dataclass
+class InitTemp:
+    temp: float           # T0 in the reference's unit: a change of the total distance (ΔASPL * N(N-1))
+    temp_aspl: float      # the same T0 as a change of ASPL (the unit anneal() uses)
+    avg: float            # mean uphill change of the total distance
+    uphill: int           # proposals that raised the total (connected ones only)
+    proposals: int
+    ms: float             # device time of the batched evaluation
+
+
+def initial_temperature(n, d, *, graphs=100, neighbours=100, seed=1, accept=0.4, device=0, bases=None):
+    """Initial annealing temperature, restating cppcode/initTemp.cpp:399-430 on the
+    batched evaluator: for `graphs` random d-regular graphs and `neighbours` 2-opt
+    proposals of each, the mean increase of the total distance over the proposals
+    that are connected and uphill, avg; T0 = -avg / ln(accept) (the reference
+    prints -avg/log(0.4), initTemp.cpp:425-430).  The reference sums ASPL
+    differences and multiplies by N(N-1); here the same quantity is summed exactly
+    as integer totals.  All base graphs and proposals go through one batched
+    evaluation instead of graphs * (neighbours + 1) calculator calls.
+
+    `bases` replaces the random graphs (each an n x d adjacency)."""
+    if bases is None:
+        bases = [G.random_regular(n, d, seed * 1000003 + k) for k in range(graphs)]
+    b = G.Batch(device)
+    try:
+        ids = [b.add_base(a) for a in bases]
+        none = np.zeros(len(ids), dtype=G.SWAP_DTYPE)
+        none["base"] = ids
+        none["a"] = -1
+        props = [G.gen_swaps(a, i, neighbours, (seed << 20) ^ k) for k, (a, i) in enumerate(zip(bases, ids))]
+        res = b.eval(np.concatenate([none] + props))
+        ms = b.last_ms()
+    finally:
+        b.close()
+    k = len(ids)
+    base_total = res["total"][:k].astype(np.int64)
+    base_ok = res["connected"][:k] == 1
+    cand = res[k:]
+    owner = np.repeat(np.arange(k), neighbours)
+    delta = cand["total"].astype(np.int64) - base_total[owner]
+    up = (cand["connected"] == 1) & base_ok[owner] & (delta > 0)
+    cnt = int(up.sum())
+    if cnt == 0:
+        raise ValueError("no connected uphill proposal")
+    avg = int(delta[up].sum()) / cnt
+    temp = -avg / math.log(accept)
+    npairs = n * (n - 1)
+    return InitTemp(temp=temp, temp_aspl=temp / npairs, avg=avg, uphill=cnt, proposals=len(cand), ms=ms)

@@ -75,6 +75,17 @@ namespace gg {
 __attribute__((visibility("hidden"))) void set_last_error(const char *msg) { g_err = msg; }
 }  // namespace gg
 
+// What a captured evaluation depends on (see run_eval).
+struct EvalKey {
+    const void *table, *status, *bitsets;
+    int s0, ns, cap;
+    bool wvc, want_ns;
+    bool operator==(const EvalKey &o) const {
+        return table == o.table && status == o.status && bitsets == o.bitsets && s0 == o.s0 &&
+               ns == o.ns && cap == o.cap && wvc == o.wvc && want_ns == o.want_ns;
+    }
+};
+
 struct gg_engine {
     int form = FORM_PART;
     int device = 0;
@@ -134,6 +145,10 @@ struct gg_engine {
     Ctl *h_ctl = nullptr;
     int *h_bad = nullptr;
 
+    bool use_graph = true;               // replay captured evaluations (GG_NO_GRAPH=1: never)
+    cudaGraphExec_t graph_exec = nullptr;
+    EvalKey graph_key{};
+
     double last_ms = 0.0;
     int last_launches = 0;
     int last_batches = 0;                // batches of the last evaluation
@@ -167,6 +182,13 @@ void free_counters(gg_engine *e) {
     e->cap_alloc = e->nb_alloc = 0;
 }
 
+// A captured evaluation holds buffer addresses, the plan and the wait limit:
+// drop it whenever one of them changes.
+void invalidate_graph(gg_engine *e) {
+    if (e->graph_exec) cudaGraphExecDestroy(e->graph_exec);
+    e->graph_exec = nullptr;
+}
+
 void destroy_all(gg_engine *e) {
     if (!e) return;
     cudaSetDevice(e->device);
@@ -178,6 +200,7 @@ void destroy_all(gg_engine *e) {
     cudaFreeHost(e->h_table);
     if (e->ev0) cudaEventDestroy(e->ev0);
     if (e->ev1) cudaEventDestroy(e->ev1);
+    invalidate_graph(e);
     if (e->stream) cudaStreamDestroy(e->stream);
     delete e;
 }
@@ -219,6 +242,7 @@ int tuned_width(const gg_engine *e) {
 }
 
 gg_status plan(gg_engine *e, int want_bits) {
+    invalidate_graph(e);
     const int n_src = (int)e->reps.size();
     int bits;
     if (want_bits > 0) {
@@ -305,6 +329,7 @@ gg_status ensure_counters(gg_engine *e, int cap, int nb) {
     if (cap <= e->cap_alloc && nb <= e->nb_alloc) return GG_OK;
     cap = std::max(cap, e->cap_alloc);
     nb = std::max(nb, e->nb_alloc);
+    invalidate_graph(e);
     free_counters(e);
     const size_t n = (size_t)(cap + 1) * nb;
     e->off_levels_run = 512;
@@ -376,6 +401,7 @@ gg_status create_common(gg_engine *e) {
     e->split_ppm = env_int("GG_SPLIT_PPM", e->split_ppm);
     e->push_ppm = env_int("GG_PUSH_PPM", e->push_ppm);
     e->push_min_items = env_int("GG_PUSH_MIN_ITEMS", e->push_min_items);
+    e->use_graph = env_int("GG_NO_GRAPH", 0) == 0;
     const int wait_ms = env_int("GG_WAIT_LIMIT_MS", 10000);
     e->wait_ns = (long long)std::max(wait_ms, 1) * 1000000ll;
     gg_status s = plan(e, 0);
@@ -415,38 +441,6 @@ gg_status run_eval(gg_engine *e, const int32_t *d_table_in, const gg_eval_opts *
     const int stride = cap_req + 1;      // counts of batch b at [b * stride, (b + 1) * stride)
 
     (void)cudaGetLastError();  // launch checks below must not see an earlier, unrelated error
-    GG_CK(cudaEventRecord(e->ev0, st));
-    // control block, range-check and symmetry words
-    GG_CK(cudaMemsetAsync(e->d_status, 0, sizeof(Ctl) + 2 * sizeof(int), st));
-    int launches = 0;
-    // Table -> adjacency.
-    if (e->form == FORM_GRAPH) {
-        if (d_table_in != e->d_table) {
-            GG_CK(cudaMemcpyAsync(e->d_table, d_table_in, e->table_elems * 4,
-                                  cudaMemcpyDeviceToDevice, st));
-        }
-        const long long n = (long long)e->rows * e->d;
-        if (n > 0) {
-            gg::check_table_kernel<<<(int)std::min<long long>((n + 255) / 256, 4096), 256, 0, st>>>(
-                e->d_table, n, e->rows, e->d_bad);
-            GG_CK(cudaGetLastError());
-            ++launches;
-        }
-    } else {
-        ExpandArgs x{};
-        x.table = d_table_in;
-        x.adj = e->d_adj;
-        x.form = (e->form == FORM_PART) ? 1 : (e->form == FORM_PIECE ? 2 : 3);
-        x.rows = e->rows; x.d = e->d; x.N = e->N; x.M = e->M;
-        x.Nx = e->dims[0]; x.Ny = e->dims[1]; x.Nz = e->dims[2];
-        x.Mx = e->dims[3]; x.My = e->dims[4]; x.Mz = e->dims[5];
-        const long long n = (long long)e->rows * e->d;
-        if (n > 0) {
-            gg::expand_kernel<<<(int)std::min<long long>((n + 255) / 256, 8192), 256, 0, st>>>(x);
-            GG_CK(cudaGetLastError());
-            ++launches;
-        }
-    }
     if (e->p_dirty) {
         // New buffers, or a launch that stopped early: the push buffers are
         // zero again only after these four writes.
@@ -457,64 +451,130 @@ gg_status run_eval(gg_engine *e, const int32_t *d_table_in, const gg_eval_opts *
         GG_CK(cudaMemsetAsync(e->d_pf1, 0, fbytes, st));
         e->p_dirty = false;
     }
-    if (want_ns)
-        GG_CK(cudaMemsetAsync(e->d_level_ns, 0, (size_t)(cap_req + 1) * sizeof(unsigned long long), st));
-
-    // One cooperative launch runs every source batch of the evaluation.
-    void *kern = kernel_for(e->d);
     if (fault("launch")) return fail(GG_CUDA_ERROR, "injected launch failure");
     const unsigned extra = fault("barrier") ? 1u : 0u;
-    e->p_dirty = true;  // until the launch is known to have finished cleanly
-    BfsArgs a{};
-    a.adj = e->d_adj;
-    a.inv = e->d_inv;
-    a.src_first = e->src_first;
-    a.src_begin = s0;
-    a.ns_total = ns_all;
-    a.nb = nb;
-    a.V = e->d_V; a.F0 = e->d_F0; a.F1 = e->d_F1;
-    a.fl0 = e->d_fl0; a.fl1 = e->d_fl1;
-    a.P0 = e->d_P0; a.P1 = e->d_P1; a.pf0 = e->d_pf0; a.pf1 = e->d_pf1;
-    // Below ~1M chunks a pull level costs about one grid barrier anyway.
-    a.push_ppm = (long long)e->items >= (long long)e->push_min_items ? e->push_ppm : 0;
-    a.nf = e->d_nf;
-    a.asym = e->d_asym;
-    a.counts = e->d_counts;
-    a.masks = wvc ? e->d_masks : nullptr;
-    a.stride = stride;
-    a.levels_run = e->d_levels_run;
-    a.level_ns = want_ns ? e->d_level_ns : nullptr;
-    a.batch_ns = e->d_batch_ns;
-    a.ctl = e->d_ctl;
-    a.rows = e->rows; a.d = e->d; a.nC = e->nC; a.items = e->items;
-    a.div_nc = FastDiv((uint32_t)e->nC);
-    a.max_levels = cap_req;
-    a.dense_w_ppm = e->dense_w_ppm;
-    a.dense_r_ppm = e->dense_r_ppm;
-    a.full_skip_ppm = e->full_skip_ppm;
-    a.split_ppm = e->split_ppm;
-    a.adj_smem_rows = e->adj_smem_rows;
-    a.wait_ns = e->wait_ns;
-    a.expected = (unsigned)e->grid + extra;
-    a.bad = e->form == FORM_GRAPH ? e->d_bad : nullptr;
-    void *args[] = {&a};
-    GG_CK(cudaLaunchCooperativeKernel(kern, dim3(e->grid), dim3(gg::kBlock), args, e->smem_bytes, st));
-    ++launches;
-    GG_CK(cudaEventRecord(e->ev1, st));
-    // One copy back: control block, status words, per-batch levels and times,
-    // and the counts of every batch (cap_req + 1 each).
-    uint64_t d2h = e->off_counts + (size_t)nb * stride * sizeof(unsigned long long);
-    GG_CK(cudaMemcpyAsync(e->h_status, e->d_status, d2h, cudaMemcpyDeviceToHost, st));
-    if (wvc) {
-        GG_CK(cudaMemcpyAsync(e->h_masks, e->d_masks, (size_t)nb * stride * sizeof(unsigned),
-                              cudaMemcpyDeviceToHost, st));
-        d2h += (size_t)nb * stride * sizeof(unsigned);
-    }
     const size_t lv = (size_t)cap_req + 1;
-    if (want_ns) {
-        GG_CK(cudaMemcpyAsync(e->h_level_ns, e->d_level_ns, lv * sizeof(unsigned long long),
-                              cudaMemcpyDeviceToHost, st));
-        d2h += lv * sizeof(unsigned long long);
+    uint64_t d2h = e->off_counts + (size_t)nb * stride * sizeof(unsigned long long);
+    if (wvc) d2h += (size_t)nb * stride * sizeof(unsigned);
+    if (want_ns) d2h += lv * sizeof(unsigned long long);
+    const int launches = 1 + ((long long)e->rows * e->d > 0 ? 1 : 0);
+
+    // Everything the GPU does for one evaluation, on `q`: status words zeroed,
+    // table -> adjacency (checked), one cooperative launch for every source
+    // batch, and one copy back of the status block.
+    // The timing events are recorded here only when launching directly; a
+    // replayed graph is timed by events recorded around its launch.
+    auto enqueue = [&](cudaStream_t q, bool timed) -> gg_status {
+        if (timed) GG_CK(cudaEventRecord(e->ev0, q));
+        // control block, range-check and symmetry words
+        GG_CK(cudaMemsetAsync(e->d_status, 0, sizeof(Ctl) + 2 * sizeof(int), q));
+        const long long n = (long long)e->rows * e->d;
+        if (e->form == FORM_GRAPH) {
+            if (d_table_in != e->d_table)
+                GG_CK(cudaMemcpyAsync(e->d_table, d_table_in, e->table_elems * 4, cudaMemcpyDeviceToDevice, q));
+            if (n > 0) {
+                gg::check_table_kernel<<<(int)std::min<long long>((n + 255) / 256, 4096), 256, 0, q>>>(
+                    e->d_table, n, e->rows, e->d_bad);
+                GG_CK(cudaGetLastError());
+            }
+        } else if (n > 0) {
+            ExpandArgs x{};
+            x.table = d_table_in;
+            x.adj = e->d_adj;
+            x.form = (e->form == FORM_PART) ? 1 : (e->form == FORM_PIECE ? 2 : 3);
+            x.rows = e->rows; x.d = e->d; x.N = e->N; x.M = e->M;
+            x.Nx = e->dims[0]; x.Ny = e->dims[1]; x.Nz = e->dims[2];
+            x.Mx = e->dims[3]; x.My = e->dims[4]; x.Mz = e->dims[5];
+            gg::expand_kernel<<<(int)std::min<long long>((n + 255) / 256, 8192), 256, 0, q>>>(x);
+            GG_CK(cudaGetLastError());
+        }
+        if (want_ns)
+            GG_CK(cudaMemsetAsync(e->d_level_ns, 0, lv * sizeof(unsigned long long), q));
+        BfsArgs a{};
+        a.adj = e->d_adj;
+        a.inv = e->d_inv;
+        a.src_first = e->src_first;
+        a.src_begin = s0;
+        a.ns_total = ns_all;
+        a.nb = nb;
+        a.V = e->d_V; a.F0 = e->d_F0; a.F1 = e->d_F1;
+        a.fl0 = e->d_fl0; a.fl1 = e->d_fl1;
+        a.P0 = e->d_P0; a.P1 = e->d_P1; a.pf0 = e->d_pf0; a.pf1 = e->d_pf1;
+        // Below ~1M chunks a pull level costs about one grid barrier anyway.
+        a.push_ppm = (long long)e->items >= (long long)e->push_min_items ? e->push_ppm : 0;
+        a.nf = e->d_nf;
+        a.asym = e->d_asym;
+        a.counts = e->d_counts;
+        a.masks = wvc ? e->d_masks : nullptr;
+        a.stride = stride;
+        a.levels_run = e->d_levels_run;
+        a.level_ns = want_ns ? e->d_level_ns : nullptr;
+        a.batch_ns = e->d_batch_ns;
+        a.ctl = e->d_ctl;
+        a.rows = e->rows; a.d = e->d; a.nC = e->nC; a.items = e->items;
+        a.div_nc = FastDiv((uint32_t)e->nC);
+        a.max_levels = cap_req;
+        a.dense_w_ppm = e->dense_w_ppm;
+        a.dense_r_ppm = e->dense_r_ppm;
+        a.full_skip_ppm = e->full_skip_ppm;
+        a.split_ppm = e->split_ppm;
+        a.adj_smem_rows = e->adj_smem_rows;
+        a.wait_ns = e->wait_ns;
+        a.expected = (unsigned)e->grid + extra;
+        a.bad = e->form == FORM_GRAPH ? e->d_bad : nullptr;
+        void *args[] = {&a};
+        GG_CK(cudaLaunchCooperativeKernel(kernel_for(e->d), dim3(e->grid), dim3(gg::kBlock), args,
+                                          e->smem_bytes, q));
+        if (timed) GG_CK(cudaEventRecord(e->ev1, q));
+        // One copy back: control block, status words, per-batch levels and
+        // times, and the counts of every batch (cap_req + 1 each).
+        GG_CK(cudaMemcpyAsync(e->h_status, e->d_status, e->off_counts + (size_t)nb * stride * 8,
+                              cudaMemcpyDeviceToHost, q));
+        if (wvc)
+            GG_CK(cudaMemcpyAsync(e->h_masks, e->d_masks, (size_t)nb * stride * sizeof(unsigned),
+                                  cudaMemcpyDeviceToHost, q));
+        if (want_ns)
+            GG_CK(cudaMemcpyAsync(e->h_level_ns, e->d_level_ns, lv * sizeof(unsigned long long),
+                                  cudaMemcpyDeviceToHost, q));
+        return GG_OK;
+    };
+
+    // Repeated evaluations of one shape replay a captured CUDA graph of the
+    // same work (one launch call instead of about eight).  Anything that
+    // changes the work -- the table pointer, the source range, the level cap,
+    // the outputs asked for, reallocated buffers -- captures a new graph.
+    const EvalKey key{d_table_in, e->d_status, e->d_V, s0, ns_all, cap_req, wvc, want_ns};
+    e->p_dirty = true;  // until the launch is known to have finished cleanly
+    bool replayed = false;
+    if (e->use_graph && !extra) {
+        if (!e->graph_exec || !(key == e->graph_key)) {
+            if (e->graph_exec) { cudaGraphExecDestroy(e->graph_exec); e->graph_exec = nullptr; }
+            cudaGraph_t g = nullptr;
+            gg_status cs = GG_CUDA_ERROR;
+            if (cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal) == cudaSuccess) {
+                cs = enqueue(st, false);
+                const cudaError_t ce = cudaStreamEndCapture(st, &g);
+                if (ce != cudaSuccess) cs = GG_CUDA_ERROR;
+            }
+            if (cs == GG_OK && g && cudaGraphInstantiate(&e->graph_exec, g, 0) == cudaSuccess) {
+                e->graph_key = key;
+            } else {
+                e->graph_exec = nullptr;
+                e->use_graph = false;   // this device or driver cannot capture it: launch directly
+            }
+            if (g) cudaGraphDestroy(g);
+            (void)cudaGetLastError();
+        }
+        if (e->graph_exec) {
+            GG_CK(cudaEventRecord(e->ev0, st));
+            GG_CK(cudaGraphLaunch(e->graph_exec, st));
+            GG_CK(cudaEventRecord(e->ev1, st));
+            replayed = true;
+        }
+    }
+    if (!replayed) {
+        gg_status es = enqueue(st, true);
+        if (es != GG_OK) return es;
     }
     e->last_d2h = d2h;
     GG_CK(cudaStreamSynchronize(st));
@@ -833,6 +893,7 @@ gg_status gg_autotune(gg_engine *e, const int32_t *table, int trials, int *best_
 gg_status gg_set_wait_limit_ms(gg_engine *e, int ms) {
     if (!e || ms < 1) return fail(GG_BAD_ARG, "bad wait limit");
     e->wait_ns = (long long)ms * 1000000ll;
+    invalidate_graph(e);
     return GG_OK;
 }
 

@@ -1,6 +1,8 @@
 """Batched annealing (graphgolf-cuda_b200/anneal.py): every reported ASPL is an
 exact evaluation, and the trained surrogate ranks proposals better than chance
 (what the learned part gains over random proposal)."""
+import math
+
 import numpy as np
 import pytest
 
@@ -57,3 +59,23 @@ def test_surrogate_top_k_beats_random_proposals():
     from scipy.stats import spearmanr
     rho = spearmanr(pred, all_r["total"].astype(np.float64)).correlation
     assert rho > 0.2, rho
+
+
+@pytest.mark.gpu
+def test_initial_temperature_matches_oracle():
+    """Batched initial-temperature estimate == the same proposals scored one by
+    one by the oracle (exact integer totals, so the averages are identical)."""
+    import anneal as A
+    n, d, graphs, nbr = 200, 4, 6, 25
+    t = A.initial_temperature(n, d, graphs=graphs, neighbours=nbr, seed=3)
+    bases = [G.random_regular(n, d, 3 * 1000003 + k) for k in range(graphs)]
+    ups = []
+    for k, a in enumerate(bases):
+        fx = O.bfs_pull(a, np.arange(n)).total()
+        for s in G.gen_swaps(a, k, nbr, (3 << 20) ^ k):
+            r = O.bfs_pull(G.apply_swap(a, s), np.arange(n))
+            if r.connected and r.total() > fx:
+                ups.append(r.total() - fx)
+    assert t.uphill == len(ups) and t.proposals == graphs * nbr
+    assert t.avg == sum(ups) / len(ups)
+    assert t.temp == -t.avg / math.log(0.4) and t.temp > 0

@@ -360,3 +360,32 @@ def test_bad_graph_table_rejected():
     adj[17, 2] = -5
     with pytest.raises(G.GGError):
         e.calc(adj)
+
+
+def test_replayed_evaluations_match_direct_launches(monkeypatch):
+    """Repeated evaluations replay a captured CUDA graph; a sequence that changes
+    the table, the source range, the level cap, the batch width and the wait limit
+    between calls gives the same answers as an engine that launches directly."""
+    tables = [G.random_regular(3000, 6, s) for s in (1, 2)]
+    calls = [dict(t=0), dict(t=1), dict(t=0), dict(t=1, src_range=(64, 2000)), dict(t=1, src_range=(64, 2000)),
+             dict(t=0, max_levels=3), dict(t=0, max_levels=3), dict(t=1, wvc=True), dict(t=0, bits=512),
+             dict(t=1, bits=512), dict(t=0, wait=5000), dict(t=1)]
+
+    def run(eng):
+        out = []
+        for c in calls:
+            if "bits" in c:
+                eng.set_batch_sources(c["bits"])
+            if "wait" in c:
+                eng.set_wait_limit_ms(c["wait"])
+            r = eng.eval(tables[c["t"]], max_levels=c.get("max_levels", 0), src_range=c.get("src_range"),
+                         want_wvc=c.get("wvc", False))
+            out.append((r["total"], r["reached"], r["levels"], r["capped"], r["wvc"]))
+        return out
+
+    replay = run(G.cudaASPLgraph(3000, 6, 0))
+    monkeypatch.setenv("GG_NO_GRAPH", "1")
+    direct = run(G.cudaASPLgraph(3000, 6, 0))
+    assert replay == direct
+    o = O.bfs_pull(tables[1], np.arange(3000))
+    assert replay[1][0] == o.total()

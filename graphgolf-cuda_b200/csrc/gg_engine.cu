@@ -11,6 +11,7 @@
 // and the connectivity test live on the device.
 #include "gg.h"
 #include "gg_kernels.cuh"
+#include "gg_internal.h"
 
 #include <algorithm>
 #include <cstdio>
@@ -77,12 +78,13 @@ __attribute__((visibility("hidden"))) void set_last_error(const char *msg) { g_e
 
 // What a captured evaluation depends on (see run_eval).
 struct EvalKey {
-    const void *table, *status, *bitsets;
+    const void *table, *status, *bitsets, *inv, *planes;
     int s0, ns, cap;
     bool wvc, want_ns;
     bool operator==(const EvalKey &o) const {
-        return table == o.table && status == o.status && bitsets == o.bitsets && s0 == o.s0 &&
-               ns == o.ns && cap == o.cap && wvc == o.wvc && want_ns == o.want_ns;
+        return table == o.table && status == o.status && bitsets == o.bitsets && inv == o.inv &&
+               planes == o.planes && s0 == o.s0 && ns == o.ns && cap == o.cap && wvc == o.wvc &&
+               want_ns == o.want_ns;
     }
 };
 
@@ -422,9 +424,11 @@ gg_status finish_create(gg_engine *e, gg_engine **out) {
 
 // Core evaluation with the table already on the device (d_table_in) on `st`.
 gg_status run_eval(gg_engine *e, const int32_t *d_table_in, const gg_eval_opts *o, gg_result *r,
-                   cudaStream_t st) {
-    const int n_src_all = (int)e->reps.size();
+                   cudaStream_t st, const gg::EvalExtra *x = nullptr) {
+    const int n_src_all = x && x->inv ? x->ns : (int)e->reps.size();
     int s0 = 0, s1 = n_src_all;
+    if (x && x->inv && (n_src_all < 1 || n_src_all > e->rows)) return fail(GG_BAD_ARG, "bad source list");
+    if (x && x->planes && (o && (o->src_begin || o->src_end))) return fail(GG_BAD_ARG, "planes need every source");
     if (o && (o->src_begin || o->src_end)) {
         s0 = o->src_begin;
         s1 = o->src_end;
@@ -492,8 +496,14 @@ gg_status run_eval(gg_engine *e, const int32_t *d_table_in, const gg_eval_opts *
             GG_CK(cudaMemsetAsync(e->d_level_ns, 0, lv * sizeof(unsigned long long), q));
         BfsArgs a{};
         a.adj = e->d_adj;
-        a.inv = e->d_inv;
-        a.src_first = e->src_first;
+        a.inv = x && x->inv ? x->inv : e->d_inv;
+        a.src_first = x && x->inv ? 0 : e->src_first;
+        if (x && x->planes) {
+            a.planes = x->planes;
+            a.nplanes = x->nplanes;
+            a.plane_cols = (unsigned)(nb * e->nC);
+            a.plane_stride = (unsigned long long)e->rows * a.plane_cols;
+        }
         a.src_begin = s0;
         a.ns_total = ns_all;
         a.nb = nb;
@@ -543,10 +553,11 @@ gg_status run_eval(gg_engine *e, const int32_t *d_table_in, const gg_eval_opts *
     // same work (one launch call instead of about eight).  Anything that
     // changes the work -- the table pointer, the source range, the level cap,
     // the outputs asked for, reallocated buffers -- captures a new graph.
-    const EvalKey key{d_table_in, e->d_status, e->d_V, s0, ns_all, cap_req, wvc, want_ns};
+    const EvalKey key{d_table_in, e->d_status, e->d_V, x ? (const void *)x->inv : nullptr,
+                      x ? (const void *)x->planes : nullptr, s0, ns_all, cap_req, wvc, want_ns};
     e->p_dirty = true;  // until the launch is known to have finished cleanly
     bool replayed = false;
-    if (e->use_graph && !extra) {
+    if (e->use_graph && !extra && !(x && x->no_graph)) {
         if (!e->graph_exec || !(key == e->graph_key)) {
             if (e->graph_exec) { cudaGraphExecDestroy(e->graph_exec); e->graph_exec = nullptr; }
             cudaGraph_t g = nullptr;
@@ -681,6 +692,19 @@ gg_status lifted_diameter_aspl(gg_engine *e, const int32_t *table, int *diameter
 
 }  // namespace
 
+namespace gg {
+gg_status engine_eval(gg_engine *e, const int32_t *d_table, const gg_eval_opts *o, gg_result *r,
+                      cudaStream_t st, const EvalExtra *x) {
+    if (!e || !r || !d_table) return fail(GG_BAD_ARG, "null argument");
+    GG_CK(cudaSetDevice(e->device));
+    return run_eval(e, d_table, o, r, st ? st : e->stream, x);
+}
+int engine_plane_cols(const gg_engine *e) {
+    const int n_src = (int)e->reps.size();
+    return ((n_src + e->batch_bits - 1) / e->batch_bits) * e->nC;
+}
+}  // namespace gg
+
 extern "C" {
 
 int gg_abi_version(void) { return GG_ABI_VERSION; }
@@ -781,6 +805,7 @@ gg_status gg_destroy(gg_engine *e) {
     destroy_all(e);
     return GG_OK;
 }
+
 
 gg_status gg_eval(gg_engine *e, const int32_t *table, const gg_eval_opts *opts, gg_result *out) {
     return eval_host(e, table, opts, out);

@@ -109,6 +109,23 @@ struct BfsArgs {
     // full.  Written by levels that load every visited chunk; a later level in
     // the skip-full stage passes over tiles whose word is 0.  nullptr: unused.
     uint32_t *nf;
+    // Distance bit-planes (nullptr: not written).  Plane k holds bit k of the
+    // distance of every (vertex, source) pair: planes[k * plane_stride + v *
+    // plane_cols + s / 128] bit s % 128, for the sources of the whole evaluation
+    // (batch b writes columns b * nC ...).  nplanes planes hold distances up to
+    // 2^nplanes - 1; pairs never reached keep 0.
+    uint4 *planes;
+    int nplanes;
+    unsigned plane_cols;
+    unsigned long long plane_stride;
+};
+
+// Where a level's new pairs go in the distance planes.
+struct PlaneOut {
+    uint4 *planes;
+    unsigned long long stride;
+    unsigned cols, col0;         // columns of the evaluation, first column of the batch
+    int nplanes, L;
 };
 
 __device__ __forceinline__ unsigned long long gtimer() {
@@ -328,7 +345,8 @@ __device__ __forceinline__ unsigned comp_of(const uint4 &f, const int k) {
 // atomicOr returns the old word -- are this level's new pairs and go into Pn and
 // the flag words with fire-and-forget reductions.
 __device__ __forceinline__ void push_item(uint4 *V, const uint4 f, const unsigned tw, uint4 *Pn,
-                                          uint32_t *pfn, unsigned &cnt) {
+                                          uint32_t *pfn, const PlaneOut &po, const unsigned w,
+                                          const unsigned c, unsigned &cnt) {
     unsigned any = 0u;
 #pragma unroll
     for (int k = 0; k < 4; ++k) {
@@ -339,6 +357,12 @@ __device__ __forceinline__ void push_item(uint4 *V, const uint4 f, const unsigne
             atomicOr(reinterpret_cast<unsigned *>(Pn + tw) + k, nb);
             cnt += __popc(nb);
             any = 1u;
+            if (po.planes) {
+                const size_t pi = (size_t)w * po.cols + po.col0 + c;
+                for (int p = 0; p < po.nplanes; ++p)
+                    if ((po.L >> p) & 1)
+                        atomicOr(reinterpret_cast<unsigned *>(po.planes + (size_t)p * po.stride + pi) + k, nb);
+            }
         }
     }
     if (any) atomicOr(pfn + (tw >> 5), 1u << (tw & 31u));
@@ -359,8 +383,8 @@ __device__ __forceinline__ void push_item(uint4 *V, const uint4 f, const unsigne
 template <int D>
 static __device__ __noinline__ unsigned push_level(const int32_t *adj, uint4 *V, const FastDiv div_nc,
                                             const unsigned nC, uint4 *Pc, uint4 *Pn, uint32_t *pfc,
-                                            uint32_t *pfn, const unsigned fwords, const unsigned gtid,
-                                            const unsigned nthr) {
+                                            uint32_t *pfn, const unsigned fwords, const PlaneOut po,
+                                            const unsigned gtid, const unsigned nthr) {
     static_assert(D > 0 && 32 % D == 0, "push levels need D | 32");
     unsigned cnt = 0u;
     const unsigned lane = threadIdx.x & 31u;
@@ -378,8 +402,8 @@ static __device__ __noinline__ unsigned push_level(const int32_t *adj, uint4 *V,
             const unsigned u = div_nc.div(t);
             const unsigned c = t - u * nC;
             const uint4 f = __ldcg(Pc + t);
-            const unsigned tw = (unsigned)__ldg(adj + (size_t)u * D + i) * nC + c;
-            push_item(V, f, tw, Pn, pfn, cnt);
+            const unsigned w = (unsigned)__ldg(adj + (size_t)u * D + i);
+            push_item(V, f, w * nC + c, Pn, pfn, po, w, c, cnt);
         }
         __syncwarp();
         if (i == 0u && m0) {
@@ -406,6 +430,29 @@ static __device__ __noinline__ void clear_push_buffer(uint4 *P, uint32_t *pf, co
     }
 }
 
+// After pull level po.L: OR the level's new pairs (the chunks flagged in `fn`,
+// their bits in `Fn`) into the distance planes.  One warp per flag word, one lane
+// per chunk (coalesced); each chunk has one writer.
+static __device__ __noinline__ void plane_pass(const uint32_t *fn, const uint4 *Fn, const PlaneOut po,
+                                               const FastDiv div_nc, const unsigned nC,
+                                               const unsigned fwords, const unsigned gtid,
+                                               const unsigned nthr) {
+    const unsigned lane = threadIdx.x & 31u;
+    for (unsigned k = gtid >> 5; k < fwords; k += nthr >> 5) {
+        const unsigned m = __ldcg(fn + k);
+        if (!((m >> lane) & 1u)) continue;
+        const unsigned t = k * 32u + lane;
+        const uint4 nw = __ldcg(Fn + t);
+        const unsigned v = div_nc.div(t), c = t - v * nC;
+        const size_t pi = (size_t)v * po.cols + po.col0 + c;
+        for (int p = 0; p < po.nplanes; ++p)
+            if ((po.L >> p) & 1) {
+                uint4 *q = po.planes + (size_t)p * po.stride + pi;
+                *q = u4or(*q, nw);
+            }
+    }
+}
+
 // Phase 0 of batch b: every visited chunk rewritten with its padding bits and
 // the diagonal, the diagonal stored as the level-1 frontier (push buffer P_diag
 // or F0) with its flag words.  The sources of a batch are distinct vertices, so a
@@ -415,7 +462,7 @@ static __device__ __noinline__ void phase0_tiles(const int32_t *inv, const int s
                                           const int ns, uint4 *V, uint4 *F0, uint32_t *fl0,
                                           uint4 *P_diag, uint32_t *pf_diag, const FastDiv div_nc,
                                           const unsigned nC, const unsigned items, const bool push_on,
-                                          const unsigned gtid, const unsigned nthr) {
+                                          const PlaneOut po, const unsigned gtid, const unsigned nthr) {
     const unsigned lane = threadIdx.x & 31u;
     const unsigned ntiles = (items + 31u) >> 5;
     for (unsigned tile = gtid >> 5; tile < ntiles; tile += nthr >> 5) {
@@ -432,6 +479,9 @@ static __device__ __noinline__ void phase0_tiles(const int32_t *inv, const int s
             if (comp == 0u) one.x = bit; else if (comp == 1u) one.y = bit; else if (comp == 2u) one.z = bit; else one.w = bit;
         }
         if (ok) V[t] = u4or(pad_mask((int)c, ns), one);
+        if (ok && po.planes)
+            for (int p = 0; p < po.nplanes; ++p)
+                po.planes[(size_t)p * po.stride + (size_t)v * po.cols + po.col0 + c] = u4zero();
         const unsigned fb = __ballot_sync(0xffffffffu, has);
         if (push_on) {
             if (has) P_diag[t] = one;
@@ -548,9 +598,10 @@ __global__ void __launch_bounds__(kBlock, min_blocks_for(D)) bfs_batch_kernel(co
             const int dirty = S.dirty_p, clean = dirty == 0 ? 1 : 0;
             const bool push_on = S.push_on != 0;
             if (dirty >= 0) clear_push_buffer(dirty ? a.P1 : a.P0, dirty ? a.pf1 : a.pf0, ntiles, gtid, nthr);
+            const PlaneOut po0{a.planes, a.plane_stride, a.plane_cols, (unsigned)(b * a.nC), a.nplanes, 0};
             phase0_tiles(a.inv, a.src_first, a.src_begin + b * 128 * a.nC, ns, a.V, a.F0, a.fl0,
                          clean ? a.P1 : a.P0, clean ? a.pf1 : a.pf0, a.div_nc, (unsigned)a.nC, items,
-                         push_on, gtid, nthr);
+                         push_on, po0, gtid, nthr);
             if (!grid_sync(a.ctl, a.expected, a.wait_ns, 0, epoch)) return;
             if (threadIdx.x == 0) {
                 S.reached = S.c_prev = (unsigned long long)ns;
@@ -597,6 +648,8 @@ __global__ void __launch_bounds__(kBlock, min_blocks_for(D)) bfs_batch_kernel(co
                 uint32_t *pfc = in_p ? a.pf1 : a.pf0;
                 uint32_t *pfn = in_p ? a.pf0 : a.pf1;
                 if constexpr (D > 0 && 32 % D == 0) cnt = push_level<D>(a.adj, a.V, a.div_nc, (unsigned)a.nC, Pc, Pn, pfc, pfn, ntiles,
+                                       PlaneOut{a.planes, a.plane_stride, a.plane_cols,
+                                                (unsigned)(b * a.nC), a.nplanes, L},
                                        gtid, nthr);
             } else {
                 const uint4 *Fc = in_p >= 0 ? (in_p ? a.P1 : a.P0) : (odd ? a.F0 : a.F1);
@@ -661,6 +714,15 @@ __global__ void __launch_bounds__(kBlock, min_blocks_for(D)) bfs_batch_kernel(co
                 }
             }
             if (!grid_sync(a.ctl, a.expected, a.wait_ns, L, epoch)) return;
+            if (a.planes && !push) {
+                // distances of this level's new pairs into the planes; the barrier
+                // keeps the frontier buffer unchanged until every block is done
+                const bool odd = (L & 1) != 0;
+                plane_pass(odd ? a.fl1 : a.fl0, odd ? a.F1 : a.F0,
+                           PlaneOut{a.planes, a.plane_stride, a.plane_cols, (unsigned)(b * a.nC), a.nplanes, L},
+                           a.div_nc, (unsigned)a.nC, ntiles, gtid, nthr);
+                if (!grid_sync(a.ctl, a.expected, a.wait_ns, L, epoch)) return;
+            }
             if (b == 0 && a.level_ns && gtid == 0) a.level_ns[L] = gtimer();
             if (threadIdx.x == 0) {
                 const unsigned long long cL = ld_relaxed_u64(counts + L);

@@ -118,6 +118,11 @@ _SIGS = {
     "gg_surrogate_grad": [_P, _I, _P, _P, _P, _P, ctypes.POINTER(ctypes.c_float)],
     "gg_surrogate_destroy": [_P],
     "gg_gen_random_regular": [_I, _I, ctypes.c_uint64, _P],
+    "gg_inc_create": [_I, _I, _I, _EPP],
+    "gg_inc_set_graph": [_P, _P, _P],
+    "gg_inc_eval": [_P, _P, _P, _IP],
+    "gg_inc_commit": [_P, _P, _P],
+    "gg_inc_destroy": [_P],
     "gg_gen_cyclic_lift": [_I, _I, _I, ctypes.c_uint64, _P],
 }
 
@@ -820,3 +825,45 @@ class Batch:
             self.close()
         except Exception:
             pass
+
+
+class Incremental:
+    """Exact evaluation of 2-opt moves on one current graph, searching again only
+    from the sources a move can affect (gg_inc_*)."""
+
+    def __init__(self, n, degree, device=0):
+        self.n, self.d = n, degree
+        self._h = _create("gg_inc_create", n, degree, device)
+
+    def set_graph(self, adj):
+        r = Result()
+        _check(lib().gg_inc_set_graph(self._h, _ptr(_i32(adj)), ctypes.byref(r)))
+        return r.as_dict()
+
+    def eval(self, swap):
+        """(result dict, sources searched again) of the current graph with `swap` applied."""
+        sw = np.ascontiguousarray(np.asarray(swap, dtype=SWAP_DTYPE).reshape(1))
+        out = np.zeros(1, dtype=CAND_RESULT_DTYPE)
+        aff = ctypes.c_int()
+        _check(lib().gg_inc_eval(self._h, _ptr(sw), _ptr(out), ctypes.byref(aff)))
+        o = out[0]
+        return {"total": int(o["total"]), "reached": int(o["reached"]), "levels": int(o["levels"]),
+                "connected": int(o["connected"])}, aff.value
+
+    def commit(self, swap):
+        sw = np.ascontiguousarray(np.asarray(swap, dtype=SWAP_DTYPE).reshape(1))
+        r = Result()
+        _check(lib().gg_inc_commit(self._h, _ptr(sw), ctypes.byref(r)))
+        return r.as_dict()
+
+    def close(self):
+        if self._h:
+            lib().gg_inc_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+

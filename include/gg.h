@@ -226,6 +226,27 @@ gg_status gg_batch_vertex_hist(gg_batch *b, int base_id, int K, uint32_t *hist);
 gg_status gg_batch_last_ms(gg_batch *b, double *ms);
 gg_status gg_batch_destroy(gg_batch *b);
 
+/* ---- Incremental evaluation of 2-opt moves (no reference counterpart) ----------
+ * For one current plain graph (n*degree, symmetric), a move's exact result is
+ * computed by searching again only from the sources whose distances can change:
+ * the full evaluation of the current graph also stores its distance matrix as 4
+ * bit-planes (4*n*n/8 bytes on the device), from which a per-source test picks the
+ * sources a removed edge or an added edge can affect (about 30 % of them for a
+ * random 2-opt on a random regular graph).  Exact when the current graph is
+ * connected with diameter <= 15; otherwise each call evaluates the moved graph in
+ * full.  Plays the role of the per-proposal calculator call of the reference
+ * annealers (cppcode/annealing.cpp:403-404) for large n. */
+typedef struct gg_inc gg_inc;
+gg_status gg_inc_create(int n, int degree, int device, gg_inc **out);
+/* Make adj the current graph (full evaluation; r may be NULL). */
+gg_status gg_inc_set_graph(gg_inc *h, const int32_t *adj, gg_result *r);
+/* Exact counts of the current graph with move s applied (s->base is ignored);
+ * *affected = sources searched again (may be NULL).  The current graph is kept. */
+gg_status gg_inc_eval(gg_inc *h, const gg_swap *s, gg_cand_result *out, int *affected);
+/* Apply move s to the current graph (full evaluation; r may be NULL). */
+gg_status gg_inc_commit(gg_inc *h, const gg_swap *s, gg_result *r);
+gg_status gg_inc_destroy(gg_inc *h);
+
 /* Uniform random 2-opt proposals on a base graph (adj n*degree, simple):
  * edges (a,b), (c,d) drawn uniformly, mode uniform; proposals that would create a
  * loop or a repeated edge are redrawn.  Writes `count` swaps with base = base_id. */

@@ -214,16 +214,23 @@ int kernel_degree_slot(int d) {
     }
 }
 
-void *kernel_for(int d) {
+template <bool PL>
+void *kernel_for_t(int d) {
     switch (kernel_degree_slot(d)) {
-        case 3: return (void *)gg::bfs_batch_kernel<3>;
-        case 4: return (void *)gg::bfs_batch_kernel<4>;
-        case 6: return (void *)gg::bfs_batch_kernel<6>;
-        case 8: return (void *)gg::bfs_batch_kernel<8>;
-        case 12: return (void *)gg::bfs_batch_kernel<12>;
-        case 16: return (void *)gg::bfs_batch_kernel<16>;
-        default: return (void *)gg::bfs_batch_kernel<0>;
+        case 3: return (void *)gg::bfs_batch_kernel<3, PL>;
+        case 4: return (void *)gg::bfs_batch_kernel<4, PL>;
+        case 6: return (void *)gg::bfs_batch_kernel<6, PL>;
+        case 8: return (void *)gg::bfs_batch_kernel<8, PL>;
+        case 12: return (void *)gg::bfs_batch_kernel<12, PL>;
+        case 16: return (void *)gg::bfs_batch_kernel<16, PL>;
+        default: return (void *)gg::bfs_batch_kernel<0, PL>;
     }
+}
+
+// The BFS kernel for degree d; `planes`: the variant that also writes the
+// distance planes.
+void *kernel_for(int d, bool planes = false) {
+    return planes ? kernel_for_t<true>(d) : kernel_for_t<false>(d);
 }
 
 // Source-batch plan: batch width, chunks per row, grid size.
@@ -533,7 +540,7 @@ gg_status run_eval(gg_engine *e, const int32_t *d_table_in, const gg_eval_opts *
         a.expected = (unsigned)e->grid + extra;
         a.bad = e->form == FORM_GRAPH ? e->d_bad : nullptr;
         void *args[] = {&a};
-        GG_CK(cudaLaunchCooperativeKernel(kernel_for(e->d), dim3(e->grid), dim3(gg::kBlock), args,
+        GG_CK(cudaLaunchCooperativeKernel(kernel_for(e->d, a.planes != nullptr), dim3(e->grid), dim3(gg::kBlock), args,
                                           e->smem_bytes, q));
         if (timed) GG_CK(cudaEventRecord(e->ev1, q));
         // One copy back: control block, status words, per-batch levels and

@@ -128,6 +128,14 @@ struct PlaneOut {
     int nplanes, L;
 };
 
+// The block's current PlaneOut, kept in shared memory (the plane-writing
+// kernel's thread 0 sets it between barriers), so that the functions below take
+// no extra arguments and the kernel without planes carries none of this.
+__device__ __forceinline__ PlaneOut &plane_slot() {
+    __shared__ PlaneOut s;
+    return s;
+}
+
 __device__ __forceinline__ unsigned long long gtimer() {
     unsigned long long t;
     asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
@@ -344,9 +352,10 @@ __device__ __forceinline__ unsigned comp_of(const uint4 &f, const int k) {
 // is used); the bits that were not visited yet -- exact under concurrency,
 // atomicOr returns the old word -- are this level's new pairs and go into Pn and
 // the flag words with fire-and-forget reductions.
+template <bool PL>
 __device__ __forceinline__ void push_item(uint4 *V, const uint4 f, const unsigned tw, uint4 *Pn,
-                                          uint32_t *pfn, const PlaneOut &po, const unsigned w,
-                                          const unsigned c, unsigned &cnt) {
+                                          uint32_t *pfn, const unsigned w, const unsigned c,
+                                          unsigned &cnt) {
     unsigned any = 0u;
 #pragma unroll
     for (int k = 0; k < 4; ++k) {
@@ -357,7 +366,8 @@ __device__ __forceinline__ void push_item(uint4 *V, const uint4 f, const unsigne
             atomicOr(reinterpret_cast<unsigned *>(Pn + tw) + k, nb);
             cnt += __popc(nb);
             any = 1u;
-            if (po.planes) {
+            if constexpr (PL) {
+                const PlaneOut &po = plane_slot();
                 const size_t pi = (size_t)w * po.cols + po.col0 + c;
                 for (int p = 0; p < po.nplanes; ++p)
                     if ((po.L >> p) & 1)
@@ -380,11 +390,11 @@ __device__ __forceinline__ void push_item(uint4 *V, const uint4 f, const unsigne
 // rows * nC.  Needs D to divide 32 (a group never straddles two warps).  Kept
 // out of line: it runs a few times per batch, and inlined it would take
 // registers from the pull levels.
-template <int D>
+template <int D, bool PL>
 static __device__ __noinline__ unsigned push_level(const int32_t *adj, uint4 *V, const FastDiv div_nc,
                                             const unsigned nC, uint4 *Pc, uint4 *Pn, uint32_t *pfc,
-                                            uint32_t *pfn, const unsigned fwords, const PlaneOut po,
-                                            const unsigned gtid, const unsigned nthr) {
+                                            uint32_t *pfn, const unsigned fwords, const unsigned gtid,
+                                            const unsigned nthr) {
     static_assert(D > 0 && 32 % D == 0, "push levels need D | 32");
     unsigned cnt = 0u;
     const unsigned lane = threadIdx.x & 31u;
@@ -403,7 +413,7 @@ static __device__ __noinline__ unsigned push_level(const int32_t *adj, uint4 *V,
             const unsigned c = t - u * nC;
             const uint4 f = __ldcg(Pc + t);
             const unsigned w = (unsigned)__ldg(adj + (size_t)u * D + i);
-            push_item(V, f, w * nC + c, Pn, pfn, po, w, c, cnt);
+            push_item<PL>(V, f, w * nC + c, Pn, pfn, w, c, cnt);
         }
         __syncwarp();
         if (i == 0u && m0) {
@@ -433,10 +443,10 @@ static __device__ __noinline__ void clear_push_buffer(uint4 *P, uint32_t *pf, co
 // After pull level po.L: OR the level's new pairs (the chunks flagged in `fn`,
 // their bits in `Fn`) into the distance planes.  One warp per flag word, one lane
 // per chunk (coalesced); each chunk has one writer.
-static __device__ __noinline__ void plane_pass(const uint32_t *fn, const uint4 *Fn, const PlaneOut po,
-                                               const FastDiv div_nc, const unsigned nC,
-                                               const unsigned fwords, const unsigned gtid,
-                                               const unsigned nthr) {
+static __device__ __noinline__ void plane_pass(const uint32_t *fn, const uint4 *Fn, const FastDiv div_nc,
+                                               const unsigned nC, const unsigned fwords,
+                                               const unsigned gtid, const unsigned nthr) {
+    const PlaneOut po = plane_slot();
     const unsigned lane = threadIdx.x & 31u;
     for (unsigned k = gtid >> 5; k < fwords; k += nthr >> 5) {
         const unsigned m = __ldcg(fn + k);
@@ -458,11 +468,12 @@ static __device__ __noinline__ void plane_pass(const uint32_t *fn, const uint4 *
 // or F0) with its flag words.  The sources of a batch are distinct vertices, so a
 // chunk holds at most one of them.  One warp per tile of 32 chunks.  Out of line
 // for the same reason as push_level.
+template <bool PL>
 static __device__ __noinline__ void phase0_tiles(const int32_t *inv, const int src_first, const int first,
                                           const int ns, uint4 *V, uint4 *F0, uint32_t *fl0,
                                           uint4 *P_diag, uint32_t *pf_diag, const FastDiv div_nc,
                                           const unsigned nC, const unsigned items, const bool push_on,
-                                          const PlaneOut po, const unsigned gtid, const unsigned nthr) {
+                                          const unsigned gtid, const unsigned nthr) {
     const unsigned lane = threadIdx.x & 31u;
     const unsigned ntiles = (items + 31u) >> 5;
     for (unsigned tile = gtid >> 5; tile < ntiles; tile += nthr >> 5) {
@@ -479,9 +490,12 @@ static __device__ __noinline__ void phase0_tiles(const int32_t *inv, const int s
             if (comp == 0u) one.x = bit; else if (comp == 1u) one.y = bit; else if (comp == 2u) one.z = bit; else one.w = bit;
         }
         if (ok) V[t] = u4or(pad_mask((int)c, ns), one);
-        if (ok && po.planes)
-            for (int p = 0; p < po.nplanes; ++p)
-                po.planes[(size_t)p * po.stride + (size_t)v * po.cols + po.col0 + c] = u4zero();
+        if constexpr (PL) {
+            const PlaneOut &po = plane_slot();
+            if (ok)
+                for (int p = 0; p < po.nplanes; ++p)
+                    po.planes[(size_t)p * po.stride + (size_t)v * po.cols + po.col0 + c] = u4zero();
+        }
         const unsigned fb = __ballot_sync(0xffffffffu, has);
         if (push_on) {
             if (has) P_diag[t] = one;
@@ -523,7 +537,7 @@ struct LoopState {
 // the diagonal set, level-1 frontier and its flags written) -> grid barrier ->
 // levels, each ended by a grid barrier.  One launch instead of one per batch
 // saves the launch gap and the shared-memory adjacency reload per batch.
-template <int D>
+template <int D, bool PL>
 __global__ void __launch_bounds__(kBlock, min_blocks_for(D)) bfs_batch_kernel(const BfsArgs a) {
     const int d = D > 0 ? D : a.d;
     const unsigned lane = threadIdx.x & 31u;
@@ -598,10 +612,15 @@ __global__ void __launch_bounds__(kBlock, min_blocks_for(D)) bfs_batch_kernel(co
             const int dirty = S.dirty_p, clean = dirty == 0 ? 1 : 0;
             const bool push_on = S.push_on != 0;
             if (dirty >= 0) clear_push_buffer(dirty ? a.P1 : a.P0, dirty ? a.pf1 : a.pf0, ntiles, gtid, nthr);
-            const PlaneOut po0{a.planes, a.plane_stride, a.plane_cols, (unsigned)(b * a.nC), a.nplanes, 0};
-            phase0_tiles(a.inv, a.src_first, a.src_begin + b * 128 * a.nC, ns, a.V, a.F0, a.fl0,
-                         clean ? a.P1 : a.P0, clean ? a.pf1 : a.pf0, a.div_nc, (unsigned)a.nC, items,
-                         push_on, po0, gtid, nthr);
+            if constexpr (PL) {
+                if (threadIdx.x == 0)
+                    plane_slot() = PlaneOut{a.planes, a.plane_stride, a.plane_cols, (unsigned)(b * a.nC),
+                                            a.nplanes, 0};
+                __syncthreads();
+            }
+            phase0_tiles<PL>(a.inv, a.src_first, a.src_begin + b * 128 * a.nC, ns, a.V, a.F0, a.fl0,
+                             clean ? a.P1 : a.P0, clean ? a.pf1 : a.pf0, a.div_nc, (unsigned)a.nC, items,
+                             push_on, gtid, nthr);
             if (!grid_sync(a.ctl, a.expected, a.wait_ns, 0, epoch)) return;
             if (threadIdx.x == 0) {
                 S.reached = S.c_prev = (unsigned long long)ns;
@@ -611,6 +630,7 @@ __global__ void __launch_bounds__(kBlock, min_blocks_for(D)) bfs_batch_kernel(co
                 S.wrote_all_prev = 0;
                 S.nf_valid = 0;
                 S.done = 0;
+                if constexpr (PL) plane_slot().L = 1;
             }
             __syncthreads();
         }
@@ -647,10 +667,8 @@ __global__ void __launch_bounds__(kBlock, min_blocks_for(D)) bfs_batch_kernel(co
                 uint4 *Pn = in_p ? a.P0 : a.P1;
                 uint32_t *pfc = in_p ? a.pf1 : a.pf0;
                 uint32_t *pfn = in_p ? a.pf0 : a.pf1;
-                if constexpr (D > 0 && 32 % D == 0) cnt = push_level<D>(a.adj, a.V, a.div_nc, (unsigned)a.nC, Pc, Pn, pfc, pfn, ntiles,
-                                       PlaneOut{a.planes, a.plane_stride, a.plane_cols,
-                                                (unsigned)(b * a.nC), a.nplanes, L},
-                                       gtid, nthr);
+                if constexpr (D > 0 && 32 % D == 0) cnt = push_level<D, PL>(a.adj, a.V, a.div_nc, (unsigned)a.nC, Pc, Pn, pfc, pfn, ntiles,
+                                           gtid, nthr);
             } else {
                 const uint4 *Fc = in_p >= 0 ? (in_p ? a.P1 : a.P0) : (odd ? a.F0 : a.F1);
                 const uint32_t *fc = in_p >= 0 ? (in_p ? a.pf1 : a.pf0) : (odd ? a.fl0 : a.fl1);
@@ -714,14 +732,15 @@ __global__ void __launch_bounds__(kBlock, min_blocks_for(D)) bfs_batch_kernel(co
                 }
             }
             if (!grid_sync(a.ctl, a.expected, a.wait_ns, L, epoch)) return;
-            if (a.planes && !push) {
-                // distances of this level's new pairs into the planes; the barrier
-                // keeps the frontier buffer unchanged until every block is done
-                const bool odd = (L & 1) != 0;
-                plane_pass(odd ? a.fl1 : a.fl0, odd ? a.F1 : a.F0,
-                           PlaneOut{a.planes, a.plane_stride, a.plane_cols, (unsigned)(b * a.nC), a.nplanes, L},
-                           a.div_nc, (unsigned)a.nC, ntiles, gtid, nthr);
-                if (!grid_sync(a.ctl, a.expected, a.wait_ns, L, epoch)) return;
+            if constexpr (PL) {
+                if (!push) {
+                    // distances of this level's new pairs into the planes; the barrier
+                    // keeps the frontier buffer unchanged until every block is done
+                    const bool odd = (L & 1) != 0;
+                    plane_pass(odd ? a.fl1 : a.fl0, odd ? a.F1 : a.F0, a.div_nc, (unsigned)a.nC, ntiles,
+                               gtid, nthr);
+                    if (!grid_sync(a.ctl, a.expected, a.wait_ns, L, epoch)) return;
+                }
             }
             if (b == 0 && a.level_ns && gtid == 0) a.level_ns[L] = gtimer();
             if (threadIdx.x == 0) {
@@ -739,6 +758,7 @@ __global__ void __launch_bounds__(kBlock, min_blocks_for(D)) bfs_batch_kernel(co
                 // Stop on an empty level, at the cap, or as soon as every pair is
                 // reached (the next level is then empty by construction).
                 S.done = cL == 0ull || L >= a.max_levels || S.reached == S.pairs;
+                if constexpr (PL) plane_slot().L = L + 1;
             }
             __syncthreads();
             if (S.done) break;

@@ -74,13 +74,13 @@ gg_status noalloc_fail(gg_status s, const char *msg) {
 
 void *noalloc_kernel_for(int d) {
     switch (d) {
-        case 3: return (void *)gg::bfs_batch_kernel<3>;
-        case 4: return (void *)gg::bfs_batch_kernel<4>;
-        case 6: return (void *)gg::bfs_batch_kernel<6>;
-        case 8: return (void *)gg::bfs_batch_kernel<8>;
-        case 12: return (void *)gg::bfs_batch_kernel<12>;
-        case 16: return (void *)gg::bfs_batch_kernel<16>;
-        default: return (void *)gg::bfs_batch_kernel<0>;
+        case 3: return (void *)gg::bfs_batch_kernel<3, false>;
+        case 4: return (void *)gg::bfs_batch_kernel<4, false>;
+        case 6: return (void *)gg::bfs_batch_kernel<6, false>;
+        case 8: return (void *)gg::bfs_batch_kernel<8, false>;
+        case 12: return (void *)gg::bfs_batch_kernel<12, false>;
+        case 16: return (void *)gg::bfs_batch_kernel<16, false>;
+        default: return (void *)gg::bfs_batch_kernel<0, false>;
     }
 }
 

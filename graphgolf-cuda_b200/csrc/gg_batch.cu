@@ -10,6 +10,17 @@
 // folded into per-thread popcounts and one __syncthreads_or per level.  The grid
 // barrier of the single-graph path is not needed: a task never leaves its CTA.
 //
+// Affected sources (default): per base, one pass of the same kernel also writes
+// the base's distance matrix as 4 bit-planes, from which every source's distance
+// sum and eccentricity follow.  A candidate then searches only from the sources
+// its 2-opt can affect (the test of gg_inc.cu: a removed edge between
+// consecutive BFS levels whose deeper end has no other parent, or an added edge
+// between vertices whose distances differ by 2 or more); its result is the base's
+// total minus those sources' old sums plus their new sums, and the larger of their
+// new eccentricities and the others' old ones.  Bases that are not symmetric,
+// not connected or of diameter above 15 (and the histogram pass) search every
+// source.  GG_BATCH_FULL=1 searches every source for every candidate.
+//
 // Task order: t -> chunk = maxchunks-1 - t / n_cand, cand = t % n_cand, so the
 // extra chunks of the largest bases come first and the common chunks fill the
 // tail (largest-first scheduling with no task list on the host).  Both n_cand and
@@ -18,6 +29,7 @@
 #include "gg.h"
 
 #include <algorithm>
+#include <cstdlib>
 #include <cstring>
 #include <string>
 #include <vector>
@@ -33,11 +45,30 @@ namespace {
 constexpr int kBatchBlock = 1024;
 constexpr size_t kSmemBudget = 220 * 1024;
 
+constexpr int kPlanes = 4;   // distance bit-planes: distances up to 15
+
 struct BatchBase {
     const int32_t *adj;   // [n][d] in global memory
     int n, d;
     int log_nc;           // chunks (of 128 sources) per task row = 1 << log_nc
     int chunks;           // tasks per candidate = ceil(n / (128 << log_nc))
+    // affected-source mode (valid != 0)
+    const uint4 *planes;  // [kPlanes][n][cols]: bit k of dist(source, vertex)
+    unsigned cols;        // chunks << log_nc
+    const unsigned *rowsum;  // [n]: distance sum of each source
+    const unsigned *ecc;     // [n]: eccentricity of each source
+    unsigned long long total, reached;  // the base's own counts
+    int levels;
+    int valid;            // symmetric, connected, diameter <= 15
+};
+
+// Per candidate, from the affected-source test.
+struct IncCand {
+    unsigned long long old_sum;   // base distance sums of the affected sources
+    unsigned count;               // affected sources (the candidate's search list)
+    unsigned max_other;           // largest eccentricity among the other sources
+    int full;                     // search every source instead
+    int pad;
 };
 
 struct BatchCtl {
@@ -54,6 +85,11 @@ struct BatchArgs {
     BatchCtl *ctl;
     unsigned *hist;       // nullptr, or [n][hist_k]: per-vertex new pairs at levels 1..hist_k
     int hist_k;           // (only meaningful for a launch of one candidate)
+    IncCand *inc;         // nullptr: every candidate searches every source
+    uint16_t *lists;      // [cand][list_stride]: affected sources
+    int list_stride;
+    uint4 *planes_out;    // nullptr, or the planes of the (single, full) candidate's graph
+    unsigned planes_cols;
 };
 
 __device__ __forceinline__ uint4 z4() { return make_uint4(0u, 0u, 0u, 0u); }
@@ -80,14 +116,17 @@ __global__ void __launch_bounds__(kBatchBlock, 1) batch_kernel(const BatchArgs a
         const int chunk = max_chunks - 1 - (int)(task / (unsigned)n_cand);
         const gg_swap sw = a.cands[cand];
         const BatchBase B = a.bases[sw.base];
-        if (chunk >= B.chunks) {  // this candidate has fewer chunks
+        const int n = B.n, d = B.d, lnc = B.log_nc, nC = 1 << lnc;
+        const int S = 128 << lnc;
+        // sources of this candidate: every vertex, or its affected-source list
+        const bool full = a.inc == nullptr || a.inc[cand].full;
+        const int count = full ? n : (int)a.inc[cand].count;
+        if (chunk * S >= count) {  // this candidate has fewer chunks
             __syncthreads();
             continue;
         }
-        const int n = B.n, d = B.d, lnc = B.log_nc, nC = 1 << lnc;
-        const int S = 128 << lnc;
         const int s0 = chunk * S;
-        const int ns = min(S, n - s0);
+        const int ns = min(S, count - s0);
         const int items = n << lnc;
 
         // shared memory: adjacency (uint16, padded to 16 bytes), then two bitsets
@@ -112,7 +151,7 @@ __global__ void __launch_bounds__(kBatchBlock, 1) batch_kernel(const BatchArgs a
             const int b = c * 128;
             uint4 w = make_uint4(padw(b, ns), padw(b + 32, ns), padw(b + 64, ns), padw(b + 96, ns));
             const int i = v - s0;
-            if (i >= b && i < b + 128 && i < ns) {
+            if (full && i >= b && i < b + 128 && i < ns) {
                 const unsigned bit = 1u << (i & 31);
                 switch ((i - b) >> 5) {
                     case 0: w.x |= bit; break;
@@ -124,6 +163,16 @@ __global__ void __launch_bounds__(kBatchBlock, 1) batch_kernel(const BatchArgs a
             cur[t] = w;
         }
         __syncthreads();
+        if (!full) {
+            // source j of the chunk is vertex lists[s0 + j]
+            const uint16_t *lst = a.lists + (size_t)cand * a.list_stride + s0;
+            for (int j = tid; j < ns; j += kBatchBlock) {
+                const int v = lst[j];
+                atomicOr(reinterpret_cast<unsigned *>(cur + ((v << lnc) + (j >> 7))) + ((j >> 5) & 3),
+                         1u << (j & 31));
+            }
+            __syncthreads();
+        }
 
         unsigned long long tot = 0, reach = 0;
         int L = 1;
@@ -143,6 +192,19 @@ __global__ void __launch_bounds__(kBatchBlock, 1) batch_kernel(const BatchArgs a
                     out = make_uint4(own.x | acc.x, own.y | acc.y, own.z | acc.z, own.w | acc.w);
                     const unsigned pc = __popc(acc.x & ~own.x) + __popc(acc.y & ~own.y) +
                                         __popc(acc.z & ~own.z) + __popc(acc.w & ~own.w);
+                    if (a.planes_out && pc) {
+                        // distance L of this level's new pairs into the planes
+                        const uint4 nb = make_uint4(acc.x & ~own.x, acc.y & ~own.y, acc.z & ~own.z,
+                                                    acc.w & ~own.w);
+                        const size_t pstride = (size_t)n * a.planes_cols;
+                        const size_t pi = (size_t)v * a.planes_cols + (size_t)(chunk << lnc) + c;
+                        for (int k = 0; k < kPlanes; ++k)
+                            if ((L >> k) & 1) {
+                                uint4 *q = a.planes_out + k * pstride + pi;
+                                const uint4 o = *q;
+                                *q = make_uint4(o.x | nb.x, o.y | nb.y, o.z | nb.z, o.w | nb.w);
+                            }
+                    }
                     cnt += pc;
                     if (a.hist && L <= a.hist_k && pc) atomicAdd(a.hist + (size_t)v * a.hist_k + (L - 1), pc);
                 }
@@ -176,15 +238,119 @@ __global__ void batch_finalize(const BatchArgs a) {
     const int n_cand = a.ctl->n_cand;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n_cand; i += gridDim.x * blockDim.x) {
         const BatchBase B = a.bases[a.cands[i].base];
-        a.out[i].connected = a.out[i].reached == (unsigned long long)B.n * (unsigned long long)B.n;
+        gg_cand_result r = a.out[i];
+        if (a.inc && !a.inc[i].full) {
+            // the other sources keep the base's distances
+            const IncCand &ic = a.inc[i];
+            r.total = B.total - ic.old_sum + r.total;
+            r.reached = B.reached - (unsigned long long)ic.count * B.n + r.reached;
+            r.levels = max(r.levels, (int)ic.max_other);
+        }
+        r.connected = r.reached == (unsigned long long)B.n * (unsigned long long)B.n;
+        a.out[i] = r;
     }
 }
 
 __global__ void batch_reset(const BatchArgs a) {
     const int n_cand = a.ctl->n_cand;
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n_cand; i += gridDim.x * blockDim.x)
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n_cand; i += gridDim.x * blockDim.x) {
         a.out[i] = gg_cand_result{0ull, 0ull, 0, 0};
+        if (a.inc) a.inc[i] = IncCand{0ull, 0u, 0u, 0, 0};
+    }
     if (blockIdx.x == 0 && threadIdx.x == 0) a.ctl->task_ctr = 0u;
+}
+
+__device__ __forceinline__ unsigned plane_dist(const uint32_t *pw, size_t pstride_w, unsigned cols4,
+                                               unsigned x, unsigned s) {
+    const size_t base = (size_t)x * cols4 + (s >> 5);
+    unsigned dv = 0;
+#pragma unroll
+    for (int k = 0; k < kPlanes; ++k) dv |= ((__ldg(pw + (size_t)k * pstride_w + base) >> (s & 31u)) & 1u) << k;
+    return dv;
+}
+
+// One thread per (candidate, source): the affected-source test (see the file
+// comment).  Affected sources join the candidate's list with their base
+// distance sums; the others give the largest eccentricity that stays.
+__global__ void batch_affected(const BatchArgs a, int max_n, int force_full) {
+    const int n_cand = a.ctl->n_cand;
+    const unsigned long long total = (unsigned long long)n_cand * (unsigned long long)max_n;
+    const unsigned lane = threadIdx.x & 31u;
+    for (unsigned long long g0 = (unsigned long long)blockIdx.x * blockDim.x; g0 < total;
+         g0 += (unsigned long long)gridDim.x * blockDim.x) {
+        const unsigned long long g = g0 + threadIdx.x;
+        const bool in = g < total;
+        const int cand = in ? (int)(g / (unsigned)max_n) : 0;
+        const int s = in ? (int)(g % (unsigned)max_n) : 0;
+        const gg_swap sw = a.cands[cand];
+        const BatchBase &B = a.bases[sw.base];
+        const bool live = in && s < B.n;
+        bool aff = false, other = false;
+        if (live && (force_full || !B.valid)) {
+            if (s == 0) a.inc[cand].full = 1;
+        } else if (live) {
+            other = true;
+            if (sw.a >= 0) {
+                const uint32_t *pw = reinterpret_cast<const uint32_t *>(B.planes);
+                const size_t psw = (size_t)B.n * B.cols * 4;
+                const unsigned c4 = B.cols * 4;
+                const int ends[2][2] = {{sw.a, sw.b}, {sw.c, sw.d}};
+                for (int e = 0; e < 2 && !aff; ++e) {
+                    const int x = ends[e][0], y = ends[e][1];
+                    const unsigned dx = plane_dist(pw, psw, c4, x, s), dy = plane_dist(pw, psw, c4, y, s);
+                    if (dx == dy) continue;
+                    const int lo = dx < dy ? x : y, hi = dx < dy ? y : x;
+                    const unsigned l = min(dx, dy);
+                    bool par = false, skipped = false;
+                    for (int i = 0; i < B.d && !par; ++i) {
+                        const int z = __ldg(B.adj + (size_t)hi * B.d + i);
+                        if (z == lo && !skipped) { skipped = true; continue; }
+                        par = plane_dist(pw, psw, c4, (unsigned)z, s) == l;
+                    }
+                    aff = !par;
+                }
+                if (!aff) {
+                    const int p = sw.mode ? sw.d : sw.c, q = sw.mode ? sw.c : sw.d;
+                    const unsigned da = plane_dist(pw, psw, c4, sw.a, s), dp = plane_dist(pw, psw, c4, p, s);
+                    const unsigned db = plane_dist(pw, psw, c4, sw.b, s), dq = plane_dist(pw, psw, c4, q, s);
+                    aff = (da > dp ? da - dp : dp - da) >= 2u || (db > dq ? db - dq : dq - db) >= 2u;
+                }
+            }
+            other = !aff;
+        }
+        // one set of atomics per candidate present in the warp
+        const unsigned peers = __match_any_sync(0xffffffffu, live ? cand : -1);
+        const unsigned am = __ballot_sync(0xffffffffu, aff) & peers;
+        const int leader = __ffs((int)peers) - 1;
+        const unsigned rs = __reduce_add_sync(peers, aff ? __ldg(B.rowsum + s) : 0u);
+        const unsigned mx = __reduce_max_sync(peers, other ? __ldg(B.ecc + s) : 0u);
+        unsigned first = 0;
+        if ((int)lane == leader && live) {
+            if (am) {
+                first = atomicAdd(&a.inc[cand].count, (unsigned)__popc(am));
+                atomicAdd(&a.inc[cand].old_sum, (unsigned long long)rs);
+            }
+            atomicMax(&a.inc[cand].max_other, mx);
+        }
+        first = __shfl_sync(0xffffffffu, first, leader);
+        if (aff) a.lists[(size_t)cand * a.list_stride + first + __popc(am & ((1u << lane) - 1u))] = (uint16_t)s;
+    }
+}
+
+// Distance sum and eccentricity of every source of a base, from its planes.
+__global__ void base_source_stats(const uint4 *planes, unsigned cols, int n, unsigned *rowsum, unsigned *ecc) {
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= n) return;
+    const uint32_t *pw = reinterpret_cast<const uint32_t *>(planes);
+    const size_t psw = (size_t)n * cols * 4;
+    unsigned sum = 0, mx = 0;
+    for (int v = 0; v < n; ++v) {
+        const unsigned dv = plane_dist(pw, psw, cols * 4, (unsigned)v, (unsigned)s);
+        sum += dv;
+        mx = max(mx, dv);
+    }
+    rowsum[s] = sum;
+    ecc[s] = mx;
 }
 
 gg_status bfail(gg_status s, const std::string &m) {
@@ -224,6 +390,13 @@ struct gg_batch {
     unsigned *d_hist = nullptr;            // vertex histogram output
     size_t hist_cap = 0;
     double last_ms = 0.0;
+    // affected-source mode
+    bool full_only = false;                // GG_BATCH_FULL=1: every candidate searches every source
+    std::vector<uint4 *> base_planes;      // per base: [kPlanes][n][cols]
+    std::vector<unsigned *> base_stats;    // per base: rowsum[n] then ecc[n]
+    IncCand *d_inc = nullptr;              // [cap]
+    uint16_t *d_lists = nullptr;           // [cap][list_stride]
+    int list_stride = 0;                   // largest base n
 };
 
 namespace {
@@ -271,15 +444,22 @@ gg_status refresh_plan(gg_batch *b) {
 }
 
 gg_status ensure_cap(gg_batch *b, int n) {
-    if (n <= b->cap) return GG_OK;
-    const int cap = std::max(n, 2 * b->cap);
-    cudaFree(b->d_cands); cudaFree(b->d_out);
+    int max_n = 0;
+    for (auto &B : b->bases) max_n = std::max(max_n, B.n);
+    if (n <= b->cap && max_n <= b->list_stride) return GG_OK;
+    const int cap = std::max({n, 2 * b->cap, 1});
+    cudaFree(b->d_cands); cudaFree(b->d_out); cudaFree(b->d_inc); cudaFree(b->d_lists);
     cudaFreeHost(b->h_cands); cudaFreeHost(b->h_out);
     b->d_cands = nullptr; b->d_out = nullptr; b->h_cands = nullptr; b->h_out = nullptr;
+    b->d_inc = nullptr; b->d_lists = nullptr;
+    b->cap = 0;
     GB_CK(cudaMalloc(&b->d_cands, (size_t)cap * sizeof(gg_swap)));
     GB_CK(cudaMalloc(&b->d_out, (size_t)cap * sizeof(gg_cand_result)));
     GB_CK(cudaMallocHost(&b->h_cands, (size_t)cap * sizeof(gg_swap)));
     GB_CK(cudaMallocHost(&b->h_out, (size_t)cap * sizeof(gg_cand_result)));
+    GB_CK(cudaMalloc(&b->d_inc, (size_t)cap * sizeof(IncCand)));
+    b->list_stride = std::max(max_n, 1);
+    GB_CK(cudaMalloc(&b->d_lists, (size_t)cap * b->list_stride * sizeof(uint16_t)));
     b->cap = cap;
     drop_graph(b);
     return GG_OK;
@@ -288,12 +468,82 @@ gg_status ensure_cap(gg_batch *b, int n) {
 // Enqueue reset -> batch kernel -> finalize on `st` for candidates `cands`,
 // results `out`; the candidate count and task geometry come from d_ctl.
 gg_status enqueue(gg_batch *b, const gg_swap *cands, gg_cand_result *out, cudaStream_t st,
-                  unsigned *hist = nullptr, int hist_k = 0) {
-    BatchArgs a{b->d_bases, cands, out, b->d_ctl, hist, hist_k};
+                  unsigned *hist = nullptr, int hist_k = 0, uint4 *planes_out = nullptr,
+                  unsigned planes_cols = 0) {
+    // the histogram and plane passes search every source of their one candidate
+    const bool inc = !hist && !planes_out;
+    BatchArgs a{b->d_bases, cands, out, b->d_ctl, hist, hist_k, inc ? b->d_inc : nullptr,
+                b->d_lists, b->list_stride, planes_out, planes_cols};
     batch_reset<<<64, 256, 0, st>>>(a);
+    if (inc) {
+        const unsigned long long pairs = (unsigned long long)b->cap * b->list_stride;
+        const int g = (int)std::min<unsigned long long>((pairs + 255) / 256, 148ull * 16);
+        batch_affected<<<g, 256, 0, st>>>(a, b->list_stride, b->full_only ? 1 : 0);
+    }
     batch_kernel<<<b->grid, kBatchBlock, b->smem, st>>>(a);
     batch_finalize<<<64, 256, 0, st>>>(a);
     GB_CK(cudaGetLastError());
+    return GG_OK;
+}
+
+bool symmetric(const int32_t *adj, int n, int d) {
+    for (int v = 0; v < n; ++v)
+        for (int k = 0; k < d; ++k) {
+            const int u = adj[(size_t)v * d + k];
+            bool back = false;
+            for (int j = 0; j < d && !back; ++j) back = adj[(size_t)u * d + j] == v;
+            if (!back) return false;
+        }
+    return true;
+}
+
+constexpr int kIncMaxN = 16384;   // larger bases search every source (planes of 4 n^2/8 bytes)
+
+// The base pass of base `id`: its own counts, its distance planes and every
+// source's distance sum and eccentricity (affected-source mode), or valid = 0.
+gg_status base_pass(gg_batch *b, int id, const int32_t *host_adj) {
+    BatchBase &B = b->bases[id];
+    const cudaStream_t st = b->stream;
+    const unsigned cols = (unsigned)(B.chunks << B.log_nc);
+    B.valid = 0;
+    B.cols = cols;
+    const bool want = !b->full_only && B.n <= kIncMaxN && symmetric(host_adj, B.n, B.d);
+    if (want) {
+        const size_t pbytes = (size_t)kPlanes * B.n * cols * sizeof(uint4);
+        if (!b->base_planes[id]) {
+            GB_CK(cudaMalloc(&b->base_planes[id], pbytes));
+            GB_CK(cudaMalloc(&b->base_stats[id], 2 * (size_t)B.n * sizeof(unsigned)));
+        }
+        GB_CK(cudaMemsetAsync(b->base_planes[id], 0, pbytes, st));
+    }
+    gg_status s = ensure_cap(b, 1);
+    if (s != GG_OK) return s;
+    const gg_swap self{id, -1, -1, -1, -1, 0};
+    b->h_cands[0] = self;
+    b->h_ctl->n_cand = 1;
+    b->h_ctl->task_ctr = 0;
+    GB_CK(cudaMemcpyAsync(b->d_cands, b->h_cands, sizeof(gg_swap), cudaMemcpyHostToDevice, st));
+    GB_CK(cudaMemcpyAsync(b->d_ctl, b->h_ctl, sizeof(BatchCtl), cudaMemcpyHostToDevice, st));
+    s = enqueue(b, b->d_cands, b->d_out, st, nullptr, 0, want ? b->base_planes[id] : nullptr, cols);
+    if (s != GG_OK) return s;
+    if (want) {
+        base_source_stats<<<(B.n + 255) / 256, 256, 0, st>>>(b->base_planes[id], cols, B.n, b->base_stats[id],
+                                                              b->base_stats[id] + B.n);
+        GB_CK(cudaGetLastError());
+    }
+    GB_CK(cudaMemcpyAsync(b->h_out, b->d_out, sizeof(gg_cand_result), cudaMemcpyDeviceToHost, st));
+    GB_CK(cudaStreamSynchronize(st));
+    const gg_cand_result r = b->h_out[0];
+    B.total = r.total;
+    B.reached = r.reached;
+    B.levels = r.levels;
+    if (want && r.connected && r.levels < (1 << kPlanes)) {
+        B.valid = 1;
+        B.planes = b->base_planes[id];
+        B.rowsum = b->base_stats[id];
+        B.ecc = b->base_stats[id] + B.n;
+    }
+    GB_CK(cudaMemcpy(b->d_bases + id, &B, sizeof(BatchBase), cudaMemcpyHostToDevice));
     return GG_OK;
 }
 
@@ -334,6 +584,8 @@ gg_status gg_batch_create(int device, gg_batch **out) {
         cudaMalloc(&b->d_bases, 256 * sizeof(BatchBase)) != cudaSuccess)
         return fail_and_free(bfail(GG_CUDA_ERROR, "batch set-up failed"));
     std::memset(b->h_ctl, 0, sizeof(BatchCtl));
+    const char *f = std::getenv("GG_BATCH_FULL");
+    b->full_only = f && std::atoi(f) != 0;
     *out = b;
     return GG_OK;
 }
@@ -349,11 +601,18 @@ gg_status gg_batch_add_base(gg_batch *b, int n, int degree, const int32_t *adj, 
     int32_t *d = nullptr;
     GB_CK(cudaMalloc(&d, (size_t)n * degree * sizeof(int32_t)));
     GB_CK(cudaMemcpy(d, adj, (size_t)n * degree * sizeof(int32_t), cudaMemcpyHostToDevice));
-    BatchBase B{d, n, degree, lnc, (n + (128 << lnc) - 1) / (128 << lnc)};
+    BatchBase B{};
+    B.adj = d; B.n = n; B.d = degree; B.log_nc = lnc; B.chunks = (n + (128 << lnc) - 1) / (128 << lnc);
     b->bases.push_back(B);
     b->base_adj.push_back(d);
-    *base_id = (int)b->bases.size() - 1;
-    return refresh_plan(b);
+    b->base_planes.push_back(nullptr);
+    b->base_stats.push_back(nullptr);
+    const int id = (int)b->bases.size() - 1;
+    gg_status s = refresh_plan(b);
+    if (s == GG_OK) s = base_pass(b, id, adj);
+    if (s != GG_OK) return s;
+    *base_id = id;
+    return GG_OK;
 }
 
 gg_status gg_batch_set_base(gg_batch *b, int base_id, const int32_t *adj) {
@@ -366,8 +625,7 @@ gg_status gg_batch_set_base(gg_batch *b, int base_id, const int32_t *adj) {
     // ordered on the batch stream: launches already enqueued see the old table
     GB_CK(cudaMemcpyAsync(b->base_adj[base_id], adj, (size_t)B.n * B.d * sizeof(int32_t),
                           cudaMemcpyHostToDevice, b->stream));
-    GB_CK(cudaStreamSynchronize(b->stream));
-    return GG_OK;
+    return base_pass(b, base_id, adj);
 }
 
 gg_status gg_batch_set_chunk(gg_batch *b, int base_id, int sources) {
@@ -382,7 +640,14 @@ gg_status gg_batch_set_chunk(gg_batch *b, int base_id, int sources) {
     B.log_nc = l;
     B.chunks = (B.n + (128 << l) - 1) / (128 << l);
     GB_CK(cudaSetDevice(b->device));
-    return refresh_plan(b);
+    gg_status s = refresh_plan(b);
+    if (s != GG_OK) return s;
+    // the planes' column count follows the chunk width: rebuild them
+    cudaFree(b->base_planes[base_id]); cudaFree(b->base_stats[base_id]);
+    b->base_planes[base_id] = nullptr; b->base_stats[base_id] = nullptr;
+    std::vector<int32_t> host((size_t)B.n * B.d);
+    GB_CK(cudaMemcpy(host.data(), b->base_adj[base_id], host.size() * sizeof(int32_t), cudaMemcpyDeviceToHost));
+    return base_pass(b, base_id, host.data());
 }
 
 gg_status gg_batch_eval(gg_batch *b, int n_cand, const gg_swap *cands, gg_cand_result *out) {
@@ -428,6 +693,8 @@ gg_status gg_batch_eval_device(gg_batch *b, int n_cand, const gg_swap *d_cands,
     if (n_cand == 0) return GG_OK;
     GB_CK(cudaSetDevice(b->device));
     cudaStream_t st = stream ? (cudaStream_t)stream : b->stream;
+    gg_status cs = ensure_cap(b, n_cand);   // per-candidate lists of the affected-source mode
+    if (cs != GG_OK) return cs;
     b->h_ctl->n_cand = n_cand;
     b->h_ctl->task_ctr = 0;
     GB_CK(cudaMemcpyAsync(b->d_ctl, b->h_ctl, sizeof(BatchCtl), cudaMemcpyHostToDevice, st));
@@ -487,6 +754,9 @@ gg_status gg_batch_destroy(gg_batch *b) {
     if (b->stream) cudaStreamSynchronize(b->stream);
     drop_graph(b);
     for (auto p : b->base_adj) cudaFree(p);
+    for (auto p : b->base_planes) cudaFree(p);
+    for (auto p : b->base_stats) cudaFree(p);
+    cudaFree(b->d_inc); cudaFree(b->d_lists);
     cudaFree(b->d_bases); cudaFree(b->d_ctl); cudaFreeHost(b->h_ctl);
     cudaFree(b->d_cands); cudaFree(b->d_out); cudaFreeHost(b->h_cands); cudaFreeHost(b->h_out);
     cudaFree(b->d_hist);

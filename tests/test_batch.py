@@ -100,3 +100,44 @@ def test_batch_rejects_bad_candidates():
     sw[0]["base"] = 7
     with pytest.raises(G.GGError):
         b.eval(sw)
+
+
+@pytest.mark.gpu
+def test_affected_source_mode_equals_full_search(monkeypatch):
+    """Default mode (each candidate searches only the sources its 2-opt can
+    affect) against GG_BATCH_FULL=1 (every source), on bases that use it and on
+    bases that fall back: diameter above the planes, a one-way table."""
+    rng = np.random.default_rng(5)
+    g_reg = G.random_regular(1024, 6, 31)
+    g_sm = G.random_regular(3000, 4, 32)
+    g_nr, _ = I.random_nonregular(700, 5, 33)
+    g_cyc = np.asarray(I.cycle(200), dtype=np.int32)             # diameter 100
+    g_dir = rng.integers(0, 300, size=(300, 3)).astype(np.int32)   # one-way entries
+    g_dir[:, 0] = (np.arange(300) + 1) % 300
+    bases = [g_reg, g_sm, g_nr, g_cyc, g_dir]
+
+    def run():
+        b = G.Batch(0)
+        ids = [b.add_base(g) for g in bases]
+        sw = [G.gen_swaps(g, i, 40, 50 + i) for g, i in zip(bases[:4], ids[:4])]
+        none = np.zeros(len(ids), dtype=G.SWAP_DTYPE)
+        none["base"] = ids
+        none["a"] = -1
+        allsw = np.concatenate(sw + [none])
+        r1 = b.eval(allsw)
+        # a new current graph for one base, then the same candidates again
+        b.set_base(ids[0], G.apply_swap(g_reg, sw[0][0]))
+        r2 = b.eval(allsw[40:])
+        b.close()
+        return allsw, r1, r2
+
+    monkeypatch.delenv("GG_BATCH_FULL", raising=False)
+    allsw, inc1, inc2 = run()
+    monkeypatch.setenv("GG_BATCH_FULL", "1")
+    _, full1, full2 = run()
+    assert np.array_equal(inc1, full1) and np.array_equal(inc2, full2)
+    for k in rng.choice(len(allsw), 15, replace=False):
+        s = allsw[k]
+        want = exact(G.apply_swap(bases[s["base"]], s))
+        got = inc1[k]
+        assert (int(got["total"]), int(got["reached"]), bool(got["connected"])) == (want[0], want[1], want[3])

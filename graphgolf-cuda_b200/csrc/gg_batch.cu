@@ -27,6 +27,7 @@
 // maxchunks are read from device memory, so one captured CUDA graph serves every
 // batch size up to the capacity it was captured for.
 #include "gg.h"
+#include "gg_internal.h"
 
 #include <algorithm>
 #include <cstdlib>
@@ -36,9 +37,6 @@
 
 #include <cuda_runtime.h>
 
-namespace gg {
-void set_last_error(const char *msg);  // gg_engine.cu
-}
 
 namespace {
 
@@ -88,8 +86,6 @@ struct BatchArgs {
     IncCand *inc;         // nullptr: every candidate searches every source
     uint16_t *lists;      // [cand][list_stride]: affected sources
     int list_stride;
-    uint4 *planes_out;    // nullptr, or the planes of the (single, full) candidate's graph
-    unsigned planes_cols;
 };
 
 __device__ __forceinline__ uint4 z4() { return make_uint4(0u, 0u, 0u, 0u); }
@@ -192,19 +188,6 @@ __global__ void __launch_bounds__(kBatchBlock, 1) batch_kernel(const BatchArgs a
                     out = make_uint4(own.x | acc.x, own.y | acc.y, own.z | acc.z, own.w | acc.w);
                     const unsigned pc = __popc(acc.x & ~own.x) + __popc(acc.y & ~own.y) +
                                         __popc(acc.z & ~own.z) + __popc(acc.w & ~own.w);
-                    if (a.planes_out && pc) {
-                        // distance L of this level's new pairs into the planes
-                        const uint4 nb = make_uint4(acc.x & ~own.x, acc.y & ~own.y, acc.z & ~own.z,
-                                                    acc.w & ~own.w);
-                        const size_t pstride = (size_t)n * a.planes_cols;
-                        const size_t pi = (size_t)v * a.planes_cols + (size_t)(chunk << lnc) + c;
-                        for (int k = 0; k < kPlanes; ++k)
-                            if ((L >> k) & 1) {
-                                uint4 *q = a.planes_out + k * pstride + pi;
-                                const uint4 o = *q;
-                                *q = make_uint4(o.x | nb.x, o.y | nb.y, o.z | nb.z, o.w | nb.w);
-                            }
-                    }
                     cnt += pc;
                     if (a.hist && L <= a.hist_k && pc) atomicAdd(a.hist + (size_t)v * a.hist_k + (L - 1), pc);
                 }
@@ -338,19 +321,39 @@ __global__ void batch_affected(const BatchArgs a, int max_n, int force_full) {
 }
 
 // Distance sum and eccentricity of every source of a base, from its planes.
-__global__ void base_source_stats(const uint4 *planes, unsigned cols, int n, unsigned *rowsum, unsigned *ecc) {
-    const int s = blockIdx.x * blockDim.x + threadIdx.x;
-    if (s >= n) return;
+// One block per 32-bit word of sources (lane = source); its 32 warps split the
+// vertices, so each plane word is one broadcast load for a warp.
+constexpr int kStatsBlock = 1024;
+__global__ void __launch_bounds__(kStatsBlock) base_source_stats(const uint4 *planes, unsigned cols, int n,
+                                                                 unsigned *rowsum, unsigned *ecc) {
+    __shared__ unsigned s_sum[kStatsBlock / 32][32], s_max[kStatsBlock / 32][32];
+    const unsigned lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+    const unsigned word = blockIdx.x;
     const uint32_t *pw = reinterpret_cast<const uint32_t *>(planes);
     const size_t psw = (size_t)n * cols * 4;
     unsigned sum = 0, mx = 0;
-    for (int v = 0; v < n; ++v) {
-        const unsigned dv = plane_dist(pw, psw, cols * 4, (unsigned)v, (unsigned)s);
+    for (unsigned v = warp; v < (unsigned)n; v += kStatsBlock / 32) {
+        const size_t base = (size_t)v * cols * 4 + word;
+        unsigned dv = 0;
+#pragma unroll
+        for (int k = 0; k < kPlanes; ++k) dv |= ((__ldg(pw + (size_t)k * psw + base) >> lane) & 1u) << k;
         sum += dv;
         mx = max(mx, dv);
     }
-    rowsum[s] = sum;
-    ecc[s] = mx;
+    s_sum[warp][lane] = sum;
+    s_max[warp][lane] = mx;
+    __syncthreads();
+    if (warp == 0) {
+        for (int w = 1; w < kStatsBlock / 32; ++w) {
+            sum += s_sum[w][lane];
+            mx = max(mx, s_max[w][lane]);
+        }
+        const unsigned s = word * 32u + lane;
+        if (s < (unsigned)n) {
+            rowsum[s] = sum;
+            ecc[s] = mx;
+        }
+    }
 }
 
 gg_status bfail(gg_status s, const std::string &m) {
@@ -394,6 +397,8 @@ struct gg_batch {
     bool full_only = false;                // GG_BATCH_FULL=1: every candidate searches every source
     std::vector<uint4 *> base_planes;      // per base: [kPlanes][n][cols]
     std::vector<unsigned *> base_stats;    // per base: rowsum[n] then ecc[n]
+    std::vector<std::pair<std::pair<int, int>, gg_engine *>> engines;  // per (n, degree): base passes
+    int *d_flag = nullptr, *h_flag = nullptr;
     IncCand *d_inc = nullptr;              // [cap]
     uint16_t *d_lists = nullptr;           // [cap][list_stride]
     int list_stride = 0;                   // largest base n
@@ -468,12 +473,11 @@ gg_status ensure_cap(gg_batch *b, int n) {
 // Enqueue reset -> batch kernel -> finalize on `st` for candidates `cands`,
 // results `out`; the candidate count and task geometry come from d_ctl.
 gg_status enqueue(gg_batch *b, const gg_swap *cands, gg_cand_result *out, cudaStream_t st,
-                  unsigned *hist = nullptr, int hist_k = 0, uint4 *planes_out = nullptr,
-                  unsigned planes_cols = 0) {
-    // the histogram and plane passes search every source of their one candidate
-    const bool inc = !hist && !planes_out;
+                  unsigned *hist = nullptr, int hist_k = 0) {
+    // the histogram pass searches every source of its one candidate
+    const bool inc = !hist;
     BatchArgs a{b->d_bases, cands, out, b->d_ctl, hist, hist_k, inc ? b->d_inc : nullptr,
-                b->d_lists, b->list_stride, planes_out, planes_cols};
+                b->d_lists, b->list_stride};
     batch_reset<<<64, 256, 0, st>>>(a);
     if (inc) {
         const unsigned long long pairs = (unsigned long long)b->cap * b->list_stride;
@@ -486,64 +490,72 @@ gg_status enqueue(gg_batch *b, const gg_swap *cands, gg_cand_result *out, cudaSt
     return GG_OK;
 }
 
-bool symmetric(const int32_t *adj, int n, int d) {
-    for (int v = 0; v < n; ++v)
-        for (int k = 0; k < d; ++k) {
-            const int u = adj[(size_t)v * d + k];
-            bool back = false;
-            for (int j = 0; j < d && !back; ++j) back = adj[(size_t)u * d + j] == v;
-            if (!back) return false;
-        }
-    return true;
+// 1 into *asym when some entry u of row v has no entry v in row u.
+__global__ void base_symmetry(const int32_t *adj, int n, int d, int *asym) {
+    const long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= (long long)n * d) return;
+    const int v = (int)(k / d), u = adj[k];
+    bool back = false;
+    for (int j = 0; j < d && !back; ++j) back = adj[(size_t)u * d + j] == v;
+    if (!back) *asym = 1;
 }
 
 constexpr int kIncMaxN = 16384;   // larger bases search every source (planes of 4 n^2/8 bytes)
 
-// The base pass of base `id`: its own counts, its distance planes and every
-// source's distance sum and eccentricity (affected-source mode), or valid = 0.
-gg_status base_pass(gg_batch *b, int id, const int32_t *host_adj) {
+// The base pass of base `id` (affected-source mode): the single-graph engine
+// evaluates the base with its distance planes (at most 16 levels), then every
+// source's distance sum and eccentricity follow from the planes.  valid = 0
+// (every candidate of the base searches every source) unless the base is
+// symmetric, connected and of diameter <= 15.
+gg_status base_pass(gg_batch *b, int id) {
     BatchBase &B = b->bases[id];
     const cudaStream_t st = b->stream;
-    const unsigned cols = (unsigned)(B.chunks << B.log_nc);
     B.valid = 0;
-    B.cols = cols;
-    const bool want = !b->full_only && B.n <= kIncMaxN && symmetric(host_adj, B.n, B.d);
-    if (want) {
-        const size_t pbytes = (size_t)kPlanes * B.n * cols * sizeof(uint4);
+    if (!b->full_only && B.n <= kIncMaxN) {
+        gg_engine *eng = nullptr;
+        for (auto &pe : b->engines)
+            if (pe.first == std::make_pair(B.n, B.d)) eng = pe.second;
+        if (!eng) {
+            gg_status s = gg_graph_create(B.n, B.d, b->device, &eng);
+            if (s != GG_OK) return s;
+            b->engines.push_back({{B.n, B.d}, eng});
+            GB_CK(cudaSetDevice(b->device));
+        }
         if (!b->base_planes[id]) {
-            GB_CK(cudaMalloc(&b->base_planes[id], pbytes));
+            B.cols = (unsigned)gg::engine_plane_cols(eng);
+            GB_CK(cudaMalloc(&b->base_planes[id], (size_t)kPlanes * B.n * B.cols * sizeof(uint4)));
             GB_CK(cudaMalloc(&b->base_stats[id], 2 * (size_t)B.n * sizeof(unsigned)));
         }
-        GB_CK(cudaMemsetAsync(b->base_planes[id], 0, pbytes, st));
-    }
-    gg_status s = ensure_cap(b, 1);
-    if (s != GG_OK) return s;
-    const gg_swap self{id, -1, -1, -1, -1, 0};
-    b->h_cands[0] = self;
-    b->h_ctl->n_cand = 1;
-    b->h_ctl->task_ctr = 0;
-    GB_CK(cudaMemcpyAsync(b->d_cands, b->h_cands, sizeof(gg_swap), cudaMemcpyHostToDevice, st));
-    GB_CK(cudaMemcpyAsync(b->d_ctl, b->h_ctl, sizeof(BatchCtl), cudaMemcpyHostToDevice, st));
-    s = enqueue(b, b->d_cands, b->d_out, st, nullptr, 0, want ? b->base_planes[id] : nullptr, cols);
-    if (s != GG_OK) return s;
-    if (want) {
-        base_source_stats<<<(B.n + 255) / 256, 256, 0, st>>>(b->base_planes[id], cols, B.n, b->base_stats[id],
-                                                              b->base_stats[id] + B.n);
+        GB_CK(cudaMemsetAsync(b->d_flag, 0, sizeof(int), st));
+        const long long ent = (long long)B.n * B.d;
+        base_symmetry<<<(int)((ent + 255) / 256), 256, 0, st>>>(b->base_adj[id], B.n, B.d, b->d_flag);
         GB_CK(cudaGetLastError());
+        gg_eval_opts o{};
+        o.max_levels = 1 << kPlanes;      // a base that needs more levels searches every source
+        gg::EvalExtra x;
+        x.planes = b->base_planes[id];
+        x.nplanes = kPlanes;
+        x.no_graph = true;
+        gg_result r{};
+        gg_status s = gg::engine_eval(eng, b->base_adj[id], &o, &r, st, &x);
+        if (s != GG_OK) return s;
+        base_source_stats<<<(B.n + 31) / 32, kStatsBlock, 0, st>>>(b->base_planes[id], B.cols, B.n,
+                                                                   b->base_stats[id], b->base_stats[id] + B.n);
+        GB_CK(cudaGetLastError());
+        GB_CK(cudaMemcpyAsync(b->h_flag, b->d_flag, sizeof(int), cudaMemcpyDeviceToHost, st));
+        GB_CK(cudaStreamSynchronize(st));
+        if (!*b->h_flag && r.connected && !r.capped && r.levels < (1 << kPlanes)) {
+            B.valid = 1;
+            B.total = r.total;
+            B.reached = r.reached;
+            B.levels = r.levels;
+            B.planes = b->base_planes[id];
+            B.rowsum = b->base_stats[id];
+            B.ecc = b->base_stats[id] + B.n;
+        }
     }
-    GB_CK(cudaMemcpyAsync(b->h_out, b->d_out, sizeof(gg_cand_result), cudaMemcpyDeviceToHost, st));
+    GB_CK(cudaMemcpyAsync(b->d_bases + id, &B, sizeof(BatchBase), cudaMemcpyHostToDevice, st));
     GB_CK(cudaStreamSynchronize(st));
-    const gg_cand_result r = b->h_out[0];
-    B.total = r.total;
-    B.reached = r.reached;
-    B.levels = r.levels;
-    if (want && r.connected && r.levels < (1 << kPlanes)) {
-        B.valid = 1;
-        B.planes = b->base_planes[id];
-        B.rowsum = b->base_stats[id];
-        B.ecc = b->base_stats[id] + B.n;
-    }
-    GB_CK(cudaMemcpy(b->d_bases + id, &B, sizeof(BatchBase), cudaMemcpyHostToDevice));
     return GG_OK;
 }
 
@@ -581,7 +593,9 @@ gg_status gg_batch_create(int device, gg_batch **out) {
         cudaEventCreate(&b->ev0) != cudaSuccess || cudaEventCreate(&b->ev1) != cudaSuccess ||
         cudaMalloc(&b->d_ctl, sizeof(BatchCtl)) != cudaSuccess ||
         cudaMallocHost(&b->h_ctl, sizeof(BatchCtl)) != cudaSuccess ||
-        cudaMalloc(&b->d_bases, 256 * sizeof(BatchBase)) != cudaSuccess)
+        cudaMalloc(&b->d_bases, 256 * sizeof(BatchBase)) != cudaSuccess ||
+        cudaMalloc(&b->d_flag, sizeof(int)) != cudaSuccess ||
+        cudaMallocHost(&b->h_flag, sizeof(int)) != cudaSuccess)
         return fail_and_free(bfail(GG_CUDA_ERROR, "batch set-up failed"));
     std::memset(b->h_ctl, 0, sizeof(BatchCtl));
     const char *f = std::getenv("GG_BATCH_FULL");
@@ -609,7 +623,7 @@ gg_status gg_batch_add_base(gg_batch *b, int n, int degree, const int32_t *adj, 
     b->base_stats.push_back(nullptr);
     const int id = (int)b->bases.size() - 1;
     gg_status s = refresh_plan(b);
-    if (s == GG_OK) s = base_pass(b, id, adj);
+    if (s == GG_OK) s = base_pass(b, id);
     if (s != GG_OK) return s;
     *base_id = id;
     return GG_OK;
@@ -625,7 +639,7 @@ gg_status gg_batch_set_base(gg_batch *b, int base_id, const int32_t *adj) {
     // ordered on the batch stream: launches already enqueued see the old table
     GB_CK(cudaMemcpyAsync(b->base_adj[base_id], adj, (size_t)B.n * B.d * sizeof(int32_t),
                           cudaMemcpyHostToDevice, b->stream));
-    return base_pass(b, base_id, adj);
+    return base_pass(b, base_id);
 }
 
 gg_status gg_batch_set_chunk(gg_batch *b, int base_id, int sources) {
@@ -640,14 +654,7 @@ gg_status gg_batch_set_chunk(gg_batch *b, int base_id, int sources) {
     B.log_nc = l;
     B.chunks = (B.n + (128 << l) - 1) / (128 << l);
     GB_CK(cudaSetDevice(b->device));
-    gg_status s = refresh_plan(b);
-    if (s != GG_OK) return s;
-    // the planes' column count follows the chunk width: rebuild them
-    cudaFree(b->base_planes[base_id]); cudaFree(b->base_stats[base_id]);
-    b->base_planes[base_id] = nullptr; b->base_stats[base_id] = nullptr;
-    std::vector<int32_t> host((size_t)B.n * B.d);
-    GB_CK(cudaMemcpy(host.data(), b->base_adj[base_id], host.size() * sizeof(int32_t), cudaMemcpyDeviceToHost));
-    return base_pass(b, base_id, host.data());
+    return refresh_plan(b);
 }
 
 gg_status gg_batch_eval(gg_batch *b, int n_cand, const gg_swap *cands, gg_cand_result *out) {
@@ -756,7 +763,9 @@ gg_status gg_batch_destroy(gg_batch *b) {
     for (auto p : b->base_adj) cudaFree(p);
     for (auto p : b->base_planes) cudaFree(p);
     for (auto p : b->base_stats) cudaFree(p);
+    for (auto &pe : b->engines) gg_destroy(pe.second);
     cudaFree(b->d_inc); cudaFree(b->d_lists);
+    cudaFree(b->d_flag); cudaFreeHost(b->h_flag);
     cudaFree(b->d_bases); cudaFree(b->d_ctl); cudaFreeHost(b->h_ctl);
     cudaFree(b->d_cands); cudaFree(b->d_out); cudaFreeHost(b->h_cands); cudaFreeHost(b->h_out);
     cudaFree(b->d_hist);

@@ -245,7 +245,7 @@ constexpr int kGrab = GG_GRAB;  // tiles a warp takes (and keeps in flight) at o
 // One level's work on tiles [tile0, tile0 + U) of the calling warp (a tile is 32
 // consecutive uint4 chunks, one per lane).  Every load of the U tiles is issued
 // before any result is used, so each warp keeps U*(d+1) 16-byte loads in flight.
-template <int D, int U>
+template <int D, int U, bool PL>
 __device__ __forceinline__ void level_tiles(const BfsArgs &a, const int d, const int32_t *adj,
                                             const unsigned v_base, const unsigned tile0,
                                             const unsigned t_hi, const uint4 *Fc, uint4 *Fn,
@@ -326,6 +326,18 @@ __device__ __forceinline__ void level_tiles(const BfsArgs &a, const int d, const
                 if (u4any(nw[u])) a.V[t[u]] = u4or(own[u], nw[u]);
             }
             if (write_all || u4any(nw[u])) Fn[t[u]] = nw[u];
+            if constexpr (PL) {
+                // distance L of the new pairs into the planes (one writer per chunk)
+                if (u4any(nw[u])) {
+                    const PlaneOut &po = plane_slot();
+                    const size_t pi = (size_t)a.div_nc.div(t[u]) * po.cols + po.col0 + c[u];
+                    for (int p = 0; p < po.nplanes; ++p)
+                        if ((po.L >> p) & 1) {
+                            uint4 *q = po.planes + (size_t)p * po.stride + pi;
+                            *q = u4or(*q, nw[u]);
+                        }
+                }
+            }
             if (a.masks) {
                 and_pre &= u4and(own[u]);
                 and_post &= u4and(u4or(own[u], nw[u]));
@@ -437,29 +449,6 @@ static __device__ __noinline__ void clear_push_buffer(uint4 *P, uint32_t *pf, co
             P[k * 32u + b] = u4zero();
         } while (m);
         pf[k] = 0u;
-    }
-}
-
-// After pull level po.L: OR the level's new pairs (the chunks flagged in `fn`,
-// their bits in `Fn`) into the distance planes.  One warp per flag word, one lane
-// per chunk (coalesced); each chunk has one writer.
-static __device__ __noinline__ void plane_pass(const uint32_t *fn, const uint4 *Fn, const FastDiv div_nc,
-                                               const unsigned nC, const unsigned fwords,
-                                               const unsigned gtid, const unsigned nthr) {
-    const PlaneOut po = plane_slot();
-    const unsigned lane = threadIdx.x & 31u;
-    for (unsigned k = gtid >> 5; k < fwords; k += nthr >> 5) {
-        const unsigned m = __ldcg(fn + k);
-        if (!((m >> lane) & 1u)) continue;
-        const unsigned t = k * 32u + lane;
-        const uint4 nw = __ldcg(Fn + t);
-        const unsigned v = div_nc.div(t), c = t - v * nC;
-        const size_t pi = (size_t)v * po.cols + po.col0 + c;
-        for (int p = 0; p < po.nplanes; ++p)
-            if ((po.L >> p) & 1) {
-                uint4 *q = po.planes + (size_t)p * po.stride + pi;
-                *q = u4or(*q, nw);
-            }
     }
 }
 
@@ -692,7 +681,7 @@ __global__ void __launch_bounds__(kBlock, min_blocks_for(D)) bfs_batch_kernel(co
                         if (my < t_hi && w == 0u) fn[my] = 0u;
                         for (unsigned todo = __ballot_sync(0xffffffffu, w != 0u); todo; todo &= todo - 1u) {
                             const unsigned tj = tile0 + (unsigned)(__ffs((int)todo) - 1);
-                            level_tiles<D, 1>(a, d, adj, v_base, tj, t_hi, Fc, Fn, fc, fn, dense, write_all,
+                            level_tiles<D, 1, PL>(a, d, adj, v_base, tj, t_hi, Fc, Fn, fc, fn, dense, write_all,
                                               skip_full, split, lane, cnt, and_pre, and_post);
                         }
                     }
@@ -702,7 +691,7 @@ __global__ void __launch_bounds__(kBlock, min_blocks_for(D)) bfs_batch_kernel(co
                         if (lane == 0) tile0 = atomicAdd(&s_next, (unsigned)kGrab);
                         tile0 = __shfl_sync(0xffffffffu, tile0, 0);
                         if (tile0 >= t_hi) break;
-                        level_tiles<D, kGrab>(a, d, adj, v_base, tile0, t_hi, Fc, Fn, fc, fn, dense,
+                        level_tiles<D, kGrab, PL>(a, d, adj, v_base, tile0, t_hi, Fc, Fn, fc, fn, dense,
                                               write_all, skip_full, split, lane, cnt, and_pre,
                                               and_post);
                     }
@@ -732,16 +721,6 @@ __global__ void __launch_bounds__(kBlock, min_blocks_for(D)) bfs_batch_kernel(co
                 }
             }
             if (!grid_sync(a.ctl, a.expected, a.wait_ns, L, epoch)) return;
-            if constexpr (PL) {
-                if (!push) {
-                    // distances of this level's new pairs into the planes; the barrier
-                    // keeps the frontier buffer unchanged until every block is done
-                    const bool odd = (L & 1) != 0;
-                    plane_pass(odd ? a.fl1 : a.fl0, odd ? a.F1 : a.F0, a.div_nc, (unsigned)a.nC, ntiles,
-                               gtid, nthr);
-                    if (!grid_sync(a.ctl, a.expected, a.wait_ns, L, epoch)) return;
-                }
-            }
             if (b == 0 && a.level_ns && gtid == 0) a.level_ns[L] = gtimer();
             if (threadIdx.x == 0) {
                 const unsigned long long cL = ld_relaxed_u64(counts + L);

@@ -339,6 +339,7 @@ def run_ours(args):
                        "level_steps": r["level_steps"], "diameter": r["levels"],
                        "parallelism": f"replicas{world}" if world > 1 else "single",
                        "batch_sources": -(-r["n_sources"] // r["batches"]),
+                       "bit_edge_traversals_per_s": bit_edges_per_eval(wl, r) * args.steps / (elapsed_ms / 1000.0),
                        "l2": "flushed (256 MiB write) before every timed step; steps timed by their own CUDA event pairs"},
             "e2e": {"value": world * e2e_steps / e2e_s, "unit": UNIT,
                     "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
@@ -400,7 +401,8 @@ def run_anneal(args):
     _, plain = A.anneal(adj, steps, seed=w["seed"], exact=32, device=local)
     target = plain.final_best
     t_plain = A.time_to(plain, target)
-    _, sur = A.anneal(adj, steps, seed=w["seed"], exact=32, surrogate=True, target=target, device=local)
+    _, sur = A.anneal(adj, steps, seed=w["seed"], exact=32, surrogate=True, target=target, device=local,
+                      spearman_sample=2048)
     line = {"metric": "ASPL time-to-target, plain / surrogate", "value":
             (t_plain / sur.hit_time) if sur.hit_time else None, "unit": "x", "n_gpus": world,
             "steps": steps, "warmup": 1, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
@@ -410,10 +412,19 @@ def run_anneal(args):
             "plain": {"wall_s": plain.wall, "time_to_final_s": t_plain, "steps": plain.steps,
                       "start_aspl": plain.best[0], "final_aspl": target, "ms_per_step": 1000 * plain.wall / plain.steps},
             "surrogate": {"hit_s": sur.hit_time, "hit_step": sur.hit_step, "final_aspl": sur.final_best,
-                          "train_pairs": sur.train_pairs, "ms_per_step": 1000 * sur.wall / max(sur.steps, 1)}}
+                          "train_pairs": sur.train_pairs, "ms_per_step": 1000 * sur.wall / max(sur.steps, 1),
+                          "spearman_predicted_vs_exact": sur.spearman,
+                          "spearman_sample": "2048 uniform 2-opt proposals of the final graph, after the timed run"}}
     if rank == 0:
         print(json.dumps(line), flush=True)
     return 0
+
+
+def bit_edges_per_eval(wl, r):
+    """Survey measure: sum over executed levels of N * d * S (S = sources of the
+    batch), for an evaluation with all batches of equal width."""
+    S = -(-r["n_sources"] // r["batches"])
+    return r["level_steps"] * wl["N"] * wl["d"] * S
 
 
 def run_incremental(args):

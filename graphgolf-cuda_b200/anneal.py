@@ -50,11 +50,29 @@ class Trace:
     final_best: float = math.inf
     hit_time: float | None = None                  # wall seconds when best <= target
     hit_step: int | None = None
+    spearman: float | None = None                  # surrogate: rank correlation on a fresh sample
+
+
+def rank_correlation(x, y):
+    """Spearman rank correlation (average ranks for ties)."""
+    def ranks(v):
+        v = np.asarray(v, dtype=np.float64)
+        order = np.argsort(v, kind="stable")
+        r = np.empty(len(v))
+        r[order] = np.arange(len(v), dtype=np.float64)
+        _, inv, cnt = np.unique(v, return_inverse=True, return_counts=True)
+        sums = np.bincount(inv, weights=r)
+        return (sums / cnt)[inv]
+    rx, ry = ranks(x), ranks(y)
+    rx -= rx.mean()
+    ry -= ry.mean()
+    den = math.sqrt(float((rx * rx).sum() * (ry * ry).sum()))
+    return float((rx * ry).sum() / den) if den > 0 else 0.0
 
 
 def anneal(adj0, steps, *, seed=1, exact=32, pool=4096, explore=8, surrogate=False, t0_frac=1e-3,
            t_end=1e-6, target=None, time_limit=None, lr=2e-3, feature_every=32, train_every=2,
-           device=0):
+           device=0, spearman_sample=0):
     """Anneal from `adj0` (n x d simple regular graph).  Returns (best_adj, Trace).
     With the surrogate, the adjacency it passes messages over follows every
     accepted move; its distance-histogram features are recomputed every
@@ -144,6 +162,15 @@ def anneal(adj0, steps, *, seed=1, exact=32, pool=4096, explore=8, surrogate=Fal
             break
     tr.wall = time.perf_counter() - t_start
     tr.final_best = best_aspl
+    if net is not None and spearman_sample > 0:
+        # after the timed run: predicted vs exact change of the total on a fresh
+        # uniform sample of proposals of the final graph
+        cand = G.gen_swaps(adj, bid, spearman_sample, (seed << 32) ^ 0x5eed)
+        pred = net.predict(cand)
+        r = b.eval(cand)
+        ok = r["connected"] == 1
+        if ok.sum() > 2:
+            tr.spearman = rank_correlation(pred[ok], r["total"][ok].astype(np.float64) - cur_total)
     b.close()
     if net is not None:
         net.close()

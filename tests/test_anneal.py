@@ -79,3 +79,4 @@ def test_initial_temperature_matches_oracle():
     assert t.uphill == len(ups) and t.proposals == graphs * nbr
     assert t.avg == sum(ups) / len(ups)
     assert t.temp == -t.avg / math.log(0.4) and t.temp > 0
+

@@ -28,6 +28,7 @@
 // batch size up to the capacity it was captured for.
 #include "gg.h"
 #include "gg_internal.h"
+#include "gg_planes.cuh"
 
 #include <algorithm>
 #include <cstdlib>
@@ -320,42 +321,6 @@ __global__ void batch_affected(const BatchArgs a, int max_n, int force_full) {
     }
 }
 
-// Distance sum and eccentricity of every source of a base, from its planes.
-// One block per 32-bit word of sources (lane = source); its 32 warps split the
-// vertices, so each plane word is one broadcast load for a warp.
-constexpr int kStatsBlock = 1024;
-__global__ void __launch_bounds__(kStatsBlock) base_source_stats(const uint4 *planes, unsigned cols, int n,
-                                                                 unsigned *rowsum, unsigned *ecc) {
-    __shared__ unsigned s_sum[kStatsBlock / 32][32], s_max[kStatsBlock / 32][32];
-    const unsigned lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
-    const unsigned word = blockIdx.x;
-    const uint32_t *pw = reinterpret_cast<const uint32_t *>(planes);
-    const size_t psw = (size_t)n * cols * 4;
-    unsigned sum = 0, mx = 0;
-    for (unsigned v = warp; v < (unsigned)n; v += kStatsBlock / 32) {
-        const size_t base = (size_t)v * cols * 4 + word;
-        unsigned dv = 0;
-#pragma unroll
-        for (int k = 0; k < kPlanes; ++k) dv |= ((__ldg(pw + (size_t)k * psw + base) >> lane) & 1u) << k;
-        sum += dv;
-        mx = max(mx, dv);
-    }
-    s_sum[warp][lane] = sum;
-    s_max[warp][lane] = mx;
-    __syncthreads();
-    if (warp == 0) {
-        for (int w = 1; w < kStatsBlock / 32; ++w) {
-            sum += s_sum[w][lane];
-            mx = max(mx, s_max[w][lane]);
-        }
-        const unsigned s = word * 32u + lane;
-        if (s < (unsigned)n) {
-            rowsum[s] = sum;
-            ecc[s] = mx;
-        }
-    }
-}
-
 gg_status bfail(gg_status s, const std::string &m) {
     (void)cudaGetLastError();
     gg::set_last_error(m.c_str());
@@ -490,16 +455,6 @@ gg_status enqueue(gg_batch *b, const gg_swap *cands, gg_cand_result *out, cudaSt
     return GG_OK;
 }
 
-// 1 into *asym when some entry u of row v has no entry v in row u.
-__global__ void base_symmetry(const int32_t *adj, int n, int d, int *asym) {
-    const long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (k >= (long long)n * d) return;
-    const int v = (int)(k / d), u = adj[k];
-    bool back = false;
-    for (int j = 0; j < d && !back; ++j) back = adj[(size_t)u * d + j] == v;
-    if (!back) *asym = 1;
-}
-
 constexpr int kIncMaxN = 16384;   // larger bases search every source (planes of 4 n^2/8 bytes)
 
 // The base pass of base `id` (affected-source mode): the single-graph engine
@@ -528,7 +483,7 @@ gg_status base_pass(gg_batch *b, int id) {
         }
         GB_CK(cudaMemsetAsync(b->d_flag, 0, sizeof(int), st));
         const long long ent = (long long)B.n * B.d;
-        base_symmetry<<<(int)((ent + 255) / 256), 256, 0, st>>>(b->base_adj[id], B.n, B.d, b->d_flag);
+        table_symmetry<<<(int)((ent + 255) / 256), 256, 0, st>>>(b->base_adj[id], B.n, B.d, b->d_flag);
         GB_CK(cudaGetLastError());
         gg_eval_opts o{};
         o.max_levels = 1 << kPlanes;      // a base that needs more levels searches every source
@@ -539,8 +494,13 @@ gg_status base_pass(gg_batch *b, int id) {
         gg_result r{};
         gg_status s = gg::engine_eval(eng, b->base_adj[id], &o, &r, st, &x);
         if (s != GG_OK) return s;
-        base_source_stats<<<(B.n + 31) / 32, kStatsBlock, 0, st>>>(b->base_planes[id], B.cols, B.n,
-                                                                   b->base_stats[id], b->base_stats[id] + B.n);
+        int sms = 0;
+        GB_CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, b->device));
+        // rows of the planes = sources: valid only on a symmetric base, which
+        // `valid` below requires
+        plane_row_stats<kPlanes><<<plane_row_stats_grid(B.n, sms), 256, 0, st>>>(
+            b->base_planes[id], (unsigned long long)B.n * B.cols, B.cols, B.n, b->base_stats[id],
+            b->base_stats[id] + B.n);
         GB_CK(cudaGetLastError());
         GB_CK(cudaMemcpyAsync(b->h_flag, b->d_flag, sizeof(int), cudaMemcpyDeviceToHost, st));
         GB_CK(cudaStreamSynchronize(st));

@@ -9,11 +9,13 @@
 //   * an added edge joins vertices whose distances from s differ by 2 or more
 //     (else no path gets shorter).
 // Only those sources are searched again, on the new graph.  The new total is the
-// old total minus the old distance sums of those sources (a masked popcount over
-// the planes) plus their new sums; the new diameter is the larger of their new
-// eccentricities and the largest distance of the other sources (also from the
-// planes).  Exact whenever the current graph is connected with diameter <= 15;
-// otherwise a call evaluates the moved graph in full.
+// old total minus the old distance sums of those sources plus their new sums; the
+// new diameter is the larger of their new eccentricities and the old
+// eccentricities of the other sources.  Every source's distance sum and
+// eccentricity are computed once per current graph from the planes (row
+// reductions, gg_planes.cuh), so a move reads only the planes' columns of its
+// endpoints.  Exact whenever the current graph is symmetric and connected with
+// diameter <= 15; otherwise a call evaluates the moved graph in full.
 #include <algorithm>
 #include <cstring>
 #include <string>
@@ -22,6 +24,7 @@
 #include "gg.h"
 #include "gg_internal.h"
 #include "gg_kernels.cuh"
+#include "gg_planes.cuh"
 
 namespace {
 
@@ -43,14 +46,16 @@ __device__ __forceinline__ unsigned dist_of(const uint32_t *pw, unsigned long lo
     return dv;
 }
 
-// One thread per source: the test above.  Sets the source's bit in `mask` and
-// gives it a position in the list of affected sources (inv[s], -1 preset).
+// One thread per source: the test above.  Gives each affected source a position
+// in the list of affected sources (inv[s], -1 preset) and adds its old distance
+// sum; the unaffected sources give the largest eccentricity that stays.
 __global__ void affected_kernel(const uint32_t *planes, unsigned long long pstride_w, unsigned cols4,
-                                const int32_t *adj, int n, int d, gg_swap sw, uint32_t *mask,
-                                int32_t *inv, IncStatus *st) {
+                                const int32_t *adj, int n, int d, gg_swap sw, const unsigned *rowsum,
+                                const unsigned *ecc, int32_t *inv, IncStatus *st) {
     const unsigned s = blockIdx.x * blockDim.x + threadIdx.x;
+    const bool live = s < (unsigned)n;
     bool aff = false;
-    if (s < (unsigned)n) {
+    if (live) {
         const int a = sw.a, b = sw.b, c = sw.c, dd = sw.d;
         const int p = sw.mode ? dd : c, q = sw.mode ? c : dd;
         const int ends[2][2] = {{a, b}, {c, dd}};
@@ -76,57 +81,21 @@ __global__ void affected_kernel(const uint32_t *planes, unsigned long long pstri
             aff = (da > dp ? da - dp : dp - da) >= 2u || (db > dq ? db - dq : dq - db) >= 2u;
         }
     }
-    const unsigned m = __ballot_sync(0xffffffffu, aff);
+    // one set of atomics per warp
+    const unsigned am = __ballot_sync(0xffffffffu, aff);
+    const unsigned sum = __reduce_add_sync(0xffffffffu, aff ? __ldg(rowsum + s) : 0u);
+    const unsigned mx = __reduce_max_sync(0xffffffffu, live && !aff ? __ldg(ecc + s) : 0u);
     const unsigned lane = threadIdx.x & 31u;
-    if (s < (unsigned)n && lane == 0) mask[s >> 5] = m;
-    if (aff) inv[s] = (int32_t)atomicAdd(&st->count, 1u);
-}
-
-// Over every (vertex, chunk of 128 sources): the distance sum of the affected
-// sources, and the largest distance among the unaffected ones (bitwise search
-// from the top plane down).
-__global__ void plane_sums_kernel(const uint4 *planes, unsigned long long pstride, unsigned cols, int n,
-                                  const uint32_t *mask, IncStatus *st) {
-    const unsigned long long items = (unsigned long long)n * cols;
-    unsigned long long sum = 0;
-    unsigned best = 0;
-    for (unsigned long long t = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x; t < items;
-         t += (unsigned long long)gridDim.x * blockDim.x) {
-        const unsigned C = (unsigned)(t % cols);
-        // affected bits of this chunk; bits of sources >= n belong to no source
-        uint32_t mw[4], valid[4];
-#pragma unroll
-        for (int k = 0; k < 4; ++k) {
-            const unsigned s0 = C * 128u + 32u * k;
-            mw[k] = s0 < (unsigned)n ? __ldg(mask + (s0 >> 5)) : 0u;
-            valid[k] = s0 >= (unsigned)n ? 0u : (n - s0 >= 32 ? 0xffffffffu : ((1u << (n - s0)) - 1u));
+    unsigned first = 0;
+    if (lane == 0) {
+        if (am) {
+            first = atomicAdd(&st->count, (unsigned)__popc(am));
+            atomicAdd(&st->old_sum, (unsigned long long)sum);
         }
-        uint4 w[kPlanes];
-#pragma unroll
-        for (int p = 0; p < kPlanes; ++p) w[p] = __ldg(planes + (size_t)p * pstride + t);
-#pragma unroll
-        for (int k = 0; k < 4; ++k) {
-            unsigned cand = valid[k] & ~mw[k];   // unaffected sources of this word
-            unsigned val = 0;
-#pragma unroll
-            for (int p = kPlanes - 1; p >= 0; --p) {
-                const unsigned wp = k == 0 ? w[p].x : k == 1 ? w[p].y : k == 2 ? w[p].z : w[p].w;
-                sum += (unsigned long long)__popc(wp & mw[k]) << p;
-                const unsigned hit = cand & wp;
-                if (hit) { cand = hit; val |= 1u << p; }
-            }
-            if (valid[k] & ~mw[k]) best = max(best, val);
-        }
+        atomicMax(&st->max_other, mx);
     }
-    // block reduction, one atomic each
-    for (int o = 16; o; o >>= 1) {
-        sum += __shfl_down_sync(0xffffffffu, sum, o);
-        best = max(best, __shfl_down_sync(0xffffffffu, best, o));
-    }
-    if ((threadIdx.x & 31u) == 0) {
-        atomicAdd(&st->old_sum, sum);
-        atomicMax(&st->max_other, best);
-    }
+    first = __shfl_sync(0xffffffffu, first, 0);
+    if (aff) inv[s] = (int32_t)(first + __popc(am & ((1u << lane) - 1u)));
 }
 
 // The candidate's adjacency: the current rows with the four slots of the move
@@ -165,11 +134,12 @@ struct gg_inc {
     cudaStream_t stream = nullptr;
     std::vector<int32_t> h_adj;       // current graph (host copy, validates moves)
     int32_t *d_adj = nullptr, *d_cand = nullptr, *d_inv = nullptr;
-    uint32_t *d_mask = nullptr;
+    unsigned *d_stats = nullptr;      // [2][n]: distance sum, eccentricity of each source
+    int *d_asym = nullptr, *h_asym = nullptr;
     uint4 *d_planes = nullptr;
     unsigned cols = 0;                // plane columns (chunks of 128 sources)
     IncStatus *d_st = nullptr, *h_st = nullptr;
-    bool planes_ok = false;           // connected, diameter <= 15
+    bool planes_ok = false;           // symmetric, connected, diameter <= 15
     gg_result cur{};                  // current graph's exact counts
 };
 
@@ -180,8 +150,9 @@ void inc_free(gg_inc *h) {
     cudaSetDevice(h->device);
     if (h->stream) cudaStreamSynchronize(h->stream);
     if (h->eng) gg_destroy(h->eng);
-    cudaFree(h->d_adj); cudaFree(h->d_cand); cudaFree(h->d_inv); cudaFree(h->d_mask);
+    cudaFree(h->d_adj); cudaFree(h->d_cand); cudaFree(h->d_inv); cudaFree(h->d_stats);
     cudaFree(h->d_planes); cudaFree(h->d_st); cudaFreeHost(h->h_st);
+    cudaFree(h->d_asym); cudaFreeHost(h->h_asym);
     if (h->stream) cudaStreamDestroy(h->stream);
     delete h;
 }
@@ -196,7 +167,23 @@ gg_status inc_rebuild(gg_inc *h) {
     x.no_graph = true;
     gg_status s = gg::engine_eval(h->eng, h->d_adj, &o, &h->cur, h->stream, &x);
     if (s != GG_OK) return s;
-    h->planes_ok = h->cur.connected && h->cur.levels < (1 << kPlanes);
+    h->planes_ok = false;
+    if (!h->cur.connected || h->cur.levels >= (1 << kPlanes)) return GG_OK;
+    // the table passed the engine's range check; the row reductions need a
+    // symmetric distance matrix
+    const cudaStream_t st = h->stream;
+    const long long ent = (long long)h->n * h->d;
+    GI_CK(cudaMemsetAsync(h->d_asym, 0, sizeof(int), st));
+    table_symmetry<<<(int)((ent + 255) / 256), 256, 0, st>>>(h->d_adj, h->n, h->d, h->d_asym);
+    GI_CK(cudaGetLastError());
+    int sms = 0;
+    GI_CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, h->device));
+    plane_row_stats<kPlanes><<<plane_row_stats_grid(h->n, sms), 256, 0, st>>>(
+        h->d_planes, (unsigned long long)h->n * h->cols, h->cols, h->n, h->d_stats, h->d_stats + h->n);
+    GI_CK(cudaGetLastError());
+    GI_CK(cudaMemcpyAsync(h->h_asym, h->d_asym, sizeof(int), cudaMemcpyDeviceToHost, st));
+    GI_CK(cudaStreamSynchronize(st));
+    h->planes_ok = *h->h_asym == 0;
     return GG_OK;
 }
 
@@ -250,7 +237,9 @@ gg_status gg_inc_create(int n, int degree, int device, gg_inc **out) {
     if (e == cudaSuccess) e = cudaMalloc(&h->d_adj, adj_b);
     if (e == cudaSuccess) e = cudaMalloc(&h->d_cand, adj_b);
     if (e == cudaSuccess) e = cudaMalloc(&h->d_inv, (size_t)n * sizeof(int32_t));
-    if (e == cudaSuccess) e = cudaMalloc(&h->d_mask, (size_t)((n + 31) / 32) * sizeof(uint32_t));
+    if (e == cudaSuccess) e = cudaMalloc(&h->d_stats, 2 * (size_t)n * sizeof(unsigned));
+    if (e == cudaSuccess) e = cudaMalloc(&h->d_asym, sizeof(int));
+    if (e == cudaSuccess) e = cudaMallocHost(&h->h_asym, sizeof(int));
     if (e == cudaSuccess) e = cudaMalloc(&h->d_planes, plane_b);
     if (e == cudaSuccess) e = cudaMalloc(&h->d_st, sizeof(IncStatus));
     if (e == cudaSuccess) e = cudaMallocHost(&h->h_st, sizeof(IncStatus));
@@ -302,11 +291,7 @@ gg_status gg_inc_eval(gg_inc *h, const gg_swap *sw, gg_cand_result *out, int *af
     const unsigned long long pstride = (unsigned long long)h->n * h->cols;
     affected_kernel<<<(h->n + 255) / 256, 256, 0, st>>>(reinterpret_cast<const uint32_t *>(h->d_planes),
                                                         pstride * 4, h->cols * 4, h->d_adj, h->n, h->d, *sw,
-                                                        h->d_mask, h->d_inv, h->d_st);
-    GI_CK(cudaGetLastError());
-    const unsigned long long items = pstride;
-    const int grid = (int)std::min<unsigned long long>((items + 255) / 256, 148ull * 8);
-    plane_sums_kernel<<<grid, 256, 0, st>>>(h->d_planes, pstride, h->cols, h->n, h->d_mask, h->d_st);
+                                                        h->d_stats, h->d_stats + h->n, h->d_inv, h->d_st);
     GI_CK(cudaGetLastError());
     GI_CK(cudaMemcpyAsync(h->h_st, h->d_st, sizeof(IncStatus), cudaMemcpyDeviceToHost, st));
     GI_CK(cudaStreamSynchronize(st));

@@ -128,6 +128,21 @@ def test_incremental_falls_back_beyond_the_planes():
 
 
 @pytest.mark.gpu
+def test_incremental_one_way_table_searches_every_source():
+    # a one-way entry elsewhere in the table: the distance matrix is no longer
+    # symmetric, so the per-source sums cannot come from the planes' rows
+    adj = G.random_regular(600, 6, 5)
+    adj[10][0] = next(u for u in range(600) if u != 10 and 10 not in adj[u] and u not in adj[10])
+    inc = G.Incremental(600, 6, 0)
+    r = inc.set_graph(adj)
+    assert r["total"] == O.bfs_pull(adj, np.arange(600)).total()
+    moves = [s for s in G.gen_swaps(adj, 0, 40, 2) if 10 not in (s["a"], s["b"], s["c"], s["d"])][:8]
+    for s in moves:
+        assert check(inc, adj, s) == 600
+    inc.close()
+
+
+@pytest.mark.gpu
 def test_incremental_rejects_moves_on_missing_edges():
     adj = G.random_regular(200, 4, 1)
     inc = G.Incremental(200, 4, 0)

@@ -50,6 +50,7 @@ class Trace:
     final_best: float = math.inf
     hit_time: float | None = None                  # wall seconds when best <= target
     hit_step: int | None = None
+    hit_train_pairs: int | None = None             # pairs the network had trained on at the hit
     spearman: float | None = None                  # surrogate: rank correlation on a fresh sample
 
 
@@ -72,8 +73,10 @@ def rank_correlation(x, y):
 
 def anneal(adj0, steps, *, seed=1, exact=32, pool=4096, explore=8, surrogate=False, t0_frac=1e-3,
            t_end=1e-6, target=None, time_limit=None, lr=2e-3, feature_every=32, train_every=2,
-           device=0, spearman_sample=0):
+           device=0, spearman_sample=0, min_train_pairs=0):
     """Anneal from `adj0` (n x d simple regular graph).  Returns (best_adj, Trace).
+    With a `target`, the run stops once the best ASPL reaches it and the network
+    has trained on at least `min_train_pairs` pairs (the hit time is the first).
     With the surrogate, the adjacency it passes messages over follows every
     accepted move; its distance-histogram features are recomputed every
     `feature_every` accepted moves (one 2-opt changes them only locally)."""
@@ -155,8 +158,9 @@ def anneal(adj0, steps, *, seed=1, exact=32, pool=4096, explore=8, surrogate=Fal
                     tr.best.append(best_aspl)
                     if target is not None and tr.hit_time is None and best_aspl <= target:
                         tr.hit_time, tr.hit_step = tr.times[-1], i + 1
+                        tr.hit_train_pairs = tr.train_pairs
         tr.steps = i + 1
-        if target is not None and tr.hit_time is not None:
+        if target is not None and tr.hit_time is not None and tr.train_pairs >= min_train_pairs:
             break
         if time_limit is not None and time.perf_counter() - t_start > time_limit:
             break

@@ -179,6 +179,92 @@ gg_status gg_gen_swaps(int n, int degree, const int32_t *adj, int base_id, int c
     return GG_OK;
 }
 
+// Moves of a cyclic lift (see gg.h).  Slot (r, i) of the diff table is the orbit
+// edge from orbit vertex r to vertex (r + diff) mod N, of orbit (r + diff) mod N mod M;
+// its reverse slot is the first slot of that orbit's row holding -diff mod N
+// (the search of cppcode/annealing.cpp:117-124).  A new shift for an edge from
+// orbit x to orbit y is (y - x) + M k, k uniform in [0, N/M) (:131, :178, :187).
+gg_status gg_gen_lift_moves(int N, int M, int degree, const int32_t *diffs, int count, uint64_t seed,
+                            gg_lift_edit *out) {
+    if (!diffs || !out || M < 1 || N < 2 || M > N || N % M != 0 || degree < 1 || count < 0)
+        return GG_BAD_ARG;
+    const long long NN = N;
+    auto norm = [&](long long x) { return (int32_t)(((x % NN) + NN) % NN); };
+    std::vector<int32_t> nd((size_t)M * degree);
+    for (size_t k = 0; k < nd.size(); ++k) nd[k] = norm(diffs[k]);
+    auto at = [&](int r, int i) -> int32_t & { return nd[(size_t)r * degree + i]; };
+    // reverse slot of (r, i): -1 if none
+    auto reverse = [&](int r, int i, int *rr) {
+        const int32_t df = at(r, i);
+        const int to = (int)(((long long)r + df) % NN % M);
+        const int32_t back = norm(-(long long)df);
+        for (int j = 0; j < degree; ++j)
+            if (at(to, j) == back && !(to == r && j == i)) { *rr = to; return j; }
+        return -1;
+    };
+    // rows touched by an edit stay simple: nonzero, pairwise distinct diffs
+    auto simple_after = [&](const gg_lift_edit &e) {
+        for (int j = 0; j < e.count; ++j) {
+            const int r = e.row[j];
+            std::vector<int32_t> row(nd.begin() + (size_t)r * degree, nd.begin() + (size_t)(r + 1) * degree);
+            for (int k = 0; k < e.count; ++k)
+                if (e.row[k] == r) row[e.slot[k]] = e.diff[k];
+            for (int k = 0; k < degree; ++k) {
+                bool edited = false;
+                for (int q = 0; q < e.count; ++q) edited |= e.row[q] == r && e.slot[q] == k;
+                if (edited && row[k] == 0) return false;
+                if (row[k] == 0) continue;
+                for (int q = k + 1; q < degree; ++q)
+                    if (row[q] == row[k]) return false;
+            }
+        }
+        return true;
+    };
+    const uint32_t lifts = (uint32_t)(N / M);
+    Rng rng(seed);
+    for (int c = 0; c < count; ++c) {
+        for (long long tries = 0;; ++tries) {
+            if (tries > 1000000) return GG_BAD_ARG;
+            gg_lift_edit e{};
+            const bool shift = lifts > 1 && rng.below(2) == 0;
+            const int a = (int)rng.below((uint32_t)M), ia = (int)rng.below((uint32_t)degree);
+            if (at(a, ia) == 0) continue;
+            int b = -1;
+            const int ib = reverse(a, ia, &b);
+            if (ib < 0) continue;
+            if (shift) {
+                const int32_t df = norm((long long)(b - a) + (long long)M * rng.below(lifts));
+                e.count = 2;
+                e.row[0] = a; e.slot[0] = ia; e.diff[0] = df;
+                e.row[1] = b; e.slot[1] = ib; e.diff[1] = norm(-(long long)df);
+            } else {
+                const int cc = (int)rng.below((uint32_t)M), ic = (int)rng.below((uint32_t)degree);
+                if (at(cc, ic) == 0) continue;
+                int d = -1;
+                const int id = reverse(cc, ic, &d);
+                if (id < 0) continue;
+                const int rs[4] = {a, b, cc, d}, ss[4] = {ia, ib, ic, id};
+                bool distinct = true;
+                for (int x = 0; x < 4; ++x)
+                    for (int y = x + 1; y < 4; ++y) distinct &= !(rs[x] == rs[y] && ss[x] == ss[y]);
+                if (!distinct) continue;  // the same orbit edge twice
+                // a-b, c-d -> a-d, b-c
+                const int32_t dad = norm((long long)(d - a) + (long long)M * rng.below(lifts));
+                const int32_t dbc = norm((long long)(cc - b) + (long long)M * rng.below(lifts));
+                e.count = 4;
+                e.row[0] = a;  e.slot[0] = ia; e.diff[0] = dad;
+                e.row[1] = d;  e.slot[1] = id; e.diff[1] = norm(-(long long)dad);
+                e.row[2] = b;  e.slot[2] = ib; e.diff[2] = dbc;
+                e.row[3] = cc; e.slot[3] = ic; e.diff[3] = norm(-(long long)dbc);
+            }
+            if (!simple_after(e)) continue;
+            out[c] = e;
+            break;
+        }
+    }
+    return GG_OK;
+}
+
 gg_status gg_gen_cyclic_lift(int m, int g, int d, uint64_t seed, int32_t *diffs) {
     if (!diffs || m < 1 || g < 1 || d < 1 || ((long long)m * d) % 2 != 0 ||
         (long long)m * g >= (1ll << 31))

@@ -1,0 +1,414 @@
+// gg_lift.cu -- batched exact evaluation of cyclic-lift ("part") candidates
+// (gg_lift_* in gg.h).
+//
+// The lifted form of cudaASPLconv: M orbit vertices with d diffs each; vertex v
+// of the N-vertex lift has the neighbours (v + diffs[v % M][i]) mod N, and the
+// BFS runs from the M vertices 0..M-1 (cudaASPLconv.cu:197-243).  The
+// reference's annealer changes 2 or 4 slots of the diff table per proposal
+// (cppcode/annealing.cpp:112-197) and scores each with one calculator call.
+//
+// Here one cooperative launch scores a population.  `lift_tables` writes every
+// candidate's diff table (base + edit, diffs reduced to [0, N)).  `lift_kernel`
+// runs the candidates in rounds of G side by side: a round's bitsets hold, per
+// vertex, W = G * cpc uint4 chunks (cpc = ceil(M/128)), chunk group g being the
+// M sources of candidate g of the round, source s at bit s % 128 of chunk s / 128
+// of its group.  A level is one pass over all (vertex, chunk) items:
+//     new = (OR_i F[(v + diff_g[v % M][i]) mod N][w]) & ~V[v][w];  V |= new;  F' = new
+// where g is the item's group, so neighbours always come from the item's own
+// candidate.  Lanes of a warp cover consecutive chunks of a vertex, so the
+// gathers of a neighbour row are contiguous 16-byte loads.  New pairs are
+// counted per group (warp-aggregated shared atomics, one global atomic per block,
+// group and level into counts[L][k]); after the grid barrier every block reads
+// the round's counts and the round ends when no candidate found a pair or every
+// candidate reached all M*N pairs.
+#include "gg.h"
+#include "gg_internal.h"
+#include "gg_kernels.cuh"
+
+#include <algorithm>
+#include <cstdlib>
+#include <cstring>
+#include <string>
+#include <vector>
+
+namespace {
+
+constexpr int kLiftBlock = 256;
+constexpr int kMaxGroup = 32;
+
+struct LiftArgs {
+    const int32_t *tab;              // [K][M][d] diffs in [0, N)
+    int N, M, d, K, G, cpc, W;       // W = G * cpc chunks per vertex
+    gg::FastDiv div_w, div_m, div_c; // t / W, v / M, w / cpc
+    uint4 *V, *F0, *F1;              // [N][W]
+    unsigned long long *counts;      // [max_levels + 1][K]: pairs first reached at level L
+    int max_levels;
+    gg::Ctl *ctl;
+    unsigned expected;
+    long long wait_ns;
+};
+
+// Candidate tables: entry (k, r, i) is the base entry unless candidate k's edit
+// names slot (r, i).
+__global__ void lift_tables(const int32_t *base, const gg_lift_edit *ed, int K, int M, int d, int32_t *tab) {
+    const long long per = (long long)M * d, total = per * K;
+    for (long long x = (long long)blockIdx.x * blockDim.x + threadIdx.x; x < total;
+         x += (long long)gridDim.x * blockDim.x) {
+        const int k = (int)(x / per);
+        const int e = (int)(x - (long long)k * per);
+        const int r = e / d, i = e - r * d;
+        int32_t v = __ldg(base + e);
+        const gg_lift_edit &q = ed[k];
+        for (int j = 0; j < q.count; ++j)
+            if (q.row[j] == r && q.slot[j] == i) v = q.diff[j];
+        tab[x] = v;
+    }
+}
+
+__global__ void __launch_bounds__(kLiftBlock) lift_kernel(const LiftArgs a) {
+    __shared__ unsigned s_cnt[kMaxGroup];
+    const unsigned lane = threadIdx.x & 31u;
+    if (threadIdx.x < kMaxGroup) s_cnt[threadIdx.x] = 0u;
+    unsigned epoch = 0;
+    const unsigned items = (unsigned)a.N * (unsigned)a.W;
+    const unsigned stride = gridDim.x * blockDim.x;
+    const unsigned first = blockIdx.x * blockDim.x + threadIdx.x;
+    const unsigned long long all_pairs = (unsigned long long)a.M * (unsigned long long)a.N;
+    const int rounds = (a.K + a.G - 1) / a.G;
+    int zeroed = 1;        // rows 0 and 1 of counts are zeroed by the host
+    int levels_run = 0;
+    for (int rd = 0; rd < rounds; ++rd) {
+        const int k0 = rd * a.G;
+        const int live = min(a.G, a.K - k0);
+        // phase 0: the padding bits and the diagonal (source s is vertex s)
+        for (unsigned t = first; t < items; t += stride) {
+            const unsigned v = a.div_w.div(t), w = t - v * (unsigned)a.W;
+            const unsigned g = a.div_c.div(w), cc = w - g * (unsigned)a.cpc;
+            uint4 vis = make_uint4(0xffffffffu, 0xffffffffu, 0xffffffffu, 0xffffffffu), fr = gg::u4zero();
+            if ((int)g < live) {
+                vis = gg::pad_mask((int)cc, a.M);
+                if (v < (unsigned)a.M && (v >> 7) == cc) {
+                    const unsigned bit = 1u << (v & 31u);
+                    switch ((v >> 5) & 3u) {
+                        case 0: fr.x = bit; break;
+                        case 1: fr.y = bit; break;
+                        case 2: fr.z = bit; break;
+                        default: fr.w = bit; break;
+                    }
+                    gg::or_into(vis, fr);
+                }
+            }
+            a.V[t] = vis;
+            a.F0[t] = fr;
+        }
+        if (!gg::grid_sync(a.ctl, a.expected, a.wait_ns, 0, epoch)) return;
+        unsigned long long reached = threadIdx.x < (unsigned)live ? (unsigned long long)a.M : 0ull;
+        for (int L = 1; L <= a.max_levels; ++L) {
+            const uint4 *Fc = (L & 1) ? a.F0 : a.F1;
+            uint4 *Fn = (L & 1) ? a.F1 : a.F0;
+            // the next level's count row, before any block can add to it
+            if (blockIdx.x == 0 && L + 1 > zeroed && L + 1 <= a.max_levels)
+                for (int k = threadIdx.x; k < a.K; k += blockDim.x) a.counts[(size_t)(L + 1) * a.K + k] = 0ull;
+            zeroed = max(zeroed, L + 1);
+            for (unsigned t0 = first - lane; t0 < items; t0 += stride) {
+                const unsigned t = t0 + lane;
+                unsigned c = 0;
+                int key = -1;
+                if (t < items) {
+                    const unsigned v = a.div_w.div(t), w = t - v * (unsigned)a.W;
+                    const unsigned g = a.div_c.div(w);
+                    const uint4 own = __ldcg(a.V + t);
+                    uint4 nw = gg::u4zero();
+                    if (!gg::u4full(own)) {
+                        // groups past `live` start full, so g < live here
+                        const unsigned r = v - a.div_m.div(v) * (unsigned)a.M;
+                        const int32_t *row = a.tab + ((size_t)(k0 + (int)g) * a.M + r) * a.d;
+                        uint4 acc = gg::u4zero();
+                        for (int i = 0; i < a.d; ++i) {
+                            unsigned u = v + (unsigned)__ldg(row + i);
+                            u -= u >= (unsigned)a.N ? (unsigned)a.N : 0u;
+                            gg::or_into(acc, __ldcg(Fc + (size_t)u * a.W + w));
+                        }
+                        nw = gg::andnot(acc, own);
+                        if (gg::u4any(nw)) {
+                            a.V[t] = gg::u4or(own, nw);
+                            c = gg::u4popc(nw);
+                            key = (int)g;
+                        }
+                    }
+                    Fn[t] = nw;
+                }
+                const unsigned peers = __match_any_sync(0xffffffffu, key);
+                const unsigned sum = __reduce_add_sync(peers, c);
+                if (key >= 0 && (int)lane == __ffs((int)peers) - 1) atomicAdd(&s_cnt[key], sum);
+            }
+            __syncthreads();
+            if (threadIdx.x < (unsigned)live && s_cnt[threadIdx.x]) {
+                atomicAdd(a.counts + (size_t)L * a.K + k0 + threadIdx.x, (unsigned long long)s_cnt[threadIdx.x]);
+                s_cnt[threadIdx.x] = 0u;
+            }
+            if (!gg::grid_sync(a.ctl, a.expected, a.wait_ns, L, epoch)) return;
+            levels_run = max(levels_run, L);
+            int more = 0;
+            if (threadIdx.x < (unsigned)live) {
+                const unsigned long long n = gg::ld_relaxed_u64(a.counts + (size_t)L * a.K + k0 + threadIdx.x);
+                reached += n;
+                more = n != 0ull && reached < all_pairs;
+            }
+            if (!__syncthreads_or(more)) break;
+        }
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) a.ctl->levels_run = levels_run;
+}
+
+gg_status lfail(gg_status s, const std::string &m) {
+    (void)cudaGetLastError();
+    gg::set_last_error(m.c_str());
+    return s;
+}
+
+#define GL_CK(call)                                                                          \
+    do {                                                                                     \
+        cudaError_t e_ = (call);                                                             \
+        if (e_ != cudaSuccess)                                                               \
+            return lfail(e_ == cudaErrorMemoryAllocation ? GG_OUT_OF_MEMORY : GG_CUDA_ERROR, \
+                         std::string(#call) + ": " + cudaGetErrorString(e_));                \
+    } while (0)
+
+}  // namespace
+
+struct gg_lift {
+    int N = 0, M = 0, d = 0, device = 0;
+    int cpc = 0, g_auto = 1, g_max = 0, group = 0;   // group 0: automatic
+    int grid = 0, sms = 0;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    int32_t *d_base = nullptr, *d_tab = nullptr;
+    gg_lift_edit *d_ed = nullptr, *h_ed = nullptr;
+    int cap = 0;                                     // candidates the buffers hold
+    uint4 *V = nullptr, *F0 = nullptr, *F1 = nullptr;
+    unsigned long long *d_counts = nullptr, *h_counts = nullptr;
+    size_t counts_cap = 0;                           // entries
+    gg::Ctl *d_ctl = nullptr, *h_ctl = nullptr;
+    long long wait_ns = 10ll * 1000 * 1000 * 1000;
+    bool base_set = false;
+    float last_ms = 0.f;
+};
+
+namespace {
+
+void lift_free(gg_lift *h) {
+    if (!h) return;
+    cudaSetDevice(h->device);
+    if (h->stream) cudaStreamSynchronize(h->stream);
+    cudaFree(h->d_base); cudaFree(h->d_tab); cudaFree(h->d_ed); cudaFreeHost(h->h_ed);
+    cudaFree(h->V); cudaFree(h->F0); cudaFree(h->F1);
+    cudaFree(h->d_counts); cudaFreeHost(h->h_counts);
+    cudaFree(h->d_ctl); cudaFreeHost(h->h_ctl);
+    if (h->ev0) cudaEventDestroy(h->ev0);
+    if (h->ev1) cudaEventDestroy(h->ev1);
+    if (h->stream) cudaStreamDestroy(h->stream);
+    delete h;
+}
+
+gg_status ensure_cand(gg_lift *h, int n) {
+    if (n <= h->cap) return GG_OK;
+    int cap = std::max(n, 2 * h->cap);
+    cudaFree(h->d_tab); cudaFree(h->d_ed); cudaFreeHost(h->h_ed);
+    h->d_tab = nullptr; h->d_ed = nullptr; h->h_ed = nullptr; h->cap = 0;
+    GL_CK(cudaMalloc(&h->d_tab, (size_t)cap * h->M * h->d * sizeof(int32_t)));
+    GL_CK(cudaMalloc(&h->d_ed, (size_t)cap * sizeof(gg_lift_edit)));
+    GL_CK(cudaMallocHost(&h->h_ed, (size_t)cap * sizeof(gg_lift_edit)));
+    h->cap = cap;
+    return GG_OK;
+}
+
+gg_status ensure_counts(gg_lift *h, size_t entries) {
+    if (entries <= h->counts_cap) return GG_OK;
+    const size_t cap = std::max(entries, 2 * h->counts_cap);
+    cudaFree(h->d_counts); cudaFreeHost(h->h_counts);
+    h->d_counts = nullptr; h->h_counts = nullptr; h->counts_cap = 0;
+    GL_CK(cudaMalloc(&h->d_counts, cap * sizeof(unsigned long long)));
+    GL_CK(cudaMallocHost(&h->h_counts, cap * sizeof(unsigned long long)));
+    h->counts_cap = cap;
+    return GG_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+gg_status gg_lift_create(int N, int M, int degree, int device, gg_lift **out) {
+    if (!out || N < 2 || M < 1 || M > N || N % M != 0 || degree < 1 || degree > 4096)
+        return lfail(GG_BAD_ARG, "need N >= 2, 1 <= M <= N with M dividing N, degree >= 1");
+    *out = nullptr;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || device < 0 || device >= ndev)
+        return lfail(GG_NO_DEVICE, "no such CUDA device");
+    gg_lift *h = new gg_lift();
+    h->N = N; h->M = M; h->d = degree; h->device = device;
+    h->cpc = (M + 127) / 128;
+    auto fail = [&](gg_status s) { lift_free(h); return s; };
+    if (cudaSetDevice(device) != cudaSuccess) return fail(lfail(GG_NO_DEVICE, "cudaSetDevice failed"));
+    int l2 = 0, coop = 0, per_sm = 0;
+    if (cudaDeviceGetAttribute(&l2, cudaDevAttrL2CacheSize, device) != cudaSuccess ||
+        cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, device) != cudaSuccess ||
+        cudaDeviceGetAttribute(&h->sms, cudaDevAttrMultiProcessorCount, device) != cudaSuccess ||
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, lift_kernel, kLiftBlock, 0) != cudaSuccess)
+        return fail(lfail(GG_CUDA_ERROR, "device query failed"));
+    if (!coop || per_sm < 1) return fail(lfail(GG_CUDA_ERROR, "cooperative launch unavailable"));
+    h->grid = per_sm * h->sms;
+    // one candidate's round share: three bitsets of N * cpc uint4
+    const double per_cand = 3.0 * N * h->cpc * 16.0;
+    const int fit = (int)std::max(1.0, 0.75 * l2 / per_cand);
+    // items N * W must stay below 2^31
+    const long long by_items = std::max(1ll, (1ll << 31) / ((long long)N * h->cpc));
+    h->g_auto = (int)std::min<long long>({(long long)fit, (long long)kMaxGroup, by_items});
+    cudaError_t e = cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaEventCreate(&h->ev0);
+    if (e == cudaSuccess) e = cudaEventCreate(&h->ev1);
+    if (e == cudaSuccess) e = cudaMalloc(&h->d_base, (size_t)M * degree * sizeof(int32_t));
+    if (e == cudaSuccess) e = cudaMalloc(&h->d_ctl, sizeof(gg::Ctl));
+    if (e == cudaSuccess) e = cudaMallocHost(&h->h_ctl, sizeof(gg::Ctl));
+    // bitsets for the automatic group (a larger group set later reallocates)
+    const size_t bits_auto = (size_t)N * h->cpc * h->g_auto * sizeof(uint4);
+    if (e == cudaSuccess) e = cudaMalloc(&h->V, bits_auto);
+    if (e == cudaSuccess) e = cudaMalloc(&h->F0, bits_auto);
+    if (e == cudaSuccess) e = cudaMalloc(&h->F1, bits_auto);
+    if (e != cudaSuccess)
+        return fail(lfail(e == cudaErrorMemoryAllocation ? GG_OUT_OF_MEMORY : GG_CUDA_ERROR,
+                          cudaGetErrorString(e)));
+    h->g_max = h->g_auto;   // groups the bitsets hold
+    *out = h;
+    return GG_OK;
+}
+
+gg_status gg_lift_set_base(gg_lift *h, const int32_t *diffs) {
+    if (!h || !diffs) return lfail(GG_BAD_ARG, "null argument");
+    std::vector<int32_t> nd((size_t)h->M * h->d);
+    const long long N = h->N;
+    for (size_t k = 0; k < nd.size(); ++k) nd[k] = (int32_t)((((long long)diffs[k] % N) + N) % N);
+    GL_CK(cudaSetDevice(h->device));
+    GL_CK(cudaMemcpyAsync(h->d_base, nd.data(), nd.size() * sizeof(int32_t), cudaMemcpyHostToDevice, h->stream));
+    GL_CK(cudaStreamSynchronize(h->stream));
+    h->base_set = true;
+    return GG_OK;
+}
+
+gg_status gg_lift_set_group(gg_lift *h, int group) {
+    if (!h || group < 0 || group > kMaxGroup) return lfail(GG_BAD_ARG, "group must be in [0, 32]");
+    if (group > 0 && (long long)h->N * h->cpc * group >= (1ll << 31))
+        return lfail(GG_BAD_ARG, "group too large for this lift");
+    const int need = group ? group : h->g_auto;
+    if (need > h->g_max) {
+        GL_CK(cudaSetDevice(h->device));
+        GL_CK(cudaStreamSynchronize(h->stream));
+        cudaFree(h->V); cudaFree(h->F0); cudaFree(h->F1);
+        h->V = h->F0 = h->F1 = nullptr;
+        h->g_max = 0;
+        const size_t bits = (size_t)h->N * h->cpc * need * sizeof(uint4);
+        GL_CK(cudaMalloc(&h->V, bits));
+        GL_CK(cudaMalloc(&h->F0, bits));
+        GL_CK(cudaMalloc(&h->F1, bits));
+        h->g_max = need;
+    }
+    h->group = group;
+    return GG_OK;
+}
+
+gg_status gg_lift_group(gg_lift *h, int *group) {
+    if (!h || !group) return lfail(GG_BAD_ARG, "null argument");
+    *group = h->group ? h->group : h->g_auto;
+    return GG_OK;
+}
+
+gg_status gg_lift_eval(gg_lift *h, int n_cand, const gg_lift_edit *edits, int max_levels,
+                       gg_cand_result *out) {
+    if (!h || n_cand < 0 || (n_cand && (!edits || !out)) || max_levels < 0)
+        return lfail(GG_BAD_ARG, "bad arguments");
+    if (!h->base_set) return lfail(GG_BAD_ARG, "no base table set");
+    if (n_cand == 0) return GG_OK;
+    if (h->g_max < 1) return lfail(GG_OUT_OF_MEMORY, "bitsets were not allocated");
+    GL_CK(cudaSetDevice(h->device));
+    gg_status s = ensure_cand(h, n_cand);
+    if (s != GG_OK) return s;
+    const long long N = h->N;
+    for (int k = 0; k < n_cand; ++k) {
+        const gg_lift_edit &q = edits[k];
+        if (q.count < 0 || q.count > 4) return lfail(GG_BAD_ARG, "edit count must be in [0, 4]");
+        gg_lift_edit &o = h->h_ed[k];
+        o = gg_lift_edit{};
+        o.count = q.count;
+        for (int j = 0; j < q.count; ++j) {
+            if (q.row[j] < 0 || q.row[j] >= h->M || q.slot[j] < 0 || q.slot[j] >= h->d)
+                return lfail(GG_BAD_ARG, "edit slot outside the table");
+            o.row[j] = q.row[j];
+            o.slot[j] = q.slot[j];
+            o.diff[j] = (int32_t)((((long long)q.diff[j] % N) + N) % N);
+        }
+    }
+    const int ml = max_levels > 0 ? std::min(max_levels, h->N) : h->N;
+    s = ensure_counts(h, (size_t)(ml + 1) * n_cand);
+    if (s != GG_OK) return s;
+    const int G = std::min(h->group ? h->group : h->g_auto, n_cand);
+    const cudaStream_t st = h->stream;
+    GL_CK(cudaMemcpyAsync(h->d_ed, h->h_ed, (size_t)n_cand * sizeof(gg_lift_edit), cudaMemcpyHostToDevice, st));
+    GL_CK(cudaMemsetAsync(h->d_ctl, 0, sizeof(gg::Ctl), st));
+    GL_CK(cudaMemsetAsync(h->d_counts, 0, (size_t)std::min(ml + 1, 2) * n_cand * sizeof(unsigned long long), st));
+    GL_CK(cudaEventRecord(h->ev0, st));
+    const long long tab_n = (long long)n_cand * h->M * h->d;
+    lift_tables<<<(int)std::min<long long>((tab_n + 255) / 256, (long long)h->sms * 16), 256, 0, st>>>(
+        h->d_base, h->d_ed, n_cand, h->M, h->d, h->d_tab);
+    GL_CK(cudaGetLastError());
+    LiftArgs a{};
+    a.tab = h->d_tab;
+    a.N = h->N; a.M = h->M; a.d = h->d; a.K = n_cand; a.G = G; a.cpc = h->cpc; a.W = G * h->cpc;
+    a.div_w = gg::FastDiv((uint32_t)a.W);
+    a.div_m = gg::FastDiv((uint32_t)h->M);
+    a.div_c = gg::FastDiv((uint32_t)h->cpc);
+    a.V = h->V; a.F0 = h->F0; a.F1 = h->F1;
+    a.counts = h->d_counts;
+    a.max_levels = ml;
+    a.ctl = h->d_ctl;
+    a.expected = (unsigned)h->grid;
+    a.wait_ns = h->wait_ns;
+    void *args[] = {&a};
+    GL_CK(cudaLaunchCooperativeKernel((void *)lift_kernel, dim3(h->grid), dim3(kLiftBlock), args, 0, st));
+    GL_CK(cudaEventRecord(h->ev1, st));
+    GL_CK(cudaMemcpyAsync(h->h_ctl, h->d_ctl, sizeof(gg::Ctl), cudaMemcpyDeviceToHost, st));
+    GL_CK(cudaStreamSynchronize(st));
+    if (h->h_ctl->err) return lfail(GG_TIMEOUT, "grid barrier wait exceeded the limit");
+    const int lr = std::min(h->h_ctl->levels_run, ml);
+    GL_CK(cudaMemcpyAsync(h->h_counts, h->d_counts, (size_t)(lr + 1) * n_cand * sizeof(unsigned long long),
+                          cudaMemcpyDeviceToHost, st));
+    GL_CK(cudaStreamSynchronize(st));
+    GL_CK(cudaEventElapsedTime(&h->last_ms, h->ev0, h->ev1));
+    const unsigned long long all = (unsigned long long)h->M * (unsigned long long)h->N;
+    for (int k = 0; k < n_cand; ++k) {
+        unsigned long long tot = 0, reach = (unsigned long long)h->M;
+        int lev = 0;
+        for (int L = 1; L <= lr; ++L) {
+            const unsigned long long c = h->h_counts[(size_t)L * n_cand + k];
+            if (!c) continue;
+            tot += (unsigned long long)L * c;
+            reach += c;
+            lev = L;
+        }
+        const bool capped = lev == ml && reach < all;
+        out[k] = gg_cand_result{tot, reach, lev, (!capped && reach == all) ? 1 : 0};
+    }
+    return GG_OK;
+}
+
+gg_status gg_lift_last_ms(gg_lift *h, double *ms) {
+    if (!h || !ms) return lfail(GG_BAD_ARG, "null argument");
+    *ms = h->last_ms;
+    return GG_OK;
+}
+
+gg_status gg_lift_destroy(gg_lift *h) {
+    lift_free(h);
+    return GG_OK;
+}
+
+}  // extern "C"

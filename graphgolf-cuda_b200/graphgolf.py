@@ -124,6 +124,14 @@ _SIGS = {
     "gg_inc_commit": [_P, _P, _P],
     "gg_inc_destroy": [_P],
     "gg_gen_cyclic_lift": [_I, _I, _I, ctypes.c_uint64, _P],
+    "gg_lift_create": [_I, _I, _I, _I, _EPP],
+    "gg_lift_set_base": [_P, _P],
+    "gg_lift_eval": [_P, _I, _P, _I, _P],
+    "gg_lift_set_group": [_P, _I],
+    "gg_lift_group": [_P, _IP],
+    "gg_lift_last_ms": [_P, _DP],
+    "gg_lift_destroy": [_P],
+    "gg_gen_lift_moves": [_I, _I, _I, _P, _I, ctypes.c_uint64, _P],
 }
 
 
@@ -818,6 +826,76 @@ class Batch:
     def close(self):
         if self._h:
             lib().gg_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+LIFT_EDIT_DTYPE = np.dtype([("count", np.int32), ("row", np.int32, 4), ("slot", np.int32, 4),
+                            ("diff", np.int32, 4)])
+
+
+def gen_lift_moves(N, M, diffs, count, seed):
+    """Random shift / orbit 2-opt moves of a cyclic lift (gg_gen_lift_moves) ->
+    LIFT_EDIT_DTYPE array."""
+    diffs = _i32(diffs).reshape(M, -1)
+    out = np.zeros(count, dtype=LIFT_EDIT_DTYPE)
+    _check(lib().gg_gen_lift_moves(N, M, diffs.shape[1], _ptr(diffs), count, seed, _ptr(out)))
+    return out
+
+
+def apply_lift_edit(diffs, e):
+    """Host copy of a lift edit: the diff table with the edit's slots replaced."""
+    t = np.array(diffs, dtype=np.int32, copy=True)
+    for j in range(int(e["count"])):
+        t[int(e["row"][j]), int(e["slot"][j])] = int(e["diff"][j])
+    return t
+
+
+class Lift:
+    """Scores many edits of one cyclic-lift diff table in one launch (gg_lift_*).
+    Results are over the M orbit sources: ASPL = total * (N // M) / (N * (N - 1))."""
+
+    def __init__(self, N, M, degree, device=0):
+        self.N, self.M, self.degree = N, M, degree
+        self._h = _create("gg_lift_create", N, M, degree, device)
+
+    def set_base(self, diffs):
+        self.base = _i32(diffs).reshape(self.M, self.degree)
+        _check(lib().gg_lift_set_base(self._h, _ptr(self.base)))
+
+    def eval(self, edits, max_levels=0):
+        edits = np.ascontiguousarray(edits, dtype=LIFT_EDIT_DTYPE)
+        out = np.zeros(len(edits), dtype=CAND_RESULT_DTYPE)
+        _check(lib().gg_lift_eval(self._h, len(edits), _ptr(edits), max_levels, _ptr(out)))
+        return out
+
+    def aspl(self, res):
+        """The reference's ASPL of each result (cudaASPLconv.cu:241-242); inf when
+        disconnected."""
+        tot = res["total"].astype(np.float64) * (self.N // self.M)
+        return np.where(res["connected"] == 1, tot / (self.N * (self.N - 1)), np.inf)
+
+    def set_group(self, group):
+        _check(lib().gg_lift_set_group(self._h, group))
+
+    def group(self):
+        g = ctypes.c_int()
+        _check(lib().gg_lift_group(self._h, ctypes.byref(g)))
+        return g.value
+
+    def last_ms(self):
+        ms = ctypes.c_double()
+        _check(lib().gg_lift_last_ms(self._h, ctypes.byref(ms)))
+        return ms.value
+
+    def close(self):
+        if self._h:
+            lib().gg_lift_destroy(self._h)
             self._h = None
 
     def __del__(self):

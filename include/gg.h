@@ -247,6 +247,54 @@ gg_status gg_inc_eval(gg_inc *h, const gg_swap *s, gg_cand_result *out, int *aff
 gg_status gg_inc_commit(gg_inc *h, const gg_swap *s, gg_result *r);
 gg_status gg_inc_destroy(gg_inc *h);
 
+/* ---- batched evaluation of cyclic-lift candidates (no reference counterpart) ----
+ * The reference's annealers on the lifted ("part") form propose one edit of the
+ * diff table at a time and score it with one cudaASPLconv::diameterASPL call
+ * (cppcode/annealing.cpp:112-197 proposes, :403 scores).  Here one cooperative
+ * launch scores a whole population of edits of one base table: every candidate
+ * is the base diff table (M * degree int32, the table of gg_conv_*) with up to 4
+ * slots replaced, and gets the exact counts of its own N-vertex lift with BFS
+ * from the M orbit vertices 0..M-1.  N must be a multiple of M. */
+typedef struct gg_lift gg_lift;
+
+/* Slots (row[j], slot[j]) of the base table take the value diff[j], j < count
+ * (0 <= count <= 4; count 0 is the base itself).  Diffs are taken modulo N. */
+typedef struct gg_lift_edit {
+    int32_t count;
+    int32_t row[4];
+    int32_t slot[4];
+    int32_t diff[4];
+} gg_lift_edit;
+
+gg_status gg_lift_create(int N, int M, int degree, int device, gg_lift **out);
+/* The base diff table, M * degree int32 (padding slots: diff 0). */
+gg_status gg_lift_set_base(gg_lift *h, const int32_t *diffs);
+/* Exact counts of each candidate over the M orbit sources: out[i].total = sum of
+ * distances from the sources (unscaled: the reference's ASPL is
+ * total * (N/M) / (N*(N-1)), cudaASPLconv.cu:241-242), .reached = (source, vertex)
+ * pairs reached (M*N when connected), .levels = last level that found a pair.
+ * max_levels caps the BFS (0 = no cap); a candidate still finding pairs at the cap
+ * reports connected = 0. */
+gg_status gg_lift_eval(gg_lift *h, int n_cand, const gg_lift_edit *edits, int max_levels,
+                       gg_cand_result *out);
+/* Candidates that run side by side in one round (1..32; 0 = automatic: as many as
+ * keep the round's bitsets within 3/4 of the L2). */
+gg_status gg_lift_set_group(gg_lift *h, int group);
+gg_status gg_lift_group(gg_lift *h, int *group);
+/* Device milliseconds of the last gg_lift_eval (table build and BFS launch). */
+gg_status gg_lift_last_ms(gg_lift *h, double *ms);
+gg_status gg_lift_destroy(gg_lift *h);
+
+/* Random moves of a cyclic lift, the two the reference's part annealer draws
+ * (cppcode/annealing.cpp:112-197): with probability 1/2 when N/M > 1, a new lift
+ * shift for one orbit edge (2 slots); otherwise an orbit 2-opt, edges a-b and c-d
+ * rewired to a-d and b-c, each with a uniform new lift shift (4 slots).  Padding
+ * slots (diff 0 mod N) are never moved, and moves that would give the lift a loop
+ * or a repeated edge are redrawn (the reference keeps them).  diffs: M * degree,
+ * symmetric (every slot has its reverse slot in the target orbit's row). */
+gg_status gg_gen_lift_moves(int N, int M, int degree, const int32_t *diffs, int count, uint64_t seed,
+                            gg_lift_edit *out);
+
 /* Uniform random 2-opt proposals on a base graph (adj n*degree, simple):
  * edges (a,b), (c,d) drawn uniformly, mode uniform; proposals that would create a
  * loop or a repeated edge are redrawn.  Writes `count` swaps with base = base_id. */

@@ -1,0 +1,137 @@
+"""Batched evaluation of cyclic-lift candidates (gg_lift_*) and the lift moves
+(gg_gen_lift_moves).
+
+CPU: every move keeps the lift symmetric and simple, moves only non-padding
+slots, draws shift moves only when N/M > 1, and is reproducible from its seed.
+GPU: every candidate's exact counts equal the oracle's BFS from the M orbit
+vertices of its own lift, in one round or many, at every group size, with a
+level cap, on a disconnected base, and the reference ASPL equals the
+cudaASPLconv calculator's."""
+
+import numpy as np
+import pytest
+
+import graphgolf as G
+import oracle as O
+
+
+def lift_ok(N, M, diffs):
+    """The lift of `diffs` is symmetric (each edge at both ends) and simple."""
+    adj = O.expand_part(N, M, diffs)
+    pad = np.asarray(diffs).reshape(M, -1)[np.arange(N) % M] % N == 0
+    for v in range(N):
+        row = [int(u) for u, p in zip(adj[v], pad[v]) if not p]
+        if v in row or len(set(row)) != len(row):
+            return False
+        for u in row:
+            back = [int(x) for x, p in zip(adj[u], pad[u]) if not p]
+            if v not in back:
+                return False
+    return True
+
+
+@pytest.mark.parametrize("m,g,d,seed", [(64, 8, 6, 3), (40, 5, 4, 1), (96, 1, 5, 2)])
+def test_lift_moves_keep_the_lift_simple(m, g, d, seed):
+    N, M, D = G.cyclic_lift(m, g, d, seed)
+    moves = G.gen_lift_moves(N, M, D, 60, seed + 11)
+    assert set(np.unique(moves["count"])) <= ({2, 4} if g > 1 else {4})
+    for e in moves:
+        t = G.apply_lift_edit(D, e)
+        assert lift_ok(N, M, t)
+        assert (t != D).sum() <= e["count"]
+    if g > 1:
+        assert (moves["count"] == 2).any() and (moves["count"] == 4).any()
+
+
+def test_lift_moves_are_reproducible_and_skip_padding():
+    N, M, D = G.cyclic_lift(48, 4, 6, 7)
+    a = G.gen_lift_moves(N, M, D, 30, 99)
+    b = G.gen_lift_moves(N, M, D, 30, 99)
+    c = G.gen_lift_moves(N, M, D, 30, 100)
+    assert a.tobytes() == b.tobytes() and a.tobytes() != c.tobytes()
+    # a 5-regular lift padded to degree 6: slot 5 of every row is padding (diff 0)
+    N2, M2, D5 = G.cyclic_lift(48, 4, 5, 7)
+    P = np.concatenate([D5, np.zeros((M2, 1), np.int32)], axis=1)
+    for e in G.gen_lift_moves(N2, M2, P, 40, 3):
+        assert all(int(e["slot"][j]) != 5 for j in range(int(e["count"])))
+        assert lift_ok(N2, M2, G.apply_lift_edit(P, e))
+
+
+def test_lift_moves_bad_arguments():
+    N, M, D = G.cyclic_lift(16, 4, 4, 1)
+    with pytest.raises(G.GGError):
+        G.gen_lift_moves(N + 1, M, D, 4, 1)        # M does not divide N
+
+
+# ---- GPU ---------------------------------------------------------------------
+
+def oracle_counts(N, M, t):
+    r = O.bfs_pull(O.expand_part(N, M, t), np.arange(M))
+    return r.total(), int(r.reached.sum()), r.levels, int(r.connected)
+
+
+def check_all(L, N, M, D, moves, res):
+    for e, got in zip(moves, res):
+        want = oracle_counts(N, M, G.apply_lift_edit(D, e))
+        assert (int(got["total"]), int(got["reached"]), int(got["connected"])) == (want[0], want[1], want[3])
+        if want[3]:
+            assert int(got["levels"]) == want[2]
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("m,g,d,seed", [(256, 8, 6, 1), (100, 12, 4, 2), (130, 3, 5, 3)])
+def test_lift_candidates_equal_the_oracle(m, g, d, seed):
+    N, M, D = G.cyclic_lift(m, g, d, seed)
+    L = G.Lift(N, M, d, 0)
+    L.set_base(D)
+    moves = np.concatenate([np.zeros(1, dtype=G.LIFT_EDIT_DTYPE), G.gen_lift_moves(N, M, D, 45, seed)])
+    res = L.eval(moves)
+    check_all(L, N, M, D, moves, res)
+    # the same through every group size: one candidate per round, odd, automatic
+    for grp in (1, 3, 0):
+        L.set_group(grp)
+        again = L.eval(moves)
+        assert again.tobytes() == res.tobytes()
+    # the reference ASPL of the base equals the cudaASPLconv calculator's
+    c = G.cudaASPLconv(N, M, d, 0)
+    diam, aspl = c.diameterASPL(D)
+    assert L.aspl(res[:1])[0] == aspl and int(res[0]["levels"]) == diam
+    L.close()
+
+
+@pytest.mark.gpu
+def test_lift_level_cap_and_disconnected_base():
+    N, M, D = G.cyclic_lift(200, 6, 4, 5)
+    L = G.Lift(N, M, 4, 0)
+    L.set_base(D)
+    moves = G.gen_lift_moves(N, M, D, 10, 1)
+    full = L.eval(moves)
+    capped = L.eval(moves, max_levels=3)
+    assert (capped["connected"] == 0).all() and (capped["levels"] == 3).all()
+    for a, b in zip(full, capped):
+        assert int(b["reached"]) < int(a["reached"])
+    # two disjoint cycles of length N/2 (orbit diffs +-2): disconnected
+    N2, M2 = 64, 8
+    T = np.zeros((M2, 2), np.int32)
+    T[:, 0], T[:, 1] = 2, -2
+    L2 = G.Lift(N2, M2, 2, 0)
+    L2.set_base(T)
+    base = np.zeros(1, dtype=G.LIFT_EDIT_DTYPE)
+    r = L2.eval(base)
+    want = oracle_counts(N2, M2, T)
+    assert int(r[0]["connected"]) == 0 == want[3]
+    assert (int(r[0]["total"]), int(r[0]["reached"])) == (want[0], want[1])
+    L.close()
+    L2.close()
+
+
+@pytest.mark.gpu
+def test_lift_many_rounds():
+    N, M, D = G.cyclic_lift(512, 4, 8, 9)
+    L = G.Lift(N, M, 8, 0)
+    L.set_base(D)
+    L.set_group(2)
+    moves = G.gen_lift_moves(N, M, D, 21, 4)       # 11 rounds, the last one half full
+    check_all(L, N, M, D, moves, L.eval(moves))
+    assert L.last_ms() > 0
+    L.close()

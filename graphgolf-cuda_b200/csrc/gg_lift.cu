@@ -15,11 +15,15 @@
 // of its group.  A level is one pass over all (vertex, chunk) items:
 //     new = (OR_i F[(v + diff_g[v % M][i]) mod N][w]) & ~V[v][w];  V |= new;  F' = new
 // where g is the item's group, so neighbours always come from the item's own
-// candidate.  Lanes of a warp cover consecutive chunks of a vertex, so the
-// gathers of a neighbour row are contiguous 16-byte loads.  New pairs are
-// counted per group (warp-aggregated shared atomics, one global atomic per block,
-// group and level into counts[L][k]); after the grid barrier every block reads
-// the round's counts and the round ends when no candidate found a pair or every
+// candidate.  Each thread owns one chunk column w (so one group, one counter and
+// one table) and walks the vertices v = v0, v0 + VS, ...; consecutive lanes own
+// consecutive columns, so the gathers of a neighbour row are contiguous 16-byte
+// loads, all issued before the first is used.  Late in a round (past 85 % of its
+// pairs reached) a chunk gathers half its neighbours first and the rest only
+// while it still misses sources.  New pairs are counted per thread, reduced per
+// group at the end of the level (shared atomics, then one global atomic per block
+// and group into counts[L][k]); after the grid barrier every block reads the
+// round's counts, and the round ends when no candidate found a pair or every
 // candidate reached all M*N pairs.
 #include "gg.h"
 #include "gg_internal.h"
@@ -37,12 +41,16 @@ constexpr int kLiftBlock = 256;
 constexpr int kMaxGroup = 32;
 
 struct LiftArgs {
-    const int32_t *tab;              // [K][M][d] diffs in [0, N)
+    const int32_t *tab;              // [K][M][d] diffs in [0, N), rows 16-byte aligned when d % 4 == 0
     int N, M, d, K, G, cpc, W;       // W = G * cpc chunks per vertex
-    gg::FastDiv div_w, div_m, div_c; // t / W, v / M, w / cpc
+    unsigned cols_threads;           // threads that own a column: the largest multiple of W <= grid threads
+    unsigned vstep;                  // cols_threads / W: vertices between a thread's items
+    int half_ppm;                    // past this share of the round's pairs reached: half gathers
     uint4 *V, *F0, *F1;              // [N][W]
     unsigned long long *counts;      // [max_levels + 1][K]: pairs first reached at level L
     int max_levels;
+    unsigned long long *level_ns;    // [max_levels + 1]: device clock at the end of each
+                                     // level of the first round ([0]: its phase 0)
     gg::Ctl *ctl;
     unsigned expected;
     long long wait_ns;
@@ -65,43 +73,92 @@ __global__ void lift_tables(const int32_t *base, const gg_lift_edit *ed, int K, 
     }
 }
 
-__global__ void __launch_bounds__(kLiftBlock) lift_kernel(const LiftArgs a) {
+// OR of F[u][w] over the neighbours u of slots [B, E) of `row` (u = v + diff,
+// diff in [0, N)): every load of the span is issued before the first is used.
+template <int B, int E>
+__device__ __forceinline__ void gather_span(const int32_t *row, unsigned v, unsigned w, unsigned N, unsigned W,
+                                            const uint4 *Fc, uint4 &acc) {
+    int32_t df[E - B];
+    if constexpr (B % 4 == 0 && (E - B) % 4 == 0) {
+#pragma unroll
+        for (int i = 0; i < E - B; i += 4) {
+            const int4 q = __ldg(reinterpret_cast<const int4 *>(row + B + i));
+            df[i] = q.x; df[i + 1] = q.y; df[i + 2] = q.z; df[i + 3] = q.w;
+        }
+    } else {
+#pragma unroll
+        for (int i = 0; i < E - B; ++i) df[i] = __ldg(row + B + i);
+    }
+    uint4 x[E - B];
+#pragma unroll
+    for (int i = 0; i < E - B; ++i) {
+        const unsigned y = v + (unsigned)df[i];
+        const unsigned u = y >= N ? y - N : y;
+        x[i] = __ldcg(Fc + (size_t)u * W + w);
+    }
+#pragma unroll
+    for (int i = 0; i < E - B; ++i) gg::or_into(acc, x[i]);
+}
+
+// The same for a run-time degree: slots [b, e).
+__device__ __forceinline__ void gather_any(const int32_t *row, int b, int e, unsigned v, unsigned w, unsigned N,
+                                           unsigned W, const uint4 *Fc, uint4 &acc) {
+#pragma unroll 4
+    for (int i = b; i < e; ++i) {
+        const unsigned y = v + (unsigned)__ldg(row + i);
+        const unsigned u = y >= N ? y - N : y;
+        gg::or_into(acc, __ldcg(Fc + (size_t)u * W + w));
+    }
+}
+
+// D > 0: the degree at compile time; D == 0: a.d at run time.
+template <int D>
+__global__ void __launch_bounds__(kLiftBlock, 4) lift_kernel(const LiftArgs a) {
     __shared__ unsigned s_cnt[kMaxGroup];
-    const unsigned lane = threadIdx.x & 31u;
+    __shared__ unsigned long long s_reached[kMaxGroup];
+    __shared__ int s_half;
     if (threadIdx.x < kMaxGroup) s_cnt[threadIdx.x] = 0u;
     unsigned epoch = 0;
-    const unsigned items = (unsigned)a.N * (unsigned)a.W;
-    const unsigned stride = gridDim.x * blockDim.x;
-    const unsigned first = blockIdx.x * blockDim.x + threadIdx.x;
+    const unsigned tid = blockIdx.x * blockDim.x + threadIdx.x;
+    // this thread's column (threads past cols_threads own none)
+    const bool owner = tid < a.cols_threads;
+    const unsigned w = owner ? tid % (unsigned)a.W : 0u;
+    const unsigned g = w / (unsigned)a.cpc, cc = w - g * (unsigned)a.cpc;
+    const unsigned v0 = owner ? tid / (unsigned)a.W : (unsigned)a.N;
+    const unsigned N = (unsigned)a.N, W = (unsigned)a.W, M = (unsigned)a.M;
+    const unsigned vstep = a.vstep, rstep = vstep % M;
     const unsigned long long all_pairs = (unsigned long long)a.M * (unsigned long long)a.N;
+    const int dh = a.d / 2;
     const int rounds = (a.K + a.G - 1) / a.G;
     int zeroed = 1;        // rows 0 and 1 of counts are zeroed by the host
     int levels_run = 0;
     for (int rd = 0; rd < rounds; ++rd) {
         const int k0 = rd * a.G;
         const int live = min(a.G, a.K - k0);
-        // phase 0: the padding bits and the diagonal (source s is vertex s)
-        for (unsigned t = first; t < items; t += stride) {
-            const unsigned v = a.div_w.div(t), w = t - v * (unsigned)a.W;
-            const unsigned g = a.div_c.div(w), cc = w - g * (unsigned)a.cpc;
-            uint4 vis = make_uint4(0xffffffffu, 0xffffffffu, 0xffffffffu, 0xffffffffu), fr = gg::u4zero();
-            if ((int)g < live) {
-                vis = gg::pad_mask((int)cc, a.M);
-                if (v < (unsigned)a.M && (v >> 7) == cc) {
-                    const unsigned bit = 1u << (v & 31u);
-                    switch ((v >> 5) & 3u) {
-                        case 0: fr.x = bit; break;
-                        case 1: fr.y = bit; break;
-                        case 2: fr.z = bit; break;
-                        default: fr.w = bit; break;
-                    }
-                    gg::or_into(vis, fr);
+        const bool mine = owner && (int)g < live;   // a column of a live candidate
+        const int32_t *tab = a.tab + (size_t)(k0 + (mine ? (int)g : 0)) * a.M * a.d;
+        if (threadIdx.x == 0) s_half = 0;   // read after the next barrier
+        // phase 0: the padding bits and the diagonal (source s is vertex s);
+        // columns of candidates past the last one start full
+        const uint4 pad = mine ? gg::pad_mask((int)cc, a.M)
+                               : make_uint4(0xffffffffu, 0xffffffffu, 0xffffffffu, 0xffffffffu);
+        for (unsigned v = v0; v < N; v += vstep) {
+            uint4 vis = pad, fr = gg::u4zero();
+            if (mine && v < M && (v >> 7) == cc) {
+                const unsigned bit = 1u << (v & 31u);
+                switch ((v >> 5) & 3u) {
+                    case 0: fr.x = bit; break;
+                    case 1: fr.y = bit; break;
+                    case 2: fr.z = bit; break;
+                    default: fr.w = bit; break;
                 }
+                gg::or_into(vis, fr);
             }
-            a.V[t] = vis;
-            a.F0[t] = fr;
+            a.V[(size_t)v * W + w] = vis;
+            a.F0[(size_t)v * W + w] = fr;
         }
         if (!gg::grid_sync(a.ctl, a.expected, a.wait_ns, 0, epoch)) return;
+        if (rd == 0 && a.level_ns && blockIdx.x == 0 && threadIdx.x == 0) a.level_ns[0] = gg::gtimer();
         unsigned long long reached = threadIdx.x < (unsigned)live ? (unsigned long long)a.M : 0ull;
         for (int L = 1; L <= a.max_levels; ++L) {
             const uint4 *Fc = (L & 1) ? a.F0 : a.F1;
@@ -110,55 +167,85 @@ __global__ void __launch_bounds__(kLiftBlock) lift_kernel(const LiftArgs a) {
             if (blockIdx.x == 0 && L + 1 > zeroed && L + 1 <= a.max_levels)
                 for (int k = threadIdx.x; k < a.K; k += blockDim.x) a.counts[(size_t)(L + 1) * a.K + k] = 0ull;
             zeroed = max(zeroed, L + 1);
-            for (unsigned t0 = first - lane; t0 < items; t0 += stride) {
-                const unsigned t = t0 + lane;
-                unsigned c = 0;
-                int key = -1;
-                if (t < items) {
-                    const unsigned v = a.div_w.div(t), w = t - v * (unsigned)a.W;
-                    const unsigned g = a.div_c.div(w);
-                    const uint4 own = __ldcg(a.V + t);
-                    uint4 nw = gg::u4zero();
-                    if (!gg::u4full(own)) {
-                        // groups past `live` start full, so g < live here
-                        const unsigned r = v - a.div_m.div(v) * (unsigned)a.M;
-                        const int32_t *row = a.tab + ((size_t)(k0 + (int)g) * a.M + r) * a.d;
-                        uint4 acc = gg::u4zero();
-                        for (int i = 0; i < a.d; ++i) {
-                            unsigned u = v + (unsigned)__ldg(row + i);
-                            u -= u >= (unsigned)a.N ? (unsigned)a.N : 0u;
-                            gg::or_into(acc, __ldcg(Fc + (size_t)u * a.W + w));
+            const bool half = s_half != 0;
+            unsigned cnt = 0;
+            unsigned r = v0 % M;
+            for (unsigned v = v0; v < N; v += vstep) {
+                const size_t t = (size_t)v * W + w;
+                const uint4 own = __ldcg(a.V + t);
+                uint4 nw = gg::u4zero();
+                if (!gg::u4full(own)) {
+                    // full from phase 0 unless the column is a live candidate's
+                    const int32_t *row = tab + (size_t)r * a.d;
+                    uint4 acc = gg::u4zero();
+                    if constexpr (D > 0) {
+                        if (!half && D <= 12) {
+                            gather_span<0, D>(row, v, w, N, W, Fc, acc);
+                        } else if (!half) {   // two spans keep the loads within the registers
+                            gather_span<0, D / 2>(row, v, w, N, W, Fc, acc);
+                            gather_span<D / 2, D>(row, v, w, N, W, Fc, acc);
+                        } else {
+                            gather_span<0, D / 2>(row, v, w, N, W, Fc, acc);
+                            if (!gg::u4full(gg::u4or(own, acc))) gather_span<D / 2, D>(row, v, w, N, W, Fc, acc);
                         }
-                        nw = gg::andnot(acc, own);
-                        if (gg::u4any(nw)) {
-                            a.V[t] = gg::u4or(own, nw);
-                            c = gg::u4popc(nw);
-                            key = (int)g;
-                        }
+                    } else {
+                        gather_any(row, 0, half ? dh : a.d, v, w, N, W, Fc, acc);
+                        if (half && !gg::u4full(gg::u4or(own, acc))) gather_any(row, dh, a.d, v, w, N, W, Fc, acc);
                     }
-                    Fn[t] = nw;
+                    nw = gg::andnot(acc, own);
+                    if (gg::u4any(nw)) {
+                        a.V[t] = gg::u4or(own, nw);
+                        cnt += gg::u4popc(nw);
+                    }
                 }
-                const unsigned peers = __match_any_sync(0xffffffffu, key);
-                const unsigned sum = __reduce_add_sync(peers, c);
-                if (key >= 0 && (int)lane == __ffs((int)peers) - 1) atomicAdd(&s_cnt[key], sum);
+                Fn[t] = nw;
+                r += rstep;   // (v + vstep) % M
+                r -= r >= M ? M : 0u;
             }
+            // per group: lanes of one group share a key
+            const int key = cnt ? (int)g : -1;
+            const unsigned peers = __match_any_sync(0xffffffffu, key);
+            const unsigned sum = __reduce_add_sync(peers, cnt);
+            if (key >= 0 && (int)(threadIdx.x & 31u) == __ffs((int)peers) - 1) atomicAdd(&s_cnt[key], sum);
             __syncthreads();
             if (threadIdx.x < (unsigned)live && s_cnt[threadIdx.x]) {
                 atomicAdd(a.counts + (size_t)L * a.K + k0 + threadIdx.x, (unsigned long long)s_cnt[threadIdx.x]);
                 s_cnt[threadIdx.x] = 0u;
             }
             if (!gg::grid_sync(a.ctl, a.expected, a.wait_ns, L, epoch)) return;
+            if (rd == 0 && a.level_ns && blockIdx.x == 0 && threadIdx.x == 0) a.level_ns[L] = gg::gtimer();
             levels_run = max(levels_run, L);
             int more = 0;
             if (threadIdx.x < (unsigned)live) {
                 const unsigned long long n = gg::ld_relaxed_u64(a.counts + (size_t)L * a.K + k0 + threadIdx.x);
                 reached += n;
                 more = n != 0ull && reached < all_pairs;
+                s_reached[threadIdx.x] = reached;
+            }
+            __syncthreads();
+            if (threadIdx.x == 0) {
+                unsigned long long sum_r = 0;
+                for (int q = 0; q < live; ++q) sum_r += s_reached[q];
+                s_half = (double)sum_r > (double)a.half_ppm * 1e-6 * (double)live * (double)all_pairs;
             }
             if (!__syncthreads_or(more)) break;
         }
     }
     if (blockIdx.x == 0 && threadIdx.x == 0) a.ctl->levels_run = levels_run;
+}
+
+void *lift_kernel_for(int d) {
+    switch (d) {
+        case 3: return (void *)lift_kernel<3>;
+        case 4: return (void *)lift_kernel<4>;
+        case 5: return (void *)lift_kernel<5>;
+        case 6: return (void *)lift_kernel<6>;
+        case 8: return (void *)lift_kernel<8>;
+        case 10: return (void *)lift_kernel<10>;
+        case 12: return (void *)lift_kernel<12>;
+        case 16: return (void *)lift_kernel<16>;
+        default: return (void *)lift_kernel<0>;
+    }
 }
 
 gg_status lfail(gg_status s, const std::string &m) {
@@ -180,7 +267,7 @@ gg_status lfail(gg_status s, const std::string &m) {
 struct gg_lift {
     int N = 0, M = 0, d = 0, device = 0;
     int cpc = 0, g_auto = 1, g_max = 0, group = 0;   // group 0: automatic
-    int grid = 0, sms = 0;
+    int sms = 0;
     cudaStream_t stream = nullptr;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     int32_t *d_base = nullptr, *d_tab = nullptr;
@@ -190,6 +277,10 @@ struct gg_lift {
     unsigned long long *d_counts = nullptr, *h_counts = nullptr;
     size_t counts_cap = 0;                           // entries
     gg::Ctl *d_ctl = nullptr, *h_ctl = nullptr;
+    unsigned long long *d_level_ns = nullptr, *h_level_ns = nullptr;
+    int level_ns_n = 0;                              // entries the buffers hold
+    int grid = 0;                                    // blocks of the cooperative launch
+    int half_ppm = 850000;
     long long wait_ns = 10ll * 1000 * 1000 * 1000;
     bool base_set = false;
     float last_ms = 0.f;
@@ -204,6 +295,7 @@ void lift_free(gg_lift *h) {
     cudaFree(h->d_base); cudaFree(h->d_tab); cudaFree(h->d_ed); cudaFreeHost(h->h_ed);
     cudaFree(h->V); cudaFree(h->F0); cudaFree(h->F1);
     cudaFree(h->d_counts); cudaFreeHost(h->h_counts);
+    cudaFree(h->d_level_ns); cudaFreeHost(h->h_level_ns);
     cudaFree(h->d_ctl); cudaFreeHost(h->h_ctl);
     if (h->ev0) cudaEventDestroy(h->ev0);
     if (h->ev1) cudaEventDestroy(h->ev1);
@@ -234,6 +326,18 @@ gg_status ensure_counts(gg_lift *h, size_t entries) {
     return GG_OK;
 }
 
+gg_status alloc_group(gg_lift *h, int groups) {
+    cudaFree(h->V); cudaFree(h->F0); cudaFree(h->F1);
+    h->V = h->F0 = h->F1 = nullptr;
+    h->g_max = 0;
+    const size_t bits = (size_t)h->N * h->cpc * groups * sizeof(uint4);
+    GL_CK(cudaMalloc(&h->V, bits));
+    GL_CK(cudaMalloc(&h->F0, bits));
+    GL_CK(cudaMalloc(&h->F1, bits));
+    h->g_max = groups;
+    return GG_OK;
+}
+
 }  // namespace
 
 extern "C" {
@@ -254,13 +358,16 @@ gg_status gg_lift_create(int N, int M, int degree, int device, gg_lift **out) {
     if (cudaDeviceGetAttribute(&l2, cudaDevAttrL2CacheSize, device) != cudaSuccess ||
         cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, device) != cudaSuccess ||
         cudaDeviceGetAttribute(&h->sms, cudaDevAttrMultiProcessorCount, device) != cudaSuccess ||
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, lift_kernel, kLiftBlock, 0) != cudaSuccess)
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, lift_kernel_for(degree), kLiftBlock, 0) !=
+            cudaSuccess)
         return fail(lfail(GG_CUDA_ERROR, "device query failed"));
     if (!coop || per_sm < 1) return fail(lfail(GG_CUDA_ERROR, "cooperative launch unavailable"));
     h->grid = per_sm * h->sms;
     // one candidate's round share: three bitsets of N * cpc uint4
+    // (half the L2: lines gathered from both dies' SMs are held in both halves;
+    // at m=1024, g=32, d=12 a sweep of 2-7 candidates per round put the optimum at 5)
     const double per_cand = 3.0 * N * h->cpc * 16.0;
-    const int fit = (int)std::max(1.0, 0.75 * l2 / per_cand);
+    const int fit = (int)std::max(1.0, 0.5 * l2 / per_cand);
     // items N * W must stay below 2^31
     const long long by_items = std::max(1ll, (1ll << 31) / ((long long)N * h->cpc));
     h->g_auto = (int)std::min<long long>({(long long)fit, (long long)kMaxGroup, by_items});
@@ -270,15 +377,12 @@ gg_status gg_lift_create(int N, int M, int degree, int device, gg_lift **out) {
     if (e == cudaSuccess) e = cudaMalloc(&h->d_base, (size_t)M * degree * sizeof(int32_t));
     if (e == cudaSuccess) e = cudaMalloc(&h->d_ctl, sizeof(gg::Ctl));
     if (e == cudaSuccess) e = cudaMallocHost(&h->h_ctl, sizeof(gg::Ctl));
-    // bitsets for the automatic group (a larger group set later reallocates)
-    const size_t bits_auto = (size_t)N * h->cpc * h->g_auto * sizeof(uint4);
-    if (e == cudaSuccess) e = cudaMalloc(&h->V, bits_auto);
-    if (e == cudaSuccess) e = cudaMalloc(&h->F0, bits_auto);
-    if (e == cudaSuccess) e = cudaMalloc(&h->F1, bits_auto);
     if (e != cudaSuccess)
         return fail(lfail(e == cudaErrorMemoryAllocation ? GG_OUT_OF_MEMORY : GG_CUDA_ERROR,
                           cudaGetErrorString(e)));
-    h->g_max = h->g_auto;   // groups the bitsets hold
+    // bitsets for the automatic group (a larger group set later reallocates)
+    const gg_status s = alloc_group(h, h->g_auto);
+    if (s != GG_OK) return fail(s);
     *out = h;
     return GG_OK;
 }
@@ -303,14 +407,8 @@ gg_status gg_lift_set_group(gg_lift *h, int group) {
     if (need > h->g_max) {
         GL_CK(cudaSetDevice(h->device));
         GL_CK(cudaStreamSynchronize(h->stream));
-        cudaFree(h->V); cudaFree(h->F0); cudaFree(h->F1);
-        h->V = h->F0 = h->F1 = nullptr;
-        h->g_max = 0;
-        const size_t bits = (size_t)h->N * h->cpc * need * sizeof(uint4);
-        GL_CK(cudaMalloc(&h->V, bits));
-        GL_CK(cudaMalloc(&h->F0, bits));
-        GL_CK(cudaMalloc(&h->F1, bits));
-        h->g_max = need;
+        const gg_status s = alloc_group(h, need);
+        if (s != GG_OK) return s;
     }
     h->group = group;
     return GG_OK;
@@ -350,6 +448,13 @@ gg_status gg_lift_eval(gg_lift *h, int n_cand, const gg_lift_edit *edits, int ma
     const int ml = max_levels > 0 ? std::min(max_levels, h->N) : h->N;
     s = ensure_counts(h, (size_t)(ml + 1) * n_cand);
     if (s != GG_OK) return s;
+    if (ml + 1 > h->level_ns_n) {
+        cudaFree(h->d_level_ns); cudaFreeHost(h->h_level_ns);
+        h->d_level_ns = nullptr; h->h_level_ns = nullptr; h->level_ns_n = 0;
+        GL_CK(cudaMalloc(&h->d_level_ns, (size_t)(ml + 1) * sizeof(unsigned long long)));
+        GL_CK(cudaMallocHost(&h->h_level_ns, (size_t)(ml + 1) * sizeof(unsigned long long)));
+        h->level_ns_n = ml + 1;
+    }
     const int G = std::min(h->group ? h->group : h->g_auto, n_cand);
     const cudaStream_t st = h->stream;
     GL_CK(cudaMemcpyAsync(h->d_ed, h->h_ed, (size_t)n_cand * sizeof(gg_lift_edit), cudaMemcpyHostToDevice, st));
@@ -363,23 +468,29 @@ gg_status gg_lift_eval(gg_lift *h, int n_cand, const gg_lift_edit *edits, int ma
     LiftArgs a{};
     a.tab = h->d_tab;
     a.N = h->N; a.M = h->M; a.d = h->d; a.K = n_cand; a.G = G; a.cpc = h->cpc; a.W = G * h->cpc;
-    a.div_w = gg::FastDiv((uint32_t)a.W);
-    a.div_m = gg::FastDiv((uint32_t)h->M);
-    a.div_c = gg::FastDiv((uint32_t)h->cpc);
     a.V = h->V; a.F0 = h->F0; a.F1 = h->F1;
     a.counts = h->d_counts;
     a.max_levels = ml;
+    const unsigned threads = (unsigned)h->grid * kLiftBlock;
+    if ((unsigned)a.W > threads) return lfail(GG_BAD_ARG, "more chunk columns than threads: lower the group");
+    a.cols_threads = threads / (unsigned)a.W * (unsigned)a.W;
+    a.vstep = a.cols_threads / (unsigned)a.W;
+    a.half_ppm = h->half_ppm;
+    a.level_ns = h->d_level_ns;
     a.ctl = h->d_ctl;
-    a.expected = (unsigned)h->grid;
     a.wait_ns = h->wait_ns;
+    a.expected = (unsigned)h->grid;
+    GL_CK(cudaMemsetAsync(h->d_level_ns, 0, (size_t)(ml + 1) * sizeof(unsigned long long), st));
     void *args[] = {&a};
-    GL_CK(cudaLaunchCooperativeKernel((void *)lift_kernel, dim3(h->grid), dim3(kLiftBlock), args, 0, st));
+    GL_CK(cudaLaunchCooperativeKernel(lift_kernel_for(h->d), dim3(h->grid), dim3(kLiftBlock), args, 0, st));
     GL_CK(cudaEventRecord(h->ev1, st));
     GL_CK(cudaMemcpyAsync(h->h_ctl, h->d_ctl, sizeof(gg::Ctl), cudaMemcpyDeviceToHost, st));
     GL_CK(cudaStreamSynchronize(st));
     if (h->h_ctl->err) return lfail(GG_TIMEOUT, "grid barrier wait exceeded the limit");
     const int lr = std::min(h->h_ctl->levels_run, ml);
     GL_CK(cudaMemcpyAsync(h->h_counts, h->d_counts, (size_t)(lr + 1) * n_cand * sizeof(unsigned long long),
+                          cudaMemcpyDeviceToHost, st));
+    GL_CK(cudaMemcpyAsync(h->h_level_ns, h->d_level_ns, (size_t)(lr + 1) * sizeof(unsigned long long),
                           cudaMemcpyDeviceToHost, st));
     GL_CK(cudaStreamSynchronize(st));
     GL_CK(cudaEventElapsedTime(&h->last_ms, h->ev0, h->ev1));
@@ -397,6 +508,19 @@ gg_status gg_lift_eval(gg_lift *h, int n_cand, const gg_lift_edit *edits, int ma
         const bool capped = lev == ml && reach < all;
         out[k] = gg_cand_result{tot, reach, lev, (!capped && reach == all) ? 1 : 0};
     }
+    return GG_OK;
+}
+
+gg_status gg_lift_set_half_ppm(gg_lift *h, int half_ppm) {
+    if (!h || half_ppm < 0 || half_ppm > 1000000) return lfail(GG_BAD_ARG, "half_ppm must be in [0, 1e6]");
+    h->half_ppm = half_ppm;
+    return GG_OK;
+}
+
+gg_status gg_lift_last_level_ns(gg_lift *h, uint64_t *ns, int n) {
+    if (!h || !ns || n < 0) return lfail(GG_BAD_ARG, "bad arguments");
+    const int lr = h->h_ctl ? h->h_ctl->levels_run : 0;
+    for (int i = 0; i < n; ++i) ns[i] = (i <= lr && i < h->level_ns_n && h->h_level_ns) ? h->h_level_ns[i] : 0;
     return GG_OK;
 }
 

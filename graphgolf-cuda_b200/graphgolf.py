@@ -130,6 +130,8 @@ _SIGS = {
     "gg_lift_set_group": [_P, _I],
     "gg_lift_group": [_P, _IP],
     "gg_lift_last_ms": [_P, _DP],
+    "gg_lift_set_half_ppm": [_P, _I],
+    "gg_lift_last_level_ns": [_P, _P, _I],
     "gg_lift_destroy": [_P],
     "gg_gen_lift_moves": [_I, _I, _I, _P, _I, ctypes.c_uint64, _P],
 }
@@ -887,6 +889,17 @@ class Lift:
         g = ctypes.c_int()
         _check(lib().gg_lift_group(self._h, ctypes.byref(g)))
         return g.value
+
+    def set_half_ppm(self, half_ppm=850000):
+        _check(lib().gg_lift_set_half_ppm(self._h, half_ppm))
+
+    def last_level_us(self, n=64):
+        """Microseconds of each level of the last evaluation's first round
+        ([0]: phase 0 to the end of level 1 is entry 1 - entry 0)."""
+        ns = np.zeros(n, dtype=np.uint64)
+        _check(lib().gg_lift_last_level_ns(self._h, _ptr(ns), n))
+        k = int(np.count_nonzero(ns))
+        return np.diff(ns[:k].astype(np.int64)) / 1000.0
 
     def last_ms(self):
         ms = ctypes.c_double()

@@ -278,9 +278,16 @@ gg_status gg_lift_set_base(gg_lift *h, const int32_t *diffs);
 gg_status gg_lift_eval(gg_lift *h, int n_cand, const gg_lift_edit *edits, int max_levels,
                        gg_cand_result *out);
 /* Candidates that run side by side in one round (1..32; 0 = automatic: as many as
- * keep the round's bitsets within 3/4 of the L2). */
+ * keep the round's bitsets within half of the L2). */
 gg_status gg_lift_set_group(gg_lift *h, int group);
 gg_status gg_lift_group(gg_lift *h, int *group);
+/* Tuning: past half_ppm parts per million of a round's pairs reached, a chunk
+ * gathers half its neighbours first and the rest only while it still misses
+ * sources (default 850000; 1000000 = never). */
+gg_status gg_lift_set_half_ppm(gg_lift *h, int half_ppm);
+/* Device clock (ns) at the end of each level of the last evaluation's first round
+ * ([0]: its phase 0), entries past the levels run are 0. */
+gg_status gg_lift_last_level_ns(gg_lift *h, uint64_t *ns, int n);
 /* Device milliseconds of the last gg_lift_eval (table build and BFS launch). */
 gg_status gg_lift_last_ms(gg_lift *h, double *ms);
 gg_status gg_lift_destroy(gg_lift *h);

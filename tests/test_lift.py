@@ -135,3 +135,16 @@ def test_lift_many_rounds():
     check_all(L, N, M, D, moves, L.eval(moves))
     assert L.last_ms() > 0
     L.close()
+
+
+@pytest.mark.gpu
+def test_lift_annealing_improves_and_reports_exact_aspl():
+    import anneal as A
+    N, M, D = G.cyclic_lift(64, 8, 4, 2)
+    start = O.conv_diameter_aspl(N, M, D)[1]
+    best, tr = A.anneal_lift(N, M, D, 80, seed=3, exact=16)
+    assert tr.steps == 80 and tr.accepted > 0 and tr.exact_evals == 80 * 16
+    assert lift_ok(N, M, best)
+    diam, aspl = O.conv_diameter_aspl(N, M, best)
+    assert aspl == tr.final_best and aspl < start
+    assert all(b >= c for b, c in zip(tr.best, tr.best[1:]))

@@ -49,8 +49,8 @@ struct LiftArgs {
     uint4 *V, *F0, *F1;              // [N][W]
     unsigned long long *counts;      // [max_levels + 1][K]: pairs first reached at level L
     int max_levels;
-    unsigned long long *level_ns;    // [max_levels + 1]: device clock at the end of each
-                                     // level of the first round ([0]: its phase 0)
+    unsigned long long *level_ns;    // [max_levels + 1]: device clock at the start ([0]) and
+                                     // at the end of each level of the first round
     gg::Ctl *ctl;
     unsigned expected;
     long long wait_ns;
@@ -111,6 +111,82 @@ __device__ __forceinline__ void gather_any(const int32_t *row, int b, int e, uns
     }
 }
 
+// The sources among the pull neighbours of v (diff row `row`, slots [B, E))
+// that lie in the chunk of sources [lo, lo + 128) with index < M, as bits.
+template <int B, int E>
+__device__ __forceinline__ void sources_span(const int32_t *row, unsigned v, unsigned lo, unsigned N, unsigned M,
+                                             unsigned nb[4]) {
+    int32_t df[E - B];
+    if constexpr (B % 4 == 0 && (E - B) % 4 == 0) {
+#pragma unroll
+        for (int i = 0; i < E - B; i += 4) {
+            const int4 q = __ldg(reinterpret_cast<const int4 *>(row + B + i));
+            df[i] = q.x; df[i + 1] = q.y; df[i + 2] = q.z; df[i + 3] = q.w;
+        }
+    } else {
+#pragma unroll
+        for (int i = 0; i < E - B; ++i) df[i] = __ldg(row + B + i);
+    }
+#pragma unroll
+    for (int i = 0; i < E - B; ++i) {
+        const unsigned y = v + (unsigned)df[i];
+        const unsigned sv = y >= N ? y - N : y;
+        const unsigned o = sv - lo;
+        if (sv < M && o < 128u) nb[o >> 5] |= 1u << (o & 31u);
+    }
+}
+
+// The reset pass of a round with level 1 folded in: the pairs a chunk (v, w)
+// reaches at level 1 are the sources s among its pull neighbours (s = v + diff
+// < M, in the chunk), so the pass writes the padding bits, the diagonal and those
+// pairs into V and their frontier into F1 (`Fn`) without a gather.  Columns of
+// candidates past the last one (mine == false) start full.  Returns the
+// thread's new pairs.
+template <int D>
+__device__ __forceinline__ unsigned level1_pass(const LiftArgs &a, const int32_t *tab, unsigned v0,
+                                                unsigned vstep, unsigned rstep, unsigned w, unsigned cc,
+                                                bool mine, uint4 *Fn) {
+    const unsigned N = (unsigned)a.N, M = (unsigned)a.M, W = (unsigned)a.W;
+    const uint4 pad = mine ? gg::pad_mask((int)cc, a.M)
+                           : make_uint4(0xffffffffu, 0xffffffffu, 0xffffffffu, 0xffffffffu);
+    const unsigned lo = cc * 128u;     // sources of this chunk: [lo, lo + 128) of the group
+    unsigned cnt = 0, r = v0 % M;
+    for (unsigned v = v0; v < N; v += vstep) {
+        uint4 vis = pad, n1 = gg::u4zero();
+        if (mine) {
+            if (v - lo < 128u) {   // the diagonal (bits past M are padding, already set)
+                const unsigned bit = 1u << (v & 31u);
+                switch ((v - lo) >> 5) {
+                    case 0: vis.x |= bit; break;
+                    case 1: vis.y |= bit; break;
+                    case 2: vis.z |= bit; break;
+                    default: vis.w |= bit; break;
+                }
+            }
+            const int32_t *row = tab + (size_t)r * a.d;
+            unsigned nb[4] = {0u, 0u, 0u, 0u};
+            if constexpr (D > 0) {
+                sources_span<0, D>(row, v, lo, N, M, nb);
+            } else {
+                for (int i = 0; i < a.d; ++i) {
+                    const unsigned y = v + (unsigned)__ldg(row + i);
+                    const unsigned sv = y >= N ? y - N : y;
+                    const unsigned o = sv - lo;
+                    if (sv < M && o < 128u) nb[o >> 5] |= 1u << (o & 31u);
+                }
+            }
+            n1 = gg::andnot(make_uint4(nb[0], nb[1], nb[2], nb[3]), vis);
+            gg::or_into(vis, n1);
+            cnt += gg::u4popc(n1);
+        }
+        a.V[(size_t)v * W + w] = vis;
+        Fn[(size_t)v * W + w] = n1;
+        r += rstep;
+        r -= r >= M ? M : 0u;
+    }
+    return cnt;
+}
+
 // D > 0: the degree at compile time; D == 0: a.d at run time.
 template <int D>
 __global__ void __launch_bounds__(kLiftBlock, 4) lift_kernel(const LiftArgs a) {
@@ -138,26 +214,6 @@ __global__ void __launch_bounds__(kLiftBlock, 4) lift_kernel(const LiftArgs a) {
         const bool mine = owner && (int)g < live;   // a column of a live candidate
         const int32_t *tab = a.tab + (size_t)(k0 + (mine ? (int)g : 0)) * a.M * a.d;
         if (threadIdx.x == 0) s_half = 0;   // read after the next barrier
-        // phase 0: the padding bits and the diagonal (source s is vertex s);
-        // columns of candidates past the last one start full
-        const uint4 pad = mine ? gg::pad_mask((int)cc, a.M)
-                               : make_uint4(0xffffffffu, 0xffffffffu, 0xffffffffu, 0xffffffffu);
-        for (unsigned v = v0; v < N; v += vstep) {
-            uint4 vis = pad, fr = gg::u4zero();
-            if (mine && v < M && (v >> 7) == cc) {
-                const unsigned bit = 1u << (v & 31u);
-                switch ((v >> 5) & 3u) {
-                    case 0: fr.x = bit; break;
-                    case 1: fr.y = bit; break;
-                    case 2: fr.z = bit; break;
-                    default: fr.w = bit; break;
-                }
-                gg::or_into(vis, fr);
-            }
-            a.V[(size_t)v * W + w] = vis;
-            a.F0[(size_t)v * W + w] = fr;
-        }
-        if (!gg::grid_sync(a.ctl, a.expected, a.wait_ns, 0, epoch)) return;
         if (rd == 0 && a.level_ns && blockIdx.x == 0 && threadIdx.x == 0) a.level_ns[0] = gg::gtimer();
         unsigned long long reached = threadIdx.x < (unsigned)live ? (unsigned long long)a.M : 0ull;
         for (int L = 1; L <= a.max_levels; ++L) {
@@ -167,40 +223,45 @@ __global__ void __launch_bounds__(kLiftBlock, 4) lift_kernel(const LiftArgs a) {
             if (blockIdx.x == 0 && L + 1 > zeroed && L + 1 <= a.max_levels)
                 for (int k = threadIdx.x; k < a.K; k += blockDim.x) a.counts[(size_t)(L + 1) * a.K + k] = 0ull;
             zeroed = max(zeroed, L + 1);
-            const bool half = s_half != 0;
             unsigned cnt = 0;
             unsigned r = v0 % M;
-            for (unsigned v = v0; v < N; v += vstep) {
-                const size_t t = (size_t)v * W + w;
-                const uint4 own = __ldcg(a.V + t);
-                uint4 nw = gg::u4zero();
-                if (!gg::u4full(own)) {
-                    // full from phase 0 unless the column is a live candidate's
-                    const int32_t *row = tab + (size_t)r * a.d;
-                    uint4 acc = gg::u4zero();
-                    if constexpr (D > 0) {
-                        if (!half && D <= 12) {
-                            gather_span<0, D>(row, v, w, N, W, Fc, acc);
-                        } else if (!half) {   // two spans keep the loads within the registers
-                            gather_span<0, D / 2>(row, v, w, N, W, Fc, acc);
-                            gather_span<D / 2, D>(row, v, w, N, W, Fc, acc);
+            if (L == 1) {
+                // level 1 is the round's reset pass
+                cnt = level1_pass<D>(a, tab, v0, vstep, rstep, w, cc, mine, Fn);
+            } else {
+                const bool half = s_half != 0;
+                for (unsigned v = v0; v < N; v += vstep) {
+                    const size_t t = (size_t)v * W + w;
+                    const uint4 own = __ldcg(a.V + t);
+                    uint4 nw = gg::u4zero();
+                    if (!gg::u4full(own)) {
+                        // full from the reset pass unless the column is a live candidate's
+                        const int32_t *row = tab + (size_t)r * a.d;
+                        uint4 acc = gg::u4zero();
+                        if constexpr (D > 0) {
+                            if (!half && D <= 12) {
+                                gather_span<0, D>(row, v, w, N, W, Fc, acc);
+                            } else if (!half) {   // two spans keep the loads within the registers
+                                gather_span<0, D / 2>(row, v, w, N, W, Fc, acc);
+                                gather_span<D / 2, D>(row, v, w, N, W, Fc, acc);
+                            } else {
+                                gather_span<0, D / 2>(row, v, w, N, W, Fc, acc);
+                                if (!gg::u4full(gg::u4or(own, acc))) gather_span<D / 2, D>(row, v, w, N, W, Fc, acc);
+                            }
                         } else {
-                            gather_span<0, D / 2>(row, v, w, N, W, Fc, acc);
-                            if (!gg::u4full(gg::u4or(own, acc))) gather_span<D / 2, D>(row, v, w, N, W, Fc, acc);
+                            gather_any(row, 0, half ? dh : a.d, v, w, N, W, Fc, acc);
+                            if (half && !gg::u4full(gg::u4or(own, acc))) gather_any(row, dh, a.d, v, w, N, W, Fc, acc);
                         }
-                    } else {
-                        gather_any(row, 0, half ? dh : a.d, v, w, N, W, Fc, acc);
-                        if (half && !gg::u4full(gg::u4or(own, acc))) gather_any(row, dh, a.d, v, w, N, W, Fc, acc);
+                        nw = gg::andnot(acc, own);
+                        if (gg::u4any(nw)) {
+                            a.V[t] = gg::u4or(own, nw);
+                            cnt += gg::u4popc(nw);
+                        }
                     }
-                    nw = gg::andnot(acc, own);
-                    if (gg::u4any(nw)) {
-                        a.V[t] = gg::u4or(own, nw);
-                        cnt += gg::u4popc(nw);
-                    }
+                    Fn[t] = nw;
+                    r += rstep;   // (v + vstep) % M
+                    r -= r >= M ? M : 0u;
                 }
-                Fn[t] = nw;
-                r += rstep;   // (v + vstep) % M
-                r -= r >= M ? M : 0u;
             }
             // per group: lanes of one group share a key
             const int key = cnt ? (int)g : -1;

@@ -894,8 +894,8 @@ class Lift:
         _check(lib().gg_lift_set_half_ppm(self._h, half_ppm))
 
     def last_level_us(self, n=64):
-        """Microseconds of each level of the last evaluation's first round
-        ([0]: phase 0 to the end of level 1 is entry 1 - entry 0)."""
+        """Microseconds of each level of the last evaluation's first round (level 1
+        includes the reset of the round's bitsets)."""
         ns = np.zeros(n, dtype=np.uint64)
         _check(lib().gg_lift_last_level_ns(self._h, _ptr(ns), n))
         k = int(np.count_nonzero(ns))

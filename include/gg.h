@@ -285,8 +285,8 @@ gg_status gg_lift_group(gg_lift *h, int *group);
  * gathers half its neighbours first and the rest only while it still misses
  * sources (default 850000; 1000000 = never). */
 gg_status gg_lift_set_half_ppm(gg_lift *h, int half_ppm);
-/* Device clock (ns) at the end of each level of the last evaluation's first round
- * ([0]: its phase 0), entries past the levels run are 0. */
+/* Device clock (ns) at the start ([0]) and at the end of each level ([L]) of the
+ * last evaluation's first round; entries past the levels run are 0. */
 gg_status gg_lift_last_level_ns(gg_lift *h, uint64_t *ns, int n);
 /* Device milliseconds of the last gg_lift_eval (table build and BFS launch). */
 gg_status gg_lift_last_ms(gg_lift *h, double *ms);

@@ -179,67 +179,111 @@ gg_status gg_gen_swaps(int n, int degree, const int32_t *adj, int base_id, int c
     return GG_OK;
 }
 
-// Moves of a cyclic lift (see gg.h).  Slot (r, i) of the diff table is the orbit
-// edge from orbit vertex r to vertex (r + diff) mod N, of orbit (r + diff) mod N mod M;
-// its reverse slot is the first slot of that orbit's row holding -diff mod N
-// (the search of cppcode/annealing.cpp:117-124).  A new shift for an edge from
-// orbit x to orbit y is (y - x) + M k, k uniform in [0, N/M) (:131, :178, :187).
-gg_status gg_gen_lift_moves(int N, int M, int degree, const int32_t *diffs, int count, uint64_t seed,
-                            gg_lift_edit *out) {
-    if (!diffs || !out || M < 1 || N < 2 || M > N || N % M != 0 || degree < 1 || count < 0)
-        return GG_BAD_ARG;
-    const long long NN = N;
-    auto norm = [&](long long x) { return (int32_t)(((x % NN) + NN) % NN); };
-    std::vector<int32_t> nd((size_t)M * degree);
-    for (size_t k = 0; k < nd.size(); ++k) nd[k] = norm(diffs[k]);
-    auto at = [&](int r, int i) -> int32_t & { return nd[(size_t)r * degree + i]; };
-    // reverse slot of (r, i): -1 if none
+}  // extern "C"
+
+namespace {
+
+// Moves of a lift of K = 1, 2 or 3 axes (see gg.h).  Axis j has the lifted size
+// n[j] and the orbit size m[j]; orbit row r has coordinates r_j (row-major, last
+// axis fastest, the calculators' table order).  Slot (r, i) holds the diff vector
+// of an orbit edge from orbit r to orbit (r_j + diff_j) mod n_j mod m_j; its reverse
+// slot is the first slot of that orbit's row holding -diff (componentwise mod n_j),
+// the search of cppcode/annealing.cpp:117-124 and pieceannealing.cpp:126-133.  A
+// new shift for an edge from orbit x to orbit y is (y_j - x_j) + m_j k_j, k_j
+// uniform in [0, n_j / m_j) (annealing.cpp:131, pieceannealing.cpp:135-136).
+gg_status lift_moves(int K, const int n[3], const int m[3], int degree, const int32_t *table, int count,
+                     uint64_t seed, gg_lift_edit *out) {
+    if (!table || !out || K < 1 || K > 3 || degree < 1 || count < 0) return GG_BAD_ARG;
+    int M = 1;
+    bool lifted = false;
+    for (int j = 0; j < K; ++j) {
+        if (m[j] < 1 || n[j] < 1 || m[j] > n[j] || n[j] % m[j] != 0) return GG_BAD_ARG;
+        M *= m[j];
+        lifted |= n[j] / m[j] > 1;
+    }
+    struct Vec { int32_t c[3]; };
+    auto norm = [&](long long x, int j) { return (int32_t)(((x % n[j]) + n[j]) % n[j]); };
+    std::vector<Vec> nd((size_t)M * degree);
+    for (size_t q = 0; q < nd.size(); ++q) {
+        nd[q] = Vec{{0, 0, 0}};
+        for (int j = 0; j < K; ++j) nd[q].c[j] = norm(table[q * K + j], j);
+    }
+    auto at = [&](int r, int i) -> Vec & { return nd[(size_t)r * degree + i]; };
+    auto coords = [&](int r, int c[3]) {
+        for (int j = K - 1; j >= 0; --j) { c[j] = r % m[j]; r /= m[j]; }
+    };
+    auto row_of = [&](const int c[3]) {
+        int r = 0;
+        for (int j = 0; j < K; ++j) r = r * m[j] + c[j];
+        return r;
+    };
+    auto zero = [&](const Vec &v) { return v.c[0] == 0 && v.c[1] == 0 && v.c[2] == 0; };
+    auto same = [&](const Vec &a, const Vec &b) { return a.c[0] == b.c[0] && a.c[1] == b.c[1] && a.c[2] == b.c[2]; };
+    auto neg = [&](const Vec &v) {
+        Vec w{{0, 0, 0}};
+        for (int j = 0; j < K; ++j) w.c[j] = norm(-(long long)v.c[j], j);
+        return w;
+    };
+    auto target = [&](int r, const Vec &v) {
+        int c[3] = {0, 0, 0};
+        coords(r, c);
+        for (int j = 0; j < K; ++j) c[j] = (int)(((long long)c[j] + v.c[j]) % n[j] % m[j]);
+        return row_of(c);
+    };
     auto reverse = [&](int r, int i, int *rr) {
-        const int32_t df = at(r, i);
-        const int to = (int)(((long long)r + df) % NN % M);
-        const int32_t back = norm(-(long long)df);
-        for (int j = 0; j < degree; ++j)
-            if (at(to, j) == back && !(to == r && j == i)) { *rr = to; return j; }
+        const int to = target(r, at(r, i));
+        const Vec back = neg(at(r, i));
+        for (int q = 0; q < degree; ++q)
+            if (same(at(to, q), back) && !(to == r && q == i)) { *rr = to; return q; }
         return -1;
     };
-    // rows touched by an edit stay simple: nonzero, pairwise distinct diffs
-    auto simple_after = [&](const gg_lift_edit &e) {
-        for (int j = 0; j < e.count; ++j) {
-            const int r = e.row[j];
-            std::vector<int32_t> row(nd.begin() + (size_t)r * degree, nd.begin() + (size_t)(r + 1) * degree);
-            for (int k = 0; k < e.count; ++k)
-                if (e.row[k] == r) row[e.slot[k]] = e.diff[k];
+    Rng rng(seed);
+    auto shift = [&](int from, int to) {
+        int a[3] = {0, 0, 0}, b[3] = {0, 0, 0};
+        coords(from, a);
+        coords(to, b);
+        Vec v{{0, 0, 0}};
+        for (int j = 0; j < K; ++j)
+            v.c[j] = norm((long long)(b[j] - a[j]) + (long long)m[j] * rng.below((uint32_t)(n[j] / m[j])), j);
+        return v;
+    };
+    // rows touched by an edit stay simple: edited slots nonzero, nonzero diffs pairwise distinct
+    auto simple_after = [&](int cnt, const int *er, const int *es, const Vec *ev) {
+        for (int j = 0; j < cnt; ++j) {
+            std::vector<Vec> row(nd.begin() + (size_t)er[j] * degree, nd.begin() + (size_t)(er[j] + 1) * degree);
+            std::vector<char> edited(degree, 0);
+            for (int k = 0; k < cnt; ++k)
+                if (er[k] == er[j]) { row[es[k]] = ev[k]; edited[es[k]] = 1; }
             for (int k = 0; k < degree; ++k) {
-                bool edited = false;
-                for (int q = 0; q < e.count; ++q) edited |= e.row[q] == r && e.slot[q] == k;
-                if (edited && row[k] == 0) return false;
-                if (row[k] == 0) continue;
+                if (zero(row[k])) {
+                    if (edited[k]) return false;
+                    continue;
+                }
                 for (int q = k + 1; q < degree; ++q)
-                    if (row[q] == row[k]) return false;
+                    if (same(row[q], row[k])) return false;
             }
         }
         return true;
     };
-    const uint32_t lifts = (uint32_t)(N / M);
-    Rng rng(seed);
     for (int c = 0; c < count; ++c) {
         for (long long tries = 0;; ++tries) {
             if (tries > 1000000) return GG_BAD_ARG;
-            gg_lift_edit e{};
-            const bool shift = lifts > 1 && rng.below(2) == 0;
+            const bool sh = lifted && rng.below(2) == 0;
             const int a = (int)rng.below((uint32_t)M), ia = (int)rng.below((uint32_t)degree);
-            if (at(a, ia) == 0) continue;
+            if (zero(at(a, ia))) continue;
             int b = -1;
             const int ib = reverse(a, ia, &b);
             if (ib < 0) continue;
-            if (shift) {
-                const int32_t df = norm((long long)(b - a) + (long long)M * rng.below(lifts));
-                e.count = 2;
-                e.row[0] = a; e.slot[0] = ia; e.diff[0] = df;
-                e.row[1] = b; e.slot[1] = ib; e.diff[1] = norm(-(long long)df);
+            int er[4], es[4], cnt;
+            Vec ev[4];
+            if (sh) {
+                const Vec v = shift(a, b);
+                cnt = 2;
+                er[0] = a; es[0] = ia; ev[0] = v;
+                er[1] = b; es[1] = ib; ev[1] = neg(v);
             } else {
                 const int cc = (int)rng.below((uint32_t)M), ic = (int)rng.below((uint32_t)degree);
-                if (at(cc, ic) == 0) continue;
+                if (zero(at(cc, ic))) continue;
                 int d = -1;
                 const int id = reverse(cc, ic, &d);
                 if (id < 0) continue;
@@ -249,20 +293,51 @@ gg_status gg_gen_lift_moves(int N, int M, int degree, const int32_t *diffs, int 
                     for (int y = x + 1; y < 4; ++y) distinct &= !(rs[x] == rs[y] && ss[x] == ss[y]);
                 if (!distinct) continue;  // the same orbit edge twice
                 // a-b, c-d -> a-d, b-c
-                const int32_t dad = norm((long long)(d - a) + (long long)M * rng.below(lifts));
-                const int32_t dbc = norm((long long)(cc - b) + (long long)M * rng.below(lifts));
-                e.count = 4;
-                e.row[0] = a;  e.slot[0] = ia; e.diff[0] = dad;
-                e.row[1] = d;  e.slot[1] = id; e.diff[1] = norm(-(long long)dad);
-                e.row[2] = b;  e.slot[2] = ib; e.diff[2] = dbc;
-                e.row[3] = cc; e.slot[3] = ic; e.diff[3] = norm(-(long long)dbc);
+                const Vec vad = shift(a, d), vbc = shift(b, cc);
+                cnt = 4;
+                er[0] = a;  es[0] = ia; ev[0] = vad;
+                er[1] = d;  es[1] = id; ev[1] = neg(vad);
+                er[2] = b;  es[2] = ib; ev[2] = vbc;
+                er[3] = cc; es[3] = ic; ev[3] = neg(vbc);
             }
-            if (!simple_after(e)) continue;
+            if (!simple_after(cnt, er, es, ev)) continue;
+            gg_lift_edit e{};
+            e.count = cnt;
+            for (int j = 0; j < cnt; ++j) {
+                e.row[j] = er[j];
+                e.slot[j] = es[j];
+                for (int q = 0; q < 3; ++q) e.diff[j][q] = ev[j].c[q];
+            }
             out[c] = e;
             break;
         }
     }
     return GG_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+gg_status gg_gen_lift_moves(int N, int M, int degree, const int32_t *diffs, int count, uint64_t seed,
+                            gg_lift_edit *out) {
+    const int n[3] = {N, 1, 1}, m[3] = {M, 1, 1};
+    if (N < 2) return GG_BAD_ARG;
+    return lift_moves(1, n, m, degree, diffs, count, seed, out);
+}
+
+gg_status gg_gen_piece_moves(int Nx, int Ny, int Mx, int My, int degree, const int32_t *vals, int count,
+                             uint64_t seed, gg_lift_edit *out) {
+    const int n[3] = {Nx, Ny, 1}, m[3] = {Mx, My, 1};
+    if ((long long)Nx * Ny < 2) return GG_BAD_ARG;
+    return lift_moves(2, n, m, degree, vals, count, seed, out);
+}
+
+gg_status gg_gen_box_moves(int Nx, int Ny, int Nz, int Mx, int My, int Mz, int degree, const int32_t *vals,
+                           int count, uint64_t seed, gg_lift_edit *out) {
+    const int n[3] = {Nx, Ny, Nz}, m[3] = {Mx, My, Mz};
+    if ((long long)Nx * Ny * Nz < 2) return GG_BAD_ARG;
+    return lift_moves(3, n, m, degree, vals, count, seed, out);
 }
 
 gg_status gg_gen_cyclic_lift(int m, int g, int d, uint64_t seed, int32_t *diffs) {

@@ -41,7 +41,9 @@ constexpr int kLiftBlock = 256;
 constexpr int kMaxGroup = 32;
 
 struct LiftArgs {
-    const int32_t *tab;              // [K][M][d] diffs in [0, N), rows 16-byte aligned when d % 4 == 0
+    const int32_t *tab;              // part form: [K][M][d] diffs in [0, N), rows 16-byte aligned when d % 4 == 0
+    const int32_t *adj;              // piece / box: [K][N][d] pull adjacency of each candidate
+    const int32_t *inv;              // piece / box: [N] representative index of a vertex, or -1
     int N, M, d, K, G, cpc, W;       // W = G * cpc chunks per vertex
     unsigned cols_threads;           // threads that own a column: the largest multiple of W <= grid threads
     unsigned vstep;                  // cols_threads / W: vertices between a thread's items
@@ -56,26 +58,50 @@ struct LiftArgs {
     long long wait_ns;
 };
 
-// Candidate tables: entry (k, r, i) is the base entry unless candidate k's edit
-// names slot (r, i).
-__global__ void lift_tables(const int32_t *base, const gg_lift_edit *ed, int K, int M, int d, int32_t *tab) {
+// Candidate tables ([K][M][d][comps], comps = axes of the lift): slot (k, r, i)
+// is the base slot unless candidate k's edit names slot (r, i).
+__global__ void lift_tables(const int32_t *base, const gg_lift_edit *ed, int K, int M, int d, int comps,
+                            int32_t *tab) {
     const long long per = (long long)M * d, total = per * K;
     for (long long x = (long long)blockIdx.x * blockDim.x + threadIdx.x; x < total;
          x += (long long)gridDim.x * blockDim.x) {
         const int k = (int)(x / per);
         const int e = (int)(x - (long long)k * per);
         const int r = e / d, i = e - r * d;
-        int32_t v = __ldg(base + e);
         const gg_lift_edit &q = ed[k];
+        int hit = -1;
         for (int j = 0; j < q.count; ++j)
-            if (q.row[j] == r && q.slot[j] == i) v = q.diff[j];
-        tab[x] = v;
+            if (q.row[j] == r && q.slot[j] == i) hit = j;
+        for (int c = 0; c < comps; ++c)
+            tab[x * comps + c] = hit >= 0 ? q.diff[hit][c] : __ldg(base + (size_t)e * comps + c);
+    }
+}
+
+// Pull adjacency of every candidate of a 2-D or 3-D torus lift (axes sizes n,
+// orbit sizes m; vertex (x * ny + y) * nz + z), from its table of diffs already
+// reduced to [0, n): the expansion of cudaASPLpiece.cu:41-50 / cudaASPLbox.cu:44-57.
+__global__ void lift_expand(const int32_t *tab, int K, int M, int d, int comps, int nx, int ny, int nz, int mx,
+                            int my, int mz, int32_t *adj) {
+    const long long N = (long long)nx * ny * nz, per = N * d, total = per * K;
+    for (long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x; q < total;
+         q += (long long)gridDim.x * blockDim.x) {
+        const int k = (int)(q / per);
+        const long long e = q - (long long)k * per;
+        const int v = (int)(e / d), i = (int)(e - (long long)v * d);
+        const int x = v / (ny * nz), rem = v - x * (ny * nz), y = rem / nz, z = rem - y * nz;
+        const int r = ((x % mx) * my + (y % my)) * mz + (z % mz);
+        const int32_t *t = tab + (((size_t)k * M + r) * d + i) * comps;
+        int tx = x + t[0], ty = y + t[1], tz = comps > 2 ? z + t[2] : z;
+        tx -= tx >= nx ? nx : 0;
+        ty -= ty >= ny ? ny : 0;
+        tz -= tz >= nz ? nz : 0;
+        adj[q] = (tx * ny + ty) * nz + tz;
     }
 }
 
 // OR of F[u][w] over the neighbours u of slots [B, E) of `row` (u = v + diff,
 // diff in [0, N)): every load of the span is issued before the first is used.
-template <int B, int E>
+template <int B, int E, bool EXPL>
 __device__ __forceinline__ void gather_span(const int32_t *row, unsigned v, unsigned w, unsigned N, unsigned W,
                                             const uint4 *Fc, uint4 &acc) {
     int32_t df[E - B];
@@ -92,8 +118,11 @@ __device__ __forceinline__ void gather_span(const int32_t *row, unsigned v, unsi
     uint4 x[E - B];
 #pragma unroll
     for (int i = 0; i < E - B; ++i) {
-        const unsigned y = v + (unsigned)df[i];
-        const unsigned u = y >= N ? y - N : y;
+        unsigned u = (unsigned)df[i];
+        if constexpr (!EXPL) {   // a diff: u = (v + diff) mod N
+            u += v;
+            u -= u >= N ? N : 0u;
+        }
         x[i] = __ldcg(Fc + (size_t)u * W + w);
     }
 #pragma unroll
@@ -101,21 +130,33 @@ __device__ __forceinline__ void gather_span(const int32_t *row, unsigned v, unsi
 }
 
 // The same for a run-time degree: slots [b, e).
+template <bool EXPL>
 __device__ __forceinline__ void gather_any(const int32_t *row, int b, int e, unsigned v, unsigned w, unsigned N,
                                            unsigned W, const uint4 *Fc, uint4 &acc) {
 #pragma unroll 4
     for (int i = b; i < e; ++i) {
-        const unsigned y = v + (unsigned)__ldg(row + i);
-        const unsigned u = y >= N ? y - N : y;
+        unsigned u = (unsigned)__ldg(row + i);
+        if constexpr (!EXPL) {
+            u += v;
+            u -= u >= N ? N : 0u;
+        }
         gg::or_into(acc, __ldcg(Fc + (size_t)u * W + w));
     }
 }
 
-// The sources among the pull neighbours of v (diff row `row`, slots [B, E))
-// that lie in the chunk of sources [lo, lo + 128) with index < M, as bits.
-template <int B, int E>
+// Representative index of vertex u: u itself for a part (sources 0..M-1),
+// inv[u] for a piece or box; -1 for a vertex that is no source.
+template <bool EXPL>
+__device__ __forceinline__ int source_of(unsigned u, unsigned M, const int32_t *inv) {
+    if constexpr (EXPL) return __ldg(inv + u);
+    else return u < M ? (int)u : -1;
+}
+
+// The sources among the pull neighbours of v (row `row`, slots [B, E)) that lie in
+// the chunk of sources [lo, lo + 128), as bits.
+template <int B, int E, bool EXPL>
 __device__ __forceinline__ void sources_span(const int32_t *row, unsigned v, unsigned lo, unsigned N, unsigned M,
-                                             unsigned nb[4]) {
+                                             const int32_t *inv, unsigned nb[4]) {
     int32_t df[E - B];
     if constexpr (B % 4 == 0 && (E - B) % 4 == 0) {
 #pragma unroll
@@ -129,21 +170,26 @@ __device__ __forceinline__ void sources_span(const int32_t *row, unsigned v, uns
     }
 #pragma unroll
     for (int i = 0; i < E - B; ++i) {
-        const unsigned y = v + (unsigned)df[i];
-        const unsigned sv = y >= N ? y - N : y;
-        const unsigned o = sv - lo;
-        if (sv < M && o < 128u) nb[o >> 5] |= 1u << (o & 31u);
+        unsigned u = (unsigned)df[i];
+        if constexpr (!EXPL) {
+            u += v;
+            u -= u >= N ? N : 0u;
+        }
+        const int sv = source_of<EXPL>(u, M, inv);
+        const unsigned o = (unsigned)sv - lo;
+        if (sv >= 0 && o < 128u) nb[o >> 5] |= 1u << (o & 31u);
     }
 }
 
 // The reset pass of a round with level 1 folded in: the pairs a chunk (v, w)
-// reaches at level 1 are the sources s among its pull neighbours (s = v + diff
-// < M, in the chunk), so the pass writes the padding bits, the diagonal and those
-// pairs into V and their frontier into F1 (`Fn`) without a gather.  Columns of
-// candidates past the last one (mine == false) start full.  Returns the
+// reaches at level 1 are the sources among its pull neighbours that lie in the
+// chunk, so the pass writes the padding bits, the diagonal and those pairs into V
+// and their frontier into F1 (`Fn`) without a gather.  Columns of candidates past
+// the last one (mine == false) start full.  `rows`: the column's candidate's diff
+// table (part, row v % M) or pull adjacency (piece / box, row v).  Returns the
 // thread's new pairs.
-template <int D>
-__device__ __forceinline__ unsigned level1_pass(const LiftArgs &a, const int32_t *tab, unsigned v0,
+template <int D, bool EXPL>
+__device__ __forceinline__ unsigned level1_pass(const LiftArgs &a, const int32_t *rows, unsigned v0,
                                                 unsigned vstep, unsigned rstep, unsigned w, unsigned cc,
                                                 bool mine, uint4 *Fn) {
     const unsigned N = (unsigned)a.N, M = (unsigned)a.M, W = (unsigned)a.W;
@@ -154,25 +200,31 @@ __device__ __forceinline__ unsigned level1_pass(const LiftArgs &a, const int32_t
     for (unsigned v = v0; v < N; v += vstep) {
         uint4 vis = pad, n1 = gg::u4zero();
         if (mine) {
-            if (v - lo < 128u) {   // the diagonal (bits past M are padding, already set)
-                const unsigned bit = 1u << (v & 31u);
-                switch ((v - lo) >> 5) {
+            const int sv = source_of<EXPL>(v, M, a.inv);
+            const unsigned o = (unsigned)sv - lo;
+            if (sv >= 0 && o < 128u) {   // the diagonal
+                const unsigned bit = 1u << (o & 31u);
+                switch (o >> 5) {
                     case 0: vis.x |= bit; break;
                     case 1: vis.y |= bit; break;
                     case 2: vis.z |= bit; break;
                     default: vis.w |= bit; break;
                 }
             }
-            const int32_t *row = tab + (size_t)r * a.d;
+            const int32_t *row = rows + (size_t)(EXPL ? v : r) * a.d;
             unsigned nb[4] = {0u, 0u, 0u, 0u};
             if constexpr (D > 0) {
-                sources_span<0, D>(row, v, lo, N, M, nb);
+                sources_span<0, D, EXPL>(row, v, lo, N, M, a.inv, nb);
             } else {
                 for (int i = 0; i < a.d; ++i) {
-                    const unsigned y = v + (unsigned)__ldg(row + i);
-                    const unsigned sv = y >= N ? y - N : y;
-                    const unsigned o = sv - lo;
-                    if (sv < M && o < 128u) nb[o >> 5] |= 1u << (o & 31u);
+                    unsigned u = (unsigned)__ldg(row + i);
+                    if constexpr (!EXPL) {
+                        u += v;
+                        u -= u >= N ? N : 0u;
+                    }
+                    const int su = source_of<EXPL>(u, M, a.inv);
+                    const unsigned ou = (unsigned)su - lo;
+                    if (su >= 0 && ou < 128u) nb[ou >> 5] |= 1u << (ou & 31u);
                 }
             }
             n1 = gg::andnot(make_uint4(nb[0], nb[1], nb[2], nb[3]), vis);
@@ -187,8 +239,9 @@ __device__ __forceinline__ unsigned level1_pass(const LiftArgs &a, const int32_t
     return cnt;
 }
 
-// D > 0: the degree at compile time; D == 0: a.d at run time.
-template <int D>
+// D > 0: the degree at compile time; D == 0: a.d at run time.  EXPL: piece / box
+// (per-candidate pull adjacency and representative map); otherwise part (diffs).
+template <int D, bool EXPL>
 __global__ void __launch_bounds__(kLiftBlock, 4) lift_kernel(const LiftArgs a) {
     __shared__ unsigned s_cnt[kMaxGroup];
     __shared__ unsigned long long s_reached[kMaxGroup];
@@ -212,7 +265,8 @@ __global__ void __launch_bounds__(kLiftBlock, 4) lift_kernel(const LiftArgs a) {
         const int k0 = rd * a.G;
         const int live = min(a.G, a.K - k0);
         const bool mine = owner && (int)g < live;   // a column of a live candidate
-        const int32_t *tab = a.tab + (size_t)(k0 + (mine ? (int)g : 0)) * a.M * a.d;
+        const int kc = k0 + (mine ? (int)g : 0);
+        const int32_t *rows = EXPL ? a.adj + (size_t)kc * a.N * a.d : a.tab + (size_t)kc * a.M * a.d;
         if (threadIdx.x == 0) s_half = 0;   // read after the next barrier
         if (rd == 0 && a.level_ns && blockIdx.x == 0 && threadIdx.x == 0) a.level_ns[0] = gg::gtimer();
         unsigned long long reached = threadIdx.x < (unsigned)live ? (unsigned long long)a.M : 0ull;
@@ -227,7 +281,7 @@ __global__ void __launch_bounds__(kLiftBlock, 4) lift_kernel(const LiftArgs a) {
             unsigned r = v0 % M;
             if (L == 1) {
                 // level 1 is the round's reset pass
-                cnt = level1_pass<D>(a, tab, v0, vstep, rstep, w, cc, mine, Fn);
+                cnt = level1_pass<D, EXPL>(a, rows, v0, vstep, rstep, w, cc, mine, Fn);
             } else {
                 const bool half = s_half != 0;
                 for (unsigned v = v0; v < N; v += vstep) {
@@ -236,21 +290,21 @@ __global__ void __launch_bounds__(kLiftBlock, 4) lift_kernel(const LiftArgs a) {
                     uint4 nw = gg::u4zero();
                     if (!gg::u4full(own)) {
                         // full from the reset pass unless the column is a live candidate's
-                        const int32_t *row = tab + (size_t)r * a.d;
+                        const int32_t *row = rows + (size_t)(EXPL ? v : r) * a.d;
                         uint4 acc = gg::u4zero();
                         if constexpr (D > 0) {
                             if (!half && D <= 12) {
-                                gather_span<0, D>(row, v, w, N, W, Fc, acc);
+                                gather_span<0, D, EXPL>(row, v, w, N, W, Fc, acc);
                             } else if (!half) {   // two spans keep the loads within the registers
-                                gather_span<0, D / 2>(row, v, w, N, W, Fc, acc);
-                                gather_span<D / 2, D>(row, v, w, N, W, Fc, acc);
+                                gather_span<0, D / 2, EXPL>(row, v, w, N, W, Fc, acc);
+                                gather_span<D / 2, D, EXPL>(row, v, w, N, W, Fc, acc);
                             } else {
-                                gather_span<0, D / 2>(row, v, w, N, W, Fc, acc);
-                                if (!gg::u4full(gg::u4or(own, acc))) gather_span<D / 2, D>(row, v, w, N, W, Fc, acc);
+                                gather_span<0, D / 2, EXPL>(row, v, w, N, W, Fc, acc);
+                                if (!gg::u4full(gg::u4or(own, acc))) gather_span<D / 2, D, EXPL>(row, v, w, N, W, Fc, acc);
                             }
                         } else {
-                            gather_any(row, 0, half ? dh : a.d, v, w, N, W, Fc, acc);
-                            if (half && !gg::u4full(gg::u4or(own, acc))) gather_any(row, dh, a.d, v, w, N, W, Fc, acc);
+                            gather_any<EXPL>(row, 0, half ? dh : a.d, v, w, N, W, Fc, acc);
+                            if (half && !gg::u4full(gg::u4or(own, acc))) gather_any<EXPL>(row, dh, a.d, v, w, N, W, Fc, acc);
                         }
                         nw = gg::andnot(acc, own);
                         if (gg::u4any(nw)) {
@@ -295,19 +349,21 @@ __global__ void __launch_bounds__(kLiftBlock, 4) lift_kernel(const LiftArgs a) {
     if (blockIdx.x == 0 && threadIdx.x == 0) a.ctl->levels_run = levels_run;
 }
 
-void *lift_kernel_for(int d) {
+template <bool EXPL>
+void *lift_kernel_for_t(int d) {
     switch (d) {
-        case 3: return (void *)lift_kernel<3>;
-        case 4: return (void *)lift_kernel<4>;
-        case 5: return (void *)lift_kernel<5>;
-        case 6: return (void *)lift_kernel<6>;
-        case 8: return (void *)lift_kernel<8>;
-        case 10: return (void *)lift_kernel<10>;
-        case 12: return (void *)lift_kernel<12>;
-        case 16: return (void *)lift_kernel<16>;
-        default: return (void *)lift_kernel<0>;
+        case 3: return (void *)lift_kernel<3, EXPL>;
+        case 4: return (void *)lift_kernel<4, EXPL>;
+        case 5: return (void *)lift_kernel<5, EXPL>;
+        case 6: return (void *)lift_kernel<6, EXPL>;
+        case 8: return (void *)lift_kernel<8, EXPL>;
+        case 10: return (void *)lift_kernel<10, EXPL>;
+        case 12: return (void *)lift_kernel<12, EXPL>;
+        case 16: return (void *)lift_kernel<16, EXPL>;
+        default: return (void *)lift_kernel<0, EXPL>;
     }
 }
+void *lift_kernel_for(int d, bool expl) { return expl ? lift_kernel_for_t<true>(d) : lift_kernel_for_t<false>(d); }
 
 gg_status lfail(gg_status s, const std::string &m) {
     (void)cudaGetLastError();
@@ -327,6 +383,10 @@ gg_status lfail(gg_status s, const std::string &m) {
 
 struct gg_lift {
     int N = 0, M = 0, d = 0, device = 0;
+    int axes = 1;                                    // 1 part, 2 piece, 3 box
+    int n[3] = {1, 1, 1}, m[3] = {1, 1, 1};          // lifted and orbit size of each axis
+    int32_t *d_inv = nullptr;                        // piece / box: [N] representative index or -1
+    int32_t *d_adj = nullptr;                        // piece / box: [cap][N][d] candidate adjacency
     int cpc = 0, g_auto = 1, g_max = 0, group = 0;   // group 0: automatic
     int sms = 0;
     cudaStream_t stream = nullptr;
@@ -354,6 +414,7 @@ void lift_free(gg_lift *h) {
     cudaSetDevice(h->device);
     if (h->stream) cudaStreamSynchronize(h->stream);
     cudaFree(h->d_base); cudaFree(h->d_tab); cudaFree(h->d_ed); cudaFreeHost(h->h_ed);
+    cudaFree(h->d_inv); cudaFree(h->d_adj);
     cudaFree(h->V); cudaFree(h->F0); cudaFree(h->F1);
     cudaFree(h->d_counts); cudaFreeHost(h->h_counts);
     cudaFree(h->d_level_ns); cudaFreeHost(h->h_level_ns);
@@ -367,9 +428,10 @@ void lift_free(gg_lift *h) {
 gg_status ensure_cand(gg_lift *h, int n) {
     if (n <= h->cap) return GG_OK;
     int cap = std::max(n, 2 * h->cap);
-    cudaFree(h->d_tab); cudaFree(h->d_ed); cudaFreeHost(h->h_ed);
-    h->d_tab = nullptr; h->d_ed = nullptr; h->h_ed = nullptr; h->cap = 0;
-    GL_CK(cudaMalloc(&h->d_tab, (size_t)cap * h->M * h->d * sizeof(int32_t)));
+    cudaFree(h->d_tab); cudaFree(h->d_ed); cudaFreeHost(h->h_ed); cudaFree(h->d_adj);
+    h->d_tab = nullptr; h->d_ed = nullptr; h->h_ed = nullptr; h->d_adj = nullptr; h->cap = 0;
+    GL_CK(cudaMalloc(&h->d_tab, (size_t)cap * h->M * h->d * h->axes * sizeof(int32_t)));
+    if (h->axes > 1) GL_CK(cudaMalloc(&h->d_adj, (size_t)cap * h->N * h->d * sizeof(int32_t)));
     GL_CK(cudaMalloc(&h->d_ed, (size_t)cap * sizeof(gg_lift_edit)));
     GL_CK(cudaMallocHost(&h->h_ed, (size_t)cap * sizeof(gg_lift_edit)));
     h->cap = cap;
@@ -403,41 +465,68 @@ gg_status alloc_group(gg_lift *h, int groups) {
 
 extern "C" {
 
-gg_status gg_lift_create(int N, int M, int degree, int device, gg_lift **out) {
-    if (!out || N < 2 || M < 1 || M > N || N % M != 0 || degree < 1 || degree > 4096)
-        return lfail(GG_BAD_ARG, "need N >= 2, 1 <= M <= N with M dividing N, degree >= 1");
+}  // extern "C"
+
+namespace {
+
+// A handle for a lift of `axes` axes: lifted sizes n, orbit sizes m.
+gg_status lift_open(int axes, const int n_in[3], const int m_in[3], int degree, int device, gg_lift **out) {
+    if (!out) return lfail(GG_BAD_ARG, "null argument");
     *out = nullptr;
+    long long N = 1, M = 1;
+    for (int j = 0; j < axes; ++j) {
+        if (m_in[j] < 1 || n_in[j] < 1 || m_in[j] > n_in[j] || n_in[j] % m_in[j] != 0)
+            return lfail(GG_BAD_ARG, "every lifted size must be a positive multiple of its orbit size");
+        N *= n_in[j];
+        M *= m_in[j];
+    }
+    if (N < 2 || N >= (1ll << 30) || degree < 1 || degree > 4096)
+        return lfail(GG_BAD_ARG, "need 2 <= N < 2^30 vertices and 1 <= degree <= 4096");
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || device < 0 || device >= ndev)
         return lfail(GG_NO_DEVICE, "no such CUDA device");
     gg_lift *h = new gg_lift();
-    h->N = N; h->M = M; h->d = degree; h->device = device;
-    h->cpc = (M + 127) / 128;
+    h->axes = axes;
+    for (int j = 0; j < axes; ++j) { h->n[j] = n_in[j]; h->m[j] = m_in[j]; }
+    h->N = (int)N; h->M = (int)M; h->d = degree; h->device = device;
+    h->cpc = (h->M + 127) / 128;
     auto fail = [&](gg_status s) { lift_free(h); return s; };
     if (cudaSetDevice(device) != cudaSuccess) return fail(lfail(GG_NO_DEVICE, "cudaSetDevice failed"));
     int l2 = 0, coop = 0, per_sm = 0;
     if (cudaDeviceGetAttribute(&l2, cudaDevAttrL2CacheSize, device) != cudaSuccess ||
         cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, device) != cudaSuccess ||
         cudaDeviceGetAttribute(&h->sms, cudaDevAttrMultiProcessorCount, device) != cudaSuccess ||
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, lift_kernel_for(degree), kLiftBlock, 0) !=
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, lift_kernel_for(degree, axes > 1), kLiftBlock, 0) !=
             cudaSuccess)
         return fail(lfail(GG_CUDA_ERROR, "device query failed"));
     if (!coop || per_sm < 1) return fail(lfail(GG_CUDA_ERROR, "cooperative launch unavailable"));
     h->grid = per_sm * h->sms;
     // one candidate's round share: three bitsets of N * cpc uint4
     // (half the L2: lines gathered from both dies' SMs are held in both halves;
-    // at m=1024, g=32, d=12 a sweep of 2-7 candidates per round put the optimum at 5)
-    const double per_cand = 3.0 * N * h->cpc * 16.0;
+    // at m=1024, g=32, d=12 a sweep of 2-8 candidates per round put the optimum at 5)
+    const double per_cand = 3.0 * h->N * h->cpc * 16.0;
     const int fit = (int)std::max(1.0, 0.5 * l2 / per_cand);
     // items N * W must stay below 2^31
-    const long long by_items = std::max(1ll, (1ll << 31) / ((long long)N * h->cpc));
+    const long long by_items = std::max(1ll, (1ll << 31) / ((long long)h->N * h->cpc));
     h->g_auto = (int)std::min<long long>({(long long)fit, (long long)kMaxGroup, by_items});
     cudaError_t e = cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking);
     if (e == cudaSuccess) e = cudaEventCreate(&h->ev0);
     if (e == cudaSuccess) e = cudaEventCreate(&h->ev1);
-    if (e == cudaSuccess) e = cudaMalloc(&h->d_base, (size_t)M * degree * sizeof(int32_t));
+    if (e == cudaSuccess) e = cudaMalloc(&h->d_base, (size_t)h->M * degree * axes * sizeof(int32_t));
     if (e == cudaSuccess) e = cudaMalloc(&h->d_ctl, sizeof(gg::Ctl));
     if (e == cudaSuccess) e = cudaMallocHost(&h->h_ctl, sizeof(gg::Ctl));
+    if (e == cudaSuccess && axes > 1) {
+        // representatives: the corner tile, numbered like the table's rows
+        // (cpuASPLpiece.cpp:199-200, cpuASPLbox.cpp:133-134)
+        std::vector<int32_t> inv((size_t)h->N, -1);
+        const int nz = h->n[2], ny = h->n[1];
+        for (int x = 0; x < h->m[0]; ++x)
+            for (int y = 0; y < h->m[1]; ++y)
+                for (int z = 0; z < h->m[2]; ++z)
+                    inv[((size_t)x * ny + y) * nz + z] = (x * h->m[1] + y) * h->m[2] + z;
+        e = cudaMalloc(&h->d_inv, inv.size() * sizeof(int32_t));
+        if (e == cudaSuccess) e = cudaMemcpy(h->d_inv, inv.data(), inv.size() * sizeof(int32_t), cudaMemcpyHostToDevice);
+    }
     if (e != cudaSuccess)
         return fail(lfail(e == cudaErrorMemoryAllocation ? GG_OUT_OF_MEMORY : GG_CUDA_ERROR,
                           cudaGetErrorString(e)));
@@ -448,11 +537,33 @@ gg_status gg_lift_create(int N, int M, int degree, int device, gg_lift **out) {
     return GG_OK;
 }
 
-gg_status gg_lift_set_base(gg_lift *h, const int32_t *diffs) {
-    if (!h || !diffs) return lfail(GG_BAD_ARG, "null argument");
-    std::vector<int32_t> nd((size_t)h->M * h->d);
-    const long long N = h->N;
-    for (size_t k = 0; k < nd.size(); ++k) nd[k] = (int32_t)((((long long)diffs[k] % N) + N) % N);
+}  // namespace
+
+extern "C" {
+
+gg_status gg_lift_create(int N, int M, int degree, int device, gg_lift **out) {
+    const int n[3] = {N, 1, 1}, m[3] = {M, 1, 1};
+    return lift_open(1, n, m, degree, device, out);
+}
+
+gg_status gg_lift_create_piece(int Nx, int Ny, int Mx, int My, int degree, int device, gg_lift **out) {
+    const int n[3] = {Nx, Ny, 1}, m[3] = {Mx, My, 1};
+    return lift_open(2, n, m, degree, device, out);
+}
+
+gg_status gg_lift_create_box(int Nx, int Ny, int Nz, int Mx, int My, int Mz, int degree, int device,
+                             gg_lift **out) {
+    const int n[3] = {Nx, Ny, Nz}, m[3] = {Mx, My, Mz};
+    return lift_open(3, n, m, degree, device, out);
+}
+
+gg_status gg_lift_set_base(gg_lift *h, const int32_t *table) {
+    if (!h || !table) return lfail(GG_BAD_ARG, "null argument");
+    std::vector<int32_t> nd((size_t)h->M * h->d * h->axes);
+    for (size_t k = 0; k < nd.size(); ++k) {
+        const long long n = h->n[k % h->axes];
+        nd[k] = (int32_t)((((long long)table[k] % n) + n) % n);
+    }
     GL_CK(cudaSetDevice(h->device));
     GL_CK(cudaMemcpyAsync(h->d_base, nd.data(), nd.size() * sizeof(int32_t), cudaMemcpyHostToDevice, h->stream));
     GL_CK(cudaStreamSynchronize(h->stream));
@@ -491,7 +602,6 @@ gg_status gg_lift_eval(gg_lift *h, int n_cand, const gg_lift_edit *edits, int ma
     GL_CK(cudaSetDevice(h->device));
     gg_status s = ensure_cand(h, n_cand);
     if (s != GG_OK) return s;
-    const long long N = h->N;
     for (int k = 0; k < n_cand; ++k) {
         const gg_lift_edit &q = edits[k];
         if (q.count < 0 || q.count > 4) return lfail(GG_BAD_ARG, "edit count must be in [0, 4]");
@@ -503,7 +613,10 @@ gg_status gg_lift_eval(gg_lift *h, int n_cand, const gg_lift_edit *edits, int ma
                 return lfail(GG_BAD_ARG, "edit slot outside the table");
             o.row[j] = q.row[j];
             o.slot[j] = q.slot[j];
-            o.diff[j] = (int32_t)((((long long)q.diff[j] % N) + N) % N);
+            for (int c = 0; c < h->axes; ++c) {
+                const long long n = h->n[c];
+                o.diff[j][c] = (int32_t)((((long long)q.diff[j][c] % n) + n) % n);
+            }
         }
     }
     const int ml = max_levels > 0 ? std::min(max_levels, h->N) : h->N;
@@ -524,10 +637,18 @@ gg_status gg_lift_eval(gg_lift *h, int n_cand, const gg_lift_edit *edits, int ma
     GL_CK(cudaEventRecord(h->ev0, st));
     const long long tab_n = (long long)n_cand * h->M * h->d;
     lift_tables<<<(int)std::min<long long>((tab_n + 255) / 256, (long long)h->sms * 16), 256, 0, st>>>(
-        h->d_base, h->d_ed, n_cand, h->M, h->d, h->d_tab);
+        h->d_base, h->d_ed, n_cand, h->M, h->d, h->axes, h->d_tab);
     GL_CK(cudaGetLastError());
+    if (h->axes > 1) {
+        const long long adj_n = (long long)n_cand * h->N * h->d;
+        lift_expand<<<(int)std::min<long long>((adj_n + 255) / 256, (long long)h->sms * 16), 256, 0, st>>>(
+            h->d_tab, n_cand, h->M, h->d, h->axes, h->n[0], h->n[1], h->n[2], h->m[0], h->m[1], h->m[2], h->d_adj);
+        GL_CK(cudaGetLastError());
+    }
     LiftArgs a{};
     a.tab = h->d_tab;
+    a.adj = h->d_adj;
+    a.inv = h->d_inv;
     a.N = h->N; a.M = h->M; a.d = h->d; a.K = n_cand; a.G = G; a.cpc = h->cpc; a.W = G * h->cpc;
     a.V = h->V; a.F0 = h->F0; a.F1 = h->F1;
     a.counts = h->d_counts;
@@ -543,7 +664,8 @@ gg_status gg_lift_eval(gg_lift *h, int n_cand, const gg_lift_edit *edits, int ma
     a.expected = (unsigned)h->grid;
     GL_CK(cudaMemsetAsync(h->d_level_ns, 0, (size_t)(ml + 1) * sizeof(unsigned long long), st));
     void *args[] = {&a};
-    GL_CK(cudaLaunchCooperativeKernel(lift_kernel_for(h->d), dim3(h->grid), dim3(kLiftBlock), args, 0, st));
+    GL_CK(cudaLaunchCooperativeKernel(lift_kernel_for(h->d, h->axes > 1), dim3(h->grid), dim3(kLiftBlock), args, 0,
+                                      st));
     GL_CK(cudaEventRecord(h->ev1, st));
     GL_CK(cudaMemcpyAsync(h->h_ctl, h->d_ctl, sizeof(gg::Ctl), cudaMemcpyDeviceToHost, st));
     GL_CK(cudaStreamSynchronize(st));

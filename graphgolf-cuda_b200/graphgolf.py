@@ -125,6 +125,10 @@ _SIGS = {
     "gg_inc_destroy": [_P],
     "gg_gen_cyclic_lift": [_I, _I, _I, ctypes.c_uint64, _P],
     "gg_lift_create": [_I, _I, _I, _I, _EPP],
+    "gg_lift_create_piece": [_I, _I, _I, _I, _I, _I, _EPP],
+    "gg_lift_create_box": [_I, _I, _I, _I, _I, _I, _I, _I, _EPP],
+    "gg_gen_piece_moves": [_I, _I, _I, _I, _I, _P, _I, ctypes.c_uint64, _P],
+    "gg_gen_box_moves": [_I, _I, _I, _I, _I, _I, _I, _P, _I, ctypes.c_uint64, _P],
     "gg_lift_set_base": [_P, _P],
     "gg_lift_eval": [_P, _I, _P, _I, _P],
     "gg_lift_set_group": [_P, _I],
@@ -838,7 +842,7 @@ class Batch:
 
 
 LIFT_EDIT_DTYPE = np.dtype([("count", np.int32), ("row", np.int32, 4), ("slot", np.int32, 4),
-                            ("diff", np.int32, 4)])
+                            ("diff", np.int32, (4, 3))])
 
 
 def gen_lift_moves(N, M, diffs, count, seed):
@@ -850,11 +854,32 @@ def gen_lift_moves(N, M, diffs, count, seed):
     return out
 
 
-def apply_lift_edit(diffs, e):
-    """Host copy of a lift edit: the diff table with the edit's slots replaced."""
-    t = np.array(diffs, dtype=np.int32, copy=True)
+def gen_piece_moves(Nx, Ny, Mx, My, vals, count, seed):
+    """The same moves for a 2-D torus lift (vals [Mx*My, d, 2])."""
+    vals = _i32(vals).reshape(Mx * My, -1, 2)
+    out = np.zeros(count, dtype=LIFT_EDIT_DTYPE)
+    _check(lib().gg_gen_piece_moves(Nx, Ny, Mx, My, vals.shape[1], _ptr(vals), count, seed, _ptr(out)))
+    return out
+
+
+def gen_box_moves(Nx, Ny, Nz, Mx, My, Mz, vals, count, seed):
+    """The same moves for a 3-D torus lift (vals [Mx*My*Mz, d, 3])."""
+    vals = _i32(vals).reshape(Mx * My * Mz, -1, 3)
+    out = np.zeros(count, dtype=LIFT_EDIT_DTYPE)
+    _check(lib().gg_gen_box_moves(Nx, Ny, Nz, Mx, My, Mz, vals.shape[1], _ptr(vals), count, seed, _ptr(out)))
+    return out
+
+
+def apply_lift_edit(table, e):
+    """Host copy of a lift edit: the table (part [M, d], piece [M, d, 2], box
+    [M, d, 3]) with the edit's slots replaced."""
+    t = np.array(table, dtype=np.int32, copy=True)
     for j in range(int(e["count"])):
-        t[int(e["row"][j]), int(e["slot"][j])] = int(e["diff"][j])
+        r, k = int(e["row"][j]), int(e["slot"][j])
+        if t.ndim == 2:
+            t[r, k] = int(e["diff"][j][0])
+        else:
+            t[r, k, :] = e["diff"][j][:t.shape[2]]
     return t
 
 
@@ -862,12 +887,25 @@ class Lift:
     """Scores many edits of one cyclic-lift diff table in one launch (gg_lift_*).
     Results are over the M orbit sources: ASPL = total * (N // M) / (N * (N - 1))."""
 
-    def __init__(self, N, M, degree, device=0):
-        self.N, self.M, self.degree = N, M, degree
-        self._h = _create("gg_lift_create", N, M, degree, device)
+    def __init__(self, N, M, degree, device=0, _handle=None, _axes=1):
+        self.N, self.M, self.degree, self.axes = N, M, degree, _axes
+        self._h = _handle if _handle is not None else _create("gg_lift_create", N, M, degree, device)
 
-    def set_base(self, diffs):
-        self.base = _i32(diffs).reshape(self.M, self.degree)
+    @classmethod
+    def piece(cls, Nx, Ny, Mx, My, degree, device=0):
+        """Candidates of a 2-D torus lift (the cudaASPLpiece form)."""
+        h = _create("gg_lift_create_piece", Nx, Ny, Mx, My, degree, device)
+        return cls(Nx * Ny, Mx * My, degree, device, _handle=h, _axes=2)
+
+    @classmethod
+    def box(cls, Nx, Ny, Nz, Mx, My, Mz, degree, device=0):
+        """Candidates of a 3-D torus lift (the cudaASPLbox form)."""
+        h = _create("gg_lift_create_box", Nx, Ny, Nz, Mx, My, Mz, degree, device)
+        return cls(Nx * Ny * Nz, Mx * My * Mz, degree, device, _handle=h, _axes=3)
+
+    def set_base(self, table):
+        shape = (self.M, self.degree) if self.axes == 1 else (self.M, self.degree, self.axes)
+        self.base = _i32(table).reshape(shape)
         _check(lib().gg_lift_set_base(self._h, _ptr(self.base)))
 
     def eval(self, edits, max_levels=0):

@@ -247,34 +247,47 @@ gg_status gg_inc_eval(gg_inc *h, const gg_swap *s, gg_cand_result *out, int *aff
 gg_status gg_inc_commit(gg_inc *h, const gg_swap *s, gg_result *r);
 gg_status gg_inc_destroy(gg_inc *h);
 
-/* ---- batched evaluation of cyclic-lift candidates (no reference counterpart) ----
- * The reference's annealers on the lifted ("part") form propose one edit of the
- * diff table at a time and score it with one cudaASPLconv::diameterASPL call
- * (cppcode/annealing.cpp:112-197 proposes, :403 scores).  Here one cooperative
- * launch scores a whole population of edits of one base table: every candidate
- * is the base diff table (M * degree int32, the table of gg_conv_*) with up to 4
- * slots replaced, and gets the exact counts of its own N-vertex lift with BFS
- * from the M orbit vertices 0..M-1.  N must be a multiple of M. */
+/* ---- batched evaluation of lifted candidates (no reference counterpart) -----
+ * The reference's annealers on the lifted forms propose one edit of the diff
+ * table at a time and score it with one calculator call: cyclic lifts ("part",
+ * cppcode/annealing.cpp:112-197 proposes, :403 scores with
+ * cudaASPLconv::diameterASPL), 2-D torus lifts ("piece",
+ * cppcode/pieceannealing.cpp:113-204 with cudaASPLpiece) and 3-D torus lifts
+ * ("box", cppcode/boxHillClimb.cpp:113-220 with cudaASPLbox).  Here one
+ * cooperative launch scores a whole population of edits of one base table: every
+ * candidate is the base diff table (the table of gg_conv_* / gg_piece_* /
+ * gg_box_*) with up to 4 slots replaced, and gets the exact counts of its own
+ * lift with BFS from the orbit representatives (vertices 0..M-1 of a part, the
+ * corner tile of a piece or box).  Each lifted size must be a multiple of the
+ * matching orbit size. */
 typedef struct gg_lift gg_lift;
 
-/* Slots (row[j], slot[j]) of the base table take the value diff[j], j < count
- * (0 <= count <= 4; count 0 is the base itself).  Diffs are taken modulo N. */
+/* Slots (row[j], slot[j]) of the base table take the diff diff[j], j < count
+ * (0 <= count <= 4; count 0 is the base itself).  diff[j] = {d, 0, 0} for a part,
+ * {dx, dy, 0} for a piece, {dx, dy, dz} for a box; each component is taken modulo
+ * the lifted size of its axis.  Rows are numbered like the calculators' tables:
+ * x * My + y for a piece, (x * My + y) * Mz + z for a box. */
 typedef struct gg_lift_edit {
     int32_t count;
     int32_t row[4];
     int32_t slot[4];
-    int32_t diff[4];
+    int32_t diff[4][3];
 } gg_lift_edit;
 
 gg_status gg_lift_create(int N, int M, int degree, int device, gg_lift **out);
-/* The base diff table, M * degree int32 (padding slots: diff 0). */
-gg_status gg_lift_set_base(gg_lift *h, const int32_t *diffs);
-/* Exact counts of each candidate over the M orbit sources: out[i].total = sum of
- * distances from the sources (unscaled: the reference's ASPL is
- * total * (N/M) / (N*(N-1)), cudaASPLconv.cu:241-242), .reached = (source, vertex)
- * pairs reached (M*N when connected), .levels = last level that found a pair.
- * max_levels caps the BFS (0 = no cap); a candidate still finding pairs at the cap
- * reports connected = 0. */
+gg_status gg_lift_create_piece(int Nx, int Ny, int Mx, int My, int degree, int device, gg_lift **out);
+gg_status gg_lift_create_box(int Nx, int Ny, int Nz, int Mx, int My, int Mz, int degree, int device,
+                             gg_lift **out);
+/* The base table: M * degree int32 diffs (part), Mx*My * degree * 2 (piece),
+ * Mx*My*Mz * degree * 3 (box); padding slots: diff 0. */
+gg_status gg_lift_set_base(gg_lift *h, const int32_t *table);
+/* Exact counts of each candidate over the M orbit representatives: out[i].total =
+ * sum of distances from the representatives (unscaled: the reference's ASPL is
+ * total * (N/M) / (N*(N-1)), cudaASPLconv.cu:241-242, with N and M the vertex and
+ * representative counts), .reached = (representative, vertex) pairs reached (M*N
+ * when connected), .levels = last level that found a pair.  max_levels caps the
+ * BFS (0 = no cap); a candidate still finding pairs at the cap reports
+ * connected = 0. */
 gg_status gg_lift_eval(gg_lift *h, int n_cand, const gg_lift_edit *edits, int max_levels,
                        gg_cand_result *out);
 /* Candidates that run side by side in one round (1..32; 0 = automatic: as many as
@@ -292,15 +305,21 @@ gg_status gg_lift_last_level_ns(gg_lift *h, uint64_t *ns, int n);
 gg_status gg_lift_last_ms(gg_lift *h, double *ms);
 gg_status gg_lift_destroy(gg_lift *h);
 
-/* Random moves of a cyclic lift, the two the reference's part annealer draws
- * (cppcode/annealing.cpp:112-197): with probability 1/2 when N/M > 1, a new lift
- * shift for one orbit edge (2 slots); otherwise an orbit 2-opt, edges a-b and c-d
- * rewired to a-d and b-c, each with a uniform new lift shift (4 slots).  Padding
- * slots (diff 0 mod N) are never moved, and moves that would give the lift a loop
- * or a repeated edge are redrawn (the reference keeps them).  diffs: M * degree,
- * symmetric (every slot has its reverse slot in the target orbit's row). */
+/* Random moves of a lift, the two the reference's lifted annealers draw
+ * (cppcode/annealing.cpp:112-197, pieceannealing.cpp:113-204,
+ * boxHillClimb.cpp:113-220): with probability 1/2 when the lift has more than one
+ * copy of the orbit tile, a new lift shift for one orbit edge (2 slots); otherwise
+ * an orbit 2-opt, edges a-b and c-d rewired to a-d and b-c, each with a uniform new
+ * lift shift (4 slots).  Padding slots (diff 0) are never moved, and moves that
+ * would give the lift a loop or a repeated edge are redrawn (the reference keeps
+ * them).  The table must be symmetric (every slot has its reverse slot in the
+ * target orbit's row). */
 gg_status gg_gen_lift_moves(int N, int M, int degree, const int32_t *diffs, int count, uint64_t seed,
                             gg_lift_edit *out);
+gg_status gg_gen_piece_moves(int Nx, int Ny, int Mx, int My, int degree, const int32_t *vals, int count,
+                             uint64_t seed, gg_lift_edit *out);
+gg_status gg_gen_box_moves(int Nx, int Ny, int Nz, int Mx, int My, int Mz, int degree, const int32_t *vals,
+                           int count, uint64_t seed, gg_lift_edit *out);
 
 /* Uniform random 2-opt proposals on a base graph (adj n*degree, simple):
  * edges (a,b), (c,d) drawn uniformly, mode uniform; proposals that would create a

@@ -148,3 +148,96 @@ def test_lift_annealing_improves_and_reports_exact_aspl():
     diam, aspl = O.conv_diameter_aspl(N, M, best)
     assert aspl == tr.final_best and aspl < start
     assert all(b >= c for b, c in zip(tr.best, tr.best[1:]))
+
+
+# ---- 2-D and 3-D torus lifts (piece, box) ------------------------------------
+
+import instances as I
+
+
+def graph_ok(adj, pad):
+    """Pull adjacency `adj` with padding mask `pad`: simple and symmetric."""
+    n = len(adj)
+    rows = [[int(u) for u, p in zip(adj[v], pad[v]) if not p] for v in range(n)]
+    for v in range(n):
+        if v in rows[v] or len(set(rows[v])) != len(rows[v]):
+            return False
+        if any(v not in rows[u] for u in rows[v]):
+            return False
+    return True
+
+
+def simple_piece(Mx, My, kx, ky, d, seed):
+    for s in range(seed, seed + 200):
+        Nx, Ny, _, _, T = I.random_piece(Mx, My, kx, ky, d, s)
+        if graph_ok(O.expand_piece(Nx, Ny, Mx, My, T), np.zeros((Nx * Ny, d), bool)):
+            return Nx, Ny, T
+    raise AssertionError("no simple piece")
+
+
+def simple_box(Mx, My, Mz, kx, ky, kz, d, seed):
+    for s in range(seed, seed + 200):
+        Nx, Ny, Nz, _, _, _, T = I.random_box(Mx, My, Mz, kx, ky, kz, d, s)
+        if graph_ok(O.expand_box(Nx, Ny, Nz, Mx, My, Mz, T), np.zeros((Nx * Ny * Nz, d), bool)):
+            return Nx, Ny, Nz, T
+    raise AssertionError("no simple box")
+
+
+def test_piece_and_box_moves_keep_the_lift_simple():
+    Nx, Ny, T = simple_piece(6, 4, 3, 2, 4, 1)
+    moves = G.gen_piece_moves(Nx, Ny, 6, 4, T, 40, 5)
+    assert (moves["count"] == 2).any() and (moves["count"] == 4).any()
+    for e in moves:
+        t = G.apply_lift_edit(T, e)
+        assert graph_ok(O.expand_piece(Nx, Ny, 6, 4, t), np.zeros((Nx * Ny, 4), bool))
+        assert (e["diff"][:, 2] == 0).all()
+    Nx, Ny, Nz, B = simple_box(3, 2, 2, 2, 2, 3, 4, 1)
+    moves = G.gen_box_moves(Nx, Ny, Nz, 3, 2, 2, B, 40, 6)
+    for e in moves:
+        t = G.apply_lift_edit(B, e)
+        assert graph_ok(O.expand_box(Nx, Ny, Nz, 3, 2, 2, t), np.zeros((Nx * Ny * Nz, 4), bool))
+    a = G.gen_box_moves(Nx, Ny, Nz, 3, 2, 2, B, 10, 7)
+    assert a.tobytes() == G.gen_box_moves(Nx, Ny, Nz, 3, 2, 2, B, 10, 7).tobytes()
+
+
+@pytest.mark.gpu
+def test_piece_candidates_equal_the_oracle():
+    Mx, My = 16, 10
+    Nx, Ny, T = simple_piece(Mx, My, 4, 3, 4, 2)
+    L = G.Lift.piece(Nx, Ny, Mx, My, 4, 0)
+    L.set_base(T)
+    moves = np.concatenate([np.zeros(1, dtype=G.LIFT_EDIT_DTYPE), G.gen_piece_moves(Nx, Ny, Mx, My, T, 30, 3)])
+    res = L.eval(moves)
+    reps = O.piece_reps(Nx, Ny, Mx, My)
+    for e, got in zip(moves, res):
+        r = O.bfs_pull(O.expand_piece(Nx, Ny, Mx, My, G.apply_lift_edit(T, e)), reps)
+        assert (int(got["total"]), int(got["reached"]), int(got["connected"])) == \
+            (r.total(), int(r.reached.sum()), int(r.connected))
+        if r.connected:
+            assert int(got["levels"]) == r.levels
+    L.set_group(1)
+    assert L.eval(moves).tobytes() == res.tobytes()
+    diam, aspl = G.cudaASPLpiece(Nx, Ny, Mx, My, 4, 0).diameterASPL(T)
+    assert L.aspl(res[:1])[0] == aspl and int(res[0]["levels"]) == diam
+    L.close()
+
+
+@pytest.mark.gpu
+def test_box_candidates_equal_the_oracle():
+    Mx, My, Mz = 6, 5, 4
+    Nx, Ny, Nz, B = simple_box(Mx, My, Mz, 2, 3, 2, 6, 3)
+    L = G.Lift.box(Nx, Ny, Nz, Mx, My, Mz, 6, 0)
+    L.set_base(B)
+    moves = np.concatenate([np.zeros(1, dtype=G.LIFT_EDIT_DTYPE),
+                            G.gen_box_moves(Nx, Ny, Nz, Mx, My, Mz, B, 30, 4)])
+    res = L.eval(moves)
+    reps = O.box_reps(Nx, Ny, Nz, Mx, My, Mz)
+    for e, got in zip(moves, res):
+        r = O.bfs_pull(O.expand_box(Nx, Ny, Nz, Mx, My, Mz, G.apply_lift_edit(B, e)), reps)
+        assert (int(got["total"]), int(got["reached"]), int(got["connected"])) == \
+            (r.total(), int(r.reached.sum()), int(r.connected))
+        if r.connected:
+            assert int(got["levels"]) == r.levels
+    diam, aspl = G.cudaASPLbox(Nx, Ny, Nz, Mx, My, Mz, 6, 0).diameterASPL(B)
+    assert L.aspl(res[:1])[0] == aspl and int(res[0]["levels"]) == diam
+    L.close()

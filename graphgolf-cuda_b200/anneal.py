@@ -181,6 +181,59 @@ def anneal(adj0, steps, *, seed=1, exact=32, pool=4096, explore=8, surrogate=Fal
     return best_adj, tr
 
 
+def _anneal_table(L, gen, table0, steps, *, seed, exact, t0_frac, t_end, target, time_limit):
+    """Batched annealing of one lift table with handle L (a G.Lift) and move
+    generator gen(table, count, seed).  t0_frac == 0: hill climbing (only moves
+    that lower the diameter, or keep it and lower the total)."""
+    table = np.array(table0, dtype=np.int32, copy=True)
+    scale, npairs = L.N // L.M, L.N * (L.N - 1)
+    L.set_base(table)
+    r0 = L.eval(np.zeros(1, dtype=G.LIFT_EDIT_DTYPE))[0]
+    if not r0["connected"]:
+        raise ValueError("start lift is disconnected")
+    cur_total, cur_diam = int(r0["total"]), int(r0["levels"])
+    best_aspl, best = cur_total * scale / npairs, table.copy()
+    T0 = t0_frac * best_aspl
+    rng = np.random.default_rng(seed)
+    tr = Trace()
+    t_start = time.perf_counter()
+    tr.times.append(0.0)
+    tr.best.append(best_aspl)
+    for i in range(steps):
+        T = T0 * (t_end / T0) ** (i / max(steps - 1, 1)) if T0 > 0 else 0.0
+        moves = gen(table, exact, (seed << 32) ^ i)
+        res = L.eval(moves)
+        tr.exact_evals += len(moves)
+        ok = res["connected"] == 1
+        if ok.any():
+            totals = res["total"].astype(np.int64)
+            key = np.where(ok, res["levels"].astype(np.int64) * (1 << 40) + totals, np.iinfo(np.int64).max)
+            k = int(np.argmin(key))
+            dy, ty = int(res["levels"][k]), int(totals[k])
+            dA = (ty - cur_total) * scale / npairs
+            accept = dy < cur_diam or (dy == cur_diam and (dA < 0 or (T > 0 and rng.random() < math.exp(-dA / T))))
+            if accept:
+                table = G.apply_lift_edit(table, moves[k])
+                L.set_base(table)
+                cur_total, cur_diam = ty, dy
+                tr.accepted += 1
+                aspl = cur_total * scale / npairs
+                if aspl < best_aspl:
+                    best_aspl, best = aspl, table.copy()
+                    tr.times.append(time.perf_counter() - t_start)
+                    tr.best.append(best_aspl)
+                    if target is not None and tr.hit_time is None and best_aspl <= target:
+                        tr.hit_time, tr.hit_step = tr.times[-1], i + 1
+        tr.steps = i + 1
+        if target is not None and tr.hit_time is not None:
+            break
+        if time_limit is not None and time.perf_counter() - t_start > time_limit:
+            break
+    tr.wall = time.perf_counter() - t_start
+    tr.final_best = best_aspl
+    return best, tr
+
+
 def anneal_lift(N, M, diffs0, steps, *, seed=1, exact=32, t0_frac=1e-3, t_end=1e-6, target=None,
                 time_limit=None, device=0):
     """Anneal a cyclic lift in part form (the reference's main annealer,
@@ -188,58 +241,43 @@ def anneal_lift(N, M, diffs0, steps, *, seed=1, exact=32, t0_frac=1e-3, t_end=1e
     `exact` moves (gg_gen_lift_moves: new lift shifts and orbit 2-opts) and scores
     them all in one launch (gg_lift_eval); the best (smallest diameter, then
     smallest total) goes through the same acceptance rule as anneal().  ASPL is the
-    reference's total * (N/M) / (N(N-1)).  Returns (best_diffs, Trace)."""
-    diffs = np.array(diffs0, dtype=np.int32, copy=True).reshape(M, -1)
-    scale, npairs = N // M, N * (N - 1)
+    reference's total * (N/M) / (N(N-1)).  t0_frac = 0 climbs (HillClimb.cpp).
+    Returns (best_diffs, Trace)."""
+    diffs = np.asarray(diffs0, dtype=np.int32).reshape(M, -1)
     L = G.Lift(N, M, diffs.shape[1], device)
     try:
-        L.set_base(diffs)
-        r0 = L.eval(np.zeros(1, dtype=G.LIFT_EDIT_DTYPE))[0]
-        if not r0["connected"]:
-            raise ValueError("start lift is disconnected")
-        cur_total, cur_diam = int(r0["total"]), int(r0["levels"])
-        best_aspl, best = cur_total * scale / npairs, diffs.copy()
-        T0 = t0_frac * best_aspl
-        rng = np.random.default_rng(seed)
-        tr = Trace()
-        t_start = time.perf_counter()
-        tr.times.append(0.0)
-        tr.best.append(best_aspl)
-        for i in range(steps):
-            T = T0 * (t_end / T0) ** (i / max(steps - 1, 1))
-            moves = G.gen_lift_moves(N, M, diffs, exact, (seed << 32) ^ i)
-            res = L.eval(moves)
-            tr.exact_evals += len(moves)
-            ok = res["connected"] == 1
-            if ok.any():
-                totals = res["total"].astype(np.int64)
-                key = np.where(ok, res["levels"].astype(np.int64) * (1 << 40) + totals, np.iinfo(np.int64).max)
-                k = int(np.argmin(key))
-                dy, ty = int(res["levels"][k]), int(totals[k])
-                dA = (ty - cur_total) * scale / npairs
-                accept = dy < cur_diam or (dy == cur_diam and (dA < 0 or rng.random() < math.exp(-dA / T)))
-                if accept:
-                    diffs = G.apply_lift_edit(diffs, moves[k])
-                    L.set_base(diffs)
-                    cur_total, cur_diam = ty, dy
-                    tr.accepted += 1
-                    aspl = cur_total * scale / npairs
-                    if aspl < best_aspl:
-                        best_aspl, best = aspl, diffs.copy()
-                        tr.times.append(time.perf_counter() - t_start)
-                        tr.best.append(best_aspl)
-                        if target is not None and tr.hit_time is None and best_aspl <= target:
-                            tr.hit_time, tr.hit_step = tr.times[-1], i + 1
-            tr.steps = i + 1
-            if target is not None and tr.hit_time is not None:
-                break
-            if time_limit is not None and time.perf_counter() - t_start > time_limit:
-                break
-        tr.wall = time.perf_counter() - t_start
-        tr.final_best = best_aspl
+        return _anneal_table(L, lambda t, c, s: G.gen_lift_moves(N, M, t, c, s), diffs, steps, seed=seed,
+                             exact=exact, t0_frac=t0_frac, t_end=t_end, target=target, time_limit=time_limit)
     finally:
         L.close()
-    return best, tr
+
+
+def anneal_piece(Nx, Ny, Mx, My, vals0, steps, *, seed=1, exact=32, t0_frac=1e-3, t_end=1e-6, target=None,
+                 time_limit=None, device=0):
+    """The same for a 2-D torus lift (cppcode/pieceannealing.cpp; vals [Mx*My, d, 2]);
+    t0_frac = 0 is the hill climb of pieceHillClimb.cpp."""
+    vals = np.asarray(vals0, dtype=np.int32).reshape(Mx * My, -1, 2)
+    L = G.Lift.piece(Nx, Ny, Mx, My, vals.shape[1], device)
+    try:
+        return _anneal_table(L, lambda t, c, s: G.gen_piece_moves(Nx, Ny, Mx, My, t, c, s), vals, steps,
+                             seed=seed, exact=exact, t0_frac=t0_frac, t_end=t_end, target=target,
+                             time_limit=time_limit)
+    finally:
+        L.close()
+
+
+def anneal_box(Nx, Ny, Nz, Mx, My, Mz, vals0, steps, *, seed=1, exact=32, t0_frac=0.0, t_end=1e-6,
+               target=None, time_limit=None, device=0):
+    """The same for a 3-D torus lift (vals [Mx*My*Mz, d, 3]); the default t0_frac = 0
+    is the hill climb of cppcode/boxHillClimb.cpp."""
+    vals = np.asarray(vals0, dtype=np.int32).reshape(Mx * My * Mz, -1, 3)
+    L = G.Lift.box(Nx, Ny, Nz, Mx, My, Mz, vals.shape[1], device)
+    try:
+        return _anneal_table(L, lambda t, c, s: G.gen_box_moves(Nx, Ny, Nz, Mx, My, Mz, t, c, s), vals, steps,
+                             seed=seed, exact=exact, t0_frac=t0_frac, t_end=t_end, target=target,
+                             time_limit=time_limit)
+    finally:
+        L.close()
 
 
 def time_to(trace, target):

@@ -241,3 +241,21 @@ def test_box_candidates_equal_the_oracle():
     diam, aspl = G.cudaASPLbox(Nx, Ny, Nz, Mx, My, Mz, 6, 0).diameterASPL(B)
     assert L.aspl(res[:1])[0] == aspl and int(res[0]["levels"]) == diam
     L.close()
+
+
+@pytest.mark.gpu
+def test_piece_annealing_and_box_hill_climb_report_exact_aspl():
+    import anneal as A
+    Mx, My = 8, 6
+    Nx, Ny, T = simple_piece(Mx, My, 3, 2, 4, 5)
+    start = O.piece_diameter_aspl(Nx, Ny, Mx, My, T)[1]
+    best, tr = A.anneal_piece(Nx, Ny, Mx, My, T, 60, seed=2, exact=16)
+    assert tr.accepted > 0 and O.piece_diameter_aspl(Nx, Ny, Mx, My, best)[1] == tr.final_best < start
+    assert graph_ok(O.expand_piece(Nx, Ny, Mx, My, best), np.zeros((Nx * Ny, 4), bool))
+    Nx, Ny, Nz, B = simple_box(3, 2, 2, 2, 2, 3, 4, 1)
+    start = O.box_diameter_aspl(Nx, Ny, Nz, 3, 2, 2, B)[1]
+    best, tr = A.anneal_box(Nx, Ny, Nz, 3, 2, 2, B, 40, seed=3, exact=16)
+    got = O.box_diameter_aspl(Nx, Ny, Nz, 3, 2, 2, best)[1]
+    assert got == tr.final_best <= start
+    # a hill climb never accepts a worse total
+    assert all(b >= c for b, c in zip(tr.best, tr.best[1:]))

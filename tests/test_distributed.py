@@ -1,8 +1,12 @@
-"""Source-sharded evaluation over torch.distributed: two gloo ranks on CPU run
-the sharding and the all-reduce of distributed.py; each rank's share is
-computed by an oracle-backed stand-in engine (the GPU engine does the same
-through gg_eval with a source range, tests/test_parity_gpu.py checks that), and
-the combined counts must equal the unsplit evaluation."""
+"""Sharded work over torch.distributed, two gloo ranks on CPU.
+
+Source-sharded evaluation: the ranks run the sharding and the all-reduce of
+distributed.py; each rank's share is computed by an oracle-backed stand-in
+engine (the GPU engine does the same through gg_eval with a source range,
+tests/test_parity_gpu.py checks that), and the combined counts must equal the
+unsplit evaluation.  Candidate-sharded scoring: each rank scores its slice of a
+population of lift moves with an oracle-backed stand-in for Lift.eval, and the
+gathered results must equal the unsplit scoring on both ranks."""
 import os
 import socket
 
@@ -79,3 +83,48 @@ def test_two_gloo_ranks_combine_exactly(adj):
         assert res["reached"] == int(whole.reached.sum())
         assert res["levels"] == whole.levels
         assert bool(res["connected"]) == whole.connected
+
+
+def lift_oracle_eval(N, M, T):
+    """Stand-in for Lift.eval: exact counts of each edit by the oracle."""
+    import graphgolf as G
+
+    def ev(edits):
+        out = np.zeros(len(edits), dtype=G.CAND_RESULT_DTYPE)
+        for i, e in enumerate(edits):
+            r = O.bfs_pull(O.expand_part(N, M, G.apply_lift_edit(T, e)), np.arange(M))
+            out[i] = (r.total(), int(r.reached.sum()), r.levels, int(r.connected))
+        return out
+    return ev
+
+
+def _cand_worker(rank, world, port, N, M, T, moves, out):
+    import datetime
+    import torch.distributed as dist
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=60))
+    try:
+        out[rank] = D.eval_candidates_sharded(lift_oracle_eval(N, M, T), moves).tobytes()
+    finally:
+        dist.destroy_process_group()
+
+
+
+@pytest.mark.parametrize("count", [9, 1])
+def test_two_gloo_ranks_gather_candidate_results(count):
+    import graphgolf as G
+    N, M, T = G.cyclic_lift(40, 4, 4, 3)
+    moves = G.gen_lift_moves(N, M, T, count, 5)
+    mgr = mp.Manager()
+    out = mgr.dict()
+    ctx = mp.get_context("spawn")
+    port = _free_port()
+    procs = [ctx.Process(target=_cand_worker, args=(r, 2, port, N, M, T, moves, out)) for r in range(2)]
+    for p in procs:
+        p.start()
+    for p in procs:
+        p.join(120)
+        assert p.exitcode == 0
+    whole = lift_oracle_eval(N, M, T)(moves).tobytes()
+    assert out[0] == whole and out[1] == whole

@@ -57,6 +57,10 @@ WORKLOADS = {
     # 256 shift / orbit 2-opt moves of a random cyclic lift (m=1024 orbits, g=32,
     # degree 12, N=32768) per step, all scored in one launch (gg_lift_eval)
     "lift_moves_256_m1024_g32_d12": dict(form="liftbatch", m=1024, g=32, d=12, seed=1, cands=256),
+    # the same for a 2-D torus lift (piece form): tile 32 x 32, lifted 256 x 128
+    # (N=32768), degree 8
+    "piece_moves_256_32x32_x8x4_d8": dict(form="liftbatch", kind="piece", Mx=32, My=32, kx=8, ky=4, d=8, seed=1,
+                                          cands=256),
 }
 METRIC = "ASPL evals/s"
 UNIT = "evals/s"
@@ -508,10 +512,20 @@ def run_lift_batch(args):
     rank, world, local = env_rank()
     torch.cuda.set_device(local)
     w = WORKLOADS[args.workload]
-    N, M, D = G.cyclic_lift(w["m"], w["g"], w["d"], w["seed"] + 1000 * rank)
-    L = G.Lift(N, M, w["d"], local)
+    if w.get("kind") == "piece":
+        Nx, Ny, Mx, My, D = G.piece_lift(w["Mx"], w["My"], w["kx"], w["ky"], w["d"], w["seed"] + 1000 * rank)
+        N, M = Nx * Ny, Mx * My
+        L = G.Lift.piece(Nx, Ny, Mx, My, w["d"], local)
+        moves = G.gen_piece_moves(Nx, Ny, Mx, My, D, w["cands"], w["seed"] + 5)
+        conv = G.cudaASPLpiece(Nx, Ny, Mx, My, w["d"], local)
+        what = "gg_piece_diameter_aspl per candidate table, host clock"
+    else:
+        N, M, D = G.cyclic_lift(w["m"], w["g"], w["d"], w["seed"] + 1000 * rank)
+        L = G.Lift(N, M, w["d"], local)
+        moves = G.gen_lift_moves(N, M, D, w["cands"], w["seed"] + 5)
+        conv = G.cudaASPLconv(N, M, w["d"], local)
+        what = "gg_conv_diameter_aspl per candidate table, host clock"
     L.set_base(D)
-    moves = G.gen_lift_moves(N, M, D, w["cands"], w["seed"] + 5)
     n = len(moves)
     flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
     for _ in range(max(args.warmup, 1)):
@@ -528,7 +542,6 @@ def run_lift_batch(args):
         dev_ms += L.last_ms()
     ck = clocks.stop()
     # one calculator call per candidate, as the reference scores them
-    conv = G.cudaASPLconv(N, M, w["d"], local)
     sample = min(n, 32)
     tabs = [G.apply_lift_edit(D, e) for e in moves[:sample]]
     conv.diameterASPL(tabs[0])
@@ -551,8 +564,7 @@ def run_lift_batch(args):
                     "h2d_bytes_per_step": int(moves.nbytes),
                     # the control block, then the per-level count rows 0..diameter+1
                     "d2h_bytes_per_step": int(256 + (int(res["levels"].max()) + 2) * n * 8)},
-            "single_call": {"ms_per_candidate": per_call_ms, "sample": sample,
-                            "what": "gg_conv_diameter_aspl per candidate table, host clock"},
+            "single_call": {"ms_per_candidate": per_call_ms, "sample": sample, "what": what},
             "gpu_launches": 2 * args.steps, "clocks": ck}
     if rank == 0:
         print(json.dumps(line), flush=True)

@@ -382,4 +382,53 @@ gg_status gg_gen_cyclic_lift(int m, int g, int d, uint64_t seed, int32_t *diffs)
     return GG_BAD_ARG;
 }
 
+gg_status gg_gen_piece_lift(int Mx, int My, int kx, int ky, int d, uint64_t seed, int32_t *vals) {
+    const long long M = (long long)Mx * My, Nx = (long long)Mx * kx, Ny = (long long)My * ky;
+    if (!vals || Mx < 1 || My < 1 || kx < 1 || ky < 1 || d < 1 || (M * d) % 2 != 0 || Nx * Ny >= (1ll << 30))
+        return GG_BAD_ARG;
+    Rng rng(seed);
+    for (int attempt = 0; attempt < 100000; ++attempt) {
+        std::vector<int> stubs((size_t)M * d);
+        for (int v = 0; v < M; ++v)
+            for (int k = 0; k < d; ++k) stubs[(size_t)v * d + k] = v;
+        for (size_t i = stubs.size(); i > 1; --i) std::swap(stubs[i - 1], stubs[rng.below((uint32_t)i)]);
+        std::vector<std::vector<std::pair<int, int>>> rows(M);
+        for (size_t i = 0; i + 1 < stubs.size(); i += 2) {
+            const int a = stubs[i], b = stubs[i + 1];
+            const int ax = a / My, ay = a % My, bx = b / My, by = b % My;
+            const int dx = (bx - ax) + Mx * (int)rng.below((uint32_t)kx);
+            const int dy = (by - ay) + My * (int)rng.below((uint32_t)ky);
+            rows[a].push_back({dx, dy});
+            rows[b].push_back({-dx, -dy});
+        }
+        // simple lift: the neighbours of each tile vertex are distinct and differ from it
+        bool ok = true;
+        for (int u = 0; u < M && ok; ++u) {
+            std::unordered_set<long long> seen;
+            const long long ux = u / My, uy = u % My;
+            for (auto &p : rows[u]) {
+                const long long tx = ((ux + p.first) % Nx + Nx) % Nx, ty = ((uy + p.second) % Ny + Ny) % Ny;
+                const long long to = tx * Ny + ty;
+                if (to == ux * Ny + uy || !seen.insert(to).second) { ok = false; break; }
+            }
+        }
+        if (!ok) continue;
+        const int N = (int)(Nx * Ny);
+        std::vector<std::vector<int>> gl(N);
+        for (int v = 0; v < N; ++v) {
+            const long long x = v / Ny, y = v % Ny;
+            for (auto &p : rows[(x % Mx) * My + (y % My)])
+                gl[v].push_back((int)((((x + p.first) % Nx + Nx) % Nx) * Ny + (((y + p.second) % Ny + Ny) % Ny)));
+        }
+        if (!connected(N, gl)) continue;
+        for (int u = 0; u < M; ++u)
+            for (int k = 0; k < d; ++k) {
+                vals[((size_t)u * d + k) * 2] = rows[u][k].first;
+                vals[((size_t)u * d + k) * 2 + 1] = rows[u][k].second;
+            }
+        return GG_OK;
+    }
+    return GG_BAD_ARG;
+}
+
 }  // extern "C"

@@ -80,22 +80,27 @@ __global__ void lift_tables(const int32_t *base, const gg_lift_edit *ed, int K, 
 // Pull adjacency of every candidate of a 2-D or 3-D torus lift (axes sizes n,
 // orbit sizes m; vertex (x * ny + y) * nz + z), from its table of diffs already
 // reduced to [0, n): the expansion of cudaASPLpiece.cu:41-50 / cudaASPLbox.cu:44-57.
+// One thread per (candidate, vertex): the coordinates and the orbit row once, then
+// the row's d entries.
 __global__ void lift_expand(const int32_t *tab, int K, int M, int d, int comps, int nx, int ny, int nz, int mx,
                             int my, int mz, int32_t *adj) {
-    const long long N = (long long)nx * ny * nz, per = N * d, total = per * K;
+    const long long N = (long long)nx * ny * nz, total = N * K;
     for (long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x; q < total;
          q += (long long)gridDim.x * blockDim.x) {
-        const int k = (int)(q / per);
-        const long long e = q - (long long)k * per;
-        const int v = (int)(e / d), i = (int)(e - (long long)v * d);
+        const int k = (int)(q / N);
+        const int v = (int)(q - (long long)k * N);
         const int x = v / (ny * nz), rem = v - x * (ny * nz), y = rem / nz, z = rem - y * nz;
         const int r = ((x % mx) * my + (y % my)) * mz + (z % mz);
-        const int32_t *t = tab + (((size_t)k * M + r) * d + i) * comps;
-        int tx = x + t[0], ty = y + t[1], tz = comps > 2 ? z + t[2] : z;
-        tx -= tx >= nx ? nx : 0;
-        ty -= ty >= ny ? ny : 0;
-        tz -= tz >= nz ? nz : 0;
-        adj[q] = (tx * ny + ty) * nz + tz;
+        const int32_t *t = tab + ((size_t)k * M + r) * d * comps;
+        int32_t *out = adj + (size_t)q * d;
+        for (int i = 0; i < d; ++i) {
+            int tx = x + __ldg(t + i * comps), ty = y + __ldg(t + i * comps + 1);
+            int tz = comps > 2 ? z + __ldg(t + i * comps + 2) : z;
+            tx -= tx >= nx ? nx : 0;
+            ty -= ty >= ny ? ny : 0;
+            tz -= tz >= nz ? nz : 0;
+            out[i] = (tx * ny + ty) * nz + tz;
+        }
     }
 }
 
@@ -640,8 +645,8 @@ gg_status gg_lift_eval(gg_lift *h, int n_cand, const gg_lift_edit *edits, int ma
         h->d_base, h->d_ed, n_cand, h->M, h->d, h->axes, h->d_tab);
     GL_CK(cudaGetLastError());
     if (h->axes > 1) {
-        const long long adj_n = (long long)n_cand * h->N * h->d;
-        lift_expand<<<(int)std::min<long long>((adj_n + 255) / 256, (long long)h->sms * 16), 256, 0, st>>>(
+        const long long rows_n = (long long)n_cand * h->N;
+        lift_expand<<<(int)std::min<long long>((rows_n + 255) / 256, (long long)h->sms * 16), 256, 0, st>>>(
             h->d_tab, n_cand, h->M, h->d, h->axes, h->n[0], h->n[1], h->n[2], h->m[0], h->m[1], h->m[2], h->d_adj);
         GL_CK(cudaGetLastError());
     }

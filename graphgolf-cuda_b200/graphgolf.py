@@ -124,6 +124,7 @@ _SIGS = {
     "gg_inc_commit": [_P, _P, _P],
     "gg_inc_destroy": [_P],
     "gg_gen_cyclic_lift": [_I, _I, _I, ctypes.c_uint64, _P],
+    "gg_gen_piece_lift": [_I, _I, _I, _I, _I, ctypes.c_uint64, _P],
     "gg_lift_create": [_I, _I, _I, _I, _EPP],
     "gg_lift_create_piece": [_I, _I, _I, _I, _I, _I, _EPP],
     "gg_lift_create_box": [_I, _I, _I, _I, _I, _I, _I, _I, _EPP],
@@ -197,6 +198,13 @@ def cyclic_lift(m, g, d, seed):
     out = np.empty((m, d), dtype=np.int32)
     _check(lib().gg_gen_cyclic_lift(m, g, d, seed, _ptr(out)))
     return m * g, m, out
+
+
+def piece_lift(Mx, My, kx, ky, d, seed):
+    """Simple connected random 2-D torus lift -> (Nx, Ny, Mx, My, vals [Mx*My, d, 2])."""
+    out = np.empty((Mx * My, d, 2), dtype=np.int32)
+    _check(lib().gg_gen_piece_lift(Mx, My, kx, ky, d, seed, _ptr(out)))
+    return Mx * kx, My * ky, Mx, My, out
 
 
 # ----------------------------------------------------------------------------

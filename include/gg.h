@@ -372,6 +372,9 @@ gg_status gg_gen_random_regular(int n, int d, uint64_t seed, int32_t *adj);
  * diffs m*d with diff = (v-u) + m*s for the quotient edge (u,v,s) and -diff on
  * the reverse end. */
 gg_status gg_gen_cyclic_lift(int m, int g, int d, uint64_t seed, int32_t *diffs);
+/* Simple connected random 2-D torus lift: orbit tile Mx x My, lifted size
+ * (Mx*kx) x (My*ky), degree d; vals: Mx*My * d * 2 int32 (the piece table). */
+gg_status gg_gen_piece_lift(int Mx, int My, int kx, int ky, int d, uint64_t seed, int32_t *vals);
 
 const char *gg_status_str(gg_status s);
 /* Text of the last error raised on this host thread ("" if none). */

@@ -259,3 +259,13 @@ def test_piece_annealing_and_box_hill_climb_report_exact_aspl():
     assert got == tr.final_best <= start
     # a hill climb never accepts a worse total
     assert all(b >= c for b, c in zip(tr.best, tr.best[1:]))
+
+
+def test_piece_lift_generator_is_simple_and_connected():
+    Nx, Ny, Mx, My, T = G.piece_lift(8, 6, 4, 3, 4, 3)
+    assert (Nx, Ny, T.shape) == (32, 18, (48, 4, 2))
+    adj = O.expand_piece(Nx, Ny, Mx, My, T)
+    assert graph_ok(adj, np.zeros((Nx * Ny, 4), bool))
+    assert O.bfs_pull(adj, np.arange(Nx * Ny)).connected
+    again = G.piece_lift(8, 6, 4, 3, 4, 3)[4]
+    assert again.tobytes() == T.tobytes()

@@ -498,6 +498,20 @@ def run_incremental(args):
     return 0
 
 
+def lift_bitset_rate(res, group, N, M, d, ms):
+    """Bitset GB/s of one lift launch: the algorithmic bytes of a BFS level over a
+    batch of S sources, N*d*4 + N*(d+2)*S/8, for each candidate of a round at
+    each of the round's levels (its candidates' largest eccentricity), over the
+    device time; against the measured HBM copy bandwidth."""
+    per_level = N * d * 4 + N * (d + 2) * M / 8
+    levels = [int(res["levels"][i:i + group].max()) for i in range(0, len(res), group)]
+    nbytes = sum(L * min(group, len(res) - r * group) * per_level for r, L in enumerate(levels))
+    peak, src = peaks()
+    gbs = nbytes / (ms * 1e-3) / 1e9
+    return {"algorithmic_bytes": nbytes, "gbs": gbs, "peak_gbs": peak, "frac": gbs / peak,
+            "peak_source": src + " HBM copy"}
+
+
 def run_lift_batch(args):
     """Batched lifted candidates: every step scores the same population of moves
     of one cyclic lift with one blocking gg_lift_eval call (edits in, counts out).
@@ -565,7 +579,8 @@ def run_lift_batch(args):
                     # the control block, then the per-level count rows 0..diameter+1
                     "d2h_bytes_per_step": int(256 + (int(res["levels"].max()) + 2) * n * 8)},
             "single_call": {"ms_per_candidate": per_call_ms, "sample": sample, "what": what},
-            "gpu_launches": 2 * args.steps, "clocks": ck}
+            "bitset": lift_bitset_rate(res, L.group(), N, M, w["d"], dev_ms / args.steps),
+            "gpu_launches": (2 if w.get("kind") != "piece" else 3) * args.steps, "clocks": ck}
     if rank == 0:
         print(json.dumps(line), flush=True)
     L.close()

@@ -39,6 +39,7 @@ namespace {
 
 constexpr int kLiftBlock = 256;
 constexpr int kMaxGroup = 32;
+constexpr int kFirstLevels = 256;   // count rows a launch starts with (see gg_lift_eval)
 
 struct LiftArgs {
     const int32_t *tab;              // part form: [K][M][d] diffs in [0, N), rows 16-byte aligned when d % 4 == 0
@@ -624,77 +625,86 @@ gg_status gg_lift_eval(gg_lift *h, int n_cand, const gg_lift_edit *edits, int ma
             }
         }
     }
-    const int ml = max_levels > 0 ? std::min(max_levels, h->N) : h->N;
-    s = ensure_counts(h, (size_t)(ml + 1) * n_cand);
-    if (s != GG_OK) return s;
-    if (ml + 1 > h->level_ns_n) {
-        cudaFree(h->d_level_ns); cudaFreeHost(h->h_level_ns);
-        h->d_level_ns = nullptr; h->h_level_ns = nullptr; h->level_ns_n = 0;
-        GL_CK(cudaMalloc(&h->d_level_ns, (size_t)(ml + 1) * sizeof(unsigned long long)));
-        GL_CK(cudaMallocHost(&h->h_level_ns, (size_t)(ml + 1) * sizeof(unsigned long long)));
-        h->level_ns_n = ml + 1;
-    }
-    const int G = std::min(h->group ? h->group : h->g_auto, n_cand);
-    const cudaStream_t st = h->stream;
-    GL_CK(cudaMemcpyAsync(h->d_ed, h->h_ed, (size_t)n_cand * sizeof(gg_lift_edit), cudaMemcpyHostToDevice, st));
-    GL_CK(cudaMemsetAsync(h->d_ctl, 0, sizeof(gg::Ctl), st));
-    GL_CK(cudaMemsetAsync(h->d_counts, 0, (size_t)std::min(ml + 1, 2) * n_cand * sizeof(unsigned long long), st));
-    GL_CK(cudaEventRecord(h->ev0, st));
-    const long long tab_n = (long long)n_cand * h->M * h->d;
-    lift_tables<<<(int)std::min<long long>((tab_n + 255) / 256, (long long)h->sms * 16), 256, 0, st>>>(
-        h->d_base, h->d_ed, n_cand, h->M, h->d, h->axes, h->d_tab);
-    GL_CK(cudaGetLastError());
-    if (h->axes > 1) {
-        const long long rows_n = (long long)n_cand * h->N;
-        lift_expand<<<(int)std::min<long long>((rows_n + 255) / 256, (long long)h->sms * 16), 256, 0, st>>>(
-            h->d_tab, n_cand, h->M, h->d, h->axes, h->n[0], h->n[1], h->n[2], h->m[0], h->m[1], h->m[2], h->d_adj);
-        GL_CK(cudaGetLastError());
-    }
-    LiftArgs a{};
-    a.tab = h->d_tab;
-    a.adj = h->d_adj;
-    a.inv = h->d_inv;
-    a.N = h->N; a.M = h->M; a.d = h->d; a.K = n_cand; a.G = G; a.cpc = h->cpc; a.W = G * h->cpc;
-    a.V = h->V; a.F0 = h->F0; a.F1 = h->F1;
-    a.counts = h->d_counts;
-    a.max_levels = ml;
-    const unsigned threads = (unsigned)h->grid * kLiftBlock;
-    if ((unsigned)a.W > threads) return lfail(GG_BAD_ARG, "more chunk columns than threads: lower the group");
-    a.cols_threads = threads / (unsigned)a.W * (unsigned)a.W;
-    a.vstep = a.cols_threads / (unsigned)a.W;
-    a.half_ppm = h->half_ppm;
-    a.level_ns = h->d_level_ns;
-    a.ctl = h->d_ctl;
-    a.wait_ns = h->wait_ns;
-    a.expected = (unsigned)h->grid;
-    GL_CK(cudaMemsetAsync(h->d_level_ns, 0, (size_t)(ml + 1) * sizeof(unsigned long long), st));
-    void *args[] = {&a};
-    GL_CK(cudaLaunchCooperativeKernel(lift_kernel_for(h->d, h->axes > 1), dim3(h->grid), dim3(kLiftBlock), args, 0,
-                                      st));
-    GL_CK(cudaEventRecord(h->ev1, st));
-    GL_CK(cudaMemcpyAsync(h->h_ctl, h->d_ctl, sizeof(gg::Ctl), cudaMemcpyDeviceToHost, st));
-    GL_CK(cudaStreamSynchronize(st));
-    if (h->h_ctl->err) return lfail(GG_TIMEOUT, "grid barrier wait exceeded the limit");
-    const int lr = std::min(h->h_ctl->levels_run, ml);
-    GL_CK(cudaMemcpyAsync(h->h_counts, h->d_counts, (size_t)(lr + 1) * n_cand * sizeof(unsigned long long),
-                          cudaMemcpyDeviceToHost, st));
-    GL_CK(cudaMemcpyAsync(h->h_level_ns, h->d_level_ns, (size_t)(lr + 1) * sizeof(unsigned long long),
-                          cudaMemcpyDeviceToHost, st));
-    GL_CK(cudaStreamSynchronize(st));
-    GL_CK(cudaEventElapsedTime(&h->last_ms, h->ev0, h->ev1));
-    const unsigned long long all = (unsigned long long)h->M * (unsigned long long)h->N;
-    for (int k = 0; k < n_cand; ++k) {
-        unsigned long long tot = 0, reach = (unsigned long long)h->M;
-        int lev = 0;
-        for (int L = 1; L <= lr; ++L) {
-            const unsigned long long c = h->h_counts[(size_t)L * n_cand + k];
-            if (!c) continue;
-            tot += (unsigned long long)L * c;
-            reach += c;
-            lev = L;
+    // Count rows for the first kFirstLevels levels; a population where some candidate
+    // still finds pairs there (a lift of very large diameter) runs again with rows
+    // for the full cap, so the buffers stay small for the usual diameters.
+    const int ml_full = max_levels > 0 ? std::min(max_levels, h->N) : h->N;
+    for (int ml = std::min(ml_full, kFirstLevels);; ml = ml_full) {
+        s = ensure_counts(h, (size_t)(ml + 1) * n_cand);
+        if (s != GG_OK) return s;
+        if (ml + 1 > h->level_ns_n) {
+            cudaFree(h->d_level_ns); cudaFreeHost(h->h_level_ns);
+            h->d_level_ns = nullptr; h->h_level_ns = nullptr; h->level_ns_n = 0;
+            GL_CK(cudaMalloc(&h->d_level_ns, (size_t)(ml + 1) * sizeof(unsigned long long)));
+            GL_CK(cudaMallocHost(&h->h_level_ns, (size_t)(ml + 1) * sizeof(unsigned long long)));
+            h->level_ns_n = ml + 1;
         }
-        const bool capped = lev == ml && reach < all;
-        out[k] = gg_cand_result{tot, reach, lev, (!capped && reach == all) ? 1 : 0};
+        const int G = std::min(h->group ? h->group : h->g_auto, n_cand);
+        const cudaStream_t st = h->stream;
+        GL_CK(cudaMemcpyAsync(h->d_ed, h->h_ed, (size_t)n_cand * sizeof(gg_lift_edit), cudaMemcpyHostToDevice, st));
+        GL_CK(cudaMemsetAsync(h->d_ctl, 0, sizeof(gg::Ctl), st));
+        GL_CK(cudaMemsetAsync(h->d_counts, 0, (size_t)std::min(ml + 1, 2) * n_cand * sizeof(unsigned long long), st));
+        GL_CK(cudaEventRecord(h->ev0, st));
+        const long long tab_n = (long long)n_cand * h->M * h->d;
+        lift_tables<<<(int)std::min<long long>((tab_n + 255) / 256, (long long)h->sms * 16), 256, 0, st>>>(
+            h->d_base, h->d_ed, n_cand, h->M, h->d, h->axes, h->d_tab);
+        GL_CK(cudaGetLastError());
+        if (h->axes > 1) {
+            const long long rows_n = (long long)n_cand * h->N;
+            lift_expand<<<(int)std::min<long long>((rows_n + 255) / 256, (long long)h->sms * 16), 256, 0, st>>>(
+                h->d_tab, n_cand, h->M, h->d, h->axes, h->n[0], h->n[1], h->n[2], h->m[0], h->m[1], h->m[2], h->d_adj);
+            GL_CK(cudaGetLastError());
+        }
+        LiftArgs a{};
+        a.tab = h->d_tab;
+        a.adj = h->d_adj;
+        a.inv = h->d_inv;
+        a.N = h->N; a.M = h->M; a.d = h->d; a.K = n_cand; a.G = G; a.cpc = h->cpc; a.W = G * h->cpc;
+        a.V = h->V; a.F0 = h->F0; a.F1 = h->F1;
+        a.counts = h->d_counts;
+        a.max_levels = ml;
+        const unsigned threads = (unsigned)h->grid * kLiftBlock;
+        if ((unsigned)a.W > threads) return lfail(GG_BAD_ARG, "more chunk columns than threads: lower the group");
+        a.cols_threads = threads / (unsigned)a.W * (unsigned)a.W;
+        a.vstep = a.cols_threads / (unsigned)a.W;
+        a.half_ppm = h->half_ppm;
+        a.level_ns = h->d_level_ns;
+        a.ctl = h->d_ctl;
+        a.wait_ns = h->wait_ns;
+        a.expected = (unsigned)h->grid;
+        GL_CK(cudaMemsetAsync(h->d_level_ns, 0, (size_t)(ml + 1) * sizeof(unsigned long long), st));
+        void *args[] = {&a};
+        GL_CK(cudaLaunchCooperativeKernel(lift_kernel_for(h->d, h->axes > 1), dim3(h->grid), dim3(kLiftBlock), args, 0,
+                                          st));
+        GL_CK(cudaEventRecord(h->ev1, st));
+        GL_CK(cudaMemcpyAsync(h->h_ctl, h->d_ctl, sizeof(gg::Ctl), cudaMemcpyDeviceToHost, st));
+        GL_CK(cudaStreamSynchronize(st));
+        if (h->h_ctl->err) return lfail(GG_TIMEOUT, "grid barrier wait exceeded the limit");
+        const int lr = std::min(h->h_ctl->levels_run, ml);
+        GL_CK(cudaMemcpyAsync(h->h_counts, h->d_counts, (size_t)(lr + 1) * n_cand * sizeof(unsigned long long),
+                              cudaMemcpyDeviceToHost, st));
+        GL_CK(cudaMemcpyAsync(h->h_level_ns, h->d_level_ns, (size_t)(lr + 1) * sizeof(unsigned long long),
+                              cudaMemcpyDeviceToHost, st));
+        GL_CK(cudaStreamSynchronize(st));
+        GL_CK(cudaEventElapsedTime(&h->last_ms, h->ev0, h->ev1));
+        const unsigned long long all = (unsigned long long)h->M * (unsigned long long)h->N;
+        for (int k = 0; k < n_cand; ++k) {
+            unsigned long long tot = 0, reach = (unsigned long long)h->M;
+            int lev = 0;
+            for (int L = 1; L <= lr; ++L) {
+                const unsigned long long c = h->h_counts[(size_t)L * n_cand + k];
+                if (!c) continue;
+                tot += (unsigned long long)L * c;
+                reach += c;
+                lev = L;
+            }
+            const bool capped = lev == ml && reach < all;
+            out[k] = gg_cand_result{tot, reach, lev, (!capped && reach == all) ? 1 : 0};
+        }
+        bool again = false;
+        for (int k = 0; k < n_cand && ml < ml_full; ++k)
+            again |= out[k].levels == ml && out[k].reached < all;
+        if (!again) break;
     }
     return GG_OK;
 }

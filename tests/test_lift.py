@@ -269,3 +269,22 @@ def test_piece_lift_generator_is_simple_and_connected():
     assert O.bfs_pull(adj, np.arange(Nx * Ny)).connected
     again = G.piece_lift(8, 6, 4, 3, 4, 3)[4]
     assert again.tobytes() == T.tobytes()
+
+
+@pytest.mark.gpu
+def test_lift_diameter_beyond_the_first_count_rows():
+    # a cycle of 600 as a part with 2 orbits: diameter 300, past the 256 count rows a
+    # launch starts with, so the population runs again with rows for the full cap
+    N, M = 600, 2
+    T = np.array([[1, -1], [1, -1]], np.int32)
+    L = G.Lift(N, M, 2, 0)
+    L.set_base(T)
+    base = np.zeros(2, dtype=G.LIFT_EDIT_DTYPE)
+    want = oracle_counts(N, M, T)
+    r = L.eval(base)
+    assert want[2] == 300 and want[3] == 1
+    for x in r:
+        assert (int(x["total"]), int(x["reached"]), int(x["levels"]), int(x["connected"])) == want
+    capped = L.eval(base, max_levels=280)
+    assert (capped["connected"] == 0).all() and (capped["levels"] == 280).all()
+    L.close()

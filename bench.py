@@ -432,7 +432,7 @@ def run_anneal(args):
 
 
 def bit_edges_per_eval(wl, r):
-    """Survey measure: sum over executed levels of N * d * S (S = sources of the
+    """Bit-edge traversals: sum over executed levels of N * d * S (S = sources of the
     batch), for an evaluation with all batches of equal width."""
     S = -(-r["n_sources"] // r["batches"])
     return r["level_steps"] * wl["N"] * wl["d"] * S

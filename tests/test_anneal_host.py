@@ -1,4 +1,6 @@
-"""Host-side helpers of the annealer (no GPU)."""
+"""Host-side parts of the annealers (no GPU): the rank correlation, and the
+lifted annealing loop driven by an oracle-backed stand-in for the GPU lift
+evaluator (acceptance, hill-climb order, exact reported ASPL, target stop)."""
 import numpy as np
 
 import anneal as A
@@ -12,3 +14,59 @@ def test_rank_correlation_matches_scipy():
     y[::7] = y[0]                        # ties
     assert abs(A.rank_correlation(x, y) - spearmanr(x, y).correlation) < 1e-12
     assert A.rank_correlation(x, -x) == -1.0
+
+
+# ---- the lifted annealing loop, driven by an oracle-backed stand-in -----------
+
+import graphgolf as G
+import oracle as O
+
+
+class OracleLift:
+    """Stand-in for G.Lift (part form): the same set_base / eval interface, exact
+    counts from the oracle; records every base the loop installs."""
+
+    def __init__(self, N, M):
+        self.N, self.M = N, M
+        self.bases = []
+
+    def set_base(self, table):
+        self.base = np.array(table, dtype=np.int32, copy=True)
+        self.bases.append(self.base)
+
+    def eval(self, edits):
+        out = np.zeros(len(edits), dtype=G.CAND_RESULT_DTYPE)
+        for i, e in enumerate(edits):
+            r = O.bfs_pull(O.expand_part(self.N, self.M, G.apply_lift_edit(self.base, e)), np.arange(self.M))
+            out[i] = (r.total(), int(r.reached.sum()), r.levels, int(r.connected))
+        return out
+
+
+def _key(N, M, table):
+    r = O.bfs_pull(O.expand_part(N, M, table), np.arange(M))
+    return r.levels, r.total()
+
+
+def test_lifted_hill_climb_never_worsens_and_reports_exact_aspl():
+    N, M, D = G.cyclic_lift(24, 4, 4, 2)
+    L = OracleLift(N, M)
+    gen = lambda t, c, s: G.gen_lift_moves(N, M, t, c, s)  # noqa: E731
+    best, tr = A._anneal_table(L, gen, D, 25, seed=4, exact=8, t0_frac=0.0, t_end=1e-6, target=None,
+                               time_limit=None)
+    keys = [_key(N, M, b) for b in L.bases]
+    assert all(k2 <= k1 for k1, k2 in zip(keys, keys[1:]))       # (diameter, total) never rises
+    assert tr.accepted == len(L.bases) - 1 and tr.exact_evals == 25 * 8
+    assert O.conv_diameter_aspl(N, M, best)[1] == tr.final_best
+    assert tr.final_best <= O.conv_diameter_aspl(N, M, D)[1]
+
+
+def test_lifted_annealing_stops_at_the_target():
+    N, M, D = G.cyclic_lift(24, 4, 4, 2)
+    gen = lambda t, c, s: G.gen_lift_moves(N, M, t, c, s)  # noqa: E731
+    _, full = A._anneal_table(OracleLift(N, M), gen, D, 25, seed=4, exact=8, t0_frac=0.0, t_end=1e-6,
+                              target=None, time_limit=None)
+    assert len(full.best) >= 3                                   # this start improves several times
+    target = full.best[2]
+    _, tr = A._anneal_table(OracleLift(N, M), gen, D, 25, seed=4, exact=8, t0_frac=0.0, t_end=1e-6,
+                            target=target, time_limit=None)
+    assert tr.hit_time is not None and tr.final_best <= target and tr.steps == tr.hit_step

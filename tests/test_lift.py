@@ -288,3 +288,15 @@ def test_lift_diameter_beyond_the_first_count_rows():
     capped = L.eval(base, max_levels=280)
     assert (capped["connected"] == 0).all() and (capped["levels"] == 280).all()
     L.close()
+
+
+def test_piece_and_box_moves_without_copies_are_all_2opt_and_bad_sizes_fail():
+    # a tile that is the whole torus (one copy): no lift shift to redraw
+    Nx, Ny, Mx, My, T = G.piece_lift(6, 5, 1, 1, 4, 2)
+    moves = G.gen_piece_moves(Nx, Ny, Mx, My, T, 20, 1)
+    assert (moves["count"] == 4).all()
+    with pytest.raises(G.GGError):
+        G.gen_piece_moves(Nx + 1, Ny, Mx, My, T, 2, 1)          # 7 is no multiple of 6
+    Nx, Ny, Nz, B = simple_box(3, 2, 2, 2, 2, 3, 4, 1)
+    with pytest.raises(G.GGError):
+        G.gen_box_moves(Nx, Ny, Nz + 1, 3, 2, 2, B, 2, 1)

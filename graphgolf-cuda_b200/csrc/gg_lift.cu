@@ -1,14 +1,20 @@
-// gg_lift.cu -- batched exact evaluation of cyclic-lift ("part") candidates
-// (gg_lift_* in gg.h).
+// gg_lift.cu -- batched exact evaluation of lifted candidates (gg_lift_* in gg.h):
+// cyclic lifts ("part"), 2-D and 3-D torus lifts ("piece", "box").
 //
-// The lifted form of cudaASPLconv: M orbit vertices with d diffs each; vertex v
-// of the N-vertex lift has the neighbours (v + diffs[v % M][i]) mod N, and the
-// BFS runs from the M vertices 0..M-1 (cudaASPLconv.cu:197-243).  The
-// reference's annealer changes 2 or 4 slots of the diff table per proposal
-// (cppcode/annealing.cpp:112-197) and scores each with one calculator call.
+// The part form of cudaASPLconv: M orbit vertices with d diffs each; vertex v of
+// the N-vertex lift has the neighbours (v + diffs[v % M][i]) mod N, and the BFS
+// runs from the M vertices 0..M-1 (cudaASPLconv.cu:197-243).  Piece and box
+// tables hold 2- or 3-component diffs per orbit of a corner tile, the BFS runs
+// from that tile (cudaASPLpiece.cu:159-216, cudaASPLbox.cu:166-226).  The
+// reference's annealers change 2 or 4 slots of the table per proposal
+// (cppcode/annealing.cpp:112-197, pieceannealing.cpp:113-204) and score each with
+// one calculator call.
 //
 // Here one cooperative launch scores a population.  `lift_tables` writes every
-// candidate's diff table (base + edit, diffs reduced to [0, N)).  `lift_kernel`
+// candidate's table (base + edit, diffs reduced to [0, n) per axis); for piece and
+// box, `lift_expand` turns each into a pull adjacency and the kernel's EXPL
+// variant reads adjacency rows and finds sources through a vertex ->
+// representative map.  `lift_kernel`
 // runs the candidates in rounds of G side by side: a round's bitsets hold, per
 // vertex, W = G * cpc uint4 chunks (cpc = ceil(M/128)), chunk group g being the
 // M sources of candidate g of the round, source s at bit s % 128 of chunk s / 128
@@ -18,7 +24,9 @@
 // candidate.  Each thread owns one chunk column w (so one group, one counter and
 // one table) and walks the vertices v = v0, v0 + VS, ...; consecutive lanes own
 // consecutive columns, so the gathers of a neighbour row are contiguous 16-byte
-// loads, all issued before the first is used.  Late in a round (past 85 % of its
+// loads, all issued before the first is used.  Level 1 is the round's reset pass
+// (a chunk's level-1 pairs are the sources among its own neighbours: no gather).
+// Late in a round (past 85 % of its
 // pairs reached) a chunk gathers half its neighbours first and the rest only
 // while it still misses sources.  New pairs are counted per thread, reduced per
 // group at the end of the level (shared atomics, then one global atomic per block

@@ -346,6 +346,13 @@ class piece:
                 row = self.edges[x][y]
                 ost.write(" ".join([str(len(row))] + [f"{a} {b}" for a, b in row]) + "\n")
 
+    @classmethod
+    def from_table(cls, Nx, Ny, Mx, My, vals):
+        """The piece of a table [Mx*My, d, 2] (e.g. an annealer's result)."""
+        t = np.asarray(vals).reshape(Mx * My, -1, 2)
+        edges = [[[(int(a), int(b)) for a, b in t[x * My + y]] for y in range(My)] for x in range(Mx)]
+        return cls(Nx=Nx, Ny=Ny, Mx=Mx, My=My, regular=True, degree=t.shape[1], edges=edges)
+
     def table(self, degree):
         """Mx*My*degree*2 int32, padding (0,0) (cudaASPLpiece.cu:166-176)."""
         t = np.zeros((self.Mx * self.My, degree, 2), dtype=np.int32)
@@ -402,6 +409,14 @@ class box:
                 for z in range(self.Mz):
                     row = self.edges[x][y][z]
                     ost.write(" ".join([str(len(row))] + [f"{a} {b} {c}" for a, b, c in row]) + "\n")
+
+    @classmethod
+    def from_table(cls, Nx, Ny, Nz, Mx, My, Mz, vals):
+        """The box of a table [Mx*My*Mz, d, 3] (e.g. an annealer's result)."""
+        t = np.asarray(vals).reshape(Mx * My * Mz, -1, 3)
+        edges = [[[[tuple(int(c) for c in e) for e in t[(x * My + y) * Mz + z]] for z in range(Mz)]
+                  for y in range(My)] for x in range(Mx)]
+        return cls(Nx=Nx, Ny=Ny, Nz=Nz, Mx=Mx, My=My, Mz=Mz, regular=True, degree=t.shape[1], edges=edges)
 
     def table(self, degree):
         """Mx*My*Mz*degree*3 int32, padding (0,0,0) (cudaASPLbox.cu:170-184)."""

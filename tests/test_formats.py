@@ -74,6 +74,26 @@ def test_to_graph_and_text_round_trips():
     assert np.array_equal(np.unique(back, axis=0), G.piece_pairs(p))
 
 
+def test_tables_round_trip_through_the_text_formats():
+    # an annealer's result table -> form -> text -> form -> the same table
+    Nx, Ny, Mx, My, rows = I.random_piece(3, 2, 2, 3, 4, 5)
+    p = G.piece.from_table(Nx, Ny, Mx, My, rows)
+    assert p.edges == make_piece(Nx, Ny, Mx, My, rows).edges
+    s = io.StringIO()
+    p.print(s)
+    assert np.array_equal(G.piece().load(io.StringIO(s.getvalue())).table(4), rows)
+    Nx, Ny, Nz, Mx, My, Mz, rows = I.random_box(2, 2, 3, 2, 1, 2, 4, 6)
+    b = G.box.from_table(Nx, Ny, Nz, Mx, My, Mz, rows)
+    assert b.edges == make_box(Nx, Ny, Nz, Mx, My, Mz, rows).edges
+    s = io.StringIO()
+    b.print(s)
+    assert np.array_equal(G.box().load(io.StringIO(s.getvalue())).table(4), rows)
+    N, M, D = G.cyclic_lift(12, 3, 4, 2)
+    s = io.StringIO()
+    G.part.from_diffs(N, M, D).print(s)
+    assert np.array_equal(G.part().load(io.StringIO(s.getvalue())).table(4), D)
+
+
 def test_converter_drops_repeated_lifted_edges():
     # a 1x1 tile whose two diffs lift to the same edges: (1,0) and (-1,0) on Nx=2
     p = G.piece(Nx=2, Ny=1, Mx=1, My=1, degree=2)

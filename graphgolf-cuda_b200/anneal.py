@@ -336,3 +336,49 @@ def initial_temperature(n, d, *, graphs=100, neighbours=100, seed=1, accept=0.4,
     temp = -avg / math.log(accept)
     npairs = n * (n - 1)
     return InitTemp(temp=temp, temp_aspl=temp / npairs, avg=avg, uphill=cnt, proposals=len(cand), ms=ms)
+
+
+def initial_temperature_piece(Nx, Ny, Mx, My, d, *, graphs=100, neighbours=100, seed=1, accept=0.4, device=0,
+                              bases=None, make_lift=None):
+    """Initial temperature for 2-D torus lifts, restating cppcode/pieceinitTemp.cpp:211-260
+    on the batched lift evaluator: for `graphs` random pieces (tile Mx x My, lifted
+    Nx x Ny, degree d) and `neighbours` lift moves of each (gg_gen_piece_moves, the
+    moves of :113-209), the mean increase of the total distance over the connected
+    uphill moves; T0 = -avg / ln(accept) (:253-258).  Each piece and its moves are one
+    launch.  The reference's filter `fy != 1e9` (:249) does not catch
+    cudaASPLpiece's disconnected sentinel 1e8, so it counts disconnected neighbours
+    as uphill moves of about 1e8; here, as in initial_temperature, only connected
+    neighbours of connected pieces count.  The totals are exact integers (ASPL
+    differences times N(N-1) in the reference).
+
+    `bases` replaces the random pieces (each a [Mx*My, d, 2] table); `make_lift`
+    replaces the evaluator factory (G.Lift.piece)."""
+    N = Nx * Ny
+    if bases is None:
+        bases = [G.piece_lift(Mx, My, Nx // Mx, Ny // My, d, seed * 1000003 + k)[4] for k in range(graphs)]
+    if make_lift is None:
+        make_lift = lambda: G.Lift.piece(Nx, Ny, Mx, My, d, device)  # noqa: E731
+    L = make_lift()
+    deltas, proposals, ms = [], 0, 0.0
+    try:
+        for k, T in enumerate(bases):
+            L.set_base(T)
+            moves = G.gen_piece_moves(Nx, Ny, Mx, My, T, neighbours, (seed << 20) ^ k)
+            res = L.eval(np.concatenate([np.zeros(1, dtype=G.LIFT_EDIT_DTYPE), moves]))
+            ms += L.last_ms() if hasattr(L, "last_ms") else 0.0
+            proposals += len(moves)
+            if not res["connected"][0]:
+                continue
+            cand = res[1:]
+            delta = cand["total"].astype(np.int64) - int(res["total"][0])
+            deltas.append(delta[(cand["connected"] == 1) & (delta > 0)])
+    finally:
+        if hasattr(L, "close"):
+            L.close()
+    up = np.concatenate(deltas) if deltas else np.zeros(0, dtype=np.int64)
+    if len(up) == 0:
+        raise ValueError("no connected uphill proposal")
+    # the totals are over the M representatives: scale to all N sources
+    avg = int(up.sum()) * (N // (Mx * My)) / len(up)
+    temp = -avg / math.log(accept)
+    return InitTemp(temp=temp, temp_aspl=temp / (N * (N - 1)), avg=avg, uphill=len(up), proposals=proposals, ms=ms)

@@ -70,3 +70,43 @@ def test_lifted_annealing_stops_at_the_target():
     _, tr = A._anneal_table(OracleLift(N, M), gen, D, 25, seed=4, exact=8, t0_frac=0.0, t_end=1e-6,
                             target=target, time_limit=None)
     assert tr.hit_time is not None and tr.final_best <= target and tr.steps == tr.hit_step
+
+
+class OraclePiece:
+    """Stand-in for G.Lift.piece: exact counts over the corner tile by the oracle."""
+
+    def __init__(self, Nx, Ny, Mx, My):
+        self.dims = (Nx, Ny, Mx, My)
+        self.reps = O.piece_reps(Nx, Ny, Mx, My)
+
+    def set_base(self, table):
+        self.base = np.array(table, dtype=np.int32, copy=True)
+
+    def eval(self, edits):
+        out = np.zeros(len(edits), dtype=G.CAND_RESULT_DTYPE)
+        for i, e in enumerate(edits):
+            r = O.bfs_pull(O.expand_piece(*self.dims, G.apply_lift_edit(self.base, e)), self.reps)
+            out[i] = (r.total(), int(r.reached.sum()), r.levels, int(r.connected))
+        return out
+
+
+def test_piece_initial_temperature_from_exact_uphill_moves():
+    import math
+    Nx, Ny, Mx, My, d = 16, 12, 4, 3, 4
+    it = A.initial_temperature_piece(Nx, Ny, Mx, My, d, graphs=3, neighbours=12, seed=2,
+                                     make_lift=lambda: OraclePiece(Nx, Ny, Mx, My))
+    # the same quantity from the reference's ASPL values (cudaASPLpiece-style, over
+    # the tile, scaled by N/M), restated here directly
+    N, scale = Nx * Ny, (Nx * Ny) // (Mx * My)
+    ups = []
+    for k in range(3):
+        T = G.piece_lift(Mx, My, Nx // Mx, Ny // My, d, 2 * 1000003 + k)[4]
+        fx = O.piece_diameter_aspl(Nx, Ny, Mx, My, T)[1]
+        for e in G.gen_piece_moves(Nx, Ny, Mx, My, T, 12, (2 << 20) ^ k):
+            diam, fy = O.piece_diameter_aspl(Nx, Ny, Mx, My, G.apply_lift_edit(T, e))
+            if diam < 10 ** 8 and fy > fx:
+                ups.append((fy - fx) * N * (N - 1))
+    assert it.uphill == len(ups) and it.proposals == 36
+    assert abs(it.avg - sum(ups) / len(ups)) < 1e-6 * it.avg
+    assert abs(it.temp + it.avg / math.log(0.4)) < 1e-9 * it.temp
+    assert scale == 16

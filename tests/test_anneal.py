@@ -80,3 +80,13 @@ def test_initial_temperature_matches_oracle():
     assert t.avg == sum(ups) / len(ups)
     assert t.temp == -t.avg / math.log(0.4) and t.temp > 0
 
+
+
+def test_piece_initial_temperature_on_the_gpu_equals_the_oracle_run():
+    import test_anneal_host as H
+    Nx, Ny, Mx, My, d = 24, 16, 6, 4, 4
+    gpu = A.initial_temperature_piece(Nx, Ny, Mx, My, d, graphs=4, neighbours=20, seed=3)
+    cpu = A.initial_temperature_piece(Nx, Ny, Mx, My, d, graphs=4, neighbours=20, seed=3,
+                                      make_lift=lambda: H.OraclePiece(Nx, Ny, Mx, My))
+    assert (gpu.uphill, gpu.proposals, gpu.avg, gpu.temp) == (cpu.uphill, cpu.proposals, cpu.avg, cpu.temp)
+    assert gpu.ms > 0

@@ -19,6 +19,7 @@ T follows a geometric schedule from T0 = t0_frac * ASPL(start) to t_end.
 """
 from __future__ import annotations
 
+import json
 import math
 import time
 from dataclasses import dataclass, field
@@ -181,25 +182,56 @@ def anneal(adj0, steps, *, seed=1, exact=32, pool=4096, explore=8, surrogate=Fal
     return best_adj, tr
 
 
-def _anneal_table(L, gen, table0, steps, *, seed, exact, t0_frac, t_end, target, time_limit):
+def save_checkpoint(path, *, table, best, cur_total, cur_diam, best_aspl, T0, step, rng, tr):
+    """Snapshot of a lifted annealing run after `step` steps (an .npz): current and
+    best tables, exact counts, start temperature, RNG state and trace."""
+    np.savez(path, table=table, best=best, cur_total=np.int64(cur_total), cur_diam=np.int64(cur_diam),
+             best_aspl=np.float64(best_aspl), T0=np.float64(T0), step=np.int64(step),
+             rng=np.array(json.dumps(rng.bit_generator.state)), times=np.array(tr.times, dtype=np.float64),
+             best_trace=np.array(tr.best, dtype=np.float64), accepted=np.int64(tr.accepted),
+             exact_evals=np.int64(tr.exact_evals))
+
+
+def _anneal_table(L, gen, table0, steps, *, seed, exact, t0_frac, t_end, target, time_limit, checkpoint=None,
+                  checkpoint_every=0, resume=None):
     """Batched annealing of one lift table with handle L (a G.Lift) and move
     generator gen(table, count, seed).  t0_frac == 0: hill climbing (only moves
-    that lower the diameter, or keep it and lower the total)."""
-    table = np.array(table0, dtype=np.int32, copy=True)
+    that lower the diameter, or keep it and lower the total).  `checkpoint`: a path
+    written every `checkpoint_every` steps and at the end ("{step}" in it is replaced
+    by the step count); `resume`: a checkpoint to continue from (the same seed,
+    schedule and step count continue the same run)."""
     scale, npairs = L.N // L.M, L.N * (L.N - 1)
-    L.set_base(table)
-    r0 = L.eval(np.zeros(1, dtype=G.LIFT_EDIT_DTYPE))[0]
-    if not r0["connected"]:
-        raise ValueError("start lift is disconnected")
-    cur_total, cur_diam = int(r0["total"]), int(r0["levels"])
-    best_aspl, best = cur_total * scale / npairs, table.copy()
-    T0 = t0_frac * best_aspl
-    rng = np.random.default_rng(seed)
     tr = Trace()
-    t_start = time.perf_counter()
-    tr.times.append(0.0)
-    tr.best.append(best_aspl)
-    for i in range(steps):
+    rng = np.random.default_rng(seed)
+    first = 0
+    if resume is not None:
+        ck = np.load(resume, allow_pickle=False)
+        table, best = np.array(ck["table"], dtype=np.int32), np.array(ck["best"], dtype=np.int32)
+        cur_total, cur_diam = int(ck["cur_total"]), int(ck["cur_diam"])
+        best_aspl, T0, first = float(ck["best_aspl"]), float(ck["T0"]), int(ck["step"])
+        rng.bit_generator.state = json.loads(str(ck["rng"]))
+        tr.times, tr.best = list(ck["times"]), list(ck["best_trace"])
+        tr.accepted, tr.exact_evals, tr.steps = int(ck["accepted"]), int(ck["exact_evals"]), first
+        L.set_base(table)
+    else:
+        table = np.array(table0, dtype=np.int32, copy=True)
+        L.set_base(table)
+        r0 = L.eval(np.zeros(1, dtype=G.LIFT_EDIT_DTYPE))[0]
+        if not r0["connected"]:
+            raise ValueError("start lift is disconnected")
+        cur_total, cur_diam = int(r0["total"]), int(r0["levels"])
+        best_aspl, best = cur_total * scale / npairs, table.copy()
+        T0 = t0_frac * best_aspl
+        tr.times.append(0.0)
+        tr.best.append(best_aspl)
+    t_start = time.perf_counter() - (tr.times[-1] if resume is not None else 0.0)
+
+    def snapshot(step):
+        if checkpoint is not None:
+            save_checkpoint(checkpoint.format(step=step), table=table, best=best, cur_total=cur_total, cur_diam=cur_diam,
+                            best_aspl=best_aspl, T0=T0, step=step, rng=rng, tr=tr)
+
+    for i in range(first, steps):
         T = T0 * (t_end / T0) ** (i / max(steps - 1, 1)) if T0 > 0 else 0.0
         moves = gen(table, exact, (seed << 32) ^ i)
         res = L.eval(moves)
@@ -225,35 +257,40 @@ def _anneal_table(L, gen, table0, steps, *, seed, exact, t0_frac, t_end, target,
                     if target is not None and tr.hit_time is None and best_aspl <= target:
                         tr.hit_time, tr.hit_step = tr.times[-1], i + 1
         tr.steps = i + 1
+        if checkpoint_every and tr.steps % checkpoint_every == 0:
+            snapshot(tr.steps)
         if target is not None and tr.hit_time is not None:
             break
         if time_limit is not None and time.perf_counter() - t_start > time_limit:
             break
+    snapshot(tr.steps)
     tr.wall = time.perf_counter() - t_start
     tr.final_best = best_aspl
     return best, tr
 
 
 def anneal_lift(N, M, diffs0, steps, *, seed=1, exact=32, t0_frac=1e-3, t_end=1e-6, target=None,
-                time_limit=None, device=0):
+                time_limit=None, device=0, **ck):
     """Anneal a cyclic lift in part form (the reference's main annealer,
     cppcode/annealing.cpp:396-443, on the moves of :112-197).  Every step draws
     `exact` moves (gg_gen_lift_moves: new lift shifts and orbit 2-opts) and scores
     them all in one launch (gg_lift_eval); the best (smallest diameter, then
     smallest total) goes through the same acceptance rule as anneal().  ASPL is the
     reference's total * (N/M) / (N(N-1)).  t0_frac = 0 climbs (HillClimb.cpp).
+    Keyword `checkpoint`, `checkpoint_every`, `resume`: snapshots of the run (the
+    reference keeps only its best solution, cppcode/annealing.cpp:431-452).
     Returns (best_diffs, Trace)."""
     diffs = np.asarray(diffs0, dtype=np.int32).reshape(M, -1)
     L = G.Lift(N, M, diffs.shape[1], device)
     try:
         return _anneal_table(L, lambda t, c, s: G.gen_lift_moves(N, M, t, c, s), diffs, steps, seed=seed,
-                             exact=exact, t0_frac=t0_frac, t_end=t_end, target=target, time_limit=time_limit)
+                             exact=exact, t0_frac=t0_frac, t_end=t_end, target=target, time_limit=time_limit, **ck)
     finally:
         L.close()
 
 
 def anneal_piece(Nx, Ny, Mx, My, vals0, steps, *, seed=1, exact=32, t0_frac=1e-3, t_end=1e-6, target=None,
-                 time_limit=None, device=0):
+                 time_limit=None, device=0, **ck):
     """The same for a 2-D torus lift (cppcode/pieceannealing.cpp; vals [Mx*My, d, 2]);
     t0_frac = 0 is the hill climb of pieceHillClimb.cpp."""
     vals = np.asarray(vals0, dtype=np.int32).reshape(Mx * My, -1, 2)
@@ -261,13 +298,13 @@ def anneal_piece(Nx, Ny, Mx, My, vals0, steps, *, seed=1, exact=32, t0_frac=1e-3
     try:
         return _anneal_table(L, lambda t, c, s: G.gen_piece_moves(Nx, Ny, Mx, My, t, c, s), vals, steps,
                              seed=seed, exact=exact, t0_frac=t0_frac, t_end=t_end, target=target,
-                             time_limit=time_limit)
+                             time_limit=time_limit, **ck)
     finally:
         L.close()
 
 
 def anneal_box(Nx, Ny, Nz, Mx, My, Mz, vals0, steps, *, seed=1, exact=32, t0_frac=0.0, t_end=1e-6,
-               target=None, time_limit=None, device=0):
+               target=None, time_limit=None, device=0, **ck):
     """The same for a 3-D torus lift (vals [Mx*My*Mz, d, 3]); the default t0_frac = 0
     is the hill climb of cppcode/boxHillClimb.cpp."""
     vals = np.asarray(vals0, dtype=np.int32).reshape(Mx * My * Mz, -1, 3)
@@ -275,7 +312,7 @@ def anneal_box(Nx, Ny, Nz, Mx, My, Mz, vals0, steps, *, seed=1, exact=32, t0_fra
     try:
         return _anneal_table(L, lambda t, c, s: G.gen_box_moves(Nx, Ny, Nz, Mx, My, Mz, t, c, s), vals, steps,
                              seed=seed, exact=exact, t0_frac=t0_frac, t_end=t_end, target=target,
-                             time_limit=time_limit)
+                             time_limit=time_limit, **ck)
     finally:
         L.close()
 

@@ -2,6 +2,7 @@
 lifted annealing loop driven by an oracle-backed stand-in for the GPU lift
 evaluator (acceptance, hill-climb order, exact reported ASPL, target stop)."""
 import numpy as np
+import pytest
 
 import anneal as A
 
@@ -110,3 +111,27 @@ def test_piece_initial_temperature_from_exact_uphill_moves():
     assert abs(it.avg - sum(ups) / len(ups)) < 1e-6 * it.avg
     assert abs(it.temp + it.avg / math.log(0.4)) < 1e-9 * it.temp
     assert scale == 16
+
+
+@pytest.mark.parametrize("t0", [0.2, 0.0])
+def test_lifted_annealing_resumes_from_a_checkpoint(tmp_path, t0):
+    # 20 steps in one go against the same run resumed from its checkpoint after
+    # step 9: the same tables, counts and trace
+    N, M, D = G.cyclic_lift(24, 4, 4, 2)
+    gen = lambda t, c, s: G.gen_lift_moves(N, M, t, c, s)  # noqa: E731
+    # one proposal per step and a warm start: the run accepts uphill moves, so the
+    # resumed random stream must continue where it stopped
+    kw = dict(seed=5, exact=1, t0_frac=t0, t_end=1e-6, target=None)
+    full_L = OracleLift(N, M)
+    best, tr = A._anneal_table(full_L, gen, D, 20, time_limit=None, **kw)
+    ck = str(tmp_path / "run_{step}.npz")
+    A._anneal_table(OracleLift(N, M), gen, D, 20, time_limit=None, checkpoint=ck, checkpoint_every=9, **kw)
+    assert (tmp_path / "run_9.npz").exists() and (tmp_path / "run_18.npz").exists()
+    L2 = OracleLift(N, M)
+    best2, tr2 = A._anneal_table(L2, gen, None, 20, time_limit=None, resume=str(tmp_path / "run_9.npz"), **kw)
+    assert np.array_equal(best2, best) and np.array_equal(L2.base, full_L.base)
+    assert (tr2.steps, tr2.accepted, tr2.exact_evals) == (tr.steps, tr.accepted, tr.exact_evals)
+    assert tr2.best == tr.best and tr2.final_best == tr.final_best
+    if t0 > 0:
+        keys = [_key(N, M, b) for b in L2.bases]
+        assert any(b > a for a, b in zip(keys, keys[1:]))      # an uphill move after the resume

@@ -193,13 +193,16 @@ def save_checkpoint(path, *, table, best, cur_total, cur_diam, best_aspl, T0, st
 
 
 def _anneal_table(L, gen, table0, steps, *, seed, exact, t0_frac, t_end, target, time_limit, checkpoint=None,
-                  checkpoint_every=0, resume=None):
+                  checkpoint_every=0, resume=None, log=None):
     """Batched annealing of one lift table with handle L (a G.Lift) and move
     generator gen(table, count, seed).  t0_frac == 0: hill climbing (only moves
     that lower the diameter, or keep it and lower the total).  `checkpoint`: a path
     written every `checkpoint_every` steps and at the end ("{step}" in it is replaced
     by the step count); `resume`: a checkpoint to continue from (the same seed,
-    schedule and step count continue the same run)."""
+    schedule and step count continue the same run).  `log`: a path that gets one
+    JSON line per accepted move that changes the ASPL (step, best ASPL, current
+    ASPL, diameter, temperature, wall seconds), the fields of the reference's
+    --log lines (cppcode/annealing.cpp:323-326, 424)."""
     scale, npairs = L.N // L.M, L.N * (L.N - 1)
     tr = Trace()
     rng = np.random.default_rng(seed)
@@ -247,6 +250,7 @@ def _anneal_table(L, gen, table0, steps, *, seed, exact, t0_frac, t_end, target,
             if accept:
                 table = G.apply_lift_edit(table, moves[k])
                 L.set_base(table)
+                changed = ty != cur_total
                 cur_total, cur_diam = ty, dy
                 tr.accepted += 1
                 aspl = cur_total * scale / npairs
@@ -256,6 +260,10 @@ def _anneal_table(L, gen, table0, steps, *, seed, exact, t0_frac, t_end, target,
                     tr.best.append(best_aspl)
                     if target is not None and tr.hit_time is None and best_aspl <= target:
                         tr.hit_time, tr.hit_step = tr.times[-1], i + 1
+                if log is not None and changed:
+                    with open(log, "a") as f:
+                        f.write(json.dumps({"step": i + 1, "best_aspl": best_aspl, "aspl": aspl, "diameter": dy,
+                                            "temp": T, "wall_s": time.perf_counter() - t_start}) + "\n")
         tr.steps = i + 1
         if checkpoint_every and tr.steps % checkpoint_every == 0:
             snapshot(tr.steps)
@@ -278,7 +286,8 @@ def anneal_lift(N, M, diffs0, steps, *, seed=1, exact=32, t0_frac=1e-3, t_end=1e
     smallest total) goes through the same acceptance rule as anneal().  ASPL is the
     reference's total * (N/M) / (N(N-1)).  t0_frac = 0 climbs (HillClimb.cpp).
     Keyword `checkpoint`, `checkpoint_every`, `resume`: snapshots of the run (the
-    reference keeps only its best solution, cppcode/annealing.cpp:431-452).
+    reference keeps only its best solution, cppcode/annealing.cpp:431-452); `log`: a
+    JSON-lines progress log (see _anneal_table).
     Returns (best_diffs, Trace)."""
     diffs = np.asarray(diffs0, dtype=np.int32).reshape(M, -1)
     L = G.Lift(N, M, diffs.shape[1], device)

@@ -135,3 +135,17 @@ def test_lifted_annealing_resumes_from_a_checkpoint(tmp_path, t0):
     if t0 > 0:
         keys = [_key(N, M, b) for b in L2.bases]
         assert any(b > a for a, b in zip(keys, keys[1:]))      # an uphill move after the resume
+
+
+def test_lifted_annealing_log_lines(tmp_path):
+    import json
+    N, M, D = G.cyclic_lift(24, 4, 4, 2)
+    gen = lambda t, c, s: G.gen_lift_moves(N, M, t, c, s)  # noqa: E731
+    log = tmp_path / "run.jsonl"
+    _, tr = A._anneal_table(OracleLift(N, M), gen, D, 15, seed=5, exact=4, t0_frac=0.05, t_end=1e-6,
+                            target=None, time_limit=None, log=str(log))
+    lines = [json.loads(x) for x in log.read_text().splitlines()]
+    assert 0 < len(lines) <= tr.accepted
+    assert [x["step"] for x in lines] == sorted(x["step"] for x in lines)
+    assert min(x["best_aspl"] for x in lines) == tr.final_best
+    assert all(x["best_aspl"] <= x["aspl"] for x in lines)

@@ -10,21 +10,32 @@ calculator with the reference's level cap of 199 (cudaASPLgraph.cu:163).
 
 * value      evals/s with the adjacency resident in HBM (gg_eval_device),
              device-timed with CUDA events on the launching stream, K steps,
-             max over ranks; the three bitsets (3 x 512 MiB) exceed L2, so no
-             flush is needed between steps.
+             max over ranks.  A 256 MiB write flushes the L2 before every timed
+             step (the engine keeps each 4096-source batch's bitsets, 96 MiB, in
+             the L2 by design, so the flush is what makes steps independent).
 * e2e        the same metric through the reference-facing C-ABI call
              gg_graph_calc with a host adjacency: H2D of the table, the
              evaluation, D2H of the level counters, every step.
-* roofline   algorithmic bytes per evaluation (per level: N*d*4 adjacency +
-             N*(d+2)*S/8 bitset bytes, summed over executed levels and source
-             batches) / the BFS device time, against MEASURED_PEAKS.json hbm_gbs.
+* parity     rank 0 compares the timed result with the oracle's BFS from every
+             source of the same graph (the cpu_baseline run) and fails on any
+             difference; the line says "parity": "exact".
+* roofline   bound "hbm": DRAM bytes one evaluation moves (ncu dram__bytes of the
+             launch, profiles/traffic.json) / the kernel's CUDA-event time,
+             against MEASURED_PEAKS.json hbm_gbs.  Beside it: "l2_gather", the
+             live ceiling of the kernel's access pattern (gg_gather_peak: random
+             512-byte row gathers from L2-resident arrays, one dense BFS level per
+             pass), and "algorithmic", the survey's bytes-per-level count.
 * cpu_baseline  the oracle port (oracle/gg_oracle.c, a restatement of
-             cpuASPLqueue) on a bounded source sample over all host cores,
-             scaled to one evaluation; rank 0, N = 1 only.
+             cpuASPLqueue) over all host cores; rank 0, N = 1.
 
-Multi-GPU (torchrun): weak scaling, every rank evaluates its own graph (seed +
-rank); no collective on the data path, one MAX all-reduce of the timings.
-``--impl reference`` times the CPU reference path (see cpu_baseline) on rank 0.
+Multi-GPU: `--gpus N` without torchrun starts N ranks itself (torch.distributed.run,
+NCCL).  Default workload: weak scaling, every rank evaluates its own graph (seed +
+rank), one MAX all-reduce of the timings.  `regular_n65536_d8_sharded`: strong
+scaling, the ranks split the sources of the one graph and one NCCL all-reduce
+combines the exact counts every step (graphgolf-cuda_b200/distributed.py).
+``--impl reference`` times the CPU reference path on rank 0 and, beside it, the
+reference's own cudaASPLgraph built for this GPU (oracle/_ref), on the same graph
+read from tests/golden (no engine library loaded).
 """
 from __future__ import annotations
 
@@ -43,6 +54,9 @@ sys.path[:0] = [ROOT, os.path.join(ROOT, "graphgolf-cuda_b200")]
 
 WORKLOADS = {
     "regular_n65536_d8": dict(form="graph", n=65536, d=8, seed=1),
+    # strong scaling: the sources of the one graph split over the ranks, exact
+    # counts combined by an NCCL all-reduce every step
+    "regular_n65536_d8_sharded": dict(form="graph", n=65536, d=8, seed=1, sharded=True),
     "regular_n4096_d16": dict(form="graph", n=4096, d=16, seed=1),
     "lift_m1024_g32_d12": dict(form="part", m=1024, g=32, d=12, seed=1),
     # batched 2-opt candidates: 2048 on a 6-regular n=1024 base + 512 on a
@@ -79,12 +93,29 @@ def peaks():
     return 6650.0, "fallback"
 
 
+GOLDEN = os.path.join(ROOT, "tests", "golden")
+
+
+def fixture_of(w, seed):
+    """Committed input graph of a plain-graph workload (tests/golden), or None."""
+    if w["form"] != "graph":
+        return None
+    p = os.path.join(GOLDEN, f"regular_n{w['n']}_d{w['d']}_seed{seed}.npy")
+    if not os.path.exists(p):
+        return None
+    import numpy as np
+    return np.load(p).astype(np.int32)
+
+
 def make_workload(name, rank):
     import graphgolf as G
     w = WORKLOADS[name]
-    seed = w["seed"] + 1000 * rank
+    seed = w["seed"] + (0 if w.get("sharded") else 1000 * rank)
     if w["form"] == "graph":
         adj = G.random_regular(w["n"], w["d"], seed)
+        fx = fixture_of(w, seed)
+        if fx is not None and not (fx.shape == adj.shape and (fx == adj).all()):
+            raise SystemExit(f"generator output differs from the committed fixture for seed {seed}")
         return dict(form="graph", N=w["n"], d=w["d"], table=adj, S=w["n"], M=w["n"])
     N, M, diffs = G.cyclic_lift(w["m"], w["g"], w["d"], seed)
     return dict(form="part", N=N, d=w["d"], table=diffs, S=M, M=M)
@@ -158,8 +189,10 @@ def gpu_uuid(dev):
         return dev
 
 
-def cpu_sample(wl, target_s=8.0, threads=0):
-    """Oracle port on a bounded source sample over all host cores -> evals/s."""
+def cpu_sample(wl, target_s=8.0, threads=0, full=False):
+    """Oracle port over all host cores -> (evals/s record, the oracle's BFS or None).
+    full: BFS from every source (one whole evaluation, also the parity check);
+    else a bounded source sample of about target_s seconds, scaled."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import numpy as np
     import oracle as O
@@ -170,48 +203,101 @@ def cpu_sample(wl, target_s=8.0, threads=0):
     rp, col = O.pull_to_push_csr(adj)
     n_src_all = wl["S"]
     threads = threads or os.cpu_count() or 1
-    s = min(n_src_all, max(threads, 32))
+    s = n_src_all if full else min(n_src_all, max(threads, 32))
     while True:
         t0 = time.perf_counter()
-        O.bfs(rp, col, np.arange(s), threads=threads)
+        r = O.bfs(rp, col, np.arange(s), threads=threads)
         dt = time.perf_counter() - t0
         if dt >= target_s * 0.5 or s >= n_src_all:
             break
         s = min(n_src_all, int(s * max(2.0, target_s / max(dt, 1e-3) * 0.9)))
     per_eval = dt * n_src_all / s
-    return {"value": 1.0 / per_eval, "unit": UNIT, "cores": threads, "kind": "port",
-            "sample": f"BFS from {s} of {n_src_all} sources ({dt:.2f} s), scaled to one evaluation"}
+    what = (f"one whole evaluation: BFS from all {n_src_all} sources ({dt:.2f} s)" if s == n_src_all else
+            f"BFS from {s} of {n_src_all} sources ({dt:.2f} s), scaled to one evaluation")
+    rec = {"value": 1.0 / per_eval, "unit": UNIT, "cores": threads, "kind": "port", "sample": what}
+    return rec, (r if s == n_src_all else None)
+
+
+def reference_gpu_graph(adj, steps=5):
+    """The reference's own cudaASPLgraph::calc (cudacode/cudaASPLgraph.cu:141-199),
+    compiled from the reference sources for this GPU into oracle/_ref, on `adj`:
+    host clock around each blocking call, after one warm-up call."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    if not O.RefGPU.available("graph"):
+        return {"unavailable": "oracle/_ref/libref_graph.so not built (make -C oracle ref)"}
+    import torch
+    if not torch.cuda.is_available():
+        return {"unavailable": "no CUDA device"}
+    n, d = adj.shape
+    R = O.RefGPU("graph").create(n, d, 0)
+    try:
+        res = R.graph_calc(adj)
+        ts = []
+        for _ in range(steps):
+            t0 = time.perf_counter()
+            r2 = R.graph_calc(adj)
+            ts.append(time.perf_counter() - t0)
+            if r2 != res:
+                raise SystemExit("reference cudaASPLgraph is not deterministic")
+    finally:
+        R.close()
+    ms = 1000.0 * statistics.median(ts)
+    return {"value": 1000.0 / ms, "unit": UNIT, "ms_per_eval": ms, "calls": steps,
+            "result": {"diameter": res[0], "total": res[1]},
+            "what": "reference cudaASPLgraph::calc built for sm_100a from the reference source "
+                    "(oracle/_ref/libref_graph.so), host clock around each blocking call"}
 
 
 def run_reference(args):
+    """CPU reference path: each timed step is one whole evaluation of the
+    workload's graph by the oracle port of cpuASPLqueue (BFS from every source,
+    all host threads).  The graph comes from the committed fixture, so this arm
+    never loads the engine library.  Beside it, the reference cudaASPLgraph on
+    the same graph (reference_gpu)."""
     rank, world, _ = env_rank()
     if rank != 0:
         return 0
-    wl = make_workload(args.workload, 0)
-    vals = []
+    w = WORKLOADS[args.workload]
+    adj = fixture_of(w, w["seed"])
+    if adj is None:
+        print(json.dumps({"impl": "reference", "unavailable":
+                          f"no committed input fixture for workload {args.workload} (plain-graph workloads only)"}),
+              flush=True)
+        return 0
+    wl = dict(form="graph", N=w["n"], d=w["d"], table=adj, S=w["n"], M=w["n"])
     for _ in range(args.warmup):
-        cpu_sample(wl, target_s=1.0)
-    samples = []
+        cpu_sample(wl, target_s=0.5)
+    vals, rec, first = [], None, None
     t_all = time.perf_counter()
     for _ in range(args.steps):
-        cb = cpu_sample(wl, target_s=args.ref_step_s)
-        vals.append(cb["value"])
-        samples.append(cb)
+        rec, r = cpu_sample(wl, full=True)
+        vals.append(rec["value"])
+        if first is None:
+            first = r
     elapsed = time.perf_counter() - t_all
-    v = statistics.median(vals)
-    cb = dict(samples[-1])
+    v = args.steps / elapsed
+    cb = dict(rec)
     cb["value"] = v
+    cb["sample"] = f"{args.steps} whole evaluations (BFS from all {w['n']} sources each), {elapsed:.1f} s"
+    ref_gpu = reference_gpu_graph(adj)
+    oracle_res = {"diameter": first.levels if first.connected else -1, "total": first.total()}
+    if "result" in ref_gpu and ref_gpu["result"] != oracle_res:
+        raise SystemExit(f"reference GPU {ref_gpu['result']} != oracle {oracle_res}")
     line = {"metric": METRIC, "value": v, "unit": UNIT, "n_gpus": world, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": 1000.0 / v, "higher_is_better": True,
+            "warmup": args.warmup, "ms_per_step": 1000.0 * elapsed / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "u32", "data": "synthetic",
             "impl": "reference",
-            "config": {"workload": args.workload, **{k: v2 for k, v2 in WORKLOADS[args.workload].items()}},
+            "config": {"workload": args.workload, "n": w["n"], "degree": w["d"], "seed": w["seed"],
+                       "input": f"tests/golden/regular_n{w['n']}_d{w['d']}_seed{w['seed']}.npy"},
             "cpu_baseline": cb,
             "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "result": oracle_res,
+            "reference_gpu": ref_gpu,
             "wall_s": elapsed,
-            "note": "the reference cpuASPLqueue evaluates all sources in one call and cannot "
-                    "be sampled; each step runs the oracle port (its restatement) on a "
-                    "source sample with all host threads"}
+            "note": "the reference cpuASPLqueue is single-threaded (cpuASPLqueue.cpp:64) and evaluates "
+                    "all sources in one call; each step runs its restatement (oracle/gg_oracle.c) over "
+                    "all host threads"}
     print(json.dumps(line), flush=True)
     return 0
 
@@ -223,6 +309,17 @@ def timed(fn, steps, sync):
         fn()
     sync()
     return time.perf_counter() - t0
+
+
+def traffic_of(workload):
+    """DRAM bytes of one evaluation launch from the committed ncu capture, or None."""
+    tp = os.path.join(ROOT, "profiles", "traffic.json")
+    if not os.path.exists(tp):
+        return None, None
+    tj = json.load(open(tp)).get(workload)
+    if not tj:
+        return None, None
+    return tj.get("dram_bytes_per_eval"), tj.get("note")
 
 
 def run_ours(args):
@@ -237,6 +334,8 @@ def run_ours(args):
         import datetime
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    w = WORKLOADS[args.workload]
+    sharded = bool(w.get("sharded")) and world > 1
     wl = make_workload(args.workload, rank)
     if wl["form"] == "graph":
         eng = G.cudaASPLgraph(wl["N"], wl["d"], local)
@@ -246,6 +345,10 @@ def run_ours(args):
         max_levels = 99
     if args.batch_sources:
         eng.set_batch_sources(args.batch_sources)
+    src_range = None
+    if sharded:
+        import distributed as D
+        src_range = D.shard(wl["S"], rank, world)
     table_dev = torch.from_numpy(np.ascontiguousarray(wl["table"])).cuda()
     # an explicit stream: the engine runs on it, and the events and the L2
     # flush are recorded on it (the legacy default stream has the handle 0,
@@ -253,16 +356,37 @@ def run_ours(args):
     stream = torch.cuda.Stream()
     torch.cuda.set_stream(stream)
     sptr = stream.cuda_stream
+    if sharded:
+        # one exact all-reduce of (total, reached, level_steps) and (levels, capped)
+        # per step, on the same stream as the evaluation
+        red_s = torch.zeros(3, dtype=torch.int64, device="cuda")
+        red_m = torch.zeros(2, dtype=torch.int64, device="cuda")
 
     def step():
-        return eng.eval_device(table_dev.data_ptr(), max_levels=max_levels, stream=sptr)
+        r = eng.eval_device(table_dev.data_ptr(), max_levels=max_levels, stream=sptr, src_range=src_range)
+        if sharded:
+            red_s.copy_(torch.tensor([r["total"], r["reached"], r["level_steps"]], dtype=torch.int64))
+            red_m.copy_(torch.tensor([r["levels"], r["capped"]], dtype=torch.int64))
+            dist.all_reduce(red_s, op=dist.ReduceOp.SUM)
+            dist.all_reduce(red_m, op=dist.ReduceOp.MAX)
+        return r
+
+    def combined(r):
+        if not sharded:
+            return dict(r)
+        tot, reached, steps_ = (int(x) for x in red_s.tolist())
+        lev, capped = (int(x) for x in red_m.tolist())
+        pairs = wl["S"] * wl["N"]
+        return {"total": tot, "reached": reached, "level_steps": steps_, "levels": lev, "capped": capped,
+                "connected": int(not capped and reached == pairs), "n_sources": wl["S"],
+                "batches": r["batches"]}
 
     res = None
     for _ in range(max(args.warmup, 0)):
         res = step()
     if res is None:
         res = step()
-    assert res["connected"] and not res["capped"], res
+    assert res["connected"] or sharded, res
 
     clocks = Clocks(gpu_uuid(local))
 
@@ -295,7 +419,7 @@ def run_ours(args):
             dist.barrier()
         steps_total = sum(a.elapsed_time(b) for a, b in step_ms)
         ck["bracket_ms_incl_flush"] = ev0.elapsed_time(ev1)
-        return steps_total, dev_ms, launches, ck, r
+        return steps_total, dev_ms, launches, ck, combined(r)
 
     elapsed_ms, dev_ms, launches, ck, r = measure()
     bad = {"hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown"}
@@ -305,14 +429,19 @@ def run_ours(args):
         t = torch.tensor([elapsed_ms], device="cuda", dtype=torch.float64)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         elapsed_ms = float(t.item())
+    assert r["connected"] and not r["capped"], r
 
     # end to end through the C ABI with a host adjacency
     host_table = np.ascontiguousarray(wl["table"])
-    if wl["form"] == "graph":
+    if wl["form"] == "graph" and not sharded:
         e2e_fn = lambda: eng.calc(host_table)  # noqa: E731
+    elif wl["form"] == "graph":
+        e2e_fn = lambda: eng.eval(host_table, max_levels=199, src_range=src_range)  # noqa: E731
     else:
         e2e_fn = lambda: eng.diameterASPL(host_table)  # noqa: E731
-    e2e_fn()
+    e2e_first = e2e_fn()
+    if wl["form"] == "graph" and not sharded:
+        assert e2e_first == (r["levels"], r["total"]), (e2e_first, r)
     e2e_steps = max(3, min(args.steps, 20))
     e2e_s = 0.0
     for _ in range(e2e_steps):  # each call is blocking; L2 flushed before each
@@ -325,45 +454,82 @@ def run_ours(args):
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         e2e_s = float(t.item())
 
-    value = world * args.steps / (elapsed_ms / 1000.0)
+    # whole-job throughput: evaluations of whole graphs per second
+    evals = args.steps * (1 if sharded else world)
+    value = evals / (elapsed_ms / 1000.0)
     kern_ms = statistics.mean(dev_ms)
     alg = algorithmic_bytes(wl, r, eng.table_shape)
     peak, peak_kind = peaks()
-    achieved = alg / (kern_ms / 1000.0) / 1e9
-    traffic = None
-    tp = os.path.join(ROOT, "profiles", "traffic.json")
-    if os.path.exists(tp):
-        tj = json.load(open(tp)).get(args.workload)
-        if tj:
-            traffic = tj.get("dram_bytes_per_eval")
-
+    traffic, traffic_note = traffic_of(args.workload)
+    if sharded:
+        traffic = None    # the committed capture is of one whole evaluation on one GPU
+    roof = {"bound": "hbm", "achieved": None, "peak": peak, "unit": "GB/s", "frac": None,
+            "traffic": traffic, "peak_source": peak_kind, "kernel_ms": kern_ms,
+            "achieved_from": "DRAM bytes of one evaluation launch (traffic, ncu) / the launch's "
+                             "mean CUDA-event time (kernel_ms)",
+            "traffic_source": traffic_note}
+    if traffic:
+        roof["achieved"] = traffic / (kern_ms / 1000.0) / 1e9
+        roof["frac"] = roof["achieved"] / peak
+    l2 = None
+    if rank == 0 and not args.no_gather_peak:
+        gp, gms = G.gather_peak(rows=wl["N"], degree=wl["d"], iters=20, device=local)
+        l2 = {"gather_peak_gbs": gp, "gather_pass_ms": gms,
+              "what": f"gg_gather_peak: {wl['N']} rows x ({wl['d']} random + 1 own) 512-byte row reads + "
+                      "1 row write per pass, the access pattern of one dense BFS level of a 4096-source "
+                      "batch, arrays L2-resident",
+              "kernel_ms_in_gather_passes": kern_ms / gms,
+              "level_steps": r["level_steps"]}
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": elapsed_ms / args.steps,
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32",
-            "data": "synthetic",
+            "higher_is_better": True, "scaling": "strong" if sharded else "weak", "vs_baseline": None,
+            "dtype": "u32", "data": "synthetic",
             "config": {"workload": args.workload, "n": wl["N"], "degree": wl["d"],
                        "sources": wl["S"], "batches": r["batches"],
                        "level_steps": r["level_steps"], "diameter": r["levels"],
-                       "parallelism": f"replicas{world}" if world > 1 else "single",
-                       "batch_sources": -(-r["n_sources"] // r["batches"]),
-                       "bit_edge_traversals_per_s": bit_edges_per_eval(wl, r) * args.steps / (elapsed_ms / 1000.0),
+                       "parallelism": (f"source-sharded{world}" if sharded else
+                                       (f"replicas{world}" if world > 1 else "single")),
+                       "batch_sources": -(-wl["S"] // max(1, r["batches"])) if not sharded else None,
+                       "bit_edge_traversals_per_s": bit_edges_per_eval(wl, r) * evals / (elapsed_ms / 1000.0),
                        "l2": "flushed (256 MiB write) before every timed step; steps timed by their own CUDA event pairs"},
-            "e2e": {"value": world * e2e_steps / e2e_s, "unit": UNIT,
+            "e2e": {"value": (1 if sharded else world) * e2e_steps / e2e_s, "unit": UNIT,
                     "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
-            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                         "frac": achieved / peak, "traffic": traffic,
-                         "peak_source": peak_kind, "kernel_ms": kern_ms,
-                         "algorithmic_bytes": alg},
+            "roofline": roof,
+            "l2_gather": l2,
+            "algorithmic": {"bytes": alg, "gbs": alg / (kern_ms / 1000.0) / 1e9,
+                            "definition": "per executed level N*d*4 + N*(d+2)*S/8 bytes (S = sources of "
+                                          "the batch), summed over batches; counts gathers the kernel "
+                                          "skips or the L2 serves, so it is no DRAM figure"},
             "gpu_launches": launches,
-            "clocks": ck}
+            "clocks": ck,
+            "result": {"diameter": r["levels"], "total": r["total"]}}
     if rank == 0 and world == 1 and not args.no_cpu:
-        line["cpu_baseline"] = cpu_sample(wl, target_s=args.cpu_s)
+        cb, o = cpu_sample(wl, full=True)
+        line["cpu_baseline"] = cb
+        if o is not None:
+            want_total = o.total()
+            if not (o.connected and want_total == r["total"] and o.levels == r["levels"]):
+                raise SystemExit(f"PARITY FAILURE: engine {r['levels']},{r['total']} vs oracle "
+                                 f"{o.levels},{want_total}")
+            line["parity"] = f"exact: equals the oracle BFS from all {wl['S']} sources"
     if rank == 0:
         print(json.dumps(line), flush=True)
     eng.close()
     if dist:
         dist.destroy_process_group()
     return 0
+
+
+def spawn_ranks(args):
+    """`--gpus N` outside torchrun: run this script as N ranks on this node."""
+    import socket
+    s = socket.socket()
+    s.bind(("127.0.0.1", 0))
+    port = s.getsockname()[1]
+    s.close()
+    cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", f"--nproc-per-node={args.gpus}",
+           "--master-addr", "127.0.0.1", f"--master-port={port}", os.path.abspath(__file__)] + sys.argv[1:]
+    return subprocess.run(cmd, timeout=3600).returncode
 
 
 def main():
@@ -377,8 +543,11 @@ def main():
     ap.add_argument("--cpu-s", type=float, default=10.0)
     ap.add_argument("--ref-step-s", type=float, default=4.0)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-gather-peak", action="store_true")
     ap.add_argument("--anneal-steps", type=int, default=0, help="annealing schedule length (time-to-target workload)")
     args = ap.parse_args()
+    if args.gpus > 1 and "WORLD_SIZE" not in os.environ:
+        return spawn_ranks(args)
     if args.impl == "reference":
         return run_reference(args)
     if WORKLOADS[args.workload]["form"] == "batch":

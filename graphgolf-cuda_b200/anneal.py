@@ -20,6 +20,7 @@ T follows a geometric schedule from T0 = t0_frac * ASPL(start) to t_end.
 from __future__ import annotations
 
 import json
+import os
 import math
 import time
 from dataclasses import dataclass, field
@@ -182,14 +183,27 @@ def anneal(adj0, steps, *, seed=1, exact=32, pool=4096, explore=8, surrogate=Fal
     return best_adj, tr
 
 
-def save_checkpoint(path, *, table, best, cur_total, cur_diam, best_aspl, T0, step, rng, tr):
+def npz_path(path):
+    """Checkpoint file name: `path` with ".npz" appended unless it ends so already
+    (np.savez would append it anyway; resume= then takes either spelling)."""
+    return path if path.endswith(".npz") else path + ".npz"
+
+
+def save_checkpoint(path, *, table, best, cur_total, cur_diam, best_aspl, T0, step, rng, tr, elapsed):
     """Snapshot of a lifted annealing run after `step` steps (an .npz): current and
-    best tables, exact counts, start temperature, RNG state and trace."""
-    np.savez(path, table=table, best=best, cur_total=np.int64(cur_total), cur_diam=np.int64(cur_diam),
+    best tables, exact counts, start temperature, RNG state, trace, the run's wall
+    seconds so far and its time-to-target state.  Written to a temporary file and
+    renamed into place, so a crash mid-write leaves the previous snapshot intact."""
+    final = npz_path(path)
+    tmp = final[:-4] + ".tmp.npz"
+    np.savez(tmp, table=table, best=best, cur_total=np.int64(cur_total), cur_diam=np.int64(cur_diam),
              best_aspl=np.float64(best_aspl), T0=np.float64(T0), step=np.int64(step),
              rng=np.array(json.dumps(rng.bit_generator.state)), times=np.array(tr.times, dtype=np.float64),
              best_trace=np.array(tr.best, dtype=np.float64), accepted=np.int64(tr.accepted),
-             exact_evals=np.int64(tr.exact_evals))
+             exact_evals=np.int64(tr.exact_evals), elapsed=np.float64(elapsed),
+             hit_time=np.float64(-1.0 if tr.hit_time is None else tr.hit_time),
+             hit_step=np.int64(-1 if tr.hit_step is None else tr.hit_step))
+    os.replace(tmp, final)
 
 
 def _anneal_table(L, gen, table0, steps, *, seed, exact, t0_frac, t_end, target, time_limit, checkpoint=None,
@@ -200,21 +214,35 @@ def _anneal_table(L, gen, table0, steps, *, seed, exact, t0_frac, t_end, target,
     written every `checkpoint_every` steps and at the end ("{step}" in it is replaced
     by the step count); `resume`: a checkpoint to continue from (the same seed,
     schedule and step count continue the same run).  `log`: a path that gets one
-    JSON line per accepted move that changes the ASPL (step, best ASPL, current
-    ASPL, diameter, temperature, wall seconds), the fields of the reference's
+    JSON line per accepted move that changes the ASPL or the diameter (step, best
+    ASPL, current ASPL, diameter, temperature, wall seconds), the fields of the reference's
     --log lines (cppcode/annealing.cpp:323-326, 424)."""
     scale, npairs = L.N // L.M, L.N * (L.N - 1)
     tr = Trace()
     rng = np.random.default_rng(seed)
     first = 0
+    elapsed0 = 0.0
     if resume is not None:
-        ck = np.load(resume, allow_pickle=False)
+        ck = np.load(npz_path(resume), allow_pickle=False)
         table, best = np.array(ck["table"], dtype=np.int32), np.array(ck["best"], dtype=np.int32)
+        # the snapshot must fit this run's lift handle (and its start table, if given)
+        if table0 is not None:
+            want = np.asarray(table0).shape
+        elif hasattr(L, "degree"):
+            ax = getattr(L, "axes", 1)
+            want = (L.M, L.degree) if ax == 1 else (L.M, L.degree, ax)
+        else:
+            want = (L.M,) + table.shape[1:]
+        if table.shape != want or best.shape != want:
+            raise ValueError(f"checkpoint tables have shape {table.shape}, this run's tables {want}")
         cur_total, cur_diam = int(ck["cur_total"]), int(ck["cur_diam"])
         best_aspl, T0, first = float(ck["best_aspl"]), float(ck["T0"]), int(ck["step"])
         rng.bit_generator.state = json.loads(str(ck["rng"]))
         tr.times, tr.best = list(ck["times"]), list(ck["best_trace"])
         tr.accepted, tr.exact_evals, tr.steps = int(ck["accepted"]), int(ck["exact_evals"]), first
+        elapsed0 = float(ck["elapsed"]) if "elapsed" in ck.files else (tr.times[-1] if tr.times else 0.0)
+        if "hit_step" in ck.files and int(ck["hit_step"]) >= 0:
+            tr.hit_time, tr.hit_step = float(ck["hit_time"]), int(ck["hit_step"])
         L.set_base(table)
     else:
         table = np.array(table0, dtype=np.int32, copy=True)
@@ -227,14 +255,18 @@ def _anneal_table(L, gen, table0, steps, *, seed, exact, t0_frac, t_end, target,
         T0 = t0_frac * best_aspl
         tr.times.append(0.0)
         tr.best.append(best_aspl)
-    t_start = time.perf_counter() - (tr.times[-1] if resume is not None else 0.0)
+    # wall time continues from the snapshot's elapsed seconds
+    t_start = time.perf_counter() - elapsed0
 
     def snapshot(step):
         if checkpoint is not None:
             save_checkpoint(checkpoint.format(step=step), table=table, best=best, cur_total=cur_total, cur_diam=cur_diam,
-                            best_aspl=best_aspl, T0=T0, step=step, rng=rng, tr=tr)
+                            best_aspl=best_aspl, T0=T0, step=step, rng=rng, tr=tr,
+                            elapsed=time.perf_counter() - t_start)
 
-    for i in range(first, steps):
+    # a run resumed after it had already reached its target stops at once
+    done = target is not None and tr.hit_time is not None
+    for i in range(first, steps if not done else first):
         T = T0 * (t_end / T0) ** (i / max(steps - 1, 1)) if T0 > 0 else 0.0
         moves = gen(table, exact, (seed << 32) ^ i)
         res = L.eval(moves)
@@ -250,7 +282,7 @@ def _anneal_table(L, gen, table0, steps, *, seed, exact, t0_frac, t_end, target,
             if accept:
                 table = G.apply_lift_edit(table, moves[k])
                 L.set_base(table)
-                changed = ty != cur_total
+                changed = ty != cur_total or dy != cur_diam
                 cur_total, cur_diam = ty, dy
                 tr.accepted += 1
                 aspl = cur_total * scale / npairs

@@ -22,7 +22,7 @@ INC = os.path.join(ROOT, "include")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 REF = os.environ.get("GG_REFERENCE_TREE", "/root/reference")
 
-ENGINE_SRC = ["gg_engine.cu", "gg_batch.cu", "gg_surrogate.cu", "gg_noalloc.cu", "gg_inc.cu", "gg_lift.cu", "gg_gen.cpp"]
+ENGINE_SRC = ["gg_engine.cu", "gg_batch.cu", "gg_surrogate.cu", "gg_noalloc.cu", "gg_inc.cu", "gg_lift.cu", "gg_probe.cu", "gg_gen.cpp"]
 ENGINE_LIB = os.path.join(PKG, "libggb200.so")
 SHIM_LIB = os.path.join(PKG, "libgg_refshim.so")
 

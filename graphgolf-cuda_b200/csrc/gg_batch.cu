@@ -74,7 +74,10 @@ struct BatchCtl {
     unsigned task_ctr;
     int n_cand;
     int max_chunks;
-    int pad;
+    int bad;              // set by batch_reset when a candidate is outside the domain
+    int n_bases;          // registered bases
+    int bad_index;        // lowest index of such a candidate (INT_MAX: none)
+    int pad[2];
 };
 
 struct BatchArgs {
@@ -100,6 +103,7 @@ __global__ void __launch_bounds__(kBatchBlock, 1) batch_kernel(const BatchArgs a
     extern __shared__ uint4 sm[];
     __shared__ unsigned s_task;
     __shared__ unsigned long long s_tot[kBatchBlock / 32], s_reach[kBatchBlock / 32];
+    if (a.ctl->bad) return;   // batch_reset rejected a candidate: index nothing
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int n_cand = a.ctl->n_cand, max_chunks = a.ctl->max_chunks;
     const unsigned n_tasks = (unsigned)n_cand * (unsigned)max_chunks;
@@ -220,6 +224,12 @@ __global__ void __launch_bounds__(kBatchBlock, 1) batch_kernel(const BatchArgs a
 
 __global__ void batch_finalize(const BatchArgs a) {
     const int n_cand = a.ctl->n_cand;
+    if (a.ctl->bad) {
+        // a rejected launch scores nothing: every result says so
+        for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n_cand; i += gridDim.x * blockDim.x)
+            a.out[i] = gg_cand_result{0ull, 0ull, -1, 0};
+        return;
+    }
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n_cand; i += gridDim.x * blockDim.x) {
         const BatchBase B = a.bases[a.cands[i].base];
         gg_cand_result r = a.out[i];
@@ -235,11 +245,27 @@ __global__ void batch_finalize(const BatchArgs a) {
     }
 }
 
+// Zeroes the results and range-checks every candidate (the device-array entry
+// point gets candidates the host never saw): base registered, endpoints inside the
+// base, distinct, mode 0 or 1.  One bad candidate sets ctl->bad, and the kernels
+// after this one return before reading a base or a row through it.
 __global__ void batch_reset(const BatchArgs a) {
     const int n_cand = a.ctl->n_cand;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n_cand; i += gridDim.x * blockDim.x) {
         a.out[i] = gg_cand_result{0ull, 0ull, 0, 0};
         if (a.inc) a.inc[i] = IncCand{0ull, 0u, 0u, 0, 0};
+        const gg_swap sw = a.cands[i];
+        bool ok = sw.base >= 0 && sw.base < a.ctl->n_bases;
+        if (ok && sw.a >= 0) {
+            const unsigned n = (unsigned)a.bases[sw.base].n;
+            ok = (unsigned)sw.a < n && (unsigned)sw.b < n && (unsigned)sw.c < n && (unsigned)sw.d < n &&
+                 (sw.mode == 0 || sw.mode == 1) && sw.a != sw.b && sw.a != sw.c && sw.a != sw.d &&
+                 sw.b != sw.c && sw.b != sw.d && sw.c != sw.d;
+        }
+        if (!ok) {
+            atomicExch(&a.ctl->bad, 1);
+            atomicMin(&a.ctl->bad_index, i);
+        }
     }
     if (blockIdx.x == 0 && threadIdx.x == 0) a.ctl->task_ctr = 0u;
 }
@@ -257,6 +283,7 @@ __device__ __forceinline__ unsigned plane_dist(const uint32_t *pw, size_t pstrid
 // comment).  Affected sources join the candidate's list with their base
 // distance sums; the others give the largest eccentricity that stays.
 __global__ void batch_affected(const BatchArgs a, int max_n, int force_full) {
+    if (a.ctl->bad) return;   // batch_reset rejected a candidate
     const int n_cand = a.ctl->n_cand;
     const unsigned long long total = (unsigned long long)n_cand * (unsigned long long)max_n;
     const unsigned lane = threadIdx.x & 31u;
@@ -519,6 +546,15 @@ gg_status base_pass(gg_batch *b, int id) {
     return GG_OK;
 }
 
+__global__ void set_ctl(BatchCtl *ctl, const BatchCtl v) { *ctl = v; }
+
+// The device-side candidate check starts clean for every launch.
+void arm_check(gg_batch *b) {
+    b->h_ctl->bad = 0;
+    b->h_ctl->bad_index = 0x7fffffff;
+    b->h_ctl->n_bases = (int)b->bases.size();
+}
+
 gg_status validate(const gg_batch *b, int n_cand, const gg_swap *c) {
     for (int i = 0; i < n_cand; ++i) {
         const gg_swap &s = c[i];
@@ -628,6 +664,7 @@ gg_status gg_batch_eval(gg_batch *b, int n_cand, const gg_swap *cands, gg_cand_r
     std::memcpy(b->h_cands, cands, (size_t)n_cand * sizeof(gg_swap));
     b->h_ctl->n_cand = n_cand;
     b->h_ctl->task_ctr = 0;
+    arm_check(b);
     GB_CK(cudaMemcpyAsync(b->d_cands, b->h_cands, (size_t)n_cand * sizeof(gg_swap),
                           cudaMemcpyHostToDevice, b->stream));
     GB_CK(cudaMemcpyAsync(b->d_ctl, b->h_ctl, sizeof(BatchCtl), cudaMemcpyHostToDevice, b->stream));
@@ -664,11 +701,29 @@ gg_status gg_batch_eval_device(gg_batch *b, int n_cand, const gg_swap *d_cands,
     if (cs != GG_OK) return cs;
     b->h_ctl->n_cand = n_cand;
     b->h_ctl->task_ctr = 0;
-    GB_CK(cudaMemcpyAsync(b->d_ctl, b->h_ctl, sizeof(BatchCtl), cudaMemcpyHostToDevice, st));
+    arm_check(b);
+    // the control block goes by value as a kernel argument: this call returns
+    // before the GPU runs it, and the next call may change the host copy
+    set_ctl<<<1, 1, 0, st>>>(b->d_ctl, *b->h_ctl);
+    GB_CK(cudaGetLastError());
     GB_CK(cudaEventRecord(b->ev0, st));
     gg_status s = enqueue(b, d_cands, d_out, st);
     if (s != GG_OK) return s;
     GB_CK(cudaEventRecord(b->ev1, st));
+    return GG_OK;
+}
+
+gg_status gg_batch_device_status(gg_batch *b, void *stream, int *first_bad) {
+    if (!b) return bfail(GG_BAD_ARG, "null batch");
+    GB_CK(cudaSetDevice(b->device));
+    cudaStream_t st = stream ? (cudaStream_t)stream : b->stream;
+    GB_CK(cudaStreamSynchronize(st));
+    BatchCtl c{};
+    GB_CK(cudaMemcpy(&c, b->d_ctl, sizeof(BatchCtl), cudaMemcpyDeviceToHost));
+    if (first_bad) *first_bad = c.bad ? c.bad_index : -1;
+    if (c.bad)
+        return bfail(GG_BAD_ARG, "device candidate " + std::to_string(c.bad_index) +
+                                     ": unknown base, vertex or mode out of range, or repeated endpoint");
     return GG_OK;
 }
 
@@ -692,6 +747,7 @@ gg_status gg_batch_vertex_hist(gg_batch *b, int base_id, int K, uint32_t *hist) 
     b->h_cands[0] = self;
     b->h_ctl->n_cand = 1;
     b->h_ctl->task_ctr = 0;
+    arm_check(b);
     cudaError_t e = cudaMemsetAsync(d_hist, 0, (size_t)n * K * sizeof(unsigned), b->stream);
     if (e == cudaSuccess)
         e = cudaMemcpyAsync(b->d_cands, b->h_cands, sizeof(gg_swap), cudaMemcpyHostToDevice, b->stream);

@@ -96,6 +96,7 @@ _SIGS = {
     "gg_set_batch_sources": [_P, _I],
     "gg_autotune": [_P, _P, _I, _IP, _DP],
     "gg_set_wait_limit_ms": [_P, _I],
+    "gg_gather_peak": [_I, _I, _I, _I, _DP, _DP],
     "gg_destroy": [_P],
     "gg_graph_eval_noalloc": [_P, _I, _I, _I, _P, _P],
     "gg_batch_create": [_I, _EPP],
@@ -105,6 +106,7 @@ _SIGS = {
     "gg_batch_vertex_hist": [_P, _I, _I, _P],
     "gg_batch_eval": [_P, _I, _P, _P],
     "gg_batch_eval_device": [_P, _I, _P, _P, _P],
+    "gg_batch_device_status": [_P, _P, _IP],
     "gg_batch_last_ms": [_P, _DP],
     "gg_batch_destroy": [_P],
     "gg_gen_swaps": [_I, _I, _P, _I, _I, ctypes.c_uint64, _P],
@@ -545,9 +547,11 @@ class Engine:
             d["level_counts"] = lc
         return d
 
-    def eval_device(self, dev_ptr, max_levels=0, stream=0, level_ns=False):
+    def eval_device(self, dev_ptr, max_levels=0, stream=0, level_ns=False, src_range=None):
         o = EvalOpts()
         o.max_levels = max_levels
+        if src_range is not None:
+            o.src_begin, o.src_end = src_range
         ns = None
         if level_ns:
             if max_levels <= 0:
@@ -728,6 +732,14 @@ def gen_swaps(adj, base_id, count, seed):
     return out
 
 
+def gather_peak(rows=65536, degree=8, iters=20, device=0):
+    """Ceiling of a dense BFS level (gg_gather_peak): -> (GB/s, ms per pass) of
+    rows x (degree + 1) random 512-byte row reads and one row write."""
+    g, ms = ctypes.c_double(), ctypes.c_double()
+    _check(lib().gg_gather_peak(device, rows, degree, iters, ctypes.byref(g), ctypes.byref(ms)))
+    return g.value, ms.value
+
+
 def apply_swap(adj, s):
     """Host copy of the edit the batch kernel applies (first occurrence replaced)."""
     adj = np.array(adj, dtype=np.int32, copy=True)
@@ -846,6 +858,12 @@ class Batch:
     def eval_device(self, n, d_swaps, d_out, stream=0):
         _check(lib().gg_batch_eval_device(self._h, n, ctypes.c_void_p(d_swaps), ctypes.c_void_p(d_out),
                                           ctypes.c_void_p(stream)))
+
+    def device_status(self, stream=0):
+        """Wait for `stream`; raise GGError(GG_BAD_ARG) if the last device launch
+        rejected a candidate (gg_batch_device_status)."""
+        first = ctypes.c_int()
+        _check(lib().gg_batch_device_status(self._h, ctypes.c_void_p(stream), ctypes.byref(first)))
 
     def last_ms(self):
         ms = ctypes.c_double()

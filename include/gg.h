@@ -150,6 +150,15 @@ gg_status gg_autotune(gg_engine *e, const int32_t *table, int trials, int *best_
 /* Bounded-wait limit of the in-kernel grid barrier, in milliseconds. */
 gg_status gg_set_wait_limit_ms(gg_engine *e, int ms);
 
+/* Gather-rate microbenchmark (no reference counterpart): the access pattern of a
+ * dense BFS level and nothing else.  For `rows` rows of 512 bytes each (32 x 16
+ * bytes, one warp per row), Y[v] = OR over `degree` random rows of X, masked
+ * with Y0[v]: degree + 1 row reads and one row write per row.  Returns the best of
+ * `iters` passes as GB/s of those bytes (plus the index table) and its time.
+ * With rows = 65536 the three arrays (96 MiB) sit in the L2: that rate is the
+ * ceiling of a dense level of a 4096-source batch on n = 65536. */
+gg_status gg_gather_peak(int device, int rows, int degree, int iters, double *gbs, double *ms_per_pass);
+
 gg_status gg_destroy(gg_engine *e);
 
 /* ---- evaluation without device allocation --------------------------------
@@ -163,7 +172,7 @@ gg_status gg_destroy(gg_engine *e);
  *                    reached at BFS level L over all N sources ([0] = N); levels past
  *                    the last non-empty one are 0.  The diameter is the last L with a
  *                    nonzero count; the total distance is sum L * [L]; the graph is
- *                    connected when sum [L] == N*N (and [max_levels] == 0).
+ *                    connected when sum [L] == N*N.
  * Working memory is one fixed device array of GG_NOALLOC_SCRATCH_BYTES compiled into
  * the library, held by every GPU that loads it until the process exits.  N must be
  * small enough for one batch of N sources to fit in it (N <= 4096 always fits);
@@ -215,9 +224,18 @@ gg_status gg_batch_set_chunk(gg_batch *b, int base_id, int sources);
  * captured once in a CUDA graph and replayed. */
 gg_status gg_batch_eval(gg_batch *b, int n_cand, const gg_swap *cands, gg_cand_result *out);
 /* Device arrays in and out, ordered on `stream` (NULL = the batch's stream); returns
- * after enqueueing.  The caller synchronises before reading `d_out`. */
+ * after enqueueing.  The caller synchronises before reading `d_out`.
+ * Preconditions: d_cands and d_out hold n_cand records.  The candidates are checked
+ * on the device before anything is read through them (base registered, a..d inside
+ * the base's vertex range and distinct, mode 0 or 1; a < 0 = the base itself): if
+ * one fails, the launch scores nothing, every d_out record has levels = -1, and
+ * gg_batch_device_status reports GG_BAD_ARG. */
 gg_status gg_batch_eval_device(gg_batch *b, int n_cand, const gg_swap *d_cands,
                                gg_cand_result *d_out, void *stream);
+/* Waits for `stream` (NULL = the batch's stream) and returns GG_BAD_ARG if the last
+ * launch's device-side candidate check failed, else GG_OK; *first_bad (may be NULL) =
+ * the lowest rejected candidate index, or -1. */
+gg_status gg_batch_device_status(gg_batch *b, void *stream, int *first_bad);
 /* Per-vertex distance histogram of a base graph: hist[v*K + k] = number of
  * vertices at distance k+1 from v, k < K (the per-row popcounts of BFS levels
  * 1..K).  hist: host array n*K. */

@@ -113,3 +113,15 @@ def test_text_formats_roundtrip():
     assert g.N == 4 and g.degree_max == 3 and not g.is_regular()
     t = g.table()
     assert t.shape == (4, 3) and t[3].tolist() == [2, 3, 3]
+
+
+def test_bench_input_fixtures_match_the_generator():
+    """bench.py's reference arm reads these files instead of loading the engine's
+    generator; they must be exactly what the generator gives for the same seeds."""
+    import os
+    here = os.path.join(os.path.dirname(__file__), "golden")
+    for name, (n, d, seed) in (("regular_n65536_d8_seed1.npy", (65536, 8, 1)),
+                               ("regular_n4096_d16_seed1.npy", (4096, 16, 1))):
+        fx = np.load(os.path.join(here, name))
+        assert fx.dtype == np.uint16 and fx.shape == (n, d)
+        assert np.array_equal(fx.astype(np.int32), G.random_regular(n, d, seed))

@@ -149,3 +149,28 @@ def test_lifted_annealing_log_lines(tmp_path):
     assert [x["step"] for x in lines] == sorted(x["step"] for x in lines)
     assert min(x["best_aspl"] for x in lines) == tr.final_best
     assert all(x["best_aspl"] <= x["aspl"] for x in lines)
+
+
+def test_checkpoint_resume_keeps_wall_time_and_hit(tmp_path):
+    """A snapshot is written atomically (temporary file renamed into place), takes
+    the path with or without ".npz", records the elapsed wall time and the
+    time-to-target state, and a resumed run that had already reached its target
+    stops at once; a snapshot of another lift's shape is refused."""
+    N, M, D = G.cyclic_lift(24, 4, 4, 2)
+    gen = lambda t, c, s: G.gen_lift_moves(N, M, t, c, s)  # noqa: E731
+    kw = dict(seed=5, exact=4, t0_frac=0.05, t_end=1e-6, time_limit=None)
+    ck = str(tmp_path / "snap")          # no suffix: written as snap.npz
+    _, tr = A._anneal_table(OracleLift(N, M), gen, D, 12, target=10.0, checkpoint=ck, **kw)
+    assert tr.hit_step == 1 and (tmp_path / "snap.npz").exists()
+    assert not list(tmp_path.glob("*.tmp.npz"))
+    z = np.load(tmp_path / "snap.npz")
+    assert float(z["elapsed"]) >= 0.0 and int(z["hit_step"]) == 1
+    for name in (ck, ck + ".npz"):
+        L2 = OracleLift(N, M)
+        _, tr2 = A._anneal_table(L2, gen, None, 12, target=10.0, resume=name, **kw)
+        assert tr2.hit_step == 1 and tr2.steps == tr.steps and len(L2.bases) == 1
+        assert tr2.wall >= float(z["elapsed"])
+    N2, M2, D2 = G.cyclic_lift(30, 4, 4, 2)
+    with pytest.raises(ValueError):
+        A._anneal_table(OracleLift(N2, M2), lambda t, c, s: G.gen_lift_moves(N2, M2, t, c, s), D2, 12,
+                        target=None, resume=ck, **kw)

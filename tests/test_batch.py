@@ -66,11 +66,10 @@ def test_batch_config_2048_plus_512():
     sw = np.concatenate([G.gen_swaps(g1, i1, 2048, 21), G.gen_swaps(g2, i2, 512, 22)])
     res = b.eval(sw)
     assert np.all(res["connected"] == 1)
-    rng = np.random.default_rng(0)
-    for k in rng.choice(len(sw), 12, replace=False):
-        s = sw[k]
+    # every one of the 2560 candidates against the oracle's BFS of its own graph
+    for k, s in enumerate(sw):
         want = exact(G.apply_swap((g1, g2)[s["base"]], s))
-        assert (int(res[k]["total"]), int(res[k]["reached"]), int(res[k]["levels"]), True) == want
+        assert (int(res[k]["total"]), int(res[k]["reached"]), int(res[k]["levels"]), True) == want, k
 
 
 @pytest.mark.gpu
@@ -141,3 +140,35 @@ def test_affected_source_mode_equals_full_search(monkeypatch):
         want = exact(G.apply_swap(bases[s["base"]], s))
         got = inc1[k]
         assert (int(got["total"]), int(got["reached"]), bool(got["connected"])) == (want[0], want[1], want[3])
+
+
+@pytest.mark.gpu
+def test_device_candidates_checked_before_use():
+    """gg_batch_eval_device gets candidates the host never saw: each malformed one
+    (unknown base, vertex outside the base, mode not 0/1, repeated endpoint) makes
+    the launch score nothing (levels -1 everywhere) and the status call report
+    GG_BAD_ARG with its index; the kernels read no base or row through it.  A good
+    launch afterwards scores as the host-array call does."""
+    import torch
+    b = G.Batch(0)
+    g = G.random_regular(200, 4, 3)
+    i = b.add_base(g)
+    sw = G.gen_swaps(g, i, 16, 5)
+    n = len(sw)
+    d_out = torch.zeros(n * G.CAND_RESULT_DTYPE.itemsize // 4, dtype=torch.int32, device="cuda")
+    breakers = [("c", 5000), ("a", 200), ("base", 3), ("base", -1), ("mode", 2), ("d", None)]
+    for field, value in breakers:
+        bad = sw.copy()
+        bad[7][field] = bad[7]["a"] if value is None else value
+        d_sw = torch.from_numpy(bad.view(np.int32).copy()).cuda()
+        b.eval_device(n, d_sw.data_ptr(), d_out.data_ptr())
+        with pytest.raises(G.GGError) as ex:
+            b.device_status()
+        assert ex.value.status == G.GG_BAD_ARG and "candidate 7" in str(ex.value)
+        res = d_out.cpu().numpy().view(G.CAND_RESULT_DTYPE)
+        assert np.all(res["levels"] == -1) and np.all(res["total"] == 0)
+    d_sw = torch.from_numpy(sw.view(np.int32).copy()).cuda()
+    b.eval_device(n, d_sw.data_ptr(), d_out.data_ptr())
+    b.device_status()
+    res = d_out.cpu().numpy().view(G.CAND_RESULT_DTYPE)
+    assert np.array_equal(res, b.eval(sw))

@@ -233,6 +233,21 @@ def test_config_lift_32768():
     assert full == (d, r["total"] * (N // M))
 
 
+def test_config_regular_65536_8_full():
+    """The graph the headline benchmark times: the engine's exact total and
+    diameter against the oracle's BFS from every one of the 65536 sources, and
+    against the reference cudaASPLgraph built for this GPU when present."""
+    adj = G.random_regular(65536, 8, 1)
+    got = G.cudaASPLgraph(65536, 8, 0).calc(adj)
+    o = O.bfs_pull(adj, np.arange(65536))
+    assert o.connected and got == (o.levels, o.total())
+    if O.RefGPU.available("graph"):
+        R = O.RefGPU("graph")
+        R.create(65536, 8, 0)
+        assert R.graph_calc(adj) == got
+        R.close()
+
+
 def test_config_regular_65536_8_sampled():
     adj = G.random_regular(65536, 8, 1)
     e = G.cudaASPLgraph(65536, 8, 0)

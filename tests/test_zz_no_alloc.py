@@ -56,6 +56,33 @@ def test_noalloc_matches_engine_on_consecutive_calls():
         assert total == r["total"] and int(levels.max()) == r["levels"]
 
 
+@pytest.mark.parametrize("n,d,seed", [(4096, 8, 21), (2001, 5, 22), (1500, 7, 23)])
+def test_noalloc_generic_degrees_and_largest_size(n, d, seed):
+    """Degrees without a specialised kernel (5, 7: the run-time-degree kernel) and
+    the largest size the documentation promises always fits (N = 4096)."""
+    import instances as I
+    if (n * d) % 2:
+        n += 1
+    adj = G.random_regular(n, d, seed) if d in (3, 4, 6, 8, 12, 16) else I.random_regular_np(n, d, seed)
+    for _ in range(2):
+        rc, got = noalloc_counts(adj)
+        assert rc == G.GG_OK, G.lib().gg_last_error()
+        want, _ = engine_counts(adj)
+        assert np.array_equal(got, want)
+
+
+def test_noalloc_rejects_an_entry_outside_the_graph():
+    """An adjacency entry outside [0, N) is caught by the range check before any
+    gather and returns GG_BAD_ARG; the next good call is unaffected."""
+    adj = G.random_regular(512, 4, 31)
+    bad = adj.copy()
+    bad[100, 2] = 512
+    rc, _ = noalloc_counts(bad)
+    assert rc == G.GG_BAD_ARG and b"outside" in G.lib().gg_last_error()
+    rc, got = noalloc_counts(adj)
+    assert rc == G.GG_OK and np.array_equal(got, engine_counts(adj)[0])
+
+
 def test_noalloc_rejects_sizes_beyond_its_array():
     import torch
     out = torch.zeros(MAX_LEVELS + 1, dtype=torch.int64, device="cuda")

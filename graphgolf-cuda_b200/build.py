@@ -20,7 +20,9 @@ ROOT = os.path.dirname(PKG)
 CSRC = os.path.join(PKG, "csrc")
 INC = os.path.join(ROOT, "include")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
-REF = os.environ.get("GG_REFERENCE_TREE", "/root/reference")
+# The reference tree (read-only; only its headers and sources are read, never
+# copied): GG_REFERENCE_TREE, else the `reference` directory beside this repository.
+REF = os.environ.get("GG_REFERENCE_TREE", os.path.join(os.path.dirname(ROOT), "reference"))
 
 ENGINE_SRC = ["gg_engine.cu", "gg_batch.cu", "gg_surrogate.cu", "gg_noalloc.cu", "gg_inc.cu", "gg_lift.cu", "gg_probe.cu", "gg_gen.cpp"]
 ENGINE_LIB = os.path.join(PKG, "libggb200.so")
@@ -94,6 +96,42 @@ def build_driver(force=False):
     return DRIVER_BIN
 
 
+# The reference's own command-line drivers, compiled unchanged from the reference
+# tree, each twice: "<name>_shim" linked against libgg_refshim.so (this engine
+# behind the reference classes) and "<name>_orig" against the reference's own
+# calculators built for this GPU (oracle/_ref/libref_<calc>.so).  Boost is not in
+# this image; tests/boost_stub holds test-only stand-ins of the two Boost headers
+# they include.  Test infrastructure: tests/test_ref_drivers.py runs both.
+REF_DRIVERS = {"aspl_cuda": "graph", "piece2aspl": "piece", "box2aspl": "box", "main": "conv",
+               "annealing": "conv"}
+STUB = os.path.join(ROOT, "tests", "boost_stub")
+BIN = os.path.join(ROOT, "tests", "_bin")
+
+
+def build_reference_drivers(force=False):
+    if not os.path.isdir(os.path.join(REF, "cppcode")) or not os.path.exists(SHIM_LIB):
+        return []
+    os.makedirs(BIN, exist_ok=True)
+    stubs = [os.path.join(STUB, "boost", f) for f in os.listdir(os.path.join(STUB, "boost"))]
+    inc = ["-I", STUB, "-I", os.path.join(REF, "cudacode"), "-I", os.path.join(REF, "cppcode")]
+    out = []
+    for name, calc in REF_DRIVERS.items():
+        src = os.path.join(REF, "cppcode", name + ".cpp")
+        shim_bin = os.path.join(BIN, f"ref_{name}_shim")
+        if force or _stale(shim_bin, [src, SHIM_LIB, *stubs]):
+            _run(["g++", "-O2", "-std=c++17", *inc, "-o", shim_bin, src, "-L", PKG, "-lgg_refshim", "-lggb200",
+                  "-Wl,-rpath,$ORIGIN/../../graphgolf-cuda_b200"])
+        out.append(shim_bin)
+        ref_lib = os.path.join(ROOT, "oracle", "_ref", f"libref_{calc}.so")
+        if os.path.exists(ref_lib):
+            orig_bin = os.path.join(BIN, f"ref_{name}_orig")
+            if force or _stale(orig_bin, [src, ref_lib, *stubs]):
+                _run(["g++", "-O2", "-std=c++17", *inc, "-o", orig_bin, src, "-L",
+                      os.path.join(ROOT, "oracle", "_ref"), f"-lref_{calc}", "-Wl,-rpath,$ORIGIN/../../oracle/_ref"])
+            out.append(orig_bin)
+    return out
+
+
 def build_oracle():
     """The oracle (test infrastructure) and, when the reference tree is here,
     the reference's own calculators in oracle/_ref/."""
@@ -108,6 +146,7 @@ def build_all(force=False):
     build_shim(force)
     build_driver(force)
     build_oracle()
+    build_reference_drivers(force)
 
 
 if __name__ == "__main__":

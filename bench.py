@@ -356,30 +356,18 @@ def run_ours(args):
     stream = torch.cuda.Stream()
     torch.cuda.set_stream(stream)
     sptr = stream.cuda_stream
-    if sharded:
-        # one exact all-reduce of (total, reached, level_steps) and (levels, capped)
-        # per step, on the same stream as the evaluation
-        red_s = torch.zeros(3, dtype=torch.int64, device="cuda")
-        red_m = torch.zeros(2, dtype=torch.int64, device="cuda")
-
     def step():
         r = eng.eval_device(table_dev.data_ptr(), max_levels=max_levels, stream=sptr, src_range=src_range)
         if sharded:
-            red_s.copy_(torch.tensor([r["total"], r["reached"], r["level_steps"]], dtype=torch.int64))
-            red_m.copy_(torch.tensor([r["levels"], r["capped"]], dtype=torch.int64))
-            dist.all_reduce(red_s, op=dist.ReduceOp.SUM)
-            dist.all_reduce(red_m, op=dist.ReduceOp.MAX)
+            # the exact counts of the whole graph: one all-reduce of the shards'
+            # sums and maxima (distributed.combine, the function the gloo tests run)
+            c = D.combine(r, wl["S"] * wl["N"])
+            c.update(n_sources=wl["S"], batches=r["batches"])
+            return c
         return r
 
     def combined(r):
-        if not sharded:
-            return dict(r)
-        tot, reached, steps_ = (int(x) for x in red_s.tolist())
-        lev, capped = (int(x) for x in red_m.tolist())
-        pairs = wl["S"] * wl["N"]
-        return {"total": tot, "reached": reached, "level_steps": steps_, "levels": lev, "capped": capped,
-                "connected": int(not capped and reached == pairs), "n_sources": wl["S"],
-                "batches": r["batches"]}
+        return dict(r)
 
     res = None
     for _ in range(max(args.warmup, 0)):

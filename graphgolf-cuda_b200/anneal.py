@@ -77,8 +77,9 @@ def anneal(adj0, steps, *, seed=1, exact=32, pool=4096, explore=8, surrogate=Fal
            t_end=1e-6, target=None, time_limit=None, lr=2e-3, feature_every=32, train_every=2,
            device=0, spearman_sample=0, min_train_pairs=0):
     """Anneal from `adj0` (n x d simple regular graph).  Returns (best_adj, Trace).
-    With a `target`, the run stops once the best ASPL reaches it and the network
-    has trained on at least `min_train_pairs` pairs (the hit time is the first).
+    With a `target`, the run stops at the first step after which the best ASPL is
+    at or below it and the network has trained on at least `min_train_pairs` pairs;
+    that step and its wall time are the hit.
     With the surrogate, the adjacency it passes messages over follows every
     accepted move; its distance-histogram features are recomputed every
     `feature_every` accepted moves (one 2-opt changes them only locally)."""
@@ -158,11 +159,13 @@ def anneal(adj0, steps, *, seed=1, exact=32, pool=4096, explore=8, surrogate=Fal
                     best_aspl, best_adj = aspl, adj.copy()
                     tr.times.append(time.perf_counter() - t_start)
                     tr.best.append(best_aspl)
-                    if target is not None and tr.hit_time is None and best_aspl <= target:
-                        tr.hit_time, tr.hit_step = tr.times[-1], i + 1
-                        tr.hit_train_pairs = tr.train_pairs
         tr.steps = i + 1
-        if target is not None and tr.hit_time is not None and tr.train_pairs >= min_train_pairs:
+        # the target counts as reached once the best is at or below it AND the
+        # network has trained on at least min_train_pairs exact pairs
+        if (target is not None and tr.hit_time is None and best_aspl <= target and
+                tr.train_pairs >= min_train_pairs):
+            tr.hit_time, tr.hit_step = time.perf_counter() - t_start, i + 1
+            tr.hit_train_pairs = tr.train_pairs
             break
         if time_limit is not None and time.perf_counter() - t_start > time_limit:
             break

@@ -24,7 +24,7 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 # copied): GG_REFERENCE_TREE, else the `reference` directory beside this repository.
 REF = os.environ.get("GG_REFERENCE_TREE", os.path.join(os.path.dirname(ROOT), "reference"))
 
-ENGINE_SRC = ["gg_engine.cu", "gg_batch.cu", "gg_surrogate.cu", "gg_noalloc.cu", "gg_inc.cu", "gg_lift.cu", "gg_probe.cu", "gg_gen.cpp"]
+ENGINE_SRC = ["gg_engine.cu", "gg_batch.cu", "gg_surrogate.cu", "gg_noalloc.cu", "gg_inc.cu", "gg_lift.cu", "gg_probe.cu", "gg_gen.cpp", "gg_tune.cpp"]
 ENGINE_LIB = os.path.join(PKG, "libggb200.so")
 SHIM_LIB = os.path.join(PKG, "libgg_refshim.so")
 

@@ -48,6 +48,8 @@ constexpr int kPlanes = 4;   // distance bit-planes: distances up to 15
 
 struct BatchBase {
     const int32_t *adj;   // [n][d] in global memory
+    const uint16_t *adj16;   // the same rows as uint16, padded to adj16_bytes (a multiple of 16)
+    unsigned adj16_bytes;
     int n, d;
     int log_nc;           // chunks (of 128 sources) per task row = 1 << log_nc
     int chunks;           // tasks per candidate = ceil(n / (128 << log_nc))
@@ -77,7 +79,8 @@ struct BatchCtl {
     int bad;              // set by batch_reset when a candidate is outside the domain
     int n_bases;          // registered bases
     int bad_index;        // lowest index of such a candidate (INT_MAX: none)
-    int pad[2];
+    int timeout;          // a CTA's wait for its adjacency copy ran past its limit
+    int pad;
 };
 
 struct BatchArgs {
@@ -99,14 +102,43 @@ __device__ __forceinline__ unsigned padw(int lo, int ns) {
     return ~((1u << (ns - lo)) - 1u);
 }
 
+// Bulk copy (the TMA unit's untiled cp.async.bulk, no multicast, this GPU's
+// memory) of `bytes` (a multiple of 16, both addresses 16-byte aligned) from global
+// memory into this CTA's shared memory, completing on the mbarrier `bar`.
+__device__ __forceinline__ unsigned smem_addr(const void *p) {
+    return static_cast<unsigned>(__cvta_generic_to_shared(p));
+}
+__device__ __forceinline__ void bulk_to_smem(void *dst, const void *src, unsigned bytes, uint64_t *bar) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;"
+                 :: "r"(smem_addr(bar)), "r"(bytes) : "memory");
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
+                 :: "r"(smem_addr(dst)), "l"(src), "r"(bytes), "r"(smem_addr(bar)) : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, unsigned phase) {
+    unsigned ok;
+    asm volatile("{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+                 " selp.u32 %0, 1, 0, p;\n}" : "=r"(ok) : "r"(smem_addr(bar)), "r"(phase) : "memory");
+    return ok != 0;
+}
+
+constexpr long long kCopyWaitNs = 2000000000ll;   // 2 s: a copy of at most 128 KB never takes that
+
 __global__ void __launch_bounds__(kBatchBlock, 1) batch_kernel(const BatchArgs a) {
     extern __shared__ uint4 sm[];
     __shared__ unsigned s_task;
     __shared__ unsigned long long s_tot[kBatchBlock / 32], s_reach[kBatchBlock / 32];
+    __shared__ __align__(8) uint64_t s_bar;   // completion of the adjacency copy
+    __shared__ int s_late;
     if (a.ctl->bad) return;   // batch_reset rejected a candidate: index nothing
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int n_cand = a.ctl->n_cand, max_chunks = a.ctl->max_chunks;
     const unsigned n_tasks = (unsigned)n_cand * (unsigned)max_chunks;
+    if (tid == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" :: "r"(smem_addr(&s_bar)) : "memory");
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
+    unsigned phase = 0;
 
     for (;;) {
         if (tid == 0) s_task = atomicAdd(&a.ctl->task_ctr, 1u);
@@ -130,12 +162,42 @@ __global__ void __launch_bounds__(kBatchBlock, 1) batch_kernel(const BatchArgs a
         const int ns = min(S, count - s0);
         const int items = n << lnc;
 
-        // shared memory: adjacency (uint16, padded to 16 bytes), then two bitsets
+        // shared memory: adjacency (uint16, padded to 16 bytes), then two bitsets.
+        // The base's packed rows arrive by one bulk copy; every thread waits on the
+        // mbarrier (bounded: past kCopyWaitNs the CTA flags a timeout and stops).
         uint16_t *adj = reinterpret_cast<uint16_t *>(sm);
         uint4 *cur = sm + (((size_t)n * d * 2 + 15) / 16);
         uint4 *nxt = cur + items;
-        for (int k = tid; k < n * d; k += kBatchBlock) adj[k] = (uint16_t)B.adj[k];
+        if (tid == 0) {
+            // the previous task's generic-proxy accesses to this memory come first
+            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+            bulk_to_smem(adj, B.adj16, B.adj16_bytes, &s_bar);
+            s_late = 0;
+        }
+        {
+            bool done = mbar_try_wait(&s_bar, phase);
+            if (!done) {
+                unsigned long long t0;
+                asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t0));
+                for (unsigned it = 1; !done; ++it) {
+                    done = mbar_try_wait(&s_bar, phase);
+                    if (!done && (it & 63u) == 0u) {
+                        unsigned long long t;
+                        asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+                        if ((long long)(t - t0) > kCopyWaitNs) break;
+                    }
+                }
+            }
+            if (!done) s_late = 1;
+        }
+        phase ^= 1u;
         __syncthreads();
+        if (s_late) {
+            // the copy did not complete: report it and leave (the host sees
+            // GG_TIMEOUT); only this CTA's tail of tasks is left unscored
+            if (tid == 0) atomicExch(&a.ctl->timeout, 1);
+            return;
+        }
         if (sw.a >= 0 && tid < 4) {
             // 2-opt: (a,b),(c,d) -> (a,c),(b,d) [mode 0] or (a,d),(b,c) [mode 1]
             const int x[4] = {sw.a, sw.b, sw.c, sw.d};
@@ -224,8 +286,8 @@ __global__ void __launch_bounds__(kBatchBlock, 1) batch_kernel(const BatchArgs a
 
 __global__ void batch_finalize(const BatchArgs a) {
     const int n_cand = a.ctl->n_cand;
-    if (a.ctl->bad) {
-        // a rejected launch scores nothing: every result says so
+    if (a.ctl->bad || a.ctl->timeout) {
+        // a rejected or timed-out launch scores nothing: every result says so
         for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n_cand; i += gridDim.x * blockDim.x)
             a.out[i] = gg_cand_result{0ull, 0ull, -1, 0};
         return;
@@ -370,6 +432,7 @@ struct gg_batch {
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     std::vector<BatchBase> bases;          // host copy (adj = device pointers)
     std::vector<int32_t *> base_adj;       // device adjacency per base
+    std::vector<uint16_t *> base_adj16;    // the same, packed as uint16 for the bulk copy
     BatchBase *d_bases = nullptr;
     BatchCtl *d_ctl = nullptr, *h_ctl = nullptr;
     int cap = 0;                           // candidates the buffers hold
@@ -405,14 +468,24 @@ void drop_graph(gg_batch *b) {
     b->graph = nullptr;
 }
 
-// Smallest chunk count per task row (a power of two) whose bitsets and
-// adjacency fit the shared-memory budget, as wide as possible.
-int auto_log_nc(int n, int d) {
+bool log_nc_fits(int n, int d, int l) {
     const size_t adj = ((size_t)n * d * 2 + 15) / 16 * 16;
+    return adj + 2 * (size_t)n * (16u << l) <= kSmemBudget;
+}
+
+std::string batch_tune_key(int device, int n, int d) { return gg::tune_key(device, "batch", {n, d}); }
+
+// Chunk count per task row (a power of two): the one gg_batch_autotune recorded for
+// this base shape on this kind of GPU, else the widest whose bitsets and adjacency
+// fit the shared-memory budget.
+int auto_log_nc(int device, int n, int d) {
+    std::vector<int> tuned;
+    if (gg::tune_get(batch_tune_key(device, n, d), &tuned) && !tuned.empty() && tuned[0] >= 0 &&
+        tuned[0] <= 4 && log_nc_fits(n, d, tuned[0]))
+        return tuned[0];
     int best = -1;
     for (int l = 0; l <= 4; ++l) {
-        const size_t need = adj + 2 * (size_t)n * (16u << l);
-        if (need <= kSmemBudget) best = l;
+        if (log_nc_fits(n, d, l)) best = l;
         if ((128 << l) >= n) break;
     }
     return best;
@@ -548,9 +621,18 @@ gg_status base_pass(gg_batch *b, int id) {
 
 __global__ void set_ctl(BatchCtl *ctl, const BatchCtl v) { *ctl = v; }
 
+// int32 rows -> uint16 rows (vertex ids < 65536), zero padding to `padded` entries.
+__global__ void pack16_kernel(const int32_t *adj, uint16_t *out, int n_ent, int padded) {
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < padded; k += gridDim.x * blockDim.x)
+        out[k] = k < n_ent ? (uint16_t)adj[k] : (uint16_t)0;
+}
+
+unsigned adj16_bytes(int n, int d) { return (unsigned)((((size_t)n * d * 2) + 15) / 16 * 16); }
+
 // The device-side candidate check starts clean for every launch.
 void arm_check(gg_batch *b) {
     b->h_ctl->bad = 0;
+    b->h_ctl->timeout = 0;
     b->h_ctl->bad_index = 0x7fffffff;
     b->h_ctl->n_bases = (int)b->bases.size();
 }
@@ -605,16 +687,24 @@ gg_status gg_batch_add_base(gg_batch *b, int n, int degree, const int32_t *adj, 
         return bfail(GG_BAD_ARG, "need 1 <= n <= 65535, degree >= 1, at most 256 bases");
     for (long long k = 0; k < (long long)n * degree; ++k)
         if (adj[k] < 0 || adj[k] >= n) return bfail(GG_BAD_ARG, "adjacency entry outside [0, n)");
-    const int lnc = auto_log_nc(n, degree);
+    const int lnc = auto_log_nc(b->device, n, degree);
     if (lnc < 0) return bfail(GG_BAD_ARG, "base graph too large for a shared-memory task");
     GB_CK(cudaSetDevice(b->device));
     int32_t *d = nullptr;
+    uint16_t *d16 = nullptr;
+    const unsigned b16 = adj16_bytes(n, degree);
     GB_CK(cudaMalloc(&d, (size_t)n * degree * sizeof(int32_t)));
+    cudaError_t me = cudaMalloc(&d16, b16);
+    if (me != cudaSuccess) { cudaFree(d); GB_CK(me); }
     GB_CK(cudaMemcpy(d, adj, (size_t)n * degree * sizeof(int32_t), cudaMemcpyHostToDevice));
+    pack16_kernel<<<64, 256, 0, b->stream>>>(d, d16, n * degree, (int)(b16 / 2));
+    GB_CK(cudaGetLastError());
     BatchBase B{};
-    B.adj = d; B.n = n; B.d = degree; B.log_nc = lnc; B.chunks = (n + (128 << lnc) - 1) / (128 << lnc);
+    B.adj = d; B.adj16 = d16; B.adj16_bytes = b16;
+    B.n = n; B.d = degree; B.log_nc = lnc; B.chunks = (n + (128 << lnc) - 1) / (128 << lnc);
     b->bases.push_back(B);
     b->base_adj.push_back(d);
+    b->base_adj16.push_back(d16);
     b->base_planes.push_back(nullptr);
     b->base_stats.push_back(nullptr);
     const int id = (int)b->bases.size() - 1;
@@ -635,6 +725,9 @@ gg_status gg_batch_set_base(gg_batch *b, int base_id, const int32_t *adj) {
     // ordered on the batch stream: launches already enqueued see the old table
     GB_CK(cudaMemcpyAsync(b->base_adj[base_id], adj, (size_t)B.n * B.d * sizeof(int32_t),
                           cudaMemcpyHostToDevice, b->stream));
+    pack16_kernel<<<64, 256, 0, b->stream>>>(b->base_adj[base_id], b->base_adj16[base_id], B.n * B.d,
+                                            (int)(B.adj16_bytes / 2));
+    GB_CK(cudaGetLastError());
     return base_pass(b, base_id);
 }
 
@@ -651,6 +744,57 @@ gg_status gg_batch_set_chunk(gg_batch *b, int base_id, int sources) {
     B.chunks = (B.n + (128 << l) - 1) / (128 << l);
     GB_CK(cudaSetDevice(b->device));
     return refresh_plan(b);
+}
+
+gg_status gg_batch_autotune(gg_batch *b, int n_cand, const gg_swap *cands, int trials, double *best_ms) {
+    if (!b || n_cand < 1 || !cands || trials < 1) return bfail(GG_BAD_ARG, "bad arguments");
+    gg_status s = validate(b, n_cand, cands);
+    if (s != GG_OK) return s;
+    std::vector<gg_cand_result> out((size_t)n_cand);
+    auto time_it = [&](double *t) -> gg_status {
+        gg_status r = gg_batch_eval(b, n_cand, cands, out.data());  // warm (and capture)
+        if (r != GG_OK) return r;
+        *t = 1e300;
+        for (int k = 0; k < trials; ++k) {
+            r = gg_batch_eval(b, n_cand, cands, out.data());
+            if (r != GG_OK) return r;
+            *t = std::min(*t, b->last_ms);
+        }
+        return GG_OK;
+    };
+    std::vector<char> used(b->bases.size(), 0);
+    for (int i = 0; i < n_cand; ++i) used[cands[i].base] = 1;
+    double best_t = 1e300;
+    s = time_it(&best_t);
+    if (s != GG_OK) return s;
+    // coordinate descent over the bases the candidates use: each base's chunk width
+    // with the others fixed
+    for (size_t id = 0; id < b->bases.size(); ++id) {
+        if (!used[id]) continue;
+        const int n = b->bases[id].n, d = b->bases[id].d;
+        int best_l = b->bases[id].log_nc;
+        for (int l = 0; l <= 4; ++l) {
+            if (l == best_l || !log_nc_fits(n, d, l)) continue;
+            if (l > 0 && (128 << (l - 1)) >= n) break;   // wider than the base's sources
+            s = gg_batch_set_chunk(b, (int)id, 128 << l);
+            if (s != GG_OK) return s;
+            double t = 0;
+            s = time_it(&t);
+            if (s != GG_OK) return s;
+            if (t < best_t) { best_t = t; best_l = l; }
+        }
+        s = gg_batch_set_chunk(b, (int)id, 128 << best_l);
+        if (s != GG_OK) return s;
+        gg::tune_put(batch_tune_key(b->device, n, d), {best_l});
+    }
+    if (best_ms) *best_ms = best_t;
+    return GG_OK;
+}
+
+gg_status gg_batch_chunk(gg_batch *b, int base_id, int *sources) {
+    if (!b || !sources || base_id < 0 || base_id >= (int)b->bases.size()) return bfail(GG_BAD_ARG, "bad base");
+    *sources = 128 << b->bases[base_id].log_nc;
+    return GG_OK;
 }
 
 gg_status gg_batch_eval(gg_batch *b, int n_cand, const gg_swap *cands, gg_cand_result *out) {
@@ -688,6 +832,7 @@ gg_status gg_batch_eval(gg_batch *b, int n_cand, const gg_swap *cands, gg_cand_r
     GB_CK(cudaEventElapsedTime(&ms, b->ev0, b->ev1));
     b->last_ms = ms;
     std::memcpy(out, b->h_out, (size_t)n_cand * sizeof(gg_cand_result));
+    if (out[0].levels < 0) return gg_batch_device_status(b, b->stream, nullptr);  // a flagged launch
     return GG_OK;
 }
 
@@ -721,6 +866,7 @@ gg_status gg_batch_device_status(gg_batch *b, void *stream, int *first_bad) {
     BatchCtl c{};
     GB_CK(cudaMemcpy(&c, b->d_ctl, sizeof(BatchCtl), cudaMemcpyDeviceToHost));
     if (first_bad) *first_bad = c.bad ? c.bad_index : -1;
+    if (c.timeout) return bfail(GG_TIMEOUT, "a CTA's wait for its adjacency copy ran past its limit");
     if (c.bad)
         return bfail(GG_BAD_ARG, "device candidate " + std::to_string(c.bad_index) +
                                      ": unknown base, vertex or mode out of range, or repeated endpoint");
@@ -777,6 +923,7 @@ gg_status gg_batch_destroy(gg_batch *b) {
     if (b->stream) cudaStreamSynchronize(b->stream);
     drop_graph(b);
     for (auto p : b->base_adj) cudaFree(p);
+    for (auto p : b->base_adj16) cudaFree(p);
     for (auto p : b->base_planes) cudaFree(p);
     for (auto p : b->base_stats) cudaFree(p);
     for (auto &pe : b->engines) gg_destroy(pe.second);

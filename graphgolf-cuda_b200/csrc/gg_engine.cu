@@ -110,6 +110,13 @@ struct gg_engine {
     int push_min_items = 1 << 20;        // ... on bitsets of at least this many chunks
     int adj_smem_rows = 0;               // shared-memory adjacency slice (rows per block)
     size_t smem_bytes = 0;
+    int bps_cap = 0;                     // resident blocks per SM (0: as many as fit)
+    int walk_pref = -1;                  // walk depth: -1 automatic, 0 off, K > 0 forced
+    int walk_K = 0;                      // levels computed by the walk pass (0: off)
+    int walk_rpg = 1;                    // rows per walk group
+    unsigned walk_smem_off = 0;          // byte offset of the walk buffers in dynamic smem
+    int32_t *d_h2 = nullptr;             // [rows][d*d] level-2 walk ends (walk_K >= 3)
+    size_t h2_elems = 0;
     long long wait_ns = 10ll * 1000 * 1000 * 1000;
     int cap_alloc = 0;                   // levels the counter arrays hold
     int nb_alloc = 0;                    // batches the counter arrays hold
@@ -198,6 +205,7 @@ void destroy_all(gg_engine *e) {
     free_batch_buffers(e);
     free_counters(e);
     if (e->d_adj != e->d_table) cudaFree(e->d_adj);  // the graph form aliases the two
+    cudaFree(e->d_h2);
     cudaFree(e->d_table); cudaFree(e->d_inv);
     cudaFreeHost(e->h_table);
     if (e->ev0) cudaEventDestroy(e->ev0);
@@ -233,21 +241,33 @@ void *kernel_for(int d, bool planes = false) {
     return planes ? kernel_for_t<true>(d) : kernel_for_t<false>(d);
 }
 
-// Source-batch plan: batch width, chunks per row, grid size.
-// Batch widths chosen by gg_autotune, by (device, form, rows, degree, sources).
-struct TuneKey {
-    int device, form, rows, d, n_src;
-    bool operator<(const TuneKey &o) const {
-        return std::tie(device, form, rows, d, n_src) < std::tie(o.device, o.form, o.rows, o.d, o.n_src);
+// Levels the walk pass computes for this plan: the largest K <= 4 whose walk ends
+// per row, d + d^2 + ... + d^K, stay within 600 (d = 8: 3 levels, 584 ends; d = 16:
+// 2; d = 4: 4), with the level-2 table (rows * d^2 int32) within 64 MiB for K >= 3
+// and d^2 <= kWalkList for K = 4.  GG_WALK_LEVELS overrides (0 = off).
+int walk_levels(const gg_engine *e) {
+    const int env = env_int("GG_WALK_LEVELS", e->walk_pref);
+    const int d = e->d;
+    if (d <= 0 || e->nC > gg::kWalkMaxNC || env == 0) return 0;
+    int K = 0;
+    long long sum = 0, p = 1;
+    for (int k = 1; k <= 4; ++k) {
+        p *= d;
+        sum += p;
+        if (sum > 600) break;
+        K = k;
     }
-};
-std::mutex g_tune_mu;
-std::map<TuneKey, int> g_tuned;
+    if (env > 0) K = std::min(env, 4);
+    if (K >= 3 && (long long)e->rows * d * d * 4 > (64ll << 20)) K = 2;
+    if (K >= 4 && d * d > gg::kWalkList) K = 3;
+    return K;
+}
 
-int tuned_width(const gg_engine *e) {
-    std::lock_guard<std::mutex> lk(g_tune_mu);
-    auto it = g_tuned.find({e->device, e->form, e->rows, e->d, (int)e->reps.size()});
-    return it == g_tuned.end() ? 0 : it->second;
+// Source-batch plan: batch width, chunks per row, grid size.
+// gg_autotune's choices (batch width, resident blocks per SM, walk depth) are
+// kept in the tuning cache under (GPU, form, rows, degree, sources).
+std::string engine_tune_key(const gg_engine *e) {
+    return gg::tune_key(e->device, "graph", {e->form, e->rows, e->d, (long long)e->reps.size()});
 }
 
 gg_status plan(gg_engine *e, int want_bits) {
@@ -258,11 +278,13 @@ gg_status plan(gg_engine *e, int want_bits) {
         bits = want_bits;
     } else {
         const int env = env_int("GG_BATCH_SOURCES", 0);
-        const int tuned = tuned_width(e);
+        std::vector<int> tuned;
         if (env > 0) {
             bits = env;
-        } else if (tuned > 0) {
-            bits = tuned;
+        } else if (gg::tune_get(engine_tune_key(e), &tuned) && tuned.size() >= 3 && tuned[0] > 0) {
+            bits = tuned[0];
+            e->bps_cap = tuned[1];
+            e->walk_pref = tuned[2];
         } else {
             // The widest batch whose three bitsets (3 * rows * bits / 8 bytes)
             // stay within 3/4 of the L2, so that the gathers hit L2 rather than
@@ -302,32 +324,55 @@ gg_status plan(gg_engine *e, int want_bits) {
         GG_CK(cudaMalloc(&e->d_nf, fwords * 4));
         e->p_dirty = true;
     }
+    // Walk pass: levels 1..K of each batch from the walk ends of every row.
+    e->walk_K = walk_levels(e);
+    e->walk_rpg = 1;
+    size_t walk_bytes = 0;
+    if (e->walk_K > 0) {
+        int g = e->nC, b = 32;
+        while (b) { const int t = g % b; g = b; b = t; }   // gcd(nC, 32)
+        e->walk_rpg = 32 / g;
+        walk_bytes = (size_t)(gg::kBlock / 32) * gg::walk_smem_per_warp(e->nC);
+    }
+    const size_t h2_need = e->walk_K >= 3 ? (size_t)e->rows * e->d * e->d : 0;
+    if (h2_need != e->h2_elems) {
+        cudaFree(e->d_h2);
+        e->d_h2 = nullptr;
+        e->h2_elems = 0;
+        if (h2_need) {
+            GG_CK(cudaMalloc(&e->d_h2, h2_need * sizeof(int32_t)));
+            e->h2_elems = h2_need;
+        }
+    }
     int per_sm = 0, sms = 0;
     GG_CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, e->device));
-    GG_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel_for(e->d), gg::kBlock, 0));
+    GG_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel_for(e->d), gg::kBlock, walk_bytes));
     if (per_sm < 1) return fail(GG_CUDA_ERROR, "BFS kernel cannot be resident");
     const long long tiles = ((long long)e->items + 31) / 32;
     const long long want = (tiles + (gg::kBlock / 32) - 1) / (gg::kBlock / 32);
-    // GG_BLOCKS_PER_SM caps the resident blocks per SM (tuning; never above what fits).
-    const int cap_per_sm = env_int("GG_BLOCKS_PER_SM", 0);
+    // Resident blocks per SM: at most what fits; GG_BLOCKS_PER_SM, else the tuned cap.
+    const int cap_per_sm = env_int("GG_BLOCKS_PER_SM", e->bps_cap);
     if (cap_per_sm > 0) per_sm = std::min(per_sm, cap_per_sm);
     e->grid = (int)std::max<long long>(1, std::min<long long>((long long)per_sm * sms, want));
     // Shared-memory adjacency slice: a block's contiguous tile range spans at most
     // ceil(tiles/grid)*32/nC + 2 vertices.  Cached when it fits a small budget and
     // does not lower the number of resident blocks.
     e->adj_smem_rows = 0;
-    e->smem_bytes = 0;
+    e->smem_bytes = walk_bytes;
+    e->walk_smem_off = 0;
     if (env_int("GG_ADJ_SMEM", 1) && e->d > 0) {
         const long long per_block = (tiles + e->grid - 1) / e->grid;
         const long long rows = per_block * 32 / e->nC + 2;
-        const long long bytes = rows * e->d * 4;
-        if (bytes <= 32 * 1024) {
+        const long long bytes = (rows * e->d * 4 + 15) / 16 * 16;
+        // within 32 KB, and within the 48 KB a launch gets without opting in
+        if (bytes <= 32 * 1024 && bytes + (long long)walk_bytes <= 48 * 1024) {
             int per_sm2 = 0;
             GG_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm2, kernel_for(e->d), gg::kBlock,
-                                                                (size_t)bytes));
+                                                                (size_t)bytes + walk_bytes));
             if (per_sm2 >= per_sm) {
                 e->adj_smem_rows = (int)rows;
-                e->smem_bytes = (size_t)bytes;
+                e->walk_smem_off = (unsigned)bytes;
+                e->smem_bytes = (size_t)bytes + walk_bytes;
             }
         }
     }
@@ -468,7 +513,10 @@ gg_status run_eval(gg_engine *e, const int32_t *d_table_in, const gg_eval_opts *
     uint64_t d2h = e->off_counts + (size_t)nb * stride * sizeof(unsigned long long);
     if (wvc) d2h += (size_t)nb * stride * sizeof(unsigned);
     if (want_ns) d2h += lv * sizeof(unsigned long long);
-    const int launches = 1 + ((long long)e->rows * e->d > 0 ? 1 : 0);
+    // Walk pass for this evaluation: not with the WVC masks or the distance planes
+    // (their per-level bookkeeping lives in the level loop), at most the level cap.
+    const int walk_K = (wvc || (x && x->planes)) ? 0 : std::min(e->walk_K, cap_req);
+    const int launches = 1 + ((long long)e->rows * e->d > 0 ? 1 : 0) + (walk_K >= 3 ? 1 : 0);
 
     // Everything the GPU does for one evaluation, on `q`: status words zeroed,
     // table -> adjacency (checked), one cooperative launch for every source
@@ -501,6 +549,16 @@ gg_status run_eval(gg_engine *e, const int32_t *d_table_in, const gg_eval_opts *
         }
         if (want_ns)
             GG_CK(cudaMemsetAsync(e->d_level_ns, 0, lv * sizeof(unsigned long long), q));
+        if (walk_K > 0) {
+            // blocks add the walk's level counts before any grid barrier
+            GG_CK(cudaMemsetAsync(e->d_counts, 0, (size_t)nb * stride * sizeof(unsigned long long), q));
+            if (walk_K >= 3) {
+                const long long nh = (long long)e->rows * e->d * e->d;
+                gg::h2_kernel<<<(int)std::min<long long>((nh + 255) / 256, 8192), 256, 0, q>>>(
+                    e->d_adj, e->d_h2, e->rows, e->d, e->form == FORM_GRAPH ? e->d_bad : nullptr);
+                GG_CK(cudaGetLastError());
+            }
+        }
         BfsArgs a{};
         a.adj = e->d_adj;
         a.inv = x && x->inv ? x->inv : e->d_inv;
@@ -539,6 +597,10 @@ gg_status run_eval(gg_engine *e, const int32_t *d_table_in, const gg_eval_opts *
         a.wait_ns = e->wait_ns;
         a.expected = (unsigned)e->grid + extra;
         a.bad = e->form == FORM_GRAPH ? e->d_bad : nullptr;
+        a.walk_K = walk_K;
+        a.walk_rpg = e->walk_rpg;
+        a.walk_smem_off = e->walk_smem_off;
+        a.h2 = e->d_h2;
         void *args[] = {&a};
         GG_CK(cudaLaunchCooperativeKernel(kernel_for(e->d, a.planes != nullptr), dim3(e->grid), dim3(gg::kBlock), args,
                                           e->smem_bytes, q));
@@ -870,55 +932,87 @@ gg_status gg_autotune(gg_engine *e, const int32_t *table, int trials, int *best_
     GG_CK(cudaStreamSynchronize(e->stream));
     const int n_src = (int)e->reps.size();
     // the L2-resident width the default plan picks, and its neighbours
-    int base = 0;
+    int base = 0, max_bps = 0;
     {
-        const int keep = e->batch_bits;
+        const int keep = e->batch_bits, keep_bps = e->bps_cap, keep_walk = e->walk_pref;
+        e->bps_cap = 0;
+        e->walk_pref = -1;
         gg_status s = plan(e, 0);
         if (s != GG_OK) return s;
         base = e->batch_bits;
-        if (keep != base && keep > 0) { s = plan(e, keep); if (s != GG_OK) return s; }
+        GG_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&max_bps, kernel_for(e->d), gg::kBlock,
+                                                            e->smem_bytes));
+        e->bps_cap = keep_bps;
+        e->walk_pref = keep_walk;
+        if (keep > 0) { s = plan(e, keep); if (s != GG_OK) return s; }
     }
-    std::vector<int> cands;
+    std::vector<int> widths;
     for (double f : {0.25, 0.5, 1.0, 2.0, 4.0}) {
         int w = (int)(base * f);
         w = std::max(128, std::min(((w + 127) / 128) * 128, ((n_src + 127) / 128) * 128));
-        cands.push_back(w);
+        widths.push_back(w);
     }
-    cands.push_back(((n_src + 127) / 128) * 128);
-    std::sort(cands.begin(), cands.end());
-    cands.erase(std::unique(cands.begin(), cands.end()), cands.end());
+    widths.push_back(((n_src + 127) / 128) * 128);
+    std::sort(widths.begin(), widths.end());
+    widths.erase(std::unique(widths.begin(), widths.end()), widths.end());
+    std::vector<int> bps_opts;   // 0 = as many as fit, then one and two fewer
+    bps_opts.push_back(0);
+    for (int k = 1; k <= 2; ++k)
+        if (max_bps - k >= 1) bps_opts.push_back(max_bps - k);
     if (e->table_elems) {
         std::memcpy(e->h_table, table, e->table_elems * sizeof(int32_t));
         GG_CK(cudaMemcpyAsync(e->d_table, e->h_table, e->table_elems * sizeof(int32_t),
                               cudaMemcpyHostToDevice, e->stream));
     }
-    int best = 0;
+    int best = 0, best_bps = 0, best_walk = -1;
     double best_t = 1e300;
     gg_result r;
-    for (int w : cands) {
+    for (int w : widths) {
         if ((long long)e->rows * (w / 128) >= (1ll << 31)) continue;
-        gg_status s = plan(e, w);
-        if (s == GG_OUT_OF_MEMORY) { (void)cudaGetLastError(); continue; }  // too wide for this device
-        if (s != GG_OK) return s;
-        s = run_eval(e, e->d_table, nullptr, &r, e->stream);  // warm
-        if (s != GG_OK) return s;
-        double t = 1e300;
-        for (int k = 0; k < trials; ++k) {
-            s = run_eval(e, e->d_table, nullptr, &r, e->stream);
-            if (s != GG_OK) return s;
-            t = std::min(t, e->last_ms);
+        for (int bps : bps_opts) {
+            bool auto_walks = true;
+            for (int walk : {-1, 0}) {
+                if (walk == 0 && !auto_walks) continue;   // the automatic plan has no walk already
+                e->bps_cap = bps;
+                e->walk_pref = walk;
+                gg_status s = plan(e, w);
+                if (s == GG_OUT_OF_MEMORY) { (void)cudaGetLastError(); break; }  // too wide for this device
+                if (s != GG_OK) return s;
+                if (walk == -1) auto_walks = e->walk_K > 0;
+                s = run_eval(e, e->d_table, nullptr, &r, e->stream);  // warm
+                if (s != GG_OK) return s;
+                double t = 1e300;
+                for (int k = 0; k < trials; ++k) {
+                    s = run_eval(e, e->d_table, nullptr, &r, e->stream);
+                    if (s != GG_OK) return s;
+                    t = std::min(t, e->last_ms);
+                }
+                if (t < best_t) { best_t = t; best = w; best_bps = bps; best_walk = walk; }
+            }
         }
-        if (t < best_t) { best_t = t; best = w; }
     }
     if (!best) return fail(GG_OUT_OF_MEMORY, "no batch width fits");
+    e->bps_cap = best_bps;
+    e->walk_pref = best_walk;
     gg_status s = plan(e, best);
     if (s != GG_OK) return s;
-    {
-        std::lock_guard<std::mutex> lk(g_tune_mu);
-        g_tuned[{e->device, e->form, e->rows, e->d, n_src}] = best;
-    }
+    gg::tune_put(engine_tune_key(e), {best, best_bps, best_walk});
     if (best_sources) *best_sources = best;
     if (best_ms) *best_ms = best_t;
+    return GG_OK;
+}
+
+gg_status gg_engine_plan(gg_engine *e, int *batch_sources, int *blocks_per_sm, int *walk_levels) {
+    if (!e) return fail(GG_BAD_ARG, "null engine");
+    if (batch_sources) *batch_sources = e->batch_bits;
+    if (blocks_per_sm) *blocks_per_sm = e->grid;
+    if (walk_levels) *walk_levels = e->walk_K;
+    int sms = 0;
+    if (blocks_per_sm && cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, e->device) == cudaSuccess &&
+        sms > 0)
+        *blocks_per_sm = (e->grid + sms - 1) / sms;
+    else
+        (void)cudaGetLastError();
     return GG_OK;
 }
 

@@ -2,6 +2,8 @@
 // part of the C ABI; hidden symbols).
 #pragma once
 #include <cstdint>
+#include <string>
+#include <vector>
 #include <cuda_runtime.h>
 
 #include "gg.h"
@@ -18,6 +20,12 @@ struct EvalExtra {
 };
 
 __attribute__((visibility("hidden"))) void set_last_error(const char *msg);
+
+// Autotuner cache (gg_tune.cpp): key = GPU name and SM count, evaluator, shape.
+__attribute__((visibility("hidden"))) std::string tune_key(int device, const char *what,
+                                                         const std::vector<long long> &dims);
+__attribute__((visibility("hidden"))) bool tune_get(const std::string &key, std::vector<int> *vals);
+__attribute__((visibility("hidden"))) void tune_put(const std::string &key, const std::vector<int> &vals);
 
 // One evaluation of `e` on the device table `d_table` (on stream `st`, blocking),
 // with the extra options `x` (nullptr: none).

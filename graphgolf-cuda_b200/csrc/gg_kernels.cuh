@@ -118,6 +118,15 @@ struct BfsArgs {
     int nplanes;
     unsigned plane_cols;
     unsigned long long plane_stride;
+    // Walk pass (see walk_rows): levels 1..walk_K of every batch computed from the
+    // walk ends of each row instead of phase 0 and pull/push levels.  0: off.
+    // Needs the batch's counts zeroed by the host (blocks add into them before any
+    // grid barrier), h2 when walk_K >= 3, and walk buffers in dynamic shared
+    // memory at byte offset walk_smem_off.
+    int walk_K;
+    int walk_rpg;             // rows per group: lcm(nC, 32) / nC
+    unsigned walk_smem_off;
+    const int32_t *h2;
 };
 
 // Where a level's new pairs go in the distance planes.
@@ -496,6 +505,238 @@ static __device__ __noinline__ void phase0_tiles(const int32_t *inv, const int s
     }
 }
 
+// ---------------------------------------------------------------------------
+// Walk pass: phase 0 and levels 1..K of a batch in one pass over the rows.
+//
+// Pull BFS gives V_L[v] = V_{L-1}[v] | OR_{u in adj[v]} V_{L-1}[u], so by
+// induction V_L[v] holds exactly the sources whose vertex is the end of some
+// walk of length <= L from v along the pull table (adj[v], adj[adj[v]], ...),
+// for any table, symmetric or not.  The first levels of a batch touch few pairs
+// (about d^L per source) but a pull level still visits every chunk; instead one
+// warp enumerates the walk ends of its row level by level, keeps the sources of
+// the batch among them (a compare per end: consecutive source ids, or the inverse
+// list of the lifted forms' representatives), and sets their bits in a
+// shared-memory copy of the row with atomicOr, whose returned old word tells
+// whether a pair is new at this level: the level counts are exact.  The row is
+// then written once: V = V_K with the padding bits, the level-(K+1) frontier
+// F = V_K & ~V_{K-1} (every chunk, zeros included) and its flag words.
+//
+// Walk ends per row: level 1 = adj[v] (d), level 2 = H2[v] = adj of adj[v] (d^2,
+// precomputed once per evaluation into `h2` when K >= 3, else read row by row),
+// level 3 = H2 of adj[v] (d^3), level 4 = H2 of H2[v] (d^4).  K is chosen on the
+// host so that d + ... + d^K stays a few hundred.
+//
+// Rows go to warps in groups of whole rows that also cover whole 32-chunk tiles
+// (lcm(nC, 32) chunks), so that each flag word has one writer.
+// ---------------------------------------------------------------------------
+struct WalkArgs {
+    const int32_t *adj;       // [rows][d]
+    const int32_t *h2;        // [rows][d*d] or nullptr (K <= 2)
+    const int32_t *inv;       // source index of each vertex (-1: none), or nullptr
+    int src_first, first, ns; // source j of the batch is vertex src_first + first + j (inv == nullptr)
+    uint4 *V, *F;             // visited bits (V_K), frontier of level K+1
+    uint32_t *fl;             // flag words of F
+    int rows, d, nC, K;
+    unsigned items;
+    int rows_per_group;       // lcm(nC, 32) / nC
+};
+
+constexpr int kWalkList = 64;     // per-warp list of level-2 walk ends (level-4 parents)
+constexpr int kWalkMaxNC = 64;    // row width (uint4 chunks) the per-warp buffers hold
+
+// Shared-memory bytes of the walk buffers of one block.
+__host__ __device__ constexpr int walk_smem_per_warp(int nC) {
+    return nC * 16 * 2 + kWalkMaxNC * 4 + kWalkList * 4;
+}
+
+// Test one walk end w at level L: a new pair when w is a source of the batch whose
+// bit is not set in the row yet.
+__device__ __forceinline__ void walk_test(const WalkArgs &w, const int32_t end, const int L,
+                                          uint32_t *Vb, uint32_t *Fb, unsigned (&cnt)[4]) {
+    const int g = w.inv ? __ldg(w.inv + end) : end - w.src_first;
+    const int j = g - w.first;
+    if (g >= 0 && (unsigned)j < (unsigned)w.ns) {
+        const uint32_t bit = 1u << (j & 31);
+        const uint32_t old = atomicOr(Vb + (j >> 5), bit);
+        if (!(old & bit)) {
+            cnt[L - 1] += 1u;
+            if (L == w.K) atomicOr(Fb + (j >> 5), bit);
+        }
+    }
+}
+
+template <int D>
+static __device__ __noinline__ void walk_rows(const WalkArgs &w, unsigned char *smem, const unsigned gwarp,
+                                              const unsigned nwarps, unsigned long long *s_cnt) {
+    const unsigned lane = threadIdx.x & 31u;
+    const int d = D > 0 ? D : w.d;
+    const int dd = d * d;
+    const int nw = w.nC * 4;  // u32 words per row
+    unsigned char *mine = smem + (size_t)(threadIdx.x >> 5) * walk_smem_per_warp(w.nC);
+    uint32_t *Vb = reinterpret_cast<uint32_t *>(mine);
+    uint32_t *Fb = Vb + nw;
+    uint32_t *flw = Fb + nw;
+    int32_t *list2 = reinterpret_cast<int32_t *>(flw + kWalkMaxNC);
+    unsigned cnt[4] = {0u, 0u, 0u, 0u};
+    const int gchunks = w.rows_per_group * w.nC;       // a multiple of 32
+    const int gwords = gchunks >> 5;
+    const unsigned ngroups = (unsigned)((w.rows + w.rows_per_group - 1) / w.rows_per_group);
+    for (unsigned grp = gwarp; grp < ngroups; grp += nwarps) {
+        for (int k = (int)lane; k < gwords; k += 32) flw[k] = 0u;
+        for (int r = 0; r < w.rows_per_group; ++r) {
+            const int v = (int)grp * w.rows_per_group + r;
+            if (v >= w.rows) break;
+            // the row starts as its padding bits and the diagonal
+            for (int c = (int)lane; c < w.nC; c += 32) {
+                const uint4 p = pad_mask(c, w.ns);
+                Vb[4 * c] = p.x; Vb[4 * c + 1] = p.y; Vb[4 * c + 2] = p.z; Vb[4 * c + 3] = p.w;
+                Fb[4 * c] = Fb[4 * c + 1] = Fb[4 * c + 2] = Fb[4 * c + 3] = 0u;
+            }
+            __syncwarp();
+            if (lane == 0) {
+                const int g = w.inv ? __ldg(w.inv + v) : v - w.src_first;
+                const int j = g - w.first;
+                if (g >= 0 && (unsigned)j < (unsigned)w.ns) Vb[j >> 5] |= 1u << (j & 31);
+            }
+            __syncwarp();
+            const int32_t *arow = w.adj + (size_t)v * d;
+            // level 1: the row's own neighbours
+            for (int i = (int)lane; i < d; i += 32) walk_test(w, __ldg(arow + i), 1, Vb, Fb, cnt);
+            __syncwarp();
+            if (w.K >= 2) {
+                // level 2: adj of adj[v] (H2[v] when precomputed); kept as the
+                // parents of level 4
+                if constexpr (D > 0 && (D * D) % 4 == 0) {
+                    if (w.h2) {
+                        constexpr int U = D * D / 4;  // uint4 per H2 row
+                        const uint4 *src = reinterpret_cast<const uint4 *>(w.h2 + (size_t)v * dd);
+#pragma unroll
+                        for (int i0 = 0; i0 < U; i0 += 32) {
+                            const int i = i0 + (int)lane;
+                            if (i < U) {
+                                const uint4 q = __ldg(src + i);
+                                if (w.K >= 4 && 4 * i + 3 < kWalkList) {
+                                    list2[4 * i] = q.x; list2[4 * i + 1] = q.y;
+                                    list2[4 * i + 2] = q.z; list2[4 * i + 3] = q.w;
+                                }
+                                walk_test(w, q.x, 2, Vb, Fb, cnt); walk_test(w, q.y, 2, Vb, Fb, cnt);
+                                walk_test(w, q.z, 2, Vb, Fb, cnt); walk_test(w, q.w, 2, Vb, Fb, cnt);
+                            }
+                        }
+                    } else {
+                        // D*D ends from the D neighbour rows, 16 bytes at a time
+                        constexpr int R = D / 4 > 0 ? D / 4 : 1;   // uint4 per adjacency row (D % 4 == 0)
+                        if constexpr (D % 4 == 0) {
+                            constexpr int U = D * R;
+                            uint4 q[(U + 31) / 32];
+#pragma unroll
+                            for (int s = 0; s < (U + 31) / 32; ++s) {
+                                const int i = s * 32 + (int)lane;
+                                q[s] = make_uint4(0u, 0u, 0u, 0u);
+                                if (i < U) {
+                                    const int p = __ldg(arow + i / R);
+                                    q[s] = __ldg(reinterpret_cast<const uint4 *>(w.adj + (size_t)p * D) + i % R);
+                                }
+                            }
+#pragma unroll
+                            for (int s = 0; s < (U + 31) / 32; ++s) {
+                                const int i = s * 32 + (int)lane;
+                                if (i < U) {
+                                    walk_test(w, q[s].x, 2, Vb, Fb, cnt); walk_test(w, q[s].y, 2, Vb, Fb, cnt);
+                                    walk_test(w, q[s].z, 2, Vb, Fb, cnt); walk_test(w, q[s].w, 2, Vb, Fb, cnt);
+                                }
+                            }
+                        } else {
+                            for (int i = (int)lane; i < dd; i += 32)
+                                walk_test(w, __ldg(w.adj + (size_t)__ldg(arow + i / d) * d + i % d), 2, Vb, Fb, cnt);
+                        }
+                    }
+                } else {
+                    for (int i = (int)lane; i < dd; i += 32) {
+                        const int32_t e = w.h2 ? __ldg(w.h2 + (size_t)v * dd + i)
+                                               : __ldg(w.adj + (size_t)__ldg(arow + i / d) * d + i % d);
+                        if (w.K >= 4 && i < kWalkList) list2[i] = e;
+                        walk_test(w, e, 2, Vb, Fb, cnt);
+                    }
+                }
+                __syncwarp();
+            }
+            if (w.K >= 3) {
+                // level 3: H2 of each neighbour (d * d^2 ends)
+                if constexpr (D > 0 && D <= 8 && (D * D) % 4 == 0) {
+                    constexpr int Q = D * D / 4;   // uint4 per H2 row
+                    constexpr int U = D * Q;
+                    constexpr int S = (U + 31) / 32;
+                    uint4 q[S];
+#pragma unroll
+                    for (int s = 0; s < S; ++s) {
+                        const int i = s * 32 + (int)lane;
+                        q[s] = make_uint4(0u, 0u, 0u, 0u);
+                        if (i < U) {
+                            const int p = __ldg(arow + i / Q);
+                            q[s] = __ldg(reinterpret_cast<const uint4 *>(w.h2 + (size_t)p * dd) + i % Q);
+                        }
+                    }
+#pragma unroll
+                    for (int s = 0; s < S; ++s) {
+                        const int i = s * 32 + (int)lane;
+                        if (i < U) {
+                            walk_test(w, q[s].x, 3, Vb, Fb, cnt); walk_test(w, q[s].y, 3, Vb, Fb, cnt);
+                            walk_test(w, q[s].z, 3, Vb, Fb, cnt); walk_test(w, q[s].w, 3, Vb, Fb, cnt);
+                        }
+                    }
+                } else {
+                    const int n3 = d * dd;
+                    for (int i = (int)lane; i < n3; i += 32)
+                        walk_test(w, __ldg(w.h2 + (size_t)__ldg(arow + i / dd) * dd + i % dd), 3, Vb, Fb, cnt);
+                }
+                __syncwarp();
+            }
+            if (w.K >= 4) {
+                // level 4: H2 of each level-2 end (d^2 * d^2 ends; d^2 <= kWalkList)
+                const int n4 = dd * dd;
+                for (int i = (int)lane; i < n4; i += 32)
+                    walk_test(w, __ldg(w.h2 + (size_t)list2[i / dd] * dd + i % dd), 4, Vb, Fb, cnt);
+                __syncwarp();
+            }
+            // write the row: V = V_K (padding included), F = new at level K, flag bits
+            const unsigned t0 = (unsigned)v * (unsigned)w.nC;
+            const unsigned b0 = (unsigned)r * (unsigned)w.nC;   // chunk index within the group
+            for (int c = (int)lane; c < w.nC; c += 32) {
+                const uint4 vv = make_uint4(Vb[4 * c], Vb[4 * c + 1], Vb[4 * c + 2], Vb[4 * c + 3]);
+                const uint4 ff = make_uint4(Fb[4 * c], Fb[4 * c + 1], Fb[4 * c + 2], Fb[4 * c + 3]);
+                w.V[t0 + c] = vv;
+                w.F[t0 + c] = ff;
+                if (u4any(ff)) atomicOr(flw + ((b0 + c) >> 5), 1u << ((b0 + c) & 31u));
+            }
+            __syncwarp();
+        }
+        // the group's flag words (the group starts on a tile boundary)
+        const unsigned tile0 = grp * (unsigned)gwords;
+        const unsigned ntiles = (w.items + 31u) >> 5;
+        for (int k = (int)lane; k < gwords; k += 32)
+            if (tile0 + k < ntiles) w.fl[tile0 + k] = flw[k];
+        __syncwarp();
+    }
+#pragma unroll
+    for (int L = 0; L < 4; ++L) {
+        const unsigned s = __reduce_add_sync(0xffffffffu, cnt[L]);
+        if (lane == 0 && s) atomicAdd(s_cnt + L, (unsigned long long)s);
+    }
+}
+
+// H2[v][i*d + j] = adj[adj[v][i]][j]: the level-2 walk ends of every row, built once
+// per evaluation (after the table's range check: a bad table builds nothing).
+static __global__ void h2_kernel(const int32_t *adj, int32_t *h2, int rows, int d, const int *bad) {
+    if (bad && *bad) return;
+    const long long dd = (long long)d * d, n = (long long)rows * dd;
+    for (long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x; k < n;
+         k += (long long)gridDim.x * blockDim.x) {
+        const long long v = k / dd, r = k % dd;
+        h2[k] = __ldg(adj + (size_t)__ldg(adj + v * d + r / d) * d + r % d);
+    }
+}
+
 // Resident blocks per SM the register allocation targets: 6 (40 registers)
 // fits the small degrees without spills, 4 (64 registers) the larger ones.
 #ifndef GG_MIN_BLOCKS_SMALL_D
@@ -518,7 +759,68 @@ struct LoopState {
     int wrote_all_prev;          // the previous level wrote F whole
     int nf_valid;                // a.nf describes V as the previous level left it
     int done;                    // the batch's level loop ends
+    int L_next;                  // first level the level loop runs (after a walk pass)
 };
+
+// The walk pass of batch b, its counts and the loop state it leaves (levels
+// 1..K done; S.L_next = K + 1, or the level at which the batch ended).  Out of
+// line so that the level loop keeps its registers.  Returns the barrier count
+// after the pass, or kWaitGaveUp when a barrier wait gave up.
+constexpr unsigned kWaitGaveUp = 0xffffffffu;
+template <int D>
+static __device__ __noinline__ unsigned walk_batch(const BfsArgs &a, const int b, const int ns, const int d,
+                                                   const unsigned items, const unsigned gtid, const unsigned nthr,
+                                                   unsigned epoch, LoopState &S) {
+    extern __shared__ int32_t s_adj[];
+    // Levels 1..K from the walk ends of every row (walk_rows): the counts
+    // were zeroed by the host, so blocks add into them right away.
+    __shared__ unsigned long long s_wcnt[4];
+    unsigned long long *counts = a.counts + (size_t)b * (size_t)a.stride;
+    if (threadIdx.x < 4) s_wcnt[threadIdx.x] = 0ull;
+    if (blockIdx.x == 0 && threadIdx.x == 0) counts[0] = (unsigned long long)ns;
+    if (b == 0 && a.level_ns && gtid == 0) a.level_ns[0] = gtimer();
+    const int K = a.walk_K;
+    // the pass's arguments in shared memory (one copy per block, not a
+    // by-value struct on every thread's stack)
+    __shared__ WalkArgs w;
+    if (threadIdx.x == 0) {
+        w.adj = a.adj; w.h2 = a.h2; w.inv = a.inv;
+        w.src_first = a.src_first; w.first = a.src_begin + b * 128 * a.nC; w.ns = ns;
+        w.V = a.V;
+        w.F = ((K + 1) & 1) ? a.F0 : a.F1;     // what level K + 1 reads
+        w.fl = ((K + 1) & 1) ? a.fl0 : a.fl1;
+        w.rows = a.rows; w.d = d; w.nC = a.nC; w.K = K; w.items = items;
+        w.rows_per_group = a.walk_rpg;
+    }
+    __syncthreads();
+    walk_rows<D>(w, reinterpret_cast<unsigned char *>(s_adj) + a.walk_smem_off, gtid >> 5, nthr >> 5,
+                 s_wcnt);
+    __syncthreads();
+    if (threadIdx.x == 0)
+        for (int L = 1; L <= K; ++L)
+            if (s_wcnt[L - 1]) atomicAdd(counts + L, s_wcnt[L - 1]);
+    if (!grid_sync(a.ctl, a.expected, a.wait_ns, 0, epoch)) return kWaitGaveUp;
+    if (threadIdx.x == 0) {
+        S.pairs = (unsigned long long)ns * (unsigned long long)a.rows;
+        S.reached = (unsigned long long)ns;
+        S.in_p = -1;
+        S.wrote_all_prev = 1;
+        S.nf_valid = 0;
+        S.done = 0;
+        int L = 1;
+        for (; L <= K; ++L) {
+            const unsigned long long cL = ld_relaxed_u64(counts + L);
+            S.reached += cL;
+            S.c_prev = cL;
+            if (cL == 0ull || L >= a.max_levels || S.reached == S.pairs) { S.done = 1; break; }
+        }
+        S.L_next = S.done ? L : K + 1;
+        if (b == 0 && a.level_ns && blockIdx.x == 0)
+            for (int k = 1; k <= K; ++k) a.level_ns[k] = gtimer();
+    }
+    __syncthreads();
+    return epoch;
+}
 
 // One cooperative launch = every source batch of an evaluation, all levels.
 //
@@ -527,7 +829,7 @@ struct LoopState {
 // levels, each ended by a grid barrier.  One launch instead of one per batch
 // saves the launch gap and the shared-memory adjacency reload per batch.
 template <int D, bool PL>
-__global__ void __launch_bounds__(kBlock, min_blocks_for(D)) bfs_batch_kernel(const BfsArgs a) {
+__global__ void __launch_bounds__(kBlock, min_blocks_for(D)) bfs_batch_kernel(const __grid_constant__ BfsArgs a) {
     const int d = D > 0 ? D : a.d;
     const unsigned lane = threadIdx.x & 31u;
     const unsigned gtid = blockIdx.x * blockDim.x + threadIdx.x;
@@ -565,7 +867,7 @@ __global__ void __launch_bounds__(kBlock, min_blocks_for(D)) bfs_batch_kernel(co
     // levels visit).
     if (threadIdx.x == 0) {
         S.push_on = D > 0 && 32 % D == 0 && a.push_ppm > 0 && a.P0 != nullptr && a.asym != nullptr &&
-                    a.masks == nullptr;
+                    a.masks == nullptr && (PL || a.walk_K == 0);
         S.dirty_p = -1;
     }
     __syncthreads();
@@ -583,10 +885,15 @@ __global__ void __launch_bounds__(kBlock, min_blocks_for(D)) bfs_batch_kernel(co
         __syncthreads();
     }
 
+    const bool walk = !PL && a.walk_K > 0;
     for (int b = 0; b < a.nb; ++b) {
         const int ns = min(128 * a.nC, a.ns_total - b * 128 * a.nC);
         if (a.batch_ns && gtid == 0) a.batch_ns[2 * b] = gtimer();
-        {
+        if (walk) {
+            epoch = walk_batch<D>(a, b, ns, d, items, gtid, nthr, epoch, S);
+            if (epoch == kWaitGaveUp) return;
+        } else {
+            if (threadIdx.x == 0) S.L_next = 1;
             // Phase 0 (cudaASPLconv.cu:9-33): counters zeroed, padding bits and
             // the diagonal visited, the diagonal as the level-1 frontier.  The
             // sources of a batch are distinct vertices, so a chunk holds at most
@@ -623,10 +930,14 @@ __global__ void __launch_bounds__(kBlock, min_blocks_for(D)) bfs_batch_kernel(co
             }
             __syncthreads();
         }
-        if (b == 0 && a.level_ns && gtid == 0) a.level_ns[0] = gtimer();
+        if (!walk && b == 0 && a.level_ns && gtid == 0) a.level_ns[0] = gtimer();
 
         int L = 1;
         for (;; ++L) {
+            // levels a walk pass already computed; a batch the walk finished
+            // ends at its last level
+            if (L < S.L_next) continue;
+            if (S.done) break;
             // Per-level access modes.  Every block derives them from the same level
             // counts (read after the barrier), so writer and reader always agree:
             //  * push(L): top-down from the push buffer while the frontier feeding

@@ -463,6 +463,10 @@ gg_status ensure_counts(gg_lift *h, size_t entries) {
     return GG_OK;
 }
 
+std::string lift_tune_key(const gg_lift *h) {
+    return gg::tune_key(h->device, "lift", {h->axes, h->n[0], h->n[1], h->n[2], h->m[0], h->m[1], h->m[2], h->d});
+}
+
 gg_status alloc_group(gg_lift *h, int groups) {
     cudaFree(h->V); cudaFree(h->F0); cudaFree(h->F1);
     h->V = h->F0 = h->F1 = nullptr;
@@ -523,6 +527,13 @@ gg_status lift_open(int axes, const int n_in[3], const int m_in[3], int degree, 
     // items N * W must stay below 2^31
     const long long by_items = std::max(1ll, (1ll << 31) / ((long long)h->N * h->cpc));
     h->g_auto = (int)std::min<long long>({(long long)fit, (long long)kMaxGroup, by_items});
+    {
+        // a group recorded by gg_lift_autotune for this lift shape on this kind of GPU
+        std::vector<int> tuned;
+        if (gg::tune_get(lift_tune_key(h), &tuned) && !tuned.empty() && tuned[0] >= 1 &&
+            tuned[0] <= kMaxGroup && tuned[0] <= by_items)
+            h->g_auto = tuned[0];
+    }
     cudaError_t e = cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking);
     if (e == cudaSuccess) e = cudaEventCreate(&h->ev0);
     if (e == cudaSuccess) e = cudaEventCreate(&h->ev1);
@@ -597,6 +608,44 @@ gg_status gg_lift_set_group(gg_lift *h, int group) {
         if (s != GG_OK) return s;
     }
     h->group = group;
+    return GG_OK;
+}
+
+gg_status gg_lift_autotune(gg_lift *h, int n_cand, const gg_lift_edit *edits, int max_levels, int trials,
+                           int *best_group, double *best_ms) {
+    if (!h || n_cand < 1 || !edits || trials < 1 || max_levels < 0) return lfail(GG_BAD_ARG, "bad arguments");
+    if (!h->base_set) return lfail(GG_BAD_ARG, "no base table set");
+    std::vector<gg_cand_result> out((size_t)n_cand);
+    const int keep = h->group;
+    int best = 0;
+    double best_t = 1e300;
+    const long long by_items = std::max(1ll, (1ll << 31) / ((long long)h->N * h->cpc));
+    for (int G = 1; G <= std::min<long long>({(long long)kMaxGroup, by_items, (long long)n_cand}); ++G) {
+        if (G > 12 && G != 16 && G != 24 && G != 32) continue;
+        gg_status s = gg_lift_set_group(h, G);
+        if (s == GG_OUT_OF_MEMORY) { (void)cudaGetLastError(); break; }
+        if (s != GG_OK) return s;
+        s = gg_lift_eval(h, n_cand, edits, max_levels, out.data());  // warm
+        if (s == GG_BAD_ARG) break;  // more chunk columns than threads: larger groups fail too
+        if (s != GG_OK) return s;
+        double t = 1e300;
+        for (int k = 0; k < trials; ++k) {
+            s = gg_lift_eval(h, n_cand, edits, max_levels, out.data());
+            if (s != GG_OK) return s;
+            t = std::min(t, (double)h->last_ms);
+        }
+        if (t < best_t) { best_t = t; best = G; }
+    }
+    if (!best) {
+        gg_lift_set_group(h, keep);
+        return lfail(GG_OUT_OF_MEMORY, "no group fits");
+    }
+    gg::tune_put(lift_tune_key(h), {best});
+    h->g_auto = best;
+    gg_status s = gg_lift_set_group(h, 0);
+    if (s != GG_OK) return s;
+    if (best_group) *best_group = best;
+    if (best_ms) *best_ms = best_t;
     return GG_OK;
 }
 

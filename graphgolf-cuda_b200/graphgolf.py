@@ -97,6 +97,11 @@ _SIGS = {
     "gg_autotune": [_P, _P, _I, _IP, _DP],
     "gg_set_wait_limit_ms": [_P, _I],
     "gg_gather_peak": [_I, _I, _I, _I, _DP, _DP],
+    "gg_engine_plan": [_P, _IP, _IP, _IP],
+    "gg_set_tune_cache": [ctypes.c_char_p],
+    "gg_batch_autotune": [_P, _I, _P, _I, _DP],
+    "gg_batch_chunk": [_P, _I, _IP],
+    "gg_lift_autotune": [_P, _I, _P, _I, _I, _IP, _DP],
     "gg_destroy": [_P],
     "gg_graph_eval_noalloc": [_P, _I, _I, _I, _P, _P],
     "gg_batch_create": [_I, _EPP],
@@ -600,6 +605,12 @@ class Engine:
     def set_wait_limit_ms(self, ms):
         _check(lib().gg_set_wait_limit_ms(self._h, ms))
 
+    def plan(self):
+        """(sources per batch, resident blocks per SM, walk levels) of the current plan."""
+        a, b, c = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+        _check(lib().gg_engine_plan(self._h, ctypes.byref(a), ctypes.byref(b), ctypes.byref(c)))
+        return a.value, b.value, c.value
+
     def close(self):
         if self._h:
             lib().gg_destroy(self._h)
@@ -732,6 +743,11 @@ def gen_swaps(adj, base_id, count, seed):
     return out
 
 
+def set_tune_cache(path):
+    """Tuning cache file of every autotuner (gg_set_tune_cache); None or "": none."""
+    _check(lib().gg_set_tune_cache(path.encode() if path else None))
+
+
 def gather_peak(rows=65536, degree=8, iters=20, device=0):
     """Ceiling of a dense BFS level (gg_gather_peak): -> (GB/s, ms per pass) of
     rows x (degree + 1) random 512-byte row reads and one row write."""
@@ -859,6 +875,19 @@ class Batch:
         _check(lib().gg_batch_eval_device(self._h, n, ctypes.c_void_p(d_swaps), ctypes.c_void_p(d_out),
                                           ctypes.c_void_p(stream)))
 
+    def autotune(self, swaps, trials=3):
+        """Tune each used base's chunk width on these candidates (gg_batch_autotune);
+        returns the fastest launch in ms."""
+        swaps = np.ascontiguousarray(swaps, dtype=SWAP_DTYPE)
+        ms = ctypes.c_double()
+        _check(lib().gg_batch_autotune(self._h, len(swaps), _ptr(swaps), trials, ctypes.byref(ms)))
+        return ms.value
+
+    def chunk(self, base_id):
+        s = ctypes.c_int()
+        _check(lib().gg_batch_chunk(self._h, base_id, ctypes.byref(s)))
+        return s.value
+
     def device_status(self, stream=0):
         """Wait for `stream`; raise GGError(GG_BAD_ARG) if the last device launch
         rejected a candidate (gg_batch_device_status)."""
@@ -963,6 +992,14 @@ class Lift:
 
     def set_group(self, group):
         _check(lib().gg_lift_set_group(self._h, group))
+
+    def autotune(self, edits, max_levels=0, trials=3):
+        """Tune the group size on these edits (gg_lift_autotune) -> (group, ms)."""
+        edits = np.ascontiguousarray(edits, dtype=LIFT_EDIT_DTYPE)
+        g, ms = ctypes.c_int(), ctypes.c_double()
+        _check(lib().gg_lift_autotune(self._h, len(edits), _ptr(edits), max_levels, trials, ctypes.byref(g),
+                                      ctypes.byref(ms)))
+        return g.value, ms.value
 
     def group(self):
         g = ctypes.c_int()

@@ -140,13 +140,26 @@ gg_status gg_last_transfer_bytes(gg_engine *e, uint64_t *h2d, uint64_t *d2h);
 
 /* Tuning: source-batch width in bits (multiple of 128; 0 = automatic). */
 gg_status gg_set_batch_sources(gg_engine *e, int sources);
-/* Autotuner: times `trials` evaluations of `table` for each candidate source-batch
- * width (fractions and multiples of the L2-resident width, and all sources at once),
- * keeps the fastest in this engine's plan and records it for engines of the same
- * form, size and degree created later in the process.  best_sources / best_ms may be
- * NULL. */
+/* Autotuner: times `trials` evaluations of `table` for each candidate launch shape
+ * -- source-batch width (fractions and multiples of the L2-resident width, and all
+ * sources at once) x resident blocks per SM (as many as fit, one and two fewer) x
+ * the walk pass (automatic depth, or off) -- keeps the fastest in this engine's
+ * plan and records it in the tuning cache (see gg_set_tune_cache) for engines of the
+ * same form, size, degree and source count on the same kind of GPU, in this process
+ * and later ones.  best_sources / best_ms may be NULL. */
 gg_status gg_autotune(gg_engine *e, const int32_t *table, int trials, int *best_sources,
                       double *best_ms);
+/* The engine's current plan: sources per batch, resident blocks per SM, levels the
+ * walk pass computes (0: none).  Any output may be NULL. */
+gg_status gg_engine_plan(gg_engine *e, int *batch_sources, int *blocks_per_sm, int *walk_levels);
+/* Tuning cache file (no reference counterpart): tuned launch shapes of every
+ * evaluator (gg_autotune, gg_batch_autotune, gg_lift_autotune), one line per
+ * (GPU name and SM count, evaluator, shape), read when an evaluator plans and
+ * rewritten (atomically) when a tuner records a shape.  Default: GG_TUNE_CACHE
+ * ("off": none), else $XDG_CACHE_HOME/graphgolf-b200/tune.tsv or
+ * ~/.cache/graphgolf-b200/tune.tsv.  path NULL or "": keep tuned shapes in this
+ * process only. */
+gg_status gg_set_tune_cache(const char *path);
 /* Bounded-wait limit of the in-kernel grid barrier, in milliseconds. */
 gg_status gg_set_wait_limit_ms(gg_engine *e, int ms);
 
@@ -218,8 +231,16 @@ gg_status gg_batch_add_base(gg_batch *b, int n, int degree, const int32_t *adj, 
 /* Replace a registered base graph's adjacency (same n and degree), e.g. after an
  * annealer accepted a move. */
 gg_status gg_batch_set_base(gg_batch *b, int base_id, const int32_t *adj);
-/* Source bits per shared-memory task for a base (multiple of 128; 0 = automatic). */
+/* Source bits per shared-memory task for a base (128 * 2^k). */
 gg_status gg_batch_set_chunk(gg_batch *b, int base_id, int sources);
+/* Current source bits per task of a base. */
+gg_status gg_batch_chunk(gg_batch *b, int base_id, int *sources);
+/* Autotuner: for each base the candidates use, times `trials` launches of the
+ * candidates with each chunk width that fits (the other bases fixed), keeps the
+ * fastest and records it in the tuning cache (gg_set_tune_cache) for bases of the
+ * same size and degree added later, in this process and later ones on the same
+ * kind of GPU.  best_ms (may be NULL) = the fastest launch. */
+gg_status gg_batch_autotune(gg_batch *b, int n_cand, const gg_swap *cands, int trials, double *best_ms);
 /* Host arrays in and out; blocking.  The launch for a given candidate count is
  * captured once in a CUDA graph and replayed. */
 gg_status gg_batch_eval(gg_batch *b, int n_cand, const gg_swap *cands, gg_cand_result *out);
@@ -312,6 +333,12 @@ gg_status gg_lift_eval(gg_lift *h, int n_cand, const gg_lift_edit *edits, int ma
  * keep the round's bitsets within half of the L2). */
 gg_status gg_lift_set_group(gg_lift *h, int group);
 gg_status gg_lift_group(gg_lift *h, int *group);
+/* Autotuner: times `trials` evaluations of the edits for each group size, keeps the
+ * fastest as this handle's automatic group and records it in the tuning cache
+ * (gg_set_tune_cache) for lifts of the same form, sizes and degree created later on
+ * the same kind of GPU.  best_group / best_ms may be NULL. */
+gg_status gg_lift_autotune(gg_lift *h, int n_cand, const gg_lift_edit *edits, int max_levels, int trials,
+                           int *best_group, double *best_ms);
 /* Tuning: past half_ppm parts per million of a round's pairs reached, a chunk
  * gathers half its neighbours first and the rest only while it still misses
  * sources (default 850000; 1000000 = never). */

@@ -9,6 +9,12 @@ import sys
 import pytest
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+# Autotuners record launch shapes in a cache file; the tests use a file of their
+# own (one per session) instead of the user's cache directory.
+if "GG_TUNE_CACHE" not in os.environ:
+    import tempfile
+    os.environ["GG_TUNE_CACHE"] = os.path.join(tempfile.mkdtemp(prefix="gg_tune_"), "tune.tsv")
 for p in (ROOT, os.path.join(ROOT, "graphgolf-cuda_b200"), os.path.join(ROOT, "oracle"),
           os.path.join(ROOT, "tests")):
     if p not in sys.path:

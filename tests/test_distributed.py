@@ -128,3 +128,26 @@ def test_two_gloo_ranks_gather_candidate_results(count):
         assert p.exitcode == 0
     whole = lift_oracle_eval(N, M, T)(moves).tobytes()
     assert out[0] == whole and out[1] == whole
+
+
+def test_bench_gpus_flag_starts_one_rank_per_gpu(monkeypatch):
+    """`bench.py --gpus N` outside torchrun re-runs itself as N ranks with
+    torch.distributed.run on 127.0.0.1, passing every argument through."""
+    import sys
+    import types
+    import bench
+    calls = []
+
+    def fake_run(cmd, timeout):
+        calls.append(cmd)
+        return types.SimpleNamespace(returncode=0)
+
+    monkeypatch.delenv("WORLD_SIZE", raising=False)
+    monkeypatch.setattr(bench.subprocess, "run", fake_run)
+    monkeypatch.setattr(sys, "argv", ["bench.py", "--gpus", "4", "--steps", "3", "--workload",
+                                      "regular_n65536_d8_sharded"])
+    assert bench.main() == 0
+    cmd = calls[0]
+    assert cmd[1:3] == ["-m", "torch.distributed.run"]
+    assert "--nproc-per-node=4" in cmd and "127.0.0.1" in cmd and "--nnodes=1" in cmd
+    assert cmd[-6:] == ["--gpus", "4", "--steps", "3", "--workload", "regular_n65536_d8_sharded"]

@@ -1,0 +1,109 @@
+"""Walk pass of the single-graph engine: levels 1..K of every source batch
+computed from the walk ends of each row (bfs_batch_kernel's walk_rows) must give
+exactly the counts of the level-by-level BFS, on every kind of table: random
+regular graphs, self-loop padding, multigraph repeats, one-way rows, the lifted
+forms (consecutive representatives and the corner tiles found through the inverse
+list), batches that end inside the walk, and level caps below K.
+
+GG_WALK_LEVELS is read when an engine plans its batches (at creation and at
+set_batch_sources): 0 turns the pass off, K > 0 forces K levels."""
+import os
+
+import numpy as np
+import pytest
+
+import graphgolf as G
+import instances as I
+import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+
+def engine_with(walk, make):
+    old = os.environ.get("GG_WALK_LEVELS")
+    os.environ["GG_WALK_LEVELS"] = str(walk)
+    try:
+        return make()
+    finally:
+        if old is None:
+            del os.environ["GG_WALK_LEVELS"]
+        else:
+            os.environ["GG_WALK_LEVELS"] = old
+
+
+def counts(e, table, cap):
+    r = e.eval(table, max_levels=cap, level_counts=True)
+    return (r["total"], r["reached"], r["levels"], r["capped"], r["connected"],
+            tuple(int(x) for x in r["level_counts"]))
+
+
+@pytest.mark.parametrize("n,d,seed,bits", [(256, 4, 1, 0), (1000, 3, 2, 256), (2000, 6, 3, 1024),
+                                           (4096, 8, 4, 4096), (3000, 8, 5, 1152), (1500, 16, 6, 512),
+                                           (777, 5, 7, 384), (2048, 12, 8, 2048)])
+@pytest.mark.parametrize("walk", [1, 2, 3, 4])
+def test_walk_equals_level_bfs_regular(n, d, seed, bits, walk):
+    if (n * d) % 2:
+        n += 1
+    adj = G.random_regular(n, d, seed) if d in (3, 4, 6, 8, 12, 16) else I.random_regular_np(n, d, seed)
+    cap = n + 1
+    off = engine_with(0, lambda: G.cudaASPLgraph(n, d, 0))
+    on = engine_with(walk, lambda: G.cudaASPLgraph(n, d, 0))
+    if bits:
+        engine_with(0, lambda: off.set_batch_sources(bits))
+        engine_with(walk, lambda: on.set_batch_sources(bits))
+    want = counts(off, adj, cap)
+    assert counts(on, adj, cap) == want
+    o = O.bfs_pull(adj, np.arange(n))
+    assert want[0] == o.total() and want[2] == o.levels
+
+
+def test_walk_default_headline_shape_vs_oracle():
+    """Default plan (walk on) for an 8-regular graph with 4096-source batches."""
+    adj = G.random_regular(8192, 8, 11)
+    e = G.cudaASPLgraph(8192, 8, 0)
+    e.set_batch_sources(4096)
+    r = e.eval(adj, max_levels=199, level_counts=True)
+    o = O.bfs_pull(adj, np.arange(8192))
+    assert r["total"] == o.total() and r["levels"] == o.levels and r["connected"]
+    assert np.array_equal(r["level_counts"][:o.levels + 1], o.level_counts[:o.levels + 1])
+
+
+@pytest.mark.parametrize("walk", [2, 3, 4])
+def test_walk_padding_repeats_one_way(walk):
+    # self-loop padding of a non-regular graph, repeated neighbours, one-way rows
+    rng = np.random.default_rng(5)
+    n, d = 900, 6
+    adj = np.repeat(np.arange(n, dtype=np.int32)[:, None], d, axis=1)
+    for v in range(n):
+        k = int(rng.integers(0, d + 1))
+        adj[v, :k] = rng.integers(0, n, size=k)
+    for cap in (n + 1, 2, 1):
+        want = counts(engine_with(0, lambda: G.cudaASPLgraph(n, d, 0)), adj, cap)
+        got = counts(engine_with(walk, lambda: G.cudaASPLgraph(n, d, 0)), adj, cap)
+        assert got == want, cap
+
+
+@pytest.mark.parametrize("walk", [1, 3, 4])
+def test_walk_batches_ending_inside_the_walk(walk):
+    for adj in (np.asarray(I.complete(9), np.int32), np.zeros((1, 2), np.int32),
+                np.asarray(I.cycle(5), np.int32), np.asarray(I.petersen(), np.int32),
+                np.asarray(I.disjoint_union(I.cycle(10), I.cycle(12)), np.int32)):
+        n, d = adj.shape
+        want = counts(engine_with(0, lambda: G.cudaASPLgraph(n, d, 0)), adj, n + 1)
+        assert counts(engine_with(walk, lambda: G.cudaASPLgraph(n, d, 0)), adj, n + 1) == want
+
+
+@pytest.mark.parametrize("walk", [2, 3])
+def test_walk_lifted_forms(walk):
+    N, M, diffs = G.cyclic_lift(256, 16, 6, 3)
+    want = engine_with(0, lambda: G.cudaASPLconv(N, M, 6, 0)).diameterASPL(diffs)
+    assert engine_with(walk, lambda: G.cudaASPLconv(N, M, 6, 0)).diameterASPL(diffs) == want
+    assert want == O.conv_diameter_aspl(N, M, diffs)
+    Nx, Ny, Mx, My, vals = G.piece_lift(8, 8, 4, 4, 4, 2)
+    want = engine_with(0, lambda: G.cudaASPLpiece(Nx, Ny, Mx, My, 4, 0)).diameterASPL(vals)
+    assert engine_with(walk, lambda: G.cudaASPLpiece(Nx, Ny, Mx, My, 4, 0)).diameterASPL(vals) == want
+    assert want == O.piece_diameter_aspl(Nx, Ny, Mx, My, vals)
+    dims_rows = I.random_box(3, 2, 2, 2, 3, 2, 6, 4)
+    dims, rows = dims_rows[:6], dims_rows[6]
+    want = engine_with(0, lambda: G.cudaASPLbox(*dims, 6, 0)).diameterASPL(rows)
+    assert engine_with(walk, lambda: G.cudaASPLbox(*dims, 6, 0)).diameterASPL(rows) == want

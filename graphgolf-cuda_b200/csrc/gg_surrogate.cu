@@ -1,14 +1,16 @@
 // gg_surrogate.cu -- the surrogate ΔASPL ranker (gg_surrogate_* in gg.h).
 //
-// All products go through one hand-written tile GEMM: 128 threads, a 64x64
-// output tile, k steps of 16; operands are read from fp32 memory through
-// arbitrary strides (so transposes cost nothing), rounded to bf16 (round to
-// nearest even) into shared memory, and multiplied with mma.sync m16n8k16
-// (bf16 in, fp32 accumulate).  Long reductions (weight gradients, K = number of
-// vertices or swaps) split K over blocks and accumulate with fp32 atomics.
-// The remaining kernels are gathers/scatters (neighbour means, the swap
-// readout), elementwise epilogues and Adam.
+// Every product rounds its operands to bf16 (round to nearest even) in shared
+// memory and multiplies with mma.sync m16n8k16 (bf16 in, fp32 accumulate), on
+// 64x64 output tiles of 128 threads.  The forward pass (graph embedding and swap
+// readout) is one cooperative launch (surrogate_forward_kernel) with a bounded
+// grid barrier per message-passing layer.  The backward pass uses a strided tile
+// GEMM (gemm_bf16_kernel; operands read from fp32 memory through arbitrary
+// strides, so transposes cost nothing; long reductions -- weight gradients over
+// the vertices or swaps -- split K over blocks with fp32 atomics), scatters,
+// elementwise epilogues and Adam.
 #include "gg.h"
+#include "gg_kernels.cuh"
 
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
@@ -131,45 +133,9 @@ __global__ void nbr_mean_kernel(const float *H, const int32_t *adj, int n, int d
     }
 }
 
-// Y = relu(Y + b)
-__global__ void bias_relu_kernel(float *Y, const float *b, long long rows, int width) {
-    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < rows * width;
-         t += (long long)gridDim.x * blockDim.x) {
-        const float y = Y[t] + b[t % width];
-        Y[t] = y > 0.f ? y : 0.f;
-    }
-}
-
 __device__ __forceinline__ void partners(const gg_swap &s, int &p, int &q) {
     p = s.mode ? s.d : s.c;  // new edges (a,p), (b,q)
     q = s.mode ? s.c : s.d;
-}
-
-// Z[p] = [Ha+Hb+Hc+Hd, Ha*Hb + Hc*Hd, Ha*Hp + Hb*Hq]
-__global__ void readout_z_kernel(const float *H, const gg_swap *sw, int P, float *Z) {
-    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < P * kH; t += gridDim.x * blockDim.x) {
-        const int p = t / kH, j = t % kH;
-        const gg_swap s = sw[p];
-        int pa, qb;
-        partners(s, pa, qb);
-        const float ha = H[(size_t)s.a * kH + j], hb = H[(size_t)s.b * kH + j];
-        const float hc = H[(size_t)s.c * kH + j], hd = H[(size_t)s.d * kH + j];
-        const float hp = H[(size_t)pa * kH + j], hq = H[(size_t)qb * kH + j];
-        float *z = Z + (size_t)p * kZ;
-        z[j] = ha + hb + hc + hd;
-        z[kH + j] = ha * hb + hc * hd;
-        z[2 * kH + j] = ha * hp + hb * hq;
-    }
-}
-
-// y[p] = O[p] . w + b0   (one warp per swap)
-__global__ void readout_out_kernel(const float *O, const float *w, const float *b0, int P, float *y) {
-    const int lane = threadIdx.x & 31;
-    for (int p = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; p < P; p += (gridDim.x * blockDim.x) >> 5) {
-        float s = O[(size_t)p * kH + lane] * w[lane] + O[(size_t)p * kH + 32 + lane] * w[32 + lane];
-        for (int o = 16; o; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
-        if (lane == 0) y[p] = s + b0[0];
-    }
 }
 
 // Per-call scalars, written by the host before each replay: [0] 1/count of
@@ -254,6 +220,190 @@ __global__ void adam_kernel(float *p, const float *g, float *m, float *v, int co
 
 int blocks_for(long long n, int per = 256) { return (int)std::min<long long>((n + per - 1) / per, 4096); }
 
+// ---------------------------------------------------------------------------
+// Fused forward: the graph embedding (H0 .. H3, with the neighbour means M0 .. M2
+// kept for the backward pass) and the readout of P swaps (Z, O, y) in one
+// cooperative launch of 128-thread blocks, with a bounded grid barrier after each
+// layer (every block needs the whole previous layer for its neighbour means).
+// A block owns 64-row tiles (vertices, then swaps).  For each tile it stages both
+// operands as bf16 in shared memory -- A (64 x K) row-major, B transposed (64 x K)
+// -- and multiplies with mma.sync m16n8k16 (fp32 accumulate), the arithmetic of
+// gemm_bf16_kernel; a layer's two products H Ws + M Wn run as one K = 128 product
+// over [H | M] and [Ws ; Wn].
+// ---------------------------------------------------------------------------
+constexpr int kFwdBlock = 128;
+constexpr int kFwdKmax = 256;              // in_features <= 256, 2 * kH, kZ all fit
+constexpr int kFwdLd = kFwdKmax + 8;       // row stride (bf16): fragment loads spread over the banks
+
+struct FwdArgs {
+    const float *X;
+    int F;
+    const int32_t *adj;
+    int n, d;
+    const float *P;
+    int o_win, o_bin, o_ws[kLayers], o_wn[kLayers], o_b[kLayers], o_wr1, o_br1, o_wr2, o_br2;
+    float *H[kLayers + 1];
+    float *M[kLayers];
+    const gg_swap *sw;
+    int n_sw;
+    float *Z, *O, *y;
+    gg::Ctl *ctl;
+    unsigned expected;
+    long long wait_ns;
+};
+
+// acc[8][4] of this warp's 16 rows x 64 columns = As (64 x K) * Bt^T, K % 16 == 0.
+__device__ __forceinline__ void tile_mma(const uint16_t *As, const uint16_t *Bt, const int K, float acc[8][4]) {
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, gid = lane >> 2, tg = lane & 3;
+    const int r = warp * 16;
+#pragma unroll
+    for (int j = 0; j < 8; ++j) acc[j][0] = acc[j][1] = acc[j][2] = acc[j][3] = 0.f;
+    for (int k0 = 0; k0 < K; k0 += 16) {
+        uint32_t a[4];
+        a[0] = *reinterpret_cast<const uint32_t *>(As + (r + gid) * kFwdLd + k0 + 2 * tg);
+        a[1] = *reinterpret_cast<const uint32_t *>(As + (r + gid + 8) * kFwdLd + k0 + 2 * tg);
+        a[2] = *reinterpret_cast<const uint32_t *>(As + (r + gid) * kFwdLd + k0 + 2 * tg + 8);
+        a[3] = *reinterpret_cast<const uint32_t *>(As + (r + gid + 8) * kFwdLd + k0 + 2 * tg + 8);
+#pragma unroll
+        for (int j = 0; j < 8; ++j) {
+            uint32_t b[2];
+            b[0] = *reinterpret_cast<const uint32_t *>(Bt + (8 * j + gid) * kFwdLd + k0 + 2 * tg);
+            b[1] = *reinterpret_cast<const uint32_t *>(Bt + (8 * j + gid) * kFwdLd + k0 + 2 * tg + 8);
+            mma_bf16(acc[j], a, b);
+        }
+    }
+}
+
+// Rows [row0, row0 + 64) of out (width kH) = relu(acc + bias); rows >= rows are dropped.
+__device__ __forceinline__ void tile_store_relu(const float acc[8][4], const float *bias, float *out, int row0,
+                                                int rows) {
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, gid = lane >> 2, tg = lane & 3;
+#pragma unroll
+    for (int j = 0; j < 8; ++j)
+#pragma unroll
+        for (int h = 0; h < 4; ++h) {
+            const int m = row0 + warp * 16 + gid + ((h >> 1) << 3);
+            const int c = 8 * j + 2 * tg + (h & 1);
+            if (m < rows) {
+                const float v = acc[j][h] + bias[c];
+                out[(size_t)m * kH + c] = v > 0.f ? v : 0.f;
+            }
+        }
+}
+
+__global__ void __launch_bounds__(kFwdBlock) surrogate_forward_kernel(const FwdArgs a) {
+    extern __shared__ __align__(16) uint16_t fsm[];
+    uint16_t *As = fsm;                    // [64][kFwdLd]
+    uint16_t *Bt = fsm + 64 * kFwdLd;      // [64][kFwdLd]
+    __shared__ float s_o[64][kH + 1];
+    const int tid = threadIdx.x;
+    unsigned epoch = 0;
+    float acc[8][4];
+    const int nrb = (a.n + 63) / 64;
+    if (a.n > 0) {
+        // H0 = relu(X W_in + b_in); K = in_features padded to 16
+        const int K0 = (a.F + 15) / 16 * 16;
+        for (int e = tid; e < 64 * K0; e += kFwdBlock) {
+            const int c = e / K0, k = e % K0;
+            Bt[c * kFwdLd + k] = bf16_bits(k < a.F ? a.P[a.o_win + k * kH + c] : 0.f);
+        }
+        for (int rb = blockIdx.x; rb < nrb; rb += gridDim.x) {
+            for (int e = tid; e < 64 * K0; e += kFwdBlock) {
+                const int r = e / K0, k = e % K0, v = rb * 64 + r;
+                As[r * kFwdLd + k] = bf16_bits(v < a.n && k < a.F ? a.X[(size_t)v * a.F + k] : 0.f);
+            }
+            __syncthreads();
+            tile_mma(As, Bt, K0, acc);
+            tile_store_relu(acc, a.P + a.o_bin, a.H[0], rb * 64, a.n);
+            __syncthreads();
+        }
+        for (int l = 0; l < kLayers; ++l) {
+            if (!gg::grid_sync(a.ctl, a.expected, a.wait_ns, l, epoch)) return;
+            // Bt = [Ws ; Wn]^T (K = 128)
+            for (int e = tid; e < 64 * 2 * kH; e += kFwdBlock) {
+                const int c = e / (2 * kH), k = e % (2 * kH);
+                const float w = k < kH ? a.P[a.o_ws[l] + k * kH + c] : a.P[a.o_wn[l] + (k - kH) * kH + c];
+                Bt[c * kFwdLd + k] = bf16_bits(w);
+            }
+            const float inv = 1.f / (float)a.d;
+            for (int rb = blockIdx.x; rb < nrb; rb += gridDim.x) {
+                // A = [H_l | mean of the neighbours' H_l rows]; the means are kept in M_l
+                for (int e = tid; e < 64 * kH; e += kFwdBlock) {
+                    const int r = e / kH, c = e % kH, v = rb * 64 + r;
+                    float h = 0.f, m = 0.f;
+                    if (v < a.n) {
+                        h = __ldcg(a.H[l] + (size_t)v * kH + c);
+                        for (int i = 0; i < a.d; ++i)
+                            m += __ldcg(a.H[l] + (size_t)__ldg(a.adj + (size_t)v * a.d + i) * kH + c);
+                        m *= inv;
+                        a.M[l][(size_t)v * kH + c] = m;
+                    }
+                    As[r * kFwdLd + c] = bf16_bits(h);
+                    As[r * kFwdLd + kH + c] = bf16_bits(m);
+                }
+                __syncthreads();
+                tile_mma(As, Bt, 2 * kH, acc);
+                tile_store_relu(acc, a.P + a.o_b[l], a.H[l + 1], rb * 64, a.n);
+                __syncthreads();
+            }
+        }
+        if (!gg::grid_sync(a.ctl, a.expected, a.wait_ns, kLayers, epoch)) return;
+    }
+    // readout: Z = [Ha+Hb+Hc+Hd, Ha*Hb + Hc*Hd, Ha*Hp + Hb*Hq], O = relu(Z Wr1 + br1), y = O.wr2 + br2
+    if (a.n_sw > 0) {
+        for (int e = tid; e < 64 * kZ; e += kFwdBlock) {
+            const int c = e / kZ, k = e % kZ;
+            Bt[c * kFwdLd + k] = bf16_bits(a.P[a.o_wr1 + k * kH + c]);
+        }
+        const float *H3 = a.H[kLayers];
+        const int ntb = (a.n_sw + 63) / 64;
+        for (int tb = blockIdx.x; tb < ntb; tb += gridDim.x) {
+            for (int e = tid; e < 64 * kH; e += kFwdBlock) {
+                const int r = e / kH, j = e % kH, p = tb * 64 + r;
+                float z0 = 0.f, z1 = 0.f, z2 = 0.f;
+                if (p < a.n_sw) {
+                    const gg_swap s = a.sw[p];
+                    int pa, qb;
+                    partners(s, pa, qb);
+                    const float ha = __ldcg(H3 + (size_t)s.a * kH + j), hb = __ldcg(H3 + (size_t)s.b * kH + j);
+                    const float hc = __ldcg(H3 + (size_t)s.c * kH + j), hd = __ldcg(H3 + (size_t)s.d * kH + j);
+                    const float hp = __ldcg(H3 + (size_t)pa * kH + j), hq = __ldcg(H3 + (size_t)qb * kH + j);
+                    z0 = ha + hb + hc + hd;
+                    z1 = ha * hb + hc * hd;
+                    z2 = ha * hp + hb * hq;
+                    float *z = a.Z + (size_t)p * kZ;
+                    z[j] = z0; z[kH + j] = z1; z[2 * kH + j] = z2;
+                }
+                As[r * kFwdLd + j] = bf16_bits(z0);
+                As[r * kFwdLd + kH + j] = bf16_bits(z1);
+                As[r * kFwdLd + 2 * kH + j] = bf16_bits(z2);
+            }
+            __syncthreads();
+            tile_mma(As, Bt, kZ, acc);
+            tile_store_relu(acc, a.P + a.o_br1, a.O, tb * 64, a.n_sw);
+            {
+                // the block's O rows, for the output dot products
+                const int warp = tid >> 5, lane = tid & 31, gid = lane >> 2, tg = lane & 3;
+#pragma unroll
+                for (int j = 0; j < 8; ++j)
+#pragma unroll
+                    for (int h = 0; h < 4; ++h) {
+                        const int r = warp * 16 + gid + ((h >> 1) << 3), c = 8 * j + 2 * tg + (h & 1);
+                        const float v = acc[j][h] + a.P[a.o_br1 + c];
+                        s_o[r][c] = v > 0.f ? v : 0.f;
+                    }
+            }
+            __syncthreads();
+            if (tid < 64 && tb * 64 + tid < a.n_sw) {
+                float sum = 0.f;
+                for (int j = 0; j < kH; ++j) sum += s_o[tid][j] * a.P[a.o_wr2 + j];
+                a.y[tb * 64 + tid] = sum + a.P[a.o_br2];
+            }
+            __syncthreads();
+        }
+    }
+}
+
 }  // namespace
 
 // ---------------------------------------------------------------------------
@@ -279,6 +429,9 @@ struct gg_surrogate {
     int32_t *mask = nullptr, *h_mask = nullptr;
     float *loss = nullptr, *h_loss = nullptr;
     float *hyper = nullptr, *h_hyper = nullptr;
+    gg::Ctl *ctl = nullptr;                // grid barrier of the fused forward launch
+    int *h_err = nullptr;                  // its wait status, copied back after each call
+    int fwd_per_sm = 0, sms = 0;
     bool fwd_valid = false, graph_set = false;
     long long adam_step = 0;
     // captured launch sequences, per swap count: predict (with the graph
@@ -348,28 +501,37 @@ gg_status ensure_swaps(gg_surrogate *s, int P) {
     return GG_OK;
 }
 
-// Embeddings of the current graph: H0 .. H3 (and the neighbour means M0 .. M2).
-void forward_graph(gg_surrogate *s) {
-    const int n = s->n;
-    float *P = s->params;
-    gemm(s->st, n, kH, s->F, s->X, s->F, 1, P + s->o_win, kH, 1, s->Hs[0], kH, 1, false);
-    bias_relu_kernel<<<blocks_for((long long)n * kH), 256, 0, s->st>>>(s->Hs[0], P + s->o_bin, n, kH);
-    for (int l = 0; l < kLayers; ++l) {
-        nbr_mean_kernel<<<blocks_for((long long)n * kH), 256, 0, s->st>>>(s->Hs[l], s->adj, n, s->d, s->Ms[l], 0);
-        gemm(s->st, n, kH, kH, s->Hs[l], kH, 1, P + s->o_ws[l], kH, 1, s->Hs[l + 1], kH, 1, false);
-        gemm(s->st, n, kH, kH, s->Ms[l], kH, 1, P + s->o_wn[l], kH, 1, s->Hs[l + 1], kH, 1, true);
-        bias_relu_kernel<<<blocks_for((long long)n * kH), 256, 0, s->st>>>(s->Hs[l + 1], P + s->o_b[l], n, kH);
-    }
+constexpr size_t kFwdSmem = 2 * 64 * kFwdLd * sizeof(uint16_t);
+
+// One fused launch (surrogate_forward_kernel): the embeddings of the current graph
+// when `graph` (H0 .. H3 and the neighbour means M0 .. M2), then the readout of the
+// P swaps in s->sw (Z, O, y) when P > 0.  The barrier status goes to s->h_err.
+void forward_fused(gg_surrogate *s, bool graph, int P) {
+    FwdArgs a{};
+    a.X = s->X; a.F = s->F; a.adj = s->adj; a.n = graph ? s->n : 0; a.d = s->d;
+    a.P = s->params;
+    a.o_win = s->o_win; a.o_bin = s->o_bin;
+    for (int l = 0; l < kLayers; ++l) { a.o_ws[l] = s->o_ws[l]; a.o_wn[l] = s->o_wn[l]; a.o_b[l] = s->o_b[l]; }
+    a.o_wr1 = s->o_wr1; a.o_br1 = s->o_br1; a.o_wr2 = s->o_wr2; a.o_br2 = s->o_br2;
+    for (int l = 0; l <= kLayers; ++l) a.H[l] = s->Hs[l];
+    for (int l = 0; l < kLayers; ++l) a.M[l] = s->Ms[l];
+    a.sw = s->sw; a.n_sw = P; a.Z = s->Z; a.O = s->O; a.y = s->y;
+    const int tiles = std::max((a.n + 63) / 64, (P + 63) / 64);
+    const int grid = std::max(1, std::min(s->fwd_per_sm * s->sms, tiles));
+    a.ctl = s->ctl;
+    a.expected = (unsigned)grid;
+    a.wait_ns = 10ll * 1000 * 1000 * 1000;
+    cudaMemsetAsync(s->ctl, 0, sizeof(gg::Ctl), s->st);
+    void *args[] = {&a};
+    cudaLaunchCooperativeKernel((void *)surrogate_forward_kernel, dim3(grid), dim3(kFwdBlock), args, kFwdSmem, s->st);
+    cudaMemcpyAsync(s->h_err, &s->ctl->err, sizeof(int), cudaMemcpyDeviceToHost, s->st);
 }
 
+// Embeddings of the current graph: H0 .. H3 (and the neighbour means M0 .. M2).
+void forward_graph(gg_surrogate *s) { forward_fused(s, true, 0); }
+
 // Readout of the P swaps in s->sw: Z, O, y.
-void forward_readout(gg_surrogate *s, int P) {
-    float *Pm = s->params;
-    readout_z_kernel<<<blocks_for((long long)P * kH), 256, 0, s->st>>>(s->Hs[kLayers], s->sw, P, s->Z);
-    gemm(s->st, P, kH, kZ, s->Z, kZ, 1, Pm + s->o_wr1, kH, 1, s->O, kH, 1, false);
-    bias_relu_kernel<<<blocks_for((long long)P * kH), 256, 0, s->st>>>(s->O, Pm + s->o_br1, P, kH);
-    readout_out_kernel<<<blocks_for((long long)P * 32), 256, 0, s->st>>>(s->O, Pm + s->o_wr2, Pm + s->o_br2, P, s->y);
-}
+void forward_readout(gg_surrogate *s, int P) { forward_fused(s, false, P); }
 
 // Loss and full gradient into s->grad (zeroed here) for the swaps/targets/mask on the device.
 void backward(gg_surrogate *s, int P) {
@@ -410,8 +572,7 @@ enum { kPredict = 0, kGrad = 1, kTrain = 2 };
 void enqueue_kind(gg_surrogate *s, int kind, int P) {
     cudaMemcpyAsync(s->sw, s->h_sw, (size_t)P * sizeof(gg_swap), cudaMemcpyHostToDevice, s->st);
     if (kind == kPredict) {
-        forward_graph(s);
-        forward_readout(s, P);
+        forward_fused(s, true, P);
         cudaMemcpyAsync(s->h_y, s->y, (size_t)P * 4, cudaMemcpyDeviceToHost, s->st);
         return;
     }
@@ -443,6 +604,7 @@ gg_status run_kind(gg_surrogate *s, int kind, int P) {
     }
     GS_CK(cudaGraphLaunch(exec, s->st));
     GS_CK(cudaStreamSynchronize(s->st));
+    if (*s->h_err) return sfail(GG_TIMEOUT, "grid barrier wait of the fused forward exceeded its limit");
     return GG_OK;
 }
 
@@ -482,6 +644,8 @@ gg_status grad_common(gg_surrogate *s, int kind, int P, const gg_swap *swaps, co
     if (!s->fwd_valid) {  // embeddings of the current graph and parameters
         forward_graph(s);
         GS_CK(cudaGetLastError());
+        GS_CK(cudaStreamSynchronize(s->st));
+        if (*s->h_err) return sfail(GG_TIMEOUT, "grid barrier wait of the fused forward exceeded its limit");
         s->fwd_valid = true;
     }
     r = run_kind(s, kind, P);
@@ -548,11 +712,19 @@ gg_status gg_surrogate_create(int device, int n, int degree, int in_features, ui
               cudaMalloc(&s->dH1, (size_t)n * kH * 4) == cudaSuccess &&
               cudaMalloc(&s->G, (size_t)n * kH * 4) == cudaSuccess &&
               cudaMalloc(&s->loss, 4) == cudaSuccess && cudaMalloc(&s->hyper, kHypN * 4) == cudaSuccess &&
-              cudaMallocHost(&s->h_loss, 4) == cudaSuccess && cudaMallocHost(&s->h_hyper, kHypN * 4) == cudaSuccess;
+              cudaMallocHost(&s->h_loss, 4) == cudaSuccess && cudaMallocHost(&s->h_hyper, kHypN * 4) == cudaSuccess &&
+              cudaMalloc(&s->ctl, sizeof(gg::Ctl)) == cudaSuccess && cudaMallocHost(&s->h_err, sizeof(int)) == cudaSuccess;
     for (int l = 0; l <= kLayers && ok; ++l) ok = cudaMalloc(&s->Hs[l], (size_t)n * kH * 4) == cudaSuccess;
     for (int l = 0; l < kLayers && ok; ++l) ok = cudaMalloc(&s->Ms[l], (size_t)n * kH * 4) == cudaSuccess;
     if (!ok) return bad(sfail(GG_OUT_OF_MEMORY, "surrogate allocation failed"));
     std::memset(s->h_hyper, 0, kHypN * 4);
+    *s->h_err = 0;
+    if (cudaFuncSetAttribute(surrogate_forward_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kFwdSmem) !=
+            cudaSuccess ||
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&s->fwd_per_sm, surrogate_forward_kernel, kFwdBlock, kFwdSmem) !=
+            cudaSuccess ||
+        cudaDeviceGetAttribute(&s->sms, cudaDevAttrMultiProcessorCount, device) != cudaSuccess || s->fwd_per_sm < 1)
+        return bad(sfail(GG_CUDA_ERROR, "fused forward cannot be resident"));
     if (cudaMemcpy(s->params, p.data(), pb, cudaMemcpyHostToDevice) != cudaSuccess ||
         cudaMemset(s->adam_m, 0, pb) != cudaSuccess || cudaMemset(s->adam_v, 0, pb) != cudaSuccess)
         return bad(sfail(GG_CUDA_ERROR, "surrogate initialisation failed"));
@@ -630,6 +802,7 @@ gg_status gg_surrogate_destroy(gg_surrogate *s) {
     cudaFree(s->params); cudaFree(s->grad); cudaFree(s->adam_m); cudaFree(s->adam_v);
     cudaFree(s->adj); cudaFree(s->X); cudaFree(s->dH0); cudaFree(s->dH1); cudaFree(s->G); cudaFree(s->loss);
     cudaFree(s->hyper); cudaFreeHost(s->h_loss); cudaFreeHost(s->h_hyper);
+    cudaFree(s->ctl); cudaFreeHost(s->h_err);
     for (auto p : s->Hs) cudaFree(p);
     for (auto p : s->Ms) cudaFree(p);
     cudaFree(s->sw); cudaFree(s->Z); cudaFree(s->O); cudaFree(s->y); cudaFree(s->t);

@@ -117,6 +117,10 @@ struct gg_engine {
     unsigned walk_smem_off = 0;          // byte offset of the walk buffers in dynamic smem
     int32_t *d_h2 = nullptr;             // [rows][d*d] level-2 walk ends (walk_K >= 3)
     size_t h2_elems = 0;
+    // walk index (walk_index_kernel): [rows][walk_cap] entries, [rows][walk_off_stride] bucket starts
+    uint16_t *d_went = nullptr, *d_woff = nullptr;
+    size_t went_elems = 0, woff_elems = 0;
+    int walk_cap = 0, walk_off_stride = 0;
     long long wait_ns = 10ll * 1000 * 1000 * 1000;
     int cap_alloc = 0;                   // levels the counter arrays hold
     int nb_alloc = 0;                    // batches the counter arrays hold
@@ -206,6 +210,8 @@ void destroy_all(gg_engine *e) {
     free_counters(e);
     if (e->d_adj != e->d_table) cudaFree(e->d_adj);  // the graph form aliases the two
     cudaFree(e->d_h2);
+    cudaFree(e->d_went);
+    cudaFree(e->d_woff);
     cudaFree(e->d_table); cudaFree(e->d_inv);
     cudaFreeHost(e->h_table);
     if (e->ev0) cudaEventDestroy(e->ev0);
@@ -241,26 +247,47 @@ void *kernel_for(int d, bool planes = false) {
     return planes ? kernel_for_t<true>(d) : kernel_for_t<false>(d);
 }
 
+// Walk ends per row up to depth K: d + d^2 + ... + d^K.
+long long walk_cap_for(int d, int K) {
+    long long sum = 0, p = 1;
+    for (int k = 1; k <= K; ++k) { p *= d; sum += p; }
+    return sum;
+}
+
 // Levels the walk pass computes for this plan: the largest K <= 4 whose walk ends
-// per row, d + d^2 + ... + d^K, stay within 600 (d = 8: 3 levels, 584 ends; d = 16:
-// 2; d = 4: 4), with the level-2 table (rows * d^2 int32) within 64 MiB for K >= 3
-// and d^2 <= kWalkList for K = 4.  GG_WALK_LEVELS overrides (0 = off).
+// per row stay within 600 (d = 8: 3 levels, 584 ends; d = 16: 2; d = 4: 4), within
+// the index kernel's row buffer and bucket count (kIndexMaxCap ends, kIndexMaxKeys
+// = batches * K buckets), with the level-2 table (rows * d^2 int32, K >= 3) within
+// 64 MiB and the index (rows * (ends + buckets) uint16) within 1 GiB.
+// GG_WALK_LEVELS overrides the depth (0 = off; still within those limits).
 int walk_levels(const gg_engine *e) {
     const int env = env_int("GG_WALK_LEVELS", e->walk_pref);
     const int d = e->d;
     if (d <= 0 || e->nC > gg::kWalkMaxNC || env == 0) return 0;
     int K = 0;
-    long long sum = 0, p = 1;
-    for (int k = 1; k <= 4; ++k) {
-        p *= d;
-        sum += p;
-        if (sum > 600) break;
-        K = k;
-    }
+    for (int k = 1; k <= 4 && walk_cap_for(d, k) <= 600; ++k) K = k;
     if (env > 0) K = std::min(env, 4);
-    if (K >= 3 && (long long)e->rows * d * d * 4 > (64ll << 20)) K = 2;
-    if (K >= 4 && d * d > gg::kWalkList) K = 3;
+    const long long nb = ((long long)e->reps.size() + e->batch_bits - 1) / e->batch_bits;
+    for (; K > 0; --K) {
+        const long long cap = walk_cap_for(d, K), keys = nb * K;
+        const bool ok = cap <= gg::kIndexMaxCap && keys <= gg::kIndexMaxKeys &&
+                        (K < 3 || (long long)e->rows * d * d * 4 <= (64ll << 20)) &&
+                        (long long)e->rows * (cap + keys + 1) * 2 <= (1ll << 30);
+        if (ok) break;
+    }
     return K;
+}
+
+void *index_kernel_for(int d) {
+    switch (kernel_degree_slot(d)) {
+        case 3: return (void *)gg::walk_index_kernel<3>;
+        case 4: return (void *)gg::walk_index_kernel<4>;
+        case 6: return (void *)gg::walk_index_kernel<6>;
+        case 8: return (void *)gg::walk_index_kernel<8>;
+        case 12: return (void *)gg::walk_index_kernel<12>;
+        case 16: return (void *)gg::walk_index_kernel<16>;
+        default: return (void *)gg::walk_index_kernel<0>;
+    }
 }
 
 // Source-batch plan: batch width, chunks per row, grid size.
@@ -342,6 +369,21 @@ gg_status plan(gg_engine *e, int want_bits) {
         if (h2_need) {
             GG_CK(cudaMalloc(&e->d_h2, h2_need * sizeof(int32_t)));
             e->h2_elems = h2_need;
+        }
+    }
+    e->walk_cap = e->walk_K ? (int)walk_cap_for(e->d, e->walk_K) : 0;
+    e->walk_off_stride = e->walk_K ? (int)(((long long)e->reps.size() + bits - 1) / bits) * e->walk_K + 1 : 0;
+    const size_t went_need = (size_t)e->rows * e->walk_cap, woff_need = (size_t)e->rows * e->walk_off_stride;
+    if (went_need != e->went_elems || woff_need != e->woff_elems) {
+        cudaFree(e->d_went);
+        cudaFree(e->d_woff);
+        e->d_went = e->d_woff = nullptr;
+        e->went_elems = e->woff_elems = 0;
+        if (went_need) {
+            GG_CK(cudaMalloc(&e->d_went, went_need * sizeof(uint16_t)));
+            GG_CK(cudaMalloc(&e->d_woff, woff_need * sizeof(uint16_t)));
+            e->went_elems = went_need;
+            e->woff_elems = woff_need;
         }
     }
     int per_sm = 0, sms = 0;
@@ -516,7 +558,7 @@ gg_status run_eval(gg_engine *e, const int32_t *d_table_in, const gg_eval_opts *
     // Walk pass for this evaluation: not with the WVC masks or the distance planes
     // (their per-level bookkeeping lives in the level loop), at most the level cap.
     const int walk_K = (wvc || (x && x->planes)) ? 0 : std::min(e->walk_K, cap_req);
-    const int launches = 1 + ((long long)e->rows * e->d > 0 ? 1 : 0) + (walk_K >= 3 ? 1 : 0);
+    const int launches = 1 + ((long long)e->rows * e->d > 0 ? 1 : 0) + (walk_K > 0 ? 1 : 0) + (walk_K >= 3 ? 1 : 0);
 
     // Everything the GPU does for one evaluation, on `q`: status words zeroed,
     // table -> adjacency (checked), one cooperative launch for every source
@@ -558,6 +600,31 @@ gg_status run_eval(gg_engine *e, const int32_t *d_table_in, const gg_eval_opts *
                     e->d_adj, e->d_h2, e->rows, e->d, e->form == FORM_GRAPH ? e->d_bad : nullptr);
                 GG_CK(cudaGetLastError());
             }
+            // the walk index of this evaluation's sources and batches
+            gg::WalkIndexArgs wi{};
+            wi.adj = e->d_adj;
+            wi.h2 = walk_K >= 3 ? e->d_h2 : nullptr;
+            wi.inv = x && x->inv ? x->inv : e->d_inv;
+            wi.src_first = x && x->inv ? 0 : e->src_first;
+            wi.src_begin = s0;
+            wi.ns_total = ns_all;
+            wi.S = 128 * e->nC;
+            wi.div_S = FastDiv((uint32_t)wi.S);
+            wi.nb = nb;
+            wi.K = walk_K;
+            wi.rows = e->rows;
+            wi.d = e->d;
+            wi.cap = e->walk_cap;
+            wi.ent = e->d_went;
+            wi.off = e->d_woff;
+            wi.off_stride = e->walk_off_stride;
+            wi.bad = e->form == FORM_GRAPH ? e->d_bad : nullptr;
+            int sms = 0;
+            GG_CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, e->device));
+            const int wgrid = (int)std::max<long long>(1, std::min<long long>(((long long)e->rows + 7) / 8,
+                                                                              (long long)sms * 8));
+            void *wargs[] = {&wi};
+            GG_CK(cudaLaunchKernel(index_kernel_for(e->d), dim3(wgrid), dim3(gg::kIndexBlock), wargs, 0, q));
         }
         BfsArgs a{};
         a.adj = e->d_adj;
@@ -600,7 +667,10 @@ gg_status run_eval(gg_engine *e, const int32_t *d_table_in, const gg_eval_opts *
         a.walk_K = walk_K;
         a.walk_rpg = e->walk_rpg;
         a.walk_smem_off = e->walk_smem_off;
-        a.h2 = e->d_h2;
+        a.walk_ent = e->d_went;
+        a.walk_off = e->d_woff;
+        a.walk_cap = e->walk_cap;
+        a.walk_off_stride = e->walk_off_stride;
         void *args[] = {&a};
         GG_CK(cudaLaunchCooperativeKernel(kernel_for(e->d, a.planes != nullptr), dim3(e->grid), dim3(gg::kBlock), args,
                                           e->smem_bytes, q));

@@ -119,14 +119,15 @@ struct BfsArgs {
     unsigned plane_cols;
     unsigned long long plane_stride;
     // Walk pass (see walk_rows): levels 1..walk_K of every batch computed from the
-    // walk ends of each row instead of phase 0 and pull/push levels.  0: off.
-    // Needs the batch's counts zeroed by the host (blocks add into them before any
-    // grid barrier), h2 when walk_K >= 3, and walk buffers in dynamic shared
-    // memory at byte offset walk_smem_off.
+    // walk index of each row (walk_index_kernel, launched before) instead of phase 0
+    // and pull/push levels.  0: off.  Needs the batch's counts zeroed by the host
+    // (blocks add into them before any grid barrier) and walk buffers in dynamic
+    // shared memory at byte offset walk_smem_off.
     int walk_K;
     int walk_rpg;             // rows per group: lcm(nC, 32) / nC
     unsigned walk_smem_off;
-    const int32_t *h2;
+    const uint16_t *walk_ent, *walk_off;
+    int walk_cap, walk_off_stride;
 };
 
 // Where a level's new pairs go in the distance planes.
@@ -512,71 +513,175 @@ static __device__ __noinline__ void phase0_tiles(const int32_t *inv, const int s
 // induction V_L[v] holds exactly the sources whose vertex is the end of some
 // walk of length <= L from v along the pull table (adj[v], adj[adj[v]], ...),
 // for any table, symmetric or not.  The first levels of a batch touch few pairs
-// (about d^L per source) but a pull level still visits every chunk; instead one
-// warp enumerates the walk ends of its row level by level, keeps the sources of
-// the batch among them (a compare per end: consecutive source ids, or the inverse
-// list of the lifted forms' representatives), and sets their bits in a
-// shared-memory copy of the row with atomicOr, whose returned old word tells
-// whether a pair is new at this level: the level counts are exact.  The row is
-// then written once: V = V_K with the padding bits, the level-(K+1) frontier
-// F = V_K & ~V_{K-1} (every chunk, zeros included) and its flag words.
+// (about d^L per source), but a pull level still visits every chunk.  Instead:
 //
-// Walk ends per row: level 1 = adj[v] (d), level 2 = H2[v] = adj of adj[v] (d^2,
-// precomputed once per evaluation into `h2` when K >= 3, else read row by row),
-// level 3 = H2 of adj[v] (d^3), level 4 = H2 of H2[v] (d^4).  K is chosen on the
-// host so that d + ... + d^K stays a few hundred.
+//  * once per evaluation, walk_index_kernel enumerates the walk ends of every row
+//    -- level 1 = adj[v] (d), level 2 = H2[v] (d^2; H2 = adj of adj, built by
+//    h2_kernel when K >= 3, else read row by row), level 3 = H2 of adj[v] (d^3),
+//    level 4 = H2 of H2[v] (d^4) -- keeps those that are sources (consecutive ids,
+//    or the inverse list of the lifted forms' representatives) and counting-sorts
+//    them per row by (batch, level): ent[v][...] holds each kept end's source index
+//    within its batch (16 bits), off[v][b * K + L - 1] where bucket (b, L) starts;
+//  * per batch, walk_rows gives each row to one warp, which reads the row's
+//    entries of this batch (a few dozen: the ends of the other batches never come
+//    back), sets their bits level by level in a shared-memory copy of the row with
+//    atomicOr -- its returned old word says whether the pair is new at that level,
+//    so the counts are exact, repeated ends included -- and writes the row once:
+//    V = V_K with the padding bits, the level-(K+1) frontier F = V_K & ~V_{K-1}
+//    (every chunk, zeros included) and its flag words.
 //
-// Rows go to warps in groups of whole rows that also cover whole 32-chunk tiles
-// (lcm(nC, 32) chunks), so that each flag word has one writer.
+// K is chosen on the host so that d + ... + d^K stays a few hundred.  Rows go to
+// warps in groups of whole rows that also cover whole 32-chunk tiles (lcm(nC, 32)
+// chunks), so that each flag word has one writer.
 // ---------------------------------------------------------------------------
-struct WalkArgs {
+struct WalkIndexArgs {
     const int32_t *adj;       // [rows][d]
     const int32_t *h2;        // [rows][d*d] or nullptr (K <= 2)
+    const int32_t *inv;       // source index of each vertex (-1: none), or nullptr
+    int src_first, src_begin, ns_total;   // the evaluation's sources (see BfsArgs)
+    FastDiv div_S;            // division by the batch width S = 128 * nC
+    int S, nb, K;
+    int rows, d;
+    int cap;                  // entries per row: d + ... + d^K
+    uint16_t *ent;            // [rows][cap]
+    uint16_t *off;            // [rows][off_stride]: bucket starts, nb * K + 1 used
+    int off_stride;
+    const int *bad;           // nonzero: the table failed its range check
+};
+
+constexpr int kIndexBlock = 256;
+constexpr int kIndexMaxKeys = 256;   // nb * K buckets per row
+constexpr int kIndexMaxCap = 1024;   // entries per row
+
+// Every walk end of row v with its level, in level order within each lane.
+template <int D, typename Fn>
+__device__ __forceinline__ void for_walk_ends(const WalkIndexArgs &a, const int v, const unsigned lane, Fn &&fn) {
+    const int d = D > 0 ? D : a.d;
+    const int dd = d * d;
+    const int32_t *arow = a.adj + (size_t)v * d;
+    for (int i = (int)lane; i < d; i += 32) fn(__ldg(arow + i), 1);
+    if (a.K >= 2) {
+        if (a.h2) {
+            for (int i = (int)lane; i < dd; i += 32) fn(__ldg(a.h2 + (size_t)v * dd + i), 2);
+        } else {
+            for (int i = (int)lane; i < dd; i += 32) fn(__ldg(a.adj + (size_t)__ldg(arow + i / d) * d + i % d), 2);
+        }
+    }
+    if (a.K >= 3) {
+        if constexpr (D > 0 && D <= 8 && (D * D) % 4 == 0) {
+            // d H2 rows, 16 bytes at a time, every load in flight before any use
+            constexpr int Q = D * D / 4, U = D * Q, SL = (U + 31) / 32;
+            uint4 q[SL];
+#pragma unroll
+            for (int s = 0; s < SL; ++s) {
+                const int i = s * 32 + (int)lane;
+                q[s] = make_uint4(0u, 0u, 0u, 0u);
+                if (i < U)
+                    q[s] = __ldg(reinterpret_cast<const uint4 *>(a.h2 + (size_t)__ldg(arow + i / Q) * dd) + i % Q);
+            }
+#pragma unroll
+            for (int s = 0; s < SL; ++s)
+                if (s * 32 + (int)lane < U) {
+                    fn((int32_t)q[s].x, 3); fn((int32_t)q[s].y, 3); fn((int32_t)q[s].z, 3); fn((int32_t)q[s].w, 3);
+                }
+        } else {
+            for (int i = (int)lane; i < d * dd; i += 32)
+                fn(__ldg(a.h2 + (size_t)__ldg(arow + i / dd) * dd + i % dd), 3);
+        }
+    }
+    if (a.K >= 4)
+        for (int i = (int)lane; i < dd * dd; i += 32)
+            fn(__ldg(a.h2 + (size_t)__ldg(a.h2 + (size_t)v * dd + i / dd) * dd + i % dd), 4);
+}
+
+template <int D>
+__global__ void __launch_bounds__(kIndexBlock) walk_index_kernel(const WalkIndexArgs a) {
+    __shared__ unsigned s_cur[kIndexBlock / 32][kIndexMaxKeys];
+    __shared__ uint16_t s_ent[kIndexBlock / 32][kIndexMaxCap];
+    if (a.bad && *a.bad) return;
+    const unsigned lane = threadIdx.x & 31u, wib = threadIdx.x >> 5;
+    unsigned *cur = s_cur[wib];
+    uint16_t *row = s_ent[wib];
+    const int nkeys = a.nb * a.K;
+    const int per = (nkeys + 31) / 32;   // keys per lane in the scan
+    // source index within the evaluation of end w, or -1
+    auto src_of = [&](const int32_t w) -> int {
+        const int g = a.inv ? __ldg(a.inv + w) : w - a.src_first;
+        const int j = g - a.src_begin;
+        return (g >= 0 && (unsigned)j < (unsigned)a.ns_total) ? j : -1;
+    };
+    for (int v = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5); v < a.rows;
+         v += (int)((gridDim.x * blockDim.x) >> 5)) {
+        for (int k = (int)lane; k < nkeys; k += 32) cur[k] = 0u;
+        __syncwarp();
+        // pass 1: bucket sizes
+        for_walk_ends<D>(a, v, lane, [&](const int32_t w, const int L) {
+            const int j = src_of(w);
+            if (j >= 0) atomicAdd(cur + (int)a.div_S.div((unsigned)j) * a.K + (L - 1), 1u);
+        });
+        __syncwarp();
+        // exclusive prefix over the buckets: lane l owns keys [l * per, (l + 1) * per)
+        unsigned mine = 0u;
+        for (int k = (int)lane * per; k < min(nkeys, ((int)lane + 1) * per); ++k) mine += cur[k];
+        unsigned incl = mine;
+        for (int o = 1; o < 32; o <<= 1) {
+            const unsigned t = __shfl_up_sync(0xffffffffu, incl, o);
+            if ((int)lane >= o) incl += t;
+        }
+        unsigned run = incl - mine;
+        uint16_t *offrow = a.off + (size_t)v * a.off_stride;
+        for (int k = (int)lane * per; k < min(nkeys, ((int)lane + 1) * per); ++k) {
+            const unsigned c = cur[k];
+            offrow[k] = (uint16_t)run;
+            cur[k] = run;
+            run += c;
+        }
+        const unsigned total = __shfl_sync(0xffffffffu, incl, 31);
+        if (lane == 0) offrow[nkeys] = (uint16_t)total;
+        __syncwarp();
+        // pass 2: each kept end at its bucket's next slot (the row's ends again, now from L1)
+        for_walk_ends<D>(a, v, lane, [&](const int32_t w, const int L) {
+            const int j = src_of(w);
+            if (j >= 0) {
+                const unsigned b = a.div_S.div((unsigned)j);
+                const unsigned pos = atomicAdd(cur + (int)b * a.K + (L - 1), 1u);
+                row[pos] = (uint16_t)((unsigned)j - b * (unsigned)a.S);
+            }
+        });
+        __syncwarp();
+        uint16_t *dst = a.ent + (size_t)v * a.cap;
+        for (unsigned k = lane; k < total; k += 32) dst[k] = row[k];
+        __syncwarp();
+    }
+}
+
+struct WalkArgs {
+    const uint16_t *ent, *off;  // the walk index (walk_index_kernel)
+    int cap, off_stride;
+    int b;                    // the batch: buckets b * K .. b * K + K - 1
     const int32_t *inv;       // source index of each vertex (-1: none), or nullptr
     int src_first, first, ns; // source j of the batch is vertex src_first + first + j (inv == nullptr)
     uint4 *V, *F;             // visited bits (V_K), frontier of level K+1
     uint32_t *fl;             // flag words of F
-    int rows, d, nC, K;
+    int rows, nC, K;
     unsigned items;
     int rows_per_group;       // lcm(nC, 32) / nC
 };
 
-constexpr int kWalkList = 64;     // per-warp list of level-2 walk ends (level-4 parents)
 constexpr int kWalkMaxNC = 64;    // row width (uint4 chunks) the per-warp buffers hold
 
-// Shared-memory bytes of the walk buffers of one block.
-__host__ __device__ constexpr int walk_smem_per_warp(int nC) {
-    return nC * 16 * 2 + kWalkMaxNC * 4 + kWalkList * 4;
-}
+// Shared-memory bytes of the walk buffers of one warp.
+__host__ __device__ constexpr int walk_smem_per_warp(int nC) { return nC * 16 * 2 + kWalkMaxNC * 4; }
 
-// Test one walk end w at level L: a new pair when w is a source of the batch whose
-// bit is not set in the row yet.
-__device__ __forceinline__ void walk_test(const WalkArgs &w, const int32_t end, const int L,
-                                          uint32_t *Vb, uint32_t *Fb, unsigned (&cnt)[4]) {
-    const int g = w.inv ? __ldg(w.inv + end) : end - w.src_first;
-    const int j = g - w.first;
-    if (g >= 0 && (unsigned)j < (unsigned)w.ns) {
-        const uint32_t bit = 1u << (j & 31);
-        const uint32_t old = atomicOr(Vb + (j >> 5), bit);
-        if (!(old & bit)) {
-            cnt[L - 1] += 1u;
-            if (L == w.K) atomicOr(Fb + (j >> 5), bit);
-        }
-    }
-}
-
-template <int D>
 static __device__ __noinline__ void walk_rows(const WalkArgs &w, unsigned char *smem, const unsigned gwarp,
                                               const unsigned nwarps, unsigned long long *s_cnt) {
     const unsigned lane = threadIdx.x & 31u;
-    const int d = D > 0 ? D : w.d;
-    const int dd = d * d;
     const int nw = w.nC * 4;  // u32 words per row
     unsigned char *mine = smem + (size_t)(threadIdx.x >> 5) * walk_smem_per_warp(w.nC);
     uint32_t *Vb = reinterpret_cast<uint32_t *>(mine);
     uint32_t *Fb = Vb + nw;
     uint32_t *flw = Fb + nw;
-    int32_t *list2 = reinterpret_cast<int32_t *>(flw + kWalkMaxNC);
+    const int K = w.K;
     unsigned cnt[4] = {0u, 0u, 0u, 0u};
     const int gchunks = w.rows_per_group * w.nC;       // a multiple of 32
     const int gwords = gchunks >> 5;
@@ -586,6 +691,19 @@ static __device__ __noinline__ void walk_rows(const WalkArgs &w, unsigned char *
         for (int r = 0; r < w.rows_per_group; ++r) {
             const int v = (int)grp * w.rows_per_group + r;
             if (v >= w.rows) break;
+            // bucket bounds of this batch: off[bK + L - 1] .. off[bK + L]
+            const uint16_t *offrow = w.off + (size_t)v * w.off_stride + w.b * K;
+            const int o = lane <= (unsigned)K ? (int)__ldg(offrow + lane) : 0;
+            const int e0 = __shfl_sync(0xffffffffu, o, 0);
+            const int e1 = __shfl_sync(0xffffffffu, o, 1);
+            const int e2 = __shfl_sync(0xffffffffu, o, K >= 2 ? 2 : 1);
+            const int e3 = __shfl_sync(0xffffffffu, o, K >= 3 ? 3 : 1);
+            const int eK = __shfl_sync(0xffffffffu, o, K);
+            const uint16_t *ents = w.ent + (size_t)v * w.cap;
+            // the first 64 entries in flight while the row is initialised
+            const int i0 = e0 + (int)lane, i1 = e0 + 32 + (int)lane;
+            const int x0 = i0 < eK ? (int)__ldg(ents + i0) : -1;
+            const int x1 = i1 < eK ? (int)__ldg(ents + i1) : -1;
             // the row starts as its padding bits and the diagonal
             for (int c = (int)lane; c < w.nC; c += 32) {
                 const uint4 p = pad_mask(c, w.ns);
@@ -599,105 +717,32 @@ static __device__ __noinline__ void walk_rows(const WalkArgs &w, unsigned char *
                 if (g >= 0 && (unsigned)j < (unsigned)w.ns) Vb[j >> 5] |= 1u << (j & 31);
             }
             __syncwarp();
-            const int32_t *arow = w.adj + (size_t)v * d;
-            // level 1: the row's own neighbours
-            for (int i = (int)lane; i < d; i += 32) walk_test(w, __ldg(arow + i), 1, Vb, Fb, cnt);
-            __syncwarp();
-            if (w.K >= 2) {
-                // level 2: adj of adj[v] (H2[v] when precomputed); kept as the
-                // parents of level 4
-                if constexpr (D > 0 && (D * D) % 4 == 0) {
-                    if (w.h2) {
-                        constexpr int U = D * D / 4;  // uint4 per H2 row
-                        const uint4 *src = reinterpret_cast<const uint4 *>(w.h2 + (size_t)v * dd);
-#pragma unroll
-                        for (int i0 = 0; i0 < U; i0 += 32) {
-                            const int i = i0 + (int)lane;
-                            if (i < U) {
-                                const uint4 q = __ldg(src + i);
-                                if (w.K >= 4 && 4 * i + 3 < kWalkList) {
-                                    list2[4 * i] = q.x; list2[4 * i + 1] = q.y;
-                                    list2[4 * i + 2] = q.z; list2[4 * i + 3] = q.w;
-                                }
-                                walk_test(w, q.x, 2, Vb, Fb, cnt); walk_test(w, q.y, 2, Vb, Fb, cnt);
-                                walk_test(w, q.z, 2, Vb, Fb, cnt); walk_test(w, q.w, 2, Vb, Fb, cnt);
-                            }
-                        }
-                    } else {
-                        // D*D ends from the D neighbour rows, 16 bytes at a time
-                        constexpr int R = D / 4 > 0 ? D / 4 : 1;   // uint4 per adjacency row (D % 4 == 0)
-                        if constexpr (D % 4 == 0) {
-                            constexpr int U = D * R;
-                            uint4 q[(U + 31) / 32];
-#pragma unroll
-                            for (int s = 0; s < (U + 31) / 32; ++s) {
-                                const int i = s * 32 + (int)lane;
-                                q[s] = make_uint4(0u, 0u, 0u, 0u);
-                                if (i < U) {
-                                    const int p = __ldg(arow + i / R);
-                                    q[s] = __ldg(reinterpret_cast<const uint4 *>(w.adj + (size_t)p * D) + i % R);
-                                }
-                            }
-#pragma unroll
-                            for (int s = 0; s < (U + 31) / 32; ++s) {
-                                const int i = s * 32 + (int)lane;
-                                if (i < U) {
-                                    walk_test(w, q[s].x, 2, Vb, Fb, cnt); walk_test(w, q[s].y, 2, Vb, Fb, cnt);
-                                    walk_test(w, q[s].z, 2, Vb, Fb, cnt); walk_test(w, q[s].w, 2, Vb, Fb, cnt);
-                                }
-                            }
-                        } else {
-                            for (int i = (int)lane; i < dd; i += 32)
-                                walk_test(w, __ldg(w.adj + (size_t)__ldg(arow + i / d) * d + i % d), 2, Vb, Fb, cnt);
-                        }
-                    }
-                } else {
-                    for (int i = (int)lane; i < dd; i += 32) {
-                        const int32_t e = w.h2 ? __ldg(w.h2 + (size_t)v * dd + i)
-                                               : __ldg(w.adj + (size_t)__ldg(arow + i / d) * d + i % d);
-                        if (w.K >= 4 && i < kWalkList) list2[i] = e;
-                        walk_test(w, e, 2, Vb, Fb, cnt);
-                    }
+            // the entries level by level (bucket order is level order)
+            auto level_of = [&](const int i) { return i < e1 ? 1 : (i < e2 ? 2 : (i < e3 ? 3 : 4)); };
+            auto put = [&](const int j, const int L) {
+                const uint32_t bit = 1u << (j & 31);
+                const uint32_t old = atomicOr(Vb + (j >> 5), bit);
+                if (!(old & bit)) {
+                    cnt[L - 1] += 1u;
+                    if (L == K) atomicOr(Fb + (j >> 5), bit);
                 }
+            };
+            const int L0 = x0 >= 0 ? level_of(i0) : 0, L1 = x1 >= 0 ? level_of(i1) : 0;
+            for (int L = 1; L <= K; ++L) {
+                if (L0 == L) put(x0, L);
+                if (L1 == L) put(x1, L);
                 __syncwarp();
             }
-            if (w.K >= 3) {
-                // level 3: H2 of each neighbour (d * d^2 ends)
-                if constexpr (D > 0 && D <= 8 && (D * D) % 4 == 0) {
-                    constexpr int Q = D * D / 4;   // uint4 per H2 row
-                    constexpr int U = D * Q;
-                    constexpr int S = (U + 31) / 32;
-                    uint4 q[S];
-#pragma unroll
-                    for (int s = 0; s < S; ++s) {
-                        const int i = s * 32 + (int)lane;
-                        q[s] = make_uint4(0u, 0u, 0u, 0u);
-                        if (i < U) {
-                            const int p = __ldg(arow + i / Q);
-                            q[s] = __ldg(reinterpret_cast<const uint4 *>(w.h2 + (size_t)p * dd) + i % Q);
-                        }
-                    }
-#pragma unroll
-                    for (int s = 0; s < S; ++s) {
-                        const int i = s * 32 + (int)lane;
-                        if (i < U) {
-                            walk_test(w, q[s].x, 3, Vb, Fb, cnt); walk_test(w, q[s].y, 3, Vb, Fb, cnt);
-                            walk_test(w, q[s].z, 3, Vb, Fb, cnt); walk_test(w, q[s].w, 3, Vb, Fb, cnt);
-                        }
-                    }
-                } else {
-                    const int n3 = d * dd;
-                    for (int i = (int)lane; i < n3; i += 32)
-                        walk_test(w, __ldg(w.h2 + (size_t)__ldg(arow + i / dd) * dd + i % dd), 3, Vb, Fb, cnt);
+            // rows with more than 64 entries in this batch: the rest, 32 at a time,
+            // still in level order (every chunk's levels are at least the last one's)
+            for (int base = e0 + 64; base < eK; base += 32) {
+                const int i = base + (int)lane;
+                const int x = i < eK ? (int)__ldg(ents + i) : -1;
+                const int Li = x >= 0 ? level_of(i) : 0;
+                for (int L = 1; L <= K; ++L) {
+                    if (Li == L) put(x, L);
+                    __syncwarp();
                 }
-                __syncwarp();
-            }
-            if (w.K >= 4) {
-                // level 4: H2 of each level-2 end (d^2 * d^2 ends; d^2 <= kWalkList)
-                const int n4 = dd * dd;
-                for (int i = (int)lane; i < n4; i += 32)
-                    walk_test(w, __ldg(w.h2 + (size_t)list2[i / dd] * dd + i % dd), 4, Vb, Fb, cnt);
-                __syncwarp();
             }
             // write the row: V = V_K (padding included), F = new at level K, flag bits
             const unsigned t0 = (unsigned)v * (unsigned)w.nC;
@@ -784,17 +829,18 @@ static __device__ __noinline__ unsigned walk_batch(const BfsArgs &a, const int b
     // by-value struct on every thread's stack)
     __shared__ WalkArgs w;
     if (threadIdx.x == 0) {
-        w.adj = a.adj; w.h2 = a.h2; w.inv = a.inv;
+        w.ent = a.walk_ent; w.off = a.walk_off; w.cap = a.walk_cap; w.off_stride = a.walk_off_stride;
+        w.b = b;
+        w.inv = a.inv;
         w.src_first = a.src_first; w.first = a.src_begin + b * 128 * a.nC; w.ns = ns;
         w.V = a.V;
         w.F = ((K + 1) & 1) ? a.F0 : a.F1;     // what level K + 1 reads
         w.fl = ((K + 1) & 1) ? a.fl0 : a.fl1;
-        w.rows = a.rows; w.d = d; w.nC = a.nC; w.K = K; w.items = items;
+        w.rows = a.rows; w.nC = a.nC; w.K = K; w.items = items;
         w.rows_per_group = a.walk_rpg;
     }
     __syncthreads();
-    walk_rows<D>(w, reinterpret_cast<unsigned char *>(s_adj) + a.walk_smem_off, gtid >> 5, nthr >> 5,
-                 s_wcnt);
+    walk_rows(w, reinterpret_cast<unsigned char *>(s_adj) + a.walk_smem_off, gtid >> 5, nthr >> 5, s_wcnt);
     __syncthreads();
     if (threadIdx.x == 0)
         for (int L = 1; L <= K; ++L)

@@ -673,95 +673,125 @@ constexpr int kWalkMaxNC = 64;    // row width (uint4 chunks) the per-warp buffe
 // Shared-memory bytes of the walk buffers of one warp.
 __host__ __device__ constexpr int walk_smem_per_warp(int nC) { return nC * 16 * 2 + kWalkMaxNC * 4; }
 
+// A row's index entries of this batch: bucket bounds (lanes 0..K hold off[bK + lane])
+// and its first 64 entries (lanes hold entries e0 + lane and e0 + 32 + lane, or -1).
+struct WalkRowLoad {
+    int o;
+    int x0, x1;
+};
+
 static __device__ __noinline__ void walk_rows(const WalkArgs &w, unsigned char *smem, const unsigned gwarp,
                                               const unsigned nwarps, unsigned long long *s_cnt) {
     const unsigned lane = threadIdx.x & 31u;
-    const int nw = w.nC * 4;  // u32 words per row
     unsigned char *mine = smem + (size_t)(threadIdx.x >> 5) * walk_smem_per_warp(w.nC);
-    uint32_t *Vb = reinterpret_cast<uint32_t *>(mine);
-    uint32_t *Fb = Vb + nw;
-    uint32_t *flw = Fb + nw;
-    const int K = w.K;
+    uint4 *Vb4 = reinterpret_cast<uint4 *>(mine);     // the row, 16 bytes per chunk (conflict-free)
+    uint4 *Fb4 = Vb4 + w.nC;
+    uint32_t *Vb = reinterpret_cast<uint32_t *>(Vb4);
+    uint32_t *Fb = reinterpret_cast<uint32_t *>(Fb4);
+    uint32_t *flw = reinterpret_cast<uint32_t *>(Fb4 + w.nC);
+    const int K = w.K, rpg = w.rows_per_group;
     unsigned cnt[4] = {0u, 0u, 0u, 0u};
-    const int gchunks = w.rows_per_group * w.nC;       // a multiple of 32
-    const int gwords = gchunks >> 5;
-    const unsigned ngroups = (unsigned)((w.rows + w.rows_per_group - 1) / w.rows_per_group);
-    for (unsigned grp = gwarp; grp < ngroups; grp += nwarps) {
-        for (int k = (int)lane; k < gwords; k += 32) flw[k] = 0u;
-        for (int r = 0; r < w.rows_per_group; ++r) {
-            const int v = (int)grp * w.rows_per_group + r;
-            if (v >= w.rows) break;
-            // bucket bounds of this batch: off[bK + L - 1] .. off[bK + L]
-            const uint16_t *offrow = w.off + (size_t)v * w.off_stride + w.b * K;
-            const int o = lane <= (unsigned)K ? (int)__ldg(offrow + lane) : 0;
-            const int e0 = __shfl_sync(0xffffffffu, o, 0);
-            const int e1 = __shfl_sync(0xffffffffu, o, 1);
-            const int e2 = __shfl_sync(0xffffffffu, o, K >= 2 ? 2 : 1);
-            const int e3 = __shfl_sync(0xffffffffu, o, K >= 3 ? 3 : 1);
-            const int eK = __shfl_sync(0xffffffffu, o, K);
+    const int gwords = (rpg * w.nC) >> 5;               // flag words per group
+    const unsigned ntiles = (w.items + 31u) >> 5;
+    // this warp's rows in order: the rows of groups gwarp, gwarp + nwarps, ...
+    auto next_row = [&](const int v) -> int {
+        if (v < 0) return -1;
+        int n = v + 1;
+        if (n % rpg == 0) n = (n / rpg - 1 + (int)nwarps) * rpg;
+        return n < w.rows ? n : -1;
+    };
+    auto load_off = [&](const int v) -> int {
+        return (v >= 0 && lane <= (unsigned)K) ? (int)__ldg(w.off + (size_t)v * w.off_stride + w.b * K + lane) : 0;
+    };
+    auto load_ents = [&](const int v, const int o) -> WalkRowLoad {
+        WalkRowLoad r{o, -1, -1};
+        const int e0 = __shfl_sync(0xffffffffu, o, 0), eK = __shfl_sync(0xffffffffu, o, K);
+        if (v >= 0) {
             const uint16_t *ents = w.ent + (size_t)v * w.cap;
-            // the first 64 entries in flight while the row is initialised
-            const int i0 = e0 + (int)lane, i1 = e0 + 32 + (int)lane;
-            const int x0 = i0 < eK ? (int)__ldg(ents + i0) : -1;
-            const int x1 = i1 < eK ? (int)__ldg(ents + i1) : -1;
-            // the row starts as its padding bits and the diagonal
-            for (int c = (int)lane; c < w.nC; c += 32) {
-                const uint4 p = pad_mask(c, w.ns);
-                Vb[4 * c] = p.x; Vb[4 * c + 1] = p.y; Vb[4 * c + 2] = p.z; Vb[4 * c + 3] = p.w;
-                Fb[4 * c] = Fb[4 * c + 1] = Fb[4 * c + 2] = Fb[4 * c + 3] = 0u;
+            if (e0 + (int)lane < eK) r.x0 = __ldg(ents + e0 + lane);
+            if (e0 + 32 + (int)lane < eK) r.x1 = __ldg(ents + e0 + 32 + lane);
+        }
+        return r;
+    };
+    int v = (int)gwarp * rpg;
+    if (v >= w.rows) v = -1;
+    // two rows ahead: the entries of the next row and the bounds of the one after
+    WalkRowLoad cur = load_ents(v, load_off(v));
+    int vn = next_row(v);
+    int o_n = load_off(vn);
+    for (; v >= 0;) {
+        const int vnn = next_row(vn);
+        const WalkRowLoad nxt = load_ents(vn, o_n);
+        const int o_nn = load_off(vnn);
+        const int r = v % rpg;
+        if (r == 0)
+            for (int k = (int)lane; k < gwords; k += 32) flw[k] = 0u;
+        // the row starts as its padding bits and the diagonal
+        for (int c = (int)lane; c < w.nC; c += 32) {
+            Vb4[c] = pad_mask(c, w.ns);
+            Fb4[c] = u4zero();
+        }
+        __syncwarp();
+        if (lane == 0) {
+            const int g = w.inv ? __ldg(w.inv + v) : v - w.src_first;
+            const int j = g - w.first;
+            if (g >= 0 && (unsigned)j < (unsigned)w.ns) Vb[j >> 5] |= 1u << (j & 31);
+        }
+        __syncwarp();
+        // the entries level by level (bucket order is level order)
+        const int e0 = __shfl_sync(0xffffffffu, cur.o, 0);
+        const int e1 = __shfl_sync(0xffffffffu, cur.o, 1);
+        const int e2 = __shfl_sync(0xffffffffu, cur.o, K >= 2 ? 2 : 1);
+        const int e3 = __shfl_sync(0xffffffffu, cur.o, K >= 3 ? 3 : 1);
+        const int eK = __shfl_sync(0xffffffffu, cur.o, K);
+        auto level_of = [&](const int i) { return i < e1 ? 1 : (i < e2 ? 2 : (i < e3 ? 3 : 4)); };
+        auto put = [&](const int j, const int L) {
+            const uint32_t bit = 1u << (j & 31);
+            const uint32_t old = atomicOr(Vb + (j >> 5), bit);
+            if (!(old & bit)) {
+                cnt[L - 1] += 1u;
+                if (L == K) atomicOr(Fb + (j >> 5), bit);
             }
-            __syncwarp();
-            if (lane == 0) {
-                const int g = w.inv ? __ldg(w.inv + v) : v - w.src_first;
-                const int j = g - w.first;
-                if (g >= 0 && (unsigned)j < (unsigned)w.ns) Vb[j >> 5] |= 1u << (j & 31);
-            }
-            __syncwarp();
-            // the entries level by level (bucket order is level order)
-            auto level_of = [&](const int i) { return i < e1 ? 1 : (i < e2 ? 2 : (i < e3 ? 3 : 4)); };
-            auto put = [&](const int j, const int L) {
-                const uint32_t bit = 1u << (j & 31);
-                const uint32_t old = atomicOr(Vb + (j >> 5), bit);
-                if (!(old & bit)) {
-                    cnt[L - 1] += 1u;
-                    if (L == K) atomicOr(Fb + (j >> 5), bit);
-                }
-            };
-            const int L0 = x0 >= 0 ? level_of(i0) : 0, L1 = x1 >= 0 ? level_of(i1) : 0;
-            for (int L = 1; L <= K; ++L) {
-                if (L0 == L) put(x0, L);
-                if (L1 == L) put(x1, L);
-                __syncwarp();
-            }
-            // rows with more than 64 entries in this batch: the rest, 32 at a time,
-            // still in level order (every chunk's levels are at least the last one's)
-            for (int base = e0 + 64; base < eK; base += 32) {
-                const int i = base + (int)lane;
-                const int x = i < eK ? (int)__ldg(ents + i) : -1;
-                const int Li = x >= 0 ? level_of(i) : 0;
-                for (int L = 1; L <= K; ++L) {
-                    if (Li == L) put(x, L);
-                    __syncwarp();
-                }
-            }
-            // write the row: V = V_K (padding included), F = new at level K, flag bits
-            const unsigned t0 = (unsigned)v * (unsigned)w.nC;
-            const unsigned b0 = (unsigned)r * (unsigned)w.nC;   // chunk index within the group
-            for (int c = (int)lane; c < w.nC; c += 32) {
-                const uint4 vv = make_uint4(Vb[4 * c], Vb[4 * c + 1], Vb[4 * c + 2], Vb[4 * c + 3]);
-                const uint4 ff = make_uint4(Fb[4 * c], Fb[4 * c + 1], Fb[4 * c + 2], Fb[4 * c + 3]);
-                w.V[t0 + c] = vv;
-                w.F[t0 + c] = ff;
-                if (u4any(ff)) atomicOr(flw + ((b0 + c) >> 5), 1u << ((b0 + c) & 31u));
-            }
+        };
+        const int L0 = cur.x0 >= 0 ? level_of(e0 + (int)lane) : 0;
+        const int L1 = cur.x1 >= 0 ? level_of(e0 + 32 + (int)lane) : 0;
+        for (int L = 1; L <= K; ++L) {
+            if (L0 == L) put(cur.x0, L);
+            if (L1 == L) put(cur.x1, L);
             __syncwarp();
         }
-        // the group's flag words (the group starts on a tile boundary)
-        const unsigned tile0 = grp * (unsigned)gwords;
-        const unsigned ntiles = (w.items + 31u) >> 5;
-        for (int k = (int)lane; k < gwords; k += 32)
-            if (tile0 + k < ntiles) w.fl[tile0 + k] = flw[k];
+        // rows with more than 64 entries in this batch: the rest, 32 at a time,
+        // still in level order (every chunk's levels are at least the last one's)
+        for (int base = e0 + 64; base < eK; base += 32) {
+            const int i = base + (int)lane;
+            const int x = i < eK ? (int)__ldg(w.ent + (size_t)v * w.cap + i) : -1;
+            const int Li = x >= 0 ? level_of(i) : 0;
+            for (int L = 1; L <= K; ++L) {
+                if (Li == L) put(x, L);
+                __syncwarp();
+            }
+        }
+        // write the row: V = V_K (padding included), F = new at level K, flag bits
+        const unsigned t0 = (unsigned)v * (unsigned)w.nC;
+        const unsigned b0 = (unsigned)r * (unsigned)w.nC;   // chunk index within the group
+        for (int c = (int)lane; c < w.nC; c += 32) {
+            const uint4 vv = Vb4[c], ff = Fb4[c];
+            w.V[t0 + c] = vv;
+            w.F[t0 + c] = ff;
+            if (u4any(ff)) atomicOr(flw + ((b0 + c) >> 5), 1u << ((b0 + c) & 31u));
+        }
         __syncwarp();
+        if (r == rpg - 1 || v == w.rows - 1) {
+            // the group's flag words (the group starts on a tile boundary)
+            const unsigned tile0 = (unsigned)(v / rpg) * (unsigned)gwords;
+            for (int k = (int)lane; k < gwords; k += 32)
+                if (tile0 + k < ntiles) w.fl[tile0 + k] = flw[k];
+            __syncwarp();
+        }
+        v = vn;
+        vn = vnn;
+        cur = nxt;
+        o_n = o_nn;
     }
 #pragma unroll
     for (int L = 0; L < 4; ++L) {

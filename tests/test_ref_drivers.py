@@ -46,9 +46,11 @@ def without_reference_diagnostics(text):
     shape from their constructors ("width: W nBlock: B", cudaASPLconv.cu:125,
     cudaASPLbox.cu:140, cudaASPLpiece.cu) and cudaASPLgraph's per-chunk progress
     "offset/N", each after a cursor-up/erase sequence but the first
-    (cudaASPLgraph.cu:159-160).  Remove exactly those from the reference build's output."""
+    (cudaASPLgraph.cu:159-160), and the erase sequence after its last chunk
+    (cudaASPLgraph.cu:194).  Remove exactly those from the reference build's output."""
     text = re.sub(r"^width: \d+ nBlock: \d+\n", "", text, flags=re.M)
-    return re.sub(r"(?:\x1b\[F\x1b\[E\x1b\[K)?\d+/\d+(?=\x1b\[F|Diameter: )", "", text)
+    text = re.sub(r"(?:\x1b\[F\x1b\[E\x1b\[K)?\d+/\d+(?=\x1b\[F|Diameter: )", "", text)
+    return re.sub(r"\x1b\[F\x1b\[E\x1b\[K(?=Diameter: )", "", text)
 
 
 def timeless(text):
@@ -149,7 +151,7 @@ def test_annealing_trajectory_same_as_reference_build(tmp_path):
 
 def test_reference_diagnostics_are_the_only_lines_removed():
     esc = "\x1b[F\x1b[E\x1b[K"
-    raw = ("Nodes: 3000 Degrees_max: 4\n0/3000" + esc + "1024/3000" + esc + "2048/3000Diameter: 10\n"
+    raw = ("Nodes: 3000 Degrees_max: 4\n0/3000" + esc + "1024/3000" + esc + "2048/3000" + esc + "Diameter: 10\n"
            "ASPL: 6.6235365122 (29795979/4498500)\nwidth: 2 nBlock: 1\nASPL: 5.0\n")
     assert without_reference_diagnostics(raw) == ("Nodes: 3000 Degrees_max: 4\nDiameter: 10\n"
                                                   "ASPL: 6.6235365122 (29795979/4498500)\nASPL: 5.0\n")

@@ -475,10 +475,23 @@ def run_ours(args):
     l2 = None
     if rank == 0 and not args.no_gather_peak:
         gp, gms = G.gather_peak(rows=wl["N"], degree=wl["d"], iters=20, device=local)
+        # per-level device timestamps of batch 0 (one more evaluation, outside the timed steps)
+        lv = eng.eval_device(table_dev.data_ptr(), max_levels=max_levels, stream=sptr, level_ns=True,
+                             src_range=src_range)["level_ns"].astype(np.int64)
+        level_us = [round((int(lv[i]) - int(lv[i - 1])) / 1000.0, 2) for i in range(1, len(lv)) if lv[i]]
+        # a dense level moves 11 row transfers per row (own word, d = 8 gathers, two writes);
+        # the gather pass moves 10: its time x 1.1 is the dense level's floor at this rate
+        floor_us = 1000.0 * gms * (wl["d"] + 3) / (wl["d"] + 2)
+        # the dense levels: past the first (the walk pass, or level 1), within 30 % of the slowest
+        rest = level_us[1:]
+        dense = [t for t in rest if t >= 0.7 * max(rest)] if rest else []
         l2 = {"gather_peak_gbs": gp, "gather_pass_ms": gms,
               "what": f"gg_gather_peak: {wl['N']} rows x ({wl['d']} random + 1 own) 512-byte row reads + "
-                      "1 row write per pass, the access pattern of one dense BFS level of a 4096-source "
+                      "1 row write per pass, the access pattern of one dense BFS level of one source "
                       "batch, arrays L2-resident",
+              "levels_batch0_us": level_us,
+              "dense_level_floor_us": floor_us,
+              "dense_level_frac": (floor_us / statistics.median(dense)) if dense else None,
               "kernel_ms_in_gather_passes": kern_ms / gms,
               "level_steps": r["level_steps"]}
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,

@@ -771,14 +771,25 @@ static __device__ __noinline__ void walk_rows(const WalkArgs &w, unsigned char *
                 __syncwarp();
             }
         }
-        // write the row: V = V_K (padding included), F = new at level K, flag bits
+        // write the row: V = V_K (padding included), F = new at level K, and the flag
+        // bits of F (one ballot per 32 chunks; lane 0 merges it into the group's words)
         const unsigned t0 = (unsigned)v * (unsigned)w.nC;
         const unsigned b0 = (unsigned)r * (unsigned)w.nC;   // chunk index within the group
-        for (int c = (int)lane; c < w.nC; c += 32) {
-            const uint4 vv = Vb4[c], ff = Fb4[c];
-            w.V[t0 + c] = vv;
-            w.F[t0 + c] = ff;
-            if (u4any(ff)) atomicOr(flw + ((b0 + c) >> 5), 1u << ((b0 + c) & 31u));
+        for (int cb = 0; cb < w.nC; cb += 32) {
+            const int c = cb + (int)lane;
+            bool any = false;
+            if (c < w.nC) {
+                const uint4 vv = Vb4[c], ff = Fb4[c];
+                w.V[t0 + c] = vv;
+                w.F[t0 + c] = ff;
+                any = u4any(ff);
+            }
+            const unsigned m = __ballot_sync(0xffffffffu, any);
+            if (lane == 0 && m) {
+                const unsigned first = b0 + (unsigned)cb, off = first & 31u;
+                flw[first >> 5] |= m << off;
+                if (off && (m >> (32u - off))) flw[(first >> 5) + 1] |= m >> (32u - off);  // stays in the group
+            }
         }
         __syncwarp();
         if (r == rpg - 1 || v == w.rows - 1) {

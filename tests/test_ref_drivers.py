@@ -105,8 +105,8 @@ def test_aspl_cuda_same_as_reference_build(tmp_path):
     assert s_out == o_out and s_files == o_files
     assert "Diameter:" in s_out and "ASPL:" in s_files["res.txt"]
     # a non-regular graph (self-loop padding inside the calculator)
-    adj2 = I.random_nonregular(700, 5, 3)
-    pairs = [(u, v) for v, row in enumerate(adj2) for u in row if u < v]
+    _, lists = I.random_nonregular(700, 5, 3)
+    pairs = [(u, v) for v, row in enumerate(lists) for u in row if u < v]
     src2 = write(tmp_path, "g2.txt", G.graph.from_pairs(pairs))
     (s_out, s_files), (o_out, o_files) = both("aspl_cuda", ["-i", src2, "-o", "res2.txt"], tmp_path)
     assert s_out == o_out and s_files == o_files

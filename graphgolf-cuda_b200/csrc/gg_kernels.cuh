@@ -594,6 +594,95 @@ __device__ __forceinline__ void for_walk_ends(const WalkIndexArgs &a, const int 
             fn(__ldg(a.h2 + (size_t)__ldg(a.h2 + (size_t)v * dd + i / dd) * dd + i % dd), 4);
 }
 
+// One row of the walk index with its ends in registers (D <= 8 with D*D % 4 == 0,
+// K <= 3, level-2 ends from H2 or the adjacency rows): the ends are enumerated and
+// classified once, then counted and placed from registers.
+template <int D>
+__device__ __forceinline__ void index_row_regs(const WalkIndexArgs &a, const int v, const unsigned lane,
+                                               unsigned *cur, uint16_t *row, const int nkeys) {
+    constexpr int DD = D * D, Q = DD / 4;           // uint4 per level-2 list
+    constexpr int U3 = D * Q, S3 = (U3 + 31) / 32;  // uint4 of the level-3 ends, per lane
+    constexpr int NV = 1 + 4 * ((Q + 31) / 32) + 4 * S3;
+    int pk[NV];                                     // (key << 16) | payload, or -1
+    const int32_t *arow = a.adj + (size_t)v * D;
+    auto classify = [&](const int32_t w, const int L) -> int {
+        const int g = a.inv ? __ldg(a.inv + w) : w - a.src_first;
+        const int j = g - a.src_begin;
+        if (!(g >= 0 && (unsigned)j < (unsigned)a.ns_total)) return -1;
+        const unsigned b = a.div_S.div((unsigned)j);
+        return (int)(((b * (unsigned)a.K + (unsigned)(L - 1)) << 16) | ((unsigned)j - b * (unsigned)a.S));
+    };
+    // loads first (all in flight), classification after
+    const int32_t x1 = lane < (unsigned)D ? __ldg(arow + lane) : 0;
+    uint4 q2[(Q + 31) / 32];
+#pragma unroll
+    for (int s2 = 0; s2 < (Q + 31) / 32; ++s2) {
+        const int i = s2 * 32 + (int)lane;
+        q2[s2] = make_uint4(0u, 0u, 0u, 0u);
+        if (a.K >= 2 && i < Q)
+            q2[s2] = a.h2 ? __ldg(reinterpret_cast<const uint4 *>(a.h2 + (size_t)v * DD) + i)
+                          : __ldg(reinterpret_cast<const uint4 *>(a.adj + (size_t)__ldg(arow + i / (D / 4)) * D) +
+                                  i % (D / 4));
+    }
+    uint4 q3[S3];
+#pragma unroll
+    for (int s3 = 0; s3 < S3; ++s3) {
+        const int i = s3 * 32 + (int)lane;
+        q3[s3] = make_uint4(0u, 0u, 0u, 0u);
+        if (a.K >= 3 && i < U3)
+            q3[s3] = __ldg(reinterpret_cast<const uint4 *>(a.h2 + (size_t)__ldg(arow + i / Q) * DD) + i % Q);
+    }
+    int n = 0;
+    pk[n++] = lane < (unsigned)D ? classify(x1, 1) : -1;
+#pragma unroll
+    for (int s2 = 0; s2 < (Q + 31) / 32; ++s2) {
+        const bool ok = a.K >= 2 && s2 * 32 + (int)lane < Q;
+        pk[n++] = ok ? classify((int32_t)q2[s2].x, 2) : -1;
+        pk[n++] = ok ? classify((int32_t)q2[s2].y, 2) : -1;
+        pk[n++] = ok ? classify((int32_t)q2[s2].z, 2) : -1;
+        pk[n++] = ok ? classify((int32_t)q2[s2].w, 2) : -1;
+    }
+#pragma unroll
+    for (int s3 = 0; s3 < S3; ++s3) {
+        const bool ok = a.K >= 3 && s3 * 32 + (int)lane < U3;
+        pk[n++] = ok ? classify((int32_t)q3[s3].x, 3) : -1;
+        pk[n++] = ok ? classify((int32_t)q3[s3].y, 3) : -1;
+        pk[n++] = ok ? classify((int32_t)q3[s3].z, 3) : -1;
+        pk[n++] = ok ? classify((int32_t)q3[s3].w, 3) : -1;
+    }
+#pragma unroll
+    for (int k = 0; k < NV; ++k)
+        if (pk[k] >= 0) atomicAdd(cur + (pk[k] >> 16), 1u);
+    __syncwarp();
+    // exclusive prefix over the buckets: lane l owns keys [l * per, (l + 1) * per)
+    const int per = (nkeys + 31) / 32;
+    unsigned mine = 0u;
+    for (int k = (int)lane * per; k < min(nkeys, ((int)lane + 1) * per); ++k) mine += cur[k];
+    unsigned incl = mine;
+    for (int o = 1; o < 32; o <<= 1) {
+        const unsigned t = __shfl_up_sync(0xffffffffu, incl, o);
+        if ((int)lane >= o) incl += t;
+    }
+    unsigned run = incl - mine;
+    uint16_t *offrow = a.off + (size_t)v * a.off_stride;
+    for (int k = (int)lane * per; k < min(nkeys, ((int)lane + 1) * per); ++k) {
+        const unsigned c = cur[k];
+        offrow[k] = (uint16_t)run;
+        cur[k] = run;
+        run += c;
+    }
+    const unsigned total = __shfl_sync(0xffffffffu, incl, 31);
+    if (lane == 0) offrow[nkeys] = (uint16_t)total;
+    __syncwarp();
+#pragma unroll
+    for (int k = 0; k < NV; ++k)
+        if (pk[k] >= 0) row[atomicAdd(cur + (pk[k] >> 16), 1u)] = (uint16_t)(pk[k] & 0xffff);
+    __syncwarp();
+    uint16_t *dst = a.ent + (size_t)v * a.cap;
+    for (unsigned k = lane; k < total; k += 32) dst[k] = row[k];
+    __syncwarp();
+}
+
 template <int D>
 __global__ void __launch_bounds__(kIndexBlock) walk_index_kernel(const WalkIndexArgs a) {
     __shared__ unsigned s_cur[kIndexBlock / 32][kIndexMaxKeys];
@@ -614,6 +703,12 @@ __global__ void __launch_bounds__(kIndexBlock) walk_index_kernel(const WalkIndex
          v += (int)((gridDim.x * blockDim.x) >> 5)) {
         for (int k = (int)lane; k < nkeys; k += 32) cur[k] = 0u;
         __syncwarp();
+        if constexpr (D > 0 && D <= 8 && (D * D) % 4 == 0 && D % 4 == 0) {
+            if (a.K <= 3) {
+                index_row_regs<D>(a, v, lane, cur, row, nkeys);
+                continue;
+            }
+        }
         // pass 1: bucket sizes
         for_walk_ends<D>(a, v, lane, [&](const int32_t w, const int L) {
             const int j = src_of(w);
@@ -673,12 +768,9 @@ constexpr int kWalkMaxNC = 64;    // row width (uint4 chunks) the per-warp buffe
 // Shared-memory bytes of the walk buffers of one warp.
 __host__ __device__ constexpr int walk_smem_per_warp(int nC) { return nC * 16 * 2 + kWalkMaxNC * 4; }
 
-// A row's index entries of this batch: bucket bounds (lanes 0..K hold off[bK + lane])
-// and its first 64 entries (lanes hold entries e0 + lane and e0 + 32 + lane, or -1).
-struct WalkRowLoad {
-    int o;
-    int x0, x1;
-};
+// Rows a warp's walk step fetches together: one round trip for the bucket bounds
+// and one for the entries serve this many rows.
+constexpr int kWalkRows = 4;
 
 static __device__ __noinline__ void walk_rows(const WalkArgs &w, unsigned char *smem, const unsigned gwarp,
                                               const unsigned nwarps, unsigned long long *s_cnt) {
@@ -690,119 +782,119 @@ static __device__ __noinline__ void walk_rows(const WalkArgs &w, unsigned char *
     uint32_t *Fb = reinterpret_cast<uint32_t *>(Fb4);
     uint32_t *flw = reinterpret_cast<uint32_t *>(Fb4 + w.nC);
     const int K = w.K, rpg = w.rows_per_group;
+    const int lrpg = __ffs(rpg) - 1;                    // rpg = 32 / gcd(nC, 32): a power of two
     unsigned cnt[4] = {0u, 0u, 0u, 0u};
     const int gwords = (rpg * w.nC) >> 5;               // flag words per group
     const unsigned ntiles = (w.items + 31u) >> 5;
-    // this warp's rows in order: the rows of groups gwarp, gwarp + nwarps, ...
-    auto next_row = [&](const int v) -> int {
-        if (v < 0) return -1;
-        int n = v + 1;
-        if (n % rpg == 0) n = (n / rpg - 1 + (int)nwarps) * rpg;
-        return n < w.rows ? n : -1;
+    // i-th row of this warp: row i % rpg of its (i / rpg)-th group gwarp, gwarp + nwarps, ...
+    auto row_of = [&](const int i) -> int {
+        const long long v = ((long long)gwarp + (long long)nwarps * (i >> lrpg)) * rpg + (i & (rpg - 1));
+        return v < w.rows ? (int)v : -1;
     };
-    auto load_off = [&](const int v) -> int {
-        return (v >= 0 && lane <= (unsigned)K) ? (int)__ldg(w.off + (size_t)v * w.off_stride + w.b * K + lane) : 0;
+    // bucket bounds of kWalkRows rows: lane 8r + k holds off[row r][bK + k], k <= K
+    auto load_off = [&](const int i0) -> int {
+        const int r = (int)(lane >> 3), k = (int)(lane & 7u);
+        const int v = r < kWalkRows ? row_of(i0 + r) : -1;
+        return (v >= 0 && k <= K) ? (int)__ldg(w.off + (size_t)v * w.off_stride + w.b * K + k) : 0;
     };
-    auto load_ents = [&](const int v, const int o) -> WalkRowLoad {
-        WalkRowLoad r{o, -1, -1};
-        const int e0 = __shfl_sync(0xffffffffu, o, 0), eK = __shfl_sync(0xffffffffu, o, K);
-        if (v >= 0) {
-            const uint16_t *ents = w.ent + (size_t)v * w.cap;
-            if (e0 + (int)lane < eK) r.x0 = __ldg(ents + e0 + lane);
-            if (e0 + 32 + (int)lane < eK) r.x1 = __ldg(ents + e0 + 32 + lane);
+    int i0 = 0;
+    int o = load_off(0);
+    while (row_of(i0) >= 0) {
+        // the first 64 entries of each of the step's rows, all in flight together
+        int x0[kWalkRows], x1[kWalkRows];
+#pragma unroll
+        for (int r = 0; r < kWalkRows; ++r) {
+            const int v = row_of(i0 + r);
+            const int e0 = __shfl_sync(0xffffffffu, o, 8 * r), eK = __shfl_sync(0xffffffffu, o, 8 * r + K);
+            const uint16_t *ents = w.ent + (size_t)(v >= 0 ? v : 0) * w.cap;
+            x0[r] = (v >= 0 && e0 + (int)lane < eK) ? (int)__ldg(ents + e0 + lane) : -1;
+            x1[r] = (v >= 0 && e0 + 32 + (int)lane < eK) ? (int)__ldg(ents + e0 + 32 + lane) : -1;
         }
-        return r;
-    };
-    int v = (int)gwarp * rpg;
-    if (v >= w.rows) v = -1;
-    // two rows ahead: the entries of the next row and the bounds of the one after
-    WalkRowLoad cur = load_ents(v, load_off(v));
-    int vn = next_row(v);
-    int o_n = load_off(vn);
-    for (; v >= 0;) {
-        const int vnn = next_row(vn);
-        const WalkRowLoad nxt = load_ents(vn, o_n);
-        const int o_nn = load_off(vnn);
-        const int r = v % rpg;
-        if (r == 0)
-            for (int k = (int)lane; k < gwords; k += 32) flw[k] = 0u;
-        // the row starts as its padding bits and the diagonal
-        for (int c = (int)lane; c < w.nC; c += 32) {
-            Vb4[c] = pad_mask(c, w.ns);
-            Fb4[c] = u4zero();
-        }
-        __syncwarp();
-        if (lane == 0) {
-            const int g = w.inv ? __ldg(w.inv + v) : v - w.src_first;
-            const int j = g - w.first;
-            if (g >= 0 && (unsigned)j < (unsigned)w.ns) Vb[j >> 5] |= 1u << (j & 31);
-        }
-        __syncwarp();
-        // the entries level by level (bucket order is level order)
-        const int e0 = __shfl_sync(0xffffffffu, cur.o, 0);
-        const int e1 = __shfl_sync(0xffffffffu, cur.o, 1);
-        const int e2 = __shfl_sync(0xffffffffu, cur.o, K >= 2 ? 2 : 1);
-        const int e3 = __shfl_sync(0xffffffffu, cur.o, K >= 3 ? 3 : 1);
-        const int eK = __shfl_sync(0xffffffffu, cur.o, K);
-        auto level_of = [&](const int i) { return i < e1 ? 1 : (i < e2 ? 2 : (i < e3 ? 3 : 4)); };
-        auto put = [&](const int j, const int L) {
-            const uint32_t bit = 1u << (j & 31);
-            const uint32_t old = atomicOr(Vb + (j >> 5), bit);
-            if (!(old & bit)) {
-                cnt[L - 1] += 1u;
-                if (L == K) atomicOr(Fb + (j >> 5), bit);
+        const int o_next = load_off(i0 + kWalkRows);      // the next step's bounds
+#pragma unroll
+        for (int r = 0; r < kWalkRows; ++r) {
+            const int v = row_of(i0 + r);
+            if (v < 0) break;
+            const int rg = (i0 + r) & (rpg - 1);          // row within its group
+            if (rg == 0)
+                for (int k = (int)lane; k < gwords; k += 32) flw[k] = 0u;
+            // the row starts as its padding bits and the diagonal
+            for (int c = (int)lane; c < w.nC; c += 32) {
+                Vb4[c] = pad_mask(c, w.ns);
+                Fb4[c] = u4zero();
             }
-        };
-        const int L0 = cur.x0 >= 0 ? level_of(e0 + (int)lane) : 0;
-        const int L1 = cur.x1 >= 0 ? level_of(e0 + 32 + (int)lane) : 0;
-        for (int L = 1; L <= K; ++L) {
-            if (L0 == L) put(cur.x0, L);
-            if (L1 == L) put(cur.x1, L);
             __syncwarp();
-        }
-        // rows with more than 64 entries in this batch: the rest, 32 at a time,
-        // still in level order (every chunk's levels are at least the last one's)
-        for (int base = e0 + 64; base < eK; base += 32) {
-            const int i = base + (int)lane;
-            const int x = i < eK ? (int)__ldg(w.ent + (size_t)v * w.cap + i) : -1;
-            const int Li = x >= 0 ? level_of(i) : 0;
+            if (lane == 0) {
+                const int g = w.inv ? __ldg(w.inv + v) : v - w.src_first;
+                const int j = g - w.first;
+                if (g >= 0 && (unsigned)j < (unsigned)w.ns) Vb[j >> 5] |= 1u << (j & 31);
+            }
+            __syncwarp();
+            // the entries level by level (bucket order is level order)
+            const int e0 = __shfl_sync(0xffffffffu, o, 8 * r);
+            const int e1 = __shfl_sync(0xffffffffu, o, 8 * r + 1);
+            const int e2 = __shfl_sync(0xffffffffu, o, 8 * r + (K >= 2 ? 2 : 1));
+            const int e3 = __shfl_sync(0xffffffffu, o, 8 * r + (K >= 3 ? 3 : 1));
+            const int eK = __shfl_sync(0xffffffffu, o, 8 * r + K);
+            auto level_of = [&](const int i) { return i < e1 ? 1 : (i < e2 ? 2 : (i < e3 ? 3 : 4)); };
+            auto put = [&](const int j, const int L) {
+                const uint32_t bit = 1u << (j & 31);
+                const uint32_t old = atomicOr(Vb + (j >> 5), bit);
+                if (!(old & bit)) {
+                    cnt[L - 1] += 1u;
+                    if (L == K) atomicOr(Fb + (j >> 5), bit);
+                }
+            };
+            const int La = x0[r] >= 0 ? level_of(e0 + (int)lane) : 0;
+            const int Lb = x1[r] >= 0 ? level_of(e0 + 32 + (int)lane) : 0;
             for (int L = 1; L <= K; ++L) {
-                if (Li == L) put(x, L);
+                if (La == L) put(x0[r], L);
+                if (Lb == L) put(x1[r], L);
+                __syncwarp();
+            }
+            // rows with more than 64 entries in this batch: the rest, 32 at a time,
+            // still in level order (every chunk's levels are at least the last one's)
+            for (int base = e0 + 64; base < eK; base += 32) {
+                const int i = base + (int)lane;
+                const int x = i < eK ? (int)__ldg(w.ent + (size_t)v * w.cap + i) : -1;
+                const int Li = x >= 0 ? level_of(i) : 0;
+                for (int L = 1; L <= K; ++L) {
+                    if (Li == L) put(x, L);
+                    __syncwarp();
+                }
+            }
+            // write the row: V = V_K (padding included), F = new at level K, and the
+            // flag bits of F (one ballot per 32 chunks; lane 0 merges it into the
+            // group's words)
+            const unsigned t0 = (unsigned)v * (unsigned)w.nC;
+            const unsigned b0 = (unsigned)rg * (unsigned)w.nC;   // chunk index within the group
+            for (int cb = 0; cb < w.nC; cb += 32) {
+                const int c = cb + (int)lane;
+                bool any = false;
+                if (c < w.nC) {
+                    const uint4 vv = Vb4[c], ff = Fb4[c];
+                    w.V[t0 + c] = vv;
+                    w.F[t0 + c] = ff;
+                    any = u4any(ff);
+                }
+                const unsigned m = __ballot_sync(0xffffffffu, any);
+                if (lane == 0 && m) {
+                    const unsigned first = b0 + (unsigned)cb, off = first & 31u;
+                    flw[first >> 5] |= m << off;
+                    if (off && (m >> (32u - off))) flw[(first >> 5) + 1] |= m >> (32u - off);  // stays in the group
+                }
+            }
+            __syncwarp();
+            if (rg == rpg - 1 || v == w.rows - 1) {
+                // the group's flag words (the group starts on a tile boundary)
+                const unsigned tile0 = (unsigned)(v >> lrpg) * (unsigned)gwords;
+                for (int k = (int)lane; k < gwords; k += 32)
+                    if (tile0 + k < ntiles) w.fl[tile0 + k] = flw[k];
                 __syncwarp();
             }
         }
-        // write the row: V = V_K (padding included), F = new at level K, and the flag
-        // bits of F (one ballot per 32 chunks; lane 0 merges it into the group's words)
-        const unsigned t0 = (unsigned)v * (unsigned)w.nC;
-        const unsigned b0 = (unsigned)r * (unsigned)w.nC;   // chunk index within the group
-        for (int cb = 0; cb < w.nC; cb += 32) {
-            const int c = cb + (int)lane;
-            bool any = false;
-            if (c < w.nC) {
-                const uint4 vv = Vb4[c], ff = Fb4[c];
-                w.V[t0 + c] = vv;
-                w.F[t0 + c] = ff;
-                any = u4any(ff);
-            }
-            const unsigned m = __ballot_sync(0xffffffffu, any);
-            if (lane == 0 && m) {
-                const unsigned first = b0 + (unsigned)cb, off = first & 31u;
-                flw[first >> 5] |= m << off;
-                if (off && (m >> (32u - off))) flw[(first >> 5) + 1] |= m >> (32u - off);  // stays in the group
-            }
-        }
-        __syncwarp();
-        if (r == rpg - 1 || v == w.rows - 1) {
-            // the group's flag words (the group starts on a tile boundary)
-            const unsigned tile0 = (unsigned)(v / rpg) * (unsigned)gwords;
-            for (int k = (int)lane; k < gwords; k += 32)
-                if (tile0 + k < ntiles) w.fl[tile0 + k] = flw[k];
-            __syncwarp();
-        }
-        v = vn;
-        vn = vnn;
-        cur = nxt;
-        o_n = o_nn;
+        i0 += kWalkRows;
+        o = o_next;
     }
 #pragma unroll
     for (int L = 0; L < 4; ++L) {
@@ -813,9 +905,22 @@ static __device__ __noinline__ void walk_rows(const WalkArgs &w, unsigned char *
 
 // H2[v][i*d + j] = adj[adj[v][i]][j]: the level-2 walk ends of every row, built once
 // per evaluation (after the table's range check: a bad table builds nothing).
+// When d % 4 == 0 a thread copies 16 bytes (one quarter-row of a neighbour's row).
 static __global__ void h2_kernel(const int32_t *adj, int32_t *h2, int rows, int d, const int *bad) {
     if (bad && *bad) return;
-    const long long dd = (long long)d * d, n = (long long)rows * dd;
+    const long long dd = (long long)d * d;
+    if (d % 4 == 0) {
+        const int q = d / 4;                           // uint4 per adjacency row
+        const long long n = (long long)rows * d * q;   // uint4 of H2
+        for (long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x; k < n;
+             k += (long long)gridDim.x * blockDim.x) {
+            const long long v = k / ((long long)d * q), r = k % ((long long)d * q);
+            const int p = __ldg(adj + v * d + r / q);
+            reinterpret_cast<uint4 *>(h2)[k] = __ldg(reinterpret_cast<const uint4 *>(adj + (size_t)p * d) + r % q);
+        }
+        return;
+    }
+    const long long n = (long long)rows * dd;
     for (long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x; k < n;
          k += (long long)gridDim.x * blockDim.x) {
         const long long v = k / dd, r = k % dd;

@@ -258,16 +258,21 @@ long long walk_cap_for(int d, int K) {
 // per row stay within 600 (d = 8: 3 levels, 584 ends; d = 16: 2; d = 4: 4), within
 // the index kernel's row buffer and bucket count (kIndexMaxCap ends, kIndexMaxKeys
 // = batches * K buckets), with the level-2 table (rows * d^2 int32, K >= 3) within
-// 64 MiB and the index (rows * (ends + buckets) uint16) within 1 GiB.
-// GG_WALK_LEVELS overrides the depth (0 = off; still within those limits).
+// 64 MiB and the index (rows * (ends + buckets) uint16) within 1 GiB; off for
+// evaluations of a single source batch.  GG_WALK_LEVELS overrides the depth (0 = off;
+// still within the size limits).
 int walk_levels(const gg_engine *e) {
     const int env = env_int("GG_WALK_LEVELS", e->walk_pref);
     const int d = e->d;
     if (d <= 0 || e->nC > gg::kWalkMaxNC || env == 0) return 0;
     int K = 0;
     for (int k = 1; k <= 4 && walk_cap_for(d, k) <= 600; ++k) K = k;
-    if (env > 0) K = std::min(env, 4);
     const long long nb = ((long long)e->reps.size() + e->batch_bits - 1) / e->batch_bits;
+    // The index costs one pass over every row's walk ends per evaluation; with a
+    // single source batch the pass it saves is not worth it (n = 4096, d = 16: 0.070
+    // against 0.060 ms; a lift with one batch: 0.135 against 0.097 ms).
+    if (nb < 2) K = 0;
+    if (env > 0) K = std::min(env, 4);
     for (; K > 0; --K) {
         const long long cap = walk_cap_for(d, K), keys = nb * K;
         const bool ok = cap <= gg::kIndexMaxCap && keys <= gg::kIndexMaxKeys &&

@@ -768,9 +768,12 @@ constexpr int kWalkMaxNC = 64;    // row width (uint4 chunks) the per-warp buffe
 // Shared-memory bytes of the walk buffers of one warp.
 __host__ __device__ constexpr int walk_smem_per_warp(int nC) { return nC * 16 * 2 + kWalkMaxNC * 4; }
 
-// Rows a warp's walk step fetches together: one round trip for the bucket bounds
-// and one for the entries serve this many rows.
-constexpr int kWalkRows = 4;
+// A row's index entries of this batch: bucket bounds (lanes 0..K hold off[bK + lane])
+// and its first 64 entries (lanes hold entries e0 + lane and e0 + 32 + lane, or -1).
+struct WalkRowLoad {
+    int o;
+    int x0, x1;
+};
 
 static __device__ __noinline__ void walk_rows(const WalkArgs &w, unsigned char *smem, const unsigned gwarp,
                                               const unsigned nwarps, unsigned long long *s_cnt) {
@@ -782,119 +785,119 @@ static __device__ __noinline__ void walk_rows(const WalkArgs &w, unsigned char *
     uint32_t *Fb = reinterpret_cast<uint32_t *>(Fb4);
     uint32_t *flw = reinterpret_cast<uint32_t *>(Fb4 + w.nC);
     const int K = w.K, rpg = w.rows_per_group;
-    const int lrpg = __ffs(rpg) - 1;                    // rpg = 32 / gcd(nC, 32): a power of two
     unsigned cnt[4] = {0u, 0u, 0u, 0u};
     const int gwords = (rpg * w.nC) >> 5;               // flag words per group
     const unsigned ntiles = (w.items + 31u) >> 5;
-    // i-th row of this warp: row i % rpg of its (i / rpg)-th group gwarp, gwarp + nwarps, ...
-    auto row_of = [&](const int i) -> int {
-        const long long v = ((long long)gwarp + (long long)nwarps * (i >> lrpg)) * rpg + (i & (rpg - 1));
-        return v < w.rows ? (int)v : -1;
+    // this warp's rows in order: the rows of groups gwarp, gwarp + nwarps, ...
+    auto next_row = [&](const int v) -> int {
+        if (v < 0) return -1;
+        int n = v + 1;
+        if (n % rpg == 0) n = (n / rpg - 1 + (int)nwarps) * rpg;
+        return n < w.rows ? n : -1;
     };
-    // bucket bounds of kWalkRows rows: lane 8r + k holds off[row r][bK + k], k <= K
-    auto load_off = [&](const int i0) -> int {
-        const int r = (int)(lane >> 3), k = (int)(lane & 7u);
-        const int v = r < kWalkRows ? row_of(i0 + r) : -1;
-        return (v >= 0 && k <= K) ? (int)__ldg(w.off + (size_t)v * w.off_stride + w.b * K + k) : 0;
+    auto load_off = [&](const int v) -> int {
+        return (v >= 0 && lane <= (unsigned)K) ? (int)__ldg(w.off + (size_t)v * w.off_stride + w.b * K + lane) : 0;
     };
-    int i0 = 0;
-    int o = load_off(0);
-    while (row_of(i0) >= 0) {
-        // the first 64 entries of each of the step's rows, all in flight together
-        int x0[kWalkRows], x1[kWalkRows];
-#pragma unroll
-        for (int r = 0; r < kWalkRows; ++r) {
-            const int v = row_of(i0 + r);
-            const int e0 = __shfl_sync(0xffffffffu, o, 8 * r), eK = __shfl_sync(0xffffffffu, o, 8 * r + K);
-            const uint16_t *ents = w.ent + (size_t)(v >= 0 ? v : 0) * w.cap;
-            x0[r] = (v >= 0 && e0 + (int)lane < eK) ? (int)__ldg(ents + e0 + lane) : -1;
-            x1[r] = (v >= 0 && e0 + 32 + (int)lane < eK) ? (int)__ldg(ents + e0 + 32 + lane) : -1;
+    auto load_ents = [&](const int v, const int o) -> WalkRowLoad {
+        WalkRowLoad r{o, -1, -1};
+        const int e0 = __shfl_sync(0xffffffffu, o, 0), eK = __shfl_sync(0xffffffffu, o, K);
+        if (v >= 0) {
+            const uint16_t *ents = w.ent + (size_t)v * w.cap;
+            if (e0 + (int)lane < eK) r.x0 = __ldg(ents + e0 + lane);
+            if (e0 + 32 + (int)lane < eK) r.x1 = __ldg(ents + e0 + 32 + lane);
         }
-        const int o_next = load_off(i0 + kWalkRows);      // the next step's bounds
-#pragma unroll
-        for (int r = 0; r < kWalkRows; ++r) {
-            const int v = row_of(i0 + r);
-            if (v < 0) break;
-            const int rg = (i0 + r) & (rpg - 1);          // row within its group
-            if (rg == 0)
-                for (int k = (int)lane; k < gwords; k += 32) flw[k] = 0u;
-            // the row starts as its padding bits and the diagonal
-            for (int c = (int)lane; c < w.nC; c += 32) {
-                Vb4[c] = pad_mask(c, w.ns);
-                Fb4[c] = u4zero();
+        return r;
+    };
+    int v = (int)gwarp * rpg;
+    if (v >= w.rows) v = -1;
+    // two rows ahead: the entries of the next row and the bounds of the one after
+    WalkRowLoad cur = load_ents(v, load_off(v));
+    int vn = next_row(v);
+    int o_n = load_off(vn);
+    for (; v >= 0;) {
+        const int vnn = next_row(vn);
+        const WalkRowLoad nxt = load_ents(vn, o_n);
+        const int o_nn = load_off(vnn);
+        const int r = v % rpg;
+        if (r == 0)
+            for (int k = (int)lane; k < gwords; k += 32) flw[k] = 0u;
+        // the row starts as its padding bits and the diagonal
+        for (int c = (int)lane; c < w.nC; c += 32) {
+            Vb4[c] = pad_mask(c, w.ns);
+            Fb4[c] = u4zero();
+        }
+        __syncwarp();
+        if (lane == 0) {
+            const int g = w.inv ? __ldg(w.inv + v) : v - w.src_first;
+            const int j = g - w.first;
+            if (g >= 0 && (unsigned)j < (unsigned)w.ns) Vb[j >> 5] |= 1u << (j & 31);
+        }
+        __syncwarp();
+        // the entries level by level (bucket order is level order)
+        const int e0 = __shfl_sync(0xffffffffu, cur.o, 0);
+        const int e1 = __shfl_sync(0xffffffffu, cur.o, 1);
+        const int e2 = __shfl_sync(0xffffffffu, cur.o, K >= 2 ? 2 : 1);
+        const int e3 = __shfl_sync(0xffffffffu, cur.o, K >= 3 ? 3 : 1);
+        const int eK = __shfl_sync(0xffffffffu, cur.o, K);
+        auto level_of = [&](const int i) { return i < e1 ? 1 : (i < e2 ? 2 : (i < e3 ? 3 : 4)); };
+        auto put = [&](const int j, const int L) {
+            const uint32_t bit = 1u << (j & 31);
+            const uint32_t old = atomicOr(Vb + (j >> 5), bit);
+            if (!(old & bit)) {
+                cnt[L - 1] += 1u;
+                if (L == K) atomicOr(Fb + (j >> 5), bit);
             }
+        };
+        const int L0 = cur.x0 >= 0 ? level_of(e0 + (int)lane) : 0;
+        const int L1 = cur.x1 >= 0 ? level_of(e0 + 32 + (int)lane) : 0;
+        for (int L = 1; L <= K; ++L) {
+            if (L0 == L) put(cur.x0, L);
+            if (L1 == L) put(cur.x1, L);
             __syncwarp();
-            if (lane == 0) {
-                const int g = w.inv ? __ldg(w.inv + v) : v - w.src_first;
-                const int j = g - w.first;
-                if (g >= 0 && (unsigned)j < (unsigned)w.ns) Vb[j >> 5] |= 1u << (j & 31);
-            }
-            __syncwarp();
-            // the entries level by level (bucket order is level order)
-            const int e0 = __shfl_sync(0xffffffffu, o, 8 * r);
-            const int e1 = __shfl_sync(0xffffffffu, o, 8 * r + 1);
-            const int e2 = __shfl_sync(0xffffffffu, o, 8 * r + (K >= 2 ? 2 : 1));
-            const int e3 = __shfl_sync(0xffffffffu, o, 8 * r + (K >= 3 ? 3 : 1));
-            const int eK = __shfl_sync(0xffffffffu, o, 8 * r + K);
-            auto level_of = [&](const int i) { return i < e1 ? 1 : (i < e2 ? 2 : (i < e3 ? 3 : 4)); };
-            auto put = [&](const int j, const int L) {
-                const uint32_t bit = 1u << (j & 31);
-                const uint32_t old = atomicOr(Vb + (j >> 5), bit);
-                if (!(old & bit)) {
-                    cnt[L - 1] += 1u;
-                    if (L == K) atomicOr(Fb + (j >> 5), bit);
-                }
-            };
-            const int La = x0[r] >= 0 ? level_of(e0 + (int)lane) : 0;
-            const int Lb = x1[r] >= 0 ? level_of(e0 + 32 + (int)lane) : 0;
+        }
+        // rows with more than 64 entries in this batch: the rest, 32 at a time,
+        // still in level order (every chunk's levels are at least the last one's)
+        for (int base = e0 + 64; base < eK; base += 32) {
+            const int i = base + (int)lane;
+            const int x = i < eK ? (int)__ldg(w.ent + (size_t)v * w.cap + i) : -1;
+            const int Li = x >= 0 ? level_of(i) : 0;
             for (int L = 1; L <= K; ++L) {
-                if (La == L) put(x0[r], L);
-                if (Lb == L) put(x1[r], L);
-                __syncwarp();
-            }
-            // rows with more than 64 entries in this batch: the rest, 32 at a time,
-            // still in level order (every chunk's levels are at least the last one's)
-            for (int base = e0 + 64; base < eK; base += 32) {
-                const int i = base + (int)lane;
-                const int x = i < eK ? (int)__ldg(w.ent + (size_t)v * w.cap + i) : -1;
-                const int Li = x >= 0 ? level_of(i) : 0;
-                for (int L = 1; L <= K; ++L) {
-                    if (Li == L) put(x, L);
-                    __syncwarp();
-                }
-            }
-            // write the row: V = V_K (padding included), F = new at level K, and the
-            // flag bits of F (one ballot per 32 chunks; lane 0 merges it into the
-            // group's words)
-            const unsigned t0 = (unsigned)v * (unsigned)w.nC;
-            const unsigned b0 = (unsigned)rg * (unsigned)w.nC;   // chunk index within the group
-            for (int cb = 0; cb < w.nC; cb += 32) {
-                const int c = cb + (int)lane;
-                bool any = false;
-                if (c < w.nC) {
-                    const uint4 vv = Vb4[c], ff = Fb4[c];
-                    w.V[t0 + c] = vv;
-                    w.F[t0 + c] = ff;
-                    any = u4any(ff);
-                }
-                const unsigned m = __ballot_sync(0xffffffffu, any);
-                if (lane == 0 && m) {
-                    const unsigned first = b0 + (unsigned)cb, off = first & 31u;
-                    flw[first >> 5] |= m << off;
-                    if (off && (m >> (32u - off))) flw[(first >> 5) + 1] |= m >> (32u - off);  // stays in the group
-                }
-            }
-            __syncwarp();
-            if (rg == rpg - 1 || v == w.rows - 1) {
-                // the group's flag words (the group starts on a tile boundary)
-                const unsigned tile0 = (unsigned)(v >> lrpg) * (unsigned)gwords;
-                for (int k = (int)lane; k < gwords; k += 32)
-                    if (tile0 + k < ntiles) w.fl[tile0 + k] = flw[k];
+                if (Li == L) put(x, L);
                 __syncwarp();
             }
         }
-        i0 += kWalkRows;
-        o = o_next;
+        // write the row: V = V_K (padding included), F = new at level K, and the flag
+        // bits of F (one ballot per 32 chunks; lane 0 merges it into the group's words)
+        const unsigned t0 = (unsigned)v * (unsigned)w.nC;
+        const unsigned b0 = (unsigned)r * (unsigned)w.nC;   // chunk index within the group
+        for (int cb = 0; cb < w.nC; cb += 32) {
+            const int c = cb + (int)lane;
+            bool any = false;
+            if (c < w.nC) {
+                const uint4 vv = Vb4[c], ff = Fb4[c];
+                w.V[t0 + c] = vv;
+                w.F[t0 + c] = ff;
+                any = u4any(ff);
+            }
+            const unsigned m = __ballot_sync(0xffffffffu, any);
+            if (lane == 0 && m) {
+                const unsigned first = b0 + (unsigned)cb, off = first & 31u;
+                flw[first >> 5] |= m << off;
+                if (off && (m >> (32u - off))) flw[(first >> 5) + 1] |= m >> (32u - off);  // stays in the group
+            }
+        }
+        __syncwarp();
+        if (r == rpg - 1 || v == w.rows - 1) {
+            // the group's flag words (the group starts on a tile boundary)
+            const unsigned tile0 = (unsigned)(v / rpg) * (unsigned)gwords;
+            for (int k = (int)lane; k < gwords; k += 32)
+                if (tile0 + k < ntiles) w.fl[tile0 + k] = flw[k];
+            __syncwarp();
+        }
+        v = vn;
+        vn = vnn;
+        cur = nxt;
+        o_n = o_nn;
     }
 #pragma unroll
     for (int L = 0; L < 4; ++L) {
@@ -953,6 +956,100 @@ struct LoopState {
     int L_next;                  // first level the level loop runs (after a walk pass)
 };
 
+// walk_rows for rows of exactly 32 chunks (4096-source batches): a row is one tile
+// and one flag word, so lane c owns chunk c of the row, the diagonal bit is set by
+// its lane while the row is initialised, and the frontier's flag word is one ballot.
+// Launch-constant arguments are read from the kernel parameters (`a`, grid-constant:
+// no aliasing with the shared-memory row), per-batch ones come in registers.
+static __device__ __noinline__ void walk_rows32(const BfsArgs &a, const int b, const int first, const int ns,
+                                                uint4 *F, uint32_t *fl, uint4 *Vb4, uint4 *Fb4,
+                                                const unsigned gwarp, const unsigned nwarps,
+                                                unsigned long long *s_cnt) {
+    const unsigned lane = threadIdx.x & 31u;
+    uint32_t *Vb = reinterpret_cast<uint32_t *>(Vb4);
+    uint32_t *Fb = reinterpret_cast<uint32_t *>(Fb4);
+    const int K = a.walk_K, rows = a.rows;
+    const uint16_t *off_b = a.walk_off + b * K;
+    const int off_stride = a.walk_off_stride, cap = a.walk_cap;
+    const uint4 pad = pad_mask((int)lane, ns);
+    unsigned cnt[4] = {0u, 0u, 0u, 0u};
+    int v = (int)gwarp;
+    // one row ahead: the next row's bucket bounds, this row's entries
+    int o = (v < rows && lane <= (unsigned)K) ? (int)__ldg(off_b + (size_t)v * off_stride + lane) : 0;
+    int x0 = -1, x1 = -1;
+    {
+        const int e0 = __shfl_sync(0xffffffffu, o, 0), eK = __shfl_sync(0xffffffffu, o, K);
+        if (v < rows && e0 + (int)lane < eK) x0 = __ldg(a.walk_ent + (size_t)v * cap + e0 + lane);
+        if (v < rows && e0 + 32 + (int)lane < eK) x1 = __ldg(a.walk_ent + (size_t)v * cap + e0 + 32 + lane);
+    }
+    for (; v < rows; v += (int)nwarps) {
+        const int vn = v + (int)nwarps;
+        const int o_n = (vn < rows && lane <= (unsigned)K) ? (int)__ldg(off_b + (size_t)vn * off_stride + lane) : 0;
+        const int e0 = __shfl_sync(0xffffffffu, o, 0);
+        const int e1 = __shfl_sync(0xffffffffu, o, 1);
+        const int e2 = __shfl_sync(0xffffffffu, o, K >= 2 ? 2 : 1);
+        const int e3 = __shfl_sync(0xffffffffu, o, K >= 3 ? 3 : 1);
+        const int eK = __shfl_sync(0xffffffffu, o, K);
+        // the row: padding, and the diagonal in the chunk of its lane
+        uint4 init = pad;
+        {
+            const int g = a.inv ? __ldg(a.inv + v) : v - a.src_first;
+            const int j = g - first;
+            if (g >= 0 && (unsigned)j < (unsigned)ns && (unsigned)(j >> 7) == lane) {
+                const unsigned bit = 1u << (j & 31), comp = ((unsigned)j >> 5) & 3u;
+                if (comp == 0u) init.x |= bit; else if (comp == 1u) init.y |= bit;
+                else if (comp == 2u) init.z |= bit; else init.w |= bit;
+            }
+        }
+        Vb4[lane] = init;
+        Fb4[lane] = u4zero();
+        __syncwarp();
+        auto level_of = [&](const int i) { return i < e1 ? 1 : (i < e2 ? 2 : (i < e3 ? 3 : 4)); };
+        auto put = [&](const int j, const int L) {
+            const uint32_t bit = 1u << (j & 31);
+            const uint32_t old = atomicOr(Vb + (j >> 5), bit);
+            if (!(old & bit)) {
+                cnt[L - 1] += 1u;
+                if (L == K) atomicOr(Fb + (j >> 5), bit);
+            }
+        };
+        const int La = x0 >= 0 ? level_of(e0 + (int)lane) : 0;
+        const int Lb = x1 >= 0 ? level_of(e0 + 32 + (int)lane) : 0;
+        for (int L = 1; L <= K; ++L) {
+            if (La == L) put(x0, L);
+            if (Lb == L) put(x1, L);
+            __syncwarp();
+        }
+        for (int base = e0 + 64; base < eK; base += 32) {   // rows with more than 64 entries here
+            const int i = base + (int)lane;
+            const int x = i < eK ? (int)__ldg(a.walk_ent + (size_t)v * cap + i) : -1;
+            const int Li = x >= 0 ? level_of(i) : 0;
+            for (int L = 1; L <= K; ++L) {
+                if (Li == L) put(x, L);
+                __syncwarp();
+            }
+        }
+        // the next row's entries (its bounds arrived while this row was built)
+        const int en0 = __shfl_sync(0xffffffffu, o_n, 0), enK = __shfl_sync(0xffffffffu, o_n, K);
+        x0 = (vn < rows && en0 + (int)lane < enK) ? (int)__ldg(a.walk_ent + (size_t)vn * cap + en0 + lane) : -1;
+        x1 = (vn < rows && en0 + 32 + (int)lane < enK) ? (int)__ldg(a.walk_ent + (size_t)vn * cap + en0 + 32 + lane)
+                                                        : -1;
+        // write the row and its flag word
+        const uint4 vv = Vb4[lane], ff = Fb4[lane];
+        a.V[(size_t)v * 32 + lane] = vv;
+        F[(size_t)v * 32 + lane] = ff;
+        const unsigned m = __ballot_sync(0xffffffffu, u4any(ff));
+        if (lane == 0) fl[v] = m;
+        __syncwarp();
+        o = o_n;
+    }
+#pragma unroll
+    for (int L = 0; L < 4; ++L) {
+        const unsigned t = __reduce_add_sync(0xffffffffu, cnt[L]);
+        if (lane == 0 && t) atomicAdd(s_cnt + L, (unsigned long long)t);
+    }
+}
+
 // The walk pass of batch b, its counts and the loop state it leaves (levels
 // 1..K done; S.L_next = K + 1, or the level at which the batch ended).  Out of
 // line so that the level loop keeps its registers.  Returns the barrier count
@@ -986,7 +1083,14 @@ static __device__ __noinline__ unsigned walk_batch(const BfsArgs &a, const int b
         w.rows_per_group = a.walk_rpg;
     }
     __syncthreads();
-    walk_rows(w, reinterpret_cast<unsigned char *>(s_adj) + a.walk_smem_off, gtid >> 5, nthr >> 5, s_wcnt);
+    if (a.nC == 32) {
+        uint4 *Vb4 = reinterpret_cast<uint4 *>(reinterpret_cast<unsigned char *>(s_adj) + a.walk_smem_off +
+                                               (size_t)(threadIdx.x >> 5) * walk_smem_per_warp(32));
+        walk_rows32(a, b, a.src_begin + b * 128 * a.nC, ns, ((K + 1) & 1) ? a.F0 : a.F1,
+                    ((K + 1) & 1) ? a.fl0 : a.fl1, Vb4, Vb4 + 32, gtid >> 5, nthr >> 5, s_wcnt);
+    } else {
+        walk_rows(w, reinterpret_cast<unsigned char *>(s_adj) + a.walk_smem_off, gtid >> 5, nthr >> 5, s_wcnt);
+    }
     __syncthreads();
     if (threadIdx.x == 0)
         for (int L = 1; L <= K; ++L)

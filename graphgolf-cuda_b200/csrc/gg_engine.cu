@@ -624,10 +624,12 @@ gg_status run_eval(gg_engine *e, const int32_t *d_table_in, const gg_eval_opts *
             wi.off = e->d_woff;
             wi.off_stride = e->walk_off_stride;
             wi.bad = e->form == FORM_GRAPH ? e->d_bad : nullptr;
-            int sms = 0;
+            // one resident wave of blocks, each striding over the rows
+            int sms = 0, per_sm = 0;
             GG_CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, e->device));
+            GG_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, index_kernel_for(e->d), gg::kIndexBlock, 0));
             const int wgrid = (int)std::max<long long>(1, std::min<long long>(((long long)e->rows + 7) / 8,
-                                                                              (long long)sms * 8));
+                                                                              (long long)sms * std::max(per_sm, 1)));
             void *wargs[] = {&wi};
             GG_CK(cudaLaunchKernel(index_kernel_for(e->d), dim3(wgrid), dim3(gg::kIndexBlock), wargs, 0, q));
         }

@@ -766,7 +766,9 @@ struct WalkArgs {
 constexpr int kWalkMaxNC = 64;    // row width (uint4 chunks) the per-warp buffers hold
 
 // Shared-memory bytes of the walk buffers of one warp.
-__host__ __device__ constexpr int walk_smem_per_warp(int nC) { return nC * 16 * 2 + kWalkMaxNC * 4; }
+__host__ __device__ constexpr int walk_smem_per_warp(int nC) {
+    return nC == 32 ? 32 * 16 * 4 : nC * 16 * 2 + kWalkMaxNC * 4;   // walk_rows32: up to 4 level copies
+}
 
 // A row's index entries of this batch: bucket bounds (lanes 0..K hold off[bK + lane])
 // and its first 64 entries (lanes hold entries e0 + lane and e0 + 32 + lane, or -1).
@@ -957,91 +959,98 @@ struct LoopState {
 };
 
 // walk_rows for rows of exactly 32 chunks (4096-source batches): a row is one tile
-// and one flag word, so lane c owns chunk c of the row, the diagonal bit is set by
-// its lane while the row is initialised, and the frontier's flag word is one ballot.
-// Launch-constant arguments are read from the kernel parameters (`a`, grid-constant:
-// no aliasing with the shared-memory row), per-batch ones come in registers.
+// and one flag word, so lane c owns chunk c of the row.  Order-free form of the
+// level sets: each level's entries are ORed into their own shared-memory copy of the
+// row (A_L, non-returning atomics, one warp sync), then every lane builds, for its
+// own chunk, V_L = V_{L-1} | A_L from the diagonal up, counts popc(V_L) - popc(V_{L-1})
+// pairs at level L (exact: a source reached at several levels counts at the first),
+// and writes V = V_K, F = V_K & ~V_{K-1} and the frontier's flag word (one ballot).
+// Loads run two rows ahead: a row's bucket bounds two iterations before it is built,
+// its entries one iteration before.  Launch-constant arguments are read from the
+// kernel parameters (`a`, grid-constant), per-batch ones come in registers.
 static __device__ __noinline__ void walk_rows32(const BfsArgs &a, const int b, const int first, const int ns,
-                                                uint4 *F, uint32_t *fl, uint4 *Vb4, uint4 *Fb4,
+                                                uint4 *F, uint32_t *fl, uint4 *Ab4,
                                                 const unsigned gwarp, const unsigned nwarps,
                                                 unsigned long long *s_cnt) {
     const unsigned lane = threadIdx.x & 31u;
-    uint32_t *Vb = reinterpret_cast<uint32_t *>(Vb4);
-    uint32_t *Fb = reinterpret_cast<uint32_t *>(Fb4);
+    uint32_t *Ab = reinterpret_cast<uint32_t *>(Ab4);   // K copies of the row: A_1 .. A_K
     const int K = a.walk_K, rows = a.rows;
     const uint16_t *off_b = a.walk_off + b * K;
     const int off_stride = a.walk_off_stride, cap = a.walk_cap;
+    const uint16_t *ent = a.walk_ent;
     const uint4 pad = pad_mask((int)lane, ns);
     unsigned cnt[4] = {0u, 0u, 0u, 0u};
-    int v = (int)gwarp;
-    // one row ahead: the next row's bucket bounds, this row's entries
-    int o = (v < rows && lane <= (unsigned)K) ? (int)__ldg(off_b + (size_t)v * off_stride + lane) : 0;
-    int x0 = -1, x1 = -1;
-    {
+    for (int L = 0; L < K; ++L) Ab4[L * 32 + lane] = u4zero();
+    __syncwarp();
+    auto load_off = [&](const int v) -> int {
+        return (v < rows && lane <= (unsigned)K) ? (int)__ldg(off_b + (size_t)v * off_stride + lane) : 0;
+    };
+    // entries of row v: lanes hold entries e0 + lane and e0 + 32 + lane (or -1), and
+    // their levels (1..K, 0 = none)
+    auto load_ents = [&](const int v, const int o, int &x0, int &x1) {
         const int e0 = __shfl_sync(0xffffffffu, o, 0), eK = __shfl_sync(0xffffffffu, o, K);
-        if (v < rows && e0 + (int)lane < eK) x0 = __ldg(a.walk_ent + (size_t)v * cap + e0 + lane);
-        if (v < rows && e0 + 32 + (int)lane < eK) x1 = __ldg(a.walk_ent + (size_t)v * cap + e0 + 32 + lane);
-    }
+        x0 = (v < rows && e0 + (int)lane < eK) ? (int)__ldg(ent + (size_t)v * cap + e0 + lane) : -1;
+        x1 = (v < rows && e0 + 32 + (int)lane < eK) ? (int)__ldg(ent + (size_t)v * cap + e0 + 32 + lane) : -1;
+    };
+    int v = (int)gwarp;
+    int o = load_off(v);                          // this row's bounds
+    int x0, x1;
+    load_ents(v, o, x0, x1);                      // this row's entries
+    int o_n = load_off(v + (int)nwarps);          // the next row's bounds
     for (; v < rows; v += (int)nwarps) {
         const int vn = v + (int)nwarps;
-        const int o_n = (vn < rows && lane <= (unsigned)K) ? (int)__ldg(off_b + (size_t)vn * off_stride + lane) : 0;
+        // issue the next row's entries and the bounds of the row after it
+        int xn0, xn1;
+        load_ents(vn, o_n, xn0, xn1);
+        const int o_nn = load_off(vn + (int)nwarps);
         const int e0 = __shfl_sync(0xffffffffu, o, 0);
         const int e1 = __shfl_sync(0xffffffffu, o, 1);
         const int e2 = __shfl_sync(0xffffffffu, o, K >= 2 ? 2 : 1);
         const int e3 = __shfl_sync(0xffffffffu, o, K >= 3 ? 3 : 1);
         const int eK = __shfl_sync(0xffffffffu, o, K);
-        // the row: padding, and the diagonal in the chunk of its lane
-        uint4 init = pad;
+        auto level_of = [&](const int i) { return i < e1 ? 1 : (i < e2 ? 2 : (i < e3 ? 3 : 4)); };
+        if (x0 >= 0) atomicOr(Ab + (level_of(e0 + (int)lane) - 1) * 128 + (x0 >> 5), 1u << (x0 & 31));
+        if (x1 >= 0) atomicOr(Ab + (level_of(e0 + 32 + (int)lane) - 1) * 128 + (x1 >> 5), 1u << (x1 & 31));
+        for (int base = e0 + 64; base < eK; base += 32) {   // rows with more than 64 entries here
+            const int i = base + (int)lane;
+            if (i < eK) {
+                const int x = (int)__ldg(ent + (size_t)v * cap + i);
+                atomicOr(Ab + (level_of(i) - 1) * 128 + (x >> 5), 1u << (x & 31));
+            }
+        }
+        __syncwarp();
+        // this lane's chunk: the diagonal, then the levels
+        uint4 vv = pad;
         {
             const int g = a.inv ? __ldg(a.inv + v) : v - a.src_first;
             const int j = g - first;
             if (g >= 0 && (unsigned)j < (unsigned)ns && (unsigned)(j >> 7) == lane) {
                 const unsigned bit = 1u << (j & 31), comp = ((unsigned)j >> 5) & 3u;
-                if (comp == 0u) init.x |= bit; else if (comp == 1u) init.y |= bit;
-                else if (comp == 2u) init.z |= bit; else init.w |= bit;
+                if (comp == 0u) vv.x |= bit; else if (comp == 1u) vv.y |= bit;
+                else if (comp == 2u) vv.z |= bit; else vv.w |= bit;
             }
         }
-        Vb4[lane] = init;
-        Fb4[lane] = u4zero();
-        __syncwarp();
-        auto level_of = [&](const int i) { return i < e1 ? 1 : (i < e2 ? 2 : (i < e3 ? 3 : 4)); };
-        auto put = [&](const int j, const int L) {
-            const uint32_t bit = 1u << (j & 31);
-            const uint32_t old = atomicOr(Vb + (j >> 5), bit);
-            if (!(old & bit)) {
-                cnt[L - 1] += 1u;
-                if (L == K) atomicOr(Fb + (j >> 5), bit);
-            }
-        };
-        const int La = x0 >= 0 ? level_of(e0 + (int)lane) : 0;
-        const int Lb = x1 >= 0 ? level_of(e0 + 32 + (int)lane) : 0;
-        for (int L = 1; L <= K; ++L) {
-            if (La == L) put(x0, L);
-            if (Lb == L) put(x1, L);
-            __syncwarp();
+        uint4 prev = vv;
+        unsigned pc = u4popc(vv);
+        for (int L = 0; L < K; ++L) {
+            const uint4 al = Ab4[L * 32 + lane];
+            Ab4[L * 32 + lane] = u4zero();          // clean for the next row
+            prev = vv;
+            vv = u4or(vv, al);
+            const unsigned pn = u4popc(vv);
+            cnt[L] += pn - pc;
+            pc = pn;
         }
-        for (int base = e0 + 64; base < eK; base += 32) {   // rows with more than 64 entries here
-            const int i = base + (int)lane;
-            const int x = i < eK ? (int)__ldg(a.walk_ent + (size_t)v * cap + i) : -1;
-            const int Li = x >= 0 ? level_of(i) : 0;
-            for (int L = 1; L <= K; ++L) {
-                if (Li == L) put(x, L);
-                __syncwarp();
-            }
-        }
-        // the next row's entries (its bounds arrived while this row was built)
-        const int en0 = __shfl_sync(0xffffffffu, o_n, 0), enK = __shfl_sync(0xffffffffu, o_n, K);
-        x0 = (vn < rows && en0 + (int)lane < enK) ? (int)__ldg(a.walk_ent + (size_t)vn * cap + en0 + lane) : -1;
-        x1 = (vn < rows && en0 + 32 + (int)lane < enK) ? (int)__ldg(a.walk_ent + (size_t)vn * cap + en0 + 32 + lane)
-                                                        : -1;
-        // write the row and its flag word
-        const uint4 vv = Vb4[lane], ff = Fb4[lane];
+        const uint4 ff = andnot(vv, prev);
         a.V[(size_t)v * 32 + lane] = vv;
         F[(size_t)v * 32 + lane] = ff;
         const unsigned m = __ballot_sync(0xffffffffu, u4any(ff));
         if (lane == 0) fl[v] = m;
         __syncwarp();
         o = o_n;
+        o_n = o_nn;
+        x0 = xn0;
+        x1 = xn1;
     }
 #pragma unroll
     for (int L = 0; L < 4; ++L) {
@@ -1084,10 +1093,10 @@ static __device__ __noinline__ unsigned walk_batch(const BfsArgs &a, const int b
     }
     __syncthreads();
     if (a.nC == 32) {
-        uint4 *Vb4 = reinterpret_cast<uint4 *>(reinterpret_cast<unsigned char *>(s_adj) + a.walk_smem_off +
+        uint4 *Ab4 = reinterpret_cast<uint4 *>(reinterpret_cast<unsigned char *>(s_adj) + a.walk_smem_off +
                                                (size_t)(threadIdx.x >> 5) * walk_smem_per_warp(32));
         walk_rows32(a, b, a.src_begin + b * 128 * a.nC, ns, ((K + 1) & 1) ? a.F0 : a.F1,
-                    ((K + 1) & 1) ? a.fl0 : a.fl1, Vb4, Vb4 + 32, gtid >> 5, nthr >> 5, s_wcnt);
+                    ((K + 1) & 1) ? a.fl0 : a.fl1, Ab4, gtid >> 5, nthr >> 5, s_wcnt);
     } else {
         walk_rows(w, reinterpret_cast<unsigned char *>(s_adj) + a.walk_smem_off, gtid >> 5, nthr >> 5, s_wcnt);
     }

@@ -113,6 +113,7 @@ struct gg_engine {
     int bps_cap = 0;                     // resident blocks per SM (0: as many as fit)
     int walk_pref = -1;                  // walk depth: -1 automatic, 0 off, K > 0 forced
     int walk_K = 0;                      // levels computed by the walk pass (0: off)
+    int walk_vpull = 1;                  // levels after the walk pull visited sets (GG_VPULL=0: frontiers)
     int walk_rpg = 1;                    // rows per walk group
     unsigned walk_smem_off = 0;          // byte offset of the walk buffers in dynamic smem
     int32_t *d_h2 = nullptr;             // [rows][d*d] level-2 walk ends (walk_K >= 3)
@@ -142,6 +143,7 @@ struct gg_engine {
     uint4 *d_P0 = nullptr, *d_P1 = nullptr;     // push-level frontier, all zero between launches
     uint32_t *d_pf0 = nullptr, *d_pf1 = nullptr;
     uint32_t *d_nf = nullptr;            // not-full bit per visited chunk
+    uint32_t *d_nf2 = nullptr;           // its second copy (visited-set pull levels alternate)
     bool p_dirty = true;                 // push buffers must be zeroed before the next launch
     unsigned long long *d_counts = nullptr;
     unsigned *d_masks = nullptr;
@@ -175,7 +177,8 @@ void free_batch_buffers(gg_engine *e) {
     cudaFree(e->d_fl0); cudaFree(e->d_fl1);
     cudaFree(e->d_P0); cudaFree(e->d_P1); cudaFree(e->d_pf0); cudaFree(e->d_pf1);
     cudaFree(e->d_nf);
-    e->d_nf = nullptr;
+    cudaFree(e->d_nf2);
+    e->d_nf = e->d_nf2 = nullptr;
     e->d_V = e->d_F0 = e->d_F1 = nullptr;
     e->d_fl0 = e->d_fl1 = nullptr;
     e->d_P0 = e->d_P1 = nullptr;
@@ -354,6 +357,7 @@ gg_status plan(gg_engine *e, int want_bits) {
         GG_CK(cudaMalloc(&e->d_pf0, fwords * 4));
         GG_CK(cudaMalloc(&e->d_pf1, fwords * 4));
         GG_CK(cudaMalloc(&e->d_nf, fwords * 4));
+        GG_CK(cudaMalloc(&e->d_nf2, fwords * 4));
         e->p_dirty = true;
     }
     // Walk pass: levels 1..K of each batch from the walk ends of every row.
@@ -500,6 +504,7 @@ gg_status create_common(gg_engine *e) {
     e->dense_r_ppm = env_int("GG_DENSE_R_PPM", e->dense_r_ppm);
     e->full_skip_ppm = env_int("GG_FULL_SKIP_PPM", e->full_skip_ppm);
     e->split_ppm = env_int("GG_SPLIT_PPM", e->split_ppm);
+    e->walk_vpull = env_int("GG_VPULL", e->walk_vpull) != 0;
     e->push_ppm = env_int("GG_PUSH_PPM", e->push_ppm);
     e->push_min_items = env_int("GG_PUSH_MIN_ITEMS", e->push_min_items);
     e->use_graph = env_int("GG_NO_GRAPH", 0) == 0;
@@ -652,6 +657,7 @@ gg_status run_eval(gg_engine *e, const int32_t *d_table_in, const gg_eval_opts *
         // Below ~1M chunks a pull level costs about one grid barrier anyway.
         a.push_ppm = (long long)e->items >= (long long)e->push_min_items ? e->push_ppm : 0;
         a.nf = e->d_nf;
+        a.nf2 = e->d_nf2;
         a.asym = e->d_asym;
         a.counts = e->d_counts;
         a.masks = wvc ? e->d_masks : nullptr;
@@ -678,6 +684,7 @@ gg_status run_eval(gg_engine *e, const int32_t *d_table_in, const gg_eval_opts *
         a.walk_off = e->d_woff;
         a.walk_cap = e->walk_cap;
         a.walk_off_stride = e->walk_off_stride;
+        a.walk_vpull = walk_K > 0 && !wvc ? e->walk_vpull : 0;
         void *args[] = {&a};
         GG_CK(cudaLaunchCooperativeKernel(kernel_for(e->d, a.planes != nullptr), dim3(e->grid), dim3(gg::kBlock), args,
                                           e->smem_bytes, q));

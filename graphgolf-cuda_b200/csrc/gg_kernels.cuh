@@ -109,6 +109,9 @@ struct BfsArgs {
     // full.  Written by levels that load every visited chunk; a later level in
     // the skip-full stage passes over tiles whose word is 0.  nullptr: unused.
     uint32_t *nf;
+    // The second not-full array of the visited-set pull (levels alternate between
+    // nf and nf2, so that a level reads its neighbours' words of the level before).
+    uint32_t *nf2;
     // Distance bit-planes (nullptr: not written).  Plane k holds bit k of the
     // distance of every (vertex, source) pair: planes[k * plane_stride + v *
     // plane_cols + s / 128] bit s % 128, for the sources of the whole evaluation
@@ -128,6 +131,10 @@ struct BfsArgs {
     unsigned walk_smem_off;
     const uint16_t *walk_ent, *walk_off;
     int walk_cap, walk_off_stride;
+    // Nonzero (with a walk pass): the levels after the walk pull visited sets from
+    // two alternating copies (V and F0) instead of frontiers (see vpull_level), and
+    // the walk writes no frontier rows.
+    int walk_vpull;
 };
 
 // Where a level's new pairs go in the distance planes.
@@ -362,6 +369,182 @@ __device__ __forceinline__ void level_tiles(const BfsArgs &a, const int d, const
             if (lane == 0 && (tile0 + u) < t_hi) a.nf[tile0 + u] = nfb;
         }
     }
+}
+
+// Whether the levels after a walk pass pull visited sets (both not-full arrays given).
+__device__ __forceinline__ bool vpull_on(const BfsArgs &a) {
+    return a.walk_K > 0 && a.walk_vpull != 0 && a.nf != nullptr && a.nf2 != nullptr;
+}
+
+// Visited-set pull (levels after a walk pass).  With V_L[v] the sources within
+// distance L of v (chunk by chunk),
+//     V_L[v] = V_{L-1}[v] | OR of V_{L-1}[u] over the neighbours u of v
+// whose chunk changed at level L-1 (every neighbour, when dense): each V_{L-1}[u]
+// lies within V_L[v], and a source first reached at level L reaches v through a
+// neighbour that holds it at exactly L - 1, whose chunk therefore changed.  So a
+// level needs no frontier rows, only their flag words: X holds V_{L-1}, Y holds
+// V_{L-2} and is brought to V_L by writing the chunks that changed at level L-1 or
+// L (all chunks while Y holds no level yet: `wr_all`).  A dense level moves 10 row
+// transfers per chunk (own, d = 8 gathers, one write) against 11 with frontiers
+// (own, gathers, the visited and the frontier writes).  The new pairs are
+// V_L & ~V_{L-1}, as in level_tiles; fn gets their flag words, nfn the not-full
+// words of V_L.
+//
+// LAZY (the skip-full stage, nfc = the not-full words of V_{L-1}): a chunk whose
+// not-full bit is clear is full whatever X holds there, so full chunks are never
+// read or written again -- its own chunk is passed over, and a neighbour chunk that
+// is full makes the sum full without a load.  The buffers then hold V_L exactly on
+// the chunks that are not full, which is all that later levels read.
+template <int D, int U, bool LAZY>
+__device__ __forceinline__ void vpull_tiles(const BfsArgs &a, const int d, const int32_t *adj,
+                                            const unsigned v_base, const unsigned tile0, const unsigned t_hi,
+                                            const uint4 *X, uint4 *Y, const uint32_t *fc, uint32_t *fn,
+                                            const uint32_t *nfc, uint32_t *nfn, const unsigned nfo,
+                                            const bool dense, const bool wr_all, const bool skip_full,
+                                            const bool split, const unsigned lane, unsigned &cnt) {
+    unsigned t[U], c[U], chg[U];
+    bool ok[U];
+    uint4 own[U], acc[U];
+    const int32_t *arow[U];
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+        t[u] = (tile0 + u) * 32u + lane;
+        ok[u] = (tile0 + u) < t_hi && t[u] < a.items;
+        if (LAZY) ok[u] = ok[u] && ((nfo >> lane) & 1u);   // not full at L-1
+        const unsigned v = ok[u] ? a.div_nc.div(t[u]) : v_base;
+        c[u] = t[u] - v * (unsigned)a.nC;
+        arow[u] = adj + (size_t)(v - v_base) * (size_t)d;
+        own[u] = ok[u] ? __ldcg(X + t[u]) : u4zero();
+        acc[u] = u4zero();
+        chg[u] = (!wr_all && (tile0 + u) < t_hi) ? __ldcg(fc + tile0 + u) : 0u;
+    }
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+        if (!ok[u] || (skip_full && u4full(own[u]))) continue;
+        if constexpr (D > 0) {
+            unsigned tu[D];
+#pragma unroll
+            for (int i = 0; i < D; ++i) tu[i] = (unsigned)arow[u][i] * (unsigned)a.nC + c[u];
+            if constexpr (LAZY) {
+                // neighbours' not-full words first: a full neighbour fills the sum
+                unsigned nw[D], fw[D];
+                bool nb_full = false;
+#pragma unroll
+                for (int i = 0; i < D; ++i) {
+                    nw[i] = __ldcg(nfc + (tu[i] >> 5));
+                    fw[i] = dense ? ~0u : __ldcg(fc + (tu[i] >> 5));
+                }
+#pragma unroll
+                for (int i = 0; i < D; ++i) nb_full |= !((nw[i] >> (tu[i] & 31u)) & 1u);
+                if (nb_full) {
+                    acc[u] = make_uint4(~0u, ~0u, ~0u, ~0u);
+                } else {
+#pragma unroll
+                    for (int i = 0; i < D; ++i)
+                        if ((fw[i] >> (tu[i] & 31u)) & 1u) or_into(acc[u], __ldcg(X + tu[i]));
+                }
+            } else if (dense && split && D >= 8) {
+                constexpr int H = D / 2;
+                uint4 x[H];
+#pragma unroll
+                for (int i = 0; i < H; ++i) x[i] = __ldcg(X + tu[i]);
+#pragma unroll
+                for (int i = 0; i < H; ++i) or_into(acc[u], x[i]);
+                if (!u4full(u4or(own[u], acc[u]))) {
+#pragma unroll
+                    for (int i = 0; i < D - H; ++i) x[i] = __ldcg(X + tu[H + i]);
+#pragma unroll
+                    for (int i = 0; i < D - H; ++i) or_into(acc[u], x[i]);
+                }
+            } else if (dense) {
+                uint4 x[D];
+#pragma unroll
+                for (int i = 0; i < D; ++i) x[i] = __ldcg(X + tu[i]);
+#pragma unroll
+                for (int i = 0; i < D; ++i) or_into(acc[u], x[i]);
+            } else {
+                unsigned fw[D];
+#pragma unroll
+                for (int i = 0; i < D; ++i) fw[i] = __ldcg(fc + (tu[i] >> 5));
+#pragma unroll
+                for (int i = 0; i < D; ++i)
+                    if ((fw[i] >> (tu[i] & 31u)) & 1u) or_into(acc[u], __ldcg(X + tu[i]));
+            }
+        } else {
+            for (int i = 0; i < d; ++i) {
+                const unsigned tu = (unsigned)arow[u][i] * (unsigned)a.nC + c[u];
+                if (LAZY && !((__ldcg(nfc + (tu >> 5)) >> (tu & 31u)) & 1u)) {
+                    acc[u] = make_uint4(~0u, ~0u, ~0u, ~0u);
+                    break;
+                }
+                if (dense || ((__ldcg(fc + (tu >> 5)) >> (tu & 31u)) & 1u)) or_into(acc[u], __ldcg(X + tu));
+            }
+        }
+    }
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+        uint4 nw = u4zero();
+        bool not_full = false;
+        if (ok[u]) {
+            nw = andnot(acc[u], own[u]);
+            const uint4 vn = u4or(own[u], nw);
+            not_full = !u4full(vn);
+            const bool need = wr_all || u4any(nw) || ((chg[u] >> lane) & 1u);
+            if (need && (!LAZY || not_full)) Y[t[u]] = vn;
+            cnt += u4popc(nw);
+        }
+        const unsigned b = __ballot_sync(0xffffffffu, u4any(nw));
+        const unsigned nfb = __ballot_sync(0xffffffffu, not_full);
+        if (lane == 0 && (tile0 + u) < t_hi) {
+            fn[tile0 + u] = b;
+            nfn[tile0 + u] = nfb;
+        }
+    }
+}
+
+// One visited-set pull level over the block's tiles [s_next, t_hi) (s_next set by the
+// caller); returns this thread's count of new pairs.  nf_use (the skip-full stage,
+// with nfc written whole by the level before): a warp takes 32 tiles, passes over
+// those whose chunks are all full, and runs the others LAZY.
+template <int D>
+static __device__ __noinline__ unsigned vpull_level(const BfsArgs &a, const int d, const int32_t *adj,
+                                                    const unsigned v_base, const unsigned t_hi, const uint4 *X,
+                                                    uint4 *Y, const uint32_t *fc, uint32_t *fn, const uint32_t *nfc,
+                                                    uint32_t *nfn, const bool dense, const bool wr_all,
+                                                    const bool skip_full, const bool split, const bool nf_use,
+                                                    unsigned *s_next) {
+    const unsigned lane = threadIdx.x & 31u;
+    unsigned cnt = 0u;
+    if (nf_use) {
+        for (;;) {
+            unsigned tile0 = 0;
+            if (lane == 0) tile0 = atomicAdd(s_next, 32u);
+            tile0 = __shfl_sync(0xffffffffu, tile0, 0);
+            if (tile0 >= t_hi) break;
+            const unsigned my = tile0 + lane;
+            const unsigned w = my < t_hi ? __ldcg(nfc + my) : 0u;
+            if (my < t_hi && w == 0u) {
+                fn[my] = 0u;
+                nfn[my] = 0u;
+            }
+            for (unsigned todo = __ballot_sync(0xffffffffu, w != 0u); todo; todo &= todo - 1u) {
+                const int k = __ffs((int)todo) - 1;
+                const unsigned wk = __shfl_sync(0xffffffffu, w, k);
+                vpull_tiles<D, 1, true>(a, d, adj, v_base, tile0 + (unsigned)k, t_hi, X, Y, fc, fn, nfc, nfn, wk,
+                                        dense, false, skip_full, split, lane, cnt);
+            }
+        }
+    } else {
+        for (;;) {
+            unsigned tile0 = 0;
+            if (lane == 0) tile0 = atomicAdd(s_next, (unsigned)kGrab);
+            tile0 = __shfl_sync(0xffffffffu, tile0, 0);
+            if (tile0 >= t_hi) break;
+            vpull_tiles<D, kGrab, false>(a, d, adj, v_base, tile0, t_hi, X, Y, fc, fn, nfc, nfn, 0u, dense, wr_all,
+                                         skip_full, split, lane, cnt);
+        }
+    }
+    return cnt;
 }
 
 // Component k of a uint4 (k is a compile-time constant after unrolling).
@@ -878,7 +1061,7 @@ static __device__ __noinline__ void walk_rows(const WalkArgs &w, unsigned char *
             if (c < w.nC) {
                 const uint4 vv = Vb4[c], ff = Fb4[c];
                 w.V[t0 + c] = vv;
-                w.F[t0 + c] = ff;
+                if (w.F) w.F[t0 + c] = ff;
                 any = u4any(ff);
             }
             const unsigned m = __ballot_sync(0xffffffffu, any);
@@ -964,7 +1147,8 @@ struct LoopState {
 // row (A_L, non-returning atomics, one warp sync), then every lane builds, for its
 // own chunk, V_L = V_{L-1} | A_L from the diagonal up, counts popc(V_L) - popc(V_{L-1})
 // pairs at level L (exact: a source reached at several levels counts at the first),
-// and writes V = V_K, F = V_K & ~V_{K-1} and the frontier's flag word (one ballot).
+// and writes V = V_K, F = V_K & ~V_{K-1} (unless F is null) and the frontier's flag
+// word (one ballot).
 // Loads run two rows ahead: a row's bucket bounds two iterations before it is built,
 // its entries one iteration before.  Launch-constant arguments are read from the
 // kernel parameters (`a`, grid-constant), per-batch ones come in registers.
@@ -1043,7 +1227,7 @@ static __device__ __noinline__ void walk_rows32(const BfsArgs &a, const int b, c
         }
         const uint4 ff = andnot(vv, prev);
         a.V[(size_t)v * 32 + lane] = vv;
-        F[(size_t)v * 32 + lane] = ff;
+        if (F) F[(size_t)v * 32 + lane] = ff;
         const unsigned m = __ballot_sync(0xffffffffu, u4any(ff));
         if (lane == 0) fl[v] = m;
         __syncwarp();
@@ -1086,7 +1270,7 @@ static __device__ __noinline__ unsigned walk_batch(const BfsArgs &a, const int b
         w.inv = a.inv;
         w.src_first = a.src_first; w.first = a.src_begin + b * 128 * a.nC; w.ns = ns;
         w.V = a.V;
-        w.F = ((K + 1) & 1) ? a.F0 : a.F1;     // what level K + 1 reads
+        w.F = vpull_on(a) ? nullptr : (((K + 1) & 1) ? a.F0 : a.F1);   // what level K + 1 reads
         w.fl = ((K + 1) & 1) ? a.fl0 : a.fl1;
         w.rows = a.rows; w.nC = a.nC; w.K = K; w.items = items;
         w.rows_per_group = a.walk_rpg;
@@ -1095,7 +1279,7 @@ static __device__ __noinline__ unsigned walk_batch(const BfsArgs &a, const int b
     if (a.nC == 32) {
         uint4 *Ab4 = reinterpret_cast<uint4 *>(reinterpret_cast<unsigned char *>(s_adj) + a.walk_smem_off +
                                                (size_t)(threadIdx.x >> 5) * walk_smem_per_warp(32));
-        walk_rows32(a, b, a.src_begin + b * 128 * a.nC, ns, ((K + 1) & 1) ? a.F0 : a.F1,
+        walk_rows32(a, b, a.src_begin + b * 128 * a.nC, ns, vpull_on(a) ? nullptr : (((K + 1) & 1) ? a.F0 : a.F1),
                     ((K + 1) & 1) ? a.fl0 : a.fl1, Ab4, gtid >> 5, nthr >> 5, s_wcnt);
     } else {
         walk_rows(w, reinterpret_cast<unsigned char *>(s_adj) + a.walk_smem_off, gtid >> 5, nthr >> 5, s_wcnt);
@@ -1191,6 +1375,7 @@ __global__ void __launch_bounds__(kBlock, min_blocks_for(D)) bfs_batch_kernel(co
     }
 
     const bool walk = !PL && a.walk_K > 0;
+    const bool vp = walk && vpull_on(a);   // visited-set pull after the walk
     for (int b = 0; b < a.nb; ++b) {
         const int ns = min(128 * a.nC, a.ns_total - b * 128 * a.nC);
         if (a.batch_ns && gtid == 0) a.batch_ns[2 * b] = gtimer();
@@ -1258,7 +1443,8 @@ __global__ void __launch_bounds__(kBlock, min_blocks_for(D)) bfs_batch_kernel(co
             const unsigned long long c_prev = S.c_prev, pairs = S.pairs;
             const int in_p = S.in_p;
             const bool push = in_p >= 0 && c_prev * 1000000ull < pairs * (unsigned long long)a.push_ppm;
-            const bool dense = S.wrote_all_prev &&
+            // (visited-set pull levels always read complete rows: dense by the count alone)
+            const bool dense = (vp || S.wrote_all_prev) &&
                                c_prev * 1000000ull >= pairs * (unsigned long long)a.dense_r_ppm;
             const bool skip_full = S.reached * 1000000ull >= pairs * (unsigned long long)a.full_skip_ppm;
             const bool nf_use = !push && skip_full && S.nf_valid;
@@ -1274,6 +1460,14 @@ __global__ void __launch_bounds__(kBlock, min_blocks_for(D)) bfs_batch_kernel(co
                 uint32_t *pfn = in_p ? a.pf0 : a.pf1;
                 if constexpr (D > 0 && 32 % D == 0) cnt = push_level<D, PL>(a.adj, a.V, a.div_nc, (unsigned)a.nC, Pc, Pn, pfc, pfn, ntiles,
                                            gtid, nthr);
+            } else if (vp) {
+                // V_{L-1} alternates between V (level walk_K, written by the walk) and F0
+                const bool x_is_v = ((L - 1 - a.walk_K) & 1) == 0;
+                if (threadIdx.x == 0) s_next = t_lo;
+                __syncthreads();
+                cnt = vpull_level<D>(a, d, adj, v_base, t_hi, x_is_v ? a.V : a.F0, x_is_v ? a.F0 : a.V,
+                                     odd ? a.fl0 : a.fl1, odd ? a.fl1 : a.fl0, odd ? a.nf : a.nf2,
+                                     odd ? a.nf2 : a.nf, dense, L == a.walk_K + 1, skip_full, split, nf_use, &s_next);
             } else {
                 const uint4 *Fc = in_p >= 0 ? (in_p ? a.P1 : a.P0) : (odd ? a.F0 : a.F1);
                 const uint32_t *fc = in_p >= 0 ? (in_p ? a.pf1 : a.pf0) : (odd ? a.fl0 : a.fl1);
@@ -1343,7 +1537,7 @@ __global__ void __launch_bounds__(kBlock, min_blocks_for(D)) bfs_batch_kernel(co
                 S.reached += cL;
                 S.c_prev = cL;
                 S.wrote_all_prev = !push && write_all;
-                S.nf_valid = a.nf != nullptr && !push && (skip_full || dense || masks != nullptr);
+                S.nf_valid = a.nf != nullptr && !push && (vp || skip_full || dense || masks != nullptr);
                 if (push) {
                     S.in_p = in_p ^ 1;    // the frontier is now in Pn; Pc was cleared by its readers
                 } else if (in_p >= 0) {

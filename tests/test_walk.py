@@ -6,7 +6,9 @@ forms (consecutive representatives and the corner tiles found through the invers
 list), batches that end inside the walk, and level caps below K.
 
 GG_WALK_LEVELS is read when an engine plans its batches (at creation and at
-set_batch_sources): 0 turns the pass off, K > 0 forces K levels."""
+set_batch_sources): 0 turns the pass off, K > 0 forces K levels.  GG_VPULL (read at
+creation) chooses how the levels after the walk run: 1 (default) pulls visited sets
+from two alternating copies, 0 pulls frontiers."""
 import os
 
 import numpy as np
@@ -107,3 +109,36 @@ def test_walk_lifted_forms(walk):
     dims, rows = dims_rows[:6], dims_rows[6]
     want = engine_with(0, lambda: G.cudaASPLbox(*dims, 6, 0)).diameterASPL(rows)
     assert engine_with(walk, lambda: G.cudaASPLbox(*dims, 6, 0)).diameterASPL(rows) == want
+
+
+def circulant(n, steps):
+    v = np.arange(n, dtype=np.int64)[:, None]
+    s = np.asarray([x for k in steps for x in (k, -k)], np.int64)[None, :]
+    return ((v + s) % n).astype(np.int32)
+
+
+@pytest.mark.parametrize("n,steps,bits,walk", [(6000, (1, 7), 1024, 3), (5000, (1, 13, 97, 541), 2048, 2),
+                                               (4100, (1, 3, 9), 512, 4), (9000, (1, 2), 4096, 1)])
+def test_visited_pull_matches_frontier_pull(n, steps, bits, walk):
+    """Long-diameter circulants: after the walk come sparse (flag-driven), dense,
+    split and skip-full levels; the visited-set pull must count exactly what the
+    frontier pull and the oracle count."""
+    adj = circulant(n, steps)
+    d = adj.shape[1]
+    got = {}
+    for vp in (0, 1):
+        old = os.environ.get("GG_VPULL")
+        os.environ["GG_VPULL"] = str(vp)
+        try:
+            e = engine_with(walk, lambda: G.cudaASPLgraph(n, d, 0))
+            engine_with(walk, lambda: e.set_batch_sources(bits))
+            got[vp] = counts(e, adj, n + 1)
+        finally:
+            if old is None:
+                del os.environ["GG_VPULL"]
+            else:
+                os.environ["GG_VPULL"] = old
+    assert got[1] == got[0]
+    o = O.bfs_pull(adj, np.arange(n))
+    assert got[1][0] == o.total() and got[1][2] == o.levels
+    assert np.array_equal(np.asarray(got[1][5][:o.levels + 1]), o.level_counts[:o.levels + 1])

@@ -114,6 +114,7 @@ struct gg_engine {
     int walk_pref = -1;                  // walk depth: -1 automatic, 0 off, K > 0 forced
     int walk_K = 0;                      // levels computed by the walk pass (0: off)
     int walk_vpull = 1;                  // levels after the walk pull visited sets (GG_VPULL=0: frontiers)
+    int walk_own_skip = 1;               // dense ones skip own chunks on tables without one-way entries (GG_OWN_SKIP)
     int walk_rpg = 1;                    // rows per walk group
     unsigned walk_smem_off = 0;          // byte offset of the walk buffers in dynamic smem
     int32_t *d_h2 = nullptr;             // [rows][d*d] level-2 walk ends (walk_K >= 3)
@@ -144,6 +145,8 @@ struct gg_engine {
     uint32_t *d_pf0 = nullptr, *d_pf1 = nullptr;
     uint32_t *d_nf = nullptr;            // not-full bit per visited chunk
     uint32_t *d_nf2 = nullptr;           // its second copy (visited-set pull levels alternate)
+    int *d_wasym = nullptr;              // one-way flag of the table (walk_index_kernel)
+    unsigned long long *d_vtot = nullptr;   // 3 level totals (dense visited-set pull without own chunks)
     bool p_dirty = true;                 // push buffers must be zeroed before the next launch
     unsigned long long *d_counts = nullptr;
     unsigned *d_masks = nullptr;
@@ -190,7 +193,8 @@ void free_counters(gg_engine *e) {
     cudaFreeHost(e->h_status); cudaFreeHost(e->h_masks);
     cudaFreeHost(e->h_level_ns);
     e->d_status = e->h_status = nullptr;
-    e->d_bad = e->d_asym = e->h_bad = nullptr;
+    e->d_bad = e->d_asym = e->d_wasym = e->h_bad = nullptr;
+    e->d_vtot = nullptr;
     e->d_levels_run = e->h_levels_run = nullptr;
     e->d_batch_ns = e->h_batch_ns = nullptr;
     e->d_counts = nullptr; e->d_masks = nullptr; e->d_ctl = nullptr; e->d_level_ns = nullptr;
@@ -380,7 +384,9 @@ gg_status plan(gg_engine *e, int want_bits) {
             e->h2_elems = h2_need;
         }
     }
-    e->walk_cap = e->walk_K ? (int)walk_cap_for(e->d, e->walk_K) : 0;
+    // row stride of the index: the walk ends, rounded up to a multiple of 8 (rows start
+    // 16-byte aligned: the index kernel writes them 16 bytes at a time)
+    e->walk_cap = e->walk_K ? (int)((walk_cap_for(e->d, e->walk_K) + 7) & ~7ll) : 0;
     e->walk_off_stride = e->walk_K ? (int)(((long long)e->reps.size() + bits - 1) / bits) * e->walk_K + 1 : 0;
     const size_t went_need = (size_t)e->rows * e->walk_cap, woff_need = (size_t)e->rows * e->walk_off_stride;
     if (went_need != e->went_elems || woff_need != e->woff_elems) {
@@ -448,6 +454,8 @@ gg_status ensure_counters(gg_engine *e, int cap, int nb) {
     e->d_bad = reinterpret_cast<int *>(e->d_status + sizeof(Ctl));
     e->h_bad = reinterpret_cast<int *>(e->h_status + sizeof(Ctl));
     e->d_asym = e->d_bad + 1;
+    e->d_wasym = e->d_bad + 2;
+    e->d_vtot = reinterpret_cast<unsigned long long *>(e->d_status + sizeof(Ctl) + 64);
     e->d_levels_run = reinterpret_cast<int *>(e->d_status + e->off_levels_run);
     e->h_levels_run = reinterpret_cast<int *>(e->h_status + e->off_levels_run);
     e->d_batch_ns = reinterpret_cast<unsigned long long *>(e->d_status + e->off_batch_ns);
@@ -505,6 +513,7 @@ gg_status create_common(gg_engine *e) {
     e->full_skip_ppm = env_int("GG_FULL_SKIP_PPM", e->full_skip_ppm);
     e->split_ppm = env_int("GG_SPLIT_PPM", e->split_ppm);
     e->walk_vpull = env_int("GG_VPULL", e->walk_vpull) != 0;
+    e->walk_own_skip = env_int("GG_OWN_SKIP", e->walk_own_skip) != 0;
     e->push_ppm = env_int("GG_PUSH_PPM", e->push_ppm);
     e->push_min_items = env_int("GG_PUSH_MIN_ITEMS", e->push_min_items);
     e->use_graph = env_int("GG_NO_GRAPH", 0) == 0;
@@ -578,7 +587,7 @@ gg_status run_eval(gg_engine *e, const int32_t *d_table_in, const gg_eval_opts *
     auto enqueue = [&](cudaStream_t q, bool timed) -> gg_status {
         if (timed) GG_CK(cudaEventRecord(e->ev0, q));
         // control block, range-check and symmetry words
-        GG_CK(cudaMemsetAsync(e->d_status, 0, sizeof(Ctl) + 2 * sizeof(int), q));
+        GG_CK(cudaMemsetAsync(e->d_status, 0, sizeof(Ctl) + 3 * sizeof(int), q));   // ctl, bad, asym, wasym
         const long long n = (long long)e->rows * e->d;
         if (e->form == FORM_GRAPH) {
             if (d_table_in != e->d_table)
@@ -629,6 +638,7 @@ gg_status run_eval(gg_engine *e, const int32_t *d_table_in, const gg_eval_opts *
             wi.off = e->d_woff;
             wi.off_stride = e->walk_off_stride;
             wi.bad = e->form == FORM_GRAPH ? e->d_bad : nullptr;
+            wi.asym = e->walk_vpull && e->walk_own_skip ? e->d_wasym : nullptr;
             // one resident wave of blocks, each striding over the rows
             int sms = 0, per_sm = 0;
             GG_CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, e->device));
@@ -685,6 +695,8 @@ gg_status run_eval(gg_engine *e, const int32_t *d_table_in, const gg_eval_opts *
         a.walk_cap = e->walk_cap;
         a.walk_off_stride = e->walk_off_stride;
         a.walk_vpull = walk_K > 0 && !wvc ? e->walk_vpull : 0;
+        a.walk_asym = a.walk_vpull && e->walk_own_skip ? e->d_wasym : nullptr;
+        a.vtot = e->d_vtot;
         void *args[] = {&a};
         GG_CK(cudaLaunchCooperativeKernel(kernel_for(e->d, a.planes != nullptr), dim3(e->grid), dim3(gg::kBlock), args,
                                           e->smem_bytes, q));

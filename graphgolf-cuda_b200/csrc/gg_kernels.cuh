@@ -58,9 +58,13 @@ struct Ctl {
     int levels_run;           // last level executed (single-batch callers)
     int pad0[28];
     unsigned int passed;      // grid barriers completed so far
-    int pad1[31];
+    unsigned int pad_p;
+    // (epoch << 40) | value published by the last arrival of a grid_sync_value
+    unsigned long long result;
+    int pad1[28];
 };
-static_assert(offsetof(Ctl, passed) == 128 && sizeof(Ctl) == 256, "one 128-byte line each");
+static_assert(offsetof(Ctl, passed) == 128 && offsetof(Ctl, result) == 136 && sizeof(Ctl) == 256,
+              "arrivals and the published words on separate 128-byte lines");
 
 struct BfsArgs {
     const int32_t *adj;       // [rows][d] pull adjacency
@@ -135,6 +139,15 @@ struct BfsArgs {
     // two alternating copies (V and F0) instead of frontiers (see vpull_level), and
     // the walk writes no frontier rows.
     int walk_vpull;
+    // One-way flag of the table from walk_index_kernel (0: every row's entries list
+    // it back), or nullptr.  With 0, dense visited-set pull levels skip their own
+    // chunks: for L >= 2, V_{L-1}[v] lies within the union of the neighbours'
+    // V_{L-1}[u] (the source v through any neighbour, every other source through the
+    // neighbour on a shortest path).  Such a level adds its rows' popcounts into
+    // vtot[L % 3] (3 slots: zeroed two levels ahead), and its count is that total
+    // less the padding bits and the pairs reached before it.
+    const int *walk_asym;
+    unsigned long long *vtot;
 };
 
 // Where a level's new pairs go in the distance planes.
@@ -174,6 +187,22 @@ __device__ __forceinline__ unsigned long long ld_relaxed_u64(const unsigned long
     return v;
 }
 
+__device__ __forceinline__ unsigned atom_add_acq_rel(unsigned *p, unsigned v) {
+    unsigned old;
+    asm volatile("atom.add.acq_rel.gpu.global.u32 %0, [%1], %2;" : "=r"(old) : "l"(p), "r"(v) : "memory");
+    return old;
+}
+__device__ __forceinline__ void st_release(unsigned *p, unsigned v) {
+    asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+__device__ __forceinline__ void st_release_u64(unsigned long long *p, unsigned long long v) {
+    asm volatile("st.release.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+}
+__device__ __forceinline__ unsigned long long ld_acquire_u64(const unsigned long long *p) {
+    unsigned long long v;
+    asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+    return v;
+}
 __device__ __forceinline__ unsigned ld_relaxed(const unsigned *p) {
     unsigned v;
     asm volatile("ld.relaxed.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
@@ -185,7 +214,8 @@ __device__ __forceinline__ unsigned ld_relaxed(const unsigned *p) {
 // the launch (the same number in every block).  Each block adds 1 to `arrive`;
 // the block whose add makes it (epoch + 1) * expected is the last one and
 // publishes `passed` = epoch + 1; every block waits until it reads that value.
-// One atomic per block, and the waiting loads go to a line no arrival touches.
+// One acquire-release atomic per block (no separate fences), and the waiting
+// acquire loads go to a line no arrival touches.
 // `expected` above gridDim.x makes the wait run out (fault-injection tests).
 // Returns false on every block once any block's wait ran past `wait_ns`; the
 // kernel then returns and the host reports GG_TIMEOUT.
@@ -196,15 +226,14 @@ __device__ __forceinline__ bool grid_sync(Ctl *ctl, unsigned expected, long long
     const unsigned next = epoch + 1u;
     if (threadIdx.x == 0) {
         int ok = 1;
-        __threadfence();
-        const unsigned old = atomicAdd(&ctl->arrive, 1u);
-        if (old + 1u == next * expected) {
-            __threadfence();
-            atomicExch(&ctl->passed, next);
-        }
+        // release: the block's writes (ordered before this thread by the block
+        // barrier) are published with the arrival; acquire: the last arrival sees
+        // every other block's, and publishes them with its release store
+        const unsigned old = atom_add_acq_rel(&ctl->arrive, 1u);
+        if (old + 1u == next * expected) st_release(&ctl->passed, next);
         const unsigned long long t0 = gtimer();
         for (unsigned it = 1;; ++it) {
-            if (ld_relaxed(&ctl->passed) == next) break;
+            if (ld_acquire(&ctl->passed) == next) break;
             if ((it & 255u) == 0u) {
                 if (ld_acquire_i(&ctl->err)) { ok = 0; break; }
                 if ((long long)(gtimer() - t0) > wait_ns) {
@@ -214,12 +243,55 @@ __device__ __forceinline__ bool grid_sync(Ctl *ctl, unsigned expected, long long
                 }
             }
         }
-        __threadfence();
         s_ok = ok;
     }
     epoch = next;
     __syncthreads();
     return s_ok != 0;
+}
+
+// grid_sync that also hands every block one 64-bit value (< 2^40) read after all
+// arrivals: the last arrival reads *src (every block's additions into it come
+// before their arrivals) and publishes (epoch << 40) | value with a release store
+// on the line the waiters poll, so the value costs no round trip after the
+// barrier.  The value is valid in thread 0 only.  `passed` is kept up to date for
+// the plain grid_sync.
+__device__ __forceinline__ bool grid_sync_value(Ctl *ctl, unsigned expected, long long wait_ns, int level,
+                                                unsigned &epoch, const unsigned long long *src,
+                                                unsigned long long &value) {
+    __shared__ int s_ok2;
+    __syncthreads();
+    const unsigned next = epoch + 1u;
+    if (threadIdx.x == 0) {
+        int ok = 1;
+        const unsigned long long tag = (unsigned long long)(next & 0xffffffu) << 40;
+        const unsigned old = atom_add_acq_rel(&ctl->arrive, 1u);
+        if (old + 1u == next * expected) {
+            const unsigned long long v = ld_relaxed_u64(src) & ((1ull << 40) - 1ull);
+            st_release_u64(&ctl->result, tag | v);
+            st_release(&ctl->passed, next);
+        }
+        const unsigned long long t0 = gtimer();
+        for (unsigned it = 1;; ++it) {
+            const unsigned long long w = ld_acquire_u64(&ctl->result);
+            if ((w & ~((1ull << 40) - 1ull)) == tag) {
+                value = w & ((1ull << 40) - 1ull);
+                break;
+            }
+            if ((it & 255u) == 0u) {
+                if (ld_acquire_i(&ctl->err)) { ok = 0; break; }
+                if ((long long)(gtimer() - t0) > wait_ns) {
+                    if (atomicCAS(&ctl->err, 0, 1) == 0) ctl->err_level = level;
+                    ok = 0;
+                    break;
+                }
+            }
+        }
+        s_ok2 = ok;
+    }
+    epoch = next;
+    __syncthreads();
+    return s_ok2 != 0;
 }
 
 __device__ __forceinline__ uint4 u4zero() { return make_uint4(0u, 0u, 0u, 0u); }
@@ -401,7 +473,8 @@ __device__ __forceinline__ void vpull_tiles(const BfsArgs &a, const int d, const
                                             const uint4 *X, uint4 *Y, const uint32_t *fc, uint32_t *fn,
                                             const uint32_t *nfc, uint32_t *nfn, const unsigned nfo,
                                             const bool dense, const bool wr_all, const bool skip_full,
-                                            const bool split, const unsigned lane, unsigned &cnt) {
+                                            const bool split, const bool no_own, const unsigned lane,
+                                            unsigned &cnt) {
     unsigned t[U], c[U], chg[U];
     bool ok[U];
     uint4 own[U], acc[U];
@@ -414,7 +487,7 @@ __device__ __forceinline__ void vpull_tiles(const BfsArgs &a, const int d, const
         const unsigned v = ok[u] ? a.div_nc.div(t[u]) : v_base;
         c[u] = t[u] - v * (unsigned)a.nC;
         arow[u] = adj + (size_t)(v - v_base) * (size_t)d;
-        own[u] = ok[u] ? __ldcg(X + t[u]) : u4zero();
+        own[u] = ok[u] && !(!LAZY && no_own) ? __ldcg(X + t[u]) : u4zero();
         acc[u] = u4zero();
         chg[u] = (!wr_all && (tile0 + u) < t_hi) ? __ldcg(fc + tile0 + u) : 0u;
     }
@@ -503,7 +576,8 @@ __device__ __forceinline__ void vpull_tiles(const BfsArgs &a, const int d, const
 }
 
 // One visited-set pull level over the block's tiles [s_next, t_hi) (s_next set by the
-// caller); returns this thread's count of new pairs.  nf_use (the skip-full stage,
+// caller); returns this thread's count of new pairs (no_own: of the pairs in the
+// rows it wrote, padding included; every chunk is then written).  nf_use (the skip-full stage,
 // with nfc written whole by the level before): a warp takes 32 tiles, passes over
 // those whose chunks are all full, and runs the others LAZY.
 template <int D>
@@ -512,7 +586,7 @@ static __device__ __noinline__ unsigned vpull_level(const BfsArgs &a, const int 
                                                     uint4 *Y, const uint32_t *fc, uint32_t *fn, const uint32_t *nfc,
                                                     uint32_t *nfn, const bool dense, const bool wr_all,
                                                     const bool skip_full, const bool split, const bool nf_use,
-                                                    unsigned *s_next) {
+                                                    const bool no_own, unsigned *s_next) {
     const unsigned lane = threadIdx.x & 31u;
     unsigned cnt = 0u;
     if (nf_use) {
@@ -531,7 +605,7 @@ static __device__ __noinline__ unsigned vpull_level(const BfsArgs &a, const int 
                 const int k = __ffs((int)todo) - 1;
                 const unsigned wk = __shfl_sync(0xffffffffu, w, k);
                 vpull_tiles<D, 1, true>(a, d, adj, v_base, tile0 + (unsigned)k, t_hi, X, Y, fc, fn, nfc, nfn, wk,
-                                        dense, false, skip_full, split, lane, cnt);
+                                        dense, false, skip_full, split, false, lane, cnt);
             }
         }
     } else {
@@ -540,8 +614,8 @@ static __device__ __noinline__ unsigned vpull_level(const BfsArgs &a, const int 
             if (lane == 0) tile0 = atomicAdd(s_next, (unsigned)kGrab);
             tile0 = __shfl_sync(0xffffffffu, tile0, 0);
             if (tile0 >= t_hi) break;
-            vpull_tiles<D, kGrab, false>(a, d, adj, v_base, tile0, t_hi, X, Y, fc, fn, nfc, nfn, 0u, dense, wr_all,
-                                         skip_full, split, lane, cnt);
+            vpull_tiles<D, kGrab, false>(a, d, adj, v_base, tile0, t_hi, X, Y, fc, fn, nfc, nfn, 0u, dense,
+                                         wr_all || no_own, skip_full, split, no_own, lane, cnt);
         }
     }
     return cnt;
@@ -730,9 +804,32 @@ struct WalkIndexArgs {
     uint16_t *off;            // [rows][off_stride]: bucket starts, nb * K + 1 used
     int off_stride;
     const int *bad;           // nonzero: the table failed its range check
+    int *asym;                // set to 1 when some row u lacks v for an entry u of row v (nullptr: not checked)
 };
 
 constexpr int kIndexBlock = 256;
+
+// The row's entries from shared memory to the index, 16 bytes a lane (cap is a
+// multiple of 8, so rows start 16-byte aligned; the last word may carry stale
+// entries past `total`, which no reader looks at).
+__device__ __forceinline__ void copy_row_out(const WalkIndexArgs &a, const int v, const unsigned lane,
+                                             const uint16_t *row, const unsigned total) {
+    uint4 *dst = reinterpret_cast<uint4 *>(a.ent + (size_t)v * a.cap);
+    const uint4 *src = reinterpret_cast<const uint4 *>(row);
+    for (unsigned k = lane; k < (total + 7u) / 8u; k += 32) dst[k] = src[k];
+    __syncwarp();
+}
+
+// One-way check of row v: every entry u of the row must list v in its own row,
+// else *a.asym = 1 (the visited-set pull levels then read their own chunks).
+__device__ __forceinline__ void row_oneway_check(const WalkIndexArgs &a, const int v, const unsigned lane, const int d) {
+    for (int i = (int)lane; i < d; i += 32) {
+        const int32_t *ur = a.adj + (size_t)__ldg(a.adj + (size_t)v * d + i) * d;
+        bool f = false;
+        for (int j = 0; j < d; ++j) f |= __ldg(ur + j) == v;
+        if (!f) *a.asym = 1;
+    }
+}
 constexpr int kIndexMaxKeys = 256;   // nb * K buckets per row
 constexpr int kIndexMaxCap = 1024;   // entries per row
 
@@ -815,6 +912,17 @@ __device__ __forceinline__ void index_row_regs(const WalkIndexArgs &a, const int
         if (a.K >= 3 && i < U3)
             q3[s3] = __ldg(reinterpret_cast<const uint4 *>(a.h2 + (size_t)__ldg(arow + i / Q) * DD) + i % Q);
     }
+    if (a.asym) {
+        if (a.K >= 2) {
+            // the level-2 lists are the neighbours' rows, D / 4 lanes per row
+            bool f = (int)lane < Q && ((int)q2[0].x == v || (int)q2[0].y == v || (int)q2[0].z == v ||
+                                       (int)q2[0].w == v);
+            if constexpr (D / 4 == 2) f |= __shfl_xor_sync(0xffffffffu, f, 1) != 0;
+            if ((int)lane < Q && (int)lane % (D / 4) == 0 && !f) *a.asym = 1;
+        } else {
+            row_oneway_check(a, v, lane, D);
+        }
+    }
     int n = 0;
     pk[n++] = lane < (unsigned)D ? classify(x1, 1) : -1;
 #pragma unroll
@@ -861,15 +969,13 @@ __device__ __forceinline__ void index_row_regs(const WalkIndexArgs &a, const int
     for (int k = 0; k < NV; ++k)
         if (pk[k] >= 0) row[atomicAdd(cur + (pk[k] >> 16), 1u)] = (uint16_t)(pk[k] & 0xffff);
     __syncwarp();
-    uint16_t *dst = a.ent + (size_t)v * a.cap;
-    for (unsigned k = lane; k < total; k += 32) dst[k] = row[k];
-    __syncwarp();
+    copy_row_out(a, v, lane, row, total);
 }
 
 template <int D>
 __global__ void __launch_bounds__(kIndexBlock) walk_index_kernel(const WalkIndexArgs a) {
     __shared__ unsigned s_cur[kIndexBlock / 32][kIndexMaxKeys];
-    __shared__ uint16_t s_ent[kIndexBlock / 32][kIndexMaxCap];
+    __shared__ __align__(16) uint16_t s_ent[kIndexBlock / 32][kIndexMaxCap];
     if (a.bad && *a.bad) return;
     const unsigned lane = threadIdx.x & 31u, wib = threadIdx.x >> 5;
     unsigned *cur = s_cur[wib];
@@ -892,6 +998,7 @@ __global__ void __launch_bounds__(kIndexBlock) walk_index_kernel(const WalkIndex
                 continue;
             }
         }
+        if (a.asym) row_oneway_check(a, v, lane, D > 0 ? D : a.d);
         // pass 1: bucket sizes
         for_walk_ends<D>(a, v, lane, [&](const int32_t w, const int L) {
             const int j = src_of(w);
@@ -927,9 +1034,7 @@ __global__ void __launch_bounds__(kIndexBlock) walk_index_kernel(const WalkIndex
             }
         });
         __syncwarp();
-        uint16_t *dst = a.ent + (size_t)v * a.cap;
-        for (unsigned k = lane; k < total; k += 32) dst[k] = row[k];
-        __syncwarp();
+        copy_row_out(a, v, lane, row, total);
     }
 }
 
@@ -949,9 +1054,14 @@ struct WalkArgs {
 constexpr int kWalkMaxNC = 64;    // row width (uint4 chunks) the per-warp buffers hold
 
 // Shared-memory bytes of the walk buffers of one warp.
+constexpr int kWalkStageRows = 12;    // rows walk_rows32 stages at once
+constexpr int kWalkStageWords = 33;   // entry words staged per row (64 entries from an odd start)
 __host__ __device__ constexpr int walk_smem_per_warp(int nC) {
-    return nC == 32 ? 32 * 16 * 4 : nC * 16 * 2 + kWalkMaxNC * 4;   // walk_rows32: up to 4 level copies
+    // walk_rows32: 4 level copies of the row and the staged entry words
+    return nC == 32 ? 32 * 16 * 4 + kWalkStageRows * kWalkStageWords * 4 : nC * 16 * 2 + kWalkMaxNC * 4;
 }
+static_assert(walk_smem_per_warp(32) % 16 == 0, "per-warp walk buffers stay 16-byte aligned");
+static_assert(kWalkStageRows * 5 <= 64, "bounds of the staged rows fit two registers a lane");
 
 // A row's index entries of this batch: bucket bounds (lanes 0..K hold off[bK + lane])
 // and its first 64 entries (lanes hold entries e0 + lane and e0 + 32 + lane, or -1).
@@ -1139,105 +1249,125 @@ struct LoopState {
     int nf_valid;                // a.nf describes V as the previous level left it
     int done;                    // the batch's level loop ends
     int L_next;                  // first level the level loop runs (after a walk pass)
+    int sym;                     // the table has no one-way entries (walk_asym read 0)
 };
 
+// 4-byte asynchronous copy global -> shared (no registers held while in flight).
+__device__ __forceinline__ void cp_async4(void *smem_dst, const void *gmem_src) {
+    const unsigned d = (unsigned)__cvta_generic_to_shared(smem_dst);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(d), "l"(gmem_src) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+
 // walk_rows for rows of exactly 32 chunks (4096-source batches): a row is one tile
-// and one flag word, so lane c owns chunk c of the row.  Order-free form of the
-// level sets: each level's entries are ORed into their own shared-memory copy of the
-// row (A_L, non-returning atomics, one warp sync), then every lane builds, for its
-// own chunk, V_L = V_{L-1} | A_L from the diagonal up, counts popc(V_L) - popc(V_{L-1})
-// pairs at level L (exact: a source reached at several levels counts at the first),
-// and writes V = V_K, F = V_K & ~V_{K-1} (unless F is null) and the frontier's flag
-// word (one ballot).
-// Loads run two rows ahead: a row's bucket bounds two iterations before it is built,
-// its entries one iteration before.  Launch-constant arguments are read from the
-// kernel parameters (`a`, grid-constant), per-batch ones come in registers.
+// and one flag word, so lane c owns chunk c of the row.  A warp takes a contiguous
+// run of rows and works through it kWalkStageRows at a time in three steps:
+//  1. the bucket bounds of every staged row (one load round trip; lane l holds
+//     bound l % (K+1) of row l / (K+1), lanes 32.. in a second register);
+//  2. the words holding each row's first 64 entries of this batch, copied into
+//     shared memory with 4-byte cp.async (second round trip; no registers held);
+//  3. per row, from shared memory: each level's entries ORed into their own copy of
+//     the row (A_L, non-returning atomics), then every lane builds, for its chunk,
+//     V_L = V_{L-1} | A_L from the diagonal up, counts popc(V_L) - popc(V_{L-1})
+//     pairs at level L (a source reached at several levels counts at the first),
+//     and writes V = V_K, F = V_K & ~V_{K-1} (unless F is null) and the frontier's
+//     flag word (one ballot).  Entries past the first 64 of a row are read directly.
+
+template <int K>
 static __device__ __noinline__ void walk_rows32(const BfsArgs &a, const int b, const int first, const int ns,
-                                                uint4 *F, uint32_t *fl, uint4 *Ab4,
+                                                uint4 *F, uint32_t *fl, unsigned char *wsm,
                                                 const unsigned gwarp, const unsigned nwarps,
                                                 unsigned long long *s_cnt) {
     const unsigned lane = threadIdx.x & 31u;
-    uint32_t *Ab = reinterpret_cast<uint32_t *>(Ab4);   // K copies of the row: A_1 .. A_K
-    const int K = a.walk_K, rows = a.rows;
+    uint4 *Ab4 = reinterpret_cast<uint4 *>(wsm);              // A_1 .. A_K (4 copies reserved)
+    uint32_t *Ab = reinterpret_cast<uint32_t *>(wsm);
+    uint32_t *Es = reinterpret_cast<uint32_t *>(wsm + 4 * 512);   // [kWalkStageRows][kWalkStageWords]
+    const int rows = a.rows, off_stride = a.walk_off_stride, cap = a.walk_cap;
     const uint16_t *off_b = a.walk_off + b * K;
-    const int off_stride = a.walk_off_stride, cap = a.walk_cap;
     const uint16_t *ent = a.walk_ent;
+    const int32_t *inv = a.inv;
     const uint4 pad = pad_mask((int)lane, ns);
-    unsigned cnt[4] = {0u, 0u, 0u, 0u};
-    for (int L = 0; L < K; ++L) Ab4[L * 32 + lane] = u4zero();
+    unsigned cnt[K];
+#pragma unroll
+    for (int L = 0; L < K; ++L) {
+        cnt[L] = 0u;
+        Ab4[L * 32 + lane] = u4zero();
+    }
     __syncwarp();
-    auto load_off = [&](const int v) -> int {
-        return (v < rows && lane <= (unsigned)K) ? (int)__ldg(off_b + (size_t)v * off_stride + lane) : 0;
-    };
-    // entries of row v: lanes hold entries e0 + lane and e0 + 32 + lane (or -1), and
-    // their levels (1..K, 0 = none)
-    auto load_ents = [&](const int v, const int o, int &x0, int &x1) {
-        const int e0 = __shfl_sync(0xffffffffu, o, 0), eK = __shfl_sync(0xffffffffu, o, K);
-        x0 = (v < rows && e0 + (int)lane < eK) ? (int)__ldg(ent + (size_t)v * cap + e0 + lane) : -1;
-        x1 = (v < rows && e0 + 32 + (int)lane < eK) ? (int)__ldg(ent + (size_t)v * cap + e0 + 32 + lane) : -1;
-    };
-    int v = (int)gwarp;
-    int o = load_off(v);                          // this row's bounds
-    int x0, x1;
-    load_ents(v, o, x0, x1);                      // this row's entries
-    int o_n = load_off(v + (int)nwarps);          // the next row's bounds
-    for (; v < rows; v += (int)nwarps) {
-        const int vn = v + (int)nwarps;
-        // issue the next row's entries and the bounds of the row after it
-        int xn0, xn1;
-        load_ents(vn, o_n, xn0, xn1);
-        const int o_nn = load_off(vn + (int)nwarps);
-        const int e0 = __shfl_sync(0xffffffffu, o, 0);
-        const int e1 = __shfl_sync(0xffffffffu, o, 1);
-        const int e2 = __shfl_sync(0xffffffffu, o, K >= 2 ? 2 : 1);
-        const int e3 = __shfl_sync(0xffffffffu, o, K >= 3 ? 3 : 1);
-        const int eK = __shfl_sync(0xffffffffu, o, K);
-        auto level_of = [&](const int i) { return i < e1 ? 1 : (i < e2 ? 2 : (i < e3 ? 3 : 4)); };
-        if (x0 >= 0) atomicOr(Ab + (level_of(e0 + (int)lane) - 1) * 128 + (x0 >> 5), 1u << (x0 & 31));
-        if (x1 >= 0) atomicOr(Ab + (level_of(e0 + 32 + (int)lane) - 1) * 128 + (x1 >> 5), 1u << (x1 & 31));
-        for (int base = e0 + 64; base < eK; base += 32) {   // rows with more than 64 entries here
-            const int i = base + (int)lane;
-            if (i < eK) {
-                const int x = (int)__ldg(ent + (size_t)v * cap + i);
-                atomicOr(Ab + (level_of(i) - 1) * 128 + (x >> 5), 1u << (x & 31));
-            }
-        }
-        __syncwarp();
-        // this lane's chunk: the diagonal, then the levels
-        uint4 vv = pad;
+    const int per = (int)(((unsigned)rows + nwarps - 1u) / nwarps);
+    const int v_lo = min(rows, (int)gwarp * per), v_hi = min(rows, v_lo + per);
+    for (int r0 = v_lo; r0 < v_hi; r0 += kWalkStageRows) {
+        const int R = min(kWalkStageRows, v_hi - r0);
+        // 1. bucket bounds (and the lifted forms' source ids of the rows)
+        int oA = 0, oB = 0, gd = 0;
         {
-            const int g = a.inv ? __ldg(a.inv + v) : v - a.src_first;
-            const int j = g - first;
-            if (g >= 0 && (unsigned)j < (unsigned)ns && (unsigned)(j >> 7) == lane) {
-                const unsigned bit = 1u << (j & 31), comp = ((unsigned)j >> 5) & 3u;
-                if (comp == 0u) vv.x |= bit; else if (comp == 1u) vv.y |= bit;
-                else if (comp == 2u) vv.z |= bit; else vv.w |= bit;
-            }
+            const int rA = (int)lane / (K + 1), rB = ((int)lane + 32) / (K + 1);
+            if (rA < R) oA = (int)__ldg(off_b + (size_t)(r0 + rA) * off_stride + ((int)lane - rA * (K + 1)));
+            if (rB < R) oB = (int)__ldg(off_b + (size_t)(r0 + rB) * off_stride + ((int)lane + 32 - rB * (K + 1)));
+            if (inv && (int)lane < R) gd = __ldg(inv + r0 + (int)lane);
         }
-        uint4 prev = vv;
-        unsigned pc = u4popc(vv);
-        for (int L = 0; L < K; ++L) {
-            const uint4 al = Ab4[L * 32 + lane];
-            Ab4[L * 32 + lane] = u4zero();          // clean for the next row
-            prev = vv;
-            vv = u4or(vv, al);
-            const unsigned pn = u4popc(vv);
-            cnt[L] += pn - pc;
-            pc = pn;
+        auto bound = [&](const int i) {   // bound i of the staged rows (i uniform)
+            return __shfl_sync(0xffffffffu, i < 32 ? oA : oB, i & 31);
+        };
+        // 2. entry words of each row (rows start 4-byte aligned: cap is even)
+        for (int r = 0; r < R; ++r) {
+            const int e0 = bound(r * (K + 1)), eK = bound(r * (K + 1) + K);
+            const int w0 = e0 >> 1, w1 = min((eK + 1) >> 1, w0 + kWalkStageWords);
+            const uint32_t *src = reinterpret_cast<const uint32_t *>(ent + (size_t)(r0 + r) * cap);
+            for (int w = w0 + (int)lane; w < w1; w += 32) cp_async4(Es + r * kWalkStageWords + (w - w0), src + w);
         }
-        const uint4 ff = andnot(vv, prev);
-        a.V[(size_t)v * 32 + lane] = vv;
-        if (F) F[(size_t)v * 32 + lane] = ff;
-        const unsigned m = __ballot_sync(0xffffffffu, u4any(ff));
-        if (lane == 0) fl[v] = m;
+        cp_async_wait_all();
         __syncwarp();
-        o = o_n;
-        o_n = o_nn;
-        x0 = xn0;
-        x1 = xn1;
+        // 3. the rows
+        for (int r = 0; r < R; ++r) {
+            const int v = r0 + r;
+            int e[K + 1];
+#pragma unroll
+            for (int k = 0; k <= K; ++k) e[k] = bound(r * (K + 1) + k);
+            const int n = e[K] - e[0];
+            const uint16_t *Er = reinterpret_cast<const uint16_t *>(Es + r * kWalkStageWords) + (e[0] & 1);
+            for (int i = (int)lane; i < n; i += 32) {
+                const int x = i < 64 ? (int)Er[i] : (int)__ldg(ent + (size_t)v * cap + e[0] + i);
+                int L = 0;
+#pragma unroll
+                for (int k = 1; k < K; ++k) L += (e[0] + i >= e[k]) ? 1 : 0;
+                atomicOr(Ab + L * 128 + (x >> 5), 1u << (x & 31));
+            }
+            __syncwarp();
+            uint4 vv = pad;
+            {
+                const int g = inv ? __shfl_sync(0xffffffffu, gd, r) : v - a.src_first;
+                const int j = g - first;
+                if (g >= 0 && (unsigned)j < (unsigned)ns && (unsigned)(j >> 7) == lane) {
+                    const unsigned bit = 1u << (j & 31), comp = ((unsigned)j >> 5) & 3u;
+                    if (comp == 0u) vv.x |= bit; else if (comp == 1u) vv.y |= bit;
+                    else if (comp == 2u) vv.z |= bit; else vv.w |= bit;
+                }
+            }
+            // level by level (a branch-free form: skipping the popcounts and clearing
+            // stores of empty lanes measured slower)
+            uint4 prev = vv;
+            unsigned pc = u4popc(vv);
+#pragma unroll
+            for (int L = 0; L < K; ++L) {
+                const uint4 al = Ab4[L * 32 + lane];
+                Ab4[L * 32 + lane] = u4zero();          // clean for the next row
+                prev = vv;
+                vv = u4or(vv, al);
+                const unsigned pn = u4popc(vv);
+                cnt[L] += pn - pc;
+                pc = pn;
+            }
+            const uint4 ff = andnot(vv, prev);
+            a.V[(size_t)v * 32 + lane] = vv;
+            if (F) F[(size_t)v * 32 + lane] = ff;
+            const unsigned m = __ballot_sync(0xffffffffu, u4any(ff));
+            if (lane == 0) fl[v] = m;
+            __syncwarp();
+        }
     }
 #pragma unroll
-    for (int L = 0; L < 4; ++L) {
+    for (int L = 0; L < K; ++L) {
         const unsigned t = __reduce_add_sync(0xffffffffu, cnt[L]);
         if (lane == 0 && t) atomicAdd(s_cnt + L, (unsigned long long)t);
     }
@@ -1258,7 +1388,10 @@ static __device__ __noinline__ unsigned walk_batch(const BfsArgs &a, const int b
     __shared__ unsigned long long s_wcnt[4];
     unsigned long long *counts = a.counts + (size_t)b * (size_t)a.stride;
     if (threadIdx.x < 4) s_wcnt[threadIdx.x] = 0ull;
-    if (blockIdx.x == 0 && threadIdx.x == 0) counts[0] = (unsigned long long)ns;
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        counts[0] = (unsigned long long)ns;
+        if (a.vtot) a.vtot[0] = a.vtot[1] = a.vtot[2] = 0ull;   // the level totals of the batch
+    }
     if (b == 0 && a.level_ns && gtid == 0) a.level_ns[0] = gtimer();
     const int K = a.walk_K;
     // the pass's arguments in shared memory (one copy per block, not a
@@ -1277,10 +1410,17 @@ static __device__ __noinline__ unsigned walk_batch(const BfsArgs &a, const int b
     }
     __syncthreads();
     if (a.nC == 32) {
-        uint4 *Ab4 = reinterpret_cast<uint4 *>(reinterpret_cast<unsigned char *>(s_adj) + a.walk_smem_off +
-                                               (size_t)(threadIdx.x >> 5) * walk_smem_per_warp(32));
-        walk_rows32(a, b, a.src_begin + b * 128 * a.nC, ns, vpull_on(a) ? nullptr : (((K + 1) & 1) ? a.F0 : a.F1),
-                    ((K + 1) & 1) ? a.fl0 : a.fl1, Ab4, gtid >> 5, nthr >> 5, s_wcnt);
+        unsigned char *wsm = reinterpret_cast<unsigned char *>(s_adj) + a.walk_smem_off +
+                             (size_t)(threadIdx.x >> 5) * walk_smem_per_warp(32);
+        uint4 *Fw = vpull_on(a) ? nullptr : (((K + 1) & 1) ? a.F0 : a.F1);
+        uint32_t *flw = ((K + 1) & 1) ? a.fl0 : a.fl1;
+        const int first = a.src_begin + b * 128 * a.nC;
+        switch (K) {
+            case 1: walk_rows32<1>(a, b, first, ns, Fw, flw, wsm, gtid >> 5, nthr >> 5, s_wcnt); break;
+            case 2: walk_rows32<2>(a, b, first, ns, Fw, flw, wsm, gtid >> 5, nthr >> 5, s_wcnt); break;
+            case 3: walk_rows32<3>(a, b, first, ns, Fw, flw, wsm, gtid >> 5, nthr >> 5, s_wcnt); break;
+            default: walk_rows32<4>(a, b, first, ns, Fw, flw, wsm, gtid >> 5, nthr >> 5, s_wcnt); break;
+        }
     } else {
         walk_rows(w, reinterpret_cast<unsigned char *>(s_adj) + a.walk_smem_off, gtid >> 5, nthr >> 5, s_wcnt);
     }
@@ -1355,6 +1495,7 @@ __global__ void __launch_bounds__(kBlock, min_blocks_for(D)) bfs_batch_kernel(co
     // plain OR rows (the WVC masks are taken over every chunk, which only pull
     // levels visit).
     if (threadIdx.x == 0) {
+        S.sym = a.walk_asym != nullptr && a.vtot != nullptr && ld_acquire_i(a.walk_asym) == 0;
         S.push_on = D > 0 && 32 % D == 0 && a.push_ppm > 0 && a.P0 != nullptr && a.asym != nullptr &&
                     a.masks == nullptr && (PL || a.walk_K == 0);
         S.dirty_p = -1;
@@ -1451,6 +1592,8 @@ __global__ void __launch_bounds__(kBlock, min_blocks_for(D)) bfs_batch_kernel(co
             const bool split = dense && S.reached * 1000000ull >= pairs * (unsigned long long)a.split_ppm;
             const bool write_all =
                 !nf_use && c_prev * 1000000ull >= pairs * (unsigned long long)a.dense_w_ppm;
+            // dense visited-set pull on a table without one-way entries: no own chunks
+            const bool no_own = vp && S.sym && dense && !nf_use;
             const bool odd = (L & 1) != 0;
             unsigned cnt = 0u, and_pre = 0xffffffffu, and_post = 0xffffffffu;
             if (push) {
@@ -1467,7 +1610,8 @@ __global__ void __launch_bounds__(kBlock, min_blocks_for(D)) bfs_batch_kernel(co
                 __syncthreads();
                 cnt = vpull_level<D>(a, d, adj, v_base, t_hi, x_is_v ? a.V : a.F0, x_is_v ? a.F0 : a.V,
                                      odd ? a.fl0 : a.fl1, odd ? a.fl1 : a.fl0, odd ? a.nf : a.nf2,
-                                     odd ? a.nf2 : a.nf, dense, L == a.walk_K + 1, skip_full, split, nf_use, &s_next);
+                                     odd ? a.nf2 : a.nf, dense, L == a.walk_K + 1, skip_full, split, nf_use,
+                                     no_own, &s_next);
             } else {
                 const uint4 *Fc = in_p >= 0 ? (in_p ? a.P1 : a.P0) : (odd ? a.F0 : a.F1);
                 const uint32_t *fc = in_p >= 0 ? (in_p ? a.pf1 : a.pf0) : (odd ? a.fl0 : a.fl1);
@@ -1522,7 +1666,8 @@ __global__ void __launch_bounds__(kBlock, min_blocks_for(D)) bfs_batch_kernel(co
             if (threadIdx.x == 0) {
                 unsigned long long bsum = 0;
                 for (int w = 0; w < kBlock / 32; ++w) bsum += s_sum[w];
-                if (bsum) atomicAdd(counts + L, bsum);
+                if (bsum) atomicAdd(no_own ? a.vtot + L % 3 : counts + L, bsum);
+                if (vp && a.vtot && blockIdx.x == 0) a.vtot[(L + 1) % 3] = 0ull;   // read last after level L - 2
                 if (masks) {
                     unsigned m0 = 0xffffffffu, m1 = 0xffffffffu;
                     for (int w = 0; w < kBlock / 32; ++w) { m0 &= s_and[0][w]; m1 &= s_and[1][w]; }
@@ -1530,10 +1675,20 @@ __global__ void __launch_bounds__(kBlock, min_blocks_for(D)) bfs_batch_kernel(co
                     atomicAnd(masks + L, m1);
                 }
             }
-            if (!grid_sync(a.ctl, a.expected, a.wait_ns, L, epoch)) return;
+            // the level's sum comes with the barrier (read by its last arrival)
+            unsigned long long lsum = 0;
+            if (!grid_sync_value(a.ctl, a.expected, a.wait_ns, L, epoch, no_own ? a.vtot + L % 3 : counts + L,
+                                 lsum))
+                return;
             if (b == 0 && a.level_ns && gtid == 0) a.level_ns[L] = gtimer();
             if (threadIdx.x == 0) {
-                const unsigned long long cL = ld_relaxed_u64(counts + L);
+                unsigned long long cL = lsum;
+                if (no_own) {
+                    // total bits of V_L less the padding and the pairs reached before
+                    const unsigned long long pad = (unsigned long long)a.rows * (unsigned long long)(128 * a.nC - ns);
+                    cL = lsum - pad - S.reached;
+                    if (blockIdx.x == 0) counts[L] = cL;
+                }
                 S.reached += cL;
                 S.c_prev = cL;
                 S.wrote_all_prev = !push && write_all;

@@ -126,19 +126,44 @@ def test_visited_pull_matches_frontier_pull(n, steps, bits, walk):
     adj = circulant(n, steps)
     d = adj.shape[1]
     got = {}
-    for vp in (0, 1):
-        old = os.environ.get("GG_VPULL")
-        os.environ["GG_VPULL"] = str(vp)
-        try:
-            e = engine_with(walk, lambda: G.cudaASPLgraph(n, d, 0))
-            engine_with(walk, lambda: e.set_batch_sources(bits))
-            got[vp] = counts(e, adj, n + 1)
-        finally:
-            if old is None:
-                del os.environ["GG_VPULL"]
-            else:
-                os.environ["GG_VPULL"] = old
-    assert got[1] == got[0]
+    for mode in ("frontier", "visited", "visited_own"):
+        env = {"GG_VPULL": "0" if mode == "frontier" else "1", "GG_OWN_SKIP": "0" if mode == "visited_own" else "1"}
+        got[mode] = counts_with_env(env, walk, n, d, bits, adj)
+    assert got["visited"] == got["frontier"] and got["visited_own"] == got["frontier"]
     o = O.bfs_pull(adj, np.arange(n))
-    assert got[1][0] == o.total() and got[1][2] == o.levels
-    assert np.array_equal(np.asarray(got[1][5][:o.levels + 1]), o.level_counts[:o.levels + 1])
+    assert got["visited"][0] == o.total() and got["visited"][2] == o.levels
+    assert np.array_equal(np.asarray(got["visited"][5][:o.levels + 1]), o.level_counts[:o.levels + 1])
+
+
+def counts_with_env(env, walk, n, d, bits, adj):
+    old = {k: os.environ.get(k) for k in env}
+    os.environ.update(env)
+    try:
+        e = engine_with(walk, lambda: G.cudaASPLgraph(n, d, 0))
+        engine_with(walk, lambda: e.set_batch_sources(bits))
+        return counts(e, adj, n + 1)
+    finally:
+        for k, v in old.items():
+            if v is None:
+                del os.environ[k]
+            else:
+                os.environ[k] = v
+
+
+@pytest.mark.parametrize("one_way", [False, True])
+def test_dense_levels_without_own_chunks(one_way):
+    """Dense visited-set pull levels skip their own chunks only on tables whose
+    entries all list their row back (the walk index kernel's one-way flag); one
+    one-way entry must bring the own reads back, with the same exact counts."""
+    n, d = 12288, 8
+    adj = G.random_regular(n, d, 21).copy()
+    if one_way:
+        v = 777
+        u = int(adj[v, 0])
+        w = next(x for x in range(n) if x != v and x not in adj[v] and v not in adj[x] and x != u)
+        adj[v, 0] = w          # v now pulls from w; w's row does not list v
+    want = counts_with_env({"GG_VPULL": "0"}, 3, n, d, 4096, adj)
+    got = counts_with_env({"GG_VPULL": "1", "GG_OWN_SKIP": "1"}, 3, n, d, 4096, adj)
+    assert got == want
+    o = O.bfs_pull(adj, np.arange(n))
+    assert got[0] == o.total() and got[2] == o.levels

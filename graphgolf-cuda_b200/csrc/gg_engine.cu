@@ -146,7 +146,12 @@ struct gg_engine {
     uint32_t *d_nf = nullptr;            // not-full bit per visited chunk
     uint32_t *d_nf2 = nullptr;           // its second copy (visited-set pull levels alternate)
     int *d_wasym = nullptr;              // one-way flag of the table (walk_index_kernel)
-    unsigned long long *d_vtot = nullptr;   // 3 level totals (dense visited-set pull without own chunks)
+    unsigned long long *d_vtot = nullptr;   // [nb][3] level totals (dense visited-set pull without own chunks)
+    // walk_all_kernel output: the level-K rows of every batch and their flag words
+    uint4 *d_vall = nullptr;
+    uint32_t *d_vall_fl = nullptr;
+    size_t vall_batches = 0;             // batches d_vall holds
+    long long walk_all_mb = 4096;        // budget for d_vall (GG_WALK_ALL_MB; 0: per-batch walk passes)
     bool p_dirty = true;                 // push buffers must be zeroed before the next launch
     unsigned long long *d_counts = nullptr;
     unsigned *d_masks = nullptr;
@@ -176,6 +181,10 @@ struct gg_engine {
 namespace {
 
 void free_batch_buffers(gg_engine *e) {
+    cudaFree(e->d_vall); cudaFree(e->d_vall_fl);
+    e->d_vall = nullptr;
+    e->d_vall_fl = nullptr;
+    e->vall_batches = 0;
     cudaFree(e->d_V); cudaFree(e->d_F0); cudaFree(e->d_F1);
     cudaFree(e->d_fl0); cudaFree(e->d_fl1);
     cudaFree(e->d_P0); cudaFree(e->d_P1); cudaFree(e->d_pf0); cudaFree(e->d_pf1);
@@ -189,7 +198,7 @@ void free_batch_buffers(gg_engine *e) {
 }
 
 void free_counters(gg_engine *e) {
-    cudaFree(e->d_status); cudaFree(e->d_masks); cudaFree(e->d_level_ns);
+    cudaFree(e->d_status); cudaFree(e->d_masks); cudaFree(e->d_level_ns); cudaFree(e->d_vtot);
     cudaFreeHost(e->h_status); cudaFreeHost(e->h_masks);
     cudaFreeHost(e->h_level_ns);
     e->d_status = e->h_status = nullptr;
@@ -288,6 +297,40 @@ int walk_levels(const gg_engine *e) {
         if (ok) break;
     }
     return K;
+}
+
+// walk_all_kernel for an evaluation of nb batches, or nullptr (a walk pass per
+// batch): visited-set pull levels, 4096-source batches, degree 4 or 8, K <= 3, and
+// the level-K rows of all nb batches within the GG_WALK_ALL_MB budget.  Grows
+// d_vall as needed (a failed allocation falls back to the per-batch pass).
+void *walk_all_for(gg_engine *e, int K, int nb) {
+    if (!e->walk_vpull || e->nC != 32 || K < 1 || K > 3 || (e->d != 4 && e->d != 8)) return nullptr;
+    const size_t bytes = (size_t)nb * e->items * sizeof(uint4);
+    const size_t fbytes = (size_t)nb * ((e->items + 31) / 32) * sizeof(uint32_t);
+    if ((long long)(bytes >> 20) > e->walk_all_mb) return nullptr;
+    if ((size_t)nb > e->vall_batches) {
+        invalidate_graph(e);
+        cudaFree(e->d_vall); cudaFree(e->d_vall_fl);
+        e->d_vall = nullptr;
+        e->d_vall_fl = nullptr;
+        e->vall_batches = 0;
+        if (cudaMalloc(&e->d_vall, bytes) != cudaSuccess || cudaMalloc(&e->d_vall_fl, fbytes) != cudaSuccess) {
+            cudaFree(e->d_vall); cudaFree(e->d_vall_fl);
+            e->d_vall = nullptr;
+            e->d_vall_fl = nullptr;
+            (void)cudaGetLastError();
+            return nullptr;
+        }
+        e->vall_batches = (size_t)nb;
+    }
+    void *k = nullptr;
+    if (e->d == 8) k = K == 1 ? (void *)gg::walk_all_kernel<8, 1> : K == 2 ? (void *)gg::walk_all_kernel<8, 2> : (void *)gg::walk_all_kernel<8, 3>;
+    else k = K == 1 ? (void *)gg::walk_all_kernel<4, 1> : K == 2 ? (void *)gg::walk_all_kernel<4, 2> : (void *)gg::walk_all_kernel<4, 3>;
+    if (cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, gg::walk_all_smem(K)) != cudaSuccess) {
+        (void)cudaGetLastError();
+        return nullptr;
+    }
+    return k;
 }
 
 void *index_kernel_for(int d) {
@@ -455,7 +498,7 @@ gg_status ensure_counters(gg_engine *e, int cap, int nb) {
     e->h_bad = reinterpret_cast<int *>(e->h_status + sizeof(Ctl));
     e->d_asym = e->d_bad + 1;
     e->d_wasym = e->d_bad + 2;
-    e->d_vtot = reinterpret_cast<unsigned long long *>(e->d_status + sizeof(Ctl) + 64);
+    GG_CK(cudaMalloc(&e->d_vtot, (size_t)nb * 3 * sizeof(unsigned long long)));
     e->d_levels_run = reinterpret_cast<int *>(e->d_status + e->off_levels_run);
     e->h_levels_run = reinterpret_cast<int *>(e->h_status + e->off_levels_run);
     e->d_batch_ns = reinterpret_cast<unsigned long long *>(e->d_status + e->off_batch_ns);
@@ -514,6 +557,7 @@ gg_status create_common(gg_engine *e) {
     e->split_ppm = env_int("GG_SPLIT_PPM", e->split_ppm);
     e->walk_vpull = env_int("GG_VPULL", e->walk_vpull) != 0;
     e->walk_own_skip = env_int("GG_OWN_SKIP", e->walk_own_skip) != 0;
+    e->walk_all_mb = env_int("GG_WALK_ALL_MB", (int)e->walk_all_mb);
     e->push_ppm = env_int("GG_PUSH_PPM", e->push_ppm);
     e->push_min_items = env_int("GG_PUSH_MIN_ITEMS", e->push_min_items);
     e->use_graph = env_int("GG_NO_GRAPH", 0) == 0;
@@ -578,6 +622,7 @@ gg_status run_eval(gg_engine *e, const int32_t *d_table_in, const gg_eval_opts *
     // (their per-level bookkeeping lives in the level loop), at most the level cap.
     const int walk_K = (wvc || (x && x->planes)) ? 0 : std::min(e->walk_K, cap_req);
     const int launches = 1 + ((long long)e->rows * e->d > 0 ? 1 : 0) + (walk_K > 0 ? 1 : 0) + (walk_K >= 3 ? 1 : 0);
+    void *wall = walk_K > 0 ? walk_all_for(e, walk_K, nb) : nullptr;
 
     // Everything the GPU does for one evaluation, on `q`: status words zeroed,
     // table -> adjacency (checked), one cooperative launch for every source
@@ -613,6 +658,7 @@ gg_status run_eval(gg_engine *e, const int32_t *d_table_in, const gg_eval_opts *
         if (walk_K > 0) {
             // blocks add the walk's level counts before any grid barrier
             GG_CK(cudaMemsetAsync(e->d_counts, 0, (size_t)nb * stride * sizeof(unsigned long long), q));
+            GG_CK(cudaMemsetAsync(e->d_vtot, 0, (size_t)nb * 3 * sizeof(unsigned long long), q));
             if (walk_K >= 3) {
                 const long long nh = (long long)e->rows * e->d * e->d;
                 gg::h2_kernel<<<(int)std::min<long long>((nh + 255) / 256, 8192), 256, 0, q>>>(
@@ -640,13 +686,21 @@ gg_status run_eval(gg_engine *e, const int32_t *d_table_in, const gg_eval_opts *
             wi.bad = e->form == FORM_GRAPH ? e->d_bad : nullptr;
             wi.asym = e->walk_vpull && e->walk_own_skip ? e->d_wasym : nullptr;
             // one resident wave of blocks, each striding over the rows
+            void *wk = wall ? wall : index_kernel_for(e->d);
+            const size_t wsmem = wall ? (size_t)gg::walk_all_smem(walk_K) : 0;
+            if (wall) {
+                wi.vall = e->d_vall;
+                wi.vall_fl = e->d_vall_fl;
+                wi.counts = e->d_counts;
+                wi.counts_stride = stride;
+            }
             int sms = 0, per_sm = 0;
             GG_CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, e->device));
-            GG_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, index_kernel_for(e->d), gg::kIndexBlock, 0));
+            GG_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, wk, gg::kIndexBlock, wsmem));
             const int wgrid = (int)std::max<long long>(1, std::min<long long>(((long long)e->rows + 7) / 8,
                                                                               (long long)sms * std::max(per_sm, 1)));
             void *wargs[] = {&wi};
-            GG_CK(cudaLaunchKernel(index_kernel_for(e->d), dim3(wgrid), dim3(gg::kIndexBlock), wargs, 0, q));
+            GG_CK(cudaLaunchKernel(wk, dim3(wgrid), dim3(gg::kIndexBlock), wargs, wsmem, q));
         }
         BfsArgs a{};
         a.adj = e->d_adj;
@@ -697,6 +751,8 @@ gg_status run_eval(gg_engine *e, const int32_t *d_table_in, const gg_eval_opts *
         a.walk_vpull = walk_K > 0 && !wvc ? e->walk_vpull : 0;
         a.walk_asym = a.walk_vpull && e->walk_own_skip ? e->d_wasym : nullptr;
         a.vtot = e->d_vtot;
+        a.vall = wall ? e->d_vall : nullptr;
+        a.vall_fl = wall ? e->d_vall_fl : nullptr;
         void *args[] = {&a};
         GG_CK(cudaLaunchCooperativeKernel(kernel_for(e->d, a.planes != nullptr), dim3(e->grid), dim3(gg::kBlock), args,
                                           e->smem_bytes, q));

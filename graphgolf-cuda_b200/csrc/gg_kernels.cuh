@@ -144,10 +144,15 @@ struct BfsArgs {
     // chunks: for L >= 2, V_{L-1}[v] lies within the union of the neighbours'
     // V_{L-1}[u] (the source v through any neighbour, every other source through the
     // neighbour on a shortest path).  Such a level adds its rows' popcounts into
-    // vtot[L % 3] (3 slots: zeroed two levels ahead), and its count is that total
-    // less the padding bits and the pairs reached before it.
+    // vtot[3b + L % 3] (3 slots a batch: zeroed two levels ahead), and its count is
+    // that total less the padding bits and the pairs reached before it.
     const int *walk_asym;
-    unsigned long long *vtot;
+    unsigned long long *vtot;   // [nb][3], zeroed by the host
+    // walk_all_kernel's output (nullptr: a walk pass per batch): the level-K visited
+    // rows of batch b at vall + b * items (the batch's levels then alternate between
+    // that slice and V) and the level-K frontier flag words at vall_fl + b * tiles.
+    uint4 *vall;
+    const uint32_t *vall_fl;
 };
 
 // Where a level's new pairs go in the distance planes.
@@ -805,6 +810,11 @@ struct WalkIndexArgs {
     int off_stride;
     const int *bad;           // nonzero: the table failed its range check
     int *asym;                // set to 1 when some row u lacks v for an entry u of row v (nullptr: not checked)
+    // walk_all_kernel only: the level-K visited rows of every batch and their flag words
+    uint4 *vall;              // [nb][rows * 32]
+    uint32_t *vall_fl;        // [nb][rows]
+    unsigned long long *counts;   // [nb][counts_stride]: levels 1..K added
+    int counts_stride;
 };
 
 constexpr int kIndexBlock = 256;
@@ -874,16 +884,21 @@ __device__ __forceinline__ void for_walk_ends(const WalkIndexArgs &a, const int 
             fn(__ldg(a.h2 + (size_t)__ldg(a.h2 + (size_t)v * dd + i / dd) * dd + i % dd), 4);
 }
 
-// One row of the walk index with its ends in registers (D <= 8 with D*D % 4 == 0,
-// K <= 3, level-2 ends from H2 or the adjacency rows): the ends are enumerated and
-// classified once, then counted and placed from registers.
+// The walk ends of row v in registers (D <= 8 with D*D % 4 == 0, K <= 3, level-2
+// ends from H2 or the adjacency rows), each classified as (key << 16) | payload with
+// key = batch * K + level - 1 and payload the source's place in its batch, or -1;
+// also the row's one-way check.  NV slots a lane.
 template <int D>
-__device__ __forceinline__ void index_row_regs(const WalkIndexArgs &a, const int v, const unsigned lane,
-                                               unsigned *cur, uint16_t *row, const int nkeys) {
-    constexpr int DD = D * D, Q = DD / 4;           // uint4 per level-2 list
-    constexpr int U3 = D * Q, S3 = (U3 + 31) / 32;  // uint4 of the level-3 ends, per lane
-    constexpr int NV = 1 + 4 * ((Q + 31) / 32) + 4 * S3;
-    int pk[NV];                                     // (key << 16) | payload, or -1
+struct RowEnds {
+    static constexpr int DD = D * D, Q = DD / 4;           // uint4 per level-2 list
+    static constexpr int U3 = D * Q, S3 = (U3 + 31) / 32;  // uint4 of the level-3 ends, per lane
+    static constexpr int NV = 1 + 4 * ((Q + 31) / 32) + 4 * S3;
+};
+
+template <int D>
+__device__ __forceinline__ void row_ends_regs(const WalkIndexArgs &a, const int v, const unsigned lane,
+                                              int (&pk)[RowEnds<D>::NV]) {
+    constexpr int DD = RowEnds<D>::DD, Q = RowEnds<D>::Q, U3 = RowEnds<D>::U3, S3 = RowEnds<D>::S3;
     const int32_t *arow = a.adj + (size_t)v * D;
     auto classify = [&](const int32_t w, const int L) -> int {
         const int g = a.inv ? __ldg(a.inv + w) : w - a.src_first;
@@ -941,6 +956,15 @@ __device__ __forceinline__ void index_row_regs(const WalkIndexArgs &a, const int
         pk[n++] = ok ? classify((int32_t)q3[s3].z, 3) : -1;
         pk[n++] = ok ? classify((int32_t)q3[s3].w, 3) : -1;
     }
+}
+
+// One row of the walk index from its ends in registers: counted and placed.
+template <int D>
+__device__ __forceinline__ void index_row_regs(const WalkIndexArgs &a, const int v, const unsigned lane,
+                                               unsigned *cur, uint16_t *row, const int nkeys) {
+    constexpr int NV = RowEnds<D>::NV;
+    int pk[NV];
+    row_ends_regs<D>(a, v, lane, pk);
 #pragma unroll
     for (int k = 0; k < NV; ++k)
         if (pk[k] >= 0) atomicAdd(cur + (pk[k] >> 16), 1u);
@@ -970,6 +994,87 @@ __device__ __forceinline__ void index_row_regs(const WalkIndexArgs &a, const int
         if (pk[k] >= 0) row[atomicAdd(cur + (pk[k] >> 16), 1u)] = (uint16_t)(pk[k] & 0xffff);
     __syncwarp();
     copy_row_out(a, v, lane, row, total);
+}
+
+// Walk pass of every batch at once (4096-source batches, D = 4 or 8, K <= 3): one warp
+// per row enumerates the row's walk ends once (row_ends_regs), then builds the row's
+// level-K visited row of each batch, kWalkAllGroup batches at a time, exactly as
+// walk_rows32 does for one batch (each level's ends ORed into its own shared-memory
+// copy of the row; V_L = V_{L-1} | A_L from the padding and the diagonal up; the
+// level's new pairs popc(V_L) - popc(V_{L-1})), and writes it to vall[b], its
+// level-K frontier flag word to vall_fl[b], and the level counts into counts[b].
+// The levels after the walk then start from vall[b] (BfsArgs::vall).
+constexpr int kWalkAllGroup = 4;
+__host__ __device__ constexpr int walk_all_smem(int K) { return (kIndexBlock / 32) * kWalkAllGroup * K * 512; }
+
+template <int D, int K>
+__global__ void __launch_bounds__(kIndexBlock) walk_all_kernel(const WalkIndexArgs a) {
+    extern __shared__ __align__(16) unsigned char s_walk[];
+    __shared__ unsigned long long s_cnt[kIndexMaxKeys];
+    if (a.bad && *a.bad) return;
+    const unsigned lane = threadIdx.x & 31u, wib = threadIdx.x >> 5;
+    const int nb = a.nb, nkeys = nb * K;   // a.K == K
+    for (int k = (int)threadIdx.x; k < nkeys; k += (int)blockDim.x) s_cnt[k] = 0ull;
+    __syncthreads();
+    uint4 *buf4 = reinterpret_cast<uint4 *>(s_walk) + (size_t)wib * kWalkAllGroup * K * 32;
+    uint32_t *buf = reinterpret_cast<uint32_t *>(buf4);
+    constexpr int NV = RowEnds<D>::NV;
+    int pk[NV];
+    const size_t items = (size_t)a.rows * 32u;
+    for (int v = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5); v < a.rows;
+         v += (int)((gridDim.x * blockDim.x) >> 5)) {
+        row_ends_regs<D>(a, v, lane, pk);
+        // the row's own source: its diagonal bit
+        const int g = a.inv ? __ldg(a.inv + v) : v - a.src_first;
+        const int jd = (g >= 0 && (unsigned)(g - a.src_begin) < (unsigned)a.ns_total) ? g - a.src_begin : -1;
+        for (int g0 = 0; g0 < nb; g0 += kWalkAllGroup) {
+            const int G = min(kWalkAllGroup, nb - g0);
+            for (int i = 0; i < G * K; ++i) buf4[i * 32 + lane] = u4zero();
+            __syncwarp();
+#pragma unroll
+            for (int k = 0; k < NV; ++k)
+                if (pk[k] >= 0) {
+                    const int key = pk[k] >> 16, b = key / K;
+                    if (b >= g0 && b < g0 + G) {
+                        const int jj = pk[k] & 0xffff;
+                        atomicOr(buf + ((b - g0) * K + (key - b * K)) * 128 + (jj >> 5), 1u << (jj & 31));
+                    }
+                }
+            __syncwarp();
+            for (int bb = 0; bb < G; ++bb) {
+                const int b = g0 + bb;
+                const int ns = min(a.S, a.ns_total - b * a.S);
+                uint4 vv = pad_mask((int)lane, ns);
+                if (jd >= b * a.S && jd < b * a.S + ns) {
+                    const int j = jd - b * a.S;
+                    if ((unsigned)(j >> 7) == lane) {
+                        const unsigned bit = 1u << (j & 31), comp = ((unsigned)j >> 5) & 3u;
+                        if (comp == 0u) vv.x |= bit; else if (comp == 1u) vv.y |= bit;
+                        else if (comp == 2u) vv.z |= bit; else vv.w |= bit;
+                    }
+                }
+                uint4 prev = vv;
+                unsigned pc = u4popc(vv);
+#pragma unroll
+                for (int L = 0; L < K; ++L) {
+                    const uint4 al = buf4[(bb * K + L) * 32 + lane];
+                    prev = vv;
+                    vv = u4or(vv, al);
+                    const unsigned pn = u4popc(vv);
+                    const unsigned t = __reduce_add_sync(0xffffffffu, pn - pc);
+                    if (lane == 0 && t) atomicAdd(s_cnt + b * K + L, (unsigned long long)t);
+                    pc = pn;
+                }
+                a.vall[(size_t)b * items + (size_t)v * 32 + lane] = vv;
+                const unsigned m = __ballot_sync(0xffffffffu, u4any(andnot(vv, prev)));
+                if (lane == 0) a.vall_fl[(size_t)b * a.rows + v] = m;
+            }
+            __syncwarp();
+        }
+    }
+    __syncthreads();
+    for (int k = (int)threadIdx.x; k < nkeys; k += (int)blockDim.x)
+        if (s_cnt[k]) atomicAdd(a.counts + (size_t)(k / K) * a.counts_stride + (k % K) + 1, s_cnt[k]);
 }
 
 template <int D>
@@ -1226,10 +1331,12 @@ static __global__ void h2_kernel(const int32_t *adj, int32_t *h2, int rows, int 
     }
 }
 
-// Resident blocks per SM the register allocation targets: 6 (40 registers)
-// fits the small degrees without spills, 4 (64 registers) the larger ones.
+// Resident blocks per SM the register allocation targets: 4 (64 registers).  At 6
+// (40 registers) the level loop and its out-of-line level functions spill, and
+// the dense levels of a 65536-vertex, 8-regular evaluation ran about 25 % slower
+// (38 against 30 us a level); 32 resident warps a SM keep the gathers in flight.
 #ifndef GG_MIN_BLOCKS_SMALL_D
-#define GG_MIN_BLOCKS_SMALL_D 6
+#define GG_MIN_BLOCKS_SMALL_D 4
 #endif
 __host__ __device__ constexpr int min_blocks_for(int D) {
     return (D > 0 && D <= 8) ? GG_MIN_BLOCKS_SMALL_D : 4;
@@ -1250,6 +1357,9 @@ struct LoopState {
     int done;                    // the batch's level loop ends
     int L_next;                  // first level the level loop runs (after a walk pass)
     int sym;                     // the table has no one-way entries (walk_asym read 0)
+    uint4 *Pv, *Qv;              // the batch's visited-set pull buffers (Pv holds level walk_K)
+    const uint32_t *fl_walk;     // the flag words level walk_K + 1 reads
+    unsigned long long *vt;      // the batch's 3 level totals (a.vtot + 3b), or nullptr
 };
 
 // 4-byte asynchronous copy global -> shared (no registers held while in flight).
@@ -1378,6 +1488,36 @@ static __device__ __noinline__ void walk_rows32(const BfsArgs &a, const int b, c
 // line so that the level loop keeps its registers.  Returns the barrier count
 // after the pass, or kWaitGaveUp when a barrier wait gave up.
 constexpr unsigned kWaitGaveUp = 0xffffffffu;
+// The loop state after the walk's levels 1..K of batch b (their counts complete):
+// S.L_next = K + 1, or the level at which the batch ended, and the batch's buffers.
+__device__ __forceinline__ void walk_state(const BfsArgs &a, const int b, const int ns, LoopState &S) {
+    unsigned long long *counts = a.counts + (size_t)b * (size_t)a.stride;
+    const int K = a.walk_K;
+    if (threadIdx.x == 0) {
+        S.pairs = (unsigned long long)ns * (unsigned long long)a.rows;
+        S.reached = (unsigned long long)ns;
+        S.in_p = -1;
+        S.wrote_all_prev = 1;
+        S.nf_valid = 0;
+        S.done = 0;
+        int L = 1;
+        for (; L <= K; ++L) {
+            const unsigned long long cL = ld_relaxed_u64(counts + L);
+            S.reached += cL;
+            S.c_prev = cL;
+            if (cL == 0ull || L >= a.max_levels || S.reached == S.pairs) { S.done = 1; break; }
+        }
+        S.L_next = S.done ? L : K + 1;
+        S.Pv = a.vall ? a.vall + (size_t)b * a.items : a.V;
+        S.Qv = a.vall ? a.V : a.F0;
+        S.vt = a.vtot ? a.vtot + 3 * (size_t)b : nullptr;
+        S.fl_walk = a.vall ? a.vall_fl + (size_t)b * ((a.items + 31u) >> 5) : (((K + 1) & 1) ? a.fl0 : a.fl1);
+        if (b == 0 && a.level_ns && blockIdx.x == 0)
+            for (int k = 1; k <= K; ++k) a.level_ns[k] = gtimer();
+    }
+    __syncthreads();
+}
+
 template <int D>
 static __device__ __noinline__ unsigned walk_batch(const BfsArgs &a, const int b, const int ns, const int d,
                                                    const unsigned items, const unsigned gtid, const unsigned nthr,
@@ -1388,12 +1528,14 @@ static __device__ __noinline__ unsigned walk_batch(const BfsArgs &a, const int b
     __shared__ unsigned long long s_wcnt[4];
     unsigned long long *counts = a.counts + (size_t)b * (size_t)a.stride;
     if (threadIdx.x < 4) s_wcnt[threadIdx.x] = 0ull;
-    if (blockIdx.x == 0 && threadIdx.x == 0) {
-        counts[0] = (unsigned long long)ns;
-        if (a.vtot) a.vtot[0] = a.vtot[1] = a.vtot[2] = 0ull;   // the level totals of the batch
-    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) counts[0] = (unsigned long long)ns;
     if (b == 0 && a.level_ns && gtid == 0) a.level_ns[0] = gtimer();
     const int K = a.walk_K;
+    if (a.vall) {
+        // levels 1..K of every batch came from walk_all_kernel (launched before)
+        walk_state(a, b, ns, S);
+        return epoch;
+    }
     // the pass's arguments in shared memory (one copy per block, not a
     // by-value struct on every thread's stack)
     __shared__ WalkArgs w;
@@ -1429,25 +1571,7 @@ static __device__ __noinline__ unsigned walk_batch(const BfsArgs &a, const int b
         for (int L = 1; L <= K; ++L)
             if (s_wcnt[L - 1]) atomicAdd(counts + L, s_wcnt[L - 1]);
     if (!grid_sync(a.ctl, a.expected, a.wait_ns, 0, epoch)) return kWaitGaveUp;
-    if (threadIdx.x == 0) {
-        S.pairs = (unsigned long long)ns * (unsigned long long)a.rows;
-        S.reached = (unsigned long long)ns;
-        S.in_p = -1;
-        S.wrote_all_prev = 1;
-        S.nf_valid = 0;
-        S.done = 0;
-        int L = 1;
-        for (; L <= K; ++L) {
-            const unsigned long long cL = ld_relaxed_u64(counts + L);
-            S.reached += cL;
-            S.c_prev = cL;
-            if (cL == 0ull || L >= a.max_levels || S.reached == S.pairs) { S.done = 1; break; }
-        }
-        S.L_next = S.done ? L : K + 1;
-        if (b == 0 && a.level_ns && blockIdx.x == 0)
-            for (int k = 1; k <= K; ++k) a.level_ns[k] = gtimer();
-    }
-    __syncthreads();
+    walk_state(a, b, ns, S);
     return epoch;
 }
 
@@ -1604,14 +1728,16 @@ __global__ void __launch_bounds__(kBlock, min_blocks_for(D)) bfs_batch_kernel(co
                 if constexpr (D > 0 && 32 % D == 0) cnt = push_level<D, PL>(a.adj, a.V, a.div_nc, (unsigned)a.nC, Pc, Pn, pfc, pfn, ntiles,
                                            gtid, nthr);
             } else if (vp) {
-                // V_{L-1} alternates between V (level walk_K, written by the walk) and F0
-                const bool x_is_v = ((L - 1 - a.walk_K) & 1) == 0;
+                // V_{L-1} alternates between S.Pv (level walk_K: the walk's V, or the
+                // batch's walk_all_kernel slice) and S.Qv; level walk_K + 1 reads the
+                // walk's flag words
+                const bool x_is_p = ((L - 1 - a.walk_K) & 1) == 0;
                 if (threadIdx.x == 0) s_next = t_lo;
                 __syncthreads();
-                cnt = vpull_level<D>(a, d, adj, v_base, t_hi, x_is_v ? a.V : a.F0, x_is_v ? a.F0 : a.V,
-                                     odd ? a.fl0 : a.fl1, odd ? a.fl1 : a.fl0, odd ? a.nf : a.nf2,
-                                     odd ? a.nf2 : a.nf, dense, L == a.walk_K + 1, skip_full, split, nf_use,
-                                     no_own, &s_next);
+                cnt = vpull_level<D>(a, d, adj, v_base, t_hi, x_is_p ? S.Pv : S.Qv, x_is_p ? S.Qv : S.Pv,
+                                     L == a.walk_K + 1 ? S.fl_walk : (odd ? a.fl0 : a.fl1), odd ? a.fl1 : a.fl0,
+                                     odd ? a.nf : a.nf2, odd ? a.nf2 : a.nf, dense, L == a.walk_K + 1, skip_full,
+                                     split, nf_use, no_own, &s_next);
             } else {
                 const uint4 *Fc = in_p >= 0 ? (in_p ? a.P1 : a.P0) : (odd ? a.F0 : a.F1);
                 const uint32_t *fc = in_p >= 0 ? (in_p ? a.pf1 : a.pf0) : (odd ? a.fl0 : a.fl1);
@@ -1666,8 +1792,8 @@ __global__ void __launch_bounds__(kBlock, min_blocks_for(D)) bfs_batch_kernel(co
             if (threadIdx.x == 0) {
                 unsigned long long bsum = 0;
                 for (int w = 0; w < kBlock / 32; ++w) bsum += s_sum[w];
-                if (bsum) atomicAdd(no_own ? a.vtot + L % 3 : counts + L, bsum);
-                if (vp && a.vtot && blockIdx.x == 0) a.vtot[(L + 1) % 3] = 0ull;   // read last after level L - 2
+                if (bsum) atomicAdd(no_own ? S.vt + L % 3 : counts + L, bsum);
+                if (vp && S.vt && blockIdx.x == 0) S.vt[(L + 1) % 3] = 0ull;   // read last after level L - 2
                 if (masks) {
                     unsigned m0 = 0xffffffffu, m1 = 0xffffffffu;
                     for (int w = 0; w < kBlock / 32; ++w) { m0 &= s_and[0][w]; m1 &= s_and[1][w]; }
@@ -1677,7 +1803,7 @@ __global__ void __launch_bounds__(kBlock, min_blocks_for(D)) bfs_batch_kernel(co
             }
             // the level's sum comes with the barrier (read by its last arrival)
             unsigned long long lsum = 0;
-            if (!grid_sync_value(a.ctl, a.expected, a.wait_ns, L, epoch, no_own ? a.vtot + L % 3 : counts + L,
+            if (!grid_sync_value(a.ctl, a.expected, a.wait_ns, L, epoch, no_own ? S.vt + L % 3 : counts + L,
                                  lsum))
                 return;
             if (b == 0 && a.level_ns && gtid == 0) a.level_ns[L] = gtimer();

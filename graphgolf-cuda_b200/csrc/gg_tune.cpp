@@ -123,7 +123,9 @@ std::string tune_key(int device, const char *what, const std::vector<long long> 
             names[device] = gpu;
         }
     }
-    std::string k = "v1|" + gpu + "|" + what;
+    // the format version also retires entries tuned for earlier kernels (v2: the
+    // level kernel at 4 resident blocks a SM, the walk of all batches in one launch)
+    std::string k = "v2|" + gpu + "|" + what;
     for (long long d : dims) k += "|" + std::to_string(d);
     return k;
 }

@@ -167,3 +167,17 @@ def test_dense_levels_without_own_chunks(one_way):
     assert got == want
     o = O.bfs_pull(adj, np.arange(n))
     assert got[0] == o.total() and got[2] == o.levels
+
+
+@pytest.mark.parametrize("n,d,seed,walk", [(12288, 8, 31, 3), (9000, 4, 32, 3), (8200, 4, 33, 2), (8192, 8, 34, 1)])
+def test_walk_all_batches_at_once(n, d, seed, walk):
+    """walk_all_kernel (every batch's level-K rows built in one launch) against the
+    per-batch walk pass (GG_WALK_ALL_MB=0) and the oracle, with 4096-source batches
+    (the last one partial when n is not a multiple of 4096)."""
+    adj = G.random_regular(n, d, seed)
+    got = counts_with_env({"GG_VPULL": "1"}, walk, n, d, 4096, adj)
+    per_batch = counts_with_env({"GG_VPULL": "1", "GG_WALK_ALL_MB": "0"}, walk, n, d, 4096, adj)
+    assert got == per_batch
+    o = O.bfs_pull(adj, np.arange(n))
+    assert got[0] == o.total() and got[2] == o.levels
+    assert np.array_equal(np.asarray(got[5][:o.levels + 1]), o.level_counts[:o.levels + 1])

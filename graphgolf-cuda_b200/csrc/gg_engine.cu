@@ -693,6 +693,14 @@ gg_status run_eval(gg_engine *e, const int32_t *d_table_in, const gg_eval_opts *
                 wi.vall_fl = e->d_vall_fl;
                 wi.counts = e->d_counts;
                 wi.counts_stride = stride;
+                // the table's one-way flag first: walk_all_kernel reads it to choose
+                // how it counts, the level kernel whether dense levels read own chunks
+                wi.asym = nullptr;
+                wi.oneway = e->d_wasym;
+                const long long ne = (long long)e->rows * e->d;
+                gg::walk_check_kernel<<<(int)std::min<long long>((ne + 255) / 256, 8192), 256, 0, q>>>(
+                    e->d_adj, e->rows, e->d, e->d_wasym, e->form == FORM_GRAPH ? e->d_bad : nullptr);
+                GG_CK(cudaGetLastError());
             }
             int sms = 0, per_sm = 0;
             GG_CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, e->device));

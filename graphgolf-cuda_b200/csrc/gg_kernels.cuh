@@ -815,6 +815,7 @@ struct WalkIndexArgs {
     uint32_t *vall_fl;        // [nb][rows]
     unsigned long long *counts;   // [nb][counts_stride]: levels 1..K added
     int counts_stride;
+    const int *oneway;        // walk_check_kernel's flag (0: counts from the sources' side), or nullptr
 };
 
 constexpr int kIndexBlock = 256;
@@ -895,11 +896,57 @@ struct RowEnds {
     static constexpr int NV = 1 + 4 * ((Q + 31) / 32) + 4 * S3;
 };
 
+// The raw walk ends of a row in registers: level 1 (lanes < D), level 2 (lanes < Q,
+// 4 a lane), level 3 (S3 uint4 a lane, lanes' slot s3 * 32 + lane < U3).
 template <int D>
-__device__ __forceinline__ void row_ends_regs(const WalkIndexArgs &a, const int v, const unsigned lane,
-                                              int (&pk)[RowEnds<D>::NV]) {
+struct RowEndsRaw {
+    int32_t x1;
+    uint4 q2[(RowEnds<D>::Q + 31) / 32];
+    uint4 q3[RowEnds<D>::S3];
+};
+
+// Loads of row v's walk ends (all in flight together), and the row's one-way check.
+template <int D>
+__device__ __forceinline__ void row_ends_load(const WalkIndexArgs &a, const int v, const unsigned lane,
+                                              RowEndsRaw<D> &r) {
     constexpr int DD = RowEnds<D>::DD, Q = RowEnds<D>::Q, U3 = RowEnds<D>::U3, S3 = RowEnds<D>::S3;
     const int32_t *arow = a.adj + (size_t)v * D;
+    r.x1 = lane < (unsigned)D ? __ldg(arow + lane) : 0;
+#pragma unroll
+    for (int s2 = 0; s2 < (Q + 31) / 32; ++s2) {
+        const int i = s2 * 32 + (int)lane;
+        r.q2[s2] = make_uint4(0u, 0u, 0u, 0u);
+        if (a.K >= 2 && i < Q)
+            r.q2[s2] = a.h2 ? __ldg(reinterpret_cast<const uint4 *>(a.h2 + (size_t)v * DD) + i)
+                            : __ldg(reinterpret_cast<const uint4 *>(a.adj + (size_t)__ldg(arow + i / (D / 4)) * D) +
+                                    i % (D / 4));
+    }
+#pragma unroll
+    for (int s3 = 0; s3 < S3; ++s3) {
+        const int i = s3 * 32 + (int)lane;
+        r.q3[s3] = make_uint4(0u, 0u, 0u, 0u);
+        if (a.K >= 3 && i < U3)
+            r.q3[s3] = __ldg(reinterpret_cast<const uint4 *>(a.h2 + (size_t)__ldg(arow + i / Q) * DD) + i % Q);
+    }
+    if (a.asym) {
+        if (a.K >= 2) {
+            // the level-2 lists are the neighbours' rows, D / 4 lanes per row
+            bool f = (int)lane < Q && ((int)r.q2[0].x == v || (int)r.q2[0].y == v || (int)r.q2[0].z == v ||
+                                       (int)r.q2[0].w == v);
+            if constexpr (D / 4 == 2) f |= __shfl_xor_sync(0xffffffffu, f, 1) != 0;
+            if ((int)lane < Q && (int)lane % (D / 4) == 0 && !f) *a.asym = 1;
+        } else {
+            row_oneway_check(a, v, lane, D);
+        }
+    }
+}
+
+// Each raw end classified: (key << 16) | payload, key = batch * K + level - 1, payload
+// the source's place in its batch; -1 for ends that are no source of the evaluation.
+template <int D>
+__device__ __forceinline__ void row_ends_classify(const WalkIndexArgs &a, const unsigned lane, const RowEndsRaw<D> &r,
+                                                  int (&pk)[RowEnds<D>::NV]) {
+    constexpr int Q = RowEnds<D>::Q, U3 = RowEnds<D>::U3, S3 = RowEnds<D>::S3;
     auto classify = [&](const int32_t w, const int L) -> int {
         const int g = a.inv ? __ldg(a.inv + w) : w - a.src_first;
         const int j = g - a.src_begin;
@@ -907,55 +954,32 @@ __device__ __forceinline__ void row_ends_regs(const WalkIndexArgs &a, const int 
         const unsigned b = a.div_S.div((unsigned)j);
         return (int)(((b * (unsigned)a.K + (unsigned)(L - 1)) << 16) | ((unsigned)j - b * (unsigned)a.S));
     };
-    // loads first (all in flight), classification after
-    const int32_t x1 = lane < (unsigned)D ? __ldg(arow + lane) : 0;
-    uint4 q2[(Q + 31) / 32];
-#pragma unroll
-    for (int s2 = 0; s2 < (Q + 31) / 32; ++s2) {
-        const int i = s2 * 32 + (int)lane;
-        q2[s2] = make_uint4(0u, 0u, 0u, 0u);
-        if (a.K >= 2 && i < Q)
-            q2[s2] = a.h2 ? __ldg(reinterpret_cast<const uint4 *>(a.h2 + (size_t)v * DD) + i)
-                          : __ldg(reinterpret_cast<const uint4 *>(a.adj + (size_t)__ldg(arow + i / (D / 4)) * D) +
-                                  i % (D / 4));
-    }
-    uint4 q3[S3];
-#pragma unroll
-    for (int s3 = 0; s3 < S3; ++s3) {
-        const int i = s3 * 32 + (int)lane;
-        q3[s3] = make_uint4(0u, 0u, 0u, 0u);
-        if (a.K >= 3 && i < U3)
-            q3[s3] = __ldg(reinterpret_cast<const uint4 *>(a.h2 + (size_t)__ldg(arow + i / Q) * DD) + i % Q);
-    }
-    if (a.asym) {
-        if (a.K >= 2) {
-            // the level-2 lists are the neighbours' rows, D / 4 lanes per row
-            bool f = (int)lane < Q && ((int)q2[0].x == v || (int)q2[0].y == v || (int)q2[0].z == v ||
-                                       (int)q2[0].w == v);
-            if constexpr (D / 4 == 2) f |= __shfl_xor_sync(0xffffffffu, f, 1) != 0;
-            if ((int)lane < Q && (int)lane % (D / 4) == 0 && !f) *a.asym = 1;
-        } else {
-            row_oneway_check(a, v, lane, D);
-        }
-    }
     int n = 0;
-    pk[n++] = lane < (unsigned)D ? classify(x1, 1) : -1;
+    pk[n++] = lane < (unsigned)D ? classify(r.x1, 1) : -1;
 #pragma unroll
     for (int s2 = 0; s2 < (Q + 31) / 32; ++s2) {
         const bool ok = a.K >= 2 && s2 * 32 + (int)lane < Q;
-        pk[n++] = ok ? classify((int32_t)q2[s2].x, 2) : -1;
-        pk[n++] = ok ? classify((int32_t)q2[s2].y, 2) : -1;
-        pk[n++] = ok ? classify((int32_t)q2[s2].z, 2) : -1;
-        pk[n++] = ok ? classify((int32_t)q2[s2].w, 2) : -1;
+        pk[n++] = ok ? classify((int32_t)r.q2[s2].x, 2) : -1;
+        pk[n++] = ok ? classify((int32_t)r.q2[s2].y, 2) : -1;
+        pk[n++] = ok ? classify((int32_t)r.q2[s2].z, 2) : -1;
+        pk[n++] = ok ? classify((int32_t)r.q2[s2].w, 2) : -1;
     }
 #pragma unroll
     for (int s3 = 0; s3 < S3; ++s3) {
         const bool ok = a.K >= 3 && s3 * 32 + (int)lane < U3;
-        pk[n++] = ok ? classify((int32_t)q3[s3].x, 3) : -1;
-        pk[n++] = ok ? classify((int32_t)q3[s3].y, 3) : -1;
-        pk[n++] = ok ? classify((int32_t)q3[s3].z, 3) : -1;
-        pk[n++] = ok ? classify((int32_t)q3[s3].w, 3) : -1;
+        pk[n++] = ok ? classify((int32_t)r.q3[s3].x, 3) : -1;
+        pk[n++] = ok ? classify((int32_t)r.q3[s3].y, 3) : -1;
+        pk[n++] = ok ? classify((int32_t)r.q3[s3].z, 3) : -1;
+        pk[n++] = ok ? classify((int32_t)r.q3[s3].w, 3) : -1;
     }
+}
+
+template <int D>
+__device__ __forceinline__ void row_ends_regs(const WalkIndexArgs &a, const int v, const unsigned lane,
+                                              int (&pk)[RowEnds<D>::NV]) {
+    RowEndsRaw<D> r;
+    row_ends_load<D>(a, v, lane, r);
+    row_ends_classify<D>(a, lane, r, pk);
 }
 
 // One row of the walk index from its ends in registers: counted and placed.
@@ -997,39 +1021,134 @@ __device__ __forceinline__ void index_row_regs(const WalkIndexArgs &a, const int
 }
 
 // Walk pass of every batch at once (4096-source batches, D = 4 or 8, K <= 3): one warp
-// per row enumerates the row's walk ends once (row_ends_regs), then builds the row's
-// level-K visited row of each batch, kWalkAllGroup batches at a time, exactly as
-// walk_rows32 does for one batch (each level's ends ORed into its own shared-memory
-// copy of the row; V_L = V_{L-1} | A_L from the padding and the diagonal up; the
-// level's new pairs popc(V_L) - popc(V_{L-1})), and writes it to vall[b], its
-// level-K frontier flag word to vall_fl[b], and the level counts into counts[b].
-// The levels after the walk then start from vall[b] (BfsArgs::vall).
-constexpr int kWalkAllGroup = 4;
-__host__ __device__ constexpr int walk_all_smem(int K) { return (kIndexBlock / 32) * kWalkAllGroup * K * 512; }
+// per row loads the row's walk ends once (row_ends_load) and writes the row's
+// level-K visited row of every batch to vall[b] (padding, the diagonal and every
+// end of that batch), a flag word to vall_fl[b] and the level counts into counts[b].
+//
+// Tables without one-way entries (*a.oneway == 0, from walk_check_kernel): the count
+// of level L of batch b is the sum over the batch's sources s of n_L(s), the number
+// of vertices at distance exactly L from s (pairs (v, s) at distance L, counted
+// from the source's side).  Row s gives n_L(s): its ends inserted level by level
+// into a per-warp vertex set (s itself first) -- an end is new at its first level.
+// The rows then need no level split (one OR copy a batch, kWalkAllOrGroup batches at
+// a time), and the flag word marks the chunks holding any end: every source first
+// reached at level K has an end of length K there, so these flags contain the
+// level-K frontier's, which is all the visited-set pull levels need of them.
+//
+// Tables with one-way entries: per batch, exactly walk_rows32's construction (each
+// level's ends ORed into their own copy of the row, V_L = V_{L-1} | A_L from the
+// padding and the diagonal up, the level's new pairs popc(V_L) - popc(V_{L-1}), the
+// flag word from the level-K new bits), kWalkAllGroup batches at a time.
+constexpr int kWalkAllGroup = 4;       // batches a warp builds at once with level copies
+constexpr int kWalkAllOrGroup = 8;     // ... with one OR copy a batch and the full vertex set
+constexpr int kWalkAllWide = 16;       // ... when every vertex is a source (small vertex set)
+constexpr int kWalkSetSlots = 1024;    // a warp's vertex set (more than 1 + d + d^2 + d^3 for d <= 8)
+constexpr int kWalkSetSmall = 256;     // ... for levels below K only (more than 1 + d + d^2 for d <= 8)
+__host__ __device__ constexpr int cmax(int x, int y) { return x > y ? x : y; }
+__host__ __device__ constexpr int walk_all_warp_bytes(int K) {
+    return cmax(kWalkAllGroup * K * 512,
+                cmax(kWalkAllOrGroup * 512 + kWalkSetSlots * 4, kWalkAllWide * 512 + kWalkSetSmall * 4));
+}
+__host__ __device__ constexpr int walk_all_smem(int K) { return (kIndexBlock / 32) * walk_all_warp_bytes(K); }
+
+// Inserts w into a warp's open-addressing vertex set of 2^bits slots; 1 when new.
+__device__ __forceinline__ unsigned set_insert(int *T, const int w, const int bits) {
+    const unsigned mask = (1u << bits) - 1u;
+    unsigned h = ((unsigned)w * 2654435761u) >> (32 - bits);
+    for (unsigned probe = 0; probe <= mask; ++probe) {
+        const int old = atomicCAS(T + h, -1, w);
+        if (old == -1) return 1u;
+        if (old == w) return 0u;
+        h = (h + 1u) & mask;
+    }
+    return 0u;   // not reached: the set holds fewer vertices than slots
+}
+
+// One-way check of the whole table (one thread an entry): *oneway = 1 when some
+// entry u of row v has no v in row u.
+static __global__ void walk_check_kernel(const int32_t *adj, const int rows, const int d, int *oneway,
+                                         const int *bad) {
+    if (bad && *bad) return;
+    const long long n = (long long)rows * d;
+    for (long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x; k < n;
+         k += (long long)gridDim.x * blockDim.x) {
+        const int v = (int)(k / d);
+        const int32_t *ur = adj + (size_t)__ldg(adj + k) * d;
+        bool f = false;
+        for (int j = 0; j < d; ++j) f |= __ldg(ur + j) == v;
+        if (!f) *oneway = 1;
+    }
+}
 
 template <int D, int K>
-__global__ void __launch_bounds__(kIndexBlock) walk_all_kernel(const WalkIndexArgs a) {
+__global__ void __launch_bounds__(kIndexBlock, 3) walk_all_kernel(const WalkIndexArgs a) {
     extern __shared__ __align__(16) unsigned char s_walk[];
     __shared__ unsigned long long s_cnt[kIndexMaxKeys];
     if (a.bad && *a.bad) return;
     const unsigned lane = threadIdx.x & 31u, wib = threadIdx.x >> 5;
     const int nb = a.nb, nkeys = nb * K;   // a.K == K
+    // mode 0: one-way entries (level copies); 1: counts from the full vertex set;
+    // 2: every vertex a source -- the set holds levels below K, and n_K(s) is the
+    // popcount of row s's own level-K rows less the padding, s and the lower levels
+    const bool sym = a.oneway != nullptr && ld_acquire_i(a.oneway) == 0;
+    const bool every = a.inv == nullptr && a.src_first == 0 && a.src_begin == 0 && a.ns_total == a.rows;
+    const int mode = !sym ? 0 : (every ? 2 : 1);
+    const int GG = mode == 0 ? kWalkAllGroup : (mode == 1 ? kWalkAllOrGroup : kWalkAllWide);
+    const int set_bits = mode == 2 ? 8 : 10;
     for (int k = (int)threadIdx.x; k < nkeys; k += (int)blockDim.x) s_cnt[k] = 0ull;
     __syncthreads();
-    uint4 *buf4 = reinterpret_cast<uint4 *>(s_walk) + (size_t)wib * kWalkAllGroup * K * 32;
-    uint32_t *buf = reinterpret_cast<uint32_t *>(buf4);
-    constexpr int NV = RowEnds<D>::NV;
+    unsigned char *mine = s_walk + (size_t)wib * walk_all_warp_bytes(K);
+    uint4 *buf4 = reinterpret_cast<uint4 *>(mine);
+    uint32_t *buf = reinterpret_cast<uint32_t *>(mine);
+    int *set = reinterpret_cast<int *>(mine + (mode == 2 ? kWalkAllWide : kWalkAllOrGroup) * 512);
+    constexpr int Q = RowEnds<D>::Q, U3 = RowEnds<D>::U3, S3 = RowEnds<D>::S3, NV = RowEnds<D>::NV;
+    RowEndsRaw<D> r;
     int pk[NV];
     const size_t items = (size_t)a.rows * 32u;
+    const unsigned long long pad_all = (unsigned long long)nb * (unsigned long long)a.S - (unsigned long long)a.ns_total;
     for (int v = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5); v < a.rows;
          v += (int)((gridDim.x * blockDim.x) >> 5)) {
-        row_ends_regs<D>(a, v, lane, pk);
-        // the row's own source: its diagonal bit
+        row_ends_load<D>(a, v, lane, r);
+        // the row's own source: its batch and place (the diagonal bit)
         const int g = a.inv ? __ldg(a.inv + v) : v - a.src_first;
         const int jd = (g >= 0 && (unsigned)(g - a.src_begin) < (unsigned)a.ns_total) ? g - a.src_begin : -1;
-        for (int g0 = 0; g0 < nb; g0 += kWalkAllGroup) {
-            const int G = min(kWalkAllGroup, nb - g0);
-            for (int i = 0; i < G * K; ++i) buf4[i * 32 + lane] = u4zero();
+        const int bd = jd >= 0 ? jd / a.S : -1, jj_d = jd - bd * a.S;
+        unsigned n1 = 0u, n2 = 0u, n3 = 0u;   // vertices first at levels 1..3 (this lane's share)
+        if (mode != 0 && jd >= 0) {
+            // level by level into the vertex set (mode 2: levels below K)
+            const int slots = 1 << set_bits;
+            for (int i = (int)lane; i < slots / 4; i += 32) reinterpret_cast<int4 *>(set)[i] = make_int4(-1, -1, -1, -1);
+            __syncwarp();
+            if (lane == 0) set_insert(set, v, set_bits);
+            __syncwarp();
+            const int top = mode == 2 ? K - 1 : K;
+            if (top >= 1) {
+                n1 = lane < (unsigned)D ? set_insert(set, r.x1, set_bits) : 0u;
+                __syncwarp();
+            }
+            if (top >= 2) {
+#pragma unroll
+                for (int s2 = 0; s2 < (Q + 31) / 32; ++s2)
+                    if (s2 * 32 + (int)lane < Q)
+                        n2 += set_insert(set, (int)r.q2[s2].x, set_bits) + set_insert(set, (int)r.q2[s2].y, set_bits) +
+                              set_insert(set, (int)r.q2[s2].z, set_bits) + set_insert(set, (int)r.q2[s2].w, set_bits);
+                __syncwarp();
+            }
+            if (top >= 3) {
+#pragma unroll
+                for (int s3 = 0; s3 < S3; ++s3)
+                    if (s3 * 32 + (int)lane < U3)
+                        n3 += set_insert(set, (int)r.q3[s3].x, set_bits) + set_insert(set, (int)r.q3[s3].y, set_bits) +
+                              set_insert(set, (int)r.q3[s3].z, set_bits) + set_insert(set, (int)r.q3[s3].w, set_bits);
+                __syncwarp();
+            }
+        }
+        row_ends_classify<D>(a, lane, r, pk);
+        unsigned ball = 0u;   // mode 2: popcount of this lane's chunks of the row's level-K rows
+        for (int g0 = 0; g0 < nb; g0 += GG) {
+            const int G = min(GG, nb - g0);
+            const int copies = mode == 0 ? G * K : G;
+            for (int i = 0; i < copies; ++i) buf4[i * 32 + lane] = u4zero();
             __syncwarp();
 #pragma unroll
             for (int k = 0; k < NV; ++k)
@@ -1037,39 +1156,64 @@ __global__ void __launch_bounds__(kIndexBlock) walk_all_kernel(const WalkIndexAr
                     const int key = pk[k] >> 16, b = key / K;
                     if (b >= g0 && b < g0 + G) {
                         const int jj = pk[k] & 0xffff;
-                        atomicOr(buf + ((b - g0) * K + (key - b * K)) * 128 + (jj >> 5), 1u << (jj & 31));
+                        const int copy = mode == 0 ? (b - g0) * K + (key - b * K) : b - g0;
+                        atomicOr(buf + copy * 128 + (jj >> 5), 1u << (jj & 31));
                     }
                 }
             __syncwarp();
-            for (int bb = 0; bb < G; ++bb) {
+            uint4 *out = a.vall + (size_t)g0 * items + (size_t)v * 32 + lane;
+            for (int bb = 0; bb < G; ++bb, out += items) {
                 const int b = g0 + bb;
                 const int ns = min(a.S, a.ns_total - b * a.S);
-                uint4 vv = pad_mask((int)lane, ns);
-                if (jd >= b * a.S && jd < b * a.S + ns) {
-                    const int j = jd - b * a.S;
-                    if ((unsigned)(j >> 7) == lane) {
-                        const unsigned bit = 1u << (j & 31), comp = ((unsigned)j >> 5) & 3u;
-                        if (comp == 0u) vv.x |= bit; else if (comp == 1u) vv.y |= bit;
-                        else if (comp == 2u) vv.z |= bit; else vv.w |= bit;
-                    }
+                uint4 vv = ns < a.S ? pad_mask((int)lane, ns) : u4zero();
+                if (b == bd && (unsigned)(jj_d >> 7) == lane) {
+                    const unsigned bit = 1u << (jj_d & 31), comp = ((unsigned)jj_d >> 5) & 3u;
+                    if (comp == 0u) vv.x |= bit; else if (comp == 1u) vv.y |= bit;
+                    else if (comp == 2u) vv.z |= bit; else vv.w |= bit;
                 }
-                uint4 prev = vv;
-                unsigned pc = u4popc(vv);
-#pragma unroll
-                for (int L = 0; L < K; ++L) {
-                    const uint4 al = buf4[(bb * K + L) * 32 + lane];
-                    prev = vv;
+                bool flag;
+                if (mode != 0) {
+                    const uint4 al = buf4[bb * 32 + lane];
                     vv = u4or(vv, al);
-                    const unsigned pn = u4popc(vv);
-                    const unsigned t = __reduce_add_sync(0xffffffffu, pn - pc);
-                    if (lane == 0 && t) atomicAdd(s_cnt + b * K + L, (unsigned long long)t);
-                    pc = pn;
+                    flag = u4any(al);
+                    if (mode == 2) ball += u4popc(vv);
+                } else {
+                    uint4 prev = vv;
+                    unsigned pc = u4popc(vv);
+#pragma unroll
+                    for (int L = 0; L < K; ++L) {
+                        const uint4 al = buf4[(bb * K + L) * 32 + lane];
+                        prev = vv;
+                        vv = u4or(vv, al);
+                        const unsigned pn = u4popc(vv);
+                        const unsigned t = __reduce_add_sync(0xffffffffu, pn - pc);
+                        if (lane == 0 && t) atomicAdd(s_cnt + b * K + L, (unsigned long long)t);
+                        pc = pn;
+                    }
+                    flag = u4any(andnot(vv, prev));
                 }
-                a.vall[(size_t)b * items + (size_t)v * 32 + lane] = vv;
-                const unsigned m = __ballot_sync(0xffffffffu, u4any(andnot(vv, prev)));
+                *out = vv;
+                const unsigned m = __ballot_sync(0xffffffffu, flag);
                 if (lane == 0) a.vall_fl[(size_t)b * a.rows + v] = m;
             }
             __syncwarp();
+        }
+        if (mode != 0 && jd >= 0) {
+            n1 = __reduce_add_sync(0xffffffffu, n1);
+            n2 = __reduce_add_sync(0xffffffffu, n2);
+            n3 = __reduce_add_sync(0xffffffffu, n3);
+            if (mode == 2) {
+                // the vertices within K of s, less s and the levels below K
+                const unsigned long long in_ball =
+                    (unsigned long long)__reduce_add_sync(0xffffffffu, ball) - pad_all - 1ull;
+                const unsigned nK = (unsigned)in_ball - n1 - n2;
+                if (K == 1) n1 = nK; else if (K == 2) n2 = nK; else n3 = nK;
+            }
+            if (lane == 0) {
+                atomicAdd(s_cnt + bd * K, (unsigned long long)n1);
+                if (K >= 2) atomicAdd(s_cnt + bd * K + 1, (unsigned long long)n2);
+                if (K >= 3) atomicAdd(s_cnt + bd * K + 2, (unsigned long long)n3);
+            }
         }
     }
     __syncthreads();

@@ -181,3 +181,32 @@ def test_walk_all_batches_at_once(n, d, seed, walk):
     o = O.bfs_pull(adj, np.arange(n))
     assert got[0] == o.total() and got[2] == o.levels
     assert np.array_equal(np.asarray(got[5][:o.levels + 1]), o.level_counts[:o.levels + 1])
+
+
+@pytest.mark.parametrize("lo,hi", [(0, 8192), (4096, 12288), (1000, 9600), (300, 4500)])
+def test_walk_all_source_ranges(lo, hi):
+    """Source sub-ranges (not every vertex a source): walk_all_kernel counts levels
+    1..K from the full vertex set of each source's walk ends; the counts must match
+    the per-batch walk pass and the oracle restricted to the same sources."""
+    n, d = 12288, 8
+    adj = G.random_regular(n, d, 41)
+
+    def run(env):
+        old = {k: os.environ.get(k) for k in env}
+        os.environ.update(env)
+        try:
+            e = engine_with(3, lambda: G.cudaASPLgraph(n, d, 0))
+            engine_with(3, lambda: e.set_batch_sources(4096))
+            r = e.eval(adj, max_levels=n + 1, src_range=(lo, hi), level_counts=True)
+            return r["total"], r["levels"], tuple(int(x) for x in r["level_counts"])
+        finally:
+            for k, v in old.items():
+                if v is None:
+                    del os.environ[k]
+                else:
+                    os.environ[k] = v
+
+    got = run({"GG_VPULL": "1"})
+    assert got == run({"GG_VPULL": "1", "GG_WALK_ALL_MB": "0"})
+    o = O.bfs_pull(adj, np.arange(lo, hi))
+    assert got[0] == o.total() and got[1] == o.levels

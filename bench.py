@@ -19,8 +19,8 @@ calculator with the reference's level cap of 199 (cudaASPLgraph.cu:163).
 * parity     rank 0 compares the timed result with the oracle's BFS from every
              source of the same graph (the cpu_baseline run) and fails on any
              difference; the line says "parity": "exact".
-* roofline   bound "hbm": DRAM bytes one evaluation moves (ncu dram__bytes of the
-             launch, profiles/traffic.json) / the kernel's CUDA-event time,
+* roofline   bound "hbm": DRAM bytes one evaluation moves (ncu dram__bytes of its
+             launches, profiles/traffic.json) / the evaluation's CUDA-event time,
              against MEASURED_PEAKS.json hbm_gbs.  Beside it: "l2_gather", the
              live ceiling of the kernel's access pattern (gg_gather_peak: random
              512-byte row gathers from L2-resident arrays, one dense BFS level per
@@ -325,7 +325,7 @@ def timed(fn, steps, sync):
 
 
 def traffic_of(workload):
-    """DRAM bytes of one evaluation launch from the committed ncu capture, or None."""
+    """DRAM bytes of one evaluation (all its launches) from the committed ncu capture, or None."""
     tp = os.path.join(ROOT, "profiles", "traffic.json")
     if not os.path.exists(tp):
         return None, None
@@ -466,8 +466,8 @@ def run_ours(args):
         traffic = None    # the committed capture is of one whole evaluation on one GPU
     roof = {"bound": "hbm", "achieved": None, "peak": peak, "unit": "GB/s", "frac": None,
             "traffic": traffic, "peak_source": peak_kind, "kernel_ms": kern_ms,
-            "achieved_from": "DRAM bytes of one evaluation launch (traffic, ncu) / the launch's "
-                             "mean CUDA-event time (kernel_ms)",
+            "achieved_from": "DRAM bytes of one evaluation's launches (traffic, ncu) / the "
+                             "evaluation's mean CUDA-event time (kernel_ms)",
             "traffic_source": traffic_note}
     if traffic:
         roof["achieved"] = traffic / (kern_ms / 1000.0) / 1e9
@@ -479,9 +479,10 @@ def run_ours(args):
         lv = eng.eval_device(table_dev.data_ptr(), max_levels=max_levels, stream=sptr, level_ns=True,
                              src_range=src_range)["level_ns"].astype(np.int64)
         level_us = [round((int(lv[i]) - int(lv[i - 1])) / 1000.0, 2) for i in range(1, len(lv)) if lv[i]]
-        # a dense level moves 11 row transfers per row (own word, d = 8 gathers, two writes);
-        # the gather pass moves 10: its time x 1.1 is the dense level's floor at this rate
-        floor_us = 1000.0 * gms * (wl["d"] + 3) / (wl["d"] + 2)
+        # a dense visited-set pull level moves d + 1 row transfers per row (d gathers, one
+        # write: no own row on a table without one-way entries); the gather pass moves
+        # d + 2: its time x (d + 1) / (d + 2) is the dense level's floor at this rate
+        floor_us = 1000.0 * gms * (wl["d"] + 1) / (wl["d"] + 2)
         # the dense levels: past the first (the walk pass, or level 1), within 30 % of the slowest
         rest = level_us[1:]
         dense = [t for t in rest if t >= 0.7 * max(rest)] if rest else []

@@ -659,10 +659,15 @@ gg_status run_eval(gg_engine *e, const int32_t *d_table_in, const gg_eval_opts *
             // blocks add the walk's level counts before any grid barrier
             GG_CK(cudaMemsetAsync(e->d_counts, 0, (size_t)nb * stride * sizeof(unsigned long long), q));
             GG_CK(cudaMemsetAsync(e->d_vtot, 0, (size_t)nb * 3 * sizeof(unsigned long long), q));
+            // the walk of all batches needs the table's one-way flag first; h2_kernel
+            // takes the check along when its warps see whole neighbour rows
+            const long long nh = (long long)e->rows * e->d * e->d;
+            const int qd = e->d / 4;
+            const bool h2_checks = wall && walk_K >= 3 && e->d % 4 == 0 && (qd & (qd - 1)) == 0 && (nh / 4) % 32 == 0;
             if (walk_K >= 3) {
-                const long long nh = (long long)e->rows * e->d * e->d;
                 gg::h2_kernel<<<(int)std::min<long long>((nh + 255) / 256, 8192), 256, 0, q>>>(
-                    e->d_adj, e->d_h2, e->rows, e->d, e->form == FORM_GRAPH ? e->d_bad : nullptr);
+                    e->d_adj, e->d_h2, e->rows, e->d, e->form == FORM_GRAPH ? e->d_bad : nullptr,
+                    h2_checks ? e->d_wasym : nullptr);
                 GG_CK(cudaGetLastError());
             }
             // the walk index of this evaluation's sources and batches
@@ -697,10 +702,12 @@ gg_status run_eval(gg_engine *e, const int32_t *d_table_in, const gg_eval_opts *
                 // how it counts, the level kernel whether dense levels read own chunks
                 wi.asym = nullptr;
                 wi.oneway = e->d_wasym;
-                const long long ne = (long long)e->rows * e->d;
-                gg::walk_check_kernel<<<(int)std::min<long long>((ne + 255) / 256, 8192), 256, 0, q>>>(
-                    e->d_adj, e->rows, e->d, e->d_wasym, e->form == FORM_GRAPH ? e->d_bad : nullptr);
-                GG_CK(cudaGetLastError());
+                if (!h2_checks) {
+                    const long long ne = (long long)e->rows * e->d;
+                    gg::walk_check_kernel<<<(int)std::min<long long>((ne + 255) / 256, 8192), 256, 0, q>>>(
+                        e->d_adj, e->rows, e->d, e->d_wasym, e->form == FORM_GRAPH ? e->d_bad : nullptr);
+                    GG_CK(cudaGetLastError());
+                }
             }
             int sms = 0, per_sm = 0;
             GG_CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, e->device));

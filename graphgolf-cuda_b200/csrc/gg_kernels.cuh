@@ -1453,7 +1453,11 @@ static __device__ __noinline__ void walk_rows(const WalkArgs &w, unsigned char *
 // H2[v][i*d + j] = adj[adj[v][i]][j]: the level-2 walk ends of every row, built once
 // per evaluation (after the table's range check: a bad table builds nothing).
 // When d % 4 == 0 a thread copies 16 bytes (one quarter-row of a neighbour's row).
-static __global__ void h2_kernel(const int32_t *adj, int32_t *h2, int rows, int d, const int *bad) {
+// With `oneway` (d % 4 == 0, d / 4 a power of two, rows * d * d / 4 a multiple of 32,
+// so that every warp iteration is full and a neighbour's row lies within one warp):
+// also the table's one-way check, *oneway = 1 when some row u = adj[v][i] lacks v.
+static __global__ void h2_kernel(const int32_t *adj, int32_t *h2, int rows, int d, const int *bad,
+                                 int *oneway = nullptr) {
     if (bad && *bad) return;
     const long long dd = (long long)d * d;
     if (d % 4 == 0) {
@@ -1463,7 +1467,14 @@ static __global__ void h2_kernel(const int32_t *adj, int32_t *h2, int rows, int 
              k += (long long)gridDim.x * blockDim.x) {
             const long long v = k / ((long long)d * q), r = k % ((long long)d * q);
             const int p = __ldg(adj + v * d + r / q);
-            reinterpret_cast<uint4 *>(h2)[k] = __ldg(reinterpret_cast<const uint4 *>(adj + (size_t)p * d) + r % q);
+            const uint4 w = __ldg(reinterpret_cast<const uint4 *>(adj + (size_t)p * d) + r % q);
+            reinterpret_cast<uint4 *>(h2)[k] = w;
+            if (oneway) {
+                bool hit = (long long)(int)w.x == v || (long long)(int)w.y == v || (long long)(int)w.z == v ||
+                           (long long)(int)w.w == v;
+                for (int o = 1; o < q; o <<= 1) hit |= __shfl_xor_sync(0xffffffffu, hit, o) != 0;
+                if ((threadIdx.x & (unsigned)(q - 1)) == 0u && !hit) *oneway = 1;
+            }
         }
         return;
     }

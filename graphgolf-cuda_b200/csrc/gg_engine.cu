@@ -770,7 +770,7 @@ gg_status run_eval(gg_engine *e, const int32_t *d_table_in, const gg_eval_opts *
         a.vall_fl = wall ? e->d_vall_fl : nullptr;
         void *args[] = {&a};
         GG_CK(cudaLaunchCooperativeKernel(kernel_for(e->d, a.planes != nullptr), dim3(e->grid), dim3(gg::kBlock), args,
-                                          e->smem_bytes, q));
+                                          wall ? (size_t)e->walk_smem_off : e->smem_bytes, q));
         if (timed) GG_CK(cudaEventRecord(e->ev1, q));
         // One copy back: control block, status words, per-batch levels and
         // times, and the counts of every batch (cap_req + 1 each).

@@ -631,12 +631,14 @@ static __device__ __noinline__ unsigned vpull_level(const BfsArgs &a, const int 
 // chunk written, the row's flag and not-full words, and this thread's popcount of what
 // it wrote (the level's total, see BfsArgs::walk_asym).  The same result as
 // vpull_level with no_own, in a loop with nothing else in it: the generic tile function
-// measured 3-4 us slower a level on the 65536-row, 8-regular graph.  (The half-gather
-// levels stay with vpull_level: folding them in here raised the level loop's spills.)
+// measured 3-4 us slower a level on the 65536-row, 8-regular graph.  With `half`, the
+// first D/2 neighbours alone where they already fill the chunk.  Out of line: inlined,
+// it raised the level loop's spills.
 template <int D>
-__device__ __forceinline__ unsigned dense_rows32(const uint4 *X, uint4 *Y, const int32_t *adj, const unsigned v_base,
-                                                 const unsigned t_hi, uint32_t *fn, uint32_t *nfn, unsigned *s_next,
-                                                 const unsigned lane) {
+static __device__ __noinline__ unsigned dense_rows32(const uint4 *X, uint4 *Y, const int32_t *adj,
+                                                     const unsigned v_base, const unsigned t_hi, uint32_t *fn,
+                                                     uint32_t *nfn, const bool half, unsigned *s_next) {
+    const unsigned lane = threadIdx.x & 31u;
     unsigned cnt = 0u;
     for (;;) {
         unsigned v = 0u;
@@ -648,11 +650,28 @@ __device__ __forceinline__ unsigned dense_rows32(const uint4 *X, uint4 *Y, const
 #pragma unroll
         for (int i = 0; i < D; ++i) tu[i] = (unsigned)row[i] * 32u + lane;
         uint4 x[D];
+        uint4 q;
+        if (D >= 8 && half) {
+            // the first half alone where it already fills the chunk
+            constexpr int H = D / 2;
 #pragma unroll
-        for (int i = 0; i < D; ++i) x[i] = __ldcg(X + tu[i]);
-        uint4 q = x[0];
+            for (int i = 0; i < H; ++i) x[i] = __ldcg(X + tu[i]);
+            q = x[0];
 #pragma unroll
-        for (int i = 1; i < D; ++i) or_into(q, x[i]);
+            for (int i = 1; i < H; ++i) or_into(q, x[i]);
+            if (!u4full(q)) {
+#pragma unroll
+                for (int i = H; i < D; ++i) x[i] = __ldcg(X + tu[i]);
+#pragma unroll
+                for (int i = H; i < D; ++i) or_into(q, x[i]);
+            }
+        } else {
+#pragma unroll
+            for (int i = 0; i < D; ++i) x[i] = __ldcg(X + tu[i]);
+            q = x[0];
+#pragma unroll
+            for (int i = 1; i < D; ++i) or_into(q, x[i]);
+        }
         Y[(size_t)v * 32 + lane] = q;
         cnt += u4popc(q);
         const unsigned fb = __ballot_sync(0xffffffffu, u4any(q));
@@ -1928,10 +1947,10 @@ __global__ void __launch_bounds__(kBlock, min_blocks_for(D)) bfs_batch_kernel(co
                 const bool x_is_p = ((L - 1 - a.walk_K) & 1) == 0;
                 if (threadIdx.x == 0) s_next = t_lo;
                 __syncthreads();
-                if (D > 0 && no_own && !nf_use && !split && a.nC == 32)
+                if (D > 0 && no_own && !nf_use && a.nC == 32)
                     cnt = dense_rows32<(D > 0 ? D : 1)>(x_is_p ? S.Pv : S.Qv, x_is_p ? S.Qv : S.Pv, adj, v_base,
-                                                        t_hi, odd ? a.fl1 : a.fl0, odd ? a.nf2 : a.nf, &s_next,
-                                                        lane);
+                                                        t_hi, odd ? a.fl1 : a.fl0, odd ? a.nf2 : a.nf, split,
+                                                        &s_next);
                 else
                     cnt = vpull_level<D>(a, d, adj, v_base, t_hi, x_is_p ? S.Pv : S.Qv, x_is_p ? S.Qv : S.Pv,
                                          L == a.walk_K + 1 ? S.fl_walk : (odd ? a.fl0 : a.fl1), odd ? a.fl1 : a.fl0,

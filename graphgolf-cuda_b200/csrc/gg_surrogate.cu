@@ -4,11 +4,9 @@
 // memory and multiplies with mma.sync m16n8k16 (bf16 in, fp32 accumulate), on
 // 64x64 output tiles of 128 threads.  The forward pass (graph embedding and swap
 // readout) is one cooperative launch (surrogate_forward_kernel) with a bounded
-// grid barrier per message-passing layer.  The backward pass uses a strided tile
-// GEMM (gemm_bf16_kernel; operands read from fp32 memory through arbitrary
-// strides, so transposes cost nothing; long reductions -- weight gradients over
-// the vertices or swaps -- split K over blocks with fp32 atomics), scatters,
-// elementwise epilogues and Adam.
+// grid barrier per message-passing layer; the backward pass with the Adam step is
+// another (surrogate_backward_kernel: weight gradients add each tile's partial
+// product with fp32 atomics, scatters and elementwise steps in fp32).
 #include "gg.h"
 #include "gg_kernels.cuh"
 
@@ -30,21 +28,6 @@ constexpr int kH = 64;           // hidden width
 constexpr int kZ = 3 * kH;       // swap readout width
 constexpr int kLayers = 3;       // message-passing layers
 
-// ---------------------------------------------------------------------------
-// bf16 tile GEMM:  C(m, n) (=|+=) sum_k A(m, k) * B(k, n)
-// A(m, k) = A[m*sam + k*sak], B(k, n) = B[k*sbk + n*sbn], C(m, n) = C[m*scm + n*scn]
-// ---------------------------------------------------------------------------
-struct GemmArgs {
-    const float *A;
-    long long sam, sak;
-    const float *B;
-    long long sbk, sbn;
-    float *C;
-    long long scm, scn;
-    int M, N, K, kchunk;
-    int atomic;   // 0: C = result; 1: C += result (atomicAdd; used with split K)
-};
-
 __device__ __forceinline__ uint16_t bf16_bits(float x) {
     __nv_bfloat16 h = __float2bfloat16_rn(x);
     return *reinterpret_cast<uint16_t *>(&h);
@@ -58,80 +41,9 @@ __device__ __forceinline__ void mma_bf16(float c[4], const uint32_t a[4], const 
         : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b[0]), "r"(b[1]));
 }
 
-__global__ void __launch_bounds__(128) gemm_bf16_kernel(const GemmArgs g) {
-    // row stride 24 bf16 (48 B): the fragment loads of a warp hit 32 distinct banks
-    __shared__ __align__(16) uint16_t As[64][24];
-    __shared__ __align__(16) uint16_t Bt[64][24];   // B transposed: Bt[n][k]
-    const int m0 = blockIdx.x * 64, n0 = blockIdx.y * 64;
-    const int k_begin = blockIdx.z * g.kchunk;
-    const int k_end = min(g.K, k_begin + g.kchunk);
-    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31, gid = lane >> 2, tg = lane & 3;
-    float acc[8][4];
-#pragma unroll
-    for (int j = 0; j < 8; ++j) acc[j][0] = acc[j][1] = acc[j][2] = acc[j][3] = 0.f;
-
-    // consecutive threads walk whichever operand axis is contiguous in memory
-    const bool a_m_fast = g.sam == 1, b_n_fast = g.sbn == 1;
-    for (int k0 = k_begin; k0 < k_end; k0 += 16) {
-        for (int e = tid; e < 64 * 16; e += 128) {
-            const int r = a_m_fast ? (e & 63) : (e >> 4), k = a_m_fast ? (e >> 6) : (e & 15);
-            const int m = m0 + r, kk = k0 + k;
-            const float x = (m < g.M && kk < k_end) ? g.A[m * g.sam + kk * g.sak] : 0.f;
-            As[r][k] = bf16_bits(x);
-        }
-        for (int e = tid; e < 64 * 16; e += 128) {
-            const int n = b_n_fast ? (e & 63) : (e >> 4), k = b_n_fast ? (e >> 6) : (e & 15);
-            const int nn = n0 + n, kk = k0 + k;
-            const float x = (nn < g.N && kk < k_end) ? g.B[kk * g.sbk + nn * g.sbn] : 0.f;
-            Bt[n][k] = bf16_bits(x);
-        }
-        __syncthreads();
-        const int r = warp * 16;
-        uint32_t a[4];
-        a[0] = *reinterpret_cast<const uint32_t *>(&As[r + gid][2 * tg]);
-        a[1] = *reinterpret_cast<const uint32_t *>(&As[r + gid + 8][2 * tg]);
-        a[2] = *reinterpret_cast<const uint32_t *>(&As[r + gid][2 * tg + 8]);
-        a[3] = *reinterpret_cast<const uint32_t *>(&As[r + gid + 8][2 * tg + 8]);
-#pragma unroll
-        for (int j = 0; j < 8; ++j) {
-            uint32_t b[2];
-            b[0] = *reinterpret_cast<const uint32_t *>(&Bt[8 * j + gid][2 * tg]);
-            b[1] = *reinterpret_cast<const uint32_t *>(&Bt[8 * j + gid][2 * tg + 8]);
-            mma_bf16(acc[j], a, b);
-        }
-        __syncthreads();
-    }
-#pragma unroll
-    for (int j = 0; j < 8; ++j) {
-        const int c = n0 + 8 * j + 2 * tg;
-#pragma unroll
-        for (int h = 0; h < 4; ++h) {
-            const int m = m0 + warp * 16 + gid + ((h >> 1) << 3);
-            const int n = c + (h & 1);
-            if (m < g.M && n < g.N) {
-                float *p = g.C + m * g.scm + n * g.scn;
-                if (g.atomic) atomicAdd(p, acc[j][h]);
-                else *p = acc[j][h];
-            }
-        }
-    }
-}
-
 // ---------------------------------------------------------------------------
-// graph and readout kernels
+// swap readout helpers
 // ---------------------------------------------------------------------------
-
-// out[v] (=|+=) (1/d) sum_i H[adj[v][i]]   (rows of kH floats)
-__global__ void nbr_mean_kernel(const float *H, const int32_t *adj, int n, int d, float *out, int add) {
-    const float inv = 1.f / (float)d;
-    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < (long long)n * kH;
-         t += (long long)gridDim.x * blockDim.x) {
-        const int v = (int)(t / kH), j = (int)(t % kH);
-        float s = 0.f;
-        for (int i = 0; i < d; ++i) s += H[(size_t)adj[(size_t)v * d + i] * kH + j];
-        out[t] = add ? out[t] + s * inv : s * inv;
-    }
-}
 
 __device__ __forceinline__ void partners(const gg_swap &s, int &p, int &q) {
     p = s.mode ? s.d : s.c;  // new edges (a,p), (b,q)
@@ -142,84 +54,6 @@ __device__ __forceinline__ void partners(const gg_swap &s, int &p, int &q) {
 // unmasked swaps, [1] learning rate, [2] 1 - beta1^t, [3] 1 - beta2^t.
 enum { kHypInvCnt = 0, kHypLr = 1, kHypC1 = 2, kHypC2 = 3, kHypN = 4 };
 
-// dy = mask * 2 (y - t) / cnt ; loss += mask * (y - t)^2 / cnt
-__global__ void mse_kernel(const float *y, const float *t, const int32_t *mask, int P, const float *hyper,
-                           float *dy, float *loss) {
-    const float inv_cnt = hyper[kHypInvCnt];
-    for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < P; p += gridDim.x * blockDim.x) {
-        const float m = mask[p] ? 1.f : 0.f;
-        const float e = (y[p] - t[p]) * m;
-        dy[p] = 2.f * e * inv_cnt;
-        atomicAdd(loss, e * e * inv_cnt);
-    }
-}
-
-// dO[p][j] = dy[p] * w[j] * (O[p][j] > 0);  dw[j] += dy[p] O[p][j];  db0 += dy[p]
-__global__ void readout_out_back_kernel(const float *O, const float *w, const float *dy, int P, float *dO,
-                                        float *dw, float *db0) {
-    const int j = threadIdx.x;  // blockDim.x == kH
-    float gw = 0.f, gb = 0.f;
-    for (int p = blockIdx.x; p < P; p += gridDim.x) {
-        const float o = O[(size_t)p * kH + j];
-        dO[(size_t)p * kH + j] = o > 0.f ? dy[p] * w[j] : 0.f;
-        gw += dy[p] * o;
-        if (j == 0) gb += dy[p];
-    }
-    atomicAdd(dw + j, gw);
-    if (j == 0) atomicAdd(db0, gb);
-}
-
-// db[j] += sum_rows D[r][j]
-__global__ void colsum_kernel(const float *D, long long rows, float *db) {
-    const int j = threadIdx.x;  // blockDim.x == kH
-    float s = 0.f;
-    for (long long r = blockIdx.x; r < rows; r += gridDim.x) s += D[r * kH + j];
-    atomicAdd(db + j, s);
-}
-
-// D = D * (Y > 0)
-__global__ void relu_back_kernel(float *D, const float *Y, long long count) {
-    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < count;
-         t += (long long)gridDim.x * blockDim.x)
-        if (!(Y[t] > 0.f)) D[t] = 0.f;
-}
-
-// dH[a],dH[b],dH[c],dH[d] += d(Z[p]) / d(H rows)
-__global__ void readout_scatter_kernel(const float *H, const gg_swap *sw, const float *dZ, int P, float *dH) {
-    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < P * kH; t += gridDim.x * blockDim.x) {
-        const int p = t / kH, j = t % kH;
-        const gg_swap s = sw[p];
-        int pa, qb;
-        partners(s, pa, qb);
-        const float g0 = dZ[(size_t)p * kZ + j], g1 = dZ[(size_t)p * kZ + kH + j],
-                    g2 = dZ[(size_t)p * kZ + 2 * kH + j];
-        const float ha = H[(size_t)s.a * kH + j], hb = H[(size_t)s.b * kH + j];
-        const float hc = H[(size_t)s.c * kH + j], hd = H[(size_t)s.d * kH + j];
-        const float hp = H[(size_t)pa * kH + j], hq = H[(size_t)qb * kH + j];
-        atomicAdd(dH + (size_t)s.a * kH + j, g0 + g1 * hb + g2 * hp);
-        atomicAdd(dH + (size_t)s.b * kH + j, g0 + g1 * ha + g2 * hq);
-        atomicAdd(dH + (size_t)s.c * kH + j, g0 + g1 * hd);
-        atomicAdd(dH + (size_t)s.d * kH + j, g0 + g1 * hc);
-        atomicAdd(dH + (size_t)pa * kH + j, g2 * ha);
-        atomicAdd(dH + (size_t)qb * kH + j, g2 * hb);
-    }
-}
-
-__global__ void adam_kernel(float *p, const float *g, float *m, float *v, int count, const float *hyper,
-                            float b1, float b2, float eps) {
-    const float lr = hyper[kHypLr], c1 = hyper[kHypC1], c2 = hyper[kHypC2];
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x) {
-        const float gi = g[i];
-        const float mi = b1 * m[i] + (1.f - b1) * gi;
-        const float vi = b2 * v[i] + (1.f - b2) * gi * gi;
-        m[i] = mi;
-        v[i] = vi;
-        p[i] -= lr * (mi / c1) / (sqrtf(vi / c2) + eps);
-    }
-}
-
-int blocks_for(long long n, int per = 256) { return (int)std::min<long long>((n + per - 1) / per, 4096); }
-
 // ---------------------------------------------------------------------------
 // Fused forward: the graph embedding (H0 .. H3, with the neighbour means M0 .. M2
 // kept for the backward pass) and the readout of P swaps (Z, O, y) in one
@@ -228,7 +62,7 @@ int blocks_for(long long n, int per = 256) { return (int)std::min<long long>((n 
 // A block owns 64-row tiles (vertices, then swaps).  For each tile it stages both
 // operands as bf16 in shared memory -- A (64 x K) row-major, B transposed (64 x K)
 // -- and multiplies with mma.sync m16n8k16 (fp32 accumulate), the arithmetic of
-// gemm_bf16_kernel; a layer's two products H Ws + M Wn run as one K = 128 product
+// every surrogate product; a layer's two products H Ws + M Wn run as one K = 128 product
 // over [H | M] and [Ws ; Wn].
 // ---------------------------------------------------------------------------
 constexpr int kFwdBlock = 128;
@@ -404,6 +238,268 @@ __global__ void __launch_bounds__(kFwdBlock) surrogate_forward_kernel(const FwdA
     }
 }
 
+// ---------------------------------------------------------------------------
+// Fused backward (and Adam): the gradient of the masked MSE of P swap predictions with
+// respect to every parameter, in one cooperative launch of 128-thread blocks with a
+// bounded grid barrier between dependent stages:
+//   1. swap tiles: dy, dO = dy w_r2 (O > 0), dZ = dO Wr1^T, dWr1 += Z^T dO, the output
+//      biases and weights, and dZ scattered into dH3 (fp32 atomics);
+//   2. per layer l = 2, 1, 0, vertex tiles: dPre = dH (H_{l+1} > 0), db_l, dWs_l += H_l^T
+//      dPre, dWn_l += M_l^T dPre, dH_l = dPre Ws_l^T (rows) and G = dPre Wn_l^T; then,
+//      after a barrier, dH_l += the neighbour mean of G (symmetric adjacency);
+//   3. the input layer: dPre0 = dH (H0 > 0), db_in, dWin += X^T dPre0;
+//   4. with `train`, Adam on every parameter.
+// Products round both operands to bf16 in shared memory and multiply with mma.sync
+// (fp32 accumulate), as the forward does; weight gradients add each tile's partial
+// product with fp32 atomics; elementwise steps stay in fp32.  Data other blocks wrote
+// earlier in the launch is read through the L2 (__ldcg).
+// ---------------------------------------------------------------------------
+struct BwdArgs {
+    const float *X;
+    int F;
+    const int32_t *adj;
+    int n, d;
+    const float *P;
+    float *Gd;
+    int o_win, o_bin, o_ws[kLayers], o_wn[kLayers], o_b[kLayers], o_wr1, o_br1, o_wr2, o_br2;
+    const float *H[kLayers + 1];
+    const float *M[kLayers];
+    const gg_swap *sw;
+    int n_sw;
+    const float *Z, *O, *y, *t;
+    const int32_t *mask;
+    const float *hyper;
+    float *dO, *dZ, *dHa, *dHb, *Gt, *loss;
+    float *adam_m, *adam_v;
+    float *params;
+    int n_params, train;
+    gg::Ctl *ctl;
+    unsigned expected;
+    long long wait_ns;
+};
+
+// S[c][r] = bf16(src[(row0 + r) * ld + col0 + c]), c < 64 (columns past ncols: 0),
+// r < 64 (rows past nrows: 0): the transposed tile
+__device__ __forceinline__ void stage_cols(uint16_t *S, const float *src, long long ld, int row0, int nrows,
+                                           int col0, int ncols) {
+#pragma unroll 8
+    for (int e = threadIdx.x; e < 64 * 64; e += kFwdBlock) {
+        const int r = e >> 6, c = e & 63, m = row0 + r;
+        S[c * kFwdLd + r] = bf16_bits(m < nrows && col0 + c < ncols ? src[(size_t)m * ld + col0 + c] : 0.f);
+    }
+}
+
+// S[k][c] = bf16(W[(k0 + k) * ldw + c]), k, c < 64: a weight block, row k of W as row k of S
+__device__ __forceinline__ void stage_wt(uint16_t *S, const float *W, int ldw, int k0) {
+#pragma unroll 8
+    for (int e = threadIdx.x; e < 64 * 64; e += kFwdBlock) {
+        const int k = e >> 6, c = e & 63;
+        S[k * kFwdLd + c] = bf16_bits(W[(size_t)(k0 + k) * ldw + c]);
+    }
+}
+
+// dst[(r0 + m) * ld + c0 + c] (=|+= atomically) acc[m][c], m < mrows, c < ncols
+template <bool ATOMIC>
+__device__ __forceinline__ void tile_out(const float acc[8][4], float *dst, long long ld, int r0, int mrows, int c0,
+                                         int ncols) {
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, gid = lane >> 2, tg = lane & 3;
+#pragma unroll
+    for (int j = 0; j < 8; ++j)
+#pragma unroll
+        for (int h = 0; h < 4; ++h) {
+            const int m = warp * 16 + gid + ((h >> 1) << 3), c = 8 * j + 2 * tg + (h & 1);
+            if (m < mrows && c < ncols) {
+                float *q = dst + (size_t)(r0 + m) * ld + c0 + c;
+                if (ATOMIC) atomicAdd(q, acc[j][h]); else *q = acc[j][h];
+            }
+        }
+}
+
+__global__ void __launch_bounds__(kFwdBlock) surrogate_backward_kernel(const BwdArgs a) {
+    extern __shared__ __align__(16) uint16_t bsm[];
+    uint16_t *As = bsm;                    // [64][kFwdLd]
+    uint16_t *Bt = bsm + 64 * kFwdLd;      // [64][kFwdLd]
+    const int tid = threadIdx.x, jc = tid & 63;   // elementwise loops: this thread's column
+    unsigned epoch = 0;
+    float acc[8][4];
+    const float *Pm = a.P;
+    float *Gd = a.Gd;
+    // 1. swap tiles
+    {
+        const float inv_cnt = a.hyper[kHypInvCnt];
+        float g_wr2 = 0.f, g_br1 = 0.f, g_br2 = 0.f;
+        const float *H3 = a.H[kLayers];
+        const int ntb = (a.n_sw + 63) / 64;
+        for (int tb = blockIdx.x; tb < ntb; tb += gridDim.x) {
+            const int p0 = tb * 64, prow = min(64, a.n_sw - p0);
+#pragma unroll 8
+            for (int e = tid; e < 64 * kH; e += kFwdBlock) {
+                const int r = e / kH, j = e % kH, p = p0 + r;
+                float v = 0.f;
+                if (p < a.n_sw) {
+                    const float m = a.mask[p] ? 1.f : 0.f;
+                    const float err = (a.y[p] - a.t[p]) * m;
+                    const float dyp = 2.f * err * inv_cnt;
+                    const float o = a.O[(size_t)p * kH + j];
+                    v = o > 0.f ? dyp * Pm[a.o_wr2 + j] : 0.f;
+                    a.dO[(size_t)p * kH + j] = v;
+                    g_wr2 += dyp * o;
+                    g_br1 += v;
+                    if (j == 0) {
+                        g_br2 += dyp;
+                        atomicAdd(a.loss, err * err * inv_cnt);
+                    }
+                }
+                As[r * kFwdLd + j] = bf16_bits(v);
+            }
+            __syncthreads();
+            // dZ = dO Wr1^T, 64 columns of Z at a time
+            for (int zc = 0; zc < kZ / 64; ++zc) {
+                stage_wt(Bt, Pm + a.o_wr1, kH, zc * 64);   // Bt[z][j] = Wr1[zc * 64 + z][j]
+                __syncthreads();
+                tile_mma(As, Bt, kH, acc);
+                tile_out<false>(acc, a.dZ, kZ, p0, prow, zc * 64, 64);
+                __syncthreads();
+            }
+            // dWr1 += Z^T dO
+            stage_cols(Bt, a.dO, kH, p0, a.n_sw, 0, kH);   // Bt[j][r] = dO[p0 + r][j]
+            for (int zc = 0; zc < kZ / 64; ++zc) {
+                stage_cols(As, a.Z, kZ, p0, a.n_sw, zc * 64, kZ);   // As[z][r] = Z[p0 + r][zc * 64 + z]
+                __syncthreads();
+                tile_mma(As, Bt, 64, acc);
+                tile_out<true>(acc, Gd + a.o_wr1, kH, zc * 64, 64, 0, kH);
+                __syncthreads();
+            }
+            // dZ of this tile's swaps into dH3 (the readout's products, fp32 atomics)
+#pragma unroll 8
+            for (int e = tid; e < 64 * kH; e += kFwdBlock) {
+                const int r = e / kH, j = e % kH, p = p0 + r;
+                if (p >= a.n_sw) continue;
+                const gg_swap w = a.sw[p];
+                int pa, qb;
+                partners(w, pa, qb);
+                const float g0 = a.dZ[(size_t)p * kZ + j], g1 = a.dZ[(size_t)p * kZ + kH + j],
+                            g2 = a.dZ[(size_t)p * kZ + 2 * kH + j];
+                const float ha = H3[(size_t)w.a * kH + j], hb = H3[(size_t)w.b * kH + j];
+                const float hc = H3[(size_t)w.c * kH + j], hd = H3[(size_t)w.d * kH + j];
+                const float hp = H3[(size_t)pa * kH + j], hq = H3[(size_t)qb * kH + j];
+                atomicAdd(a.dHa + (size_t)w.a * kH + j, g0 + g1 * hb + g2 * hp);
+                atomicAdd(a.dHa + (size_t)w.b * kH + j, g0 + g1 * ha + g2 * hq);
+                atomicAdd(a.dHa + (size_t)w.c * kH + j, g0 + g1 * hd);
+                atomicAdd(a.dHa + (size_t)w.d * kH + j, g0 + g1 * hc);
+                atomicAdd(a.dHa + (size_t)pa * kH + j, g2 * ha);
+                atomicAdd(a.dHa + (size_t)qb * kH + j, g2 * hb);
+            }
+            __syncthreads();
+        }
+        atomicAdd(Gd + a.o_wr2 + jc, g_wr2);
+        atomicAdd(Gd + a.o_br1 + jc, g_br1);
+        if (jc == 0) atomicAdd(Gd + a.o_br2, g_br2);
+    }
+    // 2. layers 2, 1, 0 (dH holds dL/dH_{l+1}; dHn receives dL/dH_l)
+    float *dH = a.dHa, *dHn = a.dHb;
+    const int nrb = (a.n + 63) / 64;
+    const long long gtid = (long long)blockIdx.x * blockDim.x + tid, nthr = (long long)gridDim.x * blockDim.x;
+    for (int l = kLayers - 1; l >= 0; --l) {
+        if (!gg::grid_sync(a.ctl, a.expected, a.wait_ns, 2 * (kLayers - 1 - l) + 1, epoch)) return;
+        float g_b = 0.f;
+        for (int rb = blockIdx.x; rb < nrb; rb += gridDim.x) {
+            const int v0 = rb * 64, vrows = min(64, a.n - v0);
+            // dPre = dH (H_{l+1} > 0), in place; As = dPre rows
+#pragma unroll 8
+            for (int e = tid; e < 64 * kH; e += kFwdBlock) {
+                const int r = e / kH, c = e % kH, v = v0 + r;
+                float q = 0.f;
+                if (v < a.n) {
+                    q = a.H[l + 1][(size_t)v * kH + c] > 0.f ? __ldcg(dH + (size_t)v * kH + c) : 0.f;
+                    dH[(size_t)v * kH + c] = q;
+                }
+                g_b += q;
+                As[r * kFwdLd + c] = bf16_bits(q);
+            }
+            __syncthreads();
+            // dH_l rows = dPre Ws^T, G = dPre Wn^T
+            stage_wt(Bt, Pm + a.o_ws[l], kH, 0);   // Bt[k][c] = Ws[k][c]
+            __syncthreads();
+            tile_mma(As, Bt, kH, acc);
+            tile_out<false>(acc, dHn, kH, v0, vrows, 0, kH);
+            __syncthreads();
+            stage_wt(Bt, Pm + a.o_wn[l], kH, 0);
+            __syncthreads();
+            tile_mma(As, Bt, kH, acc);
+            tile_out<false>(acc, a.Gt, kH, v0, vrows, 0, kH);
+            __syncthreads();
+            // dWs_l += H_l^T dPre, dWn_l += M_l^T dPre
+            stage_cols(Bt, dH, kH, v0, a.n, 0, kH);       // Bt[c][r] = dPre[v0 + r][c]
+            stage_cols(As, a.H[l], kH, v0, a.n, 0, kH);   // As[k][r] = H_l[v0 + r][k]
+            __syncthreads();
+            tile_mma(As, Bt, 64, acc);
+            tile_out<true>(acc, Gd + a.o_ws[l], kH, 0, 64, 0, kH);
+            __syncthreads();
+            stage_cols(As, a.M[l], kH, v0, a.n, 0, kH);
+            __syncthreads();
+            tile_mma(As, Bt, 64, acc);
+            tile_out<true>(acc, Gd + a.o_wn[l], kH, 0, 64, 0, kH);
+            __syncthreads();
+        }
+        atomicAdd(Gd + a.o_b[l] + jc, g_b);
+        if (!gg::grid_sync(a.ctl, a.expected, a.wait_ns, 2 * (kLayers - 1 - l) + 2, epoch)) return;
+        // dH_l += the neighbour mean of G (a symmetric adjacency: the transpose of the mean)
+        const float inv = 1.f / (float)a.d;
+#pragma unroll 4
+        for (long long t = gtid; t < (long long)a.n * kH; t += nthr) {
+            const int v = (int)(t / kH), j = (int)(t % kH);
+            float sum = 0.f;
+            for (int i = 0; i < a.d; ++i) sum += __ldcg(a.Gt + (size_t)__ldg(a.adj + (size_t)v * a.d + i) * kH + j);
+            dHn[t] = __ldcg(dHn + t) + sum * inv;
+        }
+        float *tmp = dH;
+        dH = dHn;
+        dHn = tmp;
+    }
+    // 3. the input layer: dPre0 = dH (H0 > 0), db_in, dWin += X^T dPre0
+    if (!gg::grid_sync(a.ctl, a.expected, a.wait_ns, 2 * kLayers + 1, epoch)) return;
+    {
+        float g_b = 0.f;
+        for (int rb = blockIdx.x; rb < nrb; rb += gridDim.x) {
+            const int v0 = rb * 64;
+#pragma unroll 8
+            for (int e = tid; e < 64 * kH; e += kFwdBlock) {
+                const int r = e / kH, c = e % kH, v = v0 + r;
+                if (v < a.n) {
+                    const float q = a.H[0][(size_t)v * kH + c] > 0.f ? __ldcg(dH + (size_t)v * kH + c) : 0.f;
+                    dH[(size_t)v * kH + c] = q;
+                    g_b += q;
+                }
+            }
+            __syncthreads();
+            stage_cols(Bt, dH, kH, v0, a.n, 0, kH);   // Bt[c][r] = dPre0[v0 + r][c]
+            for (int f0 = 0; f0 < a.F; f0 += 64) {
+                stage_cols(As, a.X, a.F, v0, a.n, f0, a.F);   // As[f][r] = X[v0 + r][f0 + f]
+                __syncthreads();
+                tile_mma(As, Bt, 64, acc);
+                tile_out<true>(acc, Gd + a.o_win, kH, f0, min(64, a.F - f0), 0, kH);
+                __syncthreads();
+            }
+        }
+        atomicAdd(Gd + a.o_bin + jc, g_b);
+    }
+    // 4. Adam on every parameter
+    if (a.train) {
+        if (!gg::grid_sync(a.ctl, a.expected, a.wait_ns, 2 * kLayers + 2, epoch)) return;
+        const float lr = a.hyper[kHypLr], c1 = a.hyper[kHypC1], c2 = a.hyper[kHypC2];
+        for (long long i = gtid; i < a.n_params; i += nthr) {
+            const float gi = __ldcg(Gd + i);
+            const float b1 = 0.9f, b2 = 0.999f;
+            const float mi = b1 * a.adam_m[i] + (1.f - b1) * gi;
+            const float vi = b2 * a.adam_v[i] + (1.f - b2) * gi * gi;
+            a.adam_m[i] = mi;
+            a.adam_v[i] = vi;
+            a.params[i] -= lr * (mi / c1) / (sqrtf(vi / c2) + 1e-8f);
+        }
+    }
+}
+
 }  // namespace
 
 // ---------------------------------------------------------------------------
@@ -424,14 +520,14 @@ struct gg_surrogate {
     // per-swap device buffers and their pinned host staging (capacity `cap`)
     int cap = 0;
     gg_swap *sw = nullptr, *h_sw = nullptr;
-    float *Z = nullptr, *O = nullptr, *y = nullptr, *t = nullptr, *dy = nullptr, *dO = nullptr, *dZ = nullptr;
+    float *Z = nullptr, *O = nullptr, *y = nullptr, *t = nullptr, *dO = nullptr, *dZ = nullptr;
     float *h_y = nullptr, *h_t = nullptr;
     int32_t *mask = nullptr, *h_mask = nullptr;
     float *loss = nullptr, *h_loss = nullptr;
     float *hyper = nullptr, *h_hyper = nullptr;
     gg::Ctl *ctl = nullptr;                // grid barrier of the fused forward launch
     int *h_err = nullptr;                  // its wait status, copied back after each call
-    int fwd_per_sm = 0, sms = 0;
+    int fwd_per_sm = 0, bwd_per_sm = 0, sms = 0;
     bool fwd_valid = false, graph_set = false;
     long long adam_step = 0;
     // captured launch sequences, per swap count: predict (with the graph
@@ -456,20 +552,6 @@ gg_status sfail(gg_status s, const std::string &m) {
                          std::string(#call) + ": " + cudaGetErrorString(e_));                \
     } while (0)
 
-void gemm(cudaStream_t st, int M, int N, int K, const float *A, long long sam, long long sak, const float *B,
-          long long sbk, long long sbn, float *C, long long scm, long long scn, bool atomic, int splitk = 1) {
-    GemmArgs g{A, sam, sak, B, sbk, sbn, C, scm, scn, M, N, K, 0, atomic ? 1 : 0};
-    int kc = (K + splitk - 1) / splitk;
-    kc = std::max(16, (kc + 15) / 16 * 16);
-    g.kchunk = kc;
-    dim3 grid((M + 63) / 64, (N + 63) / 64, (K + kc - 1) / kc);
-    if (grid.z > 1) g.atomic = 1;
-    gemm_bf16_kernel<<<grid, 128, 0, st>>>(g);
-}
-
-// K split so that each block runs about four k-steps of 16 (the weight
-// gradients reduce over all vertices or swaps and have only one 64x64 tile).
-int split_for(long long K) { return (int)std::max<long long>(1, std::min<long long>(K / 64, 128)); }
 
 void drop_graphs(gg_surrogate *s) {
     for (auto &c : s->graphs) cudaGraphExecDestroy(c.exec);
@@ -481,7 +563,7 @@ gg_status ensure_swaps(gg_surrogate *s, int P) {
     const int cap = std::max(P, 2 * s->cap);
     drop_graphs(s);
     cudaFree(s->sw); cudaFree(s->Z); cudaFree(s->O); cudaFree(s->y); cudaFree(s->t);
-    cudaFree(s->dy); cudaFree(s->dO); cudaFree(s->dZ); cudaFree(s->mask);
+    cudaFree(s->dO); cudaFree(s->dZ); cudaFree(s->mask);
     cudaFreeHost(s->h_sw); cudaFreeHost(s->h_y); cudaFreeHost(s->h_t); cudaFreeHost(s->h_mask);
     s->cap = 0;
     GS_CK(cudaMalloc(&s->sw, (size_t)cap * sizeof(gg_swap)));
@@ -489,7 +571,6 @@ gg_status ensure_swaps(gg_surrogate *s, int P) {
     GS_CK(cudaMalloc(&s->O, (size_t)cap * kH * 4));
     GS_CK(cudaMalloc(&s->y, (size_t)cap * 4));
     GS_CK(cudaMalloc(&s->t, (size_t)cap * 4));
-    GS_CK(cudaMalloc(&s->dy, (size_t)cap * 4));
     GS_CK(cudaMalloc(&s->dO, (size_t)cap * kH * 4));
     GS_CK(cudaMalloc(&s->dZ, (size_t)cap * kZ * 4));
     GS_CK(cudaMalloc(&s->mask, (size_t)cap * 4));
@@ -533,37 +614,36 @@ void forward_graph(gg_surrogate *s) { forward_fused(s, true, 0); }
 // Readout of the P swaps in s->sw: Z, O, y.
 void forward_readout(gg_surrogate *s, int P) { forward_fused(s, false, P); }
 
-// Loss and full gradient into s->grad (zeroed here) for the swaps/targets/mask on the device.
-void backward(gg_surrogate *s, int P) {
-    const int n = s->n;
-    float *Pm = s->params, *Gd = s->grad;
-    cudaMemsetAsync(Gd, 0, (size_t)s->n_params * 4, s->st);
+// Loss and full gradient into s->grad (zeroed here) for the swaps/targets/mask on the
+// device, and with `train` the Adam step: one fused launch (surrogate_backward_kernel).
+// Its barrier status goes to s->h_err[1].
+void backward(gg_surrogate *s, int P, bool train) {
+    cudaMemsetAsync(s->grad, 0, (size_t)s->n_params * 4, s->st);
     cudaMemsetAsync(s->loss, 0, 4, s->st);
-    mse_kernel<<<blocks_for(P), 256, 0, s->st>>>(s->y, s->t, s->mask, P, s->hyper, s->dy, s->loss);
-    readout_out_back_kernel<<<std::min(P, 256), kH, 0, s->st>>>(s->O, Pm + s->o_wr2, s->dy, P, s->dO,
-                                                                Gd + s->o_wr2, Gd + s->o_br2);
-    colsum_kernel<<<std::min(P, 256), kH, 0, s->st>>>(s->dO, P, Gd + s->o_br1);
-    // dWr1 = Z^T dO ; dZ = dO Wr1^T
-    gemm(s->st, kZ, kH, P, s->Z, 1, kZ, s->dO, kH, 1, Gd + s->o_wr1, kH, 1, true, split_for(P));
-    gemm(s->st, P, kZ, kH, s->dO, kH, 1, Pm + s->o_wr1, 1, kH, s->dZ, kZ, 1, false);
-    cudaMemsetAsync(s->dH0, 0, (size_t)n * kH * 4, s->st);
-    readout_scatter_kernel<<<blocks_for((long long)P * kH), 256, 0, s->st>>>(s->Hs[kLayers], s->sw, s->dZ, P, s->dH0);
-    float *dH = s->dH0, *dHp = s->dH1;
-    for (int l = kLayers - 1; l >= 0; --l) {
-        // dH holds dL/dH_{l+1}; make it dL/dpre_{l+1}
-        relu_back_kernel<<<blocks_for((long long)n * kH), 256, 0, s->st>>>(dH, s->Hs[l + 1], (long long)n * kH);
-        colsum_kernel<<<std::min(n, 256), kH, 0, s->st>>>(dH, n, Gd + s->o_b[l]);
-        gemm(s->st, kH, kH, n, s->Hs[l], 1, kH, dH, kH, 1, Gd + s->o_ws[l], kH, 1, true, split_for(n));
-        gemm(s->st, kH, kH, n, s->Ms[l], 1, kH, dH, kH, 1, Gd + s->o_wn[l], kH, 1, true, split_for(n));
-        // dH_l = dPre Ws^T + mean_nbr(dPre Wn^T)   (symmetric adjacency)
-        gemm(s->st, n, kH, kH, dH, kH, 1, Pm + s->o_ws[l], 1, kH, dHp, kH, 1, false);
-        gemm(s->st, n, kH, kH, dH, kH, 1, Pm + s->o_wn[l], 1, kH, s->G, kH, 1, false);
-        nbr_mean_kernel<<<blocks_for((long long)n * kH), 256, 0, s->st>>>(s->G, s->adj, n, s->d, dHp, 1);
-        float *tmp = dH; dH = dHp; dHp = tmp;
-    }
-    relu_back_kernel<<<blocks_for((long long)n * kH), 256, 0, s->st>>>(dH, s->Hs[0], (long long)n * kH);
-    colsum_kernel<<<std::min(n, 256), kH, 0, s->st>>>(dH, n, Gd + s->o_bin);
-    gemm(s->st, s->F, kH, n, s->X, 1, s->F, dH, kH, 1, Gd + s->o_win, kH, 1, true, split_for(n));
+    cudaMemsetAsync(s->dH0, 0, (size_t)s->n * kH * 4, s->st);
+    BwdArgs a{};
+    a.X = s->X; a.F = s->F; a.adj = s->adj; a.n = s->n; a.d = s->d;
+    a.P = s->params; a.Gd = s->grad;
+    a.o_win = s->o_win; a.o_bin = s->o_bin;
+    for (int l = 0; l < kLayers; ++l) { a.o_ws[l] = s->o_ws[l]; a.o_wn[l] = s->o_wn[l]; a.o_b[l] = s->o_b[l]; }
+    a.o_wr1 = s->o_wr1; a.o_br1 = s->o_br1; a.o_wr2 = s->o_wr2; a.o_br2 = s->o_br2;
+    for (int l = 0; l <= kLayers; ++l) a.H[l] = s->Hs[l];
+    for (int l = 0; l < kLayers; ++l) a.M[l] = s->Ms[l];
+    a.sw = s->sw; a.n_sw = P;
+    a.Z = s->Z; a.O = s->O; a.y = s->y; a.t = s->t; a.mask = s->mask; a.hyper = s->hyper;
+    a.dO = s->dO; a.dZ = s->dZ; a.dHa = s->dH0; a.dHb = s->dH1; a.Gt = s->G; a.loss = s->loss;
+    a.adam_m = s->adam_m; a.adam_v = s->adam_v; a.params = s->params;
+    a.n_params = s->n_params; a.train = train ? 1 : 0;
+    // every resident block: the tile stages take one block a 64-row tile, the
+    // neighbour means and Adam use them all
+    const int grid = std::max(1, s->bwd_per_sm * s->sms);
+    a.ctl = s->ctl;
+    a.expected = (unsigned)grid;
+    a.wait_ns = 10ll * 1000 * 1000 * 1000;
+    cudaMemsetAsync(s->ctl, 0, sizeof(gg::Ctl), s->st);
+    void *args[] = {&a};
+    cudaLaunchCooperativeKernel((void *)surrogate_backward_kernel, dim3(grid), dim3(kFwdBlock), args, kFwdSmem, s->st);
+    cudaMemcpyAsync(s->h_err + 1, &s->ctl->err, sizeof(int), cudaMemcpyDeviceToHost, s->st);
 }
 
 enum { kPredict = 0, kGrad = 1, kTrain = 2 };
@@ -580,10 +660,7 @@ void enqueue_kind(gg_surrogate *s, int kind, int P) {
     cudaMemcpyAsync(s->mask, s->h_mask, (size_t)P * 4, cudaMemcpyHostToDevice, s->st);
     cudaMemcpyAsync(s->hyper, s->h_hyper, kHypN * 4, cudaMemcpyHostToDevice, s->st);
     forward_readout(s, P);
-    backward(s, P);
-    if (kind == kTrain)
-        adam_kernel<<<blocks_for(s->n_params), 256, 0, s->st>>>(s->params, s->grad, s->adam_m, s->adam_v,
-                                                               s->n_params, s->hyper, 0.9f, 0.999f, 1e-8f);
+    backward(s, P, kind == kTrain);
     cudaMemcpyAsync(s->h_loss, s->loss, 4, cudaMemcpyDeviceToHost, s->st);
 }
 
@@ -604,7 +681,9 @@ gg_status run_kind(gg_surrogate *s, int kind, int P) {
     }
     GS_CK(cudaGraphLaunch(exec, s->st));
     GS_CK(cudaStreamSynchronize(s->st));
-    if (*s->h_err) return sfail(GG_TIMEOUT, "grid barrier wait of the fused forward exceeded its limit");
+    if (s->h_err[0]) return sfail(GG_TIMEOUT, "grid barrier wait of the fused forward exceeded its limit");
+    if (kind != kPredict && s->h_err[1])
+        return sfail(GG_TIMEOUT, "grid barrier wait of the fused backward exceeded its limit");
     return GG_OK;
 }
 
@@ -713,18 +792,24 @@ gg_status gg_surrogate_create(int device, int n, int degree, int in_features, ui
               cudaMalloc(&s->G, (size_t)n * kH * 4) == cudaSuccess &&
               cudaMalloc(&s->loss, 4) == cudaSuccess && cudaMalloc(&s->hyper, kHypN * 4) == cudaSuccess &&
               cudaMallocHost(&s->h_loss, 4) == cudaSuccess && cudaMallocHost(&s->h_hyper, kHypN * 4) == cudaSuccess &&
-              cudaMalloc(&s->ctl, sizeof(gg::Ctl)) == cudaSuccess && cudaMallocHost(&s->h_err, sizeof(int)) == cudaSuccess;
+              cudaMalloc(&s->ctl, sizeof(gg::Ctl)) == cudaSuccess && cudaMallocHost(&s->h_err, 2 * sizeof(int)) == cudaSuccess;
     for (int l = 0; l <= kLayers && ok; ++l) ok = cudaMalloc(&s->Hs[l], (size_t)n * kH * 4) == cudaSuccess;
     for (int l = 0; l < kLayers && ok; ++l) ok = cudaMalloc(&s->Ms[l], (size_t)n * kH * 4) == cudaSuccess;
     if (!ok) return bad(sfail(GG_OUT_OF_MEMORY, "surrogate allocation failed"));
     std::memset(s->h_hyper, 0, kHypN * 4);
-    *s->h_err = 0;
+    s->h_err[0] = s->h_err[1] = 0;
     if (cudaFuncSetAttribute(surrogate_forward_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kFwdSmem) !=
             cudaSuccess ||
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&s->fwd_per_sm, surrogate_forward_kernel, kFwdBlock, kFwdSmem) !=
             cudaSuccess ||
         cudaDeviceGetAttribute(&s->sms, cudaDevAttrMultiProcessorCount, device) != cudaSuccess || s->fwd_per_sm < 1)
         return bad(sfail(GG_CUDA_ERROR, "fused forward cannot be resident"));
+    if (cudaFuncSetAttribute(surrogate_backward_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kFwdSmem) !=
+            cudaSuccess ||
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&s->bwd_per_sm, surrogate_backward_kernel, kFwdBlock, kFwdSmem) !=
+            cudaSuccess ||
+        s->bwd_per_sm < 1)
+        return bad(sfail(GG_CUDA_ERROR, "fused backward cannot be resident"));
     if (cudaMemcpy(s->params, p.data(), pb, cudaMemcpyHostToDevice) != cudaSuccess ||
         cudaMemset(s->adam_m, 0, pb) != cudaSuccess || cudaMemset(s->adam_v, 0, pb) != cudaSuccess)
         return bad(sfail(GG_CUDA_ERROR, "surrogate initialisation failed"));
@@ -806,7 +891,7 @@ gg_status gg_surrogate_destroy(gg_surrogate *s) {
     for (auto p : s->Hs) cudaFree(p);
     for (auto p : s->Ms) cudaFree(p);
     cudaFree(s->sw); cudaFree(s->Z); cudaFree(s->O); cudaFree(s->y); cudaFree(s->t);
-    cudaFree(s->dy); cudaFree(s->dO); cudaFree(s->dZ); cudaFree(s->mask);
+    cudaFree(s->dO); cudaFree(s->dZ); cudaFree(s->mask);
     cudaFreeHost(s->h_sw); cudaFreeHost(s->h_y); cudaFreeHost(s->h_t); cudaFreeHost(s->h_mask);
     if (s->st) cudaStreamDestroy(s->st);
     delete s;

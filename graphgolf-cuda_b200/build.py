@@ -54,8 +54,8 @@ def build_engine(force=False, extra=()):
     deps.append(os.path.join(INC, "gg.h"))
     if not force and not _stale(ENGINE_LIB, deps):
         return ENGINE_LIB
-    cmd = [nvcc(), "-O3", "-std=c++17", *ARCH, "-lineinfo", "-Xcompiler", "-fPIC,-O3",
-           "-shared", "-I", INC, "-I", CSRC, "-o", ENGINE_LIB, *srcs, *extra]
+    cmd = [nvcc(), "-O3", "-std=c++17", *ARCH, "-lineinfo", "-Xcompiler", "-fPIC,-O3,-fopenmp",
+           "-shared", "-I", INC, "-I", CSRC, "-o", ENGINE_LIB, *srcs, *extra, "-lgomp"]
     _run(cmd)
     return ENGINE_LIB
 

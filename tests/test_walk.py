@@ -210,3 +210,29 @@ def test_walk_all_source_ranges(lo, hi):
     assert got == run({"GG_VPULL": "1", "GG_WALK_ALL_MB": "0"})
     o = O.bfs_pull(adj, np.arange(lo, hi))
     assert got[0] == o.total() and got[1] == o.levels
+
+
+@pytest.mark.parametrize("Mx,My,walk", [(64, 64, 3), (128, 64, -1)])
+def test_walk_all_lifted_corner_tiles(Mx, My, walk):
+    """walk_all_kernel on a piece lift (sources = the corner tile's vertices, found
+    through the inverse list) with 4096-source batches: 4096 representatives with the
+    walk forced, and 8192 with the default plan (two batches)."""
+    Nx, Ny, Mx, My, vals = G.piece_lift(Mx, My, 2, 2, 8, 5)
+
+    def run(env):
+        old = {k: os.environ.get(k) for k in env}
+        os.environ.update(env)
+        try:
+            return G.cudaASPLpiece(Nx, Ny, Mx, My, 8, 0).diameterASPL(vals)
+        finally:
+            for k, v in old.items():
+                if v is None:
+                    del os.environ[k]
+                else:
+                    os.environ[k] = v
+
+    env = {} if walk < 0 else {"GG_WALK_LEVELS": str(walk)}
+    got = run(env)
+    assert got == run({**env, "GG_WALK_ALL_MB": "0"})
+    assert got == run({"GG_WALK_LEVELS": "0"})
+    assert got == O.piece_diameter_aspl(Nx, Ny, Mx, My, vals)

@@ -24,7 +24,7 @@ calculator with the reference's level cap of 199 (cudaASPLgraph.cu:163).
              against MEASURED_PEAKS.json hbm_gbs.  Beside it: "l2_gather", the
              live ceiling of the kernel's access pattern (gg_gather_peak: random
              512-byte row gathers from L2-resident arrays, one dense BFS level per
-             pass), and "algorithmic", the survey's bytes-per-level count.
+             pass), and "algorithmic", the bytes-per-level count N*d*4 + N*(d+2)*S/8.
 * cpu_baseline  the oracle port (oracle/gg_oracle.c, a restatement of
              cpuASPLqueue) over all host cores; rank 0, N = 1.
 

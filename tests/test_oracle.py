@@ -56,7 +56,7 @@ def test_kat_complete_bipartite(a, b):
     assert (r.levels, r.total()) == I.kat_complete_bipartite(a, b)
 
 
-def test_cycle_as_part_matches_survey_value():
+def test_cycle_as_part_matches_reference_value():
     # C8 -> diameter 4, ASPL 16/7 (value recorded from the reference cpuASPLqueue<1024>)
     N, M, diffs = I.plain_as_part(I.cycle(8))
     d, a = O.queue_diameter_aspl(N, M, diffs)

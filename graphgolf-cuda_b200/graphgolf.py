@@ -97,6 +97,7 @@ _SIGS = {
     "gg_autotune": [_P, _P, _I, _IP, _DP],
     "gg_set_wait_limit_ms": [_P, _I],
     "gg_gather_peak": [_I, _I, _I, _I, _DP, _DP],
+    "gg_level_probe": [_I, _I, _I, _I, _I, _DP],
     "gg_engine_plan": [_P, _IP, _IP, _IP],
     "gg_set_tune_cache": [ctypes.c_char_p],
     "gg_batch_autotune": [_P, _I, _P, _I, _DP],
@@ -754,6 +755,16 @@ def gather_peak(rows=65536, degree=8, iters=20, device=0):
     g, ms = ctypes.c_double(), ctypes.c_double()
     _check(lib().gg_gather_peak(device, rows, degree, iters, ctypes.byref(g), ctypes.byref(ms)))
     return g.value, ms.value
+
+
+def level_probe(rows=65536, chunks=32, levels=40, variant=0, device=0):
+    """Dense level loop outside the engine (gg_level_probe): -> microseconds a
+    level for rows of `chunks` x 16 bytes (32: 4096 sources, 16: 2048), 8 gathers
+    a row, counts, flag words and the grid barrier; variant 1 keeps a second row
+    in flight a warp through cp.async."""
+    us = ctypes.c_double()
+    _check(lib().gg_level_probe(device, rows, chunks, levels, variant, ctypes.byref(us)))
+    return us.value
 
 
 def apply_swap(adj, s):

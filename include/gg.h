@@ -172,6 +172,19 @@ gg_status gg_set_wait_limit_ms(gg_engine *e, int ms);
  * ceiling of a dense level of a 4096-source batch on n = 65536. */
 gg_status gg_gather_peak(int device, int rows, int degree, int iters, double *gbs, double *ms_per_pass);
 
+/* Level-loop microbenchmark (no reference counterpart): the dense level loop of
+ * bfs_batch_kernel outside the engine.  One cooperative launch runs `levels`
+ * levels over `rows` rows of `chunks` x 16 bytes (chunks 32: 4096 sources a
+ * batch, 16: 2048; two such arrays ping-ponged): each row ORs 8 neighbour rows
+ * (8 random permutations, so every row is gathered 8 times a level), writes the
+ * result, its popcount, flag and not-full words; the engine's grid barrier ends
+ * each level.  variant 0 gathers into registers as the engine does; variant 1
+ * also keeps a second row in flight a warp through cp.async into shared memory.
+ * Returns the best of 4 launches' mean time a level (device timestamps, levels
+ * 10.. of each launch) in microseconds.  64 <= rows <= 262144, 12 <= levels <=
+ * 1024. */
+gg_status gg_level_probe(int device, int rows, int chunks, int levels, int variant, double *us_per_level);
+
 gg_status gg_destroy(gg_engine *e);
 
 /* ---- evaluation without device allocation --------------------------------

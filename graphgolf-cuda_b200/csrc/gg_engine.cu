@@ -115,6 +115,7 @@ struct gg_engine {
     int walk_K = 0;                      // levels computed by the walk pass (0: off)
     int walk_vpull = 1;                  // levels after the walk pull visited sets (GG_VPULL=0: frontiers)
     int walk_own_skip = 1;               // dense ones skip own chunks on tables without one-way entries (GG_OWN_SKIP)
+    int walk_third = 1;                  // after the walk of all batches, levels alternate V and F0 (GG_WALK_THIRD)
     int walk_rpg = 1;                    // rows per walk group
     unsigned walk_smem_off = 0;          // byte offset of the walk buffers in dynamic smem
     int32_t *d_h2 = nullptr;             // [rows][d*d] level-2 walk ends (walk_K >= 3)
@@ -557,6 +558,7 @@ gg_status create_common(gg_engine *e) {
     e->split_ppm = env_int("GG_SPLIT_PPM", e->split_ppm);
     e->walk_vpull = env_int("GG_VPULL", e->walk_vpull) != 0;
     e->walk_own_skip = env_int("GG_OWN_SKIP", e->walk_own_skip) != 0;
+    e->walk_third = env_int("GG_WALK_THIRD", e->walk_third) != 0;
     e->walk_all_mb = env_int("GG_WALK_ALL_MB", (int)e->walk_all_mb);
     e->push_ppm = env_int("GG_PUSH_PPM", e->push_ppm);
     e->push_min_items = env_int("GG_PUSH_MIN_ITEMS", e->push_min_items);
@@ -768,6 +770,7 @@ gg_status run_eval(gg_engine *e, const int32_t *d_table_in, const gg_eval_opts *
         a.vtot = e->d_vtot;
         a.vall = wall ? e->d_vall : nullptr;
         a.vall_fl = wall ? e->d_vall_fl : nullptr;
+        a.third = wall && e->walk_third ? e->d_F0 : nullptr;
         void *args[] = {&a};
         GG_CK(cudaLaunchCooperativeKernel(kernel_for(e->d, a.planes != nullptr), dim3(e->grid), dim3(gg::kBlock), args,
                                           wall ? (size_t)e->walk_smem_off : e->smem_bytes, q));

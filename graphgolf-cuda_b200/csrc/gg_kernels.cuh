@@ -149,10 +149,15 @@ struct BfsArgs {
     const int *walk_asym;
     unsigned long long *vtot;   // [nb][3], zeroed by the host
     // walk_all_kernel's output (nullptr: a walk pass per batch): the level-K visited
-    // rows of batch b at vall + b * items (the batch's levels then alternate between
-    // that slice and V) and the level-K frontier flag words at vall_fl + b * tiles.
+    // rows of batch b at vall + b * items and the level-K frontier flag words at
+    // vall_fl + b * tiles.  Level K+1 reads the slice and writes V; the levels after
+    // it alternate between V and `third` (when set), which level K+2 writes whole,
+    // so the slice is only read and every batch writes the same two buffers.
+    // Without `third`, or when level K+2 is a skip-full level (not written whole),
+    // they alternate between the slice and V.
     uint4 *vall;
     const uint32_t *vall_fl;
+    uint4 *third;
 };
 
 // Where a level's new pairs go in the distance planes.
@@ -1571,6 +1576,8 @@ struct LoopState {
     int L_next;                  // first level the level loop runs (after a walk pass)
     int sym;                     // the table has no one-way entries (walk_asym read 0)
     uint4 *Pv, *Qv;              // the batch's visited-set pull buffers (Pv holds level walk_K)
+    uint4 *Rv;                   // the buffer levels walk_K+2.. alternate with Qv, when r_on
+    int r_on;                    // level walk_K + 2 wrote Rv whole (set by that level)
     const uint32_t *fl_walk;     // the flag words level walk_K + 1 reads
     unsigned long long *vt;      // the batch's 3 level totals (a.vtot + 3b), or nullptr
 };
@@ -1723,6 +1730,7 @@ __device__ __forceinline__ void walk_state(const BfsArgs &a, const int b, const 
         S.L_next = S.done ? L : K + 1;
         S.Pv = a.vall ? a.vall + (size_t)b * a.items : a.V;
         S.Qv = a.vall ? a.V : a.F0;
+        S.Rv = a.vall && a.third ? a.third : S.Pv;
         S.vt = a.vtot ? a.vtot + 3 * (size_t)b : nullptr;
         S.fl_walk = a.vall ? a.vall_fl + (size_t)b * ((a.items + 31u) >> 5) : (((K + 1) & 1) ? a.fl0 : a.fl1);
         if (b == 0 && a.level_ns && blockIdx.x == 0)
@@ -1941,21 +1949,35 @@ __global__ void __launch_bounds__(kBlock, min_blocks_for(D)) bfs_batch_kernel(co
                 if constexpr (D > 0 && 32 % D == 0) cnt = push_level<D, PL>(a.adj, a.V, a.div_nc, (unsigned)a.nC, Pc, Pn, pfc, pfn, ntiles,
                                            gtid, nthr);
             } else if (vp) {
-                // V_{L-1} alternates between S.Pv (level walk_K: the walk's V, or the
-                // batch's walk_all_kernel slice) and S.Qv; level walk_K + 1 reads the
-                // walk's flag words
-                const bool x_is_p = ((L - 1 - a.walk_K) & 1) == 0;
-                if (threadIdx.x == 0) s_next = t_lo;
+                // Level walk_K + 1 reads S.Pv (the walk's V, or the batch's
+                // walk_all_kernel slice) and the walk's flag words and writes S.Qv;
+                // later levels alternate between S.Qv and S.Rv, or S.Pv when level
+                // walk_K + 2 cannot write S.Rv whole (a skip-full level)
+                const bool first = L == a.walk_K + 1;
+                bool r_on = false;
+                if (L == a.walk_K + 2) {
+                    r_on = S.Rv != S.Pv && !nf_use;
+                } else {
+                    r_on = S.r_on;   // written by level walk_K + 2 before its barrier
+                }
+                uint4 *R = r_on ? S.Rv : S.Pv;
+                const bool even = ((L - a.walk_K) & 1) == 0;
+                const uint4 *X = first ? S.Pv : (even ? S.Qv : R);
+                uint4 *Y = first ? S.Qv : (even ? R : S.Qv);
+                if (threadIdx.x == 0) {
+                    s_next = t_lo;
+                    if (L == a.walk_K + 2) S.r_on = r_on;
+                }
                 __syncthreads();
                 if (D > 0 && no_own && !nf_use && a.nC == 32)
-                    cnt = dense_rows32<(D > 0 ? D : 1)>(x_is_p ? S.Pv : S.Qv, x_is_p ? S.Qv : S.Pv, adj, v_base,
-                                                        t_hi, odd ? a.fl1 : a.fl0, odd ? a.nf2 : a.nf, split,
-                                                        &s_next);
+                    cnt = dense_rows32<(D > 0 ? D : 1)>(X, Y, adj, v_base, t_hi, odd ? a.fl1 : a.fl0,
+                                                        odd ? a.nf2 : a.nf, split, &s_next);
                 else
-                    cnt = vpull_level<D>(a, d, adj, v_base, t_hi, x_is_p ? S.Pv : S.Qv, x_is_p ? S.Qv : S.Pv,
-                                         L == a.walk_K + 1 ? S.fl_walk : (odd ? a.fl0 : a.fl1), odd ? a.fl1 : a.fl0,
-                                         odd ? a.nf : a.nf2, odd ? a.nf2 : a.nf, dense, L == a.walk_K + 1,
-                                         skip_full, split, nf_use, no_own, &s_next);
+                    cnt = vpull_level<D>(a, d, adj, v_base, t_hi, X, Y,
+                                         first ? S.fl_walk : (odd ? a.fl0 : a.fl1), odd ? a.fl1 : a.fl0,
+                                         odd ? a.nf : a.nf2, odd ? a.nf2 : a.nf, dense,
+                                         first || (L == a.walk_K + 2 && r_on), skip_full, split, nf_use, no_own,
+                                         &s_next);
             } else {
                 const uint4 *Fc = in_p >= 0 ? (in_p ? a.P1 : a.P0) : (odd ? a.F0 : a.F1);
                 const uint32_t *fc = in_p >= 0 ? (in_p ? a.pf1 : a.pf0) : (odd ? a.fl0 : a.fl1);

@@ -183,6 +183,36 @@ def test_walk_all_batches_at_once(n, d, seed, walk):
     assert np.array_equal(np.asarray(got[5][:o.levels + 1]), o.level_counts[:o.levels + 1])
 
 
+@pytest.mark.parametrize("n,d,seed,walk,env,one_way", [
+    (12288, 8, 51, 3, {}, False),
+    (9000, 4, 52, 3, {}, False),
+    (8192, 8, 53, 1, {}, False),
+    (12288, 8, 54, 3, {}, True),
+    # skip-full from the first levels on: level K+2 cannot be written whole, so
+    # the batch keeps alternating with its walk slice
+    (12288, 8, 55, 3, {"GG_FULL_SKIP_PPM": "1000"}, False),
+    (12288, 8, 56, 2, {"GG_FULL_SKIP_PPM": "1000", "GG_SPLIT_PPM": "1000"}, False),
+])
+def test_walk_all_third_buffer(n, d, seed, walk, env, one_way):
+    """After the walk of all batches, levels K+2.. alternate between V and a third
+    buffer (level K+2 written whole) instead of the batch's walk slice; with and
+    without it (GG_WALK_THIRD) the counts must equal the per-batch walk pass and
+    the oracle, on one-way tables and when level K+2 is a skip-full level too."""
+    adj = G.random_regular(n, d, seed).copy()
+    if one_way:
+        v = 901
+        w = next(x for x in range(n) if x != v and x not in adj[v] and v not in adj[x] and x != int(adj[v, 0]))
+        adj[v, 0] = w
+    base = {"GG_VPULL": "1", **env}
+    on = counts_with_env({**base, "GG_WALK_THIRD": "1"}, walk, n, d, 4096, adj)
+    off = counts_with_env({**base, "GG_WALK_THIRD": "0"}, walk, n, d, 4096, adj)
+    per_batch = counts_with_env({**base, "GG_WALK_ALL_MB": "0"}, walk, n, d, 4096, adj)
+    assert on == off == per_batch
+    o = O.bfs_pull(adj, np.arange(n))
+    assert on[0] == o.total() and on[2] == o.levels
+    assert np.array_equal(np.asarray(on[5][:o.levels + 1]), o.level_counts[:o.levels + 1])
+
+
 @pytest.mark.parametrize("lo,hi", [(0, 8192), (4096, 12288), (1000, 9600), (300, 4500)])
 def test_walk_all_source_ranges(lo, hi):
     """Source sub-ranges (not every vertex a source): walk_all_kernel counts levels
